@@ -1,0 +1,315 @@
+"""Benchmark: FEM element-steps/s of the explicit 2D FEM step on B200.
+
+Default workload (N=1): the plain large single mesh -- unit square at (0, 0.2),
+256 x 256 quads split in two (131072 triangles, 66049 nodes), NeoHookean
+E=1e5 nu=0.35 rho=100, v0 = (0, -0.5) + N(0, 0.01^2), height field of 4096
+samples (8 sinusoids, amplitude 0.05), adaptive (static CFL) dt.  One bench
+"step" is one ``advanceWithTime(1/60)`` frame (548 substeps at dt = 3.04e-5);
+L2 is flushed (256 MiB write) between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank steps its own replica of the
+workload (weak scaling; the bodies of different ranks never interact, so there
+is no collective on the data path).  ``--impl reference`` times the CPU
+restatement of the reference's scheme (the reference itself, Python + NVIDIA
+Warp, is not installable here) on this host's cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+FRAME = 1.0 / 60.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mesh", type=int, default=256, help="quads per side of the large mesh")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(fw, mesh):
+    from tests import scenes
+
+    return scenes.plain_large_scene(fw, n=mesh)
+
+
+def algorithmic_bytes_per_substep(n_nodes, n_elems, n_j2, n_contact_nodes, ground_bytes):
+    """Compulsory traffic of one substep: nodes read+write x, v and read the
+    inverse mass (36 B); elements read connectivity (12), Dm^-1 (16), rest area
+    (4) and the two Lame constants (8) = 40 B; J2 elements read+write eps_p and
+    eqps (32 B); each boundary contact item reads a node id and a penalty (8);
+    ground tables once (height field 4 B/sample)."""
+    return 36 * n_nodes + 40 * n_elems + 32 * n_j2 + 8 * n_contact_nodes + ground_bytes
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._ok = False
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(device_index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            self._h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self._nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._ok = True
+        except Exception as e:  # pragma: no cover - depends on the box
+            self.error = str(e)
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and bit != 0x1:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.05)
+
+    def __enter__(self):
+        if self._ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._ok:
+            self._t.join()
+
+    def summary(self):
+        if not self._ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "note": getattr(self, "error", "no samples")}
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-substep DRAM bytes of the step kernels from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic_plain_large.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_substep")
+    return None
+
+
+def cpu_oracle_rate(fw, mesh, seconds, threads):
+    """Element-steps/s of the CPU restatement on this host (bounded sample)."""
+    import oracle
+
+    o = oracle.OracleLoop(workload(fw, mesh), 0.0, useAdapativeDT=True, precision="f32", threads=threads)
+    o.advance(3)
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds:
+        o.advance(5)
+        n += 5
+    dt = time.perf_counter() - t0
+    return o.E * n / dt, n
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import flatworld_b200 as fw
+
+    threads = os.cpu_count() or 1
+    import oracle
+
+    o = oracle.OracleLoop(workload(fw, args.mesh), 0.0, useAdapativeDT=True, precision="f32", threads=threads)
+    sample = 50  # substeps per bench step: a bounded sample of one frame
+    for _ in range(args.warmup):
+        o.advance(sample)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.advance(sample)
+    el = time.perf_counter() - t0
+    value = o.E * sample * args.steps / el
+    line = {
+        "impl": "reference", "metric": "FEM element-steps/s", "value": value, "unit": "element-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain large single mesh {args.mesh}x{args.mesh} quads, NeoHookean, height field",
+                   "elements": o.E, "nodes": o.N, "substeps_per_step": sample, "dt": o.dt},
+        "cpu_baseline": {"value": value, "unit": "element-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} substeps per step x {args.steps} steps of the workload, FP32 C "
+                                   f"restatement of the reference scheme, {threads} threads"},
+        "e2e": {"value": value, "unit": "element-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+
+    import flatworld_b200 as fw
+    from flatworld_b200.world import substep_schedule
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    domains = workload(fw, args.mesh)
+    loop = fw.ExplicitLoop(0.0, domains, useAdapativeDT=True, device=local)
+    stream = torch.cuda.Stream()
+    loop._native.set_stream(stream.cuda_stream)
+    fsm = loop.femSpringManager
+    N = int(fsm.totalNodes.numpy()[0])
+    E = int(fsm.totalElements.numpy()[0])
+    runs = substep_schedule(FRAME, loop.stableTime, loop.default_dt, True)
+    substeps = sum(n for n, _ in runs)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            loop.advanceWithTime(FRAME)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = loop.launch_count()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                loop.advanceWithTime(FRAME)
+                ends[k].record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        launches = loop.launch_count() - launches0
+        ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+        # ---- end to end: host state in, one frame, host state out (pinned)
+        xh = torch.empty((N, 2), dtype=torch.float32, pin_memory=True)
+        vh = torch.empty((N, 2), dtype=torch.float32, pin_memory=True)
+        loop._native.read_nodes_ptr(0, 0, N, xh.data_ptr())
+        loop._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
+        e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            e_s[k].record(stream)
+            loop._native.write_nodes_ptr(0, 0, N, xh.data_ptr())
+            loop._native.write_nodes_ptr(1, 0, N, vh.data_ptr())
+            loop.advanceWithTime(FRAME)
+            loop._native.read_nodes_ptr(0, 0, N, xh.data_ptr())
+            loop._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
+            e_e[k].record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = sum(s.elapsed_time(e) for s, e in zip(e_s, e_e))
+    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = float(t[0]), float(t[1])
+    if rank == 0:
+        work = world * E * substeps * args.steps
+        value = work / (ms / 1e3)
+        e2e = work / (ms_e2e / 1e3)
+        nb = sum(d.mesh.numBoundNodes for d in loop._layout.fem)
+        ground = sum(4 * c.ground.nx for c in loop._layout.pairs if c.kind == "heightfield")
+        bstep = algorithmic_bytes_per_substep(N, E, 0, nb * len(loop._layout.pairs), ground)
+        per_sub_s = (ms / 1e3) / (substeps * args.steps)
+        achieved = bstep / per_sub_s / 1e9
+        peak, which = peaks()
+        traffic = ncu_traffic()
+        line = {
+            "metric": "FEM element-steps/s", "value": value, "unit": "element-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded mesh, velocities and height field)",
+            "config": {"workload": f"plain large single mesh {args.mesh}x{args.mesh} quads, NeoHookean, "
+                                   f"height field 4096 samples",
+                       "elements": E, "nodes": N, "step": "advanceWithTime(1/60)",
+                       "substeps_per_step": substeps, "dt": loop.stableTime,
+                       "l2": "flushed between steps (256 MiB write)", "replicas": world},
+            "roofline": {"bound": "hbm", "kernel": "substep = k_elements + k_nodes",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": which, "algorithmic_bytes_per_substep": bstep,
+                         "us_per_substep": per_sub_s * 1e6,
+                         "traffic": traffic},
+            "e2e": {"value": e2e, "unit": "element-steps/s", "h2d_bytes_per_step": 2 * N * 8,
+                    "d2h_bytes_per_step": 2 * N * 8},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            rate, n = cpu_oracle_rate(fw, args.mesh, args.cpu_seconds, threads)
+            line["cpu_baseline"] = {"value": rate, "unit": "element-steps/s", "cores": threads, "kind": "port",
+                                    "sample": f"{n} substeps of the same workload, FP32 C restatement of the "
+                                              f"reference scheme, {threads} threads"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+"""ctypes binding of libfwb200.so (include/fwb200.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+visible, constructing a ``NativeWorld`` raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+FW_FIELD_X = 0
+FW_FIELD_V = 1
+FW_FIELD_MASS = 2
+FW_FIELD_X0 = 3
+
+_lock = threading.Lock()
+_lib = None
+
+_f32p = C.POINTER(C.c_float)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_vp = C.c_void_p
+
+_SIGNATURES = {
+    "fw_create": (C.c_int, [C.POINTER(_vp), C.c_int]),
+    "fw_destroy": (None, [_vp]),
+    "fw_last_error": (C.c_char_p, [_vp]),
+    "fw_set_stream": (C.c_int, [_vp, _vp]),
+    "fw_set_nodes": (C.c_int, [_vp, C.c_int32, _f32p, _f32p, _i32p, _f32p]),
+    "fw_set_elements": (C.c_int, [_vp, C.c_int32, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p, _f32p]),
+    "fw_set_bodies": (C.c_int, [_vp, C.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, C.c_int32, _i32p]),
+    "fw_set_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
+    "fw_add_plane_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "fw_add_heightfield_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, _f32p, C.c_float, C.c_float, C.c_int32]),
+    "fw_add_voxel_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, C.c_int32, _i32p, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "fw_finalize": (C.c_int, [_vp]),
+    "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
+    "fw_step_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
+    "fw_set_active": (C.c_int, [_vp, _i32p]),
+    "fw_synchronize": (C.c_int, [_vp]),
+    "fw_read_nodes": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32]),
+    "fw_write_nodes": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32]),
+    "fw_read_aabb": (C.c_int, [_vp, _f32p]),
+    "fw_read_plastic": (C.c_int, [_vp, _f32p, _f32p]),
+    "fw_read_reference_shape": (C.c_int, [_vp, _f32p, _f32p]),
+    "fw_read_counters": (C.c_int, [_vp, _i64p]),
+    "fw_launch_count": (C.c_int64, [_vp]),
+    "fw_build_info": (C.c_char_p, []),
+}
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def lib():
+    """Load libfwb200.so (built in-tree) and declare every entry point."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = _build.lib_path()
+            if not os.path.exists(path):
+                raise RuntimeError(
+                    f"{path} is not built; run `python -m flatworld_b200.build` "
+                    "(or __graft_entry__.build()) -- there is no CPU fallback")
+            handle = C.CDLL(path)
+            for name, (res, args) in _SIGNATURES.items():
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = handle
+        return _lib
+
+
+def _f(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(_f32p)
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_i32p)
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+class NativeWorld:
+    """Owner of one fw_ctx (device buffers of a packed world)."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = _vp()
+        rc = self._L.fw_create(C.byref(h), int(device))
+        if rc != 0:
+            raise NativeError(
+                f"fw_create(device={device}) failed with code {rc}: no usable CUDA device "
+                "(flatworld_b200 runs on the GPU only)")
+        self._h = h
+        self.device = device
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self._L.fw_last_error(self._h)
+            raise NativeError(f"{what}: {msg.decode() if msg else ''} (code {rc})")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fw_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    # ---- construction
+    def set_nodes(self, coords, vel, bc_bits, bc_values):
+        n = len(coords)
+        keep = [_f(coords), _f(vel), _i(bc_bits), _f(bc_values)]
+        self._check(self._L.fw_set_nodes(self._h, n, keep[0][1], keep[1][1], keep[2][1], keep[3][1]), "fw_set_nodes")
+
+    def set_elements(self, conn, mtype, E, nu, rho, sy, H):
+        k = [_i(conn), _i(mtype), _f(E), _f(nu), _f(rho), _f(sy), _f(H)]
+        self._check(self._L.fw_set_elements(self._h, len(mtype), *[x[1] for x in k]), "fw_set_elements")
+
+    def set_bodies(self, noff, ncnt, eoff, ecnt, scene, bnoff, bncnt, bnodes):
+        k = [_i(noff), _i(ncnt), _i(eoff), _i(ecnt), _i(scene), _i(bnoff), _i(bncnt)]
+        bn = _i(bnodes)
+        self._check(self._L.fw_set_bodies(self._h, len(noff), *[x[1] for x in k], len(bn[0]), bn[1]), "fw_set_bodies")
+
+    def set_scenes(self, damping):
+        d = _f(damping)
+        self._check(self._L.fw_set_scenes(self._h, len(d[0]), d[1]), "fw_set_scenes")
+
+    def add_plane(self, body, penalty, lo, hi, p, n):
+        lo, hi = _f(lo), _f(hi)
+        self._check(self._L.fw_add_plane_pair(self._h, body, penalty, lo[1], hi[1], float(p[0]), float(p[1]),
+                                              float(n[0]), float(n[1])), "fw_add_plane_pair")
+
+    def add_heightfield(self, body, penalty, lo, hi, heights, lbx, ubx, reverse):
+        lo, hi, h = _f(lo), _f(hi), _f(heights)
+        self._check(self._L.fw_add_heightfield_pair(self._h, body, penalty, lo[1], hi[1], len(h[0]), h[1],
+                                                    float(lbx), float(ubx), int(reverse)), "fw_add_heightfield_pair")
+
+    def add_voxel(self, body, penalty, lo, hi, occ, lbx, lby, dx, dz):
+        lo, hi = _f(lo), _f(hi)
+        o = _i(occ)
+        nx, ny = occ.shape
+        self._check(self._L.fw_add_voxel_pair(self._h, body, penalty, lo[1], hi[1], nx, ny, o[1], float(lbx),
+                                              float(lby), float(dx), float(dz)), "fw_add_voxel_pair")
+
+    def finalize(self):
+        self._check(self._L.fw_finalize(self._h), "fw_finalize")
+
+    # ---- stepping
+    def step(self, n: int, dt: float):
+        self._check(self._L.fw_step(self._h, int(n), float(np.float32(dt))), "fw_step")
+
+    def step_scenes(self, n: int, dt_per_scene):
+        d = _f(dt_per_scene)
+        self._check(self._L.fw_step_scenes(self._h, int(n), d[1]), "fw_step_scenes")
+
+    def set_active(self, active):
+        a = _i(active)
+        self._check(self._L.fw_set_active(self._h, a[1]), "fw_set_active")
+
+    def synchronize(self):
+        self._check(self._L.fw_synchronize(self._h), "fw_synchronize")
+
+    # ---- readback
+    def read_nodes(self, field: int, first: int, count: int) -> np.ndarray:
+        width = 1 if field == FW_FIELD_MASS else 2
+        out = np.empty((count, width), dtype=np.float32)
+        self._check(self._L.fw_read_nodes(self._h, field, first, count, out.ctypes.data, 0), "fw_read_nodes")
+        return out if width == 2 else out[:, 0]
+
+    def read_nodes_ptr(self, field: int, first: int, count: int, dst_ptr: int, on_device: bool = False):
+        """Read into caller memory (host pointer, pinned or not, or a device pointer)."""
+        self._check(self._L.fw_read_nodes(self._h, field, first, count, dst_ptr, 1 if on_device else 0),
+                    "fw_read_nodes")
+
+    def write_nodes_ptr(self, field: int, first: int, count: int, src_ptr: int, on_device: bool = False):
+        self._check(self._L.fw_write_nodes(self._h, field, first, count, src_ptr, 1 if on_device else 0),
+                    "fw_write_nodes")
+
+    def set_stream(self, stream_ptr: int | None):
+        """Queue this world's work on a caller CUDA stream (None: own stream)."""
+        self._check(self._L.fw_set_stream(self._h, stream_ptr or None), "fw_set_stream")
+
+    def write_nodes(self, field: int, first: int, values: np.ndarray):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        self._check(self._L.fw_write_nodes(self._h, field, first, len(v), v.ctypes.data, 0), "fw_write_nodes")
+
+    def read_aabb(self, n_bodies: int) -> np.ndarray:
+        out = np.empty((n_bodies, 4), dtype=np.float32)
+        self._check(self._L.fw_read_aabb(self._h, out.ctypes.data_as(_f32p)), "fw_read_aabb")
+        return out
+
+    def read_plastic(self, n_elems: int):
+        ep = np.empty((n_elems, 3), dtype=np.float32)
+        eq = np.empty((n_elems,), dtype=np.float32)
+        self._check(self._L.fw_read_plastic(self._h, ep.ctypes.data_as(_f32p), eq.ctypes.data_as(_f32p)), "fw_read_plastic")
+        return ep, eq
+
+    def read_reference_shape(self, n_elems: int):
+        area = np.empty((n_elems,), dtype=np.float32)
+        jinv = np.empty((n_elems, 4), dtype=np.float32)
+        self._check(self._L.fw_read_reference_shape(self._h, area.ctypes.data_as(_f32p), jinv.ctypes.data_as(_f32p)),
+                    "fw_read_reference_shape")
+        return area, jinv
+
+    def read_counters(self, n_scenes: int) -> np.ndarray:
+        out = np.empty((n_scenes,), dtype=np.int64)
+        self._check(self._L.fw_read_counters(self._h, out.ctypes.data_as(_i64p)), "fw_read_counters")
+        return out
+
+    def launch_count(self) -> int:
+        return int(self._L.fw_launch_count(self._h))

@@ -1,0 +1,850 @@
+// fw_world.cu -- C ABI (include/fwb200.h) and the general ("gather") step of
+// the explicit 2D FEM world: any number of scenes, bodies and contact pairs.
+//
+// Per substep two kernels run on the context stream:
+//   k_elements  one thread per triangle: deformation gradient, PK2 stress
+//               (elastic / NeoHookean / J2 radial return), the three corner
+//               forces -(B^T S)A written to a corner buffer.  Block 0 first
+//               runs the per-step control (scene modes, broad-phase gates,
+//               step counters, AABB slot reset).
+//   k_nodes     one thread per node: penalty contact (boundary nodes only),
+//               the node's corner forces summed in ascending element order,
+//               boundary conditions, symplectic Euler, and the per-body AABB of
+//               boundary nodes (warp reduction + ordered-int atomics).
+// Summing a node's corners in ascending element order after its contact terms
+// is exactly the order in which the reference's serial CPU path applies its
+// atomic adds (flatworld/mixedcontact.py:1654-1755 then
+// flatworld/femspringmanager.py:217-280), so the sum is deterministic and
+// identical run to run, with no float atomics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fwb200.h"
+#include "fw_device.cuh"
+
+using fw::ElemMat;
+using fw::Pair;
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kGraphSteps = 32;
+
+struct Dev {
+  float2* x;
+  float2* v;
+  float2* x0;
+  float2* bcv;
+  float2* corner;
+  uint32_t* node_word;
+  float* mass;
+  int32_t* csr_off;
+  int32_t* csr_slot;
+  int32_t* conn;
+  float4* jinv;
+  ElemMat* emat;
+  float2* j2par;
+  float4* j2state;
+  float* ndmass;
+  int32_t* body_scene;
+  int32_t* body_pair_off;
+  int32_t* body_pair_cnt;
+  Pair* pairs;
+  int32_t* pair_active;
+  float* heights;
+  int8_t* occ;
+  float* scene_dt;
+  float* scene_damp;
+  int32_t* scene_counter;
+  int32_t* scene_active;
+  int32_t* scene_mode_req;
+  int32_t* scene_mode;
+  int32_t* aabb_ring;  // [2][B][4] ordered ints
+  int N, E, B, S, P;
+  int has_j2;
+  // uniform_dt != 0: every scene steps dt_uniform (kernel argument, baked into
+  // the captured graph); otherwise scene_dt[] holds one dt per scene.
+  int uniform_dt;
+  float dt_uniform;
+};
+
+// ------------------------------------------------------------------ kernels
+
+__device__ void step_control(const Dev& d) {
+  const int t = threadIdx.x;
+  for (int s = t; s < d.S; s += blockDim.x) {
+    const int act = d.scene_active[s];
+    const int req = d.scene_mode_req[s];
+    d.scene_mode[s] = act ? (req ? fw::MODE_INIT : fw::MODE_STEP) : fw::MODE_FROZEN;
+    if (act && req) d.scene_mode_req[s] = 0;
+  }
+  __syncthreads();
+  for (int p = t; p < d.P; p += blockDim.x) {
+    const Pair& pr = d.pairs[p];
+    const int s = d.body_scene[pr.body];
+    if (d.scene_mode[s] != fw::MODE_STEP) continue;
+    const int k = d.scene_counter[s];
+    const int* r = d.aabb_ring + ((size_t)(k & 1) * d.B + pr.body) * 4;
+    d.pair_active[p] = fw::pair_gate(pr, fw::ord2f(r[0]), fw::ord2f(r[1]), fw::ord2f(r[2]),
+                                     fw::ord2f(r[3]), k) ? 1 : 0;
+  }
+  __syncthreads();
+  for (int s = t; s < d.S; s += blockDim.x)
+    if (d.scene_mode[s] == fw::MODE_STEP) d.scene_counter[s] += 1;
+  __syncthreads();
+  for (int b = t; b < d.B; b += blockDim.x) {
+    const int s = d.body_scene[b];
+    if (d.scene_mode[s] == fw::MODE_FROZEN) continue;
+    int* r = d.aabb_ring + ((size_t)(d.scene_counter[s] & 1) * d.B + b) * 4;
+    r[0] = fw::f2ord(1e30f);
+    r[1] = fw::f2ord(1e30f);
+    r[2] = fw::f2ord(-1e30f);
+    r[3] = fw::f2ord(-1e30f);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_elements(Dev d) {
+  if (blockIdx.x == 0) step_control(d);
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) {
+    const ElemMat m = d.emat[e];
+    const int s = d.body_scene[fw::elem_body(m.word)];
+    if (!d.scene_active[s]) continue;
+    const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
+    const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
+    const float4 ji = d.jinv[e];
+    float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float sy = 0.f, H = 0.f;
+    const bool mises = fw::elem_type(m.word) == fw::MAT_MISES;
+    if (mises) {
+      j2 = d.j2state[e];
+      const float2 q = d.j2par[e];
+      sy = q.x;
+      H = q.y;
+    }
+    float2 f1, f2, f3;
+    fw::element_forces(a, b, c, ji, m, sy, H, j2, f1, f2, f3);
+    if (mises) d.j2state[e] = j2;
+    d.corner[3 * e] = f1;
+    d.corner[3 * e + 1] = f2;
+    d.corner[3 * e + 2] = f3;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_nodes(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < d.N;
+  const uint32_t w = valid ? d.node_word[i] : 0u;
+  const int b = (int)(w >> fw::NODE_BODY_SHIFT);
+  const int s = valid ? d.body_scene[b] : 0;
+  const int mode = valid ? d.scene_mode[s] : fw::MODE_FROZEN;
+  const bool live = mode != fw::MODE_FROZEN;
+  bool bnd = false;
+  float2 x = make_float2(0.f, 0.f);
+  if (live) {
+    x = d.x[i];
+    float2 v = d.v[i];
+    const float dt = mode == fw::MODE_INIT ? 0.0f : (d.uniform_dt ? d.dt_uniform : d.scene_dt[s]);
+    const float damp = mode == fw::MODE_INIT ? 0.0f : d.scene_damp[s];
+    float2 f = make_float2(0.f, 0.f);
+    bnd = (w & fw::NODE_BOUNDARY) != 0;
+    if (bnd && mode == fw::MODE_STEP) {
+      const int p0 = d.body_pair_off[b], pn = d.body_pair_cnt[b];
+      for (int k = 0; k < pn; ++k) {
+        if (!d.pair_active[p0 + k]) continue;
+        float2 cf;
+        if (fw::contact_force(d.pairs[p0 + k], d.heights, d.occ, x, v, dt, cf)) {
+          f.x += cf.x;
+          f.y += cf.y;
+        }
+      }
+    }
+    const int k0 = d.csr_off[i], k1 = d.csr_off[i + 1];
+    for (int k = k0; k < k1; ++k) {
+      const float2 c = d.corner[d.csr_slot[k]];
+      f.x += c.x;
+      f.y += c.y;
+    }
+    const int bc = (int)(w & fw::NODE_BC_MASK);
+    const float2 bv = (bc & (fw::BC_A | fw::BC_GRAVITY | fw::BC_FORCE | fw::BC_V))
+                          ? d.bcv[i] : make_float2(0.f, 0.f);
+    fw::integrate(bc, f, d.mass[i], bv, dt, damp, x, v);
+    d.x[i] = x;
+    d.v[i] = v;
+  }
+  // Per-body AABB of boundary nodes (femspringmanager.py:361-408).
+  const unsigned full = 0xFFFFFFFFu;
+  const unsigned mb = __ballot_sync(full, bnd);
+  if (mb == 0u) return;
+  const int leader = __ffs(mb) - 1;
+  const int bl = __shfl_sync(full, b, leader);
+  const bool uniform = __all_sync(full, !bnd || b == bl);
+  float lx = bnd ? x.x : 1e30f, ly = bnd ? x.y : 1e30f;
+  float hx = bnd ? x.x : -1e30f, hy = bnd ? x.y : -1e30f;
+  if (uniform) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lx = fminf(lx, __shfl_xor_sync(full, lx, o));
+      ly = fminf(ly, __shfl_xor_sync(full, ly, o));
+      hx = fmaxf(hx, __shfl_xor_sync(full, hx, o));
+      hy = fmaxf(hy, __shfl_xor_sync(full, hy, o));
+    }
+    if ((int)(threadIdx.x & 31) == leader) {
+      int* r = d.aabb_ring + ((size_t)(d.scene_counter[s] & 1) * d.B + b) * 4;
+      atomicMin(r + 0, fw::f2ord(lx));
+      atomicMin(r + 1, fw::f2ord(ly));
+      atomicMax(r + 2, fw::f2ord(hx));
+      atomicMax(r + 3, fw::f2ord(hy));
+    }
+  } else if (bnd) {
+    int* r = d.aabb_ring + ((size_t)(d.scene_counter[s] & 1) * d.B + b) * 4;
+    atomicMin(r + 0, fw::f2ord(lx));
+    atomicMin(r + 1, fw::f2ord(ly));
+    atomicMax(r + 2, fw::f2ord(hx));
+    atomicMax(r + 3, fw::f2ord(hy));
+  }
+}
+
+// Reference-shape precompute, _prepare_fem_data_kernel
+// (flatworld/femspringmanager.py:113-138), plus the Lame constants of
+// getStress2D (materialfunctions.py:12-13), which depend only on E and nu.
+__global__ void k_prepare_elements(Dev d, const float* __restrict__ young,
+                                   const float* __restrict__ poisson,
+                                   const float* __restrict__ rho) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.E) return;
+  const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
+  const float2 a = d.x0[c0], b = d.x0[c1], c = d.x0[c2];
+  const float j00 = a.x - c.x, j01 = b.x - c.x, j10 = a.y - c.y, j11 = b.y - c.y;
+  const float det = j00 * j11 - j01 * j10;
+  const float area = fabsf(det) * 0.5f;
+  float4 ji = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (det != 0.0f) {
+    const float r = 1.0f / det;
+    ji = make_float4(j11 * r, -j01 * r, -j10 * r, j00 * r);
+  }
+  d.jinv[e] = ji;
+  const float E = young[e], nu = poisson[e];
+  ElemMat m = d.emat[e];
+  m.area = area;
+  m.lam = E * nu / ((1.0f + nu) * (1.0f - 2.0f * nu));
+  m.mu = E / (2.0f * (1.0f + nu));
+  d.emat[e] = m;
+  d.ndmass[e] = area * rho[e] / 3.0f;
+}
+
+// Lumped mass: each node adds its elements' shares in ascending element order,
+// the order of the reference's serial atomic adds.
+__global__ void k_prepare_mass(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  float m = 0.0f;
+  for (int k = d.csr_off[i]; k < d.csr_off[i + 1]; ++k) m += d.ndmass[d.csr_slot[k] / 3];
+  d.mass[i] = m;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ context
+
+struct fw_ctx {
+  int device = 0;
+  std::string err;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  bool finalized = false;
+  int64_t launches = 0;
+  // host staging
+  int N = 0, E = 0, B = 0, S = 0;
+  std::vector<float> h_x, h_v, h_bcv;
+  std::vector<int32_t> h_bc;
+  std::vector<int32_t> h_conn, h_type;
+  std::vector<float> h_E, h_nu, h_rho, h_sy, h_H;
+  std::vector<int32_t> h_noff, h_ncnt, h_eoff, h_ecnt, h_scene, h_bnoff, h_bncnt, h_bnodes;
+  std::vector<float> h_damp;
+  std::vector<Pair> h_pairs;
+  std::vector<float> h_heights;
+  std::vector<int8_t> h_occ;
+  std::vector<float> cur_dt;
+  std::vector<int32_t> cur_active;
+  Dev d{};
+  std::vector<void*> allocs;
+  // captured graphs of kGraphSteps substeps, keyed by (uniform flag, dt bits)
+  std::vector<std::pair<uint64_t, cudaGraphExec_t>> graphs;
+  cudaStream_t graph_stream = nullptr;
+  int grid_e = 1, grid_n = 1;
+};
+
+namespace {
+
+int fail(fw_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define FW_CUDA(ctx, call)                                                                 \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess)                                                                 \
+      return fail((ctx), _e == cudaErrorMemoryAllocation ? FW_ERR_OOM : FW_ERR_CUDA,       \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+  } while (0)
+
+template <typename T>
+int dalloc(fw_ctx* c, T** p, size_t count) {
+  size_t bytes = sizeof(T) * (count ? count : 1);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess)
+    return fail(c, FW_ERR_OOM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  c->allocs.push_back((void*)*p);
+  return FW_OK;
+}
+
+template <typename T>
+int upload(fw_ctx* c, T** p, const std::vector<T>& h) {
+  int rc = dalloc(c, p, h.size());
+  if (rc) return rc;
+  if (!h.empty())
+    FW_CUDA(c, cudaMemcpyAsync(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, c->stream));
+  return FW_OK;
+}
+
+int check_kernel(fw_ctx* c, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, FW_ERR_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
+  return FW_OK;
+}
+
+int launch_step(fw_ctx* c) {
+  k_elements<<<c->grid_e, kBlock, 0, c->stream>>>(c->d);
+  k_nodes<<<c->grid_n, kBlock, 0, c->stream>>>(c->d);
+  c->launches += 2;
+  return check_kernel(c, "step");
+}
+
+void drop_graphs(fw_ctx* c) {
+  for (auto& g : c->graphs) cudaGraphExecDestroy(g.second);
+  c->graphs.clear();
+}
+
+int get_graph(fw_ctx* c, cudaGraphExec_t* out) {
+  if (c->graph_stream != c->stream) {
+    drop_graphs(c);
+    c->graph_stream = c->stream;
+  }
+  uint32_t bits;
+  memcpy(&bits, &c->d.dt_uniform, sizeof(bits));
+  const uint64_t key = ((uint64_t)(c->d.uniform_dt ? 1 : 0) << 32) | (c->d.uniform_dt ? bits : 0u);
+  for (auto& g : c->graphs)
+    if (g.first == key) {
+      *out = g.second;
+      return FW_OK;
+    }
+  if (c->graphs.size() >= 8) drop_graphs(c);
+  cudaGraph_t g = nullptr;
+  FW_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < kGraphSteps; ++k) {
+    k_elements<<<c->grid_e, kBlock, 0, c->stream>>>(c->d);
+    k_nodes<<<c->grid_n, kBlock, 0, c->stream>>>(c->d);
+  }
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+  if (ce != cudaSuccess) return fail(c, FW_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+  cudaGraphExec_t exec = nullptr;
+  ce = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(c, FW_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+  c->graphs.push_back({key, exec});
+  *out = exec;
+  return FW_OK;
+}
+
+int run_steps(fw_ctx* c, int n) {
+  int rc = FW_OK;
+  if (n >= kGraphSteps) {
+    cudaGraphExec_t g = nullptr;
+    rc = get_graph(c, &g);
+    if (rc) return rc;
+    while (n >= kGraphSteps) {
+      FW_CUDA(c, cudaGraphLaunch(g, c->stream));
+      c->launches += 2 * kGraphSteps;
+      n -= kGraphSteps;
+    }
+  }
+  for (int k = 0; k < n && rc == FW_OK; ++k) rc = launch_step(c);
+  return rc;
+}
+
+int set_scene_dt(fw_ctx* c, const float* dt) {
+  bool same = c->cur_dt.size() == (size_t)c->S;
+  for (int s = 0; same && s < c->S; ++s) same = memcmp(&c->cur_dt[s], &dt[s], sizeof(float)) == 0;
+  if (same) return FW_OK;
+  c->cur_dt.assign(dt, dt + c->S);
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_dt, c->cur_dt.data(), sizeof(float) * c->S,
+                             cudaMemcpyHostToDevice, c->stream));
+  // the copy reads c->cur_dt; keep it stable until the copy ran
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+int fw_create(fw_ctx** out, int device) {
+  if (!out) return FW_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return FW_ERR_CUDA;
+  if (device < 0 || device >= ndev) return FW_ERR_ARG;
+  fw_ctx* c = new fw_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return FW_ERR_CUDA;
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return FW_OK;
+}
+
+void fw_destroy(fw_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+const char* fw_last_error(const fw_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int fw_set_stream(fw_ctx* c, void* stream) {
+  if (!c) return FW_ERR_ARG;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return FW_OK;
+}
+
+int fw_set_nodes(fw_ctx* c, int32_t n, const float* coords, const float* vel,
+                 const int32_t* bc_bits, const float* bc_values) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_nodes after fw_finalize");
+  if (n <= 0 || !coords) return fail(c, FW_ERR_ARG, "fw_set_nodes: need n_nodes > 0 and coords");
+  c->N = n;
+  c->h_x.assign(coords, coords + 2 * (size_t)n);
+  c->h_v.assign(2 * (size_t)n, 0.f);
+  if (vel) c->h_v.assign(vel, vel + 2 * (size_t)n);
+  c->h_bc.assign(n, 0);
+  if (bc_bits) c->h_bc.assign(bc_bits, bc_bits + n);
+  c->h_bcv.assign(2 * (size_t)n, 0.f);
+  if (bc_values) c->h_bcv.assign(bc_values, bc_values + 2 * (size_t)n);
+  for (int i = 0; i < n; ++i)
+    if (c->h_bc[i] & ~0x1FF) return fail(c, FW_ERR_ARG, "node %d: bc bits 0x%x outside 0x1FF", i, c->h_bc[i]);
+  return FW_OK;
+}
+
+int fw_set_elements(fw_ctx* c, int32_t n, const int32_t* conn, const int32_t* mat_type,
+                    const float* young, const float* poisson, const float* density,
+                    const float* yield_stress, const float* hardening) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_elements after fw_finalize");
+  if (n <= 0 || !conn || !mat_type || !young || !poisson || !density)
+    return fail(c, FW_ERR_ARG, "fw_set_elements: need n_elems > 0 and conn/type/E/nu/rho");
+  c->E = n;
+  c->h_conn.assign(conn, conn + 3 * (size_t)n);
+  c->h_type.assign(mat_type, mat_type + n);
+  c->h_E.assign(young, young + n);
+  c->h_nu.assign(poisson, poisson + n);
+  c->h_rho.assign(density, density + n);
+  c->h_sy.assign(n, 0.f);
+  c->h_H.assign(n, 0.f);
+  if (yield_stress) c->h_sy.assign(yield_stress, yield_stress + n);
+  if (hardening) c->h_H.assign(hardening, hardening + n);
+  for (int e = 0; e < n; ++e) {
+    const int t = c->h_type[e];
+    if (t != fw::MAT_ELASTIC && t != fw::MAT_NEOHOOKEAN && t != fw::MAT_MISES)
+      return fail(c, FW_ERR_ARG, "element %d: unknown material type %d", e, t);
+  }
+  return FW_OK;
+}
+
+int fw_set_bodies(fw_ctx* c, int32_t nb, const int32_t* noff, const int32_t* ncnt,
+                  const int32_t* eoff, const int32_t* ecnt, const int32_t* scene,
+                  const int32_t* bnoff, const int32_t* bncnt, int32_t n_bnodes,
+                  const int32_t* bnodes) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_bodies after fw_finalize");
+  if (nb <= 0 || !noff || !ncnt || !eoff || !ecnt || !scene || !bnoff || !bncnt)
+    return fail(c, FW_ERR_ARG, "fw_set_bodies: need n_bodies > 0 and all range arrays");
+  if (nb >= (1 << 22)) return fail(c, FW_ERR_ARG, "fw_set_bodies: at most 4194303 bodies");
+  c->B = nb;
+  c->h_noff.assign(noff, noff + nb);
+  c->h_ncnt.assign(ncnt, ncnt + nb);
+  c->h_eoff.assign(eoff, eoff + nb);
+  c->h_ecnt.assign(ecnt, ecnt + nb);
+  c->h_scene.assign(scene, scene + nb);
+  c->h_bnoff.assign(bnoff, bnoff + nb);
+  c->h_bncnt.assign(bncnt, bncnt + nb);
+  c->h_bnodes.assign(bnodes, bnodes + (n_bnodes > 0 ? n_bnodes : 0));
+  return FW_OK;
+}
+
+int fw_set_scenes(fw_ctx* c, int32_t ns, const float* damping) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_scenes after fw_finalize");
+  if (ns <= 0) return fail(c, FW_ERR_ARG, "fw_set_scenes: need n_scenes > 0");
+  c->S = ns;
+  c->h_damp.assign(ns, 0.f);
+  if (damping) c->h_damp.assign(damping, damping + ns);
+  return FW_OK;
+}
+
+static int add_pair(fw_ctx* c, Pair p, const float* lo, const float* hi) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "contact pair added after fw_finalize");
+  if (!lo || !hi) return fail(c, FW_ERR_ARG, "contact pair: gate box required");
+  if (p.body < 0) return fail(c, FW_ERR_ARG, "contact pair: bad body %d", p.body);
+  p.glo[0] = lo[0];
+  p.glo[1] = lo[1];
+  p.ghi[0] = hi[0];
+  p.ghi[1] = hi[1];
+  c->h_pairs.push_back(p);
+  return FW_OK;
+}
+
+int fw_add_plane_pair(fw_ctx* c, int32_t body, float penalty, const float* lo, const float* hi,
+                      float px, float py, float nx, float ny) {
+  Pair p{};
+  p.kind = fw::PAIR_PLANE;
+  p.body = body;
+  p.penalty = penalty;
+  p.f[0] = px;
+  p.f[1] = py;
+  p.f[2] = nx;
+  p.f[3] = ny;
+  return add_pair(c, p, lo, hi);
+}
+
+int fw_add_heightfield_pair(fw_ctx* c, int32_t body, float penalty, const float* lo,
+                            const float* hi, int32_t n_samples, const float* heights, float lb_x,
+                            float ub_x, int32_t reverse) {
+  if (!c) return FW_ERR_ARG;
+  if (n_samples < 2 || !heights)
+    return fail(c, FW_ERR_ARG, "heightfield pair: need >= 2 samples");
+  Pair p{};
+  p.kind = fw::PAIR_HEIGHTFIELD;
+  p.body = body;
+  p.penalty = penalty;
+  p.table = (int)c->h_heights.size();
+  p.n0 = n_samples;
+  p.n1 = reverse ? 1 : 0;
+  p.f[0] = lb_x;
+  p.f[1] = ub_x;
+  c->h_heights.insert(c->h_heights.end(), heights, heights + n_samples);
+  return add_pair(c, p, lo, hi);
+}
+
+int fw_add_voxel_pair(fw_ctx* c, int32_t body, float penalty, const float* lo, const float* hi,
+                      int32_t nx, int32_t ny, const int32_t* occ, float lb_x, float lb_y, float dx,
+                      float dz) {
+  if (!c) return FW_ERR_ARG;
+  if (nx <= 0 || ny <= 0 || !occ) return fail(c, FW_ERR_ARG, "voxel pair: need nx, ny > 0 and occupancy");
+  Pair p{};
+  p.kind = fw::PAIR_VOXEL;
+  p.body = body;
+  p.penalty = penalty;
+  p.table = (int)c->h_occ.size();
+  p.n0 = nx;
+  p.n1 = ny;
+  p.f[0] = lb_x;
+  p.f[1] = lb_y;
+  p.f[2] = dx;
+  p.f[3] = dz;
+  // 1 = occupied, 0 = free, 2 = any other value (neither test matches it)
+  const size_t n = (size_t)nx * ny;
+  const size_t base = c->h_occ.size();
+  c->h_occ.resize(base + n);
+  for (size_t k = 0; k < n; ++k) c->h_occ[base + k] = occ[k] == 1 ? 1 : (occ[k] == 0 ? 0 : 2);
+  return add_pair(c, p, lo, hi);
+}
+
+int fw_finalize(fw_ctx* c) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_finalize called twice");
+  if (c->N <= 0 || c->E <= 0 || c->B <= 0 || c->S <= 0)
+    return fail(c, FW_ERR_STATE, "fw_finalize: nodes, elements, bodies and scenes must be set");
+  FW_CUDA(c, cudaSetDevice(c->device));
+  const int N = c->N, E = c->E, B = c->B, S = c->S;
+  // ---- validation and host-side packing
+  std::vector<int32_t> node_body(N, -1), elem_body(E, -1);
+  for (int b = 0; b < B; ++b) {
+    if (c->h_scene[b] < 0 || c->h_scene[b] >= S) return fail(c, FW_ERR_ARG, "body %d: bad scene", b);
+    if (c->h_noff[b] < 0 || c->h_ncnt[b] < 0 || (int64_t)c->h_noff[b] + c->h_ncnt[b] > N)
+      return fail(c, FW_ERR_ARG, "body %d: node range outside [0, %d)", b, N);
+    if (c->h_eoff[b] < 0 || c->h_ecnt[b] < 0 || (int64_t)c->h_eoff[b] + c->h_ecnt[b] > E)
+      return fail(c, FW_ERR_ARG, "body %d: element range outside [0, %d)", b, E);
+    for (int i = c->h_noff[b]; i < c->h_noff[b] + c->h_ncnt[b]; ++i) {
+      if (node_body[i] >= 0) return fail(c, FW_ERR_ARG, "node %d in two bodies", i);
+      node_body[i] = b;
+    }
+    for (int e = c->h_eoff[b]; e < c->h_eoff[b] + c->h_ecnt[b]; ++e) {
+      if (elem_body[e] >= 0) return fail(c, FW_ERR_ARG, "element %d in two bodies", e);
+      elem_body[e] = b;
+    }
+  }
+  for (int i = 0; i < N; ++i)
+    if (node_body[i] < 0) return fail(c, FW_ERR_ARG, "node %d belongs to no body", i);
+  for (int e = 0; e < E; ++e) {
+    if (elem_body[e] < 0) return fail(c, FW_ERR_ARG, "element %d belongs to no body", e);
+    for (int k = 0; k < 3; ++k) {
+      const int n = c->h_conn[3 * e + k];
+      if (n < 0 || n >= N) return fail(c, FW_ERR_ARG, "element %d: node id %d outside [0, %d)", e, n, N);
+      if (node_body[n] != elem_body[e])
+        return fail(c, FW_ERR_ARG, "element %d references node %d of another body", e, n);
+    }
+  }
+  std::vector<uint32_t> word(N);
+  for (int i = 0; i < N; ++i)
+    word[i] = (uint32_t)c->h_bc[i] | ((uint32_t)node_body[i] << fw::NODE_BODY_SHIFT);
+  for (int b = 0; b < B; ++b) {
+    if (c->h_bnoff[b] < 0 || c->h_bncnt[b] < 0 ||
+        (size_t)c->h_bnoff[b] + c->h_bncnt[b] > c->h_bnodes.size())
+      return fail(c, FW_ERR_ARG, "body %d: boundary-node range out of bounds", b);
+    for (int k = 0; k < c->h_bncnt[b]; ++k) {
+      const int n = c->h_bnodes[c->h_bnoff[b] + k];
+      if (n < 0 || n >= N || node_body[n] != b)
+        return fail(c, FW_ERR_ARG, "body %d: boundary node %d not in the body", b, n);
+      word[n] |= fw::NODE_BOUNDARY;
+    }
+  }
+  // pairs grouped by body, launch order kept within a body
+  std::vector<Pair> pairs = c->h_pairs;
+  for (const Pair& p : pairs)
+    if (p.body >= B) return fail(c, FW_ERR_ARG, "contact pair: body %d >= %d", p.body, B);
+  std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& a, const Pair& b) { return a.body < b.body; });
+  std::vector<int32_t> poff(B, 0), pcnt(B, 0);
+  for (size_t k = 0; k < pairs.size(); ++k) pcnt[pairs[k].body]++;
+  for (int b = 1; b < B; ++b) poff[b] = poff[b - 1] + pcnt[b - 1];
+  // CSR node -> (element, corner), ascending element
+  std::vector<int32_t> off(N + 1, 0), slot(3 * (size_t)E);
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < 3; ++k) off[c->h_conn[3 * e + k] + 1]++;
+  for (int i = 0; i < N; ++i) off[i + 1] += off[i];
+  {
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (int e = 0; e < E; ++e)
+      for (int k = 0; k < 3; ++k) slot[fill[c->h_conn[3 * e + k]]++] = 3 * e + k;
+  }
+  std::vector<ElemMat> emat(E);
+  std::vector<float2> j2par(E);
+  bool has_j2 = false;
+  for (int e = 0; e < E; ++e) {
+    emat[e].area = emat[e].lam = emat[e].mu = 0.f;
+    emat[e].word = (c->h_type[e] & 3) | (elem_body[e] << 2);
+    j2par[e] = make_float2(c->h_sy[e], c->h_H[e]);
+    has_j2 |= c->h_type[e] == fw::MAT_MISES;
+  }
+  std::vector<float2> x0(N), bcv(N), v0(N);
+  for (int i = 0; i < N; ++i) {
+    x0[i] = make_float2(c->h_x[2 * i], c->h_x[2 * i + 1]);
+    v0[i] = make_float2(c->h_v[2 * i], c->h_v[2 * i + 1]);
+    bcv[i] = make_float2(c->h_bcv[2 * i], c->h_bcv[2 * i + 1]);
+  }
+  // ---- device buffers
+  Dev& d = c->d;
+  d.N = N; d.E = E; d.B = B; d.S = S; d.P = (int)pairs.size(); d.has_j2 = has_j2;
+  int rc = 0;
+  if ((rc = upload(c, &d.x0, x0)) || (rc = upload(c, &d.x, x0)) || (rc = upload(c, &d.v, v0)) ||
+      (rc = upload(c, &d.bcv, bcv)) || (rc = upload(c, &d.node_word, word)) ||
+      (rc = dalloc(c, &d.mass, N)) || (rc = upload(c, &d.csr_off, off)) ||
+      (rc = upload(c, &d.csr_slot, slot)) || (rc = upload(c, &d.conn, c->h_conn)) ||
+      (rc = dalloc(c, &d.jinv, E)) || (rc = upload(c, &d.emat, emat)) ||
+      (rc = upload(c, &d.j2par, j2par)) || (rc = dalloc(c, &d.j2state, has_j2 ? E : 1)) ||
+      (rc = dalloc(c, &d.ndmass, E)) || (rc = dalloc(c, &d.corner, 3 * (size_t)E)) ||
+      (rc = upload(c, &d.body_scene, c->h_scene)) || (rc = upload(c, &d.body_pair_off, poff)) ||
+      (rc = upload(c, &d.body_pair_cnt, pcnt)) || (rc = upload(c, &d.pairs, pairs)) ||
+      (rc = dalloc(c, &d.pair_active, pairs.size())) || (rc = upload(c, &d.heights, c->h_heights)) ||
+      (rc = upload(c, &d.occ, c->h_occ)) || (rc = dalloc(c, &d.scene_dt, S)) ||
+      (rc = upload(c, &d.scene_damp, c->h_damp)) || (rc = dalloc(c, &d.scene_counter, S)) ||
+      (rc = dalloc(c, &d.scene_active, S)) || (rc = dalloc(c, &d.scene_mode_req, S)) ||
+      (rc = dalloc(c, &d.scene_mode, S)) || (rc = dalloc(c, &d.aabb_ring, 8 * (size_t)B)))
+    return rc;
+  FW_CUDA(c, cudaMemsetAsync(d.j2state, 0, sizeof(float4) * (has_j2 ? E : 1), c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.pair_active, 0, sizeof(int32_t) * (pairs.empty() ? 1 : pairs.size()), c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_dt, 0, sizeof(float) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_counter, 0, sizeof(int32_t) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.aabb_ring, 0, sizeof(int32_t) * 8 * (size_t)B, c->stream));
+  std::vector<int32_t> ones(S, 1);
+  c->cur_active = ones;
+  FW_CUDA(c, cudaMemcpyAsync(d.scene_active, ones.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(d.scene_mode_req, ones.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, c->stream));
+  float *dE = nullptr, *dnu = nullptr, *drho = nullptr;
+  if ((rc = upload(c, &dE, c->h_E)) || (rc = upload(c, &dnu, c->h_nu)) || (rc = upload(c, &drho, c->h_rho)))
+    return rc;
+  k_prepare_elements<<<(E + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d, dE, dnu, drho);
+  k_prepare_mass<<<(N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d);
+  c->launches += 2;
+  if ((rc = check_kernel(c, "prepare"))) return rc;
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+  c->grid_e = std::max(1, std::min((E + kBlock - 1) / kBlock, dev_sms * 8));
+  c->grid_n = std::max(1, (N + kBlock - 1) / kBlock);
+  // zero-dt construction step (setGlobalAABB -> substep(0, 0))
+  if ((rc = launch_step(c))) return rc;
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->finalized = true;
+  return FW_OK;
+}
+
+int fw_step(fw_ctx* c, int32_t n_steps, float dt) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_step before fw_finalize");
+  if (n_steps < 0) return fail(c, FW_ERR_ARG, "fw_step: n_steps < 0");
+  c->d.uniform_dt = 1;
+  c->d.dt_uniform = dt;
+  return run_steps(c, n_steps);
+}
+
+int fw_step_scenes(fw_ctx* c, int32_t n_steps, const float* dt) {
+  if (!c || !dt) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_step_scenes before fw_finalize");
+  if (n_steps < 0) return fail(c, FW_ERR_ARG, "fw_step_scenes: n_steps < 0");
+  int rc = set_scene_dt(c, dt);
+  if (rc) return rc;
+  c->d.uniform_dt = 0;
+  return run_steps(c, n_steps);
+}
+
+int fw_set_active(fw_ctx* c, const int32_t* active) {
+  if (!c || !active) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_set_active before fw_finalize");
+  c->cur_active.assign(active, active + c->S);
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_active, c->cur_active.data(), sizeof(int32_t) * c->S,
+                             cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+int fw_synchronize(fw_ctx* c) {
+  if (!c) return FW_ERR_ARG;
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+int fw_read_nodes(fw_ctx* c, int32_t field, int32_t first, int32_t count, float* dst, int32_t on_device) {
+  if (!c || !dst) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_read_nodes before fw_finalize");
+  if (first < 0 || count < 0 || (int64_t)first + count > c->N)
+    return fail(c, FW_ERR_ARG, "fw_read_nodes: range [%d, %d) outside [0, %d)", first, first + count, c->N);
+  const void* src = nullptr;
+  size_t per = 2 * sizeof(float);
+  switch (field) {
+    case FW_FIELD_X: src = c->d.x + first; break;
+    case FW_FIELD_V: src = c->d.v + first; break;
+    case FW_FIELD_X0: src = c->d.x0 + first; break;
+    case FW_FIELD_MASS: src = c->d.mass + first; per = sizeof(float); break;
+    default: return fail(c, FW_ERR_ARG, "fw_read_nodes: unknown field %d", field);
+  }
+  FW_CUDA(c, cudaMemcpyAsync(dst, src, per * count,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+int fw_write_nodes(fw_ctx* c, int32_t field, int32_t first, int32_t count, const float* src, int32_t on_device) {
+  if (!c || !src) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_write_nodes before fw_finalize");
+  if (first < 0 || count < 0 || (int64_t)first + count > c->N)
+    return fail(c, FW_ERR_ARG, "fw_write_nodes: range [%d, %d) outside [0, %d)", first, first + count, c->N);
+  void* dst = nullptr;
+  switch (field) {
+    case FW_FIELD_X: dst = c->d.x + first; break;
+    case FW_FIELD_V: dst = c->d.v + first; break;
+    default: return fail(c, FW_ERR_ARG, "fw_write_nodes: field %d is not writable", field);
+  }
+  FW_CUDA(c, cudaMemcpyAsync(dst, src, 2 * sizeof(float) * count,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+int fw_read_aabb(fw_ctx* c, float* dst) {
+  if (!c || !dst) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_read_aabb before fw_finalize");
+  std::vector<int32_t> ring(8 * (size_t)c->B), cnt(c->S);
+  FW_CUDA(c, cudaMemcpyAsync(ring.data(), c->d.aabb_ring, sizeof(int32_t) * ring.size(), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(cnt.data(), c->d.scene_counter, sizeof(int32_t) * c->S, cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int b = 0; b < c->B; ++b) {
+    const int slot = cnt[c->h_scene[b]] & 1;
+    for (int k = 0; k < 4; ++k) {
+      int v = ring[((size_t)slot * c->B + b) * 4 + k];
+      v = v >= 0 ? v : v ^ 0x7FFFFFFF;
+      memcpy(&dst[4 * b + k], &v, sizeof(float));
+    }
+  }
+  return FW_OK;
+}
+
+int fw_read_plastic(fw_ctx* c, float* eps_p, float* eqps) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_read_plastic before fw_finalize");
+  std::vector<float4> st(c->d.has_j2 ? c->E : 0);
+  if (c->d.has_j2) {
+    FW_CUDA(c, cudaMemcpyAsync(st.data(), c->d.j2state, sizeof(float4) * c->E, cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  for (int e = 0; e < c->E; ++e) {
+    const float4 s = c->d.has_j2 ? st[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (eps_p) {
+      eps_p[3 * e] = s.x;
+      eps_p[3 * e + 1] = s.y;
+      eps_p[3 * e + 2] = s.z;
+    }
+    if (eqps) eqps[e] = s.w;
+  }
+  return FW_OK;
+}
+
+int fw_read_reference_shape(fw_ctx* c, float* area, float* jinv) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_read_reference_shape before fw_finalize");
+  std::vector<ElemMat> m(c->E);
+  FW_CUDA(c, cudaMemcpyAsync(m.data(), c->d.emat, sizeof(ElemMat) * c->E, cudaMemcpyDeviceToHost, c->stream));
+  if (jinv) FW_CUDA(c, cudaMemcpyAsync(jinv, c->d.jinv, sizeof(float4) * c->E, cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (area)
+    for (int e = 0; e < c->E; ++e) area[e] = m[e].area;
+  return FW_OK;
+}
+
+int fw_read_counters(fw_ctx* c, int64_t* counters) {
+  if (!c || !counters) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_read_counters before fw_finalize");
+  std::vector<int32_t> cnt(c->S);
+  FW_CUDA(c, cudaMemcpyAsync(cnt.data(), c->d.scene_counter, sizeof(int32_t) * c->S, cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < c->S; ++s) counters[s] = cnt[s];
+  return FW_OK;
+}
+
+int64_t fw_launch_count(const fw_ctx* c) { return c ? c->launches : 0; }
+
+const char* fw_build_info(void) {
+  return "libfwb200: sm_100a, -fmad=false, IEEE div/sqrt, gather step v1";
+}
+
+}  // extern "C"

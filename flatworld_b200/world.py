@@ -1,0 +1,272 @@
+"""Host-side packing of one or many scenes into one device world.
+
+A *scene* is what one reference ``ExplicitLoop`` holds: FEM domains plus static
+grounds, one time step, one step counter.  ``SceneLayout`` restates the
+construction logic of the reference's ExplicitLoop / FemSpringManager /
+MixedContact for one scene (explicitloop.py:72-398, femspringmanager.py:509-813,
+femcontact.py:84-303, mixedcontact.py:1756-2270); ``World`` concatenates any
+number of scenes into flat node / element / body / pair arrays and hands them
+to the native library.  Scenes never interact, so a world of S scenes gives
+the same per-scene results as S separate loops.
+"""
+
+from __future__ import annotations
+
+import warnings
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from .definitions import ContactType, DomainType
+
+_SUPPORTED = (DomainType.FEM, DomainType.ANALYTICAL, DomainType.HEIGHTFIELD, DomainType.VOXELMAP)
+
+
+def bulk_modulus(mat) -> float:
+    """femcontact.py:94-98"""
+    nu = min(mat.nu, 0.4999)
+    return mat.E / (3.0 * (1.0 - 2.0 * nu))
+
+
+def segment_penalty(dom) -> float:
+    """femcontact.py:100-119, 2D branch: k = 2 K."""
+    return 2.0 * 1.0 * bulk_modulus(dom.prop.mat)
+
+
+def contact_stable_time(penalty: float, dom) -> float:
+    """femcontact.py:121-141: 0.9 sqrt(m_node / k), m_node = rho L^2/2 / 3."""
+    mat = dom.prop.mat
+    L = dom.mesh.charLength
+    m_node = mat.rho * (L * L * 0.5) / 3.0
+    return 0.9 * (m_node / penalty) ** 0.5
+
+
+@dataclass
+class ContactSpec:
+    kind: str  # "plane" | "heightfield" | "voxel"
+    fem: object
+    ground: object
+    pair_ids: tuple  # (later domain index, earlier domain index), explicitloop.py:275-276
+    penalty: float
+    stableTime: float
+
+
+def _contact_helper(di, dj, ctype, i, j):
+    """contactHelper (femcontact.py:283-303) restricted to the FEM-ground pairs."""
+    kinds = {
+        ContactType.FLEXANLAYTICAL: "plane",
+        ContactType.FEXHEIGHTFIELD: "heightfield",
+        ContactType.FLEXVOXELMAP: "voxel",
+    }
+    if ctype == ContactType.FLEXFLEX:
+        raise NotImplementedError(
+            "FEM-FEM contact (two FEM domains with considerContact=True in one loop) is outside "
+            "flatworld_b200's scope; set considerContact=False on the FEM domains that need not touch")
+    if ctype not in kinds:
+        return None
+    fem, ground = (di, dj) if di.type == DomainType.FEM else (dj, di)
+    pen = segment_penalty(fem)
+    return ContactSpec(kinds[ctype], fem, ground, (i, j), pen, contact_stable_time(pen, fem))
+
+
+class SceneLayout:
+    """Construction-time state of one scene (one reference ExplicitLoop)."""
+
+    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True):
+        for d in domains:
+            if d.type not in _SUPPORTED:
+                raise NotImplementedError(
+                    f"domain type {d.type} (rigid bodies, springs) is outside flatworld_b200's scope")
+        self.domains = list(domains)
+        self.fem = [d for d in domains if d.type == DomainType.FEM]
+        if not self.fem:
+            raise ValueError("a scene needs at least one FemDomain")
+        self.damping = float(damping)
+        self.useAdapative = bool(useAdapativeDT)
+        # explicitloop.py:145-170: 1.0, capped by the rigid manager's 1e-3 when an
+        # analytical plane exists, then by every FEM domain's CFL bound
+        stable = 1.0
+        if any(d.type in (DomainType.RIGID, DomainType.ANALYTICAL) for d in domains):
+            stable = min(1.0 / 1000.0, stable)
+        fsm_stable = 1.0
+        for d in self.fem:
+            fsm_stable = min(d.stableTime, fsm_stable)
+        stable = min(fsm_stable, stable)
+        # explicitloop.py:237-277: O(D^2) pair loop over contact domains
+        contacts = []
+        contact_domains = [(i, d) for i, d in enumerate(domains) if d.considerContact]
+        if any(d.type == DomainType.FEM for d in domains if d.considerContact):
+            for a, (i, di) in enumerate(contact_domains):
+                for b in range(a):
+                    j, dj = contact_domains[b]
+                    ctype = di.type | dj.type
+                    if di.category_bits & dj.collide_bits == 0:
+                        continue
+                    if di.collide_bits & dj.category_bits == 0:
+                        continue
+                    if ctype in (ContactType.RIGIDRIGID, ContactType.RIGIDANLAYTICAL,
+                                 ContactType.ANALYTICALANALYTICAL):
+                        continue
+                    if hasattr(di, "env_id") and hasattr(dj, "env_id") and di.env_id != dj.env_id:
+                        continue
+                    spec = _contact_helper(di, dj, ctype, i, j)
+                    if spec is not None:
+                        contacts.append(spec)
+        self.contacts = contacts
+        for c in contacts:  # explicitloop.py:313-315
+            stable = min(stable, c.stableTime)
+        self.stableTime = stable
+        self.default_dt = dt
+        self.dt = stable if useAdapativeDT else dt  # explicitloop.py:329-334
+        # mixedcontact.py:1794-2261: planes, then the single height field, then
+        # the single voxel grid; a second distinct height field (or voxel grid)
+        # sends all of that kind to the never-executed "unbatched" list
+        anal = [c for c in contacts if c.kind == "plane"]
+        hf = [c for c in contacts if c.kind == "heightfield"]
+        vox = [c for c in contacts if c.kind == "voxel"]
+        self.unbatched = []
+        if len({id(c.ground) for c in hf}) > 1:
+            warnings.warn("more than one HeightFieldDomain in a loop: like the reference, height-field "
+                          "contact is not executed for any of them", RuntimeWarning)
+            self.unbatched += hf
+            hf = []
+        if len({id(c.ground) for c in vox}) > 1:
+            warnings.warn("more than one VoxelGridDomain in a loop: like the reference, voxel contact "
+                          "is not executed for any of them", RuntimeWarning)
+            self.unbatched += vox
+            vox = []
+        self.pairs = anal + hf + vox
+        self.n_nodes = sum(d.nnodes for d in self.fem)
+        self.n_elems = sum(d.nelements for d in self.fem)
+
+
+class PackedWorld:
+    """Flat arrays of a list of scenes (scene-major, FEM domains in order)."""
+
+    def __init__(self, scenes: list[SceneLayout]):
+        self.scenes = scenes
+        N = sum(s.n_nodes for s in scenes)
+        E = sum(s.n_elems for s in scenes)
+        self.N, self.E = N, E
+        coords = np.zeros((N, 2), np.float32)
+        vel = np.zeros((N, 2), np.float32)
+        bc_bits = np.zeros(N, np.int32)
+        bc_vals = np.zeros((N, 2), np.float32)
+        conn = np.zeros((E, 3), np.int32)
+        mtype = np.zeros(E, np.int32)
+        Ev = np.zeros(E, np.float32)
+        nuv = np.zeros(E, np.float32)
+        rhov = np.zeros(E, np.float32)
+        syv = np.zeros(E, np.float32)
+        Hv = np.zeros(E, np.float32)
+        noff, ncnt, eoff, ecnt, bscene, bnoff, bncnt, bnodes = [], [], [], [], [], [], [], []
+        self.body_of = {}  # (scene idx, fem idx) -> global body id
+        self.scene_bodies = []
+        n0 = e0 = b0 = 0
+        for si, sc in enumerate(scenes):
+            bodies = []
+            for fi, dom in enumerate(sc.fem):
+                mesh = dom.mesh
+                nn, ne = mesh.numNodes, mesh.numElements
+                coords[n0:n0 + nn] = np.asarray(mesh.coords, dtype=np.float32)[:, :2]
+                conn[e0:e0 + ne] = np.asarray(mesh.connectivity, dtype=np.int64)[:, :3] + n0
+                mat = dom.prop.getMaterial()
+                mtype[e0:e0 + ne] = int(mat.type)
+                Ev[e0:e0 + ne] = float(mat.E)
+                nuv[e0:e0 + ne] = float(mat.nu)
+                rhov[e0:e0 + ne] = float(mat.rho)
+                syv[e0:e0 + ne] = float(getattr(mat, "sigma_y", 0.0))
+                Hv[e0:e0 + ne] = float(getattr(mat, "H", 0.0))
+                # processConditions (femspringmanager.py:660-705)
+                for bc in dom.bcs:
+                    t, nodes, values = bc.processData()
+                    if values is None:
+                        values = [0.0] * dom.d
+                    idx = np.arange(nn) if nodes is None else np.asarray(nodes, dtype=np.int64).reshape(-1)
+                    bc_bits[n0 + idx] |= int(t)
+                    bc_vals[n0 + idx, 0] = float(values[0])
+                    bc_vals[n0 + idx, 1] = float(values[1])
+                for ic in dom.initials:
+                    if not hasattr(ic, "vel"):
+                        raise NotImplementedError(f"initial condition {type(ic).__name__} is not an FEM initial condition")
+                    vx, vy = float(ic.vel[0]), float(ic.vel[1])
+                    if getattr(ic, "is_all_nodes", False):
+                        vel[n0:n0 + nn] = (vx, vy)
+                    else:
+                        ids = n0 + np.asarray(ic.nds, dtype=np.int64).reshape(-1)
+                        vel[ids] = (vx, vy)
+                b = b0 + fi
+                self.body_of[(si, fi)] = b
+                bodies.append(b)
+                noff.append(n0)
+                ncnt.append(nn)
+                eoff.append(e0)
+                ecnt.append(ne)
+                bscene.append(si)
+                bnoff.append(sum(len(x) for x in bnodes))
+                bn = n0 + np.asarray(mesh.boundaryNodes, dtype=np.int64)
+                bncnt.append(len(bn))
+                bnodes.append(bn)
+                n0 += nn
+                e0 += ne
+            b0 += len(sc.fem)
+            self.scene_bodies.append(bodies)
+        self.coords, self.vel, self.bc_bits, self.bc_vals = coords, vel, bc_bits, bc_vals
+        self.conn, self.mtype, self.Ev, self.nuv, self.rhov, self.syv, self.Hv = conn, mtype, Ev, nuv, rhov, syv, Hv
+        self.noff = np.asarray(noff, np.int32)
+        self.ncnt = np.asarray(ncnt, np.int32)
+        self.eoff = np.asarray(eoff, np.int32)
+        self.ecnt = np.asarray(ecnt, np.int32)
+        self.bscene = np.asarray(bscene, np.int32)
+        self.bnoff = np.asarray(bnoff, np.int32)
+        self.bncnt = np.asarray(bncnt, np.int32)
+        self.bnodes = np.concatenate(bnodes).astype(np.int32) if bnodes else np.zeros(0, np.int32)
+        self.B = len(noff)
+        self.S = len(scenes)
+
+    def pair_records(self):
+        """(kind, body, penalty f32, gate lo, gate hi, ground) in launch order."""
+        out = []
+        for si, sc in enumerate(self.scenes):
+            fem_index = {id(d): k for k, d in enumerate(sc.fem)}
+            for c in sc.pairs:
+                body = self.body_of[(si, fem_index[id(c.fem)])]
+                lo, hi = c.ground.getBBox()
+                out.append((c.kind, body, np.float32(c.penalty), np.asarray(lo, np.float32),
+                            np.asarray(hi, np.float32), c.ground))
+        return out
+
+
+def build_native(packed: PackedWorld, device: int = 0) -> _native.NativeWorld:
+    nw = _native.NativeWorld(device)
+    nw.set_nodes(packed.coords, packed.vel, packed.bc_bits, packed.bc_vals)
+    nw.set_elements(packed.conn, packed.mtype, packed.Ev, packed.nuv, packed.rhov, packed.syv, packed.Hv)
+    nw.set_bodies(packed.noff, packed.ncnt, packed.eoff, packed.ecnt, packed.bscene, packed.bnoff,
+                  packed.bncnt, packed.bnodes)
+    nw.set_scenes(np.asarray([s.damping for s in packed.scenes], np.float32))
+    for kind, body, pen, lo, hi, g in packed.pair_records():
+        if kind == "plane":
+            nw.add_plane(body, pen, lo, hi, g.point, g.normal)
+        elif kind == "heightfield":
+            nw.add_heightfield(body, pen, lo, hi, g.height, g.lb[0], g.ub[0], 1 if g.reverse else 0)
+        else:
+            nw.add_voxel(body, pen, lo, hi, np.asarray(g.occ, np.int32), g.lb[0], g.lb[1], g.dx, g.dz)
+    nw.finalize()
+    return nw
+
+
+def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):
+    """advanceWithTime's float64 substep loop (explicitloop.py:573-586) as a list
+    of (count, dt) runs."""
+    remaining = float(frame_dt)
+    runs = []
+    while remaining > 1e-12:
+        cur = stable if adaptive else default_dt
+        sub = max(min(cur, remaining), 1e-8)
+        if runs and runs[-1][1] == sub:
+            runs[-1][0] += 1
+        else:
+            runs.append([1, sub])
+        remaining -= sub
+    return [(n, d) for n, d in runs]

@@ -1,0 +1,181 @@
+/*
+ * fwb200.h -- C ABI of the B200 explicit 2D FEM step (libfwb200.so).
+ *
+ * The reference (FlatWorld) has no foreign-function interface: its "plugin
+ * API" is the Python object model, and the device work happens in Warp kernels
+ * launched by two Python classes.  Each entry point below replaces one of those
+ * launch sites; the Python package flatworld_b200 binds them with ctypes and
+ * keeps the reference's class names on top.  References are file:line in the
+ * FlatWorld project.
+ *
+ * Conventions
+ *   - Plain C types only: pointers, sizes, float/double/int.  No torch types.
+ *   - Every function returns 0 (FW_OK) or a negative FW_ERR_* code; the text of
+ *     the last error of a context is fw_last_error(ctx).  No C++ exception
+ *     crosses this boundary.
+ *   - Host arrays passed in are copied during the call; the library owns all
+ *     device memory of a context.  Arrays are little-endian, C order.
+ *   - A world holds S independent scenes (S = 1 for one ExplicitLoop).  Each
+ *     scene has its own time step, damping, step counter and active flag;
+ *     scenes never exchange forces.  Bodies (FEM domains) belong to a scene,
+ *     contact pairs to a body.
+ *   - Calls on one context are not re-entrant; different contexts are
+ *     independent.  Device work is queued on the context's stream
+ *     (fw_set_stream, default: a non-blocking stream the context creates).
+ */
+#ifndef FWB200_H
+#define FWB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FW_OK 0
+#define FW_ERR_ARG -1       /* bad argument (size, index, pointer) */
+#define FW_ERR_OOM -2       /* device allocation failed */
+#define FW_ERR_CUDA -3      /* a CUDA runtime call failed */
+#define FW_ERR_TIMEOUT -4   /* a bounded device wait gave up */
+#define FW_ERR_NONFINITE -5 /* a NaN/inf was found in the state */
+#define FW_ERR_STATE -6     /* call out of order (e.g. step before finalize) */
+
+/* Node boundary-condition bits: same values as the reference's
+ * flatworld/definitions.py:96-104. */
+#define FW_BC_U 0x1
+#define FW_BC_V 0x2
+#define FW_BC_A 0x4
+#define FW_BC_FORCE 0x8
+#define FW_BC_GRAVITY 0x10
+
+/* Material types: flatworld/definitions.py:80-83. */
+#define FW_MAT_ELASTIC 1
+#define FW_MAT_NEOHOOKEAN 2
+#define FW_MAT_MISES 3
+
+/* Node array selectors for fw_read_nodes / fw_write_nodes. */
+#define FW_FIELD_X 0    /* current coordinates (FemSpringManager.coords) */
+#define FW_FIELD_V 1    /* velocities (FemSpringManager.V) */
+#define FW_FIELD_MASS 2 /* lumped mass, one float per node (FemSpringManager.mass) */
+#define FW_FIELD_X0 3   /* rest coordinates */
+
+typedef struct fw_ctx fw_ctx;
+
+/* Create / destroy a context on CUDA device `device`.
+ * Replaces: FemSpringManager.__init__ buffer allocation,
+ * flatworld/femspringmanager.py:509-637. */
+int fw_create(fw_ctx** out, int device);
+void fw_destroy(fw_ctx* ctx);
+const char* fw_last_error(const fw_ctx* ctx);
+/* Queue work on a caller stream (a cudaStream_t passed as void*; NULL = the
+ * context's own stream). */
+int fw_set_stream(fw_ctx* ctx, void* stream);
+
+/* Packed nodes of all bodies of all scenes: coords[2n], vel[2n] (initial
+ * velocities), bc_bits[n] (OR of FW_BC_*), bc_values[2n] (value of the last BC
+ * that touched the node).
+ * Replaces: addFemDomain coords packing and processConditions,
+ * flatworld/femspringmanager.py:660-705, 741. */
+int fw_set_nodes(fw_ctx* ctx, int32_t n_nodes, const float* coords, const float* vel,
+                 const int32_t* bc_bits, const float* bc_values);
+
+/* Packed triangles: conn[3e] (global node ids), per-element material.
+ * Replaces: addFemDomain element packing, flatworld/femspringmanager.py:743-766. */
+int fw_set_elements(fw_ctx* ctx, int32_t n_elems, const int32_t* conn, const int32_t* mat_type,
+                    const float* young, const float* poisson, const float* density,
+                    const float* yield_stress, const float* hardening);
+
+/* Bodies (FEM domains): node range, element range, owning scene and the
+ * sorted boundary-node ids (global) of each body.
+ * Replaces: addFemDomain offsets and boundary-node packing,
+ * flatworld/femspringmanager.py:735-799. */
+int fw_set_bodies(fw_ctx* ctx, int32_t n_bodies, const int32_t* node_offset,
+                  const int32_t* node_count, const int32_t* elem_offset, const int32_t* elem_count,
+                  const int32_t* scene_of_body, const int32_t* bnode_offset,
+                  const int32_t* bnode_count, int32_t n_bnodes, const int32_t* bnodes);
+
+/* Scenes: per-scene damping (ExplicitLoop damping kwarg).
+ * Replaces: ExplicitLoop.__init__ state, flatworld/explicitloop.py:72-85, 172-175. */
+int fw_set_scenes(fw_ctx* ctx, int32_t n_scenes, const float* damping);
+
+/* Contact pairs (one FEM body against one ground), in the reference's launch
+ * order within a body: planes, then height fields, then voxel grids, each in
+ * contact-creation order.  gate_lo/gate_hi is the ground's getBBox() box used
+ * by the broad-phase gate.  penalty is the float32 value of 2*K.
+ * Replaces: _build_batched_contacts work lists and the per-substep launches of
+ * _batched_analytical_contact_kernel / _batched_heightfield_contact_kernel /
+ * _batched_voxelmap_contact_kernel, flatworld/mixedcontact.py:1794-1856,
+ * 2131-2261, 660-684, 1566-1643. */
+int fw_add_plane_pair(fw_ctx* ctx, int32_t body, float penalty, const float* gate_lo,
+                      const float* gate_hi, float px, float py, float nx, float ny);
+int fw_add_heightfield_pair(fw_ctx* ctx, int32_t body, float penalty, const float* gate_lo,
+                            const float* gate_hi, int32_t n_samples, const float* heights,
+                            float lb_x, float ub_x, int32_t reverse);
+/* occupancy is nx*ny int32 in C order occ[i*ny + j] (VoxelGridDomain.occ). */
+int fw_add_voxel_pair(fw_ctx* ctx, int32_t body, float penalty, const float* gate_lo,
+                      const float* gate_hi, int32_t nx, int32_t ny, const int32_t* occupancy,
+                      float lb_x, float lb_y, float dx, float dz);
+
+/* Upload, precompute reference-shape data (area, Dm^-1, lumped mass, Lame
+ * constants, node->element gather lists) and run the zero-dt step that the
+ * reference runs at construction.
+ * Replaces: prepareFEMData_ / _prepare_fem_data_kernel and setGlobalAABB ->
+ * substep(0, 0), flatworld/femspringmanager.py:113-138, 872-897. */
+int fw_finalize(fw_ctx* ctx);
+
+/* Advance every active scene by n_steps substeps of dt (float32), i.e. n_steps
+ * calls of ExplicitLoop.advance(): gated contact, element force, integration,
+ * body AABB.  Queued on the stream; returns without waiting.
+ * Replaces: ExplicitLoop.advance / FemSpringManager.femStep,
+ * flatworld/explicitloop.py:473-555, flatworld/femspringmanager.py:941-1012. */
+int fw_step(fw_ctx* ctx, int32_t n_steps, float dt);
+
+/* Like fw_step with a per-scene dt[] (float32, n_scenes entries) for the
+ * batched and served forms, where each scene has its own step. */
+int fw_step_scenes(fw_ctx* ctx, int32_t n_steps, const float* dt_per_scene);
+
+/* Mark scenes active (1) / frozen (0).  Frozen scenes keep their state and do
+ * not advance. */
+int fw_set_active(fw_ctx* ctx, const int32_t* active);
+
+/* Wait for all queued work of the context. */
+int fw_synchronize(fw_ctx* ctx);
+
+/* Read / write a node field for nodes [first, first+count).  X, V, X0: 2 floats
+ * per node; MASS: 1 float.  on_device != 0 means dst/src is a device pointer.
+ * Replaces: coords.numpy(), V.numpy(), mass.numpy(); FemDomain.getCurrentCoords,
+ * flatworld/femdomain.py:47-50. */
+int fw_read_nodes(fw_ctx* ctx, int32_t field, int32_t first, int32_t count, float* dst,
+                  int32_t on_device);
+int fw_write_nodes(fw_ctx* ctx, int32_t field, int32_t first, int32_t count, const float* src,
+                   int32_t on_device);
+
+/* Per-body boundary AABB after the last step: 4 floats per body
+ * (lb.x, lb.y, ub.x, ub.y).  Replaces: _update_bbox_kernel output aabb[],
+ * flatworld/femspringmanager.py:361-408; FemDomain.getBBox femdomain.py:23-29. */
+int fw_read_aabb(fw_ctx* ctx, float* dst);
+
+/* Per-element J2 state: eps_p (3 floats per element) and equivalent plastic
+ * strain (1 float); zeros for non-J2 elements.  Replaces: plasticStrain /
+ * eqPlasticStrain .numpy(), flatworld/femspringmanager.py:592-593. */
+int fw_read_plastic(fw_ctx* ctx, float* eps_p, float* eqps);
+
+/* Precomputed reference-shape data: area[e], jinv[4e] (row-major Dm^-1).
+ * Replaces: elemVolume / J_inv .numpy(), femspringmanager.py:581-582. */
+int fw_read_reference_shape(fw_ctx* ctx, float* area, float* jinv);
+
+/* Per-scene step counters (number of advance() calls since finalize). */
+int fw_read_counters(fw_ctx* ctx, int64_t* counters);
+
+/* Number of kernel launches this context queued since creation (evidence
+ * that the CUDA path ran; used by the benchmark's gpu_launches field). */
+int64_t fw_launch_count(const fw_ctx* ctx);
+
+/* Library build identification string (arch, flags). */
+const char* fw_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FWB200_H */

@@ -1,0 +1,770 @@
+/*
+ * fw_oracle.c -- CPU restatement of FlatWorld's explicit 2D FEM substep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle that the CUDA path is
+ * checked against; nothing in the product (flatworld_b200/) links, loads or
+ * calls it.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * and reference legs use it.
+ *
+ * Built twice from this one source (see oracle/Makefile):
+ *   liboracle_f32.so : REAL=float  -- the reference's FP32 scheme, operation by
+ *                      operation, compiled with -ffp-contract=off so that every
+ *                      product and sum is rounded the way the source reads.
+ *   liboracle_f64.so : REAL=double -- the same scheme in FP64 (error oracle).
+ * A third build, liboracle_f32fma.so, contracts a*b+c into FMAs; the distance
+ * between the two FP32 builds is the rounding noise floor of the scheme itself
+ * (the reference's Warp GPU path is compiled by NVRTC with FMA contraction on).
+ *
+ * Restated reference code (all paths relative to the FlatWorld project root):
+ *   flatworld/femspringmanager.py:59-68    get_jacobian_2d, get_weights_2d
+ *   flatworld/femspringmanager.py:71-105   get_b_matrix_2d
+ *   flatworld/femspringmanager.py:113-138  _prepare_fem_data_kernel
+ *   flatworld/femspringmanager.py:217-280  _fem_internal_force_kernel
+ *   flatworld/femspringmanager.py:315-358  _integrate_nodes_kernel
+ *   flatworld/femspringmanager.py:361-408  _update_bbox_kernel
+ *   flatworld/femspringmanager.py:941-1012 femStep (launch order)
+ *   flatworld/materials/materialfunctions.py:10-29  getStress2D
+ *   flatworld/materials/materialfunctions.py:35-101 misesReturnMap2D
+ *   flatworld/mixedcontact.py:166-217      _nearest_on_curve_2d
+ *   flatworld/mixedcontact.py:220-302      _voxel_signed_distance_2d
+ *   flatworld/mixedcontact.py:495-515      _activate_pairs_kernel (+ bvh.py:40-46,
+ *                                          321-342, 393-478: box test semantics)
+ *   flatworld/mixedcontact.py:660-684      _batched_analytical_contact_kernel
+ *   flatworld/mixedcontact.py:1566-1643    heightfield / voxel contact kernels
+ *   flatworld/mixedcontact.py:1654-1755    run_batched_contacts (launch order)
+ *   flatworld/explicitloop.py:473-555      advance (contacts -> femStep)
+ *
+ * Warp builtins (warp-lang, unpinned: requirements.txt `warp-lang>=1.7.0`) are
+ * restated from their published definitions: mat22 @ mat22 and mat @ vec sum
+ * products in index order; determinant(m) = m00*m11 - m01*m10; inverse(m22) =
+ * adjugate * (1/det), the zero matrix when det == 0; round() rounds half away
+ * from zero (C roundf); floor, sqrt, log are the C library functions; the
+ * serial CPU device applies atomic_add in launch order.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+#ifndef REAL
+#define REAL float
+#endif
+
+#if defined(REAL_IS_DOUBLE)
+#define R_SQRT sqrt
+#define R_LOG log
+#define R_FLOOR floor
+#define R_ROUND round
+#define R_FABS fabs
+#else
+#define R_SQRT sqrtf
+#define R_LOG logf
+#define R_FLOOR floorf
+#define R_ROUND roundf
+#define R_FABS fabsf
+#endif
+
+/* Bit constants: flatworld/definitions.py:96-104 */
+#define BC_U 0x1
+#define BC_V 0x2
+#define BC_A 0x4
+#define BC_FORCE 0x8
+#define BC_GRAVITY 0x10
+
+/* MaterialType: flatworld/definitions.py:80-83 */
+#define MAT_ELASTIC 1
+#define MAT_NEOHOOKEAN 2
+#define MAT_MISES 3
+
+#define PAIR_PLANE 0
+#define PAIR_HEIGHTFIELD 1
+#define PAIR_VOXEL 2
+
+typedef struct {
+  int kind;
+  int body;
+  REAL penalty;
+  REAL glb[2], gub[2]; /* ground getBBox(), gate box */
+  /* plane */
+  REAL p[2], n[2];
+  /* heightfield */
+  int hnx, reverse;
+  REAL hlbx, hubx;
+  REAL* h;
+  /* voxel */
+  int vnx, vny;
+  REAL vlb[2], vdx, vdz;
+  int32_t* occ; /* occ[i*vny + j] */
+} or_pair;
+
+typedef struct {
+  int n_nodes, n_elems, n_bodies, n_pairs, n_threads;
+  REAL *x, *v, *u, *fext, *mass, *bcv;
+  int32_t* bc;
+  int32_t* conn; /* 3 per element */
+  int32_t* type;
+  REAL *E, *nu, *rho, *sy, *H;
+  REAL *area, *jinv, *epsp, *eqps;
+  int32_t *bn_off, *bn_cnt, *bnodes;
+  REAL* aabb; /* per body: lbx, lby, ubx, uby */
+  or_pair* pairs;
+  /* CSR (node -> element corners, ascending element) for the threaded path */
+  int32_t *csr_off, *csr_slot;
+  REAL* corner; /* 6 per element */
+} or_world;
+
+static REAL* dupf(const float* src, size_t n) {
+  REAL* d = (REAL*)malloc(sizeof(REAL) * (n ? n : 1));
+  for (size_t i = 0; i < n; ++i) d[i] = (REAL)src[i];
+  return d;
+}
+static int32_t* dupi(const int32_t* src, size_t n) {
+  int32_t* d = (int32_t*)malloc(sizeof(int32_t) * (n ? n : 1));
+  if (n) memcpy(d, src, sizeof(int32_t) * n);
+  return d;
+}
+
+/* _prepare_fem_data_kernel (femspringmanager.py:113-138), serial element order. */
+static void prepare(or_world* w) {
+  for (int i = 0; i < w->n_nodes; ++i) w->mass[i] = 0;
+  for (int e = 0; e < w->n_elems; ++e) {
+    int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
+    REAL j00 = w->x[2 * n1] - w->x[2 * n3], j01 = w->x[2 * n2] - w->x[2 * n3];
+    REAL j10 = w->x[2 * n1 + 1] - w->x[2 * n3 + 1], j11 = w->x[2 * n2 + 1] - w->x[2 * n3 + 1];
+    REAL det_w = j00 * j11 - j01 * j10;
+    REAL vol = R_FABS(det_w) * (REAL)0.5;
+    w->area[e] = vol;
+    REAL det = j00 * j11 - j01 * j10;
+    REAL* ji = w->jinv + 4 * e;
+    if (det != (REAL)0) {
+      REAL r = (REAL)1.0 / det;
+      ji[0] = j11 * r;
+      ji[1] = -j01 * r;
+      ji[2] = -j10 * r;
+      ji[3] = j00 * r;
+    } else {
+      ji[0] = ji[1] = ji[2] = ji[3] = 0;
+    }
+    REAL nd_mass = vol * w->rho[e] / (REAL)3.0;
+    w->mass[n1] += nd_mass;
+    w->mass[n2] += nd_mass;
+    w->mass[n3] += nd_mass;
+  }
+}
+
+/* getStress2D (materialfunctions.py:10-29) for ELASTIC / NEOHOOKEAN and
+ * misesReturnMap2D (35-101) for MISES.  Returns Voigt PK2 (S11, S22, S12). */
+static void stress(const or_world* w, int e, REAL F00, REAL F01, REAL F10, REAL F11,
+                   REAL* s, REAL* epsp_out, REAL* eqps_out) {
+  REAL E = w->E[e], nu = w->nu[e];
+  REAL lam = E * nu / (((REAL)1.0 + nu) * ((REAL)1.0 - (REAL)2.0 * nu));
+  REAL mu = E / ((REAL)2.0 * ((REAL)1.0 + nu));
+  /* C = F^T F ; strain = 0.5 (C - I) */
+  REAL C00 = F00 * F00 + F10 * F10;
+  REAL C01 = F00 * F01 + F10 * F11;
+  REAL C10 = F01 * F00 + F11 * F10;
+  REAL C11 = F01 * F01 + F11 * F11;
+  REAL e00 = (REAL)0.5 * (C00 - (REAL)1.0);
+  REAL e01 = (REAL)0.5 * (C01 - (REAL)0.0);
+  REAL e11 = (REAL)0.5 * (C11 - (REAL)1.0);
+  int t = w->type[e];
+  if (t == MAT_MISES) {
+    REAL ep0 = w->epsp[3 * e], ep1 = w->epsp[3 * e + 1], ep2 = w->epsp[3 * e + 2];
+    REAL eq = w->eqps[e];
+    REAL t0 = e00 - ep0, t1 = e11 - ep1, t2 = e01 - ep2;
+    REAL tr = t0 + t1;
+    REAL s0 = lam * tr + (REAL)2.0 * mu * t0;
+    REAL s1 = lam * tr + (REAL)2.0 * mu * t1;
+    REAL s2 = (REAL)2.0 * mu * t2;
+    REAL p = (s0 + s1) / (REAL)3.0;
+    REAL d0 = s0 - p, d1 = s1 - p, d2 = s2;
+    REAL vm = R_SQRT(d0 * d0 + d1 * d1 - d0 * d1 + (REAL)3.0 * d2 * d2);
+    REAL f = vm - (w->sy[e] + w->H[e] * eq);
+    s[0] = s0;
+    s[1] = s1;
+    s[2] = s2;
+    epsp_out[0] = ep0;
+    epsp_out[1] = ep1;
+    epsp_out[2] = ep2;
+    *eqps_out = eq;
+    if (f > (REAL)0.0) {
+      REAL denom = (REAL)3.0 * mu + w->H[e];
+      REAL dg = f / denom;
+      *eqps_out = eq + dg;
+      REAL scale = (REAL)1.0 - (REAL)3.0 * mu * dg / vm;
+      REAL n0 = d0 * scale, n1 = d1 * scale, n2 = d2 * scale;
+      s[0] = n0 + p;
+      s[1] = n1 + p;
+      s[2] = n2;
+      REAL h0 = d0 / vm, h1 = d1 / vm, h2 = d2 / vm;
+      epsp_out[0] = ep0 + dg * h0;
+      epsp_out[1] = ep1 + dg * h1;
+      epsp_out[2] = ep2 + dg * h2;
+    }
+    return;
+  }
+  if (t == MAT_ELASTIC) {
+    REAL tr = e00 + e11;
+    REAL lt = lam * tr;
+    REAL tm = (REAL)2.0 * mu;
+    s[0] = lt * (REAL)1.0 + tm * e00;
+    s[1] = lt * (REAL)1.0 + tm * e11;
+    s[2] = lt * (REAL)0.0 + tm * e01;
+  } else if (t == MAT_NEOHOOKEAN) {
+    REAL cdet = C00 * C11 - C01 * C10;
+    REAL i00 = 0, i01 = 0, i11 = 0;
+    if (cdet != (REAL)0) {
+      REAL r = (REAL)1.0 / cdet;
+      i00 = C11 * r;
+      i01 = -C01 * r;
+      i11 = C00 * r;
+    }
+    REAL J = F00 * F11 - F01 * F10;
+    REAL c = lam * R_LOG(J) - mu;
+    s[0] = c * i00 + mu * (REAL)1.0;
+    s[1] = c * i11 + mu * (REAL)1.0;
+    s[2] = c * i01 + mu * (REAL)0.0;
+  } else {
+    s[0] = s[1] = s[2] = 0;
+  }
+}
+
+/* _fem_internal_force_kernel (femspringmanager.py:217-280): writes the three
+ * corner forces -(B^T S)*A of element e into out[6] and updates J2 state. */
+static void element_force(or_world* w, int e, REAL* out) {
+  int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
+  const REAL* x = w->x;
+  REAL j00 = x[2 * n1] - x[2 * n3], j01 = x[2 * n2] - x[2 * n3];
+  REAL j10 = x[2 * n1 + 1] - x[2 * n3 + 1], j11 = x[2 * n2 + 1] - x[2 * n3 + 1];
+  const REAL* ji = w->jinv + 4 * e;
+  REAL F00 = j00 * ji[0] + j01 * ji[2];
+  REAL F01 = j00 * ji[1] + j01 * ji[3];
+  REAL F10 = j10 * ji[0] + j11 * ji[2];
+  REAL F11 = j10 * ji[1] + j11 * ji[3];
+  /* get_b_matrix_2d (femspringmanager.py:71-105) */
+  REAL d00 = ji[0], d01 = ji[1], d10 = ji[2], d11 = ji[3];
+  REAL d20 = -ji[0] - ji[2], d21 = -ji[1] - ji[3];
+  REAL B[3][6];
+  B[0][0] = d00 * F00; B[0][1] = d00 * F10;
+  B[1][0] = d01 * F01; B[1][1] = d01 * F11;
+  B[2][0] = d01 * F00 + d00 * F01; B[2][1] = d00 * F11 + d01 * F10;
+  B[0][2] = d10 * F00; B[0][3] = d10 * F10;
+  B[1][2] = d11 * F01; B[1][3] = d11 * F11;
+  B[2][2] = d11 * F00 + d10 * F01; B[2][3] = d10 * F11 + d11 * F10;
+  B[0][4] = d20 * F00; B[0][5] = d20 * F10;
+  B[1][4] = d21 * F01; B[1][5] = d21 * F11;
+  B[2][4] = d21 * F00 + d20 * F01; B[2][5] = d20 * F11 + d21 * F10;
+  REAL s[3], ep[3], eq;
+  stress(w, e, F00, F01, F10, F11, s, ep, &eq);
+  if (w->type[e] == MAT_MISES) {
+    w->epsp[3 * e] = ep[0];
+    w->epsp[3 * e + 1] = ep[1];
+    w->epsp[3 * e + 2] = ep[2];
+    w->eqps[e] = eq;
+  }
+  REAL a = w->area[e];
+  for (int r = 0; r < 6; ++r) {
+    REAL fi = B[0][r] * s[0] + B[1][r] * s[1] + B[2][r] * s[2];
+    fi = fi * a;
+    out[r] = -fi;
+  }
+}
+
+/* _nearest_on_curve_2d (mixedcontact.py:166-217): returns n and signed. */
+static REAL hf_signed(const or_pair* c, REAL px, REAL pz, REAL* nx_out, REAL* ny_out) {
+  REAL span = c->hubx - c->hlbx;
+  REAL u = 0;
+  if (span > (REAL)1e-12) u = (px - c->hlbx) / span;
+  if (u < (REAL)0.0) u = 0;
+  if (u > (REAL)1.0) u = 1;
+  int nx = c->hnx;
+  REAL s = u * (REAL)(nx - 1);
+  int i0 = (int)R_FLOOR(s);
+  int i1 = i0 + 1;
+  if (i1 >= nx) i1 = nx - 1;
+  if (i0 < 0) i0 = 0;
+  REAL t = s - (REAL)i0;
+  REAL h = c->h[i0] + (c->h[i1] - c->h[i0]) * t;
+  int ir = (int)R_ROUND(s);
+  if (ir < 0) ir = 0;
+  if (ir >= nx) ir = nx - 1;
+  int j0 = ir - 1, j1 = ir + 1;
+  if (j0 < 0) j0 = 0;
+  if (j1 >= nx) j1 = nx - 1;
+  REAL dxw = span / (REAL)(nx - 1);
+  REAL denom = dxw * (REAL)(j1 - j0);
+  REAL dhdx = 0;
+  if (denom > (REAL)1e-6) dhdx = (c->h[j1] - c->h[j0]) / denom;
+  REAL n0 = -dhdx, n1 = (REAL)1.0;
+  if (c->reverse == 1) {
+    n0 = -n0;
+    n1 = -n1;
+  }
+  REAL nl = R_SQRT(n0 * n0 + n1 * n1);
+  if (nl > (REAL)1e-12) {
+    n0 = n0 / nl;
+    n1 = n1 / nl;
+  }
+  *nx_out = n0;
+  *ny_out = n1;
+  return (px - px) * n0 + (pz - h) * n1;
+}
+
+/* _voxel_signed_distance_2d (mixedcontact.py:220-302). */
+static REAL voxel_signed(const or_pair* c, REAL px, REAL py, REAL* nx_out, REAL* ny_out) {
+  REAL best_d = (REAL)1e9;
+  REAL b0 = 0, b1 = 1;
+  int nx = c->vnx, ny = c->vny;
+  int i = (int)R_FLOOR((px - c->vlb[0]) / c->vdx);
+  int j = (int)R_FLOOR((py - c->vlb[1]) / c->vdz);
+  if (0 <= i && i < nx && 0 <= j && j < ny && c->occ[i * ny + j] == 1) {
+    REAL dnx = (REAL)1e9, dpx = (REAL)1e9, dny = (REAL)1e9, dpy = (REAL)1e9;
+    for (int st = 0; st < nx; ++st) {
+      int idx = i - 1 - st;
+      if (idx < 0 || c->occ[idx * ny + j] == 0) {
+        dnx = px - (c->vlb[0] + (REAL)(idx + 1) * c->vdx);
+        break;
+      }
+    }
+    for (int st = 0; st < nx; ++st) {
+      int idx = i + 1 + st;
+      if (idx >= nx || c->occ[idx * ny + j] == 0) {
+        dpx = (c->vlb[0] + (REAL)idx * c->vdx) - px;
+        break;
+      }
+    }
+    for (int st = 0; st < ny; ++st) {
+      int idx = j - 1 - st;
+      if (idx < 0 || c->occ[i * ny + idx] == 0) {
+        dny = py - (c->vlb[1] + (REAL)(idx + 1) * c->vdz);
+        break;
+      }
+    }
+    for (int st = 0; st < ny; ++st) {
+      int idx = j + 1 + st;
+      if (idx >= ny || c->occ[i * ny + idx] == 0) {
+        dpy = (c->vlb[1] + (REAL)idx * c->vdz) - py;
+        break;
+      }
+    }
+    REAL mv = dnx;
+    int face = 0;
+    if (dpx < mv) { mv = dpx; face = 1; }
+    if (dny < mv) { mv = dny; face = 2; }
+    if (dpy < mv) { mv = dpy; face = 3; }
+    if (face == 0) { best_d = -dnx; b0 = -1; b1 = 0; }
+    else if (face == 1) { best_d = -dpx; b0 = 1; b1 = 0; }
+    else if (face == 2) { best_d = -dny; b0 = 0; b1 = -1; }
+    else { best_d = -dpy; b0 = 0; b1 = 1; }
+  }
+  *nx_out = b0;
+  *ny_out = b1;
+  return best_d;
+}
+
+/* Pair gate: the broad phase reports (fem, ground) when their leaf boxes
+ * overlap (bvh.py:40-46 inclusive test).  On steps with counter % 100 == 0 the
+ * tree is rebuilt from boxes grown by 10% of their extent (bvh.py:321-342); on
+ * the other steps the leaves are refit to the raw boxes (bvh.py:393-416). */
+static int pair_active(const or_world* w, const or_pair* c, long counter) {
+  const REAL* bb = w->aabb + 4 * c->body;
+  REAL alo[2] = {bb[0], bb[1]}, ahi[2] = {bb[2], bb[3]};
+  REAL blo[2] = {c->glb[0], c->glb[1]}, bhi[2] = {c->gub[0], c->gub[1]};
+  if (counter % 100 == 0) {
+    for (int k = 0; k < 2; ++k) {
+      REAL ba = (REAL)0.1 * (ahi[k] - alo[k]);
+      REAL bbuf = (REAL)0.1 * (bhi[k] - blo[k]);
+      alo[k] = alo[k] - ba;
+      ahi[k] = ahi[k] + ba;
+      blo[k] = blo[k] - bbuf;
+      bhi[k] = bhi[k] + bbuf;
+    }
+  }
+  return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
+}
+
+static void contacts(or_world* w, REAL dt, long counter) {
+  for (int pi = 0; pi < w->n_pairs; ++pi) {
+    const or_pair* c = &w->pairs[pi];
+    if (!pair_active(w, c, counter)) continue;
+    int off = w->bn_off[c->body], cnt = w->bn_cnt[c->body];
+    for (int k = 0; k < cnt; ++k) {
+      int nid = w->bnodes[off + k];
+      REAL px = w->x[2 * nid], py = w->x[2 * nid + 1];
+      REAL vx = w->v[2 * nid], vy = w->v[2 * nid + 1];
+      REAL fx = 0, fy = 0;
+      int hit = 0;
+      if (c->kind == PAIR_PLANE) {
+        REAL pen = (px - c->p[0]) * c->n[0] + (py - c->p[1]) * c->n[1];
+        if (pen < (REAL)0.0) {
+          fx = -(c->n[0] * c->penalty * pen);
+          fy = -(c->n[1] * c->penalty * pen);
+          hit = 1;
+        }
+      } else if (c->kind == PAIR_HEIGHTFIELD) {
+        REAL n0, n1;
+        REAL sg = hf_signed(c, px, py, &n0, &n1);
+        if (sg < (REAL)0.0) {
+          fx = -n0 * c->penalty * sg;
+          fy = -n1 * c->penalty * sg;
+          REAL vn = vx * n0 + vy * n1;
+          if (vn < (REAL)0.0) {
+            fx = fx + (-n0 * (REAL)0.5 * c->penalty * vn * dt);
+            fy = fy + (-n1 * (REAL)0.5 * c->penalty * vn * dt);
+          }
+          hit = 1;
+        }
+      } else {
+        REAL n0, n1;
+        REAL sd = voxel_signed(c, px, py, &n0, &n1);
+        if (sd < (REAL)0.0) {
+          REAL pen = -sd;
+          fx = n0 * c->penalty * pen;
+          fy = n1 * c->penalty * pen;
+          REAL vn = vx * n0 + vy * n1;
+          if (vn < (REAL)0.0) {
+            fx = fx + (-n0 * (REAL)0.5 * c->penalty * vn * dt);
+            fy = fy + (-n1 * (REAL)0.5 * c->penalty * vn * dt);
+          }
+          hit = 1;
+        }
+      }
+      if (hit) {
+        w->fext[2 * nid] += fx;
+        w->fext[2 * nid + 1] += fy;
+      }
+    }
+  }
+}
+
+/* _integrate_nodes_kernel (femspringmanager.py:315-358) for node i. */
+static void integrate_node(or_world* w, int i, REAL dt, REAL damping) {
+  int bc = w->bc[i];
+  REAL fx = w->fext[2 * i], fy = w->fext[2 * i + 1];
+  REAL m = w->mass[i];
+  REAL bx = w->bcv[2 * i], by = w->bcv[2 * i + 1];
+  if (bc & BC_U) {
+    fx = 0;
+    fy = 0;
+  } else if (bc & BC_A) {
+    fx = m * bx;
+    fy = m * by;
+  } else if (bc & BC_GRAVITY) {
+    fx = fx + m * bx;
+    fy = fy + m * by;
+  } else if (bc & BC_FORCE) {
+    fx = fx + bx;
+    fy = fy + by;
+  }
+  REAL vx = w->v[2 * i], vy = w->v[2 * i + 1];
+  REAL im = (REAL)1.0 / m;
+  REAL ax = (REAL)0.0 + (fx - damping * vx) * im;
+  REAL ay = (REAL)0.0 + (fy - damping * vy) * im;
+  REAL nvx = vx + ax * dt, nvy = vy + ay * dt;
+  if (bc & BC_V) {
+    nvx = bx;
+    nvy = by;
+  } else if (bc & BC_U) {
+    nvx = 0;
+    nvy = 0;
+  }
+  w->v[2 * i] = nvx;
+  w->v[2 * i + 1] = nvy;
+  REAL dux = nvx * dt, duy = nvy * dt;
+  w->u[2 * i] = w->u[2 * i] + dux;
+  w->u[2 * i + 1] = w->u[2 * i + 1] + duy;
+  w->x[2 * i] = w->x[2 * i] + dux;
+  w->x[2 * i + 1] = w->x[2 * i + 1] + duy;
+}
+
+/* _update_bbox_kernel (femspringmanager.py:361-408). */
+static void update_bbox(or_world* w) {
+  for (int b = 0; b < w->n_bodies; ++b) {
+    REAL lbx = (REAL)1e30, lby = (REAL)1e30, ubx = (REAL)-1e30, uby = (REAL)-1e30;
+    for (int k = 0; k < w->bn_cnt[b]; ++k) {
+      int nid = w->bnodes[w->bn_off[b] + k];
+      REAL px = w->x[2 * nid], py = w->x[2 * nid + 1];
+      lbx = lbx < px ? lbx : px;
+      lby = lby < py ? lby : py;
+      ubx = ubx > px ? ubx : px;
+      uby = uby > py ? uby : py;
+    }
+    w->aabb[4 * b] = lbx;
+    w->aabb[4 * b + 1] = lby;
+    w->aabb[4 * b + 2] = ubx;
+    w->aabb[4 * b + 3] = uby;
+  }
+}
+
+static void build_csr(or_world* w) {
+  int N = w->n_nodes, E = w->n_elems;
+  w->csr_off = (int32_t*)calloc((size_t)N + 1, sizeof(int32_t));
+  w->csr_slot = (int32_t*)malloc(sizeof(int32_t) * (3 * (size_t)E + 1));
+  w->corner = (REAL*)malloc(sizeof(REAL) * (6 * (size_t)E + 1));
+  for (int e = 0; e < E; ++e)
+    for (int c = 0; c < 3; ++c) w->csr_off[w->conn[3 * e + c] + 1]++;
+  for (int i = 0; i < N; ++i) w->csr_off[i + 1] += w->csr_off[i];
+  int32_t* fill = (int32_t*)malloc(sizeof(int32_t) * ((size_t)N + 1));
+  for (int i = 0; i < N; ++i) fill[i] = w->csr_off[i];
+  for (int e = 0; e < E; ++e)
+    for (int c = 0; c < 3; ++c) w->csr_slot[fill[w->conn[3 * e + c]]++] = 3 * e + c;
+  free(fill);
+}
+
+
+/* ------------------------------------------------------------ threading */
+
+typedef struct {
+  or_world* w;
+  int lo, hi;
+  REAL dt, damping;
+  void (*fn)(or_world*, int, int, REAL, REAL);
+} par_job;
+
+static void elem_range(or_world* w, int lo, int hi, REAL dt, REAL damping) {
+  (void)dt;
+  (void)damping;
+  for (int e = lo; e < hi; ++e) element_force(w, e, w->corner + 6 * (size_t)e);
+}
+
+static void node_range(or_world* w, int lo, int hi, REAL dt, REAL damping) {
+  for (int i = lo; i < hi; ++i) {
+    REAL fx = w->fext[2 * i], fy = w->fext[2 * i + 1];
+    for (int k = w->csr_off[i]; k < w->csr_off[i + 1]; ++k) {
+      int s = w->csr_slot[k];
+      int e = s / 3, c = s % 3;
+      fx += w->corner[6 * (size_t)e + 2 * c];
+      fy += w->corner[6 * (size_t)e + 2 * c + 1];
+    }
+    w->fext[2 * i] = fx;
+    w->fext[2 * i + 1] = fy;
+    integrate_node(w, i, dt, damping);
+  }
+}
+
+static void* par_worker(void* arg) {
+  par_job* j = (par_job*)arg;
+  j->fn(j->w, j->lo, j->hi, j->dt, j->damping);
+  return NULL;
+}
+
+static REAL g_step_dt, g_step_damping;
+
+static void par_for(or_world* w, int n, void (*fn)(or_world*, int, int, REAL, REAL)) {
+  int T = w->n_threads;
+  if (T > 256) T = 256;
+  pthread_t th[256];
+  par_job jobs[256];
+  int chunk = (n + T - 1) / T;
+  for (int t = 0; t < T; ++t) {
+    jobs[t].w = w;
+    jobs[t].lo = t * chunk < n ? t * chunk : n;
+    jobs[t].hi = (t + 1) * chunk < n ? (t + 1) * chunk : n;
+    jobs[t].dt = g_step_dt;
+    jobs[t].damping = g_step_damping;
+    jobs[t].fn = fn;
+    if (t > 0) pthread_create(&th[t], NULL, par_worker, &jobs[t]);
+  }
+  par_worker(&jobs[0]);
+  for (int t = 1; t < T; ++t) pthread_join(th[t], NULL);
+}
+
+/* ---------------------------------------------------------------- C API */
+
+or_world* or_create(int n_nodes, const float* x, const float* v, const int32_t* bc, const float* bcv,
+                    int n_elems, const int32_t* conn, const int32_t* type, const float* E,
+                    const float* nu, const float* rho, const float* sy, const float* H,
+                    int n_bodies, const int32_t* bn_off, const int32_t* bn_cnt,
+                    int n_bnodes, const int32_t* bnodes) {
+  or_world* w = (or_world*)calloc(1, sizeof(or_world));
+  w->n_nodes = n_nodes;
+  w->n_elems = n_elems;
+  w->n_bodies = n_bodies;
+  w->n_threads = 1;
+  w->x = dupf(x, 2 * (size_t)n_nodes);
+  w->v = dupf(v, 2 * (size_t)n_nodes);
+  w->u = (REAL*)calloc(2 * (size_t)n_nodes + 1, sizeof(REAL));
+  w->fext = (REAL*)calloc(2 * (size_t)n_nodes + 1, sizeof(REAL));
+  w->mass = (REAL*)calloc((size_t)n_nodes + 1, sizeof(REAL));
+  w->bc = dupi(bc, n_nodes);
+  w->bcv = dupf(bcv, 2 * (size_t)n_nodes);
+  w->conn = dupi(conn, 3 * (size_t)n_elems);
+  w->type = dupi(type, n_elems);
+  w->E = dupf(E, n_elems);
+  w->nu = dupf(nu, n_elems);
+  w->rho = dupf(rho, n_elems);
+  w->sy = dupf(sy, n_elems);
+  w->H = dupf(H, n_elems);
+  w->area = (REAL*)calloc((size_t)n_elems + 1, sizeof(REAL));
+  w->jinv = (REAL*)calloc(4 * (size_t)n_elems + 1, sizeof(REAL));
+  w->epsp = (REAL*)calloc(3 * (size_t)n_elems + 1, sizeof(REAL));
+  w->eqps = (REAL*)calloc((size_t)n_elems + 1, sizeof(REAL));
+  w->bn_off = dupi(bn_off, n_bodies);
+  w->bn_cnt = dupi(bn_cnt, n_bodies);
+  w->bnodes = dupi(bnodes, n_bnodes);
+  w->aabb = (REAL*)calloc(4 * (size_t)n_bodies + 1, sizeof(REAL));
+  w->pairs = NULL;
+  w->n_pairs = 0;
+  prepare(w);
+  build_csr(w);
+  return w;
+}
+
+static or_pair* new_pair(or_world* w) {
+  w->pairs = (or_pair*)realloc(w->pairs, sizeof(or_pair) * (size_t)(w->n_pairs + 1));
+  or_pair* c = &w->pairs[w->n_pairs++];
+  memset(c, 0, sizeof(*c));
+  return c;
+}
+
+/* Pairs must be added in launch order: planes, then heightfields, then voxels
+ * (mixedcontact.py:1657-1754), each group in contact-creation order. */
+int or_add_plane(or_world* w, int body, float penalty, const float* glb, const float* gub,
+                 float px, float py, float nx, float ny) {
+  or_pair* c = new_pair(w);
+  c->kind = PAIR_PLANE;
+  c->body = body;
+  c->penalty = penalty;
+  c->glb[0] = glb[0]; c->glb[1] = glb[1]; c->gub[0] = gub[0]; c->gub[1] = gub[1];
+  c->p[0] = px; c->p[1] = py; c->n[0] = nx; c->n[1] = ny;
+  return w->n_pairs - 1;
+}
+
+int or_add_heightfield(or_world* w, int body, float penalty, const float* glb, const float* gub,
+                       int nx, const float* h, float lbx, float ubx, int reverse) {
+  or_pair* c = new_pair(w);
+  c->kind = PAIR_HEIGHTFIELD;
+  c->body = body;
+  c->penalty = penalty;
+  c->glb[0] = glb[0]; c->glb[1] = glb[1]; c->gub[0] = gub[0]; c->gub[1] = gub[1];
+  c->hnx = nx;
+  c->h = dupf(h, nx);
+  c->hlbx = lbx;
+  c->hubx = ubx;
+  c->reverse = reverse;
+  return w->n_pairs - 1;
+}
+
+int or_add_voxel(or_world* w, int body, float penalty, const float* glb, const float* gub,
+                 int nx, int ny, const int32_t* occ, float lbx, float lby, float dx, float dz) {
+  or_pair* c = new_pair(w);
+  c->kind = PAIR_VOXEL;
+  c->body = body;
+  c->penalty = penalty;
+  c->glb[0] = glb[0]; c->glb[1] = glb[1]; c->gub[0] = gub[0]; c->gub[1] = gub[1];
+  c->vnx = nx;
+  c->vny = ny;
+  c->occ = dupi(occ, (size_t)nx * ny);
+  c->vlb[0] = lbx; c->vlb[1] = lby; c->vdx = dx; c->vdz = dz;
+  return w->n_pairs - 1;
+}
+
+void or_set_threads(or_world* w, int n) { w->n_threads = n < 1 ? 1 : n; }
+
+/* One FemSpringManager.femStep plus, unless init_step, the contact launches of
+ * ExplicitLoop.advance that precede it.  init_step reproduces the zero-dt step
+ * setGlobalAABB runs at construction (femspringmanager.py:872-879). */
+void or_step(or_world* w, float dt_f, float damping_f, long counter, int init_step) {
+  REAL dt = (REAL)dt_f, damping = (REAL)damping_f;
+  int N = w->n_nodes, E = w->n_elems;
+  g_step_dt = dt;
+  g_step_damping = damping;
+  for (int i = 0; i < 2 * N; ++i) w->fext[i] = 0;
+  if (!init_step) contacts(w, dt, counter);
+  if (w->n_threads <= 1) {
+    REAL f[6];
+    for (int e = 0; e < E; ++e) {
+      element_force(w, e, f);
+      int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
+      w->fext[2 * n1] += f[0];
+      w->fext[2 * n1 + 1] += f[1];
+      w->fext[2 * n2] += f[2];
+      w->fext[2 * n2 + 1] += f[3];
+      w->fext[2 * n3] += f[4];
+      w->fext[2 * n3 + 1] += f[5];
+    }
+    for (int i = 0; i < N; ++i) integrate_node(w, i, dt, damping);
+  } else {
+    /* Threaded variant: element forces into a corner buffer, then each node
+     * sums its corners in ascending element order -- the same additions in
+     * the same order as the serial scatter above, so identical bits. */
+    par_for(w, E, elem_range);
+    par_for(w, N, node_range);
+  }
+  update_bbox(w);
+}
+
+void or_get_state(const or_world* w, double* x, double* v, double* u) {
+  for (int i = 0; i < 2 * w->n_nodes; ++i) {
+    if (x) x[i] = (double)w->x[i];
+    if (v) v[i] = (double)w->v[i];
+    if (u) u[i] = (double)w->u[i];
+  }
+}
+
+void or_get_prepared(const or_world* w, double* mass, double* area, double* jinv) {
+  for (int i = 0; i < w->n_nodes; ++i)
+    if (mass) mass[i] = (double)w->mass[i];
+  for (int e = 0; e < w->n_elems; ++e) {
+    if (area) area[e] = (double)w->area[e];
+    for (int k = 0; k < 4; ++k)
+      if (jinv) jinv[4 * e + k] = (double)w->jinv[4 * e + k];
+  }
+}
+
+void or_get_plastic(const or_world* w, double* epsp, double* eqps) {
+  for (int e = 0; e < w->n_elems; ++e) {
+    for (int k = 0; k < 3; ++k)
+      if (epsp) epsp[3 * e + k] = (double)w->epsp[3 * e + k];
+    if (eqps) eqps[e] = (double)w->eqps[e];
+  }
+}
+
+void or_get_aabb(const or_world* w, double* aabb) {
+  for (int i = 0; i < 4 * w->n_bodies; ++i) aabb[i] = (double)w->aabb[i];
+}
+
+/* Copy x (and v) from float arrays: lets a test restart the oracle from a
+ * state that the GPU produced, to measure one-step error in isolation. */
+void or_set_state(or_world* w, const float* x, const float* v) {
+  for (int i = 0; i < 2 * w->n_nodes; ++i) {
+    if (x) w->x[i] = (REAL)x[i];
+    if (v) w->v[i] = (REAL)v[i];
+  }
+}
+
+/* Stress of one material point, for unit tests of the material laws
+ * (test2D/test_2Dmaterial_functions.py:85-105). */
+void or_point_stress(int type, float E, float nu, float sy, float H, const float* F,
+                     const float* epsp_in, float eqps_in, double* s_out, double* epsp_out,
+                     double* eqps_out) {
+  or_world w;
+  memset(&w, 0, sizeof(w));
+  REAL Ev = E, nuv = nu, syv = sy, Hv = H, eqv = eqps_in;
+  REAL ep[3] = {epsp_in ? epsp_in[0] : 0, epsp_in ? epsp_in[1] : 0, epsp_in ? epsp_in[2] : 0};
+  int32_t t = type;
+  w.E = &Ev; w.nu = &nuv; w.sy = &syv; w.H = &Hv; w.type = &t; w.epsp = ep; w.eqps = &eqv;
+  REAL s[3], epo[3], eqo;
+  stress(&w, 0, F[0], F[1], F[2], F[3], s, epo, &eqo);
+  for (int k = 0; k < 3; ++k) {
+    s_out[k] = s[k];
+    if (epsp_out) epsp_out[k] = (type == MAT_MISES) ? epo[k] : ep[k];
+  }
+  if (eqps_out) *eqps_out = (type == MAT_MISES) ? eqo : eqv;
+}
+
+void or_destroy(or_world* w) {
+  if (!w) return;
+  free(w->x); free(w->v); free(w->u); free(w->fext); free(w->mass); free(w->bc); free(w->bcv);
+  free(w->conn); free(w->type); free(w->E); free(w->nu); free(w->rho); free(w->sy); free(w->H);
+  free(w->area); free(w->jinv); free(w->epsp); free(w->eqps);
+  free(w->bn_off); free(w->bn_cnt); free(w->bnodes); free(w->aabb);
+  for (int i = 0; i < w->n_pairs; ++i) {
+    free(w->pairs[i].h);
+    free(w->pairs[i].occ);
+  }
+  free(w->pairs);
+  free(w->csr_off); free(w->csr_slot); free(w->corner);
+  free(w);
+}

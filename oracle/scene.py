@@ -1,0 +1,337 @@
+"""Oracle driver: literal restatement of the reference's host-side construction
+and stepping logic, running the C oracle (fw_oracle.c) for the device work.
+
+TEST INFRASTRUCTURE ONLY -- imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU legs as the checker; never by the product package.
+
+It deliberately shares no code with flatworld_b200: boundary edges, edge
+lengths, stable time, contact pairs, penalties, work lists and BC packing are
+recomputed here with the reference's own loops:
+  flatworld/mesh.py:40-112                 boundary edges, char lengths
+  flatworld/femdomain.py:24                FemDomain.stableTime
+  flatworld/femcontact.py:94-141, 155-197  penalty 2K, contact stable time
+  flatworld/explicitloop.py:145-334        stable dt, O(D^2) contact pairs
+  flatworld/femspringmanager.py:660-813    packing, processConditions
+  flatworld/mixedcontact.py:1794-2261      work lists (one HF / voxel domain)
+  flatworld/grounddomain.py:54-70, heightfielddomain.py:26-27,190-194,
+  voxeldomain.py:194-195                   broad-phase boxes
+  flatworld/explicitloop.py:558-589        advanceWithTime substep loop
+Domain objects are read through the reference's attribute names only
+(mesh.coords, mesh.connectivity, prop.mat, bcs, initials, point, normal,
+height, lb, ub, reverse, occ, nx, ny, dx, dz, considerContact, type, ...).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from collections import defaultdict
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# flatworld/definitions.py
+FEM, ANALYTICAL, RIGID, SPRINGMASS, HEIGHTFIELD, VOXELMAP = 0b10, 0b1, 0b100, 0b1000, 0b100000, 0b1000000
+FLEXANLAYTICAL, FLEXFLEX, FEXHEIGHTFIELD, FLEXVOXELMAP = 0b11, 0b10, 0b100010, 0b1000010
+RIGIDRIGID, RIGIDANLAYTICAL, ANALYTICALANALYTICAL = 0b100, 0b101, 0b1
+
+_LIBS = {}
+_f32p = C.POINTER(C.c_float)
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+
+
+def _lib(precision: str):
+    name = {"f32": "liboracle_f32.so", "f32fma": "liboracle_f32fma.so", "f64": "liboracle_f64.so"}[precision]
+    if name not in _LIBS:
+        path = os.path.join(HERE, name)
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle`")
+        L = C.CDLL(path)
+        L.or_create.restype = C.c_void_p
+        L.or_create.argtypes = [C.c_int, _f32p, _f32p, _i32p, _f32p, C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p,
+                                _f32p, _f32p, C.c_int, _i32p, _i32p, C.c_int, _i32p]
+        L.or_add_plane.argtypes = [C.c_void_p, C.c_int, C.c_float, _f32p, _f32p, C.c_float, C.c_float, C.c_float,
+                                   C.c_float]
+        L.or_add_heightfield.argtypes = [C.c_void_p, C.c_int, C.c_float, _f32p, _f32p, C.c_int, _f32p, C.c_float,
+                                         C.c_float, C.c_int]
+        L.or_add_voxel.argtypes = [C.c_void_p, C.c_int, C.c_float, _f32p, _f32p, C.c_int, C.c_int, _i32p,
+                                   C.c_float, C.c_float, C.c_float, C.c_float]
+        L.or_set_threads.argtypes = [C.c_void_p, C.c_int]
+        L.or_step.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_long, C.c_int]
+        L.or_get_state.argtypes = [C.c_void_p, _f64p, _f64p, _f64p]
+        L.or_get_prepared.argtypes = [C.c_void_p, _f64p, _f64p, _f64p]
+        L.or_get_plastic.argtypes = [C.c_void_p, _f64p, _f64p]
+        L.or_get_aabb.argtypes = [C.c_void_p, _f64p]
+        L.or_set_state.argtypes = [C.c_void_p, _f32p, _f32p]
+        L.or_point_stress.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _f32p, _f32p, C.c_float,
+                                      _f64p, _f64p, _f64p]
+        L.or_destroy.argtypes = [C.c_void_p]
+        _LIBS[name] = L
+    return _LIBS[name]
+
+
+def _fp(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(_f32p)
+
+
+def _ip(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_i32p)
+
+
+# ---------------------------------------------------------------- host restatement
+
+def boundary_nodes_literal(conns):
+    """mesh.py:53-71 and 40-47, loop for loop."""
+    edge_count = defaultdict(int)
+    for cell in np.asarray(conns).tolist():
+        for i in range(3):
+            v1, v2 = cell[i], cell[(i + 1) % 3]
+            if (v2, v1) in edge_count:
+                edge_count[(v2, v1)] += 1
+            else:
+                edge_count[(v1, v2)] += 1
+    nodes = set()
+    for e, c in edge_count.items():
+        if c == 1:
+            nodes.update(e)
+    return np.array(sorted(nodes), dtype=np.int64)
+
+
+def char_length_literal(conns, coords):
+    """mesh.py:73-78, 90-112: min over float32 norm(a - b) of element edges."""
+    coords = np.asarray(coords)
+    lengths = []
+    for conn in np.asarray(conns):
+        for ia, ib in ((0, 1), (1, 2), (2, 0)):
+            lengths.append(np.linalg.norm(coords[conn[ia]] - coords[conn[ib]]))
+    return float(np.min(np.asarray(lengths, dtype=np.float32)))
+
+
+def point_stress(mtype, E, nu, F, sigma_y=0.0, H=0.0, eps_p=None, eqps=0.0, precision="f32"):
+    """One material-point evaluation of getStress2D / misesReturnMap2D."""
+    L = _lib(precision)
+    Fa = _fp(np.asarray(F, np.float32).reshape(4))
+    ep = _fp(np.zeros(3, np.float32) if eps_p is None else eps_p)
+    s = np.zeros(3)
+    epo = np.zeros(3)
+    eqo = np.zeros(1)
+    L.or_point_stress(int(mtype), float(E), float(nu), float(sigma_y), float(H), Fa[1], ep[1], float(eqps),
+                      s.ctypes.data_as(_f64p), epo.ctypes.data_as(_f64p), eqo.ctypes.data_as(_f64p))
+    return s, epo, float(eqo[0])
+
+
+class OracleLoop:
+    """CPU restatement of one reference ExplicitLoop over FEM + ground domains."""
+
+    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, precision="f32", threads=1):
+        self.precision = precision
+        L = self._L = _lib(precision)
+        self.domains = list(domains)
+        fem = [d for d in domains if d.type == FEM]
+        self.fem = fem
+        # --- stable time (explicitloop.py:145-170, femdomain.py:24)
+        stable = 1.0
+        if any(d.type in (RIGID, ANALYTICAL) for d in domains):
+            stable = min(1.0 / 1000.0, stable)
+        self.char_len = [char_length_literal(d.mesh.connectivity, d.mesh.coords) for d in fem]
+        fsm = 1.0
+        for d, Lc in zip(fem, self.char_len):
+            fsm = min(0.4 * Lc / (d.prop.mat.E / d.prop.mat.rho) ** 0.5, fsm)
+        stable = min(fsm, stable)
+        # --- contacts (explicitloop.py:237-277; femcontact.py:155-197)
+        contacts = []
+        cds = [(i, d) for i, d in enumerate(domains) if d.considerContact]
+        if any(d.type == FEM for d in domains if d.considerContact):
+            for a, (i, di) in enumerate(cds):
+                for b in range(a):
+                    j, dj = cds[b]
+                    ct = di.type | dj.type
+                    if di.category_bits & dj.collide_bits == 0 or di.collide_bits & dj.category_bits == 0:
+                        continue
+                    if ct in (RIGIDRIGID, RIGIDANLAYTICAL, ANALYTICALANALYTICAL):
+                        continue
+                    if ct not in (FLEXANLAYTICAL, FEXHEIGHTFIELD, FLEXVOXELMAP):
+                        if ct == FLEXFLEX:
+                            raise NotImplementedError("FEM-FEM contact is not restated")
+                        continue
+                    femd, gnd = (di, dj) if di.type == FEM else (dj, di)
+                    mat = femd.prop.mat
+                    nu = min(mat.nu, 0.4999)
+                    K = mat.E / (3.0 * (1.0 - 2.0 * nu))
+                    pen = 2.0 * 1.0 * K * 1.0
+                    Lc = self.char_len[fem.index(femd)]
+                    m_node = mat.rho * (Lc * Lc * 0.5) / 3.0
+                    contacts.append((ct, femd, gnd, pen, 0.9 * (m_node / pen) ** 0.5))
+        for c in contacts:
+            stable = min(stable, c[4])
+        self.stableTime = stable
+        self.useAdapative = useAdapativeDT
+        self.default_dt = dt
+        self.dt = stable if useAdapativeDT else dt
+        self.damping = damping
+        self.contacts = contacts
+        # --- packing (femspringmanager.py:706-813, 660-705)
+        xs, vs, bcs, bcv, conns, types, Es, nus, rhos, sys_, Hs = [], [], [], [], [], [], [], [], [], [], []
+        bn_off, bn_cnt, bnodes = [], [], []
+        off = 0
+        self.node_ranges = []
+        for d in fem:
+            m = d.mesh
+            nn = m.numNodes
+            c = np.asarray(m.coords, dtype=np.float32)[:, :2]
+            xs.append(c)
+            v = np.zeros((nn, 2), np.float32)
+            bits = np.zeros(nn, np.int64)
+            vals = np.zeros((nn, 2), np.float32)
+            for bc in d.bcs:
+                t, nodes, values = bc.processData()
+                if values is None:
+                    values = [0.0] * d.d
+                if nodes is None:
+                    nodes = range(nn)
+                for idx in nodes:
+                    nd = int(idx)
+                    bits[nd] |= int(t)
+                    vals[nd, 0] = float(values[0])
+                    vals[nd, 1] = float(values[1])
+            for ic in d.initials:
+                vx, vy = float(ic.vel[0]), float(ic.vel[1])
+                if getattr(ic, "is_all_nodes", False):
+                    v[:, 0] = vx
+                    v[:, 1] = vy
+                else:
+                    for nid in np.asarray(ic.nds):
+                        v[int(nid)] = (vx, vy)
+            vs.append(v)
+            bcs.append(bits)
+            bcv.append(vals)
+            conns.append(np.asarray(m.connectivity, np.int64)[:, :3] + off)
+            ne = m.numElements
+            mat = d.prop.getMaterial()
+            types.append(np.full(ne, int(mat.type)))
+            Es.append(np.full(ne, float(mat.E), np.float32))
+            nus.append(np.full(ne, float(mat.nu), np.float32))
+            rhos.append(np.full(ne, float(mat.rho), np.float32))
+            sys_.append(np.full(ne, float(getattr(mat, "sigma_y", 0.0)), np.float32))
+            Hs.append(np.full(ne, float(getattr(mat, "H", 0.0)), np.float32))
+            bn = boundary_nodes_literal(m.connectivity) + off
+            bn_off.append(sum(len(x) for x in bnodes))
+            bn_cnt.append(len(bn))
+            bnodes.append(bn)
+            self.node_ranges.append((off, nn))
+            off += nn
+        self.N = off
+        self.E = sum(len(t) for t in types)
+        cat = np.concatenate
+        self._keep = [_fp(cat(xs)), _fp(cat(vs)), _ip(cat(bcs)), _fp(cat(bcv)), _ip(cat(conns)), _ip(cat(types)),
+                      _fp(cat(Es)), _fp(cat(nus)), _fp(cat(rhos)), _fp(cat(sys_)), _fp(cat(Hs)), _ip(bn_off),
+                      _ip(bn_cnt), _ip(cat(bnodes))]
+        k = self._keep
+        self._w = L.or_create(self.N, k[0][1], k[1][1], k[2][1], k[3][1], self.E, k[4][1], k[5][1], k[6][1],
+                              k[7][1], k[8][1], k[9][1], k[10][1], len(fem), k[11][1], k[12][1], len(k[13][0]),
+                              k[13][1])
+        L.or_set_threads(self._w, int(threads))
+        # --- work lists in launch order (mixedcontact.py:1794-2261)
+        anal = [c for c in contacts if c[0] == FLEXANLAYTICAL]
+        hf = [c for c in contacts if c[0] == FEXHEIGHTFIELD]
+        vox = [c for c in contacts if c[0] == FLEXVOXELMAP]
+        if len({id(c[2]) for c in hf}) > 1:
+            hf = []
+        if len({id(c[2]) for c in vox}) > 1:
+            vox = []
+        for ct, femd, g, pen, _ in anal + hf + vox:
+            body = fem.index(femd)
+            lo, hi = self._ground_box(g)
+            pen32 = float(np.float32(pen))
+            if ct == FLEXANLAYTICAL:
+                pt = np.asarray(g.point, np.float32)
+                nm = np.asarray(g.normal, np.float32)
+                L.or_add_plane(self._w, body, pen32, lo[1], hi[1], float(pt[0]), float(pt[1]), float(nm[0]),
+                               float(nm[1]))
+            elif ct == FEXHEIGHTFIELD:
+                h = _fp(g.height)
+                L.or_add_heightfield(self._w, body, pen32, lo[1], hi[1], len(h[0]), h[1], float(g.lb[0]),
+                                     float(g.ub[0]), 1 if g.reverse else 0)
+            else:
+                occ = _ip(np.asarray(g.occ, np.int32))
+                L.or_add_voxel(self._w, body, pen32, lo[1], hi[1], int(g.nx), int(g.ny), occ[1], float(g.lb[0]),
+                               float(g.lb[1]), float(np.float32(g.dx)), float(np.float32(g.dz)))
+        self.counter = 0
+        # setGlobalAABB -> substep(0.0, 0.0) (femspringmanager.py:872-879)
+        L.or_step(self._w, 0.0, 0.0, 0, 1)
+
+    @staticmethod
+    def _ground_box(g):
+        if g.type == ANALYTICAL:
+            n = np.asarray(g.normal, np.float32)
+            p = np.asarray(g.point, np.float32)
+            t = np.array([-n[1], n[0]], dtype=np.float32)
+            lo_raw = p - t * 10000.0 - n * 0.1
+            hi_raw = p + t * 10000.0 + n * 0.1
+            lo, hi = np.minimum(lo_raw, hi_raw), np.maximum(lo_raw, hi_raw)
+        elif g.type == HEIGHTFIELD:
+            h = np.asarray(g.height, np.float32)
+            lo = np.array([g.lb[0], float(np.min(h)) - 0.1], dtype=np.float32)
+            hi = np.array([g.ub[0], float(np.max(h)) + 0.1], dtype=np.float32)
+        else:
+            lo, hi = np.asarray(g.lb, np.float32), np.asarray(g.ub, np.float32)
+        return _fp(lo), _fp(hi)
+
+    def close(self):
+        if getattr(self, "_w", None):
+            self._L.or_destroy(self._w)
+            self._w = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, n: int = 1, dt: float | None = None):
+        d = self.dt if dt is None else dt
+        for _ in range(n):
+            self._L.or_step(self._w, float(np.float32(d)), float(np.float32(self.damping)), self.counter, 0)
+            self.counter += 1
+
+    def advance_with_time(self, frame_dt=1.0 / 60.0):
+        remaining = float(frame_dt)
+        while remaining > 1e-12:
+            cur = self.stableTime if self.useAdapative else self.default_dt
+            sub = max(min(cur, remaining), 1e-8)
+            self.dt = sub
+            self.advance(1)
+            remaining -= sub
+
+    def state(self):
+        x = np.zeros((self.N, 2))
+        v = np.zeros((self.N, 2))
+        u = np.zeros((self.N, 2))
+        self._L.or_get_state(self._w, x.ctypes.data_as(_f64p), v.ctypes.data_as(_f64p), u.ctypes.data_as(_f64p))
+        return x, v, u
+
+    def set_state(self, x, v):
+        xa, va = _fp(x), _fp(v)
+        self._L.or_set_state(self._w, xa[1], va[1])
+
+    def prepared(self):
+        m = np.zeros(self.N)
+        a = np.zeros(self.E)
+        j = np.zeros((self.E, 4))
+        self._L.or_get_prepared(self._w, m.ctypes.data_as(_f64p), a.ctypes.data_as(_f64p), j.ctypes.data_as(_f64p))
+        return m, a, j
+
+    def plastic(self):
+        ep = np.zeros((self.E, 3))
+        eq = np.zeros(self.E)
+        self._L.or_get_plastic(self._w, ep.ctypes.data_as(_f64p), eq.ctypes.data_as(_f64p))
+        return ep, eq
+
+    def aabb(self):
+        out = np.zeros((len(self.fem), 4))
+        self._L.or_get_aabb(self._w, out.ctypes.data_as(_f64p))
+        return out

@@ -1,0 +1,119 @@
+"""Scene builders shared by the tests and the benchmark (seeded, synthetic).
+
+The small scenes restate the reference's own test fixtures
+(test2D/test_2Dfem_elastic.py:17-25, test_2Dfem_elastic10000.py:17-32,
+test_2Dfem_force.py:17-24, test_2Dfem_heightfield_contact.py:14-46,
+test_2Dfem_voxel_contact.py:14-50); the large ones follow the benchmark
+workload descriptions (plain small / large mesh, ragged batch, gradient block).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def two_triangle_square(fw, bcs_fn=None, mat=None):
+    conn = np.array([[0, 1, 3], [0, 3, 2]], dtype=np.int32)
+    coords = np.array([[0.5, 0.5], [0.7, 0.5], [0.5, 0.7], [0.7, 0.7]], dtype=np.float32)
+    mesh = fw.Mesh(2, conn, coords)
+    mat = mat or fw.Elastic(E=2e4, nu=0.2, rho=40.0)
+    bcs = bcs_fn() if bcs_fn else [fw.Gravity([0, -1.0])]
+    return fw.FemDomain(mesh, fw.SolidProp(mat), bcs)
+
+
+def elastic10000_mesh(fw, num_el=100):
+    """test_2Dfem_elastic10000.py:17-32, loop for loop."""
+    dx = 0.6 / num_el
+    conn = np.zeros((2 * num_el * num_el, 3), dtype=np.int32)
+    coords = np.zeros(((num_el + 1) * (num_el + 1), 2), dtype=np.float32)
+    nd = 0
+    for i in range(num_el + 1):
+        for j in range(num_el + 1):
+            coords[nd] = np.array([dx * i, dx * j])
+            nd += 1
+    el = 0
+    for i in range(num_el):
+        for j in range(num_el):
+            conn[el] = [i * (num_el + 1) + j, i * (num_el + 1) + j + 1, (i + 1) * (num_el + 1) + j]
+            conn[el + 1] = [i * (num_el + 1) + j + 1, (i + 1) * (num_el + 1) + j + 1, (i + 1) * (num_el + 1) + j]
+            el += 2
+    return fw.Mesh(2, conn, coords + 0.3)
+
+
+def heightfield_bowl(nx=513, cx=0.5, r=0.5, zc=0.7):
+    xs = np.linspace(0.0, 1.0, nx, dtype=np.float32)
+    h = np.empty(nx, dtype=np.float32)
+    for i, x in enumerate(xs):
+        dx = x - cx
+        inside = r * r - dx * dx
+        h[i] = zc - np.sqrt(inside) if inside >= 0.0 else zc
+    return h
+
+
+def voxel_pit(nx=160, ny=100):
+    occ = np.zeros((nx, ny), dtype=np.int32)
+    cx = nx * 0.5
+    r = nx * 0.45
+    max_h = int(ny * 0.55)
+    for i in range(nx):
+        dx = i - cx
+        inside = r * r - dx * dx
+        if inside > 0:
+            depth = inside / (r * r)
+            h = int(max_h * (1.3 - depth))
+        else:
+            h = max_h
+        if h > 0:
+            occ[i, :h] = 1
+    return occ
+
+
+def hf_disk_scene(fw):
+    mesh = fw.FEMesher(2).createCircle([0.5, 0.65], 0.1)
+    fem = fw.FemDomain(mesh, fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)), [fw.Gravity([0.0, -10.0])],
+                       considerContact=True, initials=[])
+    hf = fw.HeightFieldDomain(2, heightfield_bowl(), lb=[0.0, 0.0], ub=[1.0, 1.0], considerContact=True)
+    return [hf, fem]
+
+
+def voxel_disk_scene(fw):
+    mesh = fw.FEMesher(2).createCircle([0.5, 0.75], 0.07)
+    fem = fw.FemDomain(mesh, fw.SolidProp(fw.Elastic(E=2e4, nu=0.25, rho=50.0)), [fw.Gravity([0.0, -9.8])],
+                       considerContact=True, initials=[])
+    vox = fw.VoxelGridDomain(d=2, nx=12, ny=8, lb=[0.0, 0.0], ub=[1.0, 1.0], considerContact=True,
+                             occupancy_np=voxel_pit(12, 8))
+    return [vox, fem]
+
+
+def plain_small_scene(fw, seed=0):
+    """Plain small workload: 1.0 x 0.25 rectangle at (0, 0.3), 64 x 16 quads
+    split in two (2048 triangles, 1105 nodes), interior nodes jittered
+    U(+-0.1h); Elastic E=2e4 nu=0.2 rho=40; gravity (0, -1); ground plane y=0."""
+    conn, coords = fw.structured_rectangle(64, 16, 1.0, 0.25, origin=(0.0, 0.3), jitter=0.1, seed=seed)
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)),
+                       [fw.Gravity([0.0, -1.0])])
+    ground = fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0])
+    return [ground, fem]
+
+
+def plain_large_scene(fw, seed=0, n=256, hf_offset=0.15):
+    """Plain large workload: unit square at (0, 0.2), n x n quads (n=256: 131072
+    triangles, 66049 nodes); NeoHookean E=1e5 nu=0.35 rho=100; v0 = (0, -0.5) +
+    N(0, 0.01^2) per component; height field of 4096 samples over x in [-1, 2],
+    sum of 8 sinusoids of total amplitude 0.05 with random phase, raised by
+    ``hf_offset`` so that the body reaches it within the run; no gravity."""
+    rng = np.random.default_rng(seed)
+    conn, coords = fw.structured_rectangle(n, n, 1.0, 1.0, origin=(0.0, 0.2))
+    nn = coords.shape[0]
+    v0 = np.array([0.0, -0.5]) + rng.normal(0.0, 0.01, size=(nn, 2))
+    ics = [fw.InitialVel([i], v0[i]) for i in range(nn)]
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.HyperElastic(E=1e5, nu=0.35, rho=100.0)), [],
+                       initials=ics)
+    xs = np.linspace(-1.0, 2.0, 4096)
+    amps = rng.uniform(0.5, 1.0, size=8)
+    amps = amps / amps.sum() * 0.05
+    omegas = 2.0 * np.pi * rng.uniform(0.5, 6.0, size=8)
+    phases = rng.uniform(0.0, 2.0 * np.pi, size=8)
+    h = hf_offset + sum(a * np.sin(w * xs + p) for a, w, p in zip(amps, omegas, phases))
+    hf = fw.HeightFieldDomain(2, h.astype(np.float32), lb=[-1.0, -1.0], ub=[2.0, 1.0])
+    return [hf, fem]
