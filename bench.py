@@ -289,8 +289,11 @@ def main():
                                    f"height field 4096 samples",
                        "elements": E, "nodes": N, "step": "advanceWithTime(1/60)",
                        "substeps_per_step": substeps, "dt": loop.stableTime,
-                       "l2": "flushed between steps (256 MiB write)", "replicas": world},
-            "roofline": {"bound": "hbm", "kernel": "substep = k_elements + k_nodes",
+                       "l2": "flushed between steps (256 MiB write)", "replicas": world,
+                       "path": {1: "gather", 2: "resident"}.get(loop.path, loop.path), "patches": loop.patches},
+            "roofline": {"bound": "hbm",
+                         "kernel": "k_resident (all substeps of a step)" if loop.path == 2 else
+                                   "substep = k_elements + k_nodes",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": which, "algorithmic_bytes_per_substep": bstep,
                          "us_per_substep": per_sub_s * 1e6,

@@ -19,6 +19,11 @@ FW_FIELD_V = 1
 FW_FIELD_MASS = 2
 FW_FIELD_X0 = 3
 
+FW_PATH_AUTO = 0
+FW_PATH_GATHER = 1
+FW_PATH_RESIDENT = 2
+PATHS = {"auto": FW_PATH_AUTO, "gather": FW_PATH_GATHER, "resident": FW_PATH_RESIDENT}
+
 _lock = threading.Lock()
 _lib = None
 
@@ -39,6 +44,8 @@ _SIGNATURES = {
     "fw_add_plane_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_float, C.c_float, C.c_float, C.c_float]),
     "fw_add_heightfield_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, _f32p, C.c_float, C.c_float, C.c_int32]),
     "fw_add_voxel_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, C.c_int32, _i32p, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_finalize": (C.c_int, [_vp]),
     "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_step_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
@@ -161,6 +168,15 @@ class NativeWorld:
         nx, ny = occ.shape
         self._check(self._L.fw_add_voxel_pair(self._h, body, penalty, lo[1], hi[1], nx, ny, o[1], float(lbx),
                                               float(lby), float(dx), float(dz)), "fw_add_voxel_pair")
+
+    def set_path(self, path: int, patches: int = 0):
+        self._check(self._L.fw_set_path(self._h, int(path), int(patches)), "fw_set_path")
+
+    def get_path(self):
+        p = C.c_int32()
+        n = C.c_int32()
+        self._check(self._L.fw_get_path(self._h, C.byref(p), C.byref(n)), "fw_get_path")
+        return int(p.value), int(n.value)
 
     def finalize(self):
         self._check(self._L.fw_finalize(self._h), "fw_finalize")

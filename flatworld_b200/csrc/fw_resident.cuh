@@ -1,0 +1,327 @@
+// fw_resident.cuh -- persistent, shared-memory-resident substep kernel.
+//
+// When the whole world fits in the SMs' shared memory (one scene, a few
+// hundred thousand triangles), the mesh is cut into patches, one per CTA
+// (recursive coordinate bisection of the nodes).  A patch owns a set of nodes
+// and holds every triangle that touches one of them (triangles on a cut are
+// held, and evaluated, by each patch that touches them), plus the positions of
+// the one-ring "halo" nodes it does not own.  One cooperative launch advances
+// all CTAs through n substeps; across substeps the patch's node state, element
+// data and corner forces never leave shared memory.  The only traffic per
+// substep is the positions of nodes that other patches read (published to a
+// double-buffered array in L2) and the body bounding boxes.
+//
+// Per substep, per CTA:
+//   1. corner forces of the patch's interior triangles (owned nodes only)
+//   2. wait for every CTA to have finished the previous substep (split-phase
+//      grid barrier: the arrive happened at the end of the previous substep,
+//      so step 1 overlaps the wait), then read the halo positions
+//   3. corner forces of the cut triangles; broad-phase gates from the body
+//      boxes of the previous substep
+//   4. owned nodes: contact, corner forces summed in ascending element order,
+//      boundary conditions, symplectic Euler; publish positions read by other
+//      patches; body-box reduction (ordered-int atomics)
+//   5. arrive at the barrier
+// The node sums use the same ascending-element order as the gather path, so
+// both paths produce identical bits.  Every wait is bounded: after
+// kSpinLimit polls the CTA sets the error flag and leaves the loop, so a
+// missing CTA cannot hang the device.
+#pragma once
+#include <cuda/atomic>
+
+namespace {
+
+constexpr int kResThreads = 512;
+constexpr int kResMaxPairs = 64;
+constexpr long long kSpinLimit = 1ll << 26;
+
+struct ResPatch {
+  int node_off, no;      // owned nodes: res.nodes[node_off .. +no)
+  int halo_off, nh;      // halo nodes: res.halo[halo_off .. +nh)
+  int elem_off, ne;      // patch triangles: interior first, each group ascending
+  int n_int;             // number of interior triangles
+  int csr_ptr_off;       // res.csr_ptr[csr_ptr_off .. +no+1): local offsets
+  int csr_off, ncsr;     // res.csr_slot[csr_off .. +ncsr)
+  int pad[2];
+};
+
+struct Res {
+  const ResPatch* patch;
+  const int32_t* nodes;     // owned global node ids; bit 31 = read by another patch
+  const int32_t* halo;      // halo global node ids
+  const uint2* conn;        // local corner ids: x = c0 | c1 << 16, y = c2 | flags << 16
+  const int32_t* eid;       // global triangle id of each patch triangle
+  const int32_t* csr_ptr;
+  const uint16_t* csr_slot; // 3 * local triangle + corner
+  float2* xpub;             // [2][N] published positions
+  int* aabb3;               // [3][B][4] ordered-int body boxes
+  int* bar;                 // arrivals counter (reset by the prologue)
+  int* err;                 // != 0: a wait gave up
+  int P, no_max, nh_max, ne_max, ncsr_max;
+  int has_j2;
+};
+
+constexpr uint32_t kExported = 0x80000000u;
+constexpr uint32_t kJ2Writer = 1u;  // flag bit in conn.y >> 16
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  cuda::atomic_ref<const int, cuda::thread_scope_device> a(*p);
+  return a.load(cuda::memory_order_acquire);
+}
+
+struct ResSmem {
+  float4* jinv;
+  ElemMat* mat;
+  float4* j2;
+  float2* j2p;
+  float2* f;
+  float2* x;
+  float2* v;
+  float2* bcv;
+  uint2* conn;
+  float* m;
+  uint32_t* w;
+  int32_t* gid;
+  uint16_t* csrp;
+  uint16_t* csrs;
+  int* gate;
+};
+
+__host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Shared-memory carve-up; returns the byte count (device: also the pointers).
+__host__ __device__ inline size_t res_layout(const Res& r, unsigned char* base, ResSmem* s) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* p = base ? base + o : nullptr;
+    o += res_align(bytes);
+    return p;
+  };
+  ResSmem t;
+  t.jinv = (float4*)take(sizeof(float4) * r.ne_max);
+  t.mat = (ElemMat*)take(sizeof(ElemMat) * r.ne_max);
+  t.j2 = (float4*)take(r.has_j2 ? sizeof(float4) * r.ne_max : 0);
+  t.j2p = (float2*)take(r.has_j2 ? sizeof(float2) * r.ne_max : 0);
+  t.f = (float2*)take(sizeof(float2) * 3 * (size_t)r.ne_max);
+  t.x = (float2*)take(sizeof(float2) * (size_t)(r.no_max + r.nh_max));
+  t.v = (float2*)take(sizeof(float2) * r.no_max);
+  t.bcv = (float2*)take(sizeof(float2) * r.no_max);
+  t.conn = (uint2*)take(sizeof(uint2) * r.ne_max);
+  t.m = (float*)take(sizeof(float) * r.no_max);
+  t.w = (uint32_t*)take(sizeof(uint32_t) * r.no_max);
+  t.gid = (int32_t*)take(sizeof(int32_t) * r.no_max);
+  t.csrp = (uint16_t*)take(sizeof(uint16_t) * (r.no_max + 1));
+  t.csrs = (uint16_t*)take(sizeof(uint16_t) * r.ncsr_max);
+  t.gate = (int*)take(sizeof(int) * kResMaxPairs);
+  if (s) *s = t;
+  return o;
+}
+
+__device__ __forceinline__ void res_element(const ResSmem& s, int q) {
+  const uint2 c = s.conn[q];
+  const float2 a = s.x[c.x & 0xFFFFu], b = s.x[c.x >> 16], cc = s.x[c.y & 0xFFFFu];
+  const ElemMat m = s.mat[q];
+  float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float sy = 0.f, H = 0.f;
+  const bool mises = fw::elem_type(m.word) == fw::MAT_MISES;
+  if (mises) {
+    j2 = s.j2[q];
+    sy = s.j2p[q].x;
+    H = s.j2p[q].y;
+  }
+  float2 f1, f2, f3;
+  fw::element_forces(a, b, cc, s.jinv[q], m, sy, H, j2, f1, f2, f3);
+  if (mises) s.j2[q] = j2;
+  s.f[3 * q] = f1;
+  s.f[3 * q + 1] = f2;
+  s.f[3 * q + 2] = f3;
+}
+
+__device__ __forceinline__ void aabb_reset(int* r) {
+  r[0] = fw::f2ord(1e30f);
+  r[1] = fw::f2ord(1e30f);
+  r[2] = fw::f2ord(-1e30f);
+  r[3] = fw::f2ord(-1e30f);
+}
+
+__global__ void __launch_bounds__(kResThreads, 1)
+k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ResSmem s;
+  res_layout(r, smem_raw, &s);
+  const ResPatch P = r.patch[blockIdx.x];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int N = d.N, B = d.B;
+  // ---- load the patch once
+  for (int q = t; q < P.ne; q += T) {
+    const int e = r.eid[P.elem_off + q];
+    s.jinv[q] = d.jinv[e];
+    s.mat[q] = d.emat[e];
+    s.conn[q] = r.conn[P.elem_off + q];
+    if (r.has_j2) {
+      s.j2[q] = d.j2state[e];
+      s.j2p[q] = d.j2par[e];
+    }
+  }
+  for (int i = t; i < P.no; i += T) {
+    const int g = r.nodes[P.node_off + i];
+    const int gi = g & 0x7FFFFFFF;
+    s.gid[i] = g;
+    s.x[i] = d.x[gi];
+    s.v[i] = d.v[gi];
+    s.m[i] = d.mass[gi];
+    s.w[i] = d.node_word[gi];
+    s.bcv[i] = d.bcv[gi];
+  }
+  for (int i = t; i < P.nh; i += T) s.x[P.no + i] = d.x[r.halo[P.halo_off + i]];
+  for (int i = t; i <= P.no; i += T) s.csrp[i] = (uint16_t)r.csr_ptr[P.csr_ptr_off + i];
+  for (int i = t; i < P.ncsr; i += T) s.csrs[i] = r.csr_slot[P.csr_off + i];
+  __syncthreads();
+
+  const int node_trips = (P.no + T - 1) / T;
+  for (int k = 0; k < nsteps; ++k) {
+    const int g = step0 + k;
+    // 1. interior triangles (owned nodes only)
+    for (int q = t; q < P.n_int; q += T) res_element(s, q);
+    // 2. previous substep complete everywhere -> halo positions
+    if (k > 0) {
+      if (t == 0) {
+        long long it = 0;
+        const int target = r.P * k;
+        while (ld_acquire(r.bar) < target) {
+          if (++it > kSpinLimit || *(volatile int*)r.err) {
+            atomicExch(r.err, 1);
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __syncthreads();
+      if (*(volatile int*)r.err) break;
+      const float2* src = r.xpub + (size_t)(k & 1) * N;
+      for (int i = t; i < P.nh; i += T) s.x[P.no + i] = src[r.halo[P.halo_off + i]];
+      __syncthreads();
+    }
+    // 3. cut triangles, gates, box-slot reset
+    for (int q = P.n_int + t; q < P.ne; q += T) res_element(s, q);
+    if (t < d.P) {
+      const Pair& pr = d.pairs[t];
+      const int* bb = r.aabb3 + ((size_t)(g % 3) * B + pr.body) * 4;
+      s.gate[t] = fw::pair_gate(pr, fw::ord2f(bb[0]), fw::ord2f(bb[1]), fw::ord2f(bb[2]),
+                                fw::ord2f(bb[3]), g) ? 1 : 0;
+    }
+    if (blockIdx.x == 0)
+      for (int b = t; b < B; b += T) aabb_reset(r.aabb3 + ((size_t)((g + 2) % 3) * B + b) * 4);
+    __syncthreads();
+    // 4. owned nodes
+    float2* dst = r.xpub + (size_t)((k + 1) & 1) * N;
+    int* box_w = r.aabb3 + (size_t)((g + 1) % 3) * B * 4;
+    for (int trip = 0; trip < node_trips; ++trip) {
+      const int i = trip * T + t;
+      bool bnd = false;
+      int body = 0;
+      float2 x = make_float2(0.f, 0.f);
+      if (i < P.no) {
+        const uint32_t w = s.w[i];
+        body = (int)(w >> fw::NODE_BODY_SHIFT);
+        x = s.x[i];
+        float2 v = s.v[i];
+        float2 f = make_float2(0.f, 0.f);
+        bnd = (w & fw::NODE_BOUNDARY) != 0;
+        if (bnd) {
+          const int p0 = d.body_pair_off[body], pn = d.body_pair_cnt[body];
+          for (int q = 0; q < pn; ++q) {
+            if (!s.gate[p0 + q]) continue;
+            float2 cf;
+            if (fw::contact_force(d.pairs[p0 + q], d.heights, d.occ, x, v, dt, cf)) {
+              f.x += cf.x;
+              f.y += cf.y;
+            }
+          }
+        }
+        for (int q = s.csrp[i]; q < s.csrp[i + 1]; ++q) {
+          const float2 c = s.f[s.csrs[q]];
+          f.x += c.x;
+          f.y += c.y;
+        }
+        const int bc = (int)(w & fw::NODE_BC_MASK);
+        fw::integrate(bc, f, s.m[i], s.bcv[i], dt, damp, x, v);
+        s.x[i] = x;
+        s.v[i] = v;
+        const int gid = s.gid[i];
+        if (gid < 0) dst[gid & 0x7FFFFFFF] = x;
+      }
+      const unsigned full = 0xFFFFFFFFu;
+      const unsigned mb = __ballot_sync(full, bnd);
+      if (mb != 0u) {
+        const int leader = __ffs(mb) - 1;
+        const int bl = __shfl_sync(full, body, leader);
+        const bool uniform = __all_sync(full, !bnd || body == bl);
+        float lx = bnd ? x.x : 1e30f, ly = bnd ? x.y : 1e30f;
+        float hx = bnd ? x.x : -1e30f, hy = bnd ? x.y : -1e30f;
+        if (uniform) {
+          for (int o = 16; o > 0; o >>= 1) {
+            lx = fminf(lx, __shfl_xor_sync(full, lx, o));
+            ly = fminf(ly, __shfl_xor_sync(full, ly, o));
+            hx = fmaxf(hx, __shfl_xor_sync(full, hx, o));
+            hy = fmaxf(hy, __shfl_xor_sync(full, hy, o));
+          }
+        }
+        if ((uniform && (int)(t & 31) == leader) || (!uniform && bnd)) {
+          int* rb = box_w + (size_t)body * 4;
+          atomicMin(rb + 0, fw::f2ord(lx));
+          atomicMin(rb + 1, fw::f2ord(ly));
+          atomicMax(rb + 2, fw::f2ord(hx));
+          atomicMax(rb + 3, fw::f2ord(hy));
+        }
+      }
+    }
+    // 5. arrive
+    __syncthreads();
+    if (t == 0) {
+      __threadfence();
+      atomicAdd(r.bar, 1);
+    }
+  }
+  // ---- write the patch state back
+  __syncthreads();
+  for (int i = t; i < P.no; i += T) {
+    const int gi = s.gid[i] & 0x7FFFFFFF;
+    d.x[gi] = s.x[i];
+    d.v[gi] = s.v[i];
+  }
+  if (r.has_j2)
+    for (int q = t; q < P.ne; q += T)
+      if ((s.conn[q].y >> 16) & kJ2Writer) d.j2state[r.eid[P.elem_off + q]] = s.j2[q];
+}
+
+// Before a resident launch: reset the barrier and error flag, copy the body
+// boxes of the last substep into slot step0 % 3 and clear slot (step0+1) % 3.
+__global__ void k_resident_prologue(Dev d, Res r, int step0) {
+  if (threadIdx.x == 0) {
+    *r.bar = 0;
+    *r.err = 0;
+  }
+  const int cur = d.scene_counter[0] & 1;
+  for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
+    const int* src = d.aabb_ring + ((size_t)cur * d.B + b) * 4;
+    int* a = r.aabb3 + ((size_t)(step0 % 3) * d.B + b) * 4;
+    for (int k = 0; k < 4; ++k) a[k] = src[k];
+    aabb_reset(r.aabb3 + ((size_t)((step0 + 1) % 3) * d.B + b) * 4);
+  }
+}
+
+// After a resident launch: publish the final body boxes to the gather path's
+// slots and advance the step counter.
+__global__ void k_resident_epilogue(Dev d, Res r, int step0, int nsteps) {
+  const int last = step0 + nsteps;
+  const int dst_slot = last & 1;
+  for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
+    const int* a = r.aabb3 + ((size_t)(last % 3) * d.B + b) * 4;
+    int* dst = d.aabb_ring + ((size_t)dst_slot * d.B + b) * 4;
+    for (int k = 0; k < 4; ++k) dst[k] = a[k];
+  }
+  if (threadIdx.x == 0) d.scene_counter[0] = last;
+}
+
+}  // namespace

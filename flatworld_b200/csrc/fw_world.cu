@@ -250,6 +250,8 @@ __global__ void k_prepare_mass(Dev d) {
 
 }  // namespace
 
+#include "fw_resident.cuh"
+
 // ------------------------------------------------------------------ context
 
 struct fw_ctx {
@@ -278,6 +280,13 @@ struct fw_ctx {
   std::vector<std::pair<uint64_t, cudaGraphExec_t>> graphs;
   cudaStream_t graph_stream = nullptr;
   int grid_e = 1, grid_n = 1;
+  // path selection and the resident (shared-memory) step
+  int path_req = FW_PATH_AUTO, patches_req = 0;
+  int path = FW_PATH_GATHER;
+  Res res{};
+  size_t res_smem = 0;
+  std::string res_reason;
+  int64_t host_counter = 0;  // step counter of scene 0 (single-scene worlds)
 };
 
 namespace {
@@ -368,8 +377,12 @@ int get_graph(fw_ctx* c, cudaGraphExec_t* out) {
   return FW_OK;
 }
 
+int launch_resident(fw_ctx* c, int n);
+
 int run_steps(fw_ctx* c, int n) {
   int rc = FW_OK;
+  if (c->path == FW_PATH_RESIDENT && c->d.uniform_dt) return launch_resident(c, n);
+  c->host_counter += n;
   if (n >= kGraphSteps) {
     cudaGraphExec_t g = nullptr;
     rc = get_graph(c, &g);
@@ -382,6 +395,205 @@ int run_steps(fw_ctx* c, int n) {
   }
   for (int k = 0; k < n && rc == FW_OK; ++k) rc = launch_step(c);
   return rc;
+}
+
+
+void rcb(const std::vector<float2>& x, std::vector<int>& idx, int lo, int hi, int p0, int np,
+         std::vector<int>& part) {
+  if (np <= 1 || hi - lo <= 1) {
+    for (int k = lo; k < hi; ++k) part[idx[k]] = p0;
+    return;
+  }
+  float mnx = 3e38f, mny = 3e38f, mxx = -3e38f, mxy = -3e38f;
+  for (int k = lo; k < hi; ++k) {
+    const float2 q = x[idx[k]];
+    mnx = std::min(mnx, q.x); mxx = std::max(mxx, q.x);
+    mny = std::min(mny, q.y); mxy = std::max(mxy, q.y);
+  }
+  const int axis = (mxx - mnx) >= (mxy - mny) ? 0 : 1;
+  const int k1 = np / 2;
+  const int mid = lo + (int)(((int64_t)(hi - lo) * k1) / np);
+  std::nth_element(idx.begin() + lo, idx.begin() + mid, idx.begin() + hi, [&](int a, int b) {
+    const float va = axis ? x[a].y : x[a].x, vb = axis ? x[b].y : x[b].x;
+    return va < vb || (va == vb && a < b);
+  });
+  rcb(x, idx, lo, mid, p0, k1, part);
+  rcb(x, idx, mid, hi, p0 + k1, np - k1, part);
+}
+
+// Build the patches of the resident path; returns FW_OK, or a positive value
+// (with c->res_reason) when the world does not fit and the gather path is used.
+int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<int32_t>& slot,
+                   const std::vector<float2>& x0, bool has_j2) {
+  const int N = c->N, E = c->E;
+  if (c->S != 1) { c->res_reason = "more than one scene"; return 1; }
+  if ((int)c->h_pairs.size() > kResMaxPairs) { c->res_reason = "more than 64 contact pairs"; return 1; }
+  int sms = 148, optin = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  int P = c->patches_req > 0 ? c->patches_req : std::max(1, std::min(sms, (N + 127) / 128));
+  if (P > N) P = N;
+  std::vector<int> idx(N), part(N, 0);
+  for (int i = 0; i < N; ++i) idx[i] = i;
+  rcb(x0, idx, 0, N, 0, P, part);
+  std::vector<std::vector<int>> owned(P), pel(P);
+  for (int i = 0; i < N; ++i) owned[part[i]].push_back(i);
+  for (int e = 0; e < E; ++e) {
+    int ps[3] = {part[c->h_conn[3 * e]], part[c->h_conn[3 * e + 1]], part[c->h_conn[3 * e + 2]]};
+    for (int k = 0; k < 3; ++k) {
+      bool dup = false;
+      for (int j = 0; j < k; ++j) dup |= ps[j] == ps[k];
+      if (!dup) pel[ps[k]].push_back(e);
+    }
+  }
+  std::vector<char> exported(N, 0);
+  std::vector<std::vector<int>> halo(P);
+  for (int p = 0; p < P; ++p) {
+    std::vector<int>& h = halo[p];
+    for (int e : pel[p])
+      for (int k = 0; k < 3; ++k) {
+        const int n = c->h_conn[3 * e + k];
+        if (part[n] != p) h.push_back(n);
+      }
+    std::sort(h.begin(), h.end());
+    h.erase(std::unique(h.begin(), h.end()), h.end());
+    for (int n : h) exported[n] = 1;
+  }
+  std::vector<ResPatch> patches(P);
+  std::vector<int32_t> rnodes, rhalo, reid, rcsrp;
+  std::vector<uint2> rconn;
+  std::vector<uint16_t> rcsrs;
+  std::vector<int> loc(N, -1), eloc(E, -1);
+  int no_max = 0, nh_max = 0, ne_max = 0, ncsr_max = 0;
+  for (int p = 0; p < P; ++p) {
+    ResPatch& rp = patches[p];
+    const std::vector<int>& ow = owned[p];
+    const std::vector<int>& h = halo[p];
+    rp.node_off = (int)rnodes.size();
+    rp.no = (int)ow.size();
+    rp.halo_off = (int)rhalo.size();
+    rp.nh = (int)h.size();
+    if (rp.no + rp.nh >= 65536) { c->res_reason = "patch with >= 65536 nodes"; return 1; }
+    for (int i = 0; i < rp.no; ++i) {
+      loc[ow[i]] = i;
+      rnodes.push_back(ow[i] | (exported[ow[i]] ? (int32_t)kExported : 0));
+    }
+    for (int j = 0; j < rp.nh; ++j) {
+      loc[h[j]] = rp.no + j;
+      rhalo.push_back(h[j]);
+    }
+    std::vector<int> inter, cut;
+    for (int e : pel[p]) {
+      const bool in = part[c->h_conn[3 * e]] == p && part[c->h_conn[3 * e + 1]] == p &&
+                      part[c->h_conn[3 * e + 2]] == p;
+      (in ? inter : cut).push_back(e);
+    }
+    rp.elem_off = (int)reid.size();
+    rp.ne = (int)pel[p].size();
+    rp.n_int = (int)inter.size();
+    if (3 * rp.ne >= 65536) { c->res_reason = "patch with > 21845 triangles"; return 1; }
+    int q = 0;
+    for (const std::vector<int>* grp : {&inter, &cut})
+      for (int e : *grp) {
+        eloc[e] = q++;
+        reid.push_back(e);
+        const uint32_t a = loc[c->h_conn[3 * e]], b = loc[c->h_conn[3 * e + 1]], cc = loc[c->h_conn[3 * e + 2]];
+        const uint32_t writer = part[c->h_conn[3 * e]] == p ? kJ2Writer : 0u;
+        rconn.push_back(make_uint2(a | (b << 16), cc | (writer << 16)));
+      }
+    rp.csr_ptr_off = (int)rcsrp.size();
+    rp.csr_off = (int)rcsrs.size();
+    int cnt = 0;
+    for (int i = 0; i < rp.no; ++i) {
+      rcsrp.push_back(cnt);
+      const int n = ow[i];
+      for (int k = off[n]; k < off[n + 1]; ++k) {
+        const int sl = slot[k];
+        rcsrs.push_back((uint16_t)(3 * eloc[sl / 3] + sl % 3));
+        ++cnt;
+      }
+    }
+    rcsrp.push_back(cnt);
+    rp.ncsr = cnt;
+    for (int n : ow) loc[n] = -1;
+    for (int n : h) loc[n] = -1;
+    for (int e : pel[p]) eloc[e] = -1;
+    no_max = std::max(no_max, rp.no);
+    nh_max = std::max(nh_max, rp.nh);
+    ne_max = std::max(ne_max, rp.ne);
+    ncsr_max = std::max(ncsr_max, rp.ncsr);
+  }
+  Res& r = c->res;
+  r.P = P;
+  r.no_max = no_max;
+  r.nh_max = nh_max;
+  r.ne_max = ne_max;
+  r.ncsr_max = ncsr_max;
+  r.has_j2 = has_j2 ? 1 : 0;
+  const size_t smem = res_layout(r, nullptr, nullptr);
+  if ((long)smem > optin) {
+    c->res_reason = "patch needs " + std::to_string(smem) + " B of shared memory";
+    return 1;
+  }
+  cudaError_t e1 = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident, kResThreads, smem);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || per_sm * sms < P) {
+    cudaGetLastError();
+    c->res_reason = "patches cannot all be resident";
+    return 1;
+  }
+  int rc;
+  ResPatch* dpatch = nullptr;
+  int32_t *dn = nullptr, *dh = nullptr, *de = nullptr, *dcp = nullptr;
+  uint2* dc = nullptr;
+  uint16_t* dcs = nullptr;
+  if ((rc = upload(c, &dpatch, patches)) || (rc = upload(c, &dn, rnodes)) || (rc = upload(c, &dh, rhalo)) ||
+      (rc = upload(c, &de, reid)) || (rc = upload(c, &dc, rconn)) || (rc = upload(c, &dcp, rcsrp)) ||
+      (rc = upload(c, &dcs, rcsrs)) || (rc = dalloc(c, &r.xpub, 2 * (size_t)N)) ||
+      (rc = dalloc(c, &r.aabb3, 12 * (size_t)c->B)) || (rc = dalloc(c, &r.bar, 1)) ||
+      (rc = dalloc(c, &r.err, 1)))
+    return rc;
+  r.patch = dpatch;
+  r.nodes = dn;
+  r.halo = dh;
+  r.eid = de;
+  r.conn = dc;
+  r.csr_ptr = dcp;
+  r.csr_slot = dcs;
+  FW_CUDA(c, cudaMemsetAsync(r.err, 0, sizeof(int), c->stream));
+  c->res_smem = smem;
+  return FW_OK;
+}
+
+int launch_resident(fw_ctx* c, int n) {
+  // keep the arrivals counter (P * steps) far from int overflow
+  constexpr int kMaxStepsPerLaunch = 1 << 20;
+  while (n > kMaxStepsPerLaunch) {
+    int rc = launch_resident(c, kMaxStepsPerLaunch);
+    if (rc) return rc;
+    n -= kMaxStepsPerLaunch;
+  }
+  if (n <= 0) return FW_OK;
+  const int step0 = (int)c->host_counter;
+  k_resident_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0);
+  float dt = c->d.dt_uniform, damp = c->h_damp[0];
+  void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&step0, (void*)&n, (void*)&dt, (void*)&damp};
+  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_resident, dim3(c->res.P), dim3(kResThreads), args,
+                                         c->res_smem, c->stream));
+  k_resident_epilogue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
+  c->launches += 3;
+  c->host_counter += n;
+  return check_kernel(c, "resident step");
+}
+
+int check_device_error(fw_ctx* c) {
+  if (c->path != FW_PATH_RESIDENT) return FW_OK;
+  int err = 0;
+  FW_CUDA(c, cudaMemcpyAsync(&err, c->res.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (err) return fail(c, FW_ERR_TIMEOUT, "resident step: a CTA gave up waiting for the others");
+  return FW_OK;
 }
 
 int set_scene_dt(fw_ctx* c, const float* dt) {
@@ -705,7 +917,36 @@ int fw_finalize(fw_ctx* c) {
   // zero-dt construction step (setGlobalAABB -> substep(0, 0))
   if ((rc = launch_step(c))) return rc;
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->path = FW_PATH_GATHER;
+  if (c->path_req != FW_PATH_GATHER) {
+    rc = build_resident(c, off, slot, x0, has_j2);
+    if (rc < 0) return rc;
+    if (rc == 0) {
+      c->path = FW_PATH_RESIDENT;
+    } else if (c->path_req == FW_PATH_RESIDENT) {
+      return fail(c, FW_ERR_ARG, "resident path requested but unavailable: %s", c->res_reason.c_str());
+    }
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   c->finalized = true;
+  return FW_OK;
+}
+
+int fw_set_path(fw_ctx* c, int32_t path, int32_t patches) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_path after fw_finalize");
+  if (path != FW_PATH_AUTO && path != FW_PATH_GATHER && path != FW_PATH_RESIDENT)
+    return fail(c, FW_ERR_ARG, "fw_set_path: unknown path %d", path);
+  if (patches < 0) return fail(c, FW_ERR_ARG, "fw_set_path: patches < 0");
+  c->path_req = path;
+  c->patches_req = patches;
+  return FW_OK;
+}
+
+int fw_get_path(const fw_ctx* c, int32_t* path, int32_t* patches) {
+  if (!c || !path) return FW_ERR_ARG;
+  *path = c->finalized ? c->path : FW_PATH_AUTO;
+  if (patches) *patches = c->path == FW_PATH_RESIDENT ? c->res.P : 0;
   return FW_OK;
 }
 
@@ -741,7 +982,7 @@ int fw_set_active(fw_ctx* c, const int32_t* active) {
 int fw_synchronize(fw_ctx* c) {
   if (!c) return FW_ERR_ARG;
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
-  return FW_OK;
+  return c->finalized ? check_device_error(c) : FW_OK;
 }
 
 int fw_read_nodes(fw_ctx* c, int32_t field, int32_t first, int32_t count, float* dst, int32_t on_device) {
@@ -761,7 +1002,7 @@ int fw_read_nodes(fw_ctx* c, int32_t field, int32_t first, int32_t count, float*
   FW_CUDA(c, cudaMemcpyAsync(dst, src, per * count,
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
-  return FW_OK;
+  return check_device_error(c);
 }
 
 int fw_write_nodes(fw_ctx* c, int32_t field, int32_t first, int32_t count, const float* src, int32_t on_device) {
@@ -844,7 +1085,7 @@ int fw_read_counters(fw_ctx* c, int64_t* counters) {
 int64_t fw_launch_count(const fw_ctx* c) { return c ? c->launches : 0; }
 
 const char* fw_build_info(void) {
-  return "libfwb200: sm_100a, -fmad=false, IEEE div/sqrt, gather step v1";
+  return "libfwb200: sm_100a, -fmad=false, IEEE div/sqrt; gather step + shared-memory-resident step";
 }
 
 }  // extern "C"

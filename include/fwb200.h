@@ -59,6 +59,11 @@ extern "C" {
 #define FW_FIELD_MASS 2 /* lumped mass, one float per node (FemSpringManager.mass) */
 #define FW_FIELD_X0 3   /* rest coordinates */
 
+/* Step implementations (fw_set_path). */
+#define FW_PATH_AUTO 0     /* resident when the world fits, else gather */
+#define FW_PATH_GATHER 1   /* two kernels per substep, any world */
+#define FW_PATH_RESIDENT 2 /* one persistent kernel per fw_step call */
+
 typedef struct fw_ctx fw_ctx;
 
 /* Create / destroy a context on CUDA device `device`.
@@ -122,6 +127,18 @@ int fw_add_voxel_pair(fw_ctx* ctx, int32_t body, float penalty, const float* gat
  * Replaces: prepareFEMData_ / _prepare_fem_data_kernel and setGlobalAABB ->
  * substep(0, 0), flatworld/femspringmanager.py:113-138, 872-897. */
 int fw_finalize(fw_ctx* ctx);
+
+/* Choose the step implementation before fw_finalize.  GATHER: per substep an
+ * element kernel writes corner forces and a node kernel gathers them (any
+ * number of scenes).  RESIDENT: the mesh is cut into `patches` patches (0 =
+ * automatic, at most one per SM) that stay in shared memory while one
+ * cooperative launch runs all substeps of an fw_step call (single-scene worlds
+ * that fit on chip).  AUTO picks RESIDENT when possible.  Both paths give
+ * identical results.  No reference counterpart: the reference has one Warp
+ * path (flatworld/femspringmanager.py:941-1012). */
+int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
+/* Active path (FW_PATH_GATHER or FW_PATH_RESIDENT) and patch count. */
+int fw_get_path(const fw_ctx* ctx, int32_t* path, int32_t* patches);
 
 /* Advance every active scene by n_steps substeps of dt (float32), i.e. n_steps
  * calls of ExplicitLoop.advance(): gated contact, element force, integration,

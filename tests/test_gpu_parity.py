@@ -21,6 +21,12 @@ RTOL = 1e-5
 FRAME = 1.0 / 60.0
 
 
+@pytest.fixture(params=["gather", "resident"])
+def path(request):
+    """Both step implementations must meet the same bar."""
+    return request.param
+
+
 def rel_linf(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
@@ -34,12 +40,12 @@ def gpu_state(loop):
     return m.coords.numpy()[:n], m.V.numpy()[:n]
 
 
-def run_pair(domains, steps, every, dt=None, adaptive=True, exact=False, build=None, track=None):
+def run_pair(domains, steps, every, dt=None, adaptive=True, exact=False, build=None, track=None, path="auto"):
     """Step GPU and FP32 oracle side by side; compare every `every` steps.
     ``track`` (a list) receives the lowest node height at every checkpoint."""
     doms_gpu = build() if build else domains
     doms_or = build() if build else domains
-    loop = fw.ExplicitLoop(dt or 0.0, doms_gpu, useAdapativeDT=adaptive)
+    loop = fw.ExplicitLoop(dt or 0.0, doms_gpu, useAdapativeDT=adaptive, path=path)
     o32 = oracle.OracleLoop(doms_or, dt or 0.0, useAdapativeDT=adaptive, precision="f32", threads=8)
     assert loop.dt == o32.dt
     worst = (0.0, 0.0)
@@ -68,25 +74,25 @@ def fp64_error(domains, steps, dt, xg, adaptive=False):
     return rel_linf(xg, o64.state()[0])
 
 
-def test_plain_small_2000_steps_bitwise():
+def test_plain_small_2000_steps_bitwise(path):
     doms = scenes.plain_small_scene(fw)
-    loop, o32, worst = run_pair(doms, 2000, 100, dt=1e-4, adaptive=False, exact=True)
+    loop, o32, worst = run_pair(doms, 2000, 100, dt=1e-4, adaptive=False, exact=True, path=path)
     xg, _ = gpu_state(loop)
     e64 = fp64_error(scenes.plain_small_scene(fw), 2000, 1e-4, xg)
     print(f"plain small 2000 steps: vs FP32 oracle {worst}, vs FP64 {e64:.3e}")
 
 
-def test_plain_small_with_ground_contact_bitwise():
+def test_plain_small_with_ground_contact_bitwise(path):
     """12000 steps of 1e-4: the body lands on the plane (about 0.77 s of fall)."""
     doms = scenes.plain_small_scene(fw)
     low = []
-    run_pair(doms, 12000, 500, dt=1e-4, adaptive=False, exact=True, track=low)
+    run_pair(doms, 12000, 500, dt=1e-4, adaptive=False, exact=True, track=low, path=path)
     assert min(low) < 0.01  # it reached the plane (and bounced: the plane penalty is undamped)
     assert min(low) > -0.05
 
 
-def test_heightfield_disk_bitwise():
-    loop = fw.ExplicitLoop(0.0, scenes.hf_disk_scene(fw), useAdapativeDT=True)
+def test_heightfield_disk_bitwise(path):
+    loop = fw.ExplicitLoop(0.0, scenes.hf_disk_scene(fw), useAdapativeDT=True, path=path)
     o32 = oracle.OracleLoop(scenes.hf_disk_scene(fw), 0.0, useAdapativeDT=True)
     for f in range(60):
         loop.advanceWithTime(FRAME)
@@ -99,8 +105,8 @@ def test_heightfield_disk_bitwise():
     assert xg[:, 1].min() > 0.05  # test_2Dfem_heightfield_contact.py:66
 
 
-def test_voxel_disk_bitwise():
-    loop = fw.ExplicitLoop(0.0, scenes.voxel_disk_scene(fw), useAdapativeDT=True)
+def test_voxel_disk_bitwise(path):
+    loop = fw.ExplicitLoop(0.0, scenes.voxel_disk_scene(fw), useAdapativeDT=True, path=path)
     o32 = oracle.OracleLoop(scenes.voxel_disk_scene(fw), 0.0, useAdapativeDT=True)
     for f in range(60):
         loop.advanceWithTime(FRAME)
@@ -111,30 +117,30 @@ def test_voxel_disk_bitwise():
     assert xg[:, 1].min() > 0.02  # test_2Dfem_voxel_contact.py:70
 
 
-def test_neohookean_heightfield_tolerance():
+def test_neohookean_heightfield_tolerance(path):
     """Reduced large-mesh workload (64 x 64 quads, NeoHookean, height field)."""
     build = lambda: scenes.plain_large_scene(fw, n=64, hf_offset=0.17)  # noqa: E731
-    loop, o32, worst = run_pair(None, 3000, 250, adaptive=True, build=build)
+    loop, o32, worst = run_pair(None, 3000, 250, adaptive=True, build=build, path=path)
     xg, _ = gpu_state(loop)
     e64 = fp64_error(build(), 3000, loop.dt, xg, adaptive=True)
     print(f"NeoHookean 64x64: vs FP32 oracle {worst}, vs FP64 {e64:.3e}")
 
 
-def test_j2_plastic_block_on_plane_bitwise():
+def test_j2_plastic_block_on_plane_bitwise(path):
     def build():
         conn, coords = fw.structured_rectangle(24, 12, 0.4, 0.2, origin=(0.1, 0.05), jitter=0.1, seed=3)
         mat = fw.MisesPlastic(E=1e5, nu=0.3, rho=100.0, sigma_y=2e3, H=1e3)
         fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])],
                            initials=[fw.InitialVel("ALL", [0.3, -2.0])])
         return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), fem]
-    loop, o32, _ = run_pair(None, 4000, 500, dt=5e-5, adaptive=False, exact=True, build=build)
+    loop, o32, _ = run_pair(None, 4000, 500, dt=5e-5, adaptive=False, exact=True, build=build, path=path)
     ep_g = loop.femSpringManager.eqPlasticStrain.numpy()
     _, eq_o = o32.plastic()
     assert ep_g.max() > 0.0, "the block must yield"
     assert np.array_equal(ep_g.astype(np.float64), eq_o)
 
 
-def test_bcs_scene_bitwise():
+def test_bcs_scene_bitwise(path):
     """test_2Dfem_bcs.py: Force+Fixed, EnforceVel+Fixed, EnforceAcc+Fixed bodies."""
     def build():
         conn = np.array([[0, 1, 3], [0, 3, 2]], dtype=np.int32)
@@ -147,7 +153,7 @@ def test_bcs_scene_bitwise():
                           False)
         d3 = fw.FemDomain(fw.Mesh(2, conn, c + 0.5), prop, [], False, initials=[fw.InitialVel([0, 1], [0, -1.0])])
         return [d0, d1, d2, d3]
-    loop = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True)
+    loop = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, path=path)
     o32 = oracle.OracleLoop(build(), 0.0, useAdapativeDT=True)
     for _ in range(60):
         loop.advanceWithTime(FRAME)
@@ -200,11 +206,41 @@ def test_run_to_run_determinism():
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
 
 
-def test_aabb_and_getbbox():
+def test_aabb_and_getbbox(path):
     doms = scenes.plain_small_scene(fw)
-    loop = fw.ExplicitLoop(1e-4, doms, useAdapativeDT=False)
+    loop = fw.ExplicitLoop(1e-4, doms, useAdapativeDT=False, path=path)
     loop.advance_n(50)
     lb, ub = doms[1].getBBox()
     xg, _ = gpu_state(loop)
     bn = doms[1].mesh.boundaryNodes
     assert np.array_equal(lb, xg[bn].min(axis=0)) and np.array_equal(ub, xg[bn].max(axis=0))
+
+
+def test_resident_is_chosen_for_large_mesh_and_matches_gather():
+    """The 256 x 256 workload runs on the resident path by default; it and the
+    gather path give identical bits (same sums in the same order)."""
+    a = fw.ExplicitLoop(0.0, scenes.plain_large_scene(fw, n=256), useAdapativeDT=True)
+    assert a.path == 2 and a.patches >= 64, (a.path, a.patches)
+    b = fw.ExplicitLoop(0.0, scenes.plain_large_scene(fw, n=256), useAdapativeDT=True, path="gather")
+    assert b.path == 1
+    for _ in range(3):
+        a.advanceWithTime(FRAME)
+        b.advanceWithTime(FRAME)
+    xa, va = gpu_state(a)
+    xb, vb = gpu_state(b)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    assert np.array_equal(np.asarray(a.femSpringManager.domains[0].getBBox()),
+                          np.asarray(b.femSpringManager.domains[0].getBBox()))
+
+
+@pytest.mark.parametrize("patches", [1, 7, 64, 148])
+def test_resident_patch_counts_bitwise(patches):
+    doms = lambda: scenes.plain_large_scene(fw, n=32, hf_offset=0.17)  # noqa: E731
+    a = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="resident", patches=patches)
+    b = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="gather")
+    for _ in range(20):
+        a.advanceWithTime(FRAME)
+        b.advanceWithTime(FRAME)
+    xa, va = gpu_state(a)
+    xb, vb = gpu_state(b)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
