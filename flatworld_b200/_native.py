@@ -23,6 +23,7 @@ FW_PATH_AUTO = 0
 FW_PATH_GATHER = 1
 FW_PATH_RESIDENT = 2
 PATHS = {"auto": FW_PATH_AUTO, "gather": FW_PATH_GATHER, "resident": FW_PATH_RESIDENT}
+FW_OPT_FRONT_WARPS = 1
 
 _lock = threading.Lock()
 _lib = None
@@ -46,6 +47,7 @@ _SIGNATURES = {
     "fw_add_voxel_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, C.c_int32, _i32p, C.c_float, C.c_float, C.c_float, C.c_float]),
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
+    "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_finalize": (C.c_int, [_vp]),
     "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_step_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
@@ -171,6 +173,9 @@ class NativeWorld:
 
     def set_path(self, path: int, patches: int = 0):
         self._check(self._L.fw_set_path(self._h, int(path), int(patches)), "fw_set_path")
+
+    def set_option(self, option: int, value: int):
+        self._check(self._L.fw_set_option(self._h, int(option), int(value)), "fw_set_option")
 
     def get_path(self):
         p = C.c_int32()

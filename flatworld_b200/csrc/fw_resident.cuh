@@ -7,21 +7,21 @@
 // held, and evaluated, by each patch that touches them), plus the positions of
 // the one-ring "halo" nodes it does not own.  One cooperative launch advances
 // all CTAs through n substeps; across substeps the patch's node state, element
-// data and corner forces never leave shared memory.  The only traffic per
-// substep is the positions of nodes that other patches read (published to a
-// double-buffered array in L2) and the body bounding boxes.
+// data, corner forces and the ground tables stay in shared memory.  Per
+// substep only the positions other patches read (a double-buffered array in
+// L2) and the body bounding boxes move between SMs.
 //
-// Per substep, per CTA:
-//   1. corner forces of the patch's interior triangles (owned nodes only)
-//   2. wait for every CTA to have finished the previous substep (split-phase
-//      grid barrier: the arrive happened at the end of the previous substep,
-//      so step 1 overlaps the wait), then read the halo positions
-//   3. corner forces of the cut triangles; broad-phase gates from the body
-//      boxes of the previous substep
-//   4. owned nodes: contact, corner forces summed in ascending element order,
-//      boundary conditions, symplectic Euler; publish positions read by other
-//      patches; body-box reduction (ordered-int atomics)
-//   5. arrive at the barrier
+// Owned nodes are ordered so that the ones other CTAs need -- positions read
+// as halo, and body-boundary nodes that feed the body box -- come first
+// ("group 1").  Per substep, per CTA:
+//   1. wait until every CTA has arrived for the previous substep (bounded
+//      spin), then fetch halo positions and the body boxes (one L2 round trip)
+//   2. broad-phase gates; corner forces of the cut triangles
+//   3. group-1 nodes: contact, corner forces summed in ascending element
+//      order, boundary conditions, symplectic Euler; publish positions; box
+//      reduction (ordered-int atomics); then fence and arrive
+//   4. group-2 nodes, then the interior triangles of the next substep -- this
+//      work overlaps the other CTAs' progress towards the barrier
 // The node sums use the same ascending-element order as the gather path, so
 // both paths produce identical bits.  Every wait is bounded: after
 // kSpinLimit polls the CTA sets the error flag and leaves the loop, so a
@@ -34,6 +34,7 @@ namespace {
 constexpr int kResThreads = 512;
 constexpr int kResMaxPairs = 64;
 constexpr long long kSpinLimit = 1ll << 26;
+constexpr int kResTableBytes = 48 * 1024;
 
 struct ResPatch {
   int node_off, no;      // owned nodes: res.nodes[node_off .. +no)
@@ -42,7 +43,8 @@ struct ResPatch {
   int n_int;             // number of interior triangles
   int csr_ptr_off;       // res.csr_ptr[csr_ptr_off .. +no+1): local offsets
   int csr_off, ncsr;     // res.csr_slot[csr_off .. +ncsr)
-  int pad[2];
+  int n_g1;              // owned nodes [0, n_g1) are read by other CTAs / feed body boxes
+  int pad;
 };
 
 struct Res {
@@ -59,6 +61,8 @@ struct Res {
   int* err;                 // != 0: a wait gave up
   int P, no_max, nh_max, ne_max, ncsr_max;
   int has_j2;
+  int tab_h, tab_o;         // ground tables staged in shared memory (floats, bytes)
+  int n_bodies;
 };
 
 constexpr uint32_t kExported = 0x80000000u;
@@ -80,11 +84,18 @@ struct ResSmem {
   float2* bcv;
   uint2* conn;
   float* m;
+  float* im;
+  int32_t* hidx;
+  float* heights;
+  int8_t* occ;
   uint32_t* w;
   int32_t* gid;
   uint16_t* csrp;
   uint16_t* csrs;
   int* gate;
+  Pair* pairs;
+  int* bpo;  // body -> first pair
+  int* bpc;  // body -> pair count
 };
 
 __host__ __device__ inline size_t res_align(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -108,11 +119,18 @@ __host__ __device__ inline size_t res_layout(const Res& r, unsigned char* base, 
   t.bcv = (float2*)take(sizeof(float2) * r.no_max);
   t.conn = (uint2*)take(sizeof(uint2) * r.ne_max);
   t.m = (float*)take(sizeof(float) * r.no_max);
+  t.im = (float*)take(sizeof(float) * r.no_max);
+  t.hidx = (int32_t*)take(sizeof(int32_t) * r.nh_max);
+  t.heights = (float*)take(sizeof(float) * r.tab_h);
+  t.occ = (int8_t*)take(r.tab_o);
   t.w = (uint32_t*)take(sizeof(uint32_t) * r.no_max);
   t.gid = (int32_t*)take(sizeof(int32_t) * r.no_max);
   t.csrp = (uint16_t*)take(sizeof(uint16_t) * (r.no_max + 1));
   t.csrs = (uint16_t*)take(sizeof(uint16_t) * r.ncsr_max);
   t.gate = (int*)take(sizeof(int) * kResMaxPairs);
+  t.pairs = (Pair*)take(sizeof(Pair) * kResMaxPairs);
+  t.bpo = (int*)take(sizeof(int) * r.n_bodies);
+  t.bpc = (int*)take(sizeof(int) * r.n_bodies);
   if (s) *s = t;
   return o;
 }
@@ -144,9 +162,52 @@ __device__ __forceinline__ void aabb_reset(int* r) {
   r[3] = fw::f2ord(-1e30f);
 }
 
+// Update one owned node (shared-memory state) for the current substep.
+__device__ __forceinline__ float2 res_node(const Dev& d, const ResSmem& s, const float* heights,
+                                           const int8_t* occ, int i, float dt, float damp) {
+  const uint32_t w = s.w[i];
+  const int body = (int)(w >> fw::NODE_BODY_SHIFT);
+  float2 x = s.x[i];
+  float2 v = s.v[i];
+  float2 f = make_float2(0.f, 0.f);
+  if (w & fw::NODE_BOUNDARY) {
+    const int p0 = s.bpo[body], pn = s.bpc[body];
+    for (int q = 0; q < pn; ++q) {
+      if (!s.gate[p0 + q]) continue;
+      float2 cf;
+      if (fw::contact_force(s.pairs[p0 + q], heights, occ, x, v, dt, cf)) {
+        f.x += cf.x;
+        f.y += cf.y;
+      }
+    }
+  }
+  for (int q = s.csrp[i]; q < s.csrp[i + 1]; ++q) {
+    const float2 c = s.f[s.csrs[q]];
+    f.x += c.x;
+    f.y += c.y;
+  }
+  fw::integrate_im((int)(w & fw::NODE_BC_MASK), f, s.m[i], s.im[i], s.bcv[i], dt, damp, x, v);
+  s.x[i] = x;
+  s.v[i] = v;
+  return x;
+}
+
+__device__ __forceinline__ void named_bar(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Warp-specialised substep loop.  Warps [0, FRONT) run the critical chain
+// (barrier wait, halo and box loads, gates, cut triangles, group-1 nodes,
+// publish + arrive); the other warps compute the interior triangles of the
+// next substep and the group-2 nodes, which need no data from other CTAs.
+// Shared-memory hazards: interior and cut triangles write disjoint corner
+// slots; group-1 and group-2 nodes are disjoint; the halo part of x is only
+// read by the front warps; two CTA-wide barriers per substep order the rest.
+template <int FRONT>
 __global__ void __launch_bounds__(kResThreads, 1)
 k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_abort;
   ResSmem s;
   res_layout(r, smem_raw, &s);
   const ResPatch P = r.patch[blockIdx.x];
@@ -170,118 +231,124 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
     s.x[i] = d.x[gi];
     s.v[i] = d.v[gi];
     s.m[i] = d.mass[gi];
+    s.im[i] = 1.0f / d.mass[gi];
     s.w[i] = d.node_word[gi];
     s.bcv[i] = d.bcv[gi];
   }
-  for (int i = t; i < P.nh; i += T) s.x[P.no + i] = d.x[r.halo[P.halo_off + i]];
+  for (int i = t; i < P.nh; i += T) {
+    const int h = r.halo[P.halo_off + i];
+    s.hidx[i] = h;
+    s.x[P.no + i] = d.x[h];
+  }
   for (int i = t; i <= P.no; i += T) s.csrp[i] = (uint16_t)r.csr_ptr[P.csr_ptr_off + i];
   for (int i = t; i < P.ncsr; i += T) s.csrs[i] = r.csr_slot[P.csr_off + i];
+  for (int i = t; i < r.tab_h; i += T) s.heights[i] = d.heights[i];
+  for (int i = t; i < r.tab_o; i += T) s.occ[i] = d.occ[i];
+  for (int i = t; i < d.P; i += T) s.pairs[i] = d.pairs[i];
+  for (int b = t; b < B; b += T) {
+    s.bpo[b] = d.body_pair_off[b];
+    s.bpc[b] = d.body_pair_cnt[b];
+  }
+  if (t == 0) s_abort = 0;
+  const float* heights = r.tab_h ? s.heights : d.heights;
+  const int8_t* occ = r.tab_o ? s.occ : d.occ;
   __syncthreads();
 
-  const int node_trips = (P.no + T - 1) / T;
+  constexpr int FT = FRONT * 32;
+  const bool front = t < FT;
+  const int BT = T - FT, bt = t - FT;
+  if (!front)
+    for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
+  const int g1_trips = (P.n_g1 + FT - 1) / FT;
   for (int k = 0; k < nsteps; ++k) {
     const int g = step0 + k;
-    // 1. interior triangles (owned nodes only)
-    for (int q = t; q < P.n_int; q += T) res_element(s, q);
-    // 2. previous substep complete everywhere -> halo positions
-    if (k > 0) {
-      if (t == 0) {
-        long long it = 0;
-        const int target = r.P * k;
-        while (ld_acquire(r.bar) < target) {
-          if (++it > kSpinLimit || *(volatile int*)r.err) {
-            atomicExch(r.err, 1);
-            break;
+    if (front) {
+      // previous substep complete everywhere -> halo positions, body boxes
+      if (k > 0) {
+        if (t == 0) {
+          long long it = 0;
+          const int target = r.P * k;
+          while (ld_acquire(r.bar) < target) {
+            if (++it > kSpinLimit || *(volatile int*)r.err) {
+              atomicExch(r.err, 1);
+              s_abort = 1;
+              break;
+            }
+            __nanosleep(20);
           }
-          __nanosleep(32);
+        }
+        named_bar(1, FT);
+        if (!s_abort) {
+          const float2* src = r.xpub + (size_t)(k & 1) * N;
+          for (int i = t; i < P.nh; i += FT) s.x[P.no + i] = __ldcg(src + s.hidx[i]);
         }
       }
-      __syncthreads();
-      if (*(volatile int*)r.err) break;
-      const float2* src = r.xpub + (size_t)(k & 1) * N;
-      for (int i = t; i < P.nh; i += T) s.x[P.no + i] = src[r.halo[P.halo_off + i]];
-      __syncthreads();
+      if (!s_abort) {
+        if (t < d.P) {
+          const Pair& pr = s.pairs[t];
+          const int4 bb = __ldcg(reinterpret_cast<const int4*>(r.aabb3 + ((size_t)(g % 3) * B + pr.body) * 4));
+          s.gate[t] = fw::pair_gate(pr, fw::ord2f(bb.x), fw::ord2f(bb.y), fw::ord2f(bb.z), fw::ord2f(bb.w), g) ? 1 : 0;
+        }
+        if (blockIdx.x == 0)
+          for (int b = t; b < B; b += FT) aabb_reset(r.aabb3 + ((size_t)((g + 2) % 3) * B + b) * 4);
+        named_bar(1, FT);
+        for (int q = P.n_int + t; q < P.ne; q += FT) res_element(s, q);
+      }
     }
-    // 3. cut triangles, gates, box-slot reset
-    for (int q = P.n_int + t; q < P.ne; q += T) res_element(s, q);
-    if (t < d.P) {
-      const Pair& pr = d.pairs[t];
-      const int* bb = r.aabb3 + ((size_t)(g % 3) * B + pr.body) * 4;
-      s.gate[t] = fw::pair_gate(pr, fw::ord2f(bb[0]), fw::ord2f(bb[1]), fw::ord2f(bb[2]),
-                                fw::ord2f(bb[3]), g) ? 1 : 0;
-    }
-    if (blockIdx.x == 0)
-      for (int b = t; b < B; b += T) aabb_reset(r.aabb3 + ((size_t)((g + 2) % 3) * B + b) * 4);
-    __syncthreads();
-    // 4. owned nodes
-    float2* dst = r.xpub + (size_t)((k + 1) & 1) * N;
-    int* box_w = r.aabb3 + (size_t)((g + 1) % 3) * B * 4;
-    for (int trip = 0; trip < node_trips; ++trip) {
-      const int i = trip * T + t;
-      bool bnd = false;
-      int body = 0;
-      float2 x = make_float2(0.f, 0.f);
-      if (i < P.no) {
-        const uint32_t w = s.w[i];
-        body = (int)(w >> fw::NODE_BODY_SHIFT);
-        x = s.x[i];
-        float2 v = s.v[i];
-        float2 f = make_float2(0.f, 0.f);
-        bnd = (w & fw::NODE_BOUNDARY) != 0;
-        if (bnd) {
-          const int p0 = d.body_pair_off[body], pn = d.body_pair_cnt[body];
-          for (int q = 0; q < pn; ++q) {
-            if (!s.gate[p0 + q]) continue;
-            float2 cf;
-            if (fw::contact_force(d.pairs[p0 + q], d.heights, d.occ, x, v, dt, cf)) {
-              f.x += cf.x;
-              f.y += cf.y;
+    __syncthreads();  // every triangle of substep k is done
+    if (s_abort) break;
+    if (front) {
+      float2* dst = r.xpub + (size_t)((k + 1) & 1) * N;
+      int* box_w = r.aabb3 + (size_t)((g + 1) % 3) * B * 4;
+      for (int trip = 0; trip < g1_trips; ++trip) {
+        const int i = trip * FT + t;
+        bool bnd = false;
+        int body = 0;
+        float2 x = make_float2(0.f, 0.f);
+        if (i < P.n_g1) {
+          x = res_node(d, s, heights, occ, i, dt, damp);
+          const uint32_t w = s.w[i];
+          body = (int)(w >> fw::NODE_BODY_SHIFT);
+          bnd = (w & fw::NODE_BOUNDARY) != 0;
+          const int gid = s.gid[i];
+          if (gid < 0) __stcg(dst + (gid & 0x7FFFFFFF), x);
+        }
+        const unsigned full = 0xFFFFFFFFu;
+        const unsigned mb = __ballot_sync(full, bnd);
+        if (mb != 0u) {
+          const int leader = __ffs(mb) - 1;
+          const int bl = __shfl_sync(full, body, leader);
+          const bool uniform = __all_sync(full, !bnd || body == bl);
+          float lx = bnd ? x.x : 1e30f, ly = bnd ? x.y : 1e30f;
+          float hx = bnd ? x.x : -1e30f, hy = bnd ? x.y : -1e30f;
+          if (uniform) {
+            for (int o = 16; o > 0; o >>= 1) {
+              lx = fminf(lx, __shfl_xor_sync(full, lx, o));
+              ly = fminf(ly, __shfl_xor_sync(full, ly, o));
+              hx = fmaxf(hx, __shfl_xor_sync(full, hx, o));
+              hy = fmaxf(hy, __shfl_xor_sync(full, hy, o));
             }
           }
-        }
-        for (int q = s.csrp[i]; q < s.csrp[i + 1]; ++q) {
-          const float2 c = s.f[s.csrs[q]];
-          f.x += c.x;
-          f.y += c.y;
-        }
-        const int bc = (int)(w & fw::NODE_BC_MASK);
-        fw::integrate(bc, f, s.m[i], s.bcv[i], dt, damp, x, v);
-        s.x[i] = x;
-        s.v[i] = v;
-        const int gid = s.gid[i];
-        if (gid < 0) dst[gid & 0x7FFFFFFF] = x;
-      }
-      const unsigned full = 0xFFFFFFFFu;
-      const unsigned mb = __ballot_sync(full, bnd);
-      if (mb != 0u) {
-        const int leader = __ffs(mb) - 1;
-        const int bl = __shfl_sync(full, body, leader);
-        const bool uniform = __all_sync(full, !bnd || body == bl);
-        float lx = bnd ? x.x : 1e30f, ly = bnd ? x.y : 1e30f;
-        float hx = bnd ? x.x : -1e30f, hy = bnd ? x.y : -1e30f;
-        if (uniform) {
-          for (int o = 16; o > 0; o >>= 1) {
-            lx = fminf(lx, __shfl_xor_sync(full, lx, o));
-            ly = fminf(ly, __shfl_xor_sync(full, ly, o));
-            hx = fmaxf(hx, __shfl_xor_sync(full, hx, o));
-            hy = fmaxf(hy, __shfl_xor_sync(full, hy, o));
+          if ((uniform && (int)(t & 31) == leader) || (!uniform && bnd)) {
+            int* rb = box_w + (size_t)body * 4;
+            atomicMin(rb + 0, fw::f2ord(lx));
+            atomicMin(rb + 1, fw::f2ord(ly));
+            atomicMax(rb + 2, fw::f2ord(hx));
+            atomicMax(rb + 3, fw::f2ord(hy));
           }
         }
-        if ((uniform && (int)(t & 31) == leader) || (!uniform && bnd)) {
-          int* rb = box_w + (size_t)body * 4;
-          atomicMin(rb + 0, fw::f2ord(lx));
-          atomicMin(rb + 1, fw::f2ord(ly));
-          atomicMax(rb + 2, fw::f2ord(hx));
-          atomicMax(rb + 3, fw::f2ord(hy));
-        }
       }
+      named_bar(1, FT);
+      if (t == 0) {
+        cuda::atomic_ref<int, cuda::thread_scope_device> a(*r.bar);
+        a.fetch_add(1, cuda::memory_order_release);
+      }
+    } else {
+      for (int i = P.n_g1 + bt; i < P.no; i += BT) res_node(d, s, heights, occ, i, dt, damp);
     }
-    // 5. arrive
-    __syncthreads();
-    if (t == 0) {
-      __threadfence();
-      atomicAdd(r.bar, 1);
-    }
+    __syncthreads();  // every owned node of substep k is updated
+    if (!front && k + 1 < nsteps)
+      for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
   }
   // ---- write the patch state back
   __syncthreads();
@@ -295,9 +362,20 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
       if ((s.conn[q].y >> 16) & kJ2Writer) d.j2state[r.eid[P.elem_off + q]] = s.j2[q];
 }
 
+using ResKernel = void (*)(Dev, Res, int, int, float, float);
+constexpr int kFrontChoices[] = {2, 4, 6, 8};
+inline ResKernel res_kernel(int front) {
+  switch (front) {
+    case 2: return k_resident<2>;
+    case 6: return k_resident<6>;
+    case 8: return k_resident<8>;
+    default: return k_resident<4>;
+  }
+}
+
 // Before a resident launch: reset the barrier and error flag, copy the body
 // boxes of the last substep into slot step0 % 3 and clear slot (step0+1) % 3.
-__global__ void k_resident_prologue(Dev d, Res r, int step0) {
+__global__ void k_res_prologue(Dev d, Res r, int step0) {
   if (threadIdx.x == 0) {
     *r.bar = 0;
     *r.err = 0;
@@ -313,7 +391,7 @@ __global__ void k_resident_prologue(Dev d, Res r, int step0) {
 
 // After a resident launch: publish the final body boxes to the gather path's
 // slots and advance the step counter.
-__global__ void k_resident_epilogue(Dev d, Res r, int step0, int nsteps) {
+__global__ void k_res_epilogue(Dev d, Res r, int step0, int nsteps) {
   const int last = step0 + nsteps;
   const int dst_slot = last & 1;
   for (int b = threadIdx.x; b < d.B; b += blockDim.x) {

@@ -282,6 +282,7 @@ struct fw_ctx {
   int grid_e = 1, grid_n = 1;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
+  int front_warps = 6;
   int path = FW_PATH_GATHER;
   Res res{};
   size_t res_smem = 0;
@@ -459,6 +460,12 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
     h.erase(std::unique(h.begin(), h.end()), h.end());
     for (int n : h) exported[n] = 1;
   }
+  std::vector<char> body_bnd(N, 0);
+  for (size_t k = 0; k < c->h_bnodes.size(); ++k) body_bnd[c->h_bnodes[k]] = 1;
+  // group 1 first (read by other patches or on a body boundary), each group ascending
+  for (int p = 0; p < P; ++p)
+    std::stable_partition(owned[p].begin(), owned[p].end(),
+                          [&](int n) { return exported[n] || body_bnd[n]; });
   std::vector<ResPatch> patches(P);
   std::vector<int32_t> rnodes, rhalo, reid, rcsrp;
   std::vector<uint2> rconn;
@@ -471,6 +478,8 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
     const std::vector<int>& h = halo[p];
     rp.node_off = (int)rnodes.size();
     rp.no = (int)ow.size();
+    rp.n_g1 = 0;
+    for (int n : ow) rp.n_g1 += (exported[n] || body_bnd[n]) ? 1 : 0;
     rp.halo_off = (int)rhalo.size();
     rp.nh = (int)h.size();
     if (rp.no + rp.nh >= 65536) { c->res_reason = "patch with >= 65536 nodes"; return 1; }
@@ -530,14 +539,21 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
   r.ne_max = ne_max;
   r.ncsr_max = ncsr_max;
   r.has_j2 = has_j2 ? 1 : 0;
+  const size_t tab_bytes = c->h_heights.size() * sizeof(float) + c->h_occ.size();
+  const bool stage = tab_bytes <= (size_t)kResTableBytes;
+  r.tab_h = stage ? (int)c->h_heights.size() : 0;
+  r.tab_o = stage ? (int)c->h_occ.size() : 0;
+  r.n_bodies = c->B;
+  if (c->B > 4096) { c->res_reason = "more than 4096 bodies"; return 1; }
   const size_t smem = res_layout(r, nullptr, nullptr);
   if ((long)smem > optin) {
     c->res_reason = "patch needs " + std::to_string(smem) + " B of shared memory";
     return 1;
   }
-  cudaError_t e1 = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  ResKernel kern = res_kernel(c->front_warps);
+  cudaError_t e1 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
-  cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident, kResThreads, smem);
+  cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kResThreads, smem);
   if (e1 != cudaSuccess || e2 != cudaSuccess || per_sm * sms < P) {
     cudaGetLastError();
     c->res_reason = "patches cannot all be resident";
@@ -576,12 +592,12 @@ int launch_resident(fw_ctx* c, int n) {
   }
   if (n <= 0) return FW_OK;
   const int step0 = (int)c->host_counter;
-  k_resident_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0);
+  k_res_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0);
   float dt = c->d.dt_uniform, damp = c->h_damp[0];
   void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&step0, (void*)&n, (void*)&dt, (void*)&damp};
-  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_resident, dim3(c->res.P), dim3(kResThreads), args,
-                                         c->res_smem, c->stream));
-  k_resident_epilogue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
+  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)res_kernel(c->front_warps), dim3(c->res.P),
+                                         dim3(kResThreads), args, c->res_smem, c->stream));
+  k_res_epilogue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
   c->launches += 3;
   c->host_counter += n;
   return check_kernel(c, "resident step");
@@ -941,6 +957,22 @@ int fw_set_path(fw_ctx* c, int32_t path, int32_t patches) {
   c->path_req = path;
   c->patches_req = patches;
   return FW_OK;
+}
+
+int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
+  if (!c) return FW_ERR_ARG;
+  switch (option) {
+    case FW_OPT_FRONT_WARPS: {
+      if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_FRONT_WARPS after fw_finalize");
+      bool ok = false;
+      for (int v : kFrontChoices) ok |= v == value;
+      if (!ok) return fail(c, FW_ERR_ARG, "FW_OPT_FRONT_WARPS must be 2, 4, 6 or 8");
+      c->front_warps = value;
+      return FW_OK;
+    }
+    default:
+      return fail(c, FW_ERR_ARG, "fw_set_option: unknown option %d", option);
+  }
 }
 
 int fw_get_path(const fw_ctx* c, int32_t* path, int32_t* patches) {

@@ -238,11 +238,15 @@ class PackedWorld:
         return out
 
 
-def build_native(packed: PackedWorld, device: int = 0, path: str = "auto", patches: int = 0) -> _native.NativeWorld:
+def build_native(packed: PackedWorld, device: int = 0, path: str = "auto", patches: int = 0,
+                 front_warps: int = 0) -> _native.NativeWorld:
     """Create the device world.  ``path``: "auto" (shared-memory-resident step
-    when the world fits on chip, else the gather step), "gather" or "resident"."""
+    when the world fits on chip, else the gather step), "gather" or "resident";
+    ``patches`` / ``front_warps``: resident-step tuning (0 = default)."""
     nw = _native.NativeWorld(device)
     nw.set_path(_native.PATHS[path], patches)
+    if front_warps:
+        nw.set_option(_native.FW_OPT_FRONT_WARPS, front_warps)
     nw.set_nodes(packed.coords, packed.vel, packed.bc_bits, packed.bc_vals)
     nw.set_elements(packed.conn, packed.mtype, packed.Ev, packed.nuv, packed.rhov, packed.syv, packed.Hv)
     nw.set_bodies(packed.noff, packed.ncnt, packed.eoff, packed.ecnt, packed.bscene, packed.bnoff,

@@ -137,6 +137,12 @@ int fw_finalize(fw_ctx* ctx);
  * identical results.  No reference counterpart: the reference has one Warp
  * path (flatworld/femspringmanager.py:941-1012). */
 int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
+/* Tuning options (fw_set_option), set before fw_finalize.
+ * FW_OPT_FRONT_WARPS: warps of a resident CTA that run the cross-CTA critical
+ * chain (2, 4, 6 or 8 of 16; default 6). */
+#define FW_OPT_FRONT_WARPS 1
+int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
+
 /* Active path (FW_PATH_GATHER or FW_PATH_RESIDENT) and patch count. */
 int fw_get_path(const fw_ctx* ctx, int32_t* path, int32_t* patches);
 

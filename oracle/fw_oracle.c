@@ -14,6 +14,8 @@
  * A third build, liboracle_f32fma.so, contracts a*b+c into FMAs; the distance
  * between the two FP32 builds is the rounding noise floor of the scheme itself
  * (the reference's Warp GPU path is compiled by NVRTC with FMA contraction on).
+ * A fourth, liboracle_f32libm.so, takes log from the C library, as the
+ * reference's Warp CPU device does.
  *
  * Restated reference code (all paths relative to the FlatWorld project root):
  *   flatworld/femspringmanager.py:59-68    get_jacobian_2d, get_weights_2d
@@ -38,8 +40,9 @@
  * restated from their published definitions: mat22 @ mat22 and mat @ vec sum
  * products in index order; determinant(m) = m00*m11 - m01*m10; inverse(m22) =
  * adjugate * (1/det), the zero matrix when det == 0; round() rounds half away
- * from zero (C roundf); floor, sqrt, log are the C library functions; the
- * serial CPU device applies atomic_add in launch order.
+ * from zero (C roundf); floor and sqrt are the C library functions; log is
+ * or_logf below (or the C library's logf in liboracle_f32libm.so); the serial
+ * CPU device applies atomic_add in launch order.
  */
 #include <math.h>
 #include <stdint.h>
@@ -51,6 +54,46 @@
 #define REAL float
 #endif
 
+/* log of the FP32 builds: unless USE_LIBM_LOG is defined, the method below
+ * (Cody-Waite reduction + atanh series, IEEE + - * / only), which the CUDA
+ * kernels evaluate with the same operations in the same order.  Any accurate
+ * log is a faithful reading of the reference's wp.log; this one makes CPU and
+ * GPU agree bit for bit.  USE_LIBM_LOG builds use the C library's logf, as the
+ * reference's Warp CPU device does. */
+static float or_logf(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;
+  if (x == INFINITY) return x;
+  uint32_t u;
+  memcpy(&u, &x, sizeof(u));
+  int e = 0;
+  if (u < 0x00800000u) {
+    x = x * 8388608.0f;
+    memcpy(&u, &x, sizeof(u));
+    e = -23;
+  }
+  e += (int)((u >> 23) & 0xFFu) - 127;
+  u = (u & 0x007FFFFFu) | 0x3F800000u;
+  float m;
+  memcpy(&m, &u, sizeof(m));
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float z = s * s;
+  float p = 1.0f / 13.0f;
+  p = p * z + 1.0f / 11.0f;
+  p = p * z + 1.0f / 9.0f;
+  p = p * z + 1.0f / 7.0f;
+  p = p * z + 1.0f / 5.0f;
+  p = p * z + 1.0f / 3.0f;
+  const float r = z * p;
+  const float s2 = 2.0f * s;
+  const float lm = s2 + s2 * r;
+  const float fe = (float)e;
+  return fe * 0.693115234375f + (fe * 3.194618329871446e-05f + lm);
+}
+
 #if defined(REAL_IS_DOUBLE)
 #define R_SQRT sqrt
 #define R_LOG log
@@ -59,7 +102,11 @@
 #define R_FABS fabs
 #else
 #define R_SQRT sqrtf
+#if defined(USE_LIBM_LOG)
 #define R_LOG logf
+#else
+#define R_LOG or_logf
+#endif
 #define R_FLOOR floorf
 #define R_ROUND roundf
 #define R_FABS fabsf
@@ -753,6 +800,9 @@ void or_point_stress(int type, float E, float nu, float sy, float H, const float
   }
   if (eqps_out) *eqps_out = (type == MAT_MISES) ? eqo : eqv;
 }
+
+/* The oracle's FP32 log, exported for its accuracy test. */
+float or_log32(float x) { return R_LOG(x); }
 
 void or_destroy(or_world* w) {
   if (!w) return;

@@ -43,7 +43,8 @@ _f64p = C.POINTER(C.c_double)
 
 
 def _lib(precision: str):
-    name = {"f32": "liboracle_f32.so", "f32fma": "liboracle_f32fma.so", "f64": "liboracle_f64.so"}[precision]
+    name = {"f32": "liboracle_f32.so", "f32fma": "liboracle_f32fma.so", "f32libm": "liboracle_f32libm.so",
+            "f64": "liboracle_f64.so"}[precision]
     if name not in _LIBS:
         path = os.path.join(HERE, name)
         if not os.path.exists(path):
@@ -68,6 +69,8 @@ def _lib(precision: str):
         L.or_point_stress.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _f32p, _f32p, C.c_float,
                                       _f64p, _f64p, _f64p]
         L.or_destroy.argtypes = [C.c_void_p]
+        L.or_log32.argtypes = [C.c_float]
+        L.or_log32.restype = C.c_float
         _LIBS[name] = L
     return _LIBS[name]
 
@@ -122,6 +125,11 @@ def point_stress(mtype, E, nu, F, sigma_y=0.0, H=0.0, eps_p=None, eqps=0.0, prec
     L.or_point_stress(int(mtype), float(E), float(nu), float(sigma_y), float(H), Fa[1], ep[1], float(eqps),
                       s.ctypes.data_as(_f64p), epo.ctypes.data_as(_f64p), eqo.ctypes.data_as(_f64p))
     return s, epo, float(eqo[0])
+
+
+def log32(x, precision="f32"):
+    """The FP32 log the oracle uses (for its accuracy test)."""
+    return float(_lib(precision).or_log32(float(x)))
 
 
 class OracleLoop:

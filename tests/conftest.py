@@ -18,7 +18,8 @@ def _built_oracle():
     """The oracle libraries are built from oracle/fw_oracle.c when missing."""
     import subprocess
 
-    need = [os.path.join(ROOT, "oracle", f) for f in ("liboracle_f32.so", "liboracle_f64.so", "liboracle_f32fma.so")]
+    need = [os.path.join(ROOT, "oracle", f) for f in ("liboracle_f32.so", "liboracle_f64.so", "liboracle_f32fma.so",
+                                                          "liboracle_f32libm.so")]
     if not all(os.path.exists(p) for p in need):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
     yield
