@@ -61,6 +61,8 @@ _SIGNATURES = {
     "fw_read_counters": (C.c_int, [_vp, _i64p]),
     "fw_launch_count": (C.c_int64, [_vp]),
     "fw_build_info": (C.c_char_p, []),
+    "fw_step_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp,
+                                  _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_int32]),
 }
 
 

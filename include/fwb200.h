@@ -194,6 +194,38 @@ int fw_read_counters(fw_ctx* ctx, int64_t* counters);
  * that the CUDA path ran; used by the benchmark's gpu_launches field). */
 int64_t fw_launch_count(const fw_ctx* ctx);
 
+/* Allocation-free substep for callers that must not allocate device memory
+ * (a real-time loop where cudaMalloc may block and synchronise the device, or
+ * a process whose device memory is handed out by its own pool allocator under
+ * a fixed budget).  No counterpart in the reference: it has no C interface.
+ * Advances n_steps substeps of the gather step without ground contact
+ * (elastic / NeoHookean / J2 triangles, nodal boundary conditions, symplectic
+ * Euler); identical arithmetic to fw_step on a world without contact pairs.
+ * Every pointer is caller-owned DEVICE memory on the current device:
+ *   x, v        [2*n_nodes]  positions / velocities, updated in place
+ *   node_bc     [n_nodes]    OR of FW_BC_*;  bc_values [2*n_nodes];  mass [n_nodes]
+ *   conn        [3*n_elems]  node ids;  jinv [4*n_elems] row-major Dm^-1
+ *   elem_mat    [4*n_elems]  rest area, lambda, mu, material type (1, 2, 3 as float)
+ *   j2_state    [4*n_elems]  eps_p (3) + eqps, updated; j2_param [2*n_elems]
+ *               (yield stress, hardening).  Both may be NULL when no triangle
+ *               is J2; J2 triangles then run with zero plastic state.
+ *   csr_off     [n_nodes+1], csr_slot [3*n_elems]  node -> (3*e + corner),
+ *               ascending e within a node
+ * The scratch (one float2 per corner) is a fixed array inside the library:
+ * at most FW_NOALLOC_MAX_ELEMS triangles (3 MiB, held by every GPU that loads
+ * the library); larger meshes are rejected with FW_ERR_ARG.  The first call on
+ * a device looks the array's address up (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU race.  Work is queued on `stream` (NULL: legacy default).
+ * err/err_len: optional buffer for the error text. */
+#define FW_NOALLOC_MAX_ELEMS 131072
+int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps, float dt, float damping,
+                    float* x, float* v, const int32_t* node_bc, const float* bc_values,
+                    const float* mass, const int32_t* conn, const float* jinv,
+                    const float* elem_mat, float* j2_state, const float* j2_param,
+                    const int32_t* csr_off, const int32_t* csr_slot, void* stream, char* err,
+                    int32_t err_len);
+
 /* Library build identification string (arch, flags). */
 const char* fw_build_info(void);
 
