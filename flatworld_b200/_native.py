@@ -24,6 +24,9 @@ FW_PATH_GATHER = 1
 FW_PATH_RESIDENT = 2
 PATHS = {"auto": FW_PATH_AUTO, "gather": FW_PATH_GATHER, "resident": FW_PATH_RESIDENT}
 FW_OPT_FRONT_WARPS = 1
+FW_OPT_BLOCK_ELEMS = 2
+FW_OPT_BLOCK_NODES = 3
+FW_OPT_GRID_ELEMS = 4
 
 _lock = threading.Lock()
 _lib = None
@@ -48,6 +51,8 @@ _SIGNATURES = {
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "fw_snapshot": (C.c_int, [_vp, C.c_int32]),
+    "fw_restore": (C.c_int, [_vp, C.c_int32]),
     "fw_finalize": (C.c_int, [_vp]),
     "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_step_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
@@ -178,6 +183,12 @@ class NativeWorld:
 
     def set_option(self, option: int, value: int):
         self._check(self._L.fw_set_option(self._h, int(option), int(value)), "fw_set_option")
+
+    def snapshot(self, slot: int = 0):
+        self._check(self._L.fw_snapshot(self._h, int(slot)), "fw_snapshot")
+
+    def restore(self, slot: int = 0):
+        self._check(self._L.fw_restore(self._h, int(slot)), "fw_restore")
 
     def get_path(self):
         p = C.c_int32()

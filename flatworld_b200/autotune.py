@@ -1,0 +1,128 @@
+"""Project autotuner for the step's launch shapes.
+
+* ``tune_batched(loop)``: times the gather step of a BatchedLoop for each
+  (element block, node block) candidate on the loop's own world -- the state
+  is saved with fw_snapshot before and restored after, so tuning does not move
+  the simulation -- and applies the fastest.
+* ``tune_resident(build_domains)``: builds the single-scene resident step with
+  each (front warps, patches) candidate and times it; returns the best kwargs
+  for ExplicitLoop.
+
+Results are cached per (GPU name, world size) in
+``$FLATWORLD_B200_CACHE`` (default ~/.cache/flatworld_b200/autotune.json).
+"""
+
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+_SNAP = 1023  # snapshot slot reserved for tuning
+
+
+def _cache_path():
+    d = os.environ.get("FLATWORLD_B200_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "flatworld_b200"))
+    os.makedirs(d, exist_ok=True)
+    return os.path.join(d, "autotune.json")
+
+
+def _load_cache():
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_cache(key, value):
+    c = _load_cache()
+    c[key] = value
+    tmp = _cache_path() + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(c, f, indent=1)
+    os.replace(tmp, _cache_path())
+
+
+def _gpu_name(device):
+    import torch
+
+    return torch.cuda.get_device_name(device)
+
+
+def _time_steps(native, steps, dt, stream):
+    import torch
+
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    native.step(steps, dt)
+    e.record(stream)
+    e.synchronize()
+    return s.elapsed_time(e) / steps
+
+
+def tune_batched(loop, blocks=(128, 256, 512), steps=16, use_cache=True):
+    """Pick the gather kernels' block sizes for ``loop`` (a BatchedLoop)."""
+    import torch
+
+    key = f"batched|{_gpu_name(loop._native.device)}|N={loop.n_nodes}|E={loop.n_elems}|S={loop.S}"
+    if use_cache:
+        hit = _load_cache().get(key)
+        if hit:
+            loop.set_launch(hit["block_elems"], hit["block_nodes"])
+            return dict(hit, cached=True)
+    stream = torch.cuda.Stream(device=loop._native.device)
+    loop.set_stream(stream.cuda_stream)
+    dt = float(np.float32(loop.dt.min()))
+    nat = loop._native
+    nat.snapshot(_SNAP)
+    results = []
+    for be in blocks:
+        for bn in blocks:
+            loop.set_launch(be, bn)
+            nat.restore(_SNAP)
+            nat.step(2, dt)
+            nat.restore(_SNAP)
+            ms = _time_steps(nat, steps, dt, stream)
+            results.append((ms, be, bn))
+    nat.restore(_SNAP)
+    nat.synchronize()
+    ms, be, bn = min(results)
+    loop.set_launch(be, bn)
+    loop.set_stream(None)
+    out = {"block_elems": be, "block_nodes": bn, "ms_per_step": ms,
+           "candidates": [{"block_elems": b, "block_nodes": n, "ms": m} for m, b, n in results]}
+    _store_cache(key, out)
+    return out
+
+
+def tune_resident(build_domains, fronts=(4, 6, 8), patches=(0, 128, 96), steps=200, device=0, use_cache=True):
+    """Pick (front_warps, patches) of the resident step for the single-scene
+    world returned by ``build_domains()``; returns ExplicitLoop kwargs."""
+    import torch
+
+    from .explicitloop import ExplicitLoop
+
+    probe = ExplicitLoop(0.0, build_domains(), device=device)
+    key = f"resident|{_gpu_name(device)}|N={probe._packed.N}|E={probe._packed.E}"
+    if use_cache:
+        hit = _load_cache().get(key)
+        if hit:
+            return {"front_warps": hit["front_warps"], "patches": hit["patches"]}
+    results = []
+    stream = torch.cuda.Stream(device=device)
+    for fwp in fronts:
+        for p in patches:
+            lp = ExplicitLoop(0.0, build_domains(), device=device, path="resident", patches=p, front_warps=fwp)
+            lp._native.set_stream(stream.cuda_stream)
+            dt = float(np.float32(lp.stableTime))
+            lp._native.step(20, dt)
+            ms = _time_steps(lp._native, steps, dt, stream)
+            results.append((ms, fwp, p))
+            lp._native.close()
+    ms, fwp, p = min(results)
+    _store_cache(key, {"front_warps": fwp, "patches": p, "ms_per_step": ms,
+                       "candidates": [{"front_warps": f, "patches": q, "ms": m} for m, f, q in results]})
+    return {"front_warps": fwp, "patches": p}

@@ -1,0 +1,144 @@
+"""Batched form: many independent scenes stepped together in one world.
+
+A *scene* is what one reference ``ExplicitLoop`` holds (FEM domains plus their
+grounds).  ``BatchedLoop`` packs S scenes of uneven sizes into one ragged
+node / triangle index space and advances all of them with the same two kernels
+per substep (captured in CUDA graphs), instead of S separate loops.  Each
+scene keeps its own time step, step counter and broad-phase gate, and scenes
+never exchange forces, so every scene's result is bit-identical to stepping it
+alone in its own ``ExplicitLoop`` (tests/test_batch.py checks this).
+
+The reference cannot batch such scenes in one loop: one ExplicitLoop batches a
+single height field and a single voxel grid (flatworld/mixedcontact.py:2140,
+2211), so per-body voxel grids need one loop per body.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native
+from .world import PackedWorld, SceneLayout, build_native, substep_schedule
+
+
+class BatchedLoop:
+    """Advance S independent scenes together.
+
+    Args:
+        scenes: list of domain lists (one per scene, as passed to ExplicitLoop)
+        dt, useAdapativeDT, damping: as ExplicitLoop, applied to every scene
+            (a sequence gives one value per scene)
+        device: CUDA ordinal
+        block_elems, block_nodes: launch shape of the step kernels (0: tuned
+            default; see flatworld_b200.autotune)
+    """
+
+    def __init__(self, scenes, dt=0.0, useAdapativeDT=True, damping=0.0, device=0,
+                 block_elems=0, block_nodes=0):
+        S = len(scenes)
+        dts = dt if np.iterable(dt) else [dt] * S
+        ada = useAdapativeDT if np.iterable(useAdapativeDT) else [useAdapativeDT] * S
+        damp = damping if np.iterable(damping) else [damping] * S
+        self.layouts = [SceneLayout(d, dt=a, damping=c, useAdapativeDT=b)
+                        for d, a, b, c in zip(scenes, dts, ada, damp)]
+        self.packed = PackedWorld(self.layouts)
+        self._native = build_native(self.packed, device=device, path="gather")
+        if block_elems or block_nodes:
+            self.set_launch(block_elems, block_nodes)
+        self.S = S
+        self.dt = np.array([lay.dt for lay in self.layouts], dtype=np.float64)
+        self.counters = np.zeros(S, dtype=np.int64)
+        self._active = np.ones(S, dtype=np.int32)
+
+    # ---- sizes
+    @property
+    def n_nodes(self):
+        return self.packed.N
+
+    @property
+    def n_elems(self):
+        return self.packed.E
+
+    def scene_elems(self, s):
+        return self.layouts[s].n_elems
+
+    def set_launch(self, block_elems=0, block_nodes=0):
+        """Change the step kernels' block sizes (cached graphs are rebuilt)."""
+        if block_elems:
+            self._native.set_option(_native.FW_OPT_BLOCK_ELEMS, block_elems)
+        if block_nodes:
+            self._native.set_option(_native.FW_OPT_BLOCK_NODES, block_nodes)
+
+    def set_stream(self, stream_ptr):
+        self._native.set_stream(stream_ptr)
+
+    # ---- stepping
+    def _set_active(self, active):
+        active = np.asarray(active, dtype=np.int32)
+        if not np.array_equal(active, self._active):
+            self._native.set_active(active)
+            self._active = active.copy()
+
+    def advance(self, n: int = 1):
+        """n substeps of every active scene, each with its own dt."""
+        d32 = self.dt.astype(np.float32)
+        if np.all(d32 == d32[0]):
+            self._native.step(int(n), float(d32[0]))
+        else:
+            self._native.step_scenes(int(n), d32)
+        self.counters += int(n) * self._active
+
+    def advanceWithTime(self, frame_dt=1.0 / 60.0):
+        """Every scene advances by frame_dt in its own substeps (the reference's
+        advanceWithTime loop per scene, explicitloop.py:558-589).  Scenes with
+        fewer substeps are frozen while the others finish."""
+        runs = [substep_schedule(frame_dt, lay.stableTime, lay.default_dt, lay.useAdapative)
+                for lay in self.layouts]
+        pos = [0] * self.S      # index into each scene's run list
+        left = [r[0][0] if r else 0 for r in runs]
+        base_active = self._active.copy()
+        while True:
+            live = [s for s in range(self.S) if base_active[s] and pos[s] < len(runs[s])]
+            if not live:
+                break
+            dts = np.zeros(self.S, dtype=np.float32)
+            act = np.zeros(self.S, dtype=np.int32)
+            for s in live:
+                dts[s] = np.float32(runs[s][pos[s]][1])
+                act[s] = 1
+            n = min(left[s] for s in live)
+            self._set_active(act)
+            self._native.step_scenes(n, dts)
+            for s in live:
+                self.counters[s] += n
+                left[s] -= n
+                self.dt[s] = runs[s][pos[s]][1]
+                if left[s] == 0:
+                    pos[s] += 1
+                    if pos[s] < len(runs[s]):
+                        left[s] = runs[s][pos[s]][0]
+        self._set_active(base_active)
+
+    def synchronize(self):
+        self._native.synchronize()
+
+    # ---- readback
+    def _node_range(self, s):
+        bodies = self.packed.scene_bodies[s]
+        n0 = int(self.packed.noff[bodies[0]])
+        nn = int(sum(int(self.packed.ncnt[b]) for b in bodies))
+        return n0, nn
+
+    def coords(self, s):
+        n0, nn = self._node_range(s)
+        return self._native.read_nodes(_native.FW_FIELD_X, n0, nn)
+
+    def velocities(self, s):
+        n0, nn = self._node_range(s)
+        return self._native.read_nodes(_native.FW_FIELD_V, n0, nn)
+
+    def all_coords(self):
+        return self._native.read_nodes(_native.FW_FIELD_X, 0, self.packed.N)
+
+    def launch_count(self):
+        return self._native.launch_count()

@@ -33,7 +33,8 @@ using fw::Pair;
 
 namespace {
 
-constexpr int kBlock = 256;
+constexpr int kBlock = 256;     // default block size of the gather kernels
+constexpr int kMaxBlock = 512;  // launch bound (block sizes are a runtime option)
 constexpr int kGraphSteps = 32;
 
 struct Dev {
@@ -109,7 +110,7 @@ __device__ void step_control(const Dev& d) {
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_elements(Dev d) {
+__global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
   if (blockIdx.x == 0) step_control(d);
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) {
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(kBlock) k_elements(Dev d) {
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_nodes(Dev d) {
+__global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < d.N;
   const uint32_t w = valid ? d.node_word[i] : 0u;
@@ -280,6 +281,16 @@ struct fw_ctx {
   std::vector<std::pair<uint64_t, cudaGraphExec_t>> graphs;
   cudaStream_t graph_stream = nullptr;
   int grid_e = 1, grid_n = 1;
+  int block_e = kBlock, block_n = kBlock, grid_e_cap = 0, sms = 148;
+  // snapshots: device copies of the full step state, one set per slot
+  struct Snap {
+    float2 *x = nullptr, *v = nullptr;
+    float4* j2 = nullptr;
+    int32_t *counter = nullptr, *ring = nullptr, *mode_req = nullptr;
+    int64_t host_counter = 0;
+    bool valid = false;
+  };
+  std::vector<Snap> snaps;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
@@ -335,9 +346,16 @@ int check_kernel(fw_ctx* c, const char* what) {
   return FW_OK;
 }
 
+void set_grids(fw_ctx* c) {
+  const int E = c->E > 0 ? c->E : 1, N = c->N > 0 ? c->N : 1;
+  const int cap = c->grid_e_cap > 0 ? c->grid_e_cap : c->sms * 8;
+  c->grid_e = std::max(1, std::min((E + c->block_e - 1) / c->block_e, cap));
+  c->grid_n = std::max(1, (N + c->block_n - 1) / c->block_n);
+}
+
 int launch_step(fw_ctx* c) {
-  k_elements<<<c->grid_e, kBlock, 0, c->stream>>>(c->d);
-  k_nodes<<<c->grid_n, kBlock, 0, c->stream>>>(c->d);
+  k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
+  k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
   c->launches += 2;
   return check_kernel(c, "step");
 }
@@ -364,8 +382,8 @@ int get_graph(fw_ctx* c, cudaGraphExec_t* out) {
   cudaGraph_t g = nullptr;
   FW_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < kGraphSteps; ++k) {
-    k_elements<<<c->grid_e, kBlock, 0, c->stream>>>(c->d);
-    k_nodes<<<c->grid_n, kBlock, 0, c->stream>>>(c->d);
+    k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
+    k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
   }
   cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
   if (ce != cudaSuccess) return fail(c, FW_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
@@ -926,10 +944,8 @@ int fw_finalize(fw_ctx* c) {
   k_prepare_mass<<<(N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d);
   c->launches += 2;
   if ((rc = check_kernel(c, "prepare"))) return rc;
-  int dev_sms = 148;
-  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
-  c->grid_e = std::max(1, std::min((E + kBlock - 1) / kBlock, dev_sms * 8));
-  c->grid_n = std::max(1, (N + kBlock - 1) / kBlock);
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+  set_grids(c);
   // zero-dt construction step (setGlobalAABB -> substep(0, 0))
   if ((rc = launch_step(c))) return rc;
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -970,9 +986,67 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
       c->front_warps = value;
       return FW_OK;
     }
+    case FW_OPT_BLOCK_ELEMS:
+    case FW_OPT_BLOCK_NODES: {
+      if (value < 32 || value > kMaxBlock || value % 32)
+        return fail(c, FW_ERR_ARG, "block size must be a multiple of 32 in [32, %d]", kMaxBlock);
+      (option == FW_OPT_BLOCK_ELEMS ? c->block_e : c->block_n) = value;
+      set_grids(c);
+      drop_graphs(c);
+      return FW_OK;
+    }
+    case FW_OPT_GRID_ELEMS: {
+      if (value < 0) return fail(c, FW_ERR_ARG, "FW_OPT_GRID_ELEMS must be >= 0");
+      c->grid_e_cap = value;
+      set_grids(c);
+      drop_graphs(c);
+      return FW_OK;
+    }
     default:
       return fail(c, FW_ERR_ARG, "fw_set_option: unknown option %d", option);
   }
+}
+
+int fw_snapshot(fw_ctx* c, int32_t slot) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_snapshot before fw_finalize");
+  if (slot < 0 || slot >= 1024) return fail(c, FW_ERR_ARG, "fw_snapshot: slot outside [0, 1024)");
+  if ((int)c->snaps.size() <= slot) c->snaps.resize(slot + 1);
+  fw_ctx::Snap& sn = c->snaps[slot];
+  const size_t E = c->d.has_j2 ? c->E : 1;
+  int rc;
+  if (!sn.x) {
+    if ((rc = dalloc(c, &sn.x, c->N)) || (rc = dalloc(c, &sn.v, c->N)) || (rc = dalloc(c, &sn.j2, E)) ||
+        (rc = dalloc(c, &sn.counter, c->S)) || (rc = dalloc(c, &sn.ring, 8 * (size_t)c->B)) ||
+        (rc = dalloc(c, &sn.mode_req, c->S)))
+      return rc;
+  }
+  FW_CUDA(c, cudaMemcpyAsync(sn.x, c->d.x, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(sn.v, c->d.v, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(sn.j2, c->d.j2state, sizeof(float4) * E, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(sn.counter, c->d.scene_counter, sizeof(int32_t) * c->S, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(sn.ring, c->d.aabb_ring, sizeof(int32_t) * 8 * c->B, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(sn.mode_req, c->d.scene_mode_req, sizeof(int32_t) * c->S, cudaMemcpyDeviceToDevice, c->stream));
+  sn.host_counter = c->host_counter;
+  sn.valid = true;
+  return FW_OK;
+}
+
+int fw_restore(fw_ctx* c, int32_t slot) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_restore before fw_finalize");
+  if (slot < 0 || slot >= (int)c->snaps.size() || !c->snaps[slot].valid)
+    return fail(c, FW_ERR_ARG, "fw_restore: slot %d holds no snapshot", slot);
+  fw_ctx::Snap& sn = c->snaps[slot];
+  const size_t E = c->d.has_j2 ? c->E : 1;
+  FW_CUDA(c, cudaMemcpyAsync(c->d.x, sn.x, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.v, sn.v, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.j2state, sn.j2, sizeof(float4) * E, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_counter, sn.counter, sizeof(int32_t) * c->S, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.aabb_ring, sn.ring, sizeof(int32_t) * 8 * c->B, cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_mode_req, sn.mode_req, sizeof(int32_t) * c->S, cudaMemcpyDeviceToDevice, c->stream));
+  c->host_counter = sn.host_counter;
+  return FW_OK;
 }
 
 int fw_get_path(const fw_ctx* c, int32_t* path, int32_t* patches) {

@@ -141,7 +141,22 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
  * FW_OPT_FRONT_WARPS: warps of a resident CTA that run the cross-CTA critical
  * chain (2, 4, 6 or 8 of 16; default 6). */
 #define FW_OPT_FRONT_WARPS 1
+/* FW_OPT_BLOCK_ELEMS / FW_OPT_BLOCK_NODES: block size of the gather path's
+ * element / node kernel (multiple of 32, <= 512; default 256).
+ * FW_OPT_GRID_ELEMS: cap on the element kernel's grid (0 = 8 x SMs).
+ * These three may also be changed after fw_finalize (used by the autotuner). */
+#define FW_OPT_BLOCK_ELEMS 2
+#define FW_OPT_BLOCK_NODES 3
+#define FW_OPT_GRID_ELEMS 4
 int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
+
+/* Checkpoint / resume: copy the whole step state (positions, velocities, J2
+ * state, step counters, body boxes) into snapshot `slot` (device memory owned
+ * by the context, allocated on first use), or back.  Queued on the stream.
+ * No reference counterpart: the reference's reset() leaves FEM state alone
+ * (flatworld/explicitloop.py:635-679). */
+int fw_snapshot(fw_ctx* ctx, int32_t slot);
+int fw_restore(fw_ctx* ctx, int32_t slot);
 
 /* Active path (FW_PATH_GATHER or FW_PATH_RESIDENT) and patch count. */
 int fw_get_path(const fw_ctx* ctx, int32_t* path, int32_t* patches);

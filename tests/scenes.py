@@ -117,3 +117,46 @@ def plain_large_scene(fw, seed=0, n=256, hf_offset=0.15):
     h = hf_offset + sum(a * np.sin(w * xs + p) for a, w, p in zip(amps, omegas, phases))
     hf = fw.HeightFieldDomain(2, h.astype(np.float32), lb=[-1.0, -1.0], ub=[2.0, 1.0])
     return [hf, fem]
+
+
+def ragged_body_scene(fw, rng, index, h=0.01, rho=2000.0, voxel_cells=128, voxel_h=0.02):
+    """One scene of the ragged batch: a structured rectangle with node count
+    log-uniform in [100, 20000] and aspect ratio U[0.25, 4]; material by
+    index % 3 (Elastic, NeoHookean, J2 with yield stress 0.02 E, H = 0),
+    E ~ U[1e4, 1e6], nu ~ U[0.2, 0.45]; its own 128 x 128 voxel grid with
+    Bernoulli(0.15) occupancy.  Fixed here (unspecified by the workload): 1 cm
+    elements, density 2000, 2 cm voxel cells, the body starting 5 cm inside the
+    grid moving down at 1 m/s under gravity 9.8 -- with these, dt = 5e-5 is
+    below every body's CFL and contact bound."""
+    n = float(np.exp(rng.uniform(np.log(100.0), np.log(20000.0))))
+    asp = float(rng.uniform(0.25, 4.0))
+    nx = max(1, int(round(np.sqrt(n * asp) - 1)))
+    ny = max(1, int(round(np.sqrt(n / asp) - 1)))
+    E = float(rng.uniform(1e4, 1e6))
+    nu = float(rng.uniform(0.2, 0.45))
+    kind = index % 3
+    if kind == 0:
+        mat = fw.Elastic(E, nu, rho)
+    elif kind == 1:
+        mat = fw.HyperElastic(E, nu, rho)
+    else:
+        mat = fw.MisesPlastic(E, nu, rho, sigma_y=0.02 * E, H=0.0)
+    W, Hh = nx * h, ny * h
+    extent = voxel_cells * voxel_h
+    lb = np.array([-0.5 * extent + 0.5 * W, -extent + 0.05], np.float32)
+    occ = (rng.random((voxel_cells, voxel_cells)) < 0.15).astype(np.int32)
+    vox = fw.VoxelGridDomain(2, voxel_cells, voxel_cells, lb, lb + extent, occupancy_np=occ)
+    conn, coords = fw.structured_rectangle(nx, ny, W, Hh, origin=(0.0, 0.0))
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])],
+                       initials=[fw.InitialVel("ALL", [0.0, -1.0])])
+    return [vox, fem]
+
+
+def ragged_batch(fw, n_scenes=2048, seed=0):
+    """Scene i draws from its own generator (seed, i), so any one scene can be
+    rebuilt alone (ragged_batch_one) for the one-body-at-a-time baseline."""
+    return [ragged_batch_one(fw, i, seed) for i in range(n_scenes)]
+
+
+def ragged_batch_one(fw, index, seed=0):
+    return ragged_body_scene(fw, np.random.default_rng([seed, index]), index)

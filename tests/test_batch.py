@@ -1,0 +1,91 @@
+"""Batched form: many independent scenes in one world (GPU).
+
+Each scene's result must be bit-identical to the same scene stepped alone by
+the plain path, and to the FP32 oracle; freezing, snapshots and the autotuner
+must not change results."""
+
+import numpy as np
+import pytest
+
+import flatworld_b200 as fw
+import oracle
+from flatworld_b200 import autotune
+from flatworld_b200.batch import BatchedLoop
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+FRAME = 1.0 / 60.0
+
+
+def small_batch(n=9, seed=7):
+    """Ragged scenes capped at ~3000 nodes so the oracle stays quick."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n:
+        sc = scenes.ragged_body_scene(fw, rng, len(out))
+        if sc[1].nnodes <= 3000:
+            out.append(sc)
+    return out
+
+
+def test_batched_equals_alone_and_oracle_fixed_dt():
+    build = lambda: small_batch()  # noqa: E731
+    b = BatchedLoop(build(), dt=5e-5, useAdapativeDT=False)
+    b.advance(300)
+    alone = build()
+    for s, doms in enumerate(alone):
+        lp = fw.ExplicitLoop(5e-5, doms, useAdapativeDT=False, path="gather")
+        lp.advance_n(300)
+        xa = lp.femSpringManager.coords.numpy()[: doms[1].nnodes]
+        assert np.array_equal(b.coords(s), xa), s
+        assert np.array_equal(b.velocities(s), lp.femSpringManager.V.numpy()[: doms[1].nnodes]), s
+    for s in (0, 1, 2):  # one scene per material law
+        o = oracle.OracleLoop(build()[s], 5e-5, useAdapativeDT=False, threads=8)
+        o.advance(300)
+        xo, vo, _ = o.state()
+        assert np.array_equal(b.coords(s).astype(np.float64), xo), s
+        assert np.array_equal(b.velocities(s).astype(np.float64), vo), s
+
+
+def test_batched_advance_with_time_per_scene_dt():
+    """Adaptive dt differs per scene: each scene takes its own substeps."""
+    build = lambda: small_batch(n=6, seed=11)  # noqa: E731
+    b = BatchedLoop(build(), useAdapativeDT=True)
+    assert len(set(np.round(b.dt, 12))) > 1
+    for _ in range(2):
+        b.advanceWithTime(FRAME)
+    for s, doms in enumerate(build()):
+        lp = fw.ExplicitLoop(0.0, doms, useAdapativeDT=True, path="gather")
+        for _ in range(2):
+            lp.advanceWithTime(FRAME)
+        assert np.array_equal(b.coords(s), lp.femSpringManager.coords.numpy()[: doms[1].nnodes]), s
+        assert b.counters[s] == lp._counter_py
+
+
+def test_snapshot_restore_and_frozen_scenes():
+    b = BatchedLoop(small_batch(n=4), dt=5e-5, useAdapativeDT=False)
+    b.advance(50)
+    b._native.snapshot(3)
+    b.advance(60)
+    xa = b.all_coords()
+    b._native.restore(3)
+    b.advance(60)
+    assert np.array_equal(xa, b.all_coords())
+    frozen = b.coords(1)
+    b._set_active([1, 0, 1, 1])
+    b.advance(40)
+    assert np.array_equal(frozen, b.coords(1))
+    assert not np.array_equal(xa[: len(b.coords(0))], b.coords(0))
+
+
+def test_autotune_keeps_results(tmp_path, monkeypatch):
+    monkeypatch.setenv("FLATWORLD_B200_CACHE", str(tmp_path))
+    a = BatchedLoop(small_batch(n=5), dt=5e-5, useAdapativeDT=False)
+    c = BatchedLoop(small_batch(n=5), dt=5e-5, useAdapativeDT=False)
+    best = autotune.tune_batched(a, blocks=(128, 256), steps=4)
+    assert best["block_elems"] in (128, 256) and len(best["candidates"]) == 4
+    a.advance(100)
+    c.advance(100)
+    assert np.array_equal(a.all_coords(), c.all_coords())
+    again = autotune.tune_batched(a, blocks=(128, 256), steps=4)
+    assert again.get("cached")
