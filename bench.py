@@ -236,6 +236,7 @@ def run_batched(args, rank, world, local):
     lat = [s_.elapsed_time(e_) for s_, e_ in ev]
     ms = float(sum(lat))
     E = b.n_elems
+    finite = bool(np.isfinite(b.all_coords()).all())
     value = E * substeps / (ms / 1e3)
     # plain path: sample of the same bodies, one loop per body
     rng = np.random.default_rng(1234)
@@ -271,7 +272,7 @@ def run_batched(args, rank, world, local):
         "config": {"workload": f"ragged batch of {args.scenes} bodies on voxel grids, dt 5e-5",
                    "elements": E, "nodes": b.n_nodes, "bodies": args.scenes, "substeps": substeps,
                    "step": "100 substeps", "l2": "working set larger than L2", "launch": tuned,
-                   "host_build_s": build_s},
+                   "host_build_s": build_s, "state_finite": finite},
         "batched_vs_plain": {"plain_value": plain_value, "ratio": value / plain_value,
                              "plain_sample_bodies": len(pick),
                              "plain_p50_ms_per_substep": percentile_ms(plain_lat, 50)},
