@@ -52,10 +52,15 @@ _SIGNATURES = {
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_snapshot": (C.c_int, [_vp, C.c_int32]),
+    "fw_arena_init": (C.c_int, [_vp, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int64]),
+    "fw_arena_commit": (C.c_int, [_vp, _i32p]),
+    "fw_arena_remove": (C.c_int, [_vp, C.c_int32]),
+    "fw_arena_scene_info": (C.c_int, [_vp, C.c_int32, _i64p]),
     "fw_restore": (C.c_int, [_vp, C.c_int32]),
     "fw_finalize": (C.c_int, [_vp]),
     "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_step_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
+    "fw_step_served": (C.c_int, [_vp, _f32p]),
     "fw_set_active": (C.c_int, [_vp, _i32p]),
     "fw_synchronize": (C.c_int, [_vp]),
     "fw_read_nodes": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32]),
@@ -190,6 +195,25 @@ class NativeWorld:
     def restore(self, slot: int = 0):
         self._check(self._L.fw_restore(self._h, int(slot)), "fw_restore")
 
+    # ---- arena (served form)
+    def arena_init(self, max_nodes, max_elems, max_bodies, max_scenes, max_pairs, max_heights, max_occ):
+        self._check(self._L.fw_arena_init(self._h, int(max_nodes), int(max_elems), int(max_bodies),
+                                          int(max_scenes), int(max_pairs), int(max_heights), int(max_occ)),
+                    "fw_arena_init")
+
+    def arena_commit(self) -> int:
+        s = C.c_int32()
+        self._check(self._L.fw_arena_commit(self._h, C.byref(s)), "fw_arena_commit")
+        return int(s.value)
+
+    def arena_remove(self, scene: int):
+        self._check(self._L.fw_arena_remove(self._h, int(scene)), "fw_arena_remove")
+
+    def arena_scene_info(self, scene: int):
+        out = np.zeros(8, dtype=np.int64)
+        self._check(self._L.fw_arena_scene_info(self._h, int(scene), out.ctypes.data_as(_i64p)), "fw_arena_scene_info")
+        return out
+
     def get_path(self):
         p = C.c_int32()
         n = C.c_int32()
@@ -206,6 +230,11 @@ class NativeWorld:
     def step_scenes(self, n: int, dt_per_scene):
         d = _f(dt_per_scene)
         self._check(self._L.fw_step_scenes(self._h, int(n), d[1]), "fw_step_scenes")
+
+    def step_served(self, dt_per_scene):
+        """One substep; scenes with dt <= 0 stay frozen.  dt must be float32,
+        contiguous, one entry per scene (the library copies it before returning)."""
+        self._check(self._L.fw_step_served(self._h, dt_per_scene.ctypes.data_as(_f32p)), "fw_step_served")
 
     def set_active(self, active):
         a = _i(active)

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -45,7 +46,8 @@ struct Dev {
   float2* corner;
   uint32_t* node_word;
   float* mass;
-  int32_t* csr_off;
+  int32_t* csr_off;   // node i's corners are csr_slot[csr_off[i] .. csr_end[i])
+  int32_t* csr_end;
   int32_t* csr_slot;
   int32_t* conn;
   float4* jinv;
@@ -73,6 +75,11 @@ struct Dev {
   // the captured graph); otherwise scene_dt[] holds one dt per scene.
   int uniform_dt;
   float dt_uniform;
+  // chunked launch (arena worlds): only these element / node ranges are stepped
+  int use_chunks;
+  int n_e_chunks, n_n_chunks;
+  const int2* e_chunks;  // (first element, count <= element block size)
+  const int2* n_chunks;  // (first node, count <= node block size)
 };
 
 // ------------------------------------------------------------------ kernels
@@ -110,13 +117,11 @@ __device__ void step_control(const Dev& d) {
   }
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
-  if (blockIdx.x == 0) step_control(d);
-  const int stride = gridDim.x * blockDim.x;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) {
+__device__ __forceinline__ void element_step(const Dev& d, int e) {
+  {
     const ElemMat m = d.emat[e];
     const int s = d.body_scene[fw::elem_body(m.word)];
-    if (!d.scene_active[s]) continue;
+    if (!d.scene_active[s]) return;
     const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
     const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
     const float4 ji = d.jinv[e];
@@ -138,9 +143,20 @@ __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
   }
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < d.N;
+__global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
+  if (blockIdx.x == 0) step_control(d);
+  if (d.use_chunks) {
+    for (int c = blockIdx.x; c < d.n_e_chunks; c += gridDim.x) {
+      const int2 ch = d.e_chunks[c];
+      if ((int)threadIdx.x < ch.y) element_step(d, ch.x + threadIdx.x);
+    }
+    return;
+  }
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) element_step(d, e);
+}
+
+__device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
   const uint32_t w = valid ? d.node_word[i] : 0u;
   const int b = (int)(w >> fw::NODE_BODY_SHIFT);
   const int s = valid ? d.body_scene[b] : 0;
@@ -166,7 +182,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
         }
       }
     }
-    const int k0 = d.csr_off[i], k1 = d.csr_off[i + 1];
+    const int k0 = d.csr_off[i], k1 = d.csr_end[i];
     for (int k = k0; k < k1; ++k) {
       const float2 c = d.corner[d.csr_slot[k]];
       f.x += c.x;
@@ -211,14 +227,26 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
   }
 }
 
+__global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
+  if (d.use_chunks) {
+    for (int c = blockIdx.x; c < d.n_n_chunks; c += gridDim.x) {
+      const int2 ch = d.n_chunks[c];
+      node_step(d, ch.x + (int)threadIdx.x, (int)threadIdx.x < ch.y);
+    }
+    return;
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  node_step(d, i, i < d.N);
+}
+
 // Reference-shape precompute, _prepare_fem_data_kernel
 // (flatworld/femspringmanager.py:113-138), plus the Lame constants of
 // getStress2D (materialfunctions.py:12-13), which depend only on E and nu.
 __global__ void k_prepare_elements(Dev d, const float* __restrict__ young,
                                    const float* __restrict__ poisson,
-                                   const float* __restrict__ rho) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= d.E) return;
+                                   const float* __restrict__ rho, int e_lo, int e_hi) {
+  const int e = e_lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= e_hi) return;
   const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
   const float2 a = d.x0[c0], b = d.x0[c1], c = d.x0[c2];
   const float j00 = a.x - c.x, j01 = b.x - c.x, j10 = a.y - c.y, j11 = b.y - c.y;
@@ -230,22 +258,22 @@ __global__ void k_prepare_elements(Dev d, const float* __restrict__ young,
     ji = make_float4(j11 * r, -j01 * r, -j10 * r, j00 * r);
   }
   d.jinv[e] = ji;
-  const float E = young[e], nu = poisson[e];
+  const float E = young[e - e_lo], nu = poisson[e - e_lo];
   ElemMat m = d.emat[e];
   m.area = area;
   m.lam = E * nu / ((1.0f + nu) * (1.0f - 2.0f * nu));
   m.mu = E / (2.0f * (1.0f + nu));
   d.emat[e] = m;
-  d.ndmass[e] = area * rho[e] / 3.0f;
+  d.ndmass[e] = area * rho[e - e_lo] / 3.0f;
 }
 
 // Lumped mass: each node adds its elements' shares in ascending element order,
 // the order of the reference's serial atomic adds.
-__global__ void k_prepare_mass(Dev d) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.N) return;
+__global__ void k_prepare_mass(Dev d, int n_lo, int n_hi) {
+  const int i = n_lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_hi) return;
   float m = 0.0f;
-  for (int k = d.csr_off[i]; k < d.csr_off[i + 1]; ++k) m += d.ndmass[d.csr_slot[k] / 3];
+  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) m += d.ndmass[d.csr_slot[k] / 3];
   d.mass[i] = m;
 }
 
@@ -291,6 +319,48 @@ struct fw_ctx {
     bool valid = false;
   };
   std::vector<Snap> snaps;
+  // ---- arena (serving): fixed capacity, scenes inserted / removed at run time
+  struct FreeList {
+    std::map<int64_t, int64_t> free;  // start -> length, coalesced
+    void init(int64_t cap) { free.clear(); if (cap > 0) free[0] = cap; }
+    bool take(int64_t len, int64_t* off) {
+      if (len == 0) { *off = 0; return true; }
+      for (auto it = free.begin(); it != free.end(); ++it)
+        if (it->second >= len) {
+          *off = it->first;
+          const int64_t rest = it->second - len, start = it->first + len;
+          free.erase(it);
+          if (rest) free[start] = rest;
+          return true;
+        }
+      return false;
+    }
+    void give(int64_t off, int64_t len) {
+      if (len == 0) return;
+      auto it = free.emplace(off, len).first;
+      auto nx = std::next(it);
+      if (nx != free.end() && it->first + it->second == nx->first) { it->second += nx->second; free.erase(nx); }
+      if (it != free.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) { pv->second += it->second; free.erase(it); }
+      }
+    }
+    int64_t total() const { int64_t t = 0; for (auto& f : free) t += f.second; return t; }
+  };
+  struct ArenaScene {
+    bool live = false;
+    int64_t n0 = 0, nn = 0, e0 = 0, ne = 0, b0 = 0, nb = 0, p0 = 0, np = 0, h0 = 0, nh = 0, o0 = 0, no = 0;
+  };
+  bool arena = false;
+  FreeList fl_nodes, fl_elems, fl_bodies, fl_pairs, fl_heights, fl_occ;
+  std::vector<ArenaScene> ascenes;
+  std::vector<int> free_scene_ids;
+  std::vector<int32_t> a_body_scene;
+  bool chunks_dirty = true;
+  std::vector<int2> h_echunks, h_nchunks;
+  int2 *d_echunks = nullptr, *d_nchunks = nullptr;
+  int64_t chunk_cap = 0;
+  float *a_young = nullptr, *a_poisson = nullptr, *a_rho = nullptr;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
@@ -398,8 +468,11 @@ int get_graph(fw_ctx* c, cudaGraphExec_t* out) {
 
 int launch_resident(fw_ctx* c, int n);
 
+int rebuild_chunks(fw_ctx* c);
+
 int run_steps(fw_ctx* c, int n) {
   int rc = FW_OK;
+  if (c->arena && (rc = rebuild_chunks(c))) return rc;
   if (c->path == FW_PATH_RESIDENT && c->d.uniform_dt) return launch_resident(c, n);
   c->host_counter += n;
   if (n >= kGraphSteps) {
@@ -630,6 +703,38 @@ int check_device_error(fw_ctx* c) {
   return FW_OK;
 }
 
+
+int rebuild_chunks(fw_ctx* c) {
+  if (!c->chunks_dirty) return FW_OK;
+  c->h_echunks.clear();
+  c->h_nchunks.clear();
+  for (size_t s = 0; s < c->ascenes.size(); ++s) {
+    const fw_ctx::ArenaScene& a = c->ascenes[s];
+    if (!a.live || !c->cur_active[s]) continue;
+    for (int64_t k = 0; k < a.ne; k += c->block_e)
+      c->h_echunks.push_back(make_int2((int)(a.e0 + k), (int)std::min<int64_t>(c->block_e, a.ne - k)));
+    for (int64_t k = 0; k < a.nn; k += c->block_n)
+      c->h_nchunks.push_back(make_int2((int)(a.n0 + k), (int)std::min<int64_t>(c->block_n, a.nn - k)));
+  }
+  if ((int64_t)std::max(c->h_echunks.size(), c->h_nchunks.size()) > c->chunk_cap)
+    return fail(c, FW_ERR_ARG, "arena: chunk list overflow");
+  if (!c->h_echunks.empty())
+    FW_CUDA(c, cudaMemcpyAsync(c->d_echunks, c->h_echunks.data(), sizeof(int2) * c->h_echunks.size(),
+                               cudaMemcpyHostToDevice, c->stream));
+  if (!c->h_nchunks.empty())
+    FW_CUDA(c, cudaMemcpyAsync(c->d_nchunks, c->h_nchunks.data(), sizeof(int2) * c->h_nchunks.size(),
+                               cudaMemcpyHostToDevice, c->stream));
+  // pageable-source copies are staged before cudaMemcpyAsync returns, so the
+  // host vectors may change again right away
+  c->d.n_e_chunks = (int)c->h_echunks.size();
+  c->d.n_n_chunks = (int)c->h_nchunks.size();
+  c->grid_e = std::max(1, std::min(c->d.n_e_chunks, c->sms * 8));
+  c->grid_n = std::max(1, std::min(c->d.n_n_chunks, c->sms * 8));
+  drop_graphs(c);
+  c->chunks_dirty = false;
+  return FW_OK;
+}
+
 int set_scene_dt(fw_ctx* c, const float* dt) {
   bool same = c->cur_dt.size() == (size_t)c->S;
   for (int s = 0; same && s < c->S; ++s) same = memcmp(&c->cur_dt[s], &dt[s], sizeof(float)) == 0;
@@ -687,9 +792,9 @@ int fw_set_stream(fw_ctx* c, void* stream) {
 int fw_set_nodes(fw_ctx* c, int32_t n, const float* coords, const float* vel,
                  const int32_t* bc_bits, const float* bc_values) {
   if (!c) return FW_ERR_ARG;
-  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_nodes after fw_finalize");
+  if (c->finalized && !c->arena) return fail(c, FW_ERR_STATE, "fw_set_nodes after fw_finalize");
   if (n <= 0 || !coords) return fail(c, FW_ERR_ARG, "fw_set_nodes: need n_nodes > 0 and coords");
-  c->N = n;
+  if (!c->arena) c->N = n;
   c->h_x.assign(coords, coords + 2 * (size_t)n);
   c->h_v.assign(2 * (size_t)n, 0.f);
   if (vel) c->h_v.assign(vel, vel + 2 * (size_t)n);
@@ -706,10 +811,10 @@ int fw_set_elements(fw_ctx* c, int32_t n, const int32_t* conn, const int32_t* ma
                     const float* young, const float* poisson, const float* density,
                     const float* yield_stress, const float* hardening) {
   if (!c) return FW_ERR_ARG;
-  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_elements after fw_finalize");
+  if (c->finalized && !c->arena) return fail(c, FW_ERR_STATE, "fw_set_elements after fw_finalize");
   if (n <= 0 || !conn || !mat_type || !young || !poisson || !density)
     return fail(c, FW_ERR_ARG, "fw_set_elements: need n_elems > 0 and conn/type/E/nu/rho");
-  c->E = n;
+  if (!c->arena) c->E = n;
   c->h_conn.assign(conn, conn + 3 * (size_t)n);
   c->h_type.assign(mat_type, mat_type + n);
   c->h_E.assign(young, young + n);
@@ -732,11 +837,11 @@ int fw_set_bodies(fw_ctx* c, int32_t nb, const int32_t* noff, const int32_t* ncn
                   const int32_t* bnoff, const int32_t* bncnt, int32_t n_bnodes,
                   const int32_t* bnodes) {
   if (!c) return FW_ERR_ARG;
-  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_bodies after fw_finalize");
+  if (c->finalized && !c->arena) return fail(c, FW_ERR_STATE, "fw_set_bodies after fw_finalize");
   if (nb <= 0 || !noff || !ncnt || !eoff || !ecnt || !scene || !bnoff || !bncnt)
     return fail(c, FW_ERR_ARG, "fw_set_bodies: need n_bodies > 0 and all range arrays");
   if (nb >= (1 << 22)) return fail(c, FW_ERR_ARG, "fw_set_bodies: at most 4194303 bodies");
-  c->B = nb;
+  if (!c->arena) c->B = nb;
   c->h_noff.assign(noff, noff + nb);
   c->h_ncnt.assign(ncnt, ncnt + nb);
   c->h_eoff.assign(eoff, eoff + nb);
@@ -750,9 +855,10 @@ int fw_set_bodies(fw_ctx* c, int32_t nb, const int32_t* noff, const int32_t* ncn
 
 int fw_set_scenes(fw_ctx* c, int32_t ns, const float* damping) {
   if (!c) return FW_ERR_ARG;
-  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_scenes after fw_finalize");
+  if (c->finalized && !c->arena) return fail(c, FW_ERR_STATE, "fw_set_scenes after fw_finalize");
   if (ns <= 0) return fail(c, FW_ERR_ARG, "fw_set_scenes: need n_scenes > 0");
-  c->S = ns;
+  if (c->arena && ns != 1) return fail(c, FW_ERR_ARG, "arena: stage one scene at a time");
+  if (!c->arena) c->S = ns;
   c->h_damp.assign(ns, 0.f);
   if (damping) c->h_damp.assign(damping, damping + ns);
   return FW_OK;
@@ -760,7 +866,7 @@ int fw_set_scenes(fw_ctx* c, int32_t ns, const float* damping) {
 
 static int add_pair(fw_ctx* c, Pair p, const float* lo, const float* hi) {
   if (!c) return FW_ERR_ARG;
-  if (c->finalized) return fail(c, FW_ERR_STATE, "contact pair added after fw_finalize");
+  if (c->finalized && !c->arena) return fail(c, FW_ERR_STATE, "contact pair added after fw_finalize");
   if (!lo || !hi) return fail(c, FW_ERR_ARG, "contact pair: gate box required");
   if (p.body < 0) return fail(c, FW_ERR_ARG, "contact pair: bad body %d", p.body);
   p.glo[0] = lo[0];
@@ -940,8 +1046,9 @@ int fw_finalize(fw_ctx* c) {
   float *dE = nullptr, *dnu = nullptr, *drho = nullptr;
   if ((rc = upload(c, &dE, c->h_E)) || (rc = upload(c, &dnu, c->h_nu)) || (rc = upload(c, &drho, c->h_rho)))
     return rc;
-  k_prepare_elements<<<(E + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d, dE, dnu, drho);
-  k_prepare_mass<<<(N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d);
+  d.csr_end = d.csr_off + 1;
+  k_prepare_elements<<<(E + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d, dE, dnu, drho, 0, E);
+  k_prepare_mass<<<(N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d, 0, N);
   c->launches += 2;
   if ((rc = check_kernel(c, "prepare"))) return rc;
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -1049,6 +1156,278 @@ int fw_restore(fw_ctx* c, int32_t slot) {
   return FW_OK;
 }
 
+
+int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_bodies, int32_t max_scenes,
+                  int32_t max_pairs, int64_t max_heights, int64_t max_occ) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_arena_init on a finalized context");
+  if (max_nodes <= 0 || max_elems <= 0 || max_bodies <= 0 || max_scenes <= 0 || max_pairs < 0 ||
+      max_heights < 0 || max_occ < 0)
+    return fail(c, FW_ERR_ARG, "fw_arena_init: capacities must be positive");
+  if (max_nodes >= (1ll << 31) / 2 || 3 * max_elems >= (1ll << 31) || max_bodies >= (1 << 22))
+    return fail(c, FW_ERR_ARG, "fw_arena_init: capacity beyond 32-bit indexing");
+  FW_CUDA(c, cudaSetDevice(c->device));
+  const int64_t N = max_nodes, E = max_elems;
+  const int B = max_bodies, S = max_scenes + 1;  // scene S-1: the dead scene of free bodies
+  Dev& d = c->d;
+  d = Dev{};
+  d.N = (int)N; d.E = (int)E; d.B = B; d.S = S; d.P = max_pairs; d.has_j2 = 1;
+  int rc;
+  if ((rc = dalloc(c, &d.x0, N)) || (rc = dalloc(c, &d.x, N)) || (rc = dalloc(c, &d.v, N)) ||
+      (rc = dalloc(c, &d.bcv, N)) || (rc = dalloc(c, &d.node_word, N)) || (rc = dalloc(c, &d.mass, N)) ||
+      (rc = dalloc(c, &d.csr_off, N)) || (rc = dalloc(c, &d.csr_end, N)) || (rc = dalloc(c, &d.csr_slot, 3 * E)) ||
+      (rc = dalloc(c, &d.conn, 3 * E)) || (rc = dalloc(c, &d.jinv, E)) || (rc = dalloc(c, &d.emat, E)) ||
+      (rc = dalloc(c, &d.j2par, E)) || (rc = dalloc(c, &d.j2state, E)) || (rc = dalloc(c, &d.ndmass, E)) ||
+      (rc = dalloc(c, &d.corner, 3 * E)) || (rc = dalloc(c, &d.body_scene, B)) ||
+      (rc = dalloc(c, &d.body_pair_off, B)) || (rc = dalloc(c, &d.body_pair_cnt, B)) ||
+      (rc = dalloc(c, &d.pairs, max_pairs)) || (rc = dalloc(c, &d.pair_active, max_pairs)) ||
+      (rc = dalloc(c, &d.heights, max_heights)) || (rc = dalloc(c, &d.occ, max_occ)) ||
+      (rc = dalloc(c, &d.scene_dt, S)) || (rc = dalloc(c, &d.scene_damp, S)) ||
+      (rc = dalloc(c, &d.scene_counter, S)) || (rc = dalloc(c, &d.scene_active, S)) ||
+      (rc = dalloc(c, &d.scene_mode_req, S)) || (rc = dalloc(c, &d.scene_mode, S)) ||
+      (rc = dalloc(c, &d.aabb_ring, 8 * (size_t)B)) || (rc = dalloc(c, &c->a_young, E)) ||
+      (rc = dalloc(c, &c->a_poisson, E)) || (rc = dalloc(c, &c->a_rho, E)))
+    return rc;
+  c->chunk_cap = E / 32 + N / 32 + 2 * (int64_t)S + 16;
+  if ((rc = dalloc(c, &c->d_echunks, c->chunk_cap)) || (rc = dalloc(c, &c->d_nchunks, c->chunk_cap))) return rc;
+  std::vector<int32_t> dead(B, S - 1);
+  FW_CUDA(c, cudaMemcpyAsync(d.body_scene, dead.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.body_pair_cnt, 0, sizeof(int32_t) * B, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.body_pair_off, 0, sizeof(int32_t) * B, c->stream));
+  if (max_pairs) FW_CUDA(c, cudaMemsetAsync(d.pairs, 0, sizeof(Pair) * max_pairs, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_active, 0, sizeof(int32_t) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_mode_req, 0, sizeof(int32_t) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_counter, 0, sizeof(int32_t) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_dt, 0, sizeof(float) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.scene_damp, 0, sizeof(float) * S, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.aabb_ring, 0, sizeof(int32_t) * 8 * (size_t)B, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(d.j2state, 0, sizeof(float4) * E, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  d.use_chunks = 1;
+  d.e_chunks = c->d_echunks;
+  d.n_chunks = c->d_nchunks;
+  c->fl_nodes.init(N);
+  c->fl_elems.init(E);
+  c->fl_bodies.init(B);
+  c->fl_pairs.init(max_pairs);
+  c->fl_heights.init(max_heights);
+  c->fl_occ.init(max_occ);
+  c->ascenes.assign(S, fw_ctx::ArenaScene{});
+  c->a_body_scene.assign(B, S - 1);
+  c->free_scene_ids.clear();
+  for (int s2 = S - 2; s2 >= 0; --s2) c->free_scene_ids.push_back(s2);
+  c->cur_active.assign(S, 0);
+  c->N = (int)N; c->E = (int)E; c->B = B; c->S = S;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+  c->arena = true;
+  c->finalized = true;
+  c->path = FW_PATH_GATHER;
+  c->chunks_dirty = true;
+  c->h_x.clear(); c->h_conn.clear(); c->h_pairs.clear(); c->h_heights.clear(); c->h_occ.clear();
+  return FW_OK;
+}
+
+int fw_arena_commit(fw_ctx* c, int32_t* scene_out) {
+  if (!c || !scene_out) return FW_ERR_ARG;
+  if (!c->arena) return fail(c, FW_ERR_STATE, "fw_arena_commit without fw_arena_init");
+  // staged by fw_set_nodes / fw_set_elements / fw_set_bodies / fw_add_*_pair (local ids)
+  const int64_t Ns = (int64_t)c->h_x.size() / 2, Es = (int64_t)c->h_conn.size() / 3;
+  const int Bs = (int)c->h_noff.size();
+  if (Ns <= 0 || Es <= 0 || Bs <= 0) return fail(c, FW_ERR_ARG, "fw_arena_commit: nothing staged");
+  for (int b = 0; b < Bs; ++b)
+    if (c->h_scene[b] != 0) return fail(c, FW_ERR_ARG, "fw_arena_commit: stage exactly one scene (scene 0)");
+  // validate local ranges
+  std::vector<int32_t> node_body(Ns, -1), elem_body(Es, -1);
+  for (int b = 0; b < Bs; ++b) {
+    if (c->h_noff[b] < 0 || c->h_noff[b] + (int64_t)c->h_ncnt[b] > Ns || c->h_eoff[b] < 0 ||
+        c->h_eoff[b] + (int64_t)c->h_ecnt[b] > Es)
+      return fail(c, FW_ERR_ARG, "fw_arena_commit: body %d range out of bounds", b);
+    for (int i = c->h_noff[b]; i < c->h_noff[b] + c->h_ncnt[b]; ++i) node_body[i] = b;
+    for (int e = c->h_eoff[b]; e < c->h_eoff[b] + c->h_ecnt[b]; ++e) elem_body[e] = b;
+  }
+  for (int64_t e = 0; e < Es; ++e)
+    for (int k = 0; k < 3; ++k) {
+      const int n = c->h_conn[3 * e + k];
+      if (elem_body[e] < 0 || n < 0 || n >= Ns || node_body[n] != elem_body[e])
+        return fail(c, FW_ERR_ARG, "fw_arena_commit: element %lld has a bad node id", (long long)e);
+    }
+  for (int64_t i = 0; i < Ns; ++i)
+    if (node_body[i] < 0) return fail(c, FW_ERR_ARG, "fw_arena_commit: node %lld belongs to no body", (long long)i);
+  // ranges
+  if (c->free_scene_ids.empty()) return fail(c, FW_ERR_OOM, "arena: no free scene slot");
+  fw_ctx::ArenaScene a;
+  a.nn = Ns; a.ne = Es; a.nb = Bs; a.np = (int64_t)c->h_pairs.size();
+  a.nh = (int64_t)c->h_heights.size(); a.no = (int64_t)c->h_occ.size();
+  fw_ctx::FreeList* lists[6] = {&c->fl_nodes, &c->fl_elems, &c->fl_bodies, &c->fl_pairs, &c->fl_heights, &c->fl_occ};
+  int64_t* offs[6] = {&a.n0, &a.e0, &a.b0, &a.p0, &a.h0, &a.o0};
+  const int64_t lens[6] = {a.nn, a.ne, a.nb, a.np, a.nh, a.no};
+  for (int k = 0; k < 6; ++k)
+    if (!lists[k]->take(lens[k], offs[k])) {
+      for (int j = 0; j < k; ++j) lists[j]->give(*offs[j], lens[j]);
+      return fail(c, FW_ERR_OOM, "arena: not enough free capacity for this scene");
+    }
+  const int s = c->free_scene_ids.back();
+  c->free_scene_ids.pop_back();
+  a.live = true;
+  // pack with global ids
+  std::vector<uint32_t> word(Ns);
+  std::vector<float2> x0(Ns), v0(Ns), bcv(Ns);
+  for (int64_t i = 0; i < Ns; ++i) {
+    word[i] = (uint32_t)c->h_bc[i] | ((uint32_t)(a.b0 + node_body[i]) << fw::NODE_BODY_SHIFT);
+    x0[i] = make_float2(c->h_x[2 * i], c->h_x[2 * i + 1]);
+    v0[i] = make_float2(c->h_v[2 * i], c->h_v[2 * i + 1]);
+    bcv[i] = make_float2(c->h_bcv[2 * i], c->h_bcv[2 * i + 1]);
+  }
+  for (int b = 0; b < Bs; ++b)
+    for (int k = 0; k < c->h_bncnt[b]; ++k) word[c->h_bnodes[c->h_bnoff[b] + k]] |= fw::NODE_BOUNDARY;
+  std::vector<int32_t> conn(3 * Es), cbeg(Ns), cend(Ns), slot(3 * Es);
+  std::vector<ElemMat> emat(Es);
+  std::vector<float2> j2par(Es);
+  for (int64_t e = 0; e < Es; ++e) {
+    for (int k = 0; k < 3; ++k) conn[3 * e + k] = (int32_t)(a.n0 + c->h_conn[3 * e + k]);
+    emat[e].area = emat[e].lam = emat[e].mu = 0.f;
+    emat[e].word = (c->h_type[e] & 3) | ((int)(a.b0 + elem_body[e]) << 2);
+    j2par[e] = make_float2(c->h_sy[e], c->h_H[e]);
+  }
+  {
+    std::vector<int32_t> cnt(Ns + 1, 0);
+    for (int64_t e = 0; e < Es; ++e)
+      for (int k = 0; k < 3; ++k) cnt[c->h_conn[3 * e + k] + 1]++;
+    for (int64_t i = 0; i < Ns; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+    for (int64_t e = 0; e < Es; ++e)
+      for (int k = 0; k < 3; ++k) slot[fill[c->h_conn[3 * e + k]]++] = (int32_t)(3 * (a.e0 + e) + k);
+    for (int64_t i = 0; i < Ns; ++i) {
+      cbeg[i] = (int32_t)(3 * a.e0 + cnt[i]);
+      cend[i] = (int32_t)(3 * a.e0 + cnt[i + 1]);
+    }
+  }
+  std::vector<Pair> pairs = c->h_pairs;
+  std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x.body < y.body; });
+  std::vector<int32_t> poff(Bs, 0), pcnt(Bs, 0), bscene(Bs, s);
+  for (size_t k = 0; k < pairs.size(); ++k) {
+    if (pairs[k].body < 0 || pairs[k].body >= Bs) return fail(c, FW_ERR_ARG, "fw_arena_commit: pair body out of range");
+    pcnt[pairs[k].body]++;
+  }
+  for (int b = 1; b < Bs; ++b) poff[b] = poff[b - 1] + pcnt[b - 1];
+  for (int b = 0; b < Bs; ++b) poff[b] += (int32_t)a.p0;
+  for (Pair& pr : pairs) {
+    pr.body += (int)a.b0;
+    if (pr.kind == fw::PAIR_HEIGHTFIELD) pr.table += (int)a.h0;
+    if (pr.kind == fw::PAIR_VOXEL) pr.table += (int)a.o0;
+  }
+  // upload
+  Dev& d = c->d;
+  auto up = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (!bytes) return FW_OK;
+    FW_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return FW_OK;
+  };
+  int rc;
+  if ((rc = up(d.x0 + a.n0, x0.data(), sizeof(float2) * Ns)) || (rc = up(d.x + a.n0, x0.data(), sizeof(float2) * Ns)) ||
+      (rc = up(d.v + a.n0, v0.data(), sizeof(float2) * Ns)) || (rc = up(d.bcv + a.n0, bcv.data(), sizeof(float2) * Ns)) ||
+      (rc = up(d.node_word + a.n0, word.data(), sizeof(uint32_t) * Ns)) ||
+      (rc = up(d.csr_off + a.n0, cbeg.data(), sizeof(int32_t) * Ns)) ||
+      (rc = up(d.csr_end + a.n0, cend.data(), sizeof(int32_t) * Ns)) ||
+      (rc = up(d.csr_slot + 3 * a.e0, slot.data(), sizeof(int32_t) * 3 * Es)) ||
+      (rc = up(d.conn + 3 * a.e0, conn.data(), sizeof(int32_t) * 3 * Es)) ||
+      (rc = up(d.emat + a.e0, emat.data(), sizeof(ElemMat) * Es)) ||
+      (rc = up(d.j2par + a.e0, j2par.data(), sizeof(float2) * Es)) ||
+      (rc = up(c->a_young + a.e0, c->h_E.data(), sizeof(float) * Es)) ||
+      (rc = up(c->a_poisson + a.e0, c->h_nu.data(), sizeof(float) * Es)) ||
+      (rc = up(c->a_rho + a.e0, c->h_rho.data(), sizeof(float) * Es)) ||
+      (rc = up(d.body_scene + a.b0, bscene.data(), sizeof(int32_t) * Bs)) ||
+      (rc = up(d.body_pair_off + a.b0, poff.data(), sizeof(int32_t) * Bs)) ||
+      (rc = up(d.body_pair_cnt + a.b0, pcnt.data(), sizeof(int32_t) * Bs)) ||
+      (rc = up(d.pairs + a.p0, pairs.data(), sizeof(Pair) * pairs.size())) ||
+      (rc = up(d.heights + a.h0, c->h_heights.data(), sizeof(float) * a.nh)) ||
+      (rc = up(d.occ + a.o0, c->h_occ.data(), a.no)))
+    return rc;
+  FW_CUDA(c, cudaMemsetAsync(d.j2state + a.e0, 0, sizeof(float4) * Es, c->stream));
+  const float damp = c->h_damp.empty() ? 0.f : c->h_damp[0];
+  const int32_t one = 1, zero = 0;
+  if ((rc = up(d.scene_damp + s, &damp, sizeof(float))) || (rc = up(d.scene_counter + s, &zero, sizeof(int32_t))) ||
+      (rc = up(d.scene_mode_req + s, &one, sizeof(int32_t))) || (rc = up(d.scene_active + s, &one, sizeof(int32_t))))
+    return rc;
+  const int e_lo = (int)a.e0, e_hi = (int)(a.e0 + Es), n_lo = (int)a.n0, n_hi = (int)(a.n0 + Ns);
+  k_prepare_elements<<<(int)((Es + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->a_young + a.e0, c->a_poisson + a.e0,
+                                                                                c->a_rho + a.e0, e_lo, e_hi);
+  k_prepare_mass<<<(int)((Ns + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, n_lo, n_hi);
+  c->launches += 2;
+  if ((rc = check_kernel(c, "arena prepare"))) return rc;
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->ascenes[s] = a;
+  for (int b = 0; b < Bs; ++b) c->a_body_scene[a.b0 + b] = s;
+  c->cur_active[s] = 1;
+  c->chunks_dirty = true;
+  // clear the stage for the next scene
+  c->h_x.clear(); c->h_v.clear(); c->h_bc.clear(); c->h_bcv.clear();
+  c->h_conn.clear(); c->h_type.clear(); c->h_E.clear(); c->h_nu.clear(); c->h_rho.clear(); c->h_sy.clear(); c->h_H.clear();
+  c->h_noff.clear(); c->h_ncnt.clear(); c->h_eoff.clear(); c->h_ecnt.clear(); c->h_scene.clear();
+  c->h_bnoff.clear(); c->h_bncnt.clear(); c->h_bnodes.clear(); c->h_pairs.clear(); c->h_heights.clear(); c->h_occ.clear();
+  *scene_out = s;
+  return FW_OK;
+}
+
+int fw_arena_remove(fw_ctx* c, int32_t s) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->arena) return fail(c, FW_ERR_STATE, "fw_arena_remove without fw_arena_init");
+  if (s < 0 || s >= c->S - 1 || !c->ascenes[s].live) return fail(c, FW_ERR_ARG, "fw_arena_remove: scene %d is not live", s);
+  fw_ctx::ArenaScene& a = c->ascenes[s];
+  std::vector<int32_t> dead(a.nb, c->S - 1);
+  const int32_t zero = 0;
+  FW_CUDA(c, cudaMemcpyAsync(c->d.body_scene + a.b0, dead.data(), sizeof(int32_t) * a.nb, cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_active + s, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int64_t b = 0; b < a.nb; ++b) c->a_body_scene[a.b0 + b] = c->S - 1;
+  c->fl_nodes.give(a.n0, a.nn);
+  c->fl_elems.give(a.e0, a.ne);
+  c->fl_bodies.give(a.b0, a.nb);
+  c->fl_pairs.give(a.p0, a.np);
+  c->fl_heights.give(a.h0, a.nh);
+  c->fl_occ.give(a.o0, a.no);
+  a = fw_ctx::ArenaScene{};
+  c->cur_active[s] = 0;
+  c->free_scene_ids.push_back(s);
+  c->chunks_dirty = true;
+  return FW_OK;
+}
+
+int fw_step_served(fw_ctx* c, const float* dt) {
+  if (!c || !dt) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_step_served before fw_finalize / fw_arena_init");
+  bool changed = false;
+  for (int s = 0; s < c->S; ++s) {
+    const int want = (dt[s] > 0.0f && (!c->arena || c->ascenes[s].live)) ? 1 : 0;
+    if (want != c->cur_active[s]) {
+      c->cur_active[s] = want;
+      changed = true;
+    }
+  }
+  if (changed) {
+    FW_CUDA(c, cudaMemcpyAsync(c->d.scene_active, c->cur_active.data(), sizeof(int32_t) * c->S,
+                               cudaMemcpyHostToDevice, c->stream));
+    c->chunks_dirty = true;
+  }
+  c->cur_dt.assign(dt, dt + c->S);
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_dt, c->cur_dt.data(), sizeof(float) * c->S, cudaMemcpyHostToDevice,
+                             c->stream));
+  c->d.uniform_dt = 0;
+  int rc;
+  if (c->arena && (rc = rebuild_chunks(c))) return rc;
+  return launch_step(c);
+}
+
+int fw_arena_scene_info(fw_ctx* c, int32_t s, int64_t* info) {
+  if (!c || !info) return FW_ERR_ARG;
+  if (!c->arena) return fail(c, FW_ERR_STATE, "fw_arena_scene_info without fw_arena_init");
+  if (s < 0 || s >= c->S - 1 || !c->ascenes[s].live) return fail(c, FW_ERR_ARG, "scene %d is not live", s);
+  const fw_ctx::ArenaScene& a = c->ascenes[s];
+  info[0] = a.n0; info[1] = a.nn; info[2] = a.e0; info[3] = a.ne; info[4] = a.b0; info[5] = a.nb;
+  info[6] = c->fl_nodes.total(); info[7] = c->fl_elems.total();
+  return FW_OK;
+}
+
 int fw_get_path(const fw_ctx* c, int32_t* path, int32_t* patches) {
   if (!c || !path) return FW_ERR_ARG;
   *path = c->finalized ? c->path : FW_PATH_AUTO;
@@ -1079,9 +1458,13 @@ int fw_set_active(fw_ctx* c, const int32_t* active) {
   if (!c || !active) return FW_ERR_ARG;
   if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_set_active before fw_finalize");
   c->cur_active.assign(active, active + c->S);
+  if (c->arena)  // a scene that is not live stays inactive
+    for (int s = 0; s < c->S; ++s)
+      if (!c->ascenes[s].live) c->cur_active[s] = 0;
   FW_CUDA(c, cudaMemcpyAsync(c->d.scene_active, c->cur_active.data(), sizeof(int32_t) * c->S,
                              cudaMemcpyHostToDevice, c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->chunks_dirty = true;
   return FW_OK;
 }
 
@@ -1136,7 +1519,8 @@ int fw_read_aabb(fw_ctx* c, float* dst) {
   FW_CUDA(c, cudaMemcpyAsync(cnt.data(), c->d.scene_counter, sizeof(int32_t) * c->S, cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   for (int b = 0; b < c->B; ++b) {
-    const int slot = cnt[c->h_scene[b]] & 1;
+    const int sc = c->arena ? c->a_body_scene[b] : c->h_scene[b];
+    const int slot = cnt[sc] & 1;
     for (int k = 0; k < 4; ++k) {
       int v = ring[((size_t)slot * c->B + b) * 4 + k];
       v = v >= 0 ? v : v ^ 0x7FFFFFFF;

@@ -247,6 +247,14 @@ def build_native(packed: PackedWorld, device: int = 0, path: str = "auto", patch
     nw.set_path(_native.PATHS[path], patches)
     if front_warps:
         nw.set_option(_native.FW_OPT_FRONT_WARPS, front_warps)
+    stage(nw, packed)
+    nw.finalize()
+    return nw
+
+
+def stage(nw: _native.NativeWorld, packed: PackedWorld):
+    """Hand a packed world's arrays to the native context (fw_set_* and
+    fw_add_*_pair); an arena then commits them as one scene."""
     nw.set_nodes(packed.coords, packed.vel, packed.bc_bits, packed.bc_vals)
     nw.set_elements(packed.conn, packed.mtype, packed.Ev, packed.nuv, packed.rhov, packed.syv, packed.Hv)
     nw.set_bodies(packed.noff, packed.ncnt, packed.eoff, packed.ecnt, packed.bscene, packed.bnoff,
@@ -259,8 +267,6 @@ def build_native(packed: PackedWorld, device: int = 0, path: str = "auto", patch
             nw.add_heightfield(body, pen, lo, hi, g.height, g.lb[0], g.ub[0], 1 if g.reverse else 0)
         else:
             nw.add_voxel(body, pen, lo, hi, np.asarray(g.occ, np.int32), g.lb[0], g.lb[1], g.dx, g.dz)
-    nw.finalize()
-    return nw
 
 
 def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):

@@ -172,6 +172,13 @@ int fw_step(fw_ctx* ctx, int32_t n_steps, float dt);
  * batched and served forms, where each scene has its own step. */
 int fw_step_scenes(fw_ctx* ctx, int32_t n_steps, const float* dt_per_scene);
 
+/* One substep for a served world: scene s advances by dt[s] if dt[s] > 0 and
+ * is frozen otherwise (dt has one entry per scene; for an arena world
+ * max_scenes + 1).  Never waits for the device: the active set and the step
+ * sizes are copied from staged host memory.  Replaces the per-body
+ * ExplicitLoop.advance calls of a request loop (explicitloop.py:473-555). */
+int fw_step_served(fw_ctx* ctx, const float* dt);
+
 /* Mark scenes active (1) / frozen (0).  Frozen scenes keep their state and do
  * not advance. */
 int fw_set_active(fw_ctx* ctx, const int32_t* active);
@@ -240,6 +247,25 @@ int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps, float dt,
                     const float* elem_mat, float* j2_state, const float* j2_param,
                     const int32_t* csr_off, const int32_t* csr_slot, void* stream, char* err,
                     int32_t err_len);
+
+/* Arena (served form).  fw_arena_init replaces the fw_set_* / fw_finalize
+ * flow: it reserves device capacity once (nodes, triangles, bodies, scenes,
+ * contact pairs, height samples, voxel cells).  Then, any number of times:
+ * stage ONE scene with fw_set_nodes / fw_set_elements / fw_set_bodies
+ * (scene 0) / fw_set_scenes(1, ...) / fw_add_*_pair using ids local to that
+ * scene, and fw_arena_commit copies it into free ranges, precomputes its
+ * reference shape and schedules its zero-dt construction step for the next
+ * substep; fw_arena_remove frees a scene's ranges.  Steps touch only the
+ * active scenes' ranges.  fw_step_scenes then takes max_scenes + 1 dt values.
+ * fw_arena_scene_info fills info[8] = {first node, nodes, first triangle,
+ * triangles, first body, bodies, free node capacity, free triangle capacity}.
+ * No reference counterpart: each reference ExplicitLoop is built once
+ * (flatworld/explicitloop.py:72-398). */
+int fw_arena_init(fw_ctx* ctx, int64_t max_nodes, int64_t max_elems, int32_t max_bodies,
+                  int32_t max_scenes, int32_t max_pairs, int64_t max_heights, int64_t max_occ);
+int fw_arena_commit(fw_ctx* ctx, int32_t* scene_out);
+int fw_arena_remove(fw_ctx* ctx, int32_t scene);
+int fw_arena_scene_info(fw_ctx* ctx, int32_t scene, int64_t* info);
 
 /* Library build identification string (arch, flags). */
 const char* fw_build_info(void);
