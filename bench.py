@@ -42,7 +42,10 @@ def parse():
     ap.add_argument("--mesh", type=int, default=256, help="quads per side of the large mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--workload", choices=["plain_large", "batched"], default="plain_large")
+    ap.add_argument("--workload", choices=["plain_large", "batched", "served"], default="plain_large")
+    ap.add_argument("--rate", type=float, default=2000.0, help="served: requests per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="served: seconds of arrivals")
+    ap.add_argument("--fifo-seconds", type=float, default=5.0, help="served: wall-time cap of the FIFO server")
     ap.add_argument("--scenes", type=int, default=2048, help="batched: number of bodies")
     ap.add_argument("--plain-sample", type=int, default=64, help="batched: bodies timed alone")
     return ap.parse_args()
@@ -287,6 +290,60 @@ def run_batched(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_served(args, rank, world, local):
+    """Request stream: Poisson arrivals at --rate per second for --duration s;
+    each request advances one body (drawn as in the ragged batch, a population
+    of --scenes bodies) by advanceWithTime(1/60) in U{50..400} substeps.  Bodies
+    stay resident between their requests; admission by free HBM (150 GB
+    budget).  Compared with a FIFO server that runs requests one at a time on
+    the plain path (one ExplicitLoop per body) on the same stream."""
+    import torch
+
+    import flatworld_b200 as fw
+    from flatworld_b200.serve import FifoPlainServer, Server, poisson_requests
+    from tests import scenes
+
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    population = scenes.ragged_batch(fw, args.scenes, seed=rank)  # request payloads, built client-side
+    build_s = time.perf_counter() - t0
+    reqs = poisson_requests(args.rate, args.duration, args.scenes, seed=17 + rank)
+    srv = Server(lambda b: population[b], budget_bytes=150e9, device=local)
+    # warm-up: compile paths and touch the allocator with a few bodies
+    warm = poisson_requests(200.0, 0.05, 8, seed=5)
+    Server(lambda b: scenes.ragged_batch_one(fw, 10_000 + b), arena_nodes=200_000, arena_elems=400_000,
+           arena_bodies=64, arena_scenes=64, device=local).run(warm, realtime=False)
+    with ClockSampler(local) as clk:
+        out = srv.run(reqs, realtime=True)
+    lat = out["latency_s"] * 1e3
+    fifo = FifoPlainServer(lambda b: population[b], device=local)
+    fo = fifo.run(reqs, realtime=True, time_limit=args.fifo_seconds)
+    flat = fo["latency_s"] * 1e3
+    line = {
+        "metric": "FEM element-steps/s (served, continuous batching)",
+        "value": out["element_steps"] / out["wall_s"], "unit": "element-steps/s", "n_gpus": world,
+        "steps": len(reqs), "warmup": len(warm), "ms_per_step": float(np.mean(lat)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded bodies, Poisson arrivals)",
+        "config": {"workload": f"served: {args.rate:.0f} req/s Poisson for {args.duration:.0f} s, "
+                               f"{args.scenes} resident bodies, advanceWithTime(1/60) in U{{50..400}} substeps",
+                   "requests": len(reqs), "population_build_s": build_s, "budget_bytes": 150e9,
+                   "resident_bodies": out["resident_bodies"], "resident_bytes": out["used_bytes"],
+                   "deferred_admissions": out["deferred_admissions"], "substeps_run": out["substeps"]},
+        "served": {"sims_per_s": len(reqs) / out["wall_s"], "wall_s": out["wall_s"],
+                   "latency_ms": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99),
+                                  "p99.9": percentile_ms(lat, 99.9)}},
+        "fifo_plain": {"served": fo["served"], "wall_s": fo["wall_s"],
+                       "sims_per_s": fo["served"] / fo["wall_s"],
+                       "element_steps_per_s": fo["element_steps"] / fo["wall_s"],
+                       "latency_ms": {"p50": percentile_ms(flat, 50) if len(flat) else None,
+                                      "p99": percentile_ms(flat, 99) if len(flat) else None}},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -295,6 +352,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args, rank, world, local)
+        return
+    if args.workload == "served":
+        run_served(args, rank, world, local)
         return
     import torch
 

@@ -218,6 +218,8 @@ class Server:
                     job.start = now
                     busy[s] = job
             if not busy:
+                if not arrivals and not pending_done and any(queues.values()):
+                    raise RuntimeError("requests wait for bodies that cannot be admitted (arena or budget full)")
                 # nothing on the GPU: retire finished work, then wait for the next arrival
                 self._retire(pending_done, done_at, t0, block=True)
                 if arrivals and realtime:
