@@ -383,12 +383,16 @@ int fail(fw_ctx* c, int code, const char* fmt, ...) {
   return code;
 }
 
+// On failure the runtime's last-error state is cleared too, so that a later
+// launch check of this or another context does not report a stale error.
 #define FW_CUDA(ctx, call)                                                                 \
   do {                                                                                     \
     cudaError_t _e = (call);                                                               \
-    if (_e != cudaSuccess)                                                                 \
+    if (_e != cudaSuccess) {                                                               \
+      cudaGetLastError();                                                                  \
       return fail((ctx), _e == cudaErrorMemoryAllocation ? FW_ERR_OOM : FW_ERR_CUDA,       \
                   "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    }                                                                                      \
   } while (0)
 
 template <typename T>
@@ -642,7 +646,10 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
     return 1;
   }
   ResKernel kern = res_kernel(c->front_warps);
-  cudaError_t e1 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // The attribute is per function and process-wide: every context sets it to
+  // the device maximum, so a context with small patches cannot lower the limit
+  // below what another context launches with.
+  cudaError_t e1 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   int per_sm = 0;
   cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kResThreads, smem);
   if (e1 != cudaSuccess || e2 != cudaSuccess || per_sm * sms < P) {

@@ -103,13 +103,21 @@ def poisson_requests(rate, duration, n_bodies, seed=0, substeps=(50, 400)):
     return out
 
 
+def request_substeps(req, frame_dt, stable_time):
+    """Substeps a request runs: the requested count, raised to the body's
+    stable count ceil(frame_dt / stableTime) when the requested dt would exceed
+    the reference's stability bound for that body (the adaptive rule of
+    ExplicitLoop, explicitloop.py:329-331, 580-582)."""
+    return max(int(req.substeps), int(np.ceil(frame_dt / stable_time - 1e-9)))
+
+
 class _Job:
     __slots__ = ("req", "runs", "pos", "left", "start", "init")
 
-    def __init__(self, req, frame_dt, init=False):
+    def __init__(self, req, frame_dt, stable_time, init=False):
         self.req = req
         self.init = init  # the body was just admitted: its first launch is the zero-dt construction step
-        sub = frame_dt / req.substeps
+        sub = frame_dt / request_substeps(req, frame_dt, stable_time)
         self.runs = substep_schedule(frame_dt, sub, sub, False)
         self.pos = 0
         self.left = self.runs[0][0]
@@ -214,7 +222,7 @@ class Server:
                     if not adm:
                         continue
                     s = self.resident[body]
-                    job = _Job(q.popleft(), self.frame_dt, init=(adm == "new"))
+                    job = _Job(q.popleft(), self.frame_dt, self.arena.layouts[s].stableTime, init=(adm == "new"))
                     job.start = now
                     busy[s] = job
             if not busy:
@@ -292,7 +300,7 @@ class FifoPlainServer:
             if lp is None:
                 lp = ExplicitLoop(0.0, self.make_body(r.body), useAdapativeDT=False, device=self.device)
                 self.loops[r.body] = lp
-            sub = self.frame_dt / r.substeps
+            sub = self.frame_dt / request_substeps(r, self.frame_dt, lp.stableTime)
             lp.default_dt = sub
             lp.advanceWithTime(self.frame_dt)
             lp.synchronize()

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import flatworld_b200 as fw
-from flatworld_b200.serve import Arena, FifoPlainServer, Request, Server, poisson_requests
+from flatworld_b200.serve import Arena, FifoPlainServer, Request, Server, poisson_requests, request_substeps
 from flatworld_b200.world import substep_schedule
 from tests import scenes
 
@@ -27,7 +27,7 @@ def small_body(i):
 def alone(body, reqs):
     lp = fw.ExplicitLoop(0.0, small_body(body), useAdapativeDT=False, path="gather")
     for r in reqs:
-        lp.default_dt = FRAME / r.substeps
+        lp.default_dt = FRAME / request_substeps(r, FRAME, lp.stableTime)
         lp.advanceWithTime(FRAME)
     return lp.femSpringManager.coords.numpy()[: lp._packed.N], lp.femSpringManager.V.numpy()[: lp._packed.N]
 
