@@ -641,7 +641,7 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
   r.n_bodies = c->B;
   if (c->B > 4096) { c->res_reason = "more than 4096 bodies"; return 1; }
   const size_t smem = res_layout(r, nullptr, nullptr);
-  if ((long)smem > optin) {
+  if ((long)smem + 64 > optin) {
     c->res_reason = "patch needs " + std::to_string(smem) + " B of shared memory";
     return 1;
   }
@@ -649,7 +649,10 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
   // The attribute is per function and process-wide: every context sets it to
   // the device maximum, so a context with small patches cannot lower the limit
   // below what another context launches with.
-  cudaError_t e1 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, kern);
+  cudaError_t e1 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        optin - (int)fa.sharedSizeBytes);
   int per_sm = 0;
   cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kResThreads, smem);
   if (e1 != cudaSuccess || e2 != cudaSuccess || per_sm * sms < P) {
