@@ -52,6 +52,11 @@ _SIGNATURES = {
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_snapshot": (C.c_int, [_vp, C.c_int32]),
+    "fw_set_element_young": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.c_int32]),
+    "fw_adj_begin": (C.c_int, [_vp, C.c_int32]),
+    "fw_adj_seed": (C.c_int, [_vp, _vp, _vp, C.c_int32]),
+    "fw_adj_segment": (C.c_int, [_vp, C.c_int32, C.c_float]),
+    "fw_adj_read": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32]),
     "fw_arena_init": (C.c_int, [_vp, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int64]),
     "fw_arena_commit": (C.c_int, [_vp, _i32p]),
     "fw_arena_remove": (C.c_int, [_vp, C.c_int32]),
@@ -194,6 +199,31 @@ class NativeWorld:
 
     def restore(self, slot: int = 0):
         self._check(self._L.fw_restore(self._h, int(slot)), "fw_restore")
+
+    # ---- differentiable form
+    def set_element_young(self, young, first=0):
+        y = np.ascontiguousarray(young, dtype=np.float32)
+        self._check(self._L.fw_set_element_young(self._h, int(first), len(y), y.ctypes.data, 0),
+                    "fw_set_element_young")
+
+    def adj_begin(self, max_segment_steps):
+        self._check(self._L.fw_adj_begin(self._h, int(max_segment_steps)), "fw_adj_begin")
+
+    def adj_seed(self, xbar=None, vbar=None):
+        xb = None if xbar is None else np.ascontiguousarray(xbar, dtype=np.float32)
+        vb = None if vbar is None else np.ascontiguousarray(vbar, dtype=np.float32)
+        self._check(self._L.fw_adj_seed(self._h, None if xb is None else xb.ctypes.data,
+                                        None if vb is None else vb.ctypes.data, 0), "fw_adj_seed")
+
+    def adj_segment(self, n, dt):
+        self._check(self._L.fw_adj_segment(self._h, int(n), float(np.float32(dt))), "fw_adj_segment")
+
+    def adj_read(self, n_nodes, n_elems):
+        xb = np.empty((n_nodes, 2), np.float32)
+        vb = np.empty((n_nodes, 2), np.float32)
+        eb = np.empty((n_elems,), np.float32)
+        self._check(self._L.fw_adj_read(self._h, xb.ctypes.data, vb.ctypes.data, eb.ctypes.data, 0), "fw_adj_read")
+        return xb, vb, eb
 
     # ---- arena (served form)
     def arena_init(self, max_nodes, max_elems, max_bodies, max_scenes, max_pairs, max_heights, max_occ):

@@ -28,6 +28,7 @@
 
 #include "../../include/fwb200.h"
 #include "fw_device.cuh"
+#include "fw_adjoint.cuh"
 
 using fw::ElemMat;
 using fw::Pair;
@@ -277,6 +278,96 @@ __global__ void k_prepare_mass(Dev d, int n_lo, int n_hi) {
   d.mass[i] = m;
 }
 
+// Lame constants of elements [e_lo, e_hi) from new Young's moduli (same
+// formula as k_prepare_elements).
+__global__ void k_set_young(Dev d, const float* __restrict__ young, const float* __restrict__ poisson,
+                            int e_lo, int e_hi) {
+  const int e = e_lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= e_hi) return;
+  const float E = young[e - e_lo], nu = poisson[e];
+  ElemMat m = d.emat[e];
+  m.lam = E * nu / ((1.0f + nu) * (1.0f - 2.0f * nu));
+  m.mu = E / (2.0f * (1.0f + nu));
+  d.emat[e] = m;
+}
+
+struct Adj {
+  float2* xb;    // adjoint of positions
+  float2* vb;    // adjoint of velocities
+  float2* fb;    // adjoint of the node force of the current substep
+  float* Eb;     // d loss / d Young's modulus, per element
+  float* young;  // Young's modulus per element
+  float2* traj;  // recorded positions of the segment, [K][N]
+  int32_t* gates;  // recorded broad-phase gates, [K][P]
+};
+
+// Adjoint of "v' = v + dt f / m; BC override" at every node: from (xb', vb')
+// form the force adjoint fb and the velocity adjoint of the previous substep.
+__device__ __forceinline__ void adj_node_prep(const Dev& d, const Adj& a, int i, float dt) {
+  const int bc = (int)(d.node_word[i] & fw::NODE_BC_MASK);
+  const float2 xb = a.xb[i], vb = a.vb[i];
+  const float2 vt = make_float2(vb.x + dt * xb.x, vb.y + dt * xb.y);
+  const bool vfixed = (bc & (fw::BC_U | fw::BC_V)) != 0;
+  const bool fdead = vfixed || (bc & fw::BC_A) != 0;
+  const float s = dt / d.mass[i];
+  a.fb[i] = fdead ? make_float2(0.f, 0.f) : make_float2(s * vt.x, s * vt.y);
+  a.vb[i] = vfixed ? make_float2(0.f, 0.f) : vt;
+}
+
+__global__ void k_adj_prep(Dev d, Adj a, float dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < d.N) adj_node_prep(d, a, i, dt);
+}
+
+__global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.E) return;
+  const ElemMat m = d.emat[e];
+  const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
+  const float2 w0 = a.fb[c0], w1 = a.fb[c1], w2 = a.fb[c2];
+  fw::Dual f[6];
+  fw::element_forces_jvp(x[c0], x[c1], x[c2], w0, w1, w2, d.jinv[e], fw::elem_type(m.word), m.lam, m.mu,
+                         m.area, f);
+  d.corner[3 * e] = make_float2(f[0].d, f[1].d);
+  d.corner[3 * e + 1] = make_float2(f[2].d, f[3].d);
+  d.corner[3 * e + 2] = make_float2(f[4].d, f[5].d);
+  const float dot = w0.x * f[0].v + w0.y * f[1].v + w1.x * f[2].v + w1.y * f[3].v + w2.x * f[4].v + w2.y * f[5].v;
+  a.Eb[e] += dot / a.young[e];
+}
+
+// xb <- xb' + sum of element VJPs + plane-contact VJP, then the force /
+// velocity adjoints of the previous substep.
+__global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const int32_t* __restrict__ gates,
+                            float dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  float2 xb = a.xb[i];
+  const float2 fb = a.fb[i];
+  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
+    const float2 c = d.corner[d.csr_slot[k]];
+    xb.x += c.x;
+    xb.y += c.y;
+  }
+  const uint32_t w = d.node_word[i];
+  if (w & fw::NODE_BOUNDARY) {
+    const int b = (int)(w >> fw::NODE_BODY_SHIFT);
+    const float2 xi = x[i];
+    for (int q = 0; q < d.body_pair_cnt[b]; ++q) {
+      const int p = d.body_pair_off[b] + q;
+      if (!gates[p]) continue;
+      const Pair& pr = d.pairs[p];
+      const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
+      if (pen < 0.0f) {  // c = -k n pen  ->  dc/dx = -k n n^T
+        const float t = -pr.penalty * (pr.f[2] * fb.x + pr.f[3] * fb.y);
+        xb.x += t * pr.f[2];
+        xb.y += t * pr.f[3];
+      }
+    }
+  }
+  a.xb[i] = xb;
+  adj_node_prep(d, a, i, dt);
+}
+
 }  // namespace
 
 #include "fw_resident.cuh"
@@ -361,6 +452,11 @@ struct fw_ctx {
   int2 *d_echunks = nullptr, *d_nchunks = nullptr;
   int64_t chunk_cap = 0;
   float *a_young = nullptr, *a_poisson = nullptr, *a_rho = nullptr;
+  // differentiable form
+  Adj adj{};
+  int adj_cap = 0;  // steps per segment the trajectory buffer holds
+  bool adj_dt_pending = false;  // the seed still needs its force-adjoint pass
+  float* d_poisson = nullptr;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
@@ -1435,6 +1531,111 @@ int fw_arena_scene_info(fw_ctx* c, int32_t s, int64_t* info) {
   const fw_ctx::ArenaScene& a = c->ascenes[s];
   info[0] = a.n0; info[1] = a.nn; info[2] = a.e0; info[3] = a.ne; info[4] = a.b0; info[5] = a.nb;
   info[6] = c->fl_nodes.total(); info[7] = c->fl_elems.total();
+  return FW_OK;
+}
+
+
+int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* young, int32_t on_device) {
+  if (!c || !young) return FW_ERR_ARG;
+  if (!c->finalized || c->arena || c->path != FW_PATH_GATHER)
+    return fail(c, FW_ERR_STATE, "fw_set_element_young needs a finalized world on the gather path");
+  if (first < 0 || count < 0 || (int64_t)first + count > c->E) return fail(c, FW_ERR_ARG, "element range out of bounds");
+  if (count == 0) return FW_OK;
+  int rc;
+  if (!c->d_poisson && (rc = upload(c, &c->d_poisson, c->h_nu))) return rc;
+  if (!c->adj.young && (rc = upload(c, &c->adj.young, c->h_E))) return rc;
+  float* dst = c->adj.young + first;
+  FW_CUDA(c, cudaMemcpyAsync(dst, young, sizeof(float) * count,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+  k_set_young<<<(count + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, dst, c->d_poisson, first, first + count);
+  c->launches += 1;
+  return check_kernel(c, "set young");
+}
+
+int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized || c->arena || c->path != FW_PATH_GATHER || c->S != 1)
+    return fail(c, FW_ERR_STATE, "the adjoint needs a finalized single-scene world on the gather path");
+  if (max_segment_steps <= 0) return fail(c, FW_ERR_ARG, "max_segment_steps must be > 0");
+  if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the adjoint covers Elastic and NeoHookean triangles (no J2)");
+  for (const Pair& p : c->h_pairs)
+    if (p.kind != fw::PAIR_PLANE) return fail(c, FW_ERR_ARG, "the adjoint covers plane contact only");
+  int rc;
+  Adj& a = c->adj;
+  if (!a.young) {
+    if ((rc = upload(c, &a.young, c->h_E))) return rc;
+  }
+  if (!a.xb) {
+    if ((rc = dalloc(c, &a.xb, c->N)) || (rc = dalloc(c, &a.vb, c->N)) || (rc = dalloc(c, &a.fb, c->N)) ||
+        (rc = dalloc(c, &a.Eb, c->E)))
+      return rc;
+  }
+  if (c->adj_cap < max_segment_steps) {
+    if ((rc = dalloc(c, &a.traj, (size_t)max_segment_steps * c->N)) ||
+        (rc = dalloc(c, &a.gates, (size_t)max_segment_steps * std::max(1, c->d.P))))
+      return rc;
+    c->adj_cap = max_segment_steps;
+  }
+  FW_CUDA(c, cudaMemsetAsync(a.Eb, 0, sizeof(float) * c->E, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(a.xb, 0, sizeof(float2) * c->N, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(a.vb, 0, sizeof(float2) * c->N, c->stream));
+  return FW_OK;
+}
+
+int fw_adj_seed(fw_ctx* c, const float* xbar, const float* vbar, int32_t on_device) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->adj.xb) return fail(c, FW_ERR_STATE, "fw_adj_seed before fw_adj_begin");
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (xbar) FW_CUDA(c, cudaMemcpyAsync(c->adj.xb, xbar, sizeof(float2) * c->N, k, c->stream));
+  else FW_CUDA(c, cudaMemsetAsync(c->adj.xb, 0, sizeof(float2) * c->N, c->stream));
+  if (vbar) FW_CUDA(c, cudaMemcpyAsync(c->adj.vb, vbar, sizeof(float2) * c->N, k, c->stream));
+  else FW_CUDA(c, cudaMemsetAsync(c->adj.vb, 0, sizeof(float2) * c->N, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(c->adj.Eb, 0, sizeof(float) * c->E, c->stream));
+  c->adj_dt_pending = true;
+  return FW_OK;
+}
+
+int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->adj.xb) return fail(c, FW_ERR_STATE, "fw_adj_segment before fw_adj_begin");
+  if (n_steps <= 0 || n_steps > c->adj_cap) return fail(c, FW_ERR_ARG, "n_steps outside (0, max_segment_steps]");
+  Adj& a = c->adj;
+  const int N = c->N, E = c->E, P = std::max(1, c->d.P);
+  c->d.uniform_dt = 1;
+  c->d.dt_uniform = dt;
+  int rc;
+  // recompute the segment from the current state, recording positions and gates
+  for (int j = 0; j < n_steps; ++j) {
+    FW_CUDA(c, cudaMemcpyAsync(a.traj + (size_t)j * N, c->d.x, sizeof(float2) * N, cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = launch_step(c))) return rc;
+    c->host_counter += 1;
+    if (c->d.P > 0)
+      FW_CUDA(c, cudaMemcpyAsync(a.gates + (size_t)j * P, c->d.pair_active, sizeof(int32_t) * c->d.P,
+                                 cudaMemcpyDeviceToDevice, c->stream));
+  }
+  const int gn = (N + kBlock - 1) / kBlock, ge = (E + kBlock - 1) / kBlock;
+  if (c->adj_dt_pending) {  // force / velocity adjoints of the last substep from the seed
+    k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt);
+    c->launches += 1;
+    c->adj_dt_pending = false;
+  }
+  for (int j = n_steps - 1; j >= 0; --j) {
+    const float2* x = a.traj + (size_t)j * N;
+    k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x);
+    k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt);
+    c->launches += 2;
+  }
+  return check_kernel(c, "adjoint segment");
+}
+
+int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_device) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->adj.xb) return fail(c, FW_ERR_STATE, "fw_adj_read before fw_adj_begin");
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (xbar) FW_CUDA(c, cudaMemcpyAsync(xbar, c->adj.xb, sizeof(float2) * c->N, k, c->stream));
+  if (vbar) FW_CUDA(c, cudaMemcpyAsync(vbar, c->adj.vb, sizeof(float2) * c->N, k, c->stream));
+  if (Ebar) FW_CUDA(c, cudaMemcpyAsync(Ebar, c->adj.Eb, sizeof(float) * c->E, k, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
   return FW_OK;
 }
 

@@ -173,7 +173,8 @@ class PackedWorld:
                 conn[e0:e0 + ne] = np.asarray(mesh.connectivity, dtype=np.int64)[:, :3] + n0
                 mat = dom.prop.getMaterial()
                 mtype[e0:e0 + ne] = int(mat.type)
-                Ev[e0:e0 + ne] = float(mat.E)
+                ey = getattr(dom, "elementYoung", None)  # optional per-element E (else the material's)
+                Ev[e0:e0 + ne] = float(mat.E) if ey is None else np.asarray(ey, np.float32).reshape(ne)
                 nuv[e0:e0 + ne] = float(mat.nu)
                 rhov[e0:e0 + ne] = float(mat.rho)
                 syv[e0:e0 + ne] = float(getattr(mat, "sigma_y", 0.0))

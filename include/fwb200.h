@@ -267,6 +267,26 @@ int fw_arena_commit(fw_ctx* ctx, int32_t* scene_out);
 int fw_arena_remove(fw_ctx* ctx, int32_t scene);
 int fw_arena_scene_info(fw_ctx* ctx, int32_t scene, int64_t* info);
 
+/* Differentiable form.  fw_set_element_young: new per-element Young's moduli
+ * for elements [first, first+count) (Lame constants recomputed; gather path).
+ * The reference stores E per element (femspringmanager.py:584, 753) but has no
+ * setter or adjoint.  Reverse pass of a rollout of dt-substeps:
+ *   fw_adj_begin(ctx, K)      adjoint buffers for segments of up to K substeps
+ *   fw_adj_seed(ctx, xb, vb)  adjoint of the final positions / velocities
+ *                             (NULL = zero); clears dL/dE
+ *   fw_adj_segment(ctx, n, dt) from the current state (restore the segment's
+ *                             checkpoint first with fw_restore) recompute n
+ *                             substeps, then run them backward
+ *   fw_adj_read(ctx, xb, vb, Eb) dL/dx, dL/dv at the segment start; dL/dE
+ * Covers Elastic and NeoHookean triangles, plane contact, gravity / nodal
+ * force / fixed / enforced-velocity BCs. */
+int fw_set_element_young(fw_ctx* ctx, int32_t first, int32_t count, const float* young,
+                         int32_t on_device);
+int fw_adj_begin(fw_ctx* ctx, int32_t max_segment_steps);
+int fw_adj_seed(fw_ctx* ctx, const float* xbar, const float* vbar, int32_t on_device);
+int fw_adj_segment(fw_ctx* ctx, int32_t n_steps, float dt);
+int fw_adj_read(fw_ctx* ctx, float* xbar, float* vbar, float* Ebar, int32_t on_device);
+
 /* Library build identification string (arch, flags). */
 const char* fw_build_info(void);
 

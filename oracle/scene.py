@@ -221,7 +221,8 @@ class OracleLoop:
             ne = m.numElements
             mat = d.prop.getMaterial()
             types.append(np.full(ne, int(mat.type)))
-            Es.append(np.full(ne, float(mat.E), np.float32))
+            ey = getattr(d, "elementYoung", None)
+            Es.append(np.full(ne, float(mat.E), np.float32) if ey is None else np.asarray(ey, np.float32).reshape(ne))
             nus.append(np.full(ne, float(mat.nu), np.float32))
             rhos.append(np.full(ne, float(mat.rho), np.float32))
             sys_.append(np.full(ne, float(getattr(mat, "sigma_y", 0.0)), np.float32))
@@ -323,7 +324,8 @@ class OracleLoop:
         return x, v, u
 
     def set_state(self, x, v):
-        xa, va = _fp(x), _fp(v)
+        xa = _fp(x) if x is not None else (None, None)
+        va = _fp(v) if v is not None else (None, None)
         self._L.or_set_state(self._w, xa[1], va[1])
 
     def prepared(self):

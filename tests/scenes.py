@@ -161,3 +161,19 @@ def ragged_batch(fw, n_scenes=2048, seed=0):
 
 def ragged_batch_one(fw, index, seed=0):
     return ragged_body_scene(fw, np.random.default_rng([seed, index]), index)
+
+
+def gradient_block_scene(fw, n=64, side=0.4, bottom=0.5, young=None, v0=(0.0, -2.0), seed=0):
+    """Differentiation workload: n x n quads (2 n^2 NeoHookean triangles) of
+    side ``side`` with its bottom at y = ``bottom``, dropped onto the ground
+    plane y = 0 with initial velocity v0 under gravity 9.8.  Per-element
+    Young's modulus log-normal with mean 1e5 and sigma 0.3 (unless given).
+    Fixed here (unspecified by the workload): nu = 0.3, rho = 1000, side 0.4 m,
+    v0 = (0, -2) so that the block reaches the plane within 0.2 s."""
+    from flatworld_b200.diff import lognormal_young
+
+    conn, coords = fw.structured_rectangle(n, n, side, side, origin=(0.5 - 0.5 * side, bottom))
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.HyperElastic(1e5, 0.3, 1000.0)),
+                       [fw.Gravity([0.0, -9.8])], initials=[fw.InitialVel("ALL", list(v0))])
+    fem.elementYoung = lognormal_young(2 * n * n, seed=seed) if young is None else np.asarray(young, np.float32)
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), fem]
