@@ -291,27 +291,53 @@ __global__ void k_set_young(Dev d, const float* __restrict__ young, const float*
   d.emat[e] = m;
 }
 
+// The adjoint state is accumulated in FP64, so that summing thousands of
+// substeps adds no error of its own; the element Jacobian products are FP32
+// dual numbers on the recorded FP32 trajectory, i.e. this is the exact
+// adjoint of the FP32 forward up to FP32 rounding of those products.
 struct Adj {
-  float2* xb;    // adjoint of positions
-  float2* vb;    // adjoint of velocities
-  float2* fb;    // adjoint of the node force of the current substep
-  float* Eb;     // d loss / d Young's modulus, per element
+  double2* xb;   // adjoint of positions
+  double2* vb;   // adjoint of velocities
+  double2* fb;   // adjoint of the node force of the current substep
+  double* Eb;    // d loss / d Young's modulus, per element
   float* young;  // Young's modulus per element
   float2* traj;  // recorded positions of the segment, [K][N]
   int32_t* gates;  // recorded broad-phase gates, [K][P]
+  float2* io_x;  // FP32 staging of xb / vb / Eb for the C ABI
+  float2* io_v;
+  float* io_E;
 };
 
 // Adjoint of "v' = v + dt f / m; BC override" at every node: from (xb', vb')
 // form the force adjoint fb and the velocity adjoint of the previous substep.
 __device__ __forceinline__ void adj_node_prep(const Dev& d, const Adj& a, int i, float dt) {
   const int bc = (int)(d.node_word[i] & fw::NODE_BC_MASK);
-  const float2 xb = a.xb[i], vb = a.vb[i];
-  const float2 vt = make_float2(vb.x + dt * xb.x, vb.y + dt * xb.y);
+  const double2 xb = a.xb[i], vb = a.vb[i];
+  const double h = (double)dt;
+  const double2 vt = make_double2(vb.x + h * xb.x, vb.y + h * xb.y);
   const bool vfixed = (bc & (fw::BC_U | fw::BC_V)) != 0;
   const bool fdead = vfixed || (bc & fw::BC_A) != 0;
-  const float s = dt / d.mass[i];
-  a.fb[i] = fdead ? make_float2(0.f, 0.f) : make_float2(s * vt.x, s * vt.y);
-  a.vb[i] = vfixed ? make_float2(0.f, 0.f) : vt;
+  const double s = h / (double)d.mass[i];
+  a.fb[i] = fdead ? make_double2(0.0, 0.0) : make_double2(s * vt.x, s * vt.y);
+  a.vb[i] = vfixed ? make_double2(0.0, 0.0) : vt;
+}
+
+__global__ void k_adj_seed(Adj a, int N, int has_x, int has_v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float2 x = has_x ? a.io_x[i] : make_float2(0.f, 0.f);
+  const float2 v = has_v ? a.io_v[i] : make_float2(0.f, 0.f);
+  a.xb[i] = make_double2(x.x, x.y);
+  a.vb[i] = make_double2(v.x, v.y);
+}
+
+__global__ void k_adj_out(Adj a, int N, int E) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) {
+    a.io_x[i] = make_float2((float)a.xb[i].x, (float)a.xb[i].y);
+    a.io_v[i] = make_float2((float)a.vb[i].x, (float)a.vb[i].y);
+  }
+  if (i < E) a.io_E[i] = (float)a.Eb[i];
 }
 
 __global__ void k_adj_prep(Dev d, Adj a, float dt) {
@@ -324,25 +350,27 @@ __global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
   if (e >= d.E) return;
   const ElemMat m = d.emat[e];
   const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
-  const float2 w0 = a.fb[c0], w1 = a.fb[c1], w2 = a.fb[c2];
+  const double2 b0 = a.fb[c0], b1 = a.fb[c1], b2 = a.fb[c2];
+  const float2 w0 = make_float2((float)b0.x, (float)b0.y), w1 = make_float2((float)b1.x, (float)b1.y),
+               w2 = make_float2((float)b2.x, (float)b2.y);
   fw::Dual f[6];
   fw::element_forces_jvp(x[c0], x[c1], x[c2], w0, w1, w2, d.jinv[e], fw::elem_type(m.word), m.lam, m.mu,
                          m.area, f);
   d.corner[3 * e] = make_float2(f[0].d, f[1].d);
   d.corner[3 * e + 1] = make_float2(f[2].d, f[3].d);
   d.corner[3 * e + 2] = make_float2(f[4].d, f[5].d);
-  const float dot = w0.x * f[0].v + w0.y * f[1].v + w1.x * f[2].v + w1.y * f[3].v + w2.x * f[4].v + w2.y * f[5].v;
-  a.Eb[e] += dot / a.young[e];
+  const double dot = b0.x * f[0].v + b0.y * f[1].v + b1.x * f[2].v + b1.y * f[3].v + b2.x * f[4].v + b2.y * f[5].v;
+  a.Eb[e] += dot / (double)a.young[e];
 }
 
-// xb <- xb' + sum of element VJPs + plane-contact VJP, then the force /
-// velocity adjoints of the previous substep.
+// xb <- xb' + sum of element VJPs + plane-contact VJP; with prep, also the
+// force / velocity adjoints of the previous substep (fused, saves a launch).
 __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const int32_t* __restrict__ gates,
-                            float dt) {
+                            float dt, int prep) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.N) return;
-  float2 xb = a.xb[i];
-  const float2 fb = a.fb[i];
+  double2 xb = a.xb[i];
+  const double2 fb = a.fb[i];
   for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
     const float2 c = d.corner[d.csr_slot[k]];
     xb.x += c.x;
@@ -358,14 +386,14 @@ __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const in
       const Pair& pr = d.pairs[p];
       const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
       if (pen < 0.0f) {  // c = -k n pen  ->  dc/dx = -k n n^T
-        const float t = -pr.penalty * (pr.f[2] * fb.x + pr.f[3] * fb.y);
+        const double t = -(double)pr.penalty * (pr.f[2] * fb.x + pr.f[3] * fb.y);
         xb.x += t * pr.f[2];
         xb.y += t * pr.f[3];
       }
     }
   }
   a.xb[i] = xb;
-  adj_node_prep(d, a, i, dt);
+  if (prep) adj_node_prep(d, a, i, dt);
 }
 
 }  // namespace
@@ -455,7 +483,6 @@ struct fw_ctx {
   // differentiable form
   Adj adj{};
   int adj_cap = 0;  // steps per segment the trajectory buffer holds
-  bool adj_dt_pending = false;  // the seed still needs its force-adjoint pass
   float* d_poisson = nullptr;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
@@ -1567,7 +1594,8 @@ int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
   }
   if (!a.xb) {
     if ((rc = dalloc(c, &a.xb, c->N)) || (rc = dalloc(c, &a.vb, c->N)) || (rc = dalloc(c, &a.fb, c->N)) ||
-        (rc = dalloc(c, &a.Eb, c->E)))
+        (rc = dalloc(c, &a.Eb, c->E)) || (rc = dalloc(c, &a.io_x, c->N)) || (rc = dalloc(c, &a.io_v, c->N)) ||
+        (rc = dalloc(c, &a.io_E, c->E)))
       return rc;
   }
   if (c->adj_cap < max_segment_steps) {
@@ -1576,9 +1604,9 @@ int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
       return rc;
     c->adj_cap = max_segment_steps;
   }
-  FW_CUDA(c, cudaMemsetAsync(a.Eb, 0, sizeof(float) * c->E, c->stream));
-  FW_CUDA(c, cudaMemsetAsync(a.xb, 0, sizeof(float2) * c->N, c->stream));
-  FW_CUDA(c, cudaMemsetAsync(a.vb, 0, sizeof(float2) * c->N, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(a.Eb, 0, sizeof(double) * c->E, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(a.xb, 0, sizeof(double2) * c->N, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(a.vb, 0, sizeof(double2) * c->N, c->stream));
   return FW_OK;
 }
 
@@ -1586,13 +1614,12 @@ int fw_adj_seed(fw_ctx* c, const float* xbar, const float* vbar, int32_t on_devi
   if (!c) return FW_ERR_ARG;
   if (!c->adj.xb) return fail(c, FW_ERR_STATE, "fw_adj_seed before fw_adj_begin");
   const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if (xbar) FW_CUDA(c, cudaMemcpyAsync(c->adj.xb, xbar, sizeof(float2) * c->N, k, c->stream));
-  else FW_CUDA(c, cudaMemsetAsync(c->adj.xb, 0, sizeof(float2) * c->N, c->stream));
-  if (vbar) FW_CUDA(c, cudaMemcpyAsync(c->adj.vb, vbar, sizeof(float2) * c->N, k, c->stream));
-  else FW_CUDA(c, cudaMemsetAsync(c->adj.vb, 0, sizeof(float2) * c->N, c->stream));
-  FW_CUDA(c, cudaMemsetAsync(c->adj.Eb, 0, sizeof(float) * c->E, c->stream));
-  c->adj_dt_pending = true;
-  return FW_OK;
+  if (xbar) FW_CUDA(c, cudaMemcpyAsync(c->adj.io_x, xbar, sizeof(float2) * c->N, k, c->stream));
+  if (vbar) FW_CUDA(c, cudaMemcpyAsync(c->adj.io_v, vbar, sizeof(float2) * c->N, k, c->stream));
+  k_adj_seed<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->adj, c->N, xbar != nullptr, vbar != nullptr);
+  c->launches += 1;
+  FW_CUDA(c, cudaMemsetAsync(c->adj.Eb, 0, sizeof(double) * c->E, c->stream));
+  return check_kernel(c, "adjoint seed");
 }
 
 int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
@@ -1613,16 +1640,15 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
       FW_CUDA(c, cudaMemcpyAsync(a.gates + (size_t)j * P, c->d.pair_active, sizeof(int32_t) * c->d.P,
                                  cudaMemcpyDeviceToDevice, c->stream));
   }
+  // (xb, vb) hold the adjoint of the segment's end state; the segment leaves
+  // the adjoint of its start state there (the checkpoint it was restored from).
   const int gn = (N + kBlock - 1) / kBlock, ge = (E + kBlock - 1) / kBlock;
-  if (c->adj_dt_pending) {  // force / velocity adjoints of the last substep from the seed
-    k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt);
-    c->launches += 1;
-    c->adj_dt_pending = false;
-  }
+  k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt);  // force / velocity adjoints of the last substep
+  c->launches += 1;
   for (int j = n_steps - 1; j >= 0; --j) {
     const float2* x = a.traj + (size_t)j * N;
     k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x);
-    k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt);
+    k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt, j > 0);
     c->launches += 2;
   }
   return check_kernel(c, "adjoint segment");
@@ -1632,9 +1658,12 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
   if (!c) return FW_ERR_ARG;
   if (!c->adj.xb) return fail(c, FW_ERR_STATE, "fw_adj_read before fw_adj_begin");
   const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  if (xbar) FW_CUDA(c, cudaMemcpyAsync(xbar, c->adj.xb, sizeof(float2) * c->N, k, c->stream));
-  if (vbar) FW_CUDA(c, cudaMemcpyAsync(vbar, c->adj.vb, sizeof(float2) * c->N, k, c->stream));
-  if (Ebar) FW_CUDA(c, cudaMemcpyAsync(Ebar, c->adj.Eb, sizeof(float) * c->E, k, c->stream));
+  const int n = std::max(c->N, c->E);
+  k_adj_out<<<(n + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->adj, c->N, c->E);
+  c->launches += 1;
+  if (xbar) FW_CUDA(c, cudaMemcpyAsync(xbar, c->adj.io_x, sizeof(float2) * c->N, k, c->stream));
+  if (vbar) FW_CUDA(c, cudaMemcpyAsync(vbar, c->adj.io_v, sizeof(float2) * c->N, k, c->stream));
+  if (Ebar) FW_CUDA(c, cudaMemcpyAsync(Ebar, c->adj.io_E, sizeof(float) * c->E, k, c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   return FW_OK;
 }

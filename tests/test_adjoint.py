@@ -1,6 +1,11 @@
 """Differentiable form (GPU): adjoint gradients of a rollout w.r.t.
 per-element Young's modulus and initial velocities, checked against central
-finite differences of the FP64 oracle along random directions."""
+finite differences of the FP64 oracle along random directions.
+
+The oracle takes its inputs in float32, like the reference, so a perturbed
+input p0 +- eps*d is rounded to float32 before the FP64 rollout; the adjoint
+is dotted with the direction the rollouts actually saw,
+(p+ - p-) / (2 eps), which keeps the central difference consistent."""
 
 import numpy as np
 import pytest
@@ -13,39 +18,94 @@ from tests import scenes
 pytestmark = pytest.mark.gpu
 
 
-def fd_loss64(domains_fn, young, v0, steps, dt, target):
-    doms = domains_fn(young)
-    o = oracle.OracleLoop(doms, dt, useAdapativeDT=False, precision="f64", threads=8)
+def rollout64(domains_fn, young, v0, steps, dt):
+    o = oracle.OracleLoop(domains_fn(young), dt, useAdapativeDT=False, precision="f64", threads=8)
     o.set_state(None, v0)
     o.advance(steps)
-    x, _, _ = o.state()
-    return float(np.sum((x - target) ** 2))
+    return o.state()[0]
 
 
-@pytest.mark.parametrize("n,steps", [(12, 600)])
-def test_adjoint_matches_fp64_central_differences(n, steps):
-    dt = 1e-4
-    build = lambda y=None: scenes.gradient_block_scene(fw, n=n, side=0.12, bottom=0.04, young=y, seed=1)  # noqa: E731
-    sim = DiffSim(build(), dt, steps, checkpoint_every=50)
-    E0 = sim.E0.copy()
-    v0 = np.tile(np.array([0.0, -2.0], np.float32), (sim.N, 1))
-    target = sim.forward(E0 * 1.1, v0).astype(np.float64)
-    xT = sim.forward(E0, v0)
-    assert xT[:, 1].min() < 0.005, "the block must touch the plane"
-    eb, vb, _ = sim.backward(2.0 * (xT - target))
-    rng = np.random.default_rng(0)
+def perturbed(p0, d, eps):
+    """(p0 + eps d, p0 - eps d) in float32 and the direction they span."""
+    hi = (p0.astype(np.float64) + eps * d).astype(np.float32)
+    lo = (p0.astype(np.float64) - eps * d).astype(np.float32)
+    return hi, lo, (hi.astype(np.float64) - lo.astype(np.float64)) / (2.0 * eps)
+
+
+def directional_errors(sim, build, v0, steps, dt, seed_fn, loss_fn, n_dirs, seed, eps=1e-4):
+    """Relative error |adj - fd| / |fd| along random directions: n_dirs in
+    the moduli (dE) and n_dirs in the initial velocities (dv), each checked
+    on its own (a mixed direction's two parts can cancel, which magnifies
+    the relative error of the sum).  seed_fn(x32, x64) gives dL/dx_T from
+    the GPU rollout and from the FP64 oracle rollout of the unperturbed
+    inputs."""
+    x32 = sim.forward(sim.E0, v0)
+    x64 = rollout64(build, sim.E0, v0, steps, dt)
+    eb, vb, _ = sim.backward(seed_fn(x32, x64))
+    rng = np.random.default_rng(seed)
     errs = []
-    for _ in range(4):
-        dE = E0 * rng.standard_normal(sim.E).astype(np.float32)
-        dv = rng.standard_normal((sim.N, 2)).astype(np.float32)
-        adj = float(np.dot(eb.astype(np.float64), dE) + np.sum(vb.astype(np.float64) * dv))
-        eps = 1e-4
-        lp = fd_loss64(build, (E0 + eps * dE).astype(np.float64), v0 + eps * dv, steps, dt, target)
-        lm = fd_loss64(build, (E0 - eps * dE).astype(np.float64), v0 - eps * dv, steps, dt, target)
-        fd = (lp - lm) / (2 * eps)
+    for kind in ("E", "v") * n_dirs:
+        if kind == "E":
+            Ep, Em, dE = perturbed(sim.E0, sim.E0 * rng.standard_normal(sim.E), eps)
+            vp = vm = v0
+            adj = float(np.dot(eb.astype(np.float64), dE))
+        else:
+            vp, vm, dv = perturbed(v0, rng.standard_normal((sim.N, 2)), eps)
+            Ep = Em = sim.E0
+            adj = float(np.sum(vb.astype(np.float64) * dv))
+        fd = (loss_fn(rollout64(build, Ep, vp, steps, dt)) - loss_fn(rollout64(build, Em, vm, steps, dt))) / (2 * eps)
         errs.append(abs(adj - fd) / max(abs(fd), 1e-30))
+    return errs
+
+
+@pytest.mark.parametrize("bottom,steps,seed_from", [(0.04, 600, "fp32"), (0.04, 600, "fp64"), (0.5, 300, "fp64")],
+                         ids=["contact-fp32seed", "contact", "free"])
+def test_adjoint_matches_fp64_central_differences(bottom, steps, seed_from):
+    """Quadratic loss |x_T - target|^2 (target: the rollout with 1.1 x the
+    moduli).  With seed_from="fp64" the adjoint is seeded with dL/dx_T at the
+    FP64 state, so the check measures the adjoint alone; "fp32" seeds it from
+    the GPU's FP32 state, as FEMRollout does.  In free flight the
+    centre-of-mass part of x_T - target is FP32 rounding (~2e-6 of ~8e-4),
+    which the FP64 differences do not see, so that case uses the FP64 seed.
+
+    Tolerance 2.5e-3 relative: the adjoint differentiates the FP32 forward,
+    whose element strains differ from the FP64 rollout's by a median 1.4e-3
+    relative in the free case and 4.4e-4 in the contact case (strain is
+    (F^T F - I) / 2, a difference of nearly equal numbers; measured with the
+    FP32 and FP64 oracles), and dL/dE is a sum over those stresses.  The
+    measured errors are 1e-4..1.6e-3.  The contact cases must touch the plane."""
+    dt = 1e-4
+    build = lambda y=None: scenes.gradient_block_scene(fw, n=12, side=0.12, bottom=bottom, young=y, seed=1)  # noqa: E731
+    sim = DiffSim(build(), dt, steps, checkpoint_every=50)
+    rng = np.random.default_rng(5)
+    v0 = (np.tile([0.0, -2.0], (sim.N, 1)) + 0.3 * rng.standard_normal((sim.N, 2))).astype(np.float32)
+    target = sim.forward(sim.E0 * 1.1, v0).astype(np.float64)
+    if bottom < 0.1:
+        probe = fw.ExplicitLoop(dt, build(), useAdapativeDT=False, path="gather")
+        probe._native.write_nodes(fw._native.FW_FIELD_V, 0, v0)
+        low = []
+        for _ in range(steps // 50):
+            probe.advance_n(50)
+            low.append(float(probe.femSpringManager.coords.numpy()[: sim.N, 1].min()))
+        assert min(low) < 0.0, "the block must reach the plane (penalty contact active)"
+    pick = 0 if seed_from == "fp32" else 1
+    errs = directional_errors(sim, build, v0, steps, dt, lambda *xs: 2.0 * (xs[pick] - target),
+                              lambda x: float(np.sum((x - target) ** 2)), 2, seed=0)
     print("relative error of directional derivatives:", errs)
-    assert max(errs) < 2e-2, errs
+    assert max(errs) < 2.5e-3, errs
+
+
+def test_adjoint_of_linear_functional():
+    """L = w . x_T for a fixed random w: the adjoint is J^T w exactly, with
+    no error from the seed."""
+    dt, steps = 1e-4, 600
+    build = lambda y=None: scenes.gradient_block_scene(fw, n=12, side=0.12, bottom=0.04, young=y, seed=4)  # noqa: E731
+    sim = DiffSim(build(), dt, steps, checkpoint_every=50)
+    v0 = np.tile(np.array([0.0, -2.0], np.float32), (sim.N, 1))
+    w = np.random.default_rng(9).standard_normal((sim.N, 2))
+    errs = directional_errors(sim, build, v0, steps, dt, lambda *xs: w, lambda x: float(np.sum(w * x)), 2, seed=1)
+    print("relative error of directional derivatives:", errs)
+    assert max(errs) < 1e-3, errs
 
 
 def test_checkpoint_interval_does_not_change_gradients():
