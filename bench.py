@@ -42,7 +42,8 @@ def parse():
     ap.add_argument("--mesh", type=int, default=256, help="quads per side of the large mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--workload", choices=["plain_large", "batched", "served"], default="plain_large")
+    ap.add_argument("--workload", choices=["plain_large", "batched", "served", "adjoint"], default="plain_large")
+    ap.add_argument("--fd-directions", type=int, default=16, help="adjoint: FP64 central-FD directions checked")
     ap.add_argument("--rate", type=float, default=2000.0, help="served: requests per second")
     ap.add_argument("--duration", type=float, default=10.0, help="served: seconds of arrivals")
     ap.add_argument("--fifo-seconds", type=float, default=5.0, help="served: wall-time cap of the FIFO server")
@@ -344,6 +345,143 @@ def run_served(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def fd_check(fw, build, sim, v0, steps, dt, target, eb32, vb32, eb64, vb64, n_dirs, threads):
+    """CPU leg of the adjoint workload: FP64 central finite differences of the
+    loss on the oracle along n_dirs random directions (half in the moduli,
+    half in the initial velocities).  The oracle takes float32 inputs, so the
+    perturbed inputs are rounded to float32 and the adjoint is dotted with the
+    direction the rollouts saw.  Returns (seconds per rollout, errors)."""
+    import oracle
+
+    def rollout(young, v):
+        o = oracle.OracleLoop(build(young), dt, useAdapativeDT=False, precision="f64", threads=threads)
+        o.set_state(None, v)
+        o.advance(steps)
+        return o.state()[0]
+
+    def perturbed(p0, d, eps):
+        hi = (p0.astype(np.float64) + eps * d).astype(np.float32)
+        lo = (p0.astype(np.float64) - eps * d).astype(np.float32)
+        return hi, lo, (hi.astype(np.float64) - lo.astype(np.float64)) / (2.0 * eps)
+
+    loss = lambda x: float(np.sum((x - target) ** 2))  # noqa: E731
+    rng = np.random.default_rng(2024)
+    eps, out, t_roll, n_roll = 1e-4, {"E": [], "v": []}, 0.0, 0
+    for k in range(n_dirs):
+        kind = "E" if k % 2 == 0 else "v"
+        if kind == "E":
+            Ep, Em, dE = perturbed(sim.E0, sim.E0 * rng.standard_normal(sim.E), eps)
+            vp = vm = v0
+            a32, a64 = float(np.dot(eb32.astype(np.float64), dE)), float(np.dot(eb64.astype(np.float64), dE))
+        else:
+            vp, vm, dv = perturbed(v0, rng.standard_normal((sim.N, 2)), eps)
+            Ep = Em = sim.E0
+            a32 = float(np.sum(vb32.astype(np.float64) * dv))
+            a64 = float(np.sum(vb64.astype(np.float64) * dv))
+        t0 = time.perf_counter()
+        fd = (loss(rollout(Ep, vp)) - loss(rollout(Em, vm))) / (2 * eps)
+        t_roll += time.perf_counter() - t0
+        n_roll += 2
+        out[kind].append((abs(a32 - fd) / abs(fd), abs(a64 - fd) / abs(fd)))
+    return t_roll / n_roll, out
+
+
+def run_adjoint(args, rank, world, local):
+    """Differentiable form: 64 x 64-quad NeoHookean block (8192 triangles,
+    per-element E log-normal, mean 1e5, sigma 0.3), dropped from y = 0.5 with
+    v0 = (0, -2) onto the plane y = 0, 2000 substeps at dt = 1e-4, checkpoints
+    every 50.  Loss |x_T - x_T(1.1 E)|^2.  One bench step = one gradient
+    evaluation: the forward rollout (storing checkpoints) and the adjoint
+    (recompute + reverse per segment), dL/dE per triangle and dL/dv0 per node
+    returned to the host."""
+    import torch
+
+    import flatworld_b200 as fw
+    from flatworld_b200.diff import DiffSim
+    from tests import scenes
+
+    torch.cuda.set_device(local)
+    dt, steps, K = 1e-4, 2000, 50
+    build = lambda y=None: scenes.gradient_block_scene(fw, n=64, young=y, seed=rank)  # noqa: E731
+    sim = DiffSim(build(), dt, steps, checkpoint_every=K, device=local)
+    stream = torch.cuda.Stream()
+    sim.native.set_stream(stream.cuda_stream)
+    v0 = np.tile(np.array([0.0, -2.0], np.float32), (sim.N, 1))
+    target = sim.forward(sim.E0 * 1.1, v0).astype(np.float64)
+    for _ in range(args.warmup):
+        x = sim.forward(sim.E0, v0)
+        sim.backward(2.0 * (x - target))
+    torch.cuda.synchronize()
+    l0 = sim.native.launch_count()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    walls = []
+    with ClockSampler(local) as clk:
+        for a, b, c in ev:
+            w0 = time.perf_counter()
+            a.record(stream)
+            x = sim.forward(sim.E0, v0)
+            b.record(stream)
+            eb, vb, _ = sim.backward(2.0 * (x - target))
+            c.record(stream)
+            walls.append(time.perf_counter() - w0)
+        torch.cuda.synchronize()
+    launches = sim.native.launch_count() - l0
+    fwd_ms = [a.elapsed_time(b) for a, b, _ in ev]
+    bwd_ms = [b.elapsed_time(c) for _, b, c in ev]
+    ms = float(np.sum(fwd_ms) + np.sum(bwd_ms))
+    per_eval_s = ms / 1e3 / args.steps
+    # the block must reach the plane: minimum height over the forward rollout
+    probe = fw.ExplicitLoop(dt, build(), useAdapativeDT=False, path="gather", device=local)
+    low = 1e9
+    for _ in range(steps // 100):
+        probe.advance_n(100)
+        low = min(low, float(probe.femSpringManager.coords.numpy()[: sim.N, 1].min()))
+    line = {
+        "metric": "gradient evaluations/s (forward + adjoint rollout)", "value": 1.0 / per_eval_s,
+        "unit": "gradients/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (adjoint accumulators f64)", "data": "synthetic (seeded moduli)",
+        "config": {"workload": "differentiable 64x64-quad NeoHookean block, 2000 substeps dt 1e-4, K=50",
+                   "elements": sim.E, "nodes": sim.N, "substeps": steps, "checkpoint_every": K,
+                   "min_height_m": low, "contact": bool(low < 0.0),
+                   "l2": "working set (8192 triangles) fits in L2; latency-bound rollout"},
+        "adjoint": {"forward_ms": float(np.median(fwd_ms)), "backward_ms": float(np.median(bwd_ms)),
+                    "forward_element_steps_per_s": sim.E * steps / (np.median(fwd_ms) / 1e3),
+                    "backward_over_forward": float(np.median(bwd_ms) / np.median(fwd_ms))},
+        "e2e": {"value": args.steps / float(np.sum(walls)), "unit": "gradients/s",
+                "h2d_bytes_per_step": sim.N * 8 * 2 + sim.E * 4, "d2h_bytes_per_step": sim.N * 8 * 2 + sim.E * 4},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and rank == 0:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        o = oracle.OracleLoop(build(), dt, useAdapativeDT=False, precision="f64", threads=threads)
+        o.set_state(None, v0)
+        o.advance(steps)
+        x64 = o.state()[0]
+        sim.forward(sim.E0, v0)
+        eb64, vb64, _ = sim.backward(2.0 * (x64 - target))
+        sim.forward(sim.E0, v0)
+        eb32, vb32, _ = sim.backward(2.0 * (sim.native.read_nodes(0, 0, sim.N) - target))
+        t_roll, errs = fd_check(fw, build, sim, v0, steps, dt, target, eb32, vb32, eb64, vb64,
+                                args.fd_directions, threads)
+        n_params = sim.E + 2 * sim.N
+        line["cpu_baseline"] = {"value": 1.0 / (2 * n_params * t_roll), "unit": "gradients/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"{2 * args.fd_directions} FP64 oracle rollouts of the workload "
+                                          f"({t_roll:.3f} s each); a full gradient by central differences "
+                                          f"takes 2 x {n_params} of them"}
+        line["fd_check"] = {
+            "directions": args.fd_directions, "eps": 1e-4,
+            "max_rel_err_dE": max(e[0] for e in errs["E"]), "max_rel_err_dv0": max(e[0] for e in errs["v"]),
+            "max_rel_err_dE_fp64_seed": max(e[1] for e in errs["E"]),
+            "max_rel_err_dv0_fp64_seed": max(e[1] for e in errs["v"]),
+            "median_rel_err": float(np.median([e[0] for k in errs for e in errs[k]]))}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -355,6 +493,9 @@ def main():
         return
     if args.workload == "served":
         run_served(args, rank, world, local)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args, rank, world, local)
         return
     import torch
 
