@@ -27,6 +27,7 @@ FW_OPT_FRONT_WARPS = 1
 FW_OPT_BLOCK_ELEMS = 2
 FW_OPT_BLOCK_NODES = 3
 FW_OPT_GRID_ELEMS = 4
+FW_OPT_RES_SYNC = 5
 
 _lock = threading.Lock()
 _lib = None

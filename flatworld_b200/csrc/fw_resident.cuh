@@ -26,6 +26,22 @@
 // both paths produce identical bits.  Every wait is bounded: after
 // kSpinLimit polls the CTA sets the error flag and leaves the loop, so a
 // missing CTA cannot hang the device.
+//
+// Two ways to hand a substep's results to the other CTAs:
+//  - counter (any number of bodies): positions go to a double-buffered array,
+//    body boxes to ordered-int atomics; then a release fence and an arrival
+//    count; consumers poll the count, then load halo positions and boxes.
+//  - flag-in-data (up to kLLMaxBodies bodies, the default there): every
+//    published value is a 64-bit word (epoch << 32 | value bits), stored and
+//    loaded with single-copy-atomic 64-bit relaxed accesses, so a consumer that
+//    sees the expected epoch in a word also sees its value -- no fence, no
+//    counter, one L2 round trip.  Each CTA publishes its exported positions and
+//    its partial box per body; every CTA polls its halo words and all partial
+//    boxes and reduces the boxes itself.  Because every CTA waits for every
+//    CTA's partial box, no CTA runs more than one substep ahead of another, so
+//    two slots (parity of the substep) suffice: a slot is rewritten only after
+//    all CTAs have consumed its previous contents.  Epochs count up per launch
+//    from a host-side base, so words left by earlier launches never match.
 #pragma once
 #include <cuda/atomic>
 
@@ -34,6 +50,8 @@ namespace {
 constexpr int kResThreads = 512;
 constexpr int kResMaxPairs = 64;
 constexpr long long kSpinLimit = 1ll << 26;
+constexpr long long kPollLimit = 1ll << 22;  // flag-in-data polls (each one an L2 round trip)
+constexpr int kLLMaxBodies = 8;
 constexpr int kResTableBytes = 48 * 1024;
 
 struct ResPatch {
@@ -55,8 +73,10 @@ struct Res {
   const int32_t* eid;       // global triangle id of each patch triangle
   const int32_t* csr_ptr;
   const uint16_t* csr_slot; // 3 * local triangle + corner
-  float2* xpub;             // [2][N] published positions
-  int* aabb3;               // [3][B][4] ordered-int body boxes
+  float2* xpub;             // [2][N] published positions (counter mode)
+  int* aabb3;               // [3][B][4] ordered-int body boxes (flag-in-data mode: [B][4] start box)
+  unsigned long long* xll;  // [2][N][2] flag-in-data positions (epoch << 32 | float bits)
+  unsigned long long* bll;  // [2][B][P][4] flag-in-data partial boxes (epoch << 32 | ordered int)
   int* bar;                 // arrivals counter (reset by the prologue)
   int* err;                 // != 0: a wait gave up
   int P, no_max, nh_max, ne_max, ncsr_max;
@@ -71,6 +91,22 @@ constexpr uint32_t kJ2Writer = 1u;  // flag bit in conn.y >> 16
 __device__ __forceinline__ int ld_acquire(const int* p) {
   cuda::atomic_ref<const int, cuda::thread_scope_device> a(*p);
   return a.load(cuda::memory_order_acquire);
+}
+
+// 64-bit relaxed device-scope accesses: naturally aligned, single-copy atomic.
+__device__ __forceinline__ unsigned long long ll_load(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void ll_store(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ll_pack(uint32_t epoch, uint32_t bits) {
+  return ((unsigned long long)epoch << 32) | bits;
+}
+__device__ __forceinline__ bool ll_has(unsigned long long w, uint32_t epoch) {
+  return (uint32_t)(w >> 32) == epoch;
 }
 
 struct ResSmem {
@@ -203,11 +239,13 @@ __device__ __forceinline__ void named_bar(int id, int count) {
 // Shared-memory hazards: interior and cut triangles write disjoint corner
 // slots; group-1 and group-2 nodes are disjoint; the halo part of x is only
 // read by the front warps; two CTA-wide barriers per substep order the rest.
-template <int FRONT>
+template <int FRONT, bool LL>
 __global__ void __launch_bounds__(kResThreads, 1)
-k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
+k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t ep0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_abort;
+  __shared__ int s_box[LL ? 4 * kLLMaxBodies : 1];   // reduced body boxes (ordered ints)
+  __shared__ int s_pbox[LL ? 4 * kLLMaxBodies : 1];  // this CTA's partial boxes
   ResSmem s;
   res_layout(r, smem_raw, &s);
   const ResPatch P = r.patch[blockIdx.x];
@@ -250,6 +288,11 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
     s.bpc[b] = d.body_pair_cnt[b];
   }
   if (t == 0) s_abort = 0;
+  if (LL && t < 4 * B) {
+    const int ident = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
+    s_box[t] = ident;
+    s_pbox[t] = ident;
+  }
   const float* heights = r.tab_h ? s.heights : d.heights;
   const int8_t* occ = r.tab_o ? s.occ : d.occ;
   __syncthreads();
@@ -264,7 +307,50 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
     const int g = step0 + k;
     if (front) {
       // previous substep complete everywhere -> halo positions, body boxes
-      if (k > 0) {
+      if (k > 0 && LL) {
+        const uint32_t want = ep0 + (uint32_t)k;
+        const unsigned long long* src = r.xll + (size_t)(k & 1) * N * 2;
+        for (int i = t; i < P.nh; i += FT) {
+          const unsigned long long* w = src + 2 * (size_t)s.hidx[i];
+          unsigned long long wx, wy;
+          long long it = 0;
+          while (true) {
+            wx = ll_load(w);
+            wy = ll_load(w + 1);
+            if (ll_has(wx, want) && ll_has(wy, want)) break;
+            if ((++it & 1023) == 0 && (it > kPollLimit || *(volatile int*)r.err)) {
+              atomicExch(r.err, 1);
+              s_abort = 1;
+              break;
+            }
+          }
+          s.x[P.no + i] = make_float2(__uint_as_float((uint32_t)wx), __uint_as_float((uint32_t)wy));
+        }
+        const unsigned long long* bsrc = r.bll + (size_t)(k & 1) * B * r.P * 4;
+        for (int j = t; j < B * r.P; j += FT) {
+          const unsigned long long* w = bsrc + (size_t)j * 4;
+          unsigned long long b0, b1, b2, b3;
+          long long it = 0;
+          while (true) {
+            b0 = ll_load(w);
+            b1 = ll_load(w + 1);
+            b2 = ll_load(w + 2);
+            b3 = ll_load(w + 3);
+            if (ll_has(b0, want) && ll_has(b1, want) && ll_has(b2, want) && ll_has(b3, want)) break;
+            if ((++it & 1023) == 0 && (it > kPollLimit || *(volatile int*)r.err)) {
+              atomicExch(r.err, 1);
+              s_abort = 1;
+              break;
+            }
+          }
+          int* bx = s_box + 4 * (j / r.P);
+          atomicMin(bx + 0, (int)(uint32_t)b0);
+          atomicMin(bx + 1, (int)(uint32_t)b1);
+          atomicMax(bx + 2, (int)(uint32_t)b2);
+          atomicMax(bx + 3, (int)(uint32_t)b3);
+        }
+        named_bar(1, FT);
+      } else if (k > 0) {
         if (t == 0) {
           long long it = 0;
           const int target = r.P * k;
@@ -286,12 +372,19 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
       if (!s_abort) {
         if (t < d.P) {
           const Pair& pr = s.pairs[t];
-          const int4 bb = __ldcg(reinterpret_cast<const int4*>(r.aabb3 + ((size_t)(g % 3) * B + pr.body) * 4));
+          int4 bb;
+          if (LL)
+            bb = k > 0 ? make_int4(s_box[4 * pr.body], s_box[4 * pr.body + 1], s_box[4 * pr.body + 2],
+                                   s_box[4 * pr.body + 3])
+                       : __ldcg(reinterpret_cast<const int4*>(r.aabb3 + (size_t)pr.body * 4));
+          else
+            bb = __ldcg(reinterpret_cast<const int4*>(r.aabb3 + ((size_t)(g % 3) * B + pr.body) * 4));
           s.gate[t] = fw::pair_gate(pr, fw::ord2f(bb.x), fw::ord2f(bb.y), fw::ord2f(bb.z), fw::ord2f(bb.w), g) ? 1 : 0;
         }
-        if (blockIdx.x == 0)
+        if (!LL && blockIdx.x == 0)
           for (int b = t; b < B; b += FT) aabb_reset(r.aabb3 + ((size_t)((g + 2) % 3) * B + b) * 4);
         named_bar(1, FT);
+        if (LL && t < 4 * B) s_box[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
         for (int q = P.n_int + t; q < P.ne; q += FT) res_element(s, q);
       }
     }
@@ -299,6 +392,8 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
     if (s_abort) break;
     if (front) {
       float2* dst = r.xpub + (size_t)((k + 1) & 1) * N;
+      unsigned long long* dll = r.xll + (size_t)((k + 1) & 1) * N * 2;
+      const uint32_t ep_out = ep0 + (uint32_t)k + 1u;
       int* box_w = r.aabb3 + (size_t)((g + 1) % 3) * B * 4;
       for (int trip = 0; trip < g1_trips; ++trip) {
         const int i = trip * FT + t;
@@ -311,7 +406,15 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
           body = (int)(w >> fw::NODE_BODY_SHIFT);
           bnd = (w & fw::NODE_BOUNDARY) != 0;
           const int gid = s.gid[i];
-          if (gid < 0) __stcg(dst + (gid & 0x7FFFFFFF), x);
+          if (gid < 0) {
+            const size_t gi = (size_t)(gid & 0x7FFFFFFF);
+            if (LL) {
+              ll_store(dll + 2 * gi, ll_pack(ep_out, __float_as_uint(x.x)));
+              ll_store(dll + 2 * gi + 1, ll_pack(ep_out, __float_as_uint(x.y)));
+            } else {
+              __stcg(dst + gi, x);
+            }
+          }
         }
         const unsigned full = 0xFFFFFFFFu;
         const unsigned mb = __ballot_sync(full, bnd);
@@ -330,7 +433,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
             }
           }
           if ((uniform && (int)(t & 31) == leader) || (!uniform && bnd)) {
-            int* rb = box_w + (size_t)body * 4;
+            int* rb = LL ? s_pbox + 4 * body : box_w + (size_t)body * 4;
             atomicMin(rb + 0, fw::f2ord(lx));
             atomicMin(rb + 1, fw::f2ord(ly));
             atomicMax(rb + 2, fw::f2ord(hx));
@@ -339,7 +442,13 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
         }
       }
       named_bar(1, FT);
-      if (t == 0) {
+      if (LL) {
+        if (t < 4 * B) {  // this CTA's partial box of body t / 4, component t % 4
+          unsigned long long* bdst = r.bll + ((size_t)((k + 1) & 1) * B * r.P + (size_t)(t >> 2) * r.P + blockIdx.x) * 4;
+          ll_store(bdst + (t & 3), ll_pack(ep_out, (uint32_t)s_pbox[t]));
+          s_pbox[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
+        }
+      } else if (t == 0) {
         cuda::atomic_ref<int, cuda::thread_scope_device> a(*r.bar);
         a.fetch_add(1, cuda::memory_order_release);
       }
@@ -362,20 +471,21 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp) {
       if ((s.conn[q].y >> 16) & kJ2Writer) d.j2state[r.eid[P.elem_off + q]] = s.j2[q];
 }
 
-using ResKernel = void (*)(Dev, Res, int, int, float, float);
+using ResKernel = void (*)(Dev, Res, int, int, float, float, uint32_t);
 constexpr int kFrontChoices[] = {2, 4, 6, 8};
-inline ResKernel res_kernel(int front) {
+inline ResKernel res_kernel(int front, bool ll) {
   switch (front) {
-    case 2: return k_resident<2>;
-    case 6: return k_resident<6>;
-    case 8: return k_resident<8>;
-    default: return k_resident<4>;
+    case 2: return ll ? k_resident<2, true> : k_resident<2, false>;
+    case 6: return ll ? k_resident<6, true> : k_resident<6, false>;
+    case 8: return ll ? k_resident<8, true> : k_resident<8, false>;
+    default: return ll ? k_resident<4, true> : k_resident<4, false>;
   }
 }
 
 // Before a resident launch: reset the barrier and error flag, copy the body
 // boxes of the last substep into slot step0 % 3 and clear slot (step0+1) % 3.
-__global__ void k_res_prologue(Dev d, Res r, int step0) {
+// (Flag-in-data mode: the start boxes go to slot 0, nothing else.)
+__global__ void k_res_prologue(Dev d, Res r, int step0, int ll) {
   if (threadIdx.x == 0) {
     *r.bar = 0;
     *r.err = 0;
@@ -383,9 +493,9 @@ __global__ void k_res_prologue(Dev d, Res r, int step0) {
   const int cur = d.scene_counter[0] & 1;
   for (int b = threadIdx.x; b < d.B; b += blockDim.x) {
     const int* src = d.aabb_ring + ((size_t)cur * d.B + b) * 4;
-    int* a = r.aabb3 + ((size_t)(step0 % 3) * d.B + b) * 4;
+    int* a = r.aabb3 + ((size_t)(ll ? 0 : step0 % 3) * d.B + b) * 4;
     for (int k = 0; k < 4; ++k) a[k] = src[k];
-    aabb_reset(r.aabb3 + ((size_t)((step0 + 1) % 3) * d.B + b) * 4);
+    if (!ll) aabb_reset(r.aabb3 + ((size_t)((step0 + 1) % 3) * d.B + b) * 4);
   }
 }
 
@@ -400,6 +510,29 @@ __global__ void k_res_epilogue(Dev d, Res r, int step0, int nsteps) {
     for (int k = 0; k < 4; ++k) dst[k] = a[k];
   }
   if (threadIdx.x == 0) d.scene_counter[0] = last;
+}
+
+// Flag-in-data variant: the final boxes are the reduction of the partial
+// boxes of the last substep (slot nsteps & 1); the launch has completed, so
+// plain loads see them.
+__global__ void k_res_epilogue_ll(Dev d, Res r, int step0, int nsteps) {
+  __shared__ int box[4 * kLLMaxBodies];
+  const int B = d.B, t = threadIdx.x;
+  if (t < 4 * B) box[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
+  __syncthreads();
+  const unsigned long long* src = r.bll + (size_t)(nsteps & 1) * B * r.P * 4;
+  for (int j = t; j < B * r.P; j += blockDim.x) {
+    const unsigned long long* w = src + (size_t)j * 4;
+    int* bx = box + 4 * (j / r.P);
+    atomicMin(bx + 0, (int)(uint32_t)w[0]);
+    atomicMin(bx + 1, (int)(uint32_t)w[1]);
+    atomicMax(bx + 2, (int)(uint32_t)w[2]);
+    atomicMax(bx + 3, (int)(uint32_t)w[3]);
+  }
+  __syncthreads();
+  const int last = step0 + nsteps;
+  if (t < 4 * B) d.aabb_ring[(size_t)(last & 1) * B * 4 + t] = box[t];
+  if (t == 0) d.scene_counter[0] = last;
 }
 
 }  // namespace

@@ -487,6 +487,9 @@ struct fw_ctx {
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
+  int res_sync = 0;          // FW_OPT_RES_SYNC
+  bool res_ll = false;       // resident path uses flag-in-data words
+  uint32_t res_epoch = 1;    // epoch base of the next resident launch
   int path = FW_PATH_GATHER;
   Res res{};
   size_t res_smem = 0;
@@ -768,7 +771,8 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
     c->res_reason = "patch needs " + std::to_string(smem) + " B of shared memory";
     return 1;
   }
-  ResKernel kern = res_kernel(c->front_warps);
+  const bool ll = c->res_sync == 0 && c->B <= kLLMaxBodies;
+  ResKernel kern = res_kernel(c->front_warps, ll);
   // The attribute is per function and process-wide: every context sets it to
   // the device maximum, so a context with small patches cannot lower the limit
   // below what another context launches with.
@@ -794,6 +798,13 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
       (rc = dalloc(c, &r.aabb3, 12 * (size_t)c->B)) || (rc = dalloc(c, &r.bar, 1)) ||
       (rc = dalloc(c, &r.err, 1)))
     return rc;
+  if (ll) {
+    if ((rc = dalloc(c, &r.xll, 4 * (size_t)N)) || (rc = dalloc(c, &r.bll, 8 * (size_t)c->B * P))) return rc;
+    FW_CUDA(c, cudaMemsetAsync(r.xll, 0, sizeof(unsigned long long) * 4 * (size_t)N, c->stream));
+    FW_CUDA(c, cudaMemsetAsync(r.bll, 0, sizeof(unsigned long long) * 8 * (size_t)c->B * P, c->stream));
+  }
+  c->res_ll = ll;
+  c->res_epoch = 1;
   r.patch = dpatch;
   r.nodes = dn;
   r.halo = dh;
@@ -816,12 +827,24 @@ int launch_resident(fw_ctx* c, int n) {
   }
   if (n <= 0) return FW_OK;
   const int step0 = (int)c->host_counter;
-  k_res_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0);
+  const bool ll = c->res_ll;
+  if (ll && c->res_epoch > 0xF0000000u) {  // epochs about to wrap: clear the words, restart
+    FW_CUDA(c, cudaMemsetAsync(c->res.xll, 0, sizeof(unsigned long long) * 4 * (size_t)c->N, c->stream));
+    FW_CUDA(c, cudaMemsetAsync(c->res.bll, 0, sizeof(unsigned long long) * 8 * (size_t)c->B * c->res.P,
+                               c->stream));
+    c->res_epoch = 1;
+  }
+  uint32_t ep0 = c->res_epoch;
+  c->res_epoch += (uint32_t)n + 1u;
+  k_res_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, ll ? 1 : 0);
   float dt = c->d.dt_uniform, damp = c->h_damp[0];
-  void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&step0, (void*)&n, (void*)&dt, (void*)&damp};
-  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)res_kernel(c->front_warps), dim3(c->res.P),
+  void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&step0, (void*)&n, (void*)&dt, (void*)&damp, (void*)&ep0};
+  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)res_kernel(c->front_warps, ll), dim3(c->res.P),
                                          dim3(kResThreads), args, c->res_smem, c->stream));
-  k_res_epilogue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
+  if (ll)
+    k_res_epilogue_ll<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
+  else
+    k_res_epilogue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
   c->launches += 3;
   c->host_counter += n;
   return check_kernel(c, "resident step");
@@ -1240,6 +1263,12 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
       c->grid_e_cap = value;
       set_grids(c);
       drop_graphs(c);
+      return FW_OK;
+    }
+    case FW_OPT_RES_SYNC: {
+      if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_RES_SYNC after fw_finalize");
+      if (value != 0 && value != 1) return fail(c, FW_ERR_ARG, "FW_OPT_RES_SYNC must be 0 or 1");
+      c->res_sync = value;
       return FW_OK;
     }
     default:

@@ -195,7 +195,7 @@ class ExplicitLoop:
     def __init__(self, dt, domains, joints=[], ties=None, damping=0.0, useAdapativeDT=True,
                  skip_spatial_hash=False, considerRigidRigidContact=True, use_pd=0,
                  mass_scaling_dt=0.0, max_contact_velocity=50.0, device=0, path="auto", patches=0,
-                 front_warps=0):
+                 front_warps=0, res_sync=0):
         if joints:
             raise NotImplementedError("joints belong to the rigid-body solver, outside flatworld_b200's scope")
         if mass_scaling_dt > 0.0:
@@ -219,7 +219,7 @@ class ExplicitLoop:
         self._counter_py = 0
         self._packed = PackedWorld([layout])
         self._native = build_native(self._packed, device=device, path=path, patches=patches,
-                                    front_warps=front_warps)
+                                    front_warps=front_warps, res_sync=res_sync)
         self.path, self.patches = self._native.get_path()
         self.aabb = _AABBView(self)
         self.femSpringManager = FemSpringManager(self, self._packed, self._native, 0)

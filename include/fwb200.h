@@ -148,6 +148,12 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
 #define FW_OPT_BLOCK_ELEMS 2
 #define FW_OPT_BLOCK_NODES 3
 #define FW_OPT_GRID_ELEMS 4
+/* FW_OPT_RES_SYNC: how resident CTAs hand each substep's halo positions and
+ * body boxes to each other: 0 = flag-in-data words (epoch-tagged 64-bit
+ * values polled directly; used when the scene has at most 8 bodies, default),
+ * 1 = arrival counter + release fence (any number of bodies).  Set before
+ * fw_finalize.  Both give identical results. */
+#define FW_OPT_RES_SYNC 5
 int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
 
 /* Checkpoint / resume: copy the whole step state (positions, velocities, J2

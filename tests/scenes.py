@@ -119,6 +119,25 @@ def plain_large_scene(fw, seed=0, n=256, hf_offset=0.15):
     return [hf, fem]
 
 
+def multi_block_scene(fw, n_bodies, n=10, side=0.08):
+    """n_bodies blocks of n x n quads side by side over the ground plane y=0,
+    bottoms staggered in [0.01, 0.06], falling at (0, -1) under gravity;
+    materials cycle Elastic / NeoHookean / J2 so every law meets contact.
+    The blocks do not collide with each other (collision masks)."""
+    from flatworld_b200.definitions import COLLISION_CATEGORY_FEM, COLLISION_MASK_ALL
+
+    doms = [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0])]
+    for b in range(n_bodies):
+        conn, coords = fw.structured_rectangle(n, n, side, side, origin=(b * 1.25 * side, 0.01 + 0.05 * ((b * 7) % 11) / 10))
+        mat = (fw.Elastic(E=5e4, nu=0.3, rho=500.0), fw.HyperElastic(E=5e4, nu=0.3, rho=500.0),
+               fw.MisesPlastic(E=5e4, nu=0.3, rho=500.0, sigma_y=400.0, H=1e3))[b % 3]
+        fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])],
+                           initials=[fw.InitialVel("ALL", [0.0, -1.0])])
+        fem.collide_bits = COLLISION_MASK_ALL & ~COLLISION_CATEGORY_FEM  # blocks touch the ground only
+        doms.append(fem)
+    return doms
+
+
 def ragged_body_scene(fw, rng, index, h=0.01, rho=2000.0, voxel_cells=128, voxel_h=0.02):
     """One scene of the ragged batch: a structured rectangle with node count
     log-uniform in [100, 20000] and aspect ratio U[0.25, 4]; material by

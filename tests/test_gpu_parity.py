@@ -23,10 +23,19 @@ RTOL = 1e-5
 FRAME = 1.0 / 60.0
 
 
-@pytest.fixture(params=["gather", "resident"])
+@pytest.fixture(params=["gather", "resident", "resident-counter"])
 def path(request):
-    """Both step implementations must meet the same bar."""
+    """Every step implementation must meet the same bar: the gather path and
+    the resident path with either hand-off between CTAs (flag-in-data words,
+    the default for <= 8 bodies, or the arrival counter)."""
     return request.param
+
+
+def loop_kw(path):
+    """ExplicitLoop keyword arguments for a ``path`` fixture value."""
+    if path == "resident-counter":
+        return {"path": "resident", "res_sync": 1}
+    return {"path": path}
 
 
 def rel_linf(a, b):
@@ -47,7 +56,7 @@ def run_pair(domains, steps, every, dt=None, adaptive=True, exact=False, build=N
     ``track`` (a list) receives the lowest node height at every checkpoint."""
     doms_gpu = build() if build else domains
     doms_or = build() if build else domains
-    loop = fw.ExplicitLoop(dt or 0.0, doms_gpu, useAdapativeDT=adaptive, path=path)
+    loop = fw.ExplicitLoop(dt or 0.0, doms_gpu, useAdapativeDT=adaptive, **loop_kw(path))
     o32 = oracle.OracleLoop(doms_or, dt or 0.0, useAdapativeDT=adaptive, precision="f32", threads=8)
     assert loop.dt == o32.dt
     worst = (0.0, 0.0)
@@ -94,7 +103,7 @@ def test_plain_small_with_ground_contact_bitwise(path):
 
 
 def test_heightfield_disk_bitwise(path):
-    loop = fw.ExplicitLoop(0.0, scenes.hf_disk_scene(fw), useAdapativeDT=True, path=path)
+    loop = fw.ExplicitLoop(0.0, scenes.hf_disk_scene(fw), useAdapativeDT=True, **loop_kw(path))
     o32 = oracle.OracleLoop(scenes.hf_disk_scene(fw), 0.0, useAdapativeDT=True)
     for f in range(60):
         loop.advanceWithTime(FRAME)
@@ -108,7 +117,7 @@ def test_heightfield_disk_bitwise(path):
 
 
 def test_voxel_disk_bitwise(path):
-    loop = fw.ExplicitLoop(0.0, scenes.voxel_disk_scene(fw), useAdapativeDT=True, path=path)
+    loop = fw.ExplicitLoop(0.0, scenes.voxel_disk_scene(fw), useAdapativeDT=True, **loop_kw(path))
     o32 = oracle.OracleLoop(scenes.voxel_disk_scene(fw), 0.0, useAdapativeDT=True)
     for f in range(60):
         loop.advanceWithTime(FRAME)
@@ -155,7 +164,7 @@ def test_bcs_scene_bitwise(path):
                           False)
         d3 = fw.FemDomain(fw.Mesh(2, conn, c + 0.5), prop, [], False, initials=[fw.InitialVel([0, 1], [0, -1.0])])
         return [d0, d1, d2, d3]
-    loop = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, path=path)
+    loop = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, **loop_kw(path))
     o32 = oracle.OracleLoop(build(), 0.0, useAdapativeDT=True)
     for _ in range(60):
         loop.advanceWithTime(FRAME)
@@ -210,7 +219,7 @@ def test_run_to_run_determinism():
 
 def test_aabb_and_getbbox(path):
     doms = scenes.plain_small_scene(fw)
-    loop = fw.ExplicitLoop(1e-4, doms, useAdapativeDT=False, path=path)
+    loop = fw.ExplicitLoop(1e-4, doms, useAdapativeDT=False, **loop_kw(path))
     loop.advance_n(50)
     lb, ub = doms[1].getBBox()
     xg, _ = gpu_state(loop)
@@ -235,10 +244,11 @@ def test_resident_is_chosen_for_large_mesh_and_matches_gather():
                           np.asarray(b.femSpringManager.domains[0].getBBox()))
 
 
+@pytest.mark.parametrize("res_sync", [0, 1], ids=["flag-in-data", "counter"])
 @pytest.mark.parametrize("patches", [1, 7, 64, 148])
-def test_resident_patch_counts_bitwise(patches):
+def test_resident_patch_counts_bitwise(patches, res_sync):
     doms = lambda: scenes.plain_large_scene(fw, n=32, hf_offset=0.17)  # noqa: E731
-    a = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="resident", patches=patches)
+    a = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="resident", patches=patches, res_sync=res_sync)
     b = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="gather")
     for _ in range(20):
         a.advanceWithTime(FRAME)
@@ -246,6 +256,28 @@ def test_resident_patch_counts_bitwise(patches):
     xa, va = gpu_state(a)
     xb, vb = gpu_state(b)
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+@pytest.mark.parametrize("n_bodies", [3, 10])
+def test_resident_multi_body_bitwise(n_bodies):
+    """Several bodies in one scene, all three laws, plane contact: the body
+    boxes (and so the broad-phase gates) are reduced per body across CTAs.
+    3 bodies use the flag-in-data hand-off, 10 bodies (> 8) the counter."""
+    build = lambda: scenes.multi_block_scene(fw, n_bodies)  # noqa: E731
+    a = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, path="resident", patches=37)
+    b = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, path="gather")
+    assert a.path == 2
+    low = 1e9
+    for _ in range(6):
+        a.advanceWithTime(FRAME)
+        b.advanceWithTime(FRAME)
+        xa, va = gpu_state(a)
+        low = min(low, float(xa[:, 1].min()))
+        xb, vb = gpu_state(b)
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    assert low < 0.0, "the blocks must reach the plane"
+    for d in a.femSpringManager.domains:
+        assert np.isfinite(np.asarray(d.getBBox())).all()
 
 
 def test_plain_large_full_size_5000_steps_bitwise():
