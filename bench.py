@@ -602,6 +602,7 @@ def main():
                     "d2h_bytes_per_step": 2 * N * 8},
             "gpu_launches": launches,
             "clocks": clk.summary(),
+            "energy_fp64": loop.energy(),
         }
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1

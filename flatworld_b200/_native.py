@@ -75,6 +75,7 @@ _SIGNATURES = {
     "fw_read_plastic": (C.c_int, [_vp, _f32p, _f32p]),
     "fw_read_reference_shape": (C.c_int, [_vp, _f32p, _f32p]),
     "fw_read_counters": (C.c_int, [_vp, _i64p]),
+    "fw_energy": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "fw_launch_count": (C.c_int64, [_vp]),
     "fw_build_info": (C.c_char_p, []),
     "fw_step_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp,
@@ -319,6 +320,13 @@ class NativeWorld:
     def read_counters(self, n_scenes: int) -> np.ndarray:
         out = np.empty((n_scenes,), dtype=np.int64)
         self._check(self._L.fw_read_counters(self._h, out.ctypes.data_as(_i64p)), "fw_read_counters")
+        return out
+
+    def energy(self, n_scenes: int) -> np.ndarray:
+        """Per-scene energies (FP64, reduced on the device): columns kinetic,
+        strain, external potential, contact penalty."""
+        out = np.zeros((n_scenes, 4), dtype=np.float64)
+        self._check(self._L.fw_energy(self._h, out.ctypes.data_as(C.POINTER(C.c_double))), "fw_energy")
         return out
 
     def launch_count(self) -> int:

@@ -140,5 +140,10 @@ class BatchedLoop:
     def all_coords(self):
         return self._native.read_nodes(_native.FW_FIELD_X, 0, self.packed.N)
 
+    def energies(self):
+        """Per-scene energies, FP64 reduced on the GPU: (n_scenes, 4) array of
+        kinetic, strain, external potential, contact penalty."""
+        return self._native.energy(len(self.packed.scenes))
+
     def launch_count(self):
         return self._native.launch_count()

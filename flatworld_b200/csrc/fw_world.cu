@@ -396,6 +396,117 @@ __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const in
   if (prep) adj_node_prep(d, a, i, dt);
 }
 
+// ------------------------------------------------------------------ energy
+// Total energy, reduced in FP64 (the only FP64 step of the library).  Terms
+// per node: kinetic 1/2 m |v|^2; external potential -m g.x (gravity BC) or
+// -f.x (constant nodal force), following the BC precedence of the update
+// (fixed / prescribed-acceleration nodes have none); penalty 1/2 k sd^2 for
+// every penetrating boundary node and contact pair of its body (the elastic
+// part of the contact force, evaluated at zero velocity; not gated by the
+// broad phase).  Per triangle: area x strain energy density --
+//   Elastic (St-Venant-Kirchhoff): lambda/2 tr(E)^2 + mu E:E
+//   NeoHookean: mu/2 (tr C - 2) - mu ln J + lambda/2 (ln J)^2
+//   J2: the St-Venant-Kirchhoff form of the elastic strain E - eps_p
+// -- the energies whose E-derivatives are the stresses of the step
+// (materialfunctions.py:10-101).  Positions and moduli are the FP32 state,
+// every operation after loading them is FP64.
+struct EnergyChunk {
+  int group;   // output row
+  int n0, nn;  // node range
+  int e0, ne;  // triangle range
+};
+
+__device__ double elem_energy(const Dev& d, int e) {
+  const ElemMat m = d.emat[e];
+  const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
+  const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
+  const float4 ji = d.jinv[e];
+  const double j00 = (double)a.x - (double)c.x, j01 = (double)b.x - (double)c.x;
+  const double j10 = (double)a.y - (double)c.y, j11 = (double)b.y - (double)c.y;
+  const double F00 = j00 * ji.x + j01 * ji.z, F01 = j00 * ji.y + j01 * ji.w;
+  const double F10 = j10 * ji.x + j11 * ji.z, F11 = j10 * ji.y + j11 * ji.w;
+  const double C00 = F00 * F00 + F10 * F10, C01 = F00 * F01 + F10 * F11, C11 = F01 * F01 + F11 * F11;
+  const double lam = m.lam, mu = m.mu;
+  const int type = fw::elem_type(m.word);
+  double W;
+  if (type == fw::MAT_NEOHOOKEAN) {
+    const double lj = log(F00 * F11 - F01 * F10);
+    W = 0.5 * mu * (C00 + C11 - 2.0) - mu * lj + 0.5 * lam * lj * lj;
+  } else {
+    double e0 = 0.5 * (C00 - 1.0), e1 = 0.5 * (C11 - 1.0), e2 = 0.5 * C01;
+    if (type == fw::MAT_MISES) {
+      const float4 ep = d.j2state[e];
+      e0 -= ep.x;
+      e1 -= ep.y;
+      e2 -= ep.z;
+    }
+    const double tr = e0 + e1;
+    W = 0.5 * lam * tr * tr + mu * (e0 * e0 + e1 * e1 + 2.0 * e2 * e2);
+  }
+  return (double)m.area * W;
+}
+
+__device__ void node_energy(const Dev& d, int i, double& ke, double& ext, double& pen) {
+  const float2 x = d.x[i], v = d.v[i], bcv = d.bcv[i];
+  const double m = d.mass[i];
+  ke += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y);
+  const uint32_t w = d.node_word[i];
+  const int bc = (int)(w & fw::NODE_BC_MASK);
+  if (bc & (fw::BC_U | fw::BC_A)) {
+  } else if (bc & fw::BC_GRAVITY) {
+    ext -= m * ((double)bcv.x * x.x + (double)bcv.y * x.y);
+  } else if (bc & fw::BC_FORCE) {
+    ext -= (double)bcv.x * x.x + (double)bcv.y * x.y;
+  }
+  if (w & fw::NODE_BOUNDARY) {
+    const int b = (int)(w >> fw::NODE_BODY_SHIFT);
+    for (int q = 0; q < d.body_pair_cnt[b]; ++q) {
+      const Pair& pr = d.pairs[d.body_pair_off[b] + q];
+      float2 f;
+      if (fw::contact_force(pr, d.heights, d.occ, x, make_float2(0.f, 0.f), 0.f, f))
+        pen += 0.5 * ((double)f.x * f.x + (double)f.y * f.y) / (double)pr.penalty;
+    }
+  }
+}
+
+constexpr int kEnergyThreads = 256;
+constexpr int kEnergyChunk = 8192;
+
+// One block per chunk: fixed-order strided sums, then a fixed tree.
+__global__ void __launch_bounds__(kEnergyThreads) k_energy_chunks(Dev d, const EnergyChunk* ch, double4* part) {
+  __shared__ double sm[4][kEnergyThreads];
+  const EnergyChunk c = ch[blockIdx.x];
+  const int t = threadIdx.x;
+  double ke = 0.0, st = 0.0, ext = 0.0, pen = 0.0;
+  for (int i = t; i < c.nn; i += kEnergyThreads) node_energy(d, c.n0 + i, ke, ext, pen);
+  for (int e = t; e < c.ne; e += kEnergyThreads) st += elem_energy(d, c.e0 + e);
+  sm[0][t] = ke;
+  sm[1][t] = st;
+  sm[2][t] = ext;
+  sm[3][t] = pen;
+  __syncthreads();
+  for (int h = kEnergyThreads / 2; h > 0; h >>= 1) {
+    if (t < h)
+      for (int k = 0; k < 4; ++k) sm[k][t] += sm[k][t + h];
+    __syncthreads();
+  }
+  if (t == 0) part[blockIdx.x] = make_double4(sm[0][0], sm[1][0], sm[2][0], sm[3][0]);
+}
+
+// One thread per group: its chunks' partials in chunk order.
+__global__ void k_energy_groups(const int* first, int n_groups, const double4* part, double4* out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_groups) return;
+  double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+  for (int k = first[g]; k < first[g + 1]; ++k) {
+    s.x += part[k].x;
+    s.y += part[k].y;
+    s.z += part[k].z;
+    s.w += part[k].w;
+  }
+  out[g] = s;
+}
+
 }  // namespace
 
 #include "fw_resident.cuh"
@@ -488,6 +599,12 @@ struct fw_ctx {
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
   int res_sync = 0;          // FW_OPT_RES_SYNC
+  // fw_energy scratch (plain cudaMalloc, freed in fw_destroy)
+  EnergyChunk* d_echunk = nullptr;
+  double4* d_epart = nullptr;
+  int* d_efirst = nullptr;
+  double4* d_eout = nullptr;
+  size_t energy_cap = 0, energy_gcap = 0;
   bool res_ll = false;       // resident path uses flag-in-data words
   uint32_t res_epoch = 1;    // epoch base of the next resident launch
   int path = FW_PATH_GATHER;
@@ -933,6 +1050,8 @@ void fw_destroy(fw_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   for (void* p : c->allocs) cudaFree(p);
+  for (void* p : {(void*)c->d_echunk, (void*)c->d_epart, (void*)c->d_efirst, (void*)c->d_eout})
+    if (p) cudaFree(p);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -1828,6 +1947,75 @@ int fw_read_reference_shape(fw_ctx* c, float* area, float* jinv) {
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   if (area)
     for (int e = 0; e < c->E; ++e) area[e] = m[e].area;
+  return FW_OK;
+}
+
+int fw_energy(fw_ctx* c, double* out) {
+  if (!c || !out) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_energy before fw_finalize");
+  // groups: bodies (summed per scene below) or, in an arena, scene slots
+  struct Range { int n0, nn, e0, ne; };
+  std::vector<Range> groups;
+  if (c->arena) {
+    for (const fw_ctx::ArenaScene& a : c->ascenes)
+      groups.push_back(a.live ? Range{(int)a.n0, (int)a.nn, (int)a.e0, (int)a.ne} : Range{0, 0, 0, 0});
+  } else {
+    for (int b = 0; b < c->B; ++b) groups.push_back(Range{c->h_noff[b], c->h_ncnt[b], c->h_eoff[b], c->h_ecnt[b]});
+  }
+  const int G = (int)groups.size();
+  std::vector<EnergyChunk> chunks;
+  std::vector<int> first(G + 1, 0);
+  for (int g = 0; g < G; ++g) {
+    first[g] = (int)chunks.size();
+    const Range& r = groups[g];
+    const int n = std::max(1, (std::max(r.nn, r.ne) + kEnergyChunk - 1) / kEnergyChunk);
+    for (int k = 0; k < n; ++k) {
+      EnergyChunk ch;
+      ch.group = g;
+      ch.n0 = r.n0 + std::min(r.nn, k * kEnergyChunk);
+      ch.nn = std::max(0, std::min(kEnergyChunk, r.nn - k * kEnergyChunk));
+      ch.e0 = r.e0 + std::min(r.ne, k * kEnergyChunk);
+      ch.ne = std::max(0, std::min(kEnergyChunk, r.ne - k * kEnergyChunk));
+      chunks.push_back(ch);
+    }
+  }
+  first[G] = (int)chunks.size();
+  const size_t nc = chunks.size();
+  if (nc > c->energy_cap || (size_t)G + 1 > c->energy_gcap) {
+    for (void* p : {(void*)c->d_echunk, (void*)c->d_epart, (void*)c->d_efirst, (void*)c->d_eout})
+      if (p) cudaFree(p);
+    c->d_echunk = nullptr;
+    c->d_epart = nullptr;
+    c->d_efirst = nullptr;
+    c->d_eout = nullptr;
+    c->energy_cap = c->energy_gcap = 0;
+    const size_t cap = std::max(nc, (size_t)64), gcap = std::max((size_t)G + 1, (size_t)64);
+    FW_CUDA(c, cudaMalloc((void**)&c->d_echunk, sizeof(EnergyChunk) * cap));
+    FW_CUDA(c, cudaMalloc((void**)&c->d_epart, sizeof(double4) * cap));
+    FW_CUDA(c, cudaMalloc((void**)&c->d_efirst, sizeof(int) * gcap));
+    FW_CUDA(c, cudaMalloc((void**)&c->d_eout, sizeof(double4) * gcap));
+    c->energy_cap = cap;
+    c->energy_gcap = gcap;
+  }
+  FW_CUDA(c, cudaMemcpyAsync(c->d_echunk, chunks.data(), sizeof(EnergyChunk) * nc, cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d_efirst, first.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, c->stream));
+  k_energy_chunks<<<(unsigned)nc, kEnergyThreads, 0, c->stream>>>(c->d, c->d_echunk, c->d_epart);
+  k_energy_groups<<<(G + 127) / 128, 128, 0, c->stream>>>(c->d_efirst, G, c->d_epart, c->d_eout);
+  c->launches += 2;
+  int rc = check_kernel(c, "energy");
+  if (rc) return rc;
+  std::vector<double4> res(G);
+  FW_CUDA(c, cudaMemcpyAsync(res.data(), c->d_eout, sizeof(double4) * G, cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int S = c->arena ? (int)c->ascenes.size() : c->S;
+  for (int s = 0; s < 4 * S; ++s) out[s] = 0.0;
+  for (int g = 0; g < G; ++g) {  // bodies of a scene in ascending order
+    const int sc = c->arena ? g : c->h_scene[g];
+    out[4 * sc + 0] += res[g].x;
+    out[4 * sc + 1] += res[g].y;
+    out[4 * sc + 2] += res[g].z;
+    out[4 * sc + 3] += res[g].w;
+  }
   return FW_OK;
 }
 

@@ -258,5 +258,12 @@ class ExplicitLoop:
             "ExplicitLoop.reset() does not reset FEM state in the reference either "
             "(explicitloop.py:654-656); build a new loop to restart")
 
+    def energy(self) -> dict:
+        """Total energy of the scene, reduced in FP64 on the GPU: kinetic,
+        strain, external (gravity / constant nodal force potential), contact
+        (penalty) and their sum.  No reference counterpart."""
+        k, s, e, c = (float(v) for v in self._native.energy(1)[0])
+        return {"kinetic": k, "strain": s, "external": e, "contact": c, "total": k + s + e + c}
+
     def launch_count(self) -> int:
         return self._native.launch_count()

@@ -79,6 +79,10 @@ class Arena:
         n0, nn = self.info(scene)[:2]
         return self.native.read_nodes(_native.FW_FIELD_V, int(n0), int(nn))
 
+    def energy(self, scene: int):
+        """FP64 energies of one resident scene: kinetic, strain, external, contact."""
+        return self.native.energy(self.S)[scene]
+
 
 @dataclass(order=True)
 class Request:

@@ -218,6 +218,16 @@ int fw_read_reference_shape(fw_ctx* ctx, float* area, float* jinv);
 /* Per-scene step counters (number of advance() calls since finalize). */
 int fw_read_counters(fw_ctx* ctx, int64_t* counters);
 
+/* Total energy per scene, reduced in FP64 on the device (deterministic order):
+ * out[4 s + 0..3] = kinetic, strain, external potential (gravity -m g.x or
+ * constant nodal force -f.x), contact penalty (1/2 k sd^2 of every
+ * penetrating boundary node, ungated) of scene s (arena: scene slot).  Strain
+ * energy densities: St-Venant-Kirchhoff lambda/2 tr(E)^2 + mu E:E (Elastic,
+ * and J2 on E - eps_p); mu/2 (tr C - 2) - mu ln J + lambda/2 (ln J)^2
+ * (NeoHookean).  Synchronises the stream.  No reference counterpart: the
+ * reference computes no energies. */
+int fw_energy(fw_ctx* ctx, double* out);
+
 /* Number of kernel launches this context queued since creation (evidence
  * that the CUDA path ran; used by the benchmark's gpu_launches field). */
 int64_t fw_launch_count(const fw_ctx* ctx);
