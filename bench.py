@@ -30,6 +30,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
+from flatworld_b200 import shard  # noqa: E402
+
 FRAME = 1.0 / 60.0
 
 
@@ -57,6 +59,29 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def dist_init(world, local):
+    """One process per GPU (torchrun): an NCCL group with a short timeout for
+    the barriers and the whole-job reductions; None on one GPU."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return dist
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
 
 
 def workload(fw, mesh):
@@ -217,6 +242,7 @@ def run_batched(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    dist = dist_init(world, local)
     substeps = 100 * args.steps
     t0 = time.perf_counter()
     batch = scenes.ragged_batch(fw, args.scenes, seed=rank)
@@ -227,7 +253,7 @@ def run_batched(args, rank, world, local):
     b.set_stream(stream.cuda_stream)
     with torch.cuda.stream(stream):
         b.advance(100 * args.warmup)
-        torch.cuda.synchronize()
+        barrier(dist)
         l0 = b.launch_count()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(substeps)]
         with ClockSampler(local) as clk:
@@ -237,11 +263,12 @@ def run_batched(args, rank, world, local):
                 e_.record(stream)
             torch.cuda.synchronize()
         launches = b.launch_count() - l0
+    barrier(dist)
     lat = [s_.elapsed_time(e_) for s_, e_ in ev]
-    ms = float(sum(lat))
     E = b.n_elems
+    work, ms = shard.aggregate(E * substeps, float(sum(lat)))
     finite = bool(np.isfinite(b.all_coords()).all())
-    value = E * substeps / (ms / 1e3)
+    value = work / (ms / 1e3)
     # plain path: sample of the same bodies, one loop per body
     rng = np.random.default_rng(1234)
     pick = rng.choice(args.scenes, size=min(args.plain_sample, args.scenes), replace=False)
@@ -276,7 +303,7 @@ def run_batched(args, rank, world, local):
         "config": {"workload": f"ragged batch of {args.scenes} bodies on voxel grids, dt 5e-5",
                    "elements": E, "nodes": b.n_nodes, "bodies": args.scenes, "substeps": substeps,
                    "step": "100 substeps", "l2": "working set larger than L2", "launch": tuned,
-                   "host_build_s": build_s, "state_finite": finite},
+                   "host_build_s": build_s, "state_finite": finite, "replicas": world},
         "batched_vs_plain": {"plain_value": plain_value, "ratio": value / plain_value,
                              "plain_sample_bodies": len(pick),
                              "plain_p50_ms_per_substep": percentile_ms(plain_lat, 50)},
@@ -289,6 +316,8 @@ def run_batched(args, rank, world, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_served(args, rank, world, local):
@@ -305,6 +334,7 @@ def run_served(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    dist = dist_init(world, local)
     t0 = time.perf_counter()
     population = scenes.ragged_batch(fw, args.scenes, seed=rank)  # request payloads, built client-side
     build_s = time.perf_counter() - t0
@@ -314,16 +344,22 @@ def run_served(args, rank, world, local):
     warm = poisson_requests(200.0, 0.05, 8, seed=5)
     Server(lambda b: scenes.ragged_batch_one(fw, 10_000 + b), arena_nodes=200_000, arena_elems=400_000,
            arena_bodies=64, arena_scenes=64, device=local).run(warm, realtime=False)
+    barrier(dist)
     with ClockSampler(local) as clk:
         out = srv.run(reqs, realtime=True)
+    steps_all, wall = shard.aggregate(out["element_steps"], out["wall_s"])
     lat = out["latency_s"] * 1e3
+    if dist is not None:  # every rank's requests count in the percentiles
+        gathered = [None] * world
+        dist.all_gather_object(gathered, lat.tolist())
+        lat = np.asarray([v for g in gathered for v in g])
     fifo = FifoPlainServer(lambda b: population[b], device=local)
     fo = fifo.run(reqs, realtime=True, time_limit=args.fifo_seconds)
     flat = fo["latency_s"] * 1e3
     line = {
         "metric": "FEM element-steps/s (served, continuous batching)",
-        "value": out["element_steps"] / out["wall_s"], "unit": "element-steps/s", "n_gpus": world,
-        "steps": len(reqs), "warmup": len(warm), "ms_per_step": float(np.mean(lat)),
+        "value": steps_all / wall, "unit": "element-steps/s", "n_gpus": world,
+        "steps": len(lat), "warmup": len(warm), "ms_per_step": float(np.mean(lat)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded bodies, Poisson arrivals)",
         "config": {"workload": f"served: {args.rate:.0f} req/s Poisson for {args.duration:.0f} s, "
@@ -331,7 +367,7 @@ def run_served(args, rank, world, local):
                    "requests": len(reqs), "population_build_s": build_s, "budget_bytes": 150e9,
                    "resident_bodies": out["resident_bodies"], "resident_bytes": out["used_bytes"],
                    "deferred_admissions": out["deferred_admissions"], "substeps_run": out["substeps"]},
-        "served": {"sims_per_s": len(reqs) / out["wall_s"], "wall_s": out["wall_s"],
+        "served": {"sims_per_s": len(lat) / wall, "wall_s": wall,
                    "latency_ms": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99),
                                   "p99.9": percentile_ms(lat, 99.9)}},
         "fifo_plain": {"served": fo["served"], "wall_s": fo["wall_s"],
@@ -343,6 +379,8 @@ def run_served(args, rank, world, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def fd_check(fw, build, sim, v0, steps, dt, target, eb32, vb32, eb64, vb64, n_dirs, threads):
@@ -401,6 +439,7 @@ def run_adjoint(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    dist = dist_init(world, local)
     dt, steps, K = 1e-4, 2000, 50
     build = lambda y=None: scenes.gradient_block_scene(fw, n=64, young=y, seed=rank)  # noqa: E731
     sim = DiffSim(build(), dt, steps, checkpoint_every=K, device=local)
@@ -411,7 +450,7 @@ def run_adjoint(args, rank, world, local):
     for _ in range(args.warmup):
         x = sim.forward(sim.E0, v0)
         sim.backward(2.0 * (x - target))
-    torch.cuda.synchronize()
+    barrier(dist)
     l0 = sim.native.launch_count()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     walls = []
@@ -426,10 +465,11 @@ def run_adjoint(args, rank, world, local):
             walls.append(time.perf_counter() - w0)
         torch.cuda.synchronize()
     launches = sim.native.launch_count() - l0
+    barrier(dist)
     fwd_ms = [a.elapsed_time(b) for a, b, _ in ev]
     bwd_ms = [b.elapsed_time(c) for _, b, c in ev]
-    ms = float(np.sum(fwd_ms) + np.sum(bwd_ms))
-    per_eval_s = ms / 1e3 / args.steps
+    evals, ms = shard.aggregate(args.steps, float(np.sum(fwd_ms) + np.sum(bwd_ms)))
+    per_eval_s = ms / 1e3 / evals
     # the block must reach the plane: minimum height over the forward rollout
     probe = fw.ExplicitLoop(dt, build(), useAdapativeDT=False, path="gather", device=local)
     low = 1e9
@@ -438,7 +478,7 @@ def run_adjoint(args, rank, world, local):
         low = min(low, float(probe.femSpringManager.coords.numpy()[: sim.N, 1].min()))
     line = {
         "metric": "gradient evaluations/s (forward + adjoint rollout)", "value": 1.0 / per_eval_s,
-        "unit": "gradients/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "unit": "gradients/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (adjoint accumulators f64)", "data": "synthetic (seeded moduli)",
         "config": {"workload": "differentiable 64x64-quad NeoHookean block, 2000 substeps dt 1e-4, K=50",
@@ -480,6 +520,8 @@ def run_adjoint(args, rank, world, local):
             "median_rel_err": float(np.median([e[0] for k in errs for e in errs[k]]))}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def main():
@@ -503,14 +545,7 @@ def main():
     from flatworld_b200.world import substep_schedule
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = dist_init(world, local)
     domains = workload(fw, args.mesh)
     loop = fw.ExplicitLoop(0.0, domains, useAdapativeDT=True, device=local)
     stream = torch.cuda.Stream()
@@ -522,17 +557,11 @@ def main():
     substeps = sum(n for n, _ in runs)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             flush.zero_()
             loop.advanceWithTime(FRAME)
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
+        barrier(dist)
         launches0 = loop.launch_count()
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -543,8 +572,7 @@ def main():
                 loop.advanceWithTime(FRAME)
                 ends[k].record(stream)
             torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
+        barrier(dist)
         launches = loop.launch_count() - launches0
         ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
         # ---- end to end: host state in, one frame, host state out (pinned)
