@@ -138,16 +138,20 @@ def multi_block_scene(fw, n_bodies, n=10, side=0.08):
     return doms
 
 
-def ragged_body_scene(fw, rng, index, h=0.01, rho=2000.0, voxel_cells=128, voxel_h=0.02):
+def ragged_body_scene(fw, rng, index, h=0.01, rho=2000.0, voxel_cells=128, voxel_h=0.02, v0=0.0):
     """One scene of the ragged batch: a structured rectangle with node count
     log-uniform in [100, 20000] and aspect ratio U[0.25, 4]; material by
     index % 3 (Elastic, NeoHookean, J2 with yield stress 0.02 E, H = 0),
     E ~ U[1e4, 1e6], nu ~ U[0.2, 0.45]; its own 128 x 128 voxel grid with
     Bernoulli(0.15) occupancy.  Fixed here (unspecified by the workload): 1 cm
-    elements, density 2000, 2 cm voxel cells, the body starting 1 cm above the
-    grid and moving down at 1 m/s under gravity 9.8, so it enters the voxel
-    field within the first substeps -- with these, dt = 5e-5 is below every
-    body's CFL and contact bound."""
+    elements, density 2000, 2 cm voxel cells, the body at rest 1 cm above the
+    grid under gravity 9.8, so it drops into the voxel field within the first
+    ~900 substeps and settles there.  With these, dt = 5e-5 is at most 0.77 of
+    every body's CFL and contact bound (the worst is 6.5e-5).  A faster entry
+    (1 m/s down) drives some NeoHookean bodies 5 cm into the random field,
+    where the nearest-free-face normals fold elements until J <= 0 and the
+    state turns non-finite -- the same on the FP32 oracle, i.e. a property of
+    the scheme on that input, not of the kernels."""
     n = float(np.exp(rng.uniform(np.log(100.0), np.log(20000.0))))
     asp = float(rng.uniform(0.25, 4.0))
     nx = max(1, int(round(np.sqrt(n * asp) - 1)))
@@ -168,7 +172,7 @@ def ragged_body_scene(fw, rng, index, h=0.01, rho=2000.0, voxel_cells=128, voxel
     vox = fw.VoxelGridDomain(2, voxel_cells, voxel_cells, lb, lb + extent, occupancy_np=occ)
     conn, coords = fw.structured_rectangle(nx, ny, W, Hh, origin=(0.0, 0.0))
     fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])],
-                       initials=[fw.InitialVel("ALL", [0.0, -1.0])])
+                       initials=[fw.InitialVel("ALL", [0.0, v0])])
     return [vox, fem]
 
 
