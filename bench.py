@@ -176,6 +176,17 @@ def ncu_traffic():
     return None
 
 
+def ncu_traffic_ratio_batched():
+    """DRAM bytes / algorithmic bytes of the gather kernels, measured by ncu on
+    a 256-body batch (per-triangle and per-node traffic do not depend on the
+    batch size, so the ratio scales to the full batch)."""
+    path = os.path.join(ROOT, "profiles", "traffic_batched.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("traffic_over_algorithmic")
+    return None
+
+
 def cpu_oracle_rate(fw, mesh, seconds, threads):
     """Element-steps/s of the CPU restatement on this host (bounded sample)."""
     import oracle
@@ -311,7 +322,10 @@ def run_batched(args, rank, world, local):
                                    "p99.9": percentile_ms(lat, 99.9)},
         "roofline": {"bound": "hbm", "kernel": "substep = k_elements + k_nodes", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": which,
-                     "algorithmic_bytes_per_substep": bstep, "traffic": None},
+                     "algorithmic_bytes_per_substep": bstep,
+                     "traffic": (None if ncu_traffic_ratio_batched() is None
+                                 else round(ncu_traffic_ratio_batched() * bstep)),
+                     "traffic_note": "DRAM bytes per substep scaled from an ncu capture of a 256-body batch"},
         "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0:
