@@ -4,7 +4,9 @@
 // Per substep two kernels run on the context stream:
 //   k_elements  one thread per triangle: deformation gradient, PK2 stress
 //               (elastic / NeoHookean / J2 radial return), the three corner
-//               forces -(B^T S)A written to a corner buffer.  Block 0 first
+//               forces -(B^T S)A written to a corner buffer kept in node
+//               order (each corner at its place in its node's ascending-
+//               element list, so a node reads one contiguous run).  Block 0 first
 //               runs the per-step control (scene modes, broad-phase gates,
 //               step counters, AABB slot reset).
 //   k_nodes     one thread per node: penalty contact (boundary nodes only),
@@ -44,10 +46,11 @@ struct Dev {
   float2* v;
   float2* x0;
   float2* bcv;
-  float2* corner;
+  float2* corner;      // corner forces in node (CSR) order: node i's are corner[csr_off[i] .. csr_end[i])
+  int32_t* corner_pos; // 3 per triangle: where corner (e, c) goes in corner[]
   uint32_t* node_word;
   float* mass;
-  int32_t* csr_off;   // node i's corners are csr_slot[csr_off[i] .. csr_end[i])
+  int32_t* csr_off;   // node i's corners are csr_slot[csr_off[i] .. csr_end[i]), ascending element
   int32_t* csr_end;
   int32_t* csr_slot;
   int32_t* conn;
@@ -118,14 +121,17 @@ __device__ void step_control(const Dev& d) {
   }
 }
 
+// Loads that depend only on the triangle index are issued before the scene
+// check, so the gather of corner positions does not wait for it.
 __device__ __forceinline__ void element_step(const Dev& d, int e) {
   {
     const ElemMat m = d.emat[e];
+    const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
+    const float4 ji = d.jinv[e];
+    const int q0 = d.corner_pos[3 * e], q1 = d.corner_pos[3 * e + 1], q2 = d.corner_pos[3 * e + 2];
+    const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
     const int s = d.body_scene[fw::elem_body(m.word)];
     if (!d.scene_active[s]) return;
-    const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
-    const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
-    const float4 ji = d.jinv[e];
     float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
     float sy = 0.f, H = 0.f;
     const bool mises = fw::elem_type(m.word) == fw::MAT_MISES;
@@ -138,9 +144,9 @@ __device__ __forceinline__ void element_step(const Dev& d, int e) {
     float2 f1, f2, f3;
     fw::element_forces(a, b, c, ji, m, sy, H, j2, f1, f2, f3);
     if (mises) d.j2state[e] = j2;
-    d.corner[3 * e] = f1;
-    d.corner[3 * e + 1] = f2;
-    d.corner[3 * e + 2] = f3;
+    d.corner[q0] = f1;
+    d.corner[q1] = f2;
+    d.corner[q2] = f3;
   }
 }
 
@@ -157,17 +163,33 @@ __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) element_step(d, e);
 }
 
+// The node's own state, its CSR range and its first kNodeCorners corner
+// forces are loaded before the scene lookup, so one node waits on few
+// dependent loads; the corners are then summed in the same ascending order.
+constexpr int kNodeCorners = 8;
+
 __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
   const uint32_t w = valid ? d.node_word[i] : 0u;
+  float2 x = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f), bv0 = make_float2(0.f, 0.f);
+  int k0 = 0, k1 = 0;
+  float mass = 1.0f;
+  if (valid) {
+    x = d.x[i];
+    v = d.v[i];
+    k0 = d.csr_off[i];
+    k1 = d.csr_end[i];
+    mass = d.mass[i];
+    bv0 = d.bcv[i];
+  }
+  float2 cq[kNodeCorners];
+#pragma unroll
+  for (int u = 0; u < kNodeCorners; ++u) cq[u] = k0 + u < k1 ? d.corner[k0 + u] : make_float2(0.f, 0.f);
   const int b = (int)(w >> fw::NODE_BODY_SHIFT);
   const int s = valid ? d.body_scene[b] : 0;
   const int mode = valid ? d.scene_mode[s] : fw::MODE_FROZEN;
   const bool live = mode != fw::MODE_FROZEN;
   bool bnd = false;
-  float2 x = make_float2(0.f, 0.f);
   if (live) {
-    x = d.x[i];
-    float2 v = d.v[i];
     const float dt = mode == fw::MODE_INIT ? 0.0f : (d.uniform_dt ? d.dt_uniform : d.scene_dt[s]);
     const float damp = mode == fw::MODE_INIT ? 0.0f : d.scene_damp[s];
     float2 f = make_float2(0.f, 0.f);
@@ -183,16 +205,20 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
         }
       }
     }
-    const int k0 = d.csr_off[i], k1 = d.csr_end[i];
-    for (int k = k0; k < k1; ++k) {
-      const float2 c = d.corner[d.csr_slot[k]];
+#pragma unroll
+    for (int u = 0; u < kNodeCorners; ++u)  // contiguous, ascending element
+      if (k0 + u < k1) {
+        f.x += cq[u].x;
+        f.y += cq[u].y;
+      }
+    for (int k = k0 + kNodeCorners; k < k1; ++k) {
+      const float2 c = d.corner[k];
       f.x += c.x;
       f.y += c.y;
     }
     const int bc = (int)(w & fw::NODE_BC_MASK);
-    const float2 bv = (bc & (fw::BC_A | fw::BC_GRAVITY | fw::BC_FORCE | fw::BC_V))
-                          ? d.bcv[i] : make_float2(0.f, 0.f);
-    fw::integrate(bc, f, d.mass[i], bv, dt, damp, x, v);
+    const float2 bv = (bc & (fw::BC_A | fw::BC_GRAVITY | fw::BC_FORCE | fw::BC_V)) ? bv0 : make_float2(0.f, 0.f);
+    fw::integrate(bc, f, mass, bv, dt, damp, x, v);
     d.x[i] = x;
     d.v[i] = v;
   }
@@ -356,9 +382,9 @@ __global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
   fw::Dual f[6];
   fw::element_forces_jvp(x[c0], x[c1], x[c2], w0, w1, w2, d.jinv[e], fw::elem_type(m.word), m.lam, m.mu,
                          m.area, f);
-  d.corner[3 * e] = make_float2(f[0].d, f[1].d);
-  d.corner[3 * e + 1] = make_float2(f[2].d, f[3].d);
-  d.corner[3 * e + 2] = make_float2(f[4].d, f[5].d);
+  d.corner[d.corner_pos[3 * e]] = make_float2(f[0].d, f[1].d);
+  d.corner[d.corner_pos[3 * e + 1]] = make_float2(f[2].d, f[3].d);
+  d.corner[d.corner_pos[3 * e + 2]] = make_float2(f[4].d, f[5].d);
   const double dot = b0.x * f[0].v + b0.y * f[1].v + b1.x * f[2].v + b1.y * f[3].v + b2.x * f[4].v + b2.y * f[5].v;
   a.Eb[e] += dot / (double)a.young[e];
 }
@@ -372,7 +398,7 @@ __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const in
   double2 xb = a.xb[i];
   const double2 fb = a.fb[i];
   for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
-    const float2 c = d.corner[d.csr_slot[k]];
+    const float2 c = d.corner[k];
     xb.x += c.x;
     xb.y += c.y;
   }
@@ -1270,10 +1296,15 @@ int fw_finalize(fw_ctx* c) {
   for (int e = 0; e < E; ++e)
     for (int k = 0; k < 3; ++k) off[c->h_conn[3 * e + k] + 1]++;
   for (int i = 0; i < N; ++i) off[i + 1] += off[i];
+  std::vector<int32_t> cpos(3 * (size_t)E);
   {
     std::vector<int32_t> fill(off.begin(), off.end() - 1);
     for (int e = 0; e < E; ++e)
-      for (int k = 0; k < 3; ++k) slot[fill[c->h_conn[3 * e + k]]++] = 3 * e + k;
+      for (int k = 0; k < 3; ++k) {
+        const int32_t at = fill[c->h_conn[3 * e + k]]++;
+        slot[at] = 3 * e + k;
+        cpos[3 * (size_t)e + k] = at;
+      }
   }
   std::vector<ElemMat> emat(E);
   std::vector<float2> j2par(E);
@@ -1297,7 +1328,8 @@ int fw_finalize(fw_ctx* c) {
   if ((rc = upload(c, &d.x0, x0)) || (rc = upload(c, &d.x, x0)) || (rc = upload(c, &d.v, v0)) ||
       (rc = upload(c, &d.bcv, bcv)) || (rc = upload(c, &d.node_word, word)) ||
       (rc = dalloc(c, &d.mass, N)) || (rc = upload(c, &d.csr_off, off)) ||
-      (rc = upload(c, &d.csr_slot, slot)) || (rc = upload(c, &d.conn, c->h_conn)) ||
+      (rc = upload(c, &d.csr_slot, slot)) || (rc = upload(c, &d.corner_pos, cpos)) ||
+      (rc = upload(c, &d.conn, c->h_conn)) ||
       (rc = dalloc(c, &d.jinv, E)) || (rc = upload(c, &d.emat, emat)) ||
       (rc = upload(c, &d.j2par, j2par)) || (rc = dalloc(c, &d.j2state, has_j2 ? E : 1)) ||
       (rc = dalloc(c, &d.ndmass, E)) || (rc = dalloc(c, &d.corner, 3 * (size_t)E)) ||
@@ -1457,6 +1489,7 @@ int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_b
   if ((rc = dalloc(c, &d.x0, N)) || (rc = dalloc(c, &d.x, N)) || (rc = dalloc(c, &d.v, N)) ||
       (rc = dalloc(c, &d.bcv, N)) || (rc = dalloc(c, &d.node_word, N)) || (rc = dalloc(c, &d.mass, N)) ||
       (rc = dalloc(c, &d.csr_off, N)) || (rc = dalloc(c, &d.csr_end, N)) || (rc = dalloc(c, &d.csr_slot, 3 * E)) ||
+      (rc = dalloc(c, &d.corner_pos, 3 * E)) ||
       (rc = dalloc(c, &d.conn, 3 * E)) || (rc = dalloc(c, &d.jinv, E)) || (rc = dalloc(c, &d.emat, E)) ||
       (rc = dalloc(c, &d.j2par, E)) || (rc = dalloc(c, &d.j2state, E)) || (rc = dalloc(c, &d.ndmass, E)) ||
       (rc = dalloc(c, &d.corner, 3 * E)) || (rc = dalloc(c, &d.body_scene, B)) ||
@@ -1561,7 +1594,7 @@ int fw_arena_commit(fw_ctx* c, int32_t* scene_out) {
   }
   for (int b = 0; b < Bs; ++b)
     for (int k = 0; k < c->h_bncnt[b]; ++k) word[c->h_bnodes[c->h_bnoff[b] + k]] |= fw::NODE_BOUNDARY;
-  std::vector<int32_t> conn(3 * Es), cbeg(Ns), cend(Ns), slot(3 * Es);
+  std::vector<int32_t> conn(3 * Es), cbeg(Ns), cend(Ns), slot(3 * Es), cpos(3 * Es);
   std::vector<ElemMat> emat(Es);
   std::vector<float2> j2par(Es);
   for (int64_t e = 0; e < Es; ++e) {
@@ -1577,7 +1610,11 @@ int fw_arena_commit(fw_ctx* c, int32_t* scene_out) {
     for (int64_t i = 0; i < Ns; ++i) cnt[i + 1] += cnt[i];
     std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
     for (int64_t e = 0; e < Es; ++e)
-      for (int k = 0; k < 3; ++k) slot[fill[c->h_conn[3 * e + k]]++] = (int32_t)(3 * (a.e0 + e) + k);
+      for (int k = 0; k < 3; ++k) {
+        const int32_t at = fill[c->h_conn[3 * e + k]]++;
+        slot[at] = (int32_t)(3 * (a.e0 + e) + k);
+        cpos[3 * e + k] = (int32_t)(3 * a.e0 + at);
+      }
     for (int64_t i = 0; i < Ns; ++i) {
       cbeg[i] = (int32_t)(3 * a.e0 + cnt[i]);
       cend[i] = (int32_t)(3 * a.e0 + cnt[i + 1]);
@@ -1611,6 +1648,7 @@ int fw_arena_commit(fw_ctx* c, int32_t* scene_out) {
       (rc = up(d.csr_off + a.n0, cbeg.data(), sizeof(int32_t) * Ns)) ||
       (rc = up(d.csr_end + a.n0, cend.data(), sizeof(int32_t) * Ns)) ||
       (rc = up(d.csr_slot + 3 * a.e0, slot.data(), sizeof(int32_t) * 3 * Es)) ||
+      (rc = up(d.corner_pos + 3 * a.e0, cpos.data(), sizeof(int32_t) * 3 * Es)) ||
       (rc = up(d.conn + 3 * a.e0, conn.data(), sizeof(int32_t) * 3 * Es)) ||
       (rc = up(d.emat + a.e0, emat.data(), sizeof(ElemMat) * Es)) ||
       (rc = up(d.j2par + a.e0, j2par.data(), sizeof(float2) * Es)) ||
