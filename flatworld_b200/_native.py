@@ -67,6 +67,7 @@ _SIGNATURES = {
     "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_step_scenes": (C.c_int, [_vp, C.c_int32, _f32p]),
     "fw_step_served": (C.c_int, [_vp, _f32p]),
+    "fw_step_served_n": (C.c_int, [_vp, _f32p, C.c_int32]),
     "fw_set_active": (C.c_int, [_vp, _i32p]),
     "fw_synchronize": (C.c_int, [_vp]),
     "fw_read_nodes": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32]),
@@ -267,6 +268,11 @@ class NativeWorld:
         """One substep; scenes with dt <= 0 stay frozen.  dt must be float32,
         contiguous, one entry per scene (the library copies it before returning)."""
         self._check(self._L.fw_step_served(self._h, dt_per_scene.ctypes.data_as(_f32p)), "fw_step_served")
+
+    def step_served_n(self, dt_per_scene, n_steps: int):
+        """n_steps substeps with the same per-scene dt (see step_served)."""
+        self._check(self._L.fw_step_served_n(self._h, dt_per_scene.ctypes.data_as(_f32p), int(n_steps)),
+                    "fw_step_served_n")
 
     def set_active(self, active):
         a = _i(active)

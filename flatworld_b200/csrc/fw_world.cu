@@ -1712,8 +1712,11 @@ int fw_arena_remove(fw_ctx* c, int32_t s) {
   return FW_OK;
 }
 
-int fw_step_served(fw_ctx* c, const float* dt) {
-  if (!c || !dt) return FW_ERR_ARG;
+int fw_step_served(fw_ctx* c, const float* dt) { return fw_step_served_n(c, dt, 1); }
+
+int fw_step_served_n(fw_ctx* c, const float* dt, int32_t n_steps) {
+  if (!c || !dt || n_steps < 0) return FW_ERR_ARG;
+  if (n_steps == 0) return FW_OK;
   if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_step_served before fw_finalize / fw_arena_init");
   bool changed = false;
   for (int s = 0; s < c->S; ++s) {
@@ -1734,7 +1737,9 @@ int fw_step_served(fw_ctx* c, const float* dt) {
   c->d.uniform_dt = 0;
   int rc;
   if (c->arena && (rc = rebuild_chunks(c))) return rc;
-  return launch_step(c);
+  for (int k = 0; k < n_steps; ++k)
+    if ((rc = launch_step(c))) return rc;
+  return FW_OK;
 }
 
 int fw_arena_scene_info(fw_ctx* c, int32_t s, int64_t* info) {

@@ -4,9 +4,12 @@ A request asks one soft body to advance by ``advanceWithTime(frame_dt)`` in a
 given number of substeps.  The ``Server`` keeps every admitted body resident in
 a device arena (flatworld_b200 C ABI: fw_arena_*), so a body's state carries
 over between its requests, and advances all bodies that have a request in
-flight together, one substep at a time: the batch is rebuilt every substep
-(requests that arrive join at the next substep; finished ones leave), and a
-new body is admitted when the arena and the HBM budget have room for it.
+flight together.  The batch of every substep is exactly the set of requests in
+flight: a request leaves at the substep it finishes, and requests that arrive
+join at the next native call (a call runs only as many substeps as no
+in-flight request finishes within and, with real-time arrivals, as fit before
+the next arrival).  A new body is admitted when the arena and the HBM budget
+have room for it.
 Per-body results do not depend on what else is in the batch -- scenes never
 exchange forces -- so every result equals the same requests run alone
 (tests/test_serve.py).
@@ -135,31 +138,34 @@ class _Job:
     def dt(self):
         return self.runs[self.pos][1]
 
-    def advance(self):
-        if self.init:
-            self.init = False
-            return False
-        self.left -= 1
-        if self.left == 0:
-            self.pos += 1
-            if self.pos < len(self.runs):
-                self.left = self.runs[self.pos][0]
-        return self.pos >= len(self.runs)
+    def span(self):
+        """Substeps this job can run at its current dt (its construction step
+        first, if it has not run yet)."""
+        return self.left + (1 if self.init else 0)
 
 
 class Server:
     """Continuous-batching request loop over resident bodies.
+
+    Each iteration runs K substeps in one native call (fw_step_served_n),
+    where K is the fewest substeps any in-flight request has left at its
+    current dt -- so a request leaves the batch at the very substep it
+    finishes -- and, with real-time arrivals, no more than fit before the next
+    arrival (from the measured device time per substep), so new requests join
+    within about one arrival gap.
 
     Args:
         make_body: body id -> list of domains (the scene of that body)
         budget_bytes: HBM budget for resident bodies (admission control)
         arena_*: arena capacities
         frame_dt: simulated time of one request (advanceWithTime(frame_dt))
-        max_inflight: substeps queued ahead of the GPU
+        max_inflight: native calls queued ahead of the GPU
+        max_batch_substeps: cap on K
     """
 
     def __init__(self, make_body, budget_bytes=150e9, arena_nodes=8_500_000, arena_elems=17_000_000,
-                 arena_bodies=4096, arena_scenes=4096, frame_dt=1.0 / 60.0, max_inflight=4, device=0):
+                 arena_bodies=4096, arena_scenes=4096, frame_dt=1.0 / 60.0, max_inflight=4, device=0,
+                 max_batch_substeps=64):
         import torch
 
         self.make_body = make_body
@@ -171,17 +177,22 @@ class Server:
         self.stream = torch.cuda.Stream(device=device)
         self.arena.native.set_stream(self.stream.cuda_stream)
         self.max_inflight = max_inflight
+        self.max_batch_substeps = int(max_batch_substeps)
+        self.us_per_substep = 20.0  # device time per substep, refined from events as calls complete
         self.resident = {}  # body -> scene
         self.used_bytes = 0
         self.body_bytes = {}
         self.deferred_admissions = 0
         self.element_steps = 0
+        self.admit_s = 0.0        # host time spent admitting new bodies
+        self.last_admit_t = 0.0   # run clock of the last admission
 
-    def _admit(self, body):
+    def _admit(self, body, t0=None):
         """True if resident now; "new" if admitted by this call; False if it
         does not fit (the request waits)."""
         if body in self.resident:
             return True
+        ta = time.perf_counter()
         doms = self.make_body(body)
         need = scene_device_bytes(SceneLayout(doms))
         if self.used_bytes + need > self.budget:
@@ -195,6 +206,10 @@ class Server:
         self.resident[body] = s
         self.body_bytes[body] = need
         self.used_bytes += need
+        tb = time.perf_counter()
+        self.admit_s += tb - ta
+        if t0 is not None:
+            self.last_admit_t = tb - t0
         return "new"
 
     def release(self, body):
@@ -205,58 +220,95 @@ class Server:
     def run(self, requests, realtime=True):
         """Serve ``requests`` (sorted by arrival).  With realtime, arrivals
         follow the wall clock; otherwise every request is present at t = 0.
-        Returns per-request latency (s), wall time and counters."""
+        Returns per-request latency (s), wall time and counters.
+
+        Per-scene job state lives in arrays (dt of the current run, substeps
+        left in it, busy / construction-step flags), so one iteration costs
+        O(scenes) vector work plus Python only for requests whose run ends."""
         import torch
 
         arrivals = list(requests)
         heapq.heapify(arrivals)
         queues = collections.defaultdict(collections.deque)  # body -> waiting requests
-        busy = {}  # scene -> job
-        dts = np.zeros(self.arena.S, dtype=np.float32)
+        ready = set()      # idle bodies with a waiting request
+        busy = {}          # scene -> job
+        busy_bodies = set()
+        S = self.arena.S
+        cur_dt = np.zeros(S, dtype=np.float32)
+        left = np.zeros(S, dtype=np.int64)        # substeps left at the current dt (construction step included)
+        busy_m = np.zeros(S, dtype=bool)
+        init_m = np.zeros(S, dtype=bool)
+        n_el = np.zeros(S, dtype=np.int64)
+        dts = np.zeros(S, dtype=np.float32)
         inflight = collections.deque()
         done_at = {}
-        pending_done = []  # (event, [jobs finished at that substep])
+        pending_done = []  # (event, [jobs finished in that call], start event, substeps)
         t0 = time.perf_counter()
         n_sub = 0
-        while arrivals or busy or any(queues.values()) or pending_done:
+        n_calls = 0
+        while arrivals or busy or ready or pending_done:
             now = time.perf_counter() - t0
             while arrivals and (not realtime or arrivals[0].arrival <= now):
                 r = heapq.heappop(arrivals)
                 queues[r.body].append(r)
+                if r.body not in busy_bodies:
+                    ready.add(r.body)
             # start the next request of every idle body that has one
-            busy_bodies = {j.req.body for j in busy.values()}
-            for body, q in queues.items():
-                if q and body not in busy_bodies:
-                    adm = self._admit(body)
-                    if not adm:
-                        continue
-                    s = self.resident[body]
-                    job = _Job(q.popleft(), self.frame_dt, self.arena.layouts[s].stableTime, init=(adm == "new"))
-                    job.start = now
-                    busy[s] = job
+            for body in sorted(ready):
+                adm = self._admit(body, t0)
+                if not adm:
+                    continue
+                s = self.resident[body]
+                job = _Job(queues[body].popleft(), self.frame_dt, self.arena.layouts[s].stableTime,
+                           init=(adm == "new"))
+                job.start = now
+                busy[s] = job
+                busy_bodies.add(body)
+                ready.discard(body)
+                cur_dt[s] = job.dt()
+                left[s] = job.span()
+                busy_m[s] = True
+                init_m[s] = job.init
+                n_el[s] = self.arena.layouts[s].n_elems
             if not busy:
-                if not arrivals and not pending_done and any(queues.values()):
+                if not arrivals and not pending_done and ready:
                     raise RuntimeError("requests wait for bodies that cannot be admitted (arena or budget full)")
                 # nothing on the GPU: retire finished work, then wait for the next arrival
                 self._retire(pending_done, done_at, t0, block=True)
                 if arrivals and realtime:
                     time.sleep(max(0.0, arrivals[0].arrival - (time.perf_counter() - t0)))
                 continue
-            dts[:] = 0.0
-            for s, job in busy.items():
-                dts[s] = job.dt()
-            self.arena.native.step_served(dts)
-            n_sub += 1
+            np.copyto(dts, np.where(busy_m, cur_dt, np.float32(0.0)))
+            span = int(min(self.max_batch_substeps, left[busy_m].min()))
+            if realtime and arrivals:
+                gap_us = (arrivals[0].arrival - (time.perf_counter() - t0)) * 1e6
+                span = min(span, max(1, int(gap_us / self.us_per_substep)))
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev0.record(self.stream)
+            self.arena.native.step_served_n(dts, span)
+            n_sub += span
+            n_calls += 1
+            self.element_steps += int(n_el[busy_m].sum()) * span - int(n_el[busy_m & init_m].sum())
+            init_m[busy_m] = False
+            left[busy_m] -= span
             finished = []
-            for s, job in list(busy.items()):
-                if not job.init:
-                    self.element_steps += self.arena.layouts[s].n_elems
-                if job.advance():
-                    finished.append(job)
-                    del busy[s]
-            ev = torch.cuda.Event()
+            for s in np.nonzero(busy_m & (left == 0))[0].tolist():
+                job = busy[s]
+                job.pos += 1
+                if job.pos < len(job.runs):  # next run of the same request, at its own dt
+                    cur_dt[s] = job.runs[job.pos][1]
+                    left[s] = job.runs[job.pos][0]
+                    continue
+                finished.append(job)
+                del busy[s]
+                busy_m[s] = False
+                body = job.req.body
+                busy_bodies.discard(body)
+                if queues[body]:
+                    ready.add(body)
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(self.stream)
-            pending_done.append((ev, finished))
+            pending_done.append((ev, finished, ev0, span))
             inflight.append(ev)
             if len(inflight) > self.max_inflight:
                 inflight.popleft().synchronize()
@@ -264,14 +316,14 @@ class Server:
         self._retire(pending_done, done_at, t0, block=True)
         wall = time.perf_counter() - t0
         lat = np.array([done_at[r.rid] - r.arrival if realtime else done_at[r.rid] for r in requests])
-        return {"latency_s": lat, "wall_s": wall, "substeps": n_sub, "element_steps": self.element_steps,
-                "deferred_admissions": self.deferred_admissions, "resident_bodies": len(self.resident),
-                "used_bytes": self.used_bytes}
+        return {"latency_s": lat, "wall_s": wall, "substeps": n_sub, "native_calls": n_calls,
+                "element_steps": self.element_steps, "deferred_admissions": self.deferred_admissions,
+                "resident_bodies": len(self.resident), "used_bytes": self.used_bytes,
+                "admit_s": self.admit_s, "last_admit_t": self.last_admit_t}
 
-    @staticmethod
-    def _retire(pending_done, done_at, t0, block):
+    def _retire(self, pending_done, done_at, t0, block):
         while pending_done:
-            ev, jobs = pending_done[0]
+            ev, jobs, ev0, span = pending_done[0]
             if block:
                 ev.synchronize()
             elif not ev.query():
@@ -279,6 +331,7 @@ class Server:
             t = time.perf_counter() - t0
             for j in jobs:
                 done_at[j.req.rid] = t
+            self.us_per_substep = 0.8 * self.us_per_substep + 0.2 * max(1.0, ev0.elapsed_time(ev) * 1e3 / span)
             pending_done.pop(0)
 
     def coords(self, body):

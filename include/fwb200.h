@@ -185,6 +185,12 @@ int fw_step_scenes(fw_ctx* ctx, int32_t n_steps, const float* dt_per_scene);
  * ExplicitLoop.advance calls of a request loop (explicitloop.py:473-555). */
 int fw_step_served(fw_ctx* ctx, const float* dt);
 
+/* n_steps substeps of fw_step_served with the same dt[] (one copy of dt and
+ * of the active set, then n_steps launches): a request loop calls it with
+ * n_steps no larger than the substeps any in-flight request has left at its
+ * current dt, so requests still leave the batch at the substep they finish. */
+int fw_step_served_n(fw_ctx* ctx, const float* dt, int32_t n_steps);
+
 /* Mark scenes active (1) / frozen (0).  Frozen scenes keep their state and do
  * not advance. */
 int fw_set_active(fw_ctx* ctx, const int32_t* active);
