@@ -500,6 +500,18 @@ def run_adjoint(args, rank, world, local):
     bwd_ms = [b.elapsed_time(c) for _, b, c in ev]
     evals, ms = shard.aggregate(args.steps, float(np.sum(fwd_ms) + np.sum(bwd_ms)))
     per_eval_s = ms / 1e3 / evals
+    # dot-product test at full size: adjoint of L = <w, x_T> against the tangent
+    rng_t = np.random.default_rng(77)
+    w = rng_t.standard_normal((sim.N, 2))
+    sim.forward(sim.E0, v0)
+    eb_w, vb_w, _ = sim.backward(w)
+    dot = []
+    for _ in range(2):
+        dE = (sim.E0 * rng_t.standard_normal(sim.E)).astype(np.float32)
+        dv = rng_t.standard_normal((sim.N, 2)).astype(np.float32)
+        _, dx = sim.jvp(sim.E0, v0, dE, dv)
+        a_e, a_v = float(np.dot(eb_w.astype(np.float64), dE)), float(np.sum(vb_w.astype(np.float64) * dv))
+        dot.append(abs(float(np.sum(w * dx.astype(np.float64))) - a_e - a_v) / (abs(a_e) + abs(a_v)))
     # the block must reach the plane: minimum height over the forward rollout
     probe = fw.ExplicitLoop(dt, build(), useAdapativeDT=False, path="gather", device=local)
     low = 1e9
@@ -517,7 +529,8 @@ def run_adjoint(args, rank, world, local):
                    "l2": "working set (8192 triangles) fits in L2; latency-bound rollout"},
         "adjoint": {"forward_ms": float(np.median(fwd_ms)), "backward_ms": float(np.median(bwd_ms)),
                     "forward_element_steps_per_s": sim.E * steps / (np.median(fwd_ms) / 1e3),
-                    "backward_over_forward": float(np.median(bwd_ms) / np.median(fwd_ms))},
+                    "backward_over_forward": float(np.median(bwd_ms) / np.median(fwd_ms)),
+                    "dot_product_test_max_rel": max(dot)},
         "e2e": {"value": args.steps / float(np.sum(walls)), "unit": "gradients/s",
                 "h2d_bytes_per_step": sim.N * 8 * 2 + sim.E * 4, "d2h_bytes_per_step": sim.N * 8 * 2 + sim.E * 4},
         "gpu_launches": launches, "clocks": clk.summary(),

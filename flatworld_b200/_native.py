@@ -58,6 +58,9 @@ _SIGNATURES = {
     "fw_adj_seed": (C.c_int, [_vp, _vp, _vp, C.c_int32]),
     "fw_adj_segment": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_adj_read": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32]),
+    "fw_tan_begin": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32]),
+    "fw_tan_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
+    "fw_tan_read": (C.c_int, [_vp, _vp, _vp, C.c_int32]),
     "fw_arena_init": (C.c_int, [_vp, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int64]),
     "fw_arena_commit": (C.c_int, [_vp, _i32p]),
     "fw_arena_remove": (C.c_int, [_vp, C.c_int32]),
@@ -227,6 +230,20 @@ class NativeWorld:
         eb = np.empty((n_elems,), np.float32)
         self._check(self._L.fw_adj_read(self._h, xb.ctypes.data, vb.ctypes.data, eb.ctypes.data, 0), "fw_adj_read")
         return xb, vb, eb
+
+    def tan_begin(self, dx0=None, dv0=None, dE=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (dx0, dv0, dE)]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        self._check(self._L.fw_tan_begin(self._h, ptrs[0], ptrs[1], ptrs[2], 0), "fw_tan_begin")
+
+    def tan_step(self, n_steps, dt):
+        self._check(self._L.fw_tan_step(self._h, int(n_steps), float(dt)), "fw_tan_step")
+
+    def tan_read(self, n_nodes):
+        dx = np.empty((n_nodes, 2), np.float32)
+        dv = np.empty((n_nodes, 2), np.float32)
+        self._check(self._L.fw_tan_read(self._h, dx.ctypes.data, dv.ctypes.data, 0), "fw_tan_read")
+        return dx, dv
 
     # ---- arena (served form)
     def arena_init(self, max_nodes, max_elems, max_bodies, max_scenes, max_pairs, max_heights, max_occ):

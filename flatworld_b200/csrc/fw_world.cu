@@ -336,7 +336,8 @@ struct Adj {
 
 // Adjoint of "v' = v + dt f / m; BC override" at every node: from (xb', vb')
 // form the force adjoint fb and the velocity adjoint of the previous substep.
-__device__ __forceinline__ void adj_node_prep(const Dev& d, const Adj& a, int i, float dt) {
+// With damping c, v' = v (1 - dt c / m) + dt f / m.
+__device__ __forceinline__ void adj_node_prep(const Dev& d, const Adj& a, int i, float dt, float damp) {
   const int bc = (int)(d.node_word[i] & fw::NODE_BC_MASK);
   const double2 xb = a.xb[i], vb = a.vb[i];
   const double h = (double)dt;
@@ -344,8 +345,9 @@ __device__ __forceinline__ void adj_node_prep(const Dev& d, const Adj& a, int i,
   const bool vfixed = (bc & (fw::BC_U | fw::BC_V)) != 0;
   const bool fdead = vfixed || (bc & fw::BC_A) != 0;
   const double s = h / (double)d.mass[i];
+  const double keep = 1.0 - s * (double)damp;
   a.fb[i] = fdead ? make_double2(0.0, 0.0) : make_double2(s * vt.x, s * vt.y);
-  a.vb[i] = vfixed ? make_double2(0.0, 0.0) : vt;
+  a.vb[i] = vfixed ? make_double2(0.0, 0.0) : make_double2(keep * vt.x, keep * vt.y);
 }
 
 __global__ void k_adj_seed(Adj a, int N, int has_x, int has_v) {
@@ -366,9 +368,9 @@ __global__ void k_adj_out(Adj a, int N, int E) {
   if (i < E) a.io_E[i] = (float)a.Eb[i];
 }
 
-__global__ void k_adj_prep(Dev d, Adj a, float dt) {
+__global__ void k_adj_prep(Dev d, Adj a, float dt, float damp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < d.N) adj_node_prep(d, a, i, dt);
+  if (i < d.N) adj_node_prep(d, a, i, dt, damp);
 }
 
 __global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
@@ -392,7 +394,7 @@ __global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
 // xb <- xb' + sum of element VJPs + plane-contact VJP; with prep, also the
 // force / velocity adjoints of the previous substep (fused, saves a launch).
 __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const int32_t* __restrict__ gates,
-                            float dt, int prep) {
+                            float dt, float damp, int prep) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.N) return;
   double2 xb = a.xb[i];
@@ -419,7 +421,93 @@ __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const in
     }
   }
   a.xb[i] = xb;
-  if (prep) adj_node_prep(d, a, i, dt);
+  if (prep) adj_node_prep(d, a, i, dt, damp);
+}
+
+// ------------------------------------------------------------------ tangent
+// Forward-mode derivative of the same substep along (dx, dv, dE), on the
+// recorded FP32 trajectory and gates: df = J(x) dx + f_e dE_e / E_e
+// (+ plane contact -k n (n . dx) while the node penetrates), then
+// dv' = dv (1 - dt c / m) + dt df / m (zero for fixed / enforced-velocity
+// nodes, no df for prescribed-acceleration nodes), dx' = dx + dt dv'.
+// Used to check that the adjoint is the exact transpose (dot-product test) and
+// for forward-mode gradients.
+struct Tan {
+  double2* dx;
+  double2* dv;
+  float* dE;     // perturbation of Young's modulus per element
+  float* young;  // Young's modulus per element
+  float2* xs;    // positions at the start of the substep
+  float2* io_x;  // FP32 staging for the C ABI
+  float2* io_v;
+};
+
+__global__ void k_tan_elements(Dev d, Tan t) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.E) return;
+  const ElemMat m = d.emat[e];
+  const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
+  const double2 u0 = t.dx[c0], u1 = t.dx[c1], u2 = t.dx[c2];
+  fw::Dual f[6];
+  fw::element_forces_jvp(t.xs[c0], t.xs[c1], t.xs[c2], make_float2((float)u0.x, (float)u0.y),
+                         make_float2((float)u1.x, (float)u1.y), make_float2((float)u2.x, (float)u2.y), d.jinv[e],
+                         fw::elem_type(m.word), m.lam, m.mu, m.area, f);
+  const float r = t.dE[e] / t.young[e];
+  d.corner[d.corner_pos[3 * e]] = make_float2(f[0].d + f[0].v * r, f[1].d + f[1].v * r);
+  d.corner[d.corner_pos[3 * e + 1]] = make_float2(f[2].d + f[2].v * r, f[3].d + f[3].v * r);
+  d.corner[d.corner_pos[3 * e + 2]] = make_float2(f[4].d + f[4].v * r, f[5].d + f[5].v * r);
+}
+
+__global__ void k_tan_nodes(Dev d, Tan t, float dt, float damp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const uint32_t w = d.node_word[i];
+  const int bc = (int)(w & fw::NODE_BC_MASK);
+  const double2 dx = t.dx[i], dv = t.dv[i];
+  double fx = 0.0, fy = 0.0;
+  if (w & fw::NODE_BOUNDARY) {
+    const int b = (int)(w >> fw::NODE_BODY_SHIFT);
+    const float2 xi = t.xs[i];
+    for (int q = 0; q < d.body_pair_cnt[b]; ++q) {
+      const int p = d.body_pair_off[b] + q;
+      if (!d.pair_active[p]) continue;
+      const Pair& pr = d.pairs[p];
+      const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
+      if (pen < 0.0f) {
+        const double s = -(double)pr.penalty * (pr.f[2] * dx.x + pr.f[3] * dx.y);
+        fx += s * pr.f[2];
+        fy += s * pr.f[3];
+      }
+    }
+  }
+  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
+    const float2 c = d.corner[k];
+    fx += c.x;
+    fy += c.y;
+  }
+  const double h = (double)dt, s = h / (double)d.mass[i], keep = 1.0 - s * (double)damp;
+  double2 nv;
+  if (bc & (fw::BC_U | fw::BC_V)) nv = make_double2(0.0, 0.0);
+  else if (bc & fw::BC_A) nv = make_double2(keep * dv.x, keep * dv.y);
+  else nv = make_double2(keep * dv.x + s * fx, keep * dv.y + s * fy);
+  t.dv[i] = nv;
+  t.dx[i] = make_double2(dx.x + h * nv.x, dx.y + h * nv.y);
+}
+
+__global__ void k_tan_seed(Tan t, int N, int has_x, int has_v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float2 x = has_x ? t.io_x[i] : make_float2(0.f, 0.f);
+  const float2 v = has_v ? t.io_v[i] : make_float2(0.f, 0.f);
+  t.dx[i] = make_double2(x.x, x.y);
+  t.dv[i] = make_double2(v.x, v.y);
+}
+
+__global__ void k_tan_out(Tan t, int N) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  t.io_x[i] = make_float2((float)t.dx[i].x, (float)t.dx[i].y);
+  t.io_v[i] = make_float2((float)t.dv[i].x, (float)t.dv[i].y);
 }
 
 // ------------------------------------------------------------------ energy
@@ -620,6 +708,7 @@ struct fw_ctx {
   // differentiable form
   Adj adj{};
   int adj_cap = 0;  // steps per segment the trajectory buffer holds
+  Tan tan{};
   float* d_poisson = nullptr;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
@@ -1834,12 +1923,13 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
   // (xb, vb) hold the adjoint of the segment's end state; the segment leaves
   // the adjoint of its start state there (the checkpoint it was restored from).
   const int gn = (N + kBlock - 1) / kBlock, ge = (E + kBlock - 1) / kBlock;
-  k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt);  // force / velocity adjoints of the last substep
+  const float damp = c->h_damp.empty() ? 0.0f : c->h_damp[0];
+  k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt, damp);  // force / velocity adjoints of the last substep
   c->launches += 1;
   for (int j = n_steps - 1; j >= 0; --j) {
     const float2* x = a.traj + (size_t)j * N;
     k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x);
-    k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt, j > 0);
+    k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt, damp, j > 0);
     c->launches += 2;
   }
   return check_kernel(c, "adjoint segment");
@@ -1855,6 +1945,65 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
   if (xbar) FW_CUDA(c, cudaMemcpyAsync(xbar, c->adj.io_x, sizeof(float2) * c->N, k, c->stream));
   if (vbar) FW_CUDA(c, cudaMemcpyAsync(vbar, c->adj.io_v, sizeof(float2) * c->N, k, c->stream));
   if (Ebar) FW_CUDA(c, cudaMemcpyAsync(Ebar, c->adj.io_E, sizeof(float) * c->E, k, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE, int32_t on_device) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized || c->arena || c->path != FW_PATH_GATHER || c->S != 1)
+    return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world on the gather path");
+  if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the tangent covers Elastic and NeoHookean triangles (no J2)");
+  for (const Pair& p : c->h_pairs)
+    if (p.kind != fw::PAIR_PLANE) return fail(c, FW_ERR_ARG, "the tangent covers plane contact only");
+  Tan& t = c->tan;
+  int rc;
+  if (!c->adj.young && (rc = upload(c, &c->adj.young, c->h_E))) return rc;
+  t.young = c->adj.young;
+  if (!t.dx) {
+    if ((rc = dalloc(c, &t.dx, c->N)) || (rc = dalloc(c, &t.dv, c->N)) || (rc = dalloc(c, &t.dE, c->E)) ||
+        (rc = dalloc(c, &t.xs, c->N)) || (rc = dalloc(c, &t.io_x, c->N)) || (rc = dalloc(c, &t.io_v, c->N)))
+      return rc;
+  }
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (dx0) FW_CUDA(c, cudaMemcpyAsync(t.io_x, dx0, sizeof(float2) * c->N, k, c->stream));
+  if (dv0) FW_CUDA(c, cudaMemcpyAsync(t.io_v, dv0, sizeof(float2) * c->N, k, c->stream));
+  if (dE) FW_CUDA(c, cudaMemcpyAsync(t.dE, dE, sizeof(float) * c->E, k, c->stream));
+  else FW_CUDA(c, cudaMemsetAsync(t.dE, 0, sizeof(float) * c->E, c->stream));
+  k_tan_seed<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(t, c->N, dx0 != nullptr, dv0 != nullptr);
+  c->launches += 1;
+  return check_kernel(c, "tangent seed");
+}
+
+int fw_tan_step(fw_ctx* c, int32_t n_steps, float dt) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->tan.dx) return fail(c, FW_ERR_STATE, "fw_tan_step before fw_tan_begin");
+  if (n_steps < 0) return fail(c, FW_ERR_ARG, "n_steps must be >= 0");
+  Tan& t = c->tan;
+  c->d.uniform_dt = 1;
+  c->d.dt_uniform = dt;
+  const float damp = c->h_damp.empty() ? 0.0f : c->h_damp[0];
+  const int gn = (c->N + kBlock - 1) / kBlock, ge = (c->E + kBlock - 1) / kBlock;
+  int rc;
+  for (int j = 0; j < n_steps; ++j) {
+    FW_CUDA(c, cudaMemcpyAsync(t.xs, c->d.x, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = launch_step(c))) return rc;  // the substep itself (sets this substep's gates)
+    c->host_counter += 1;
+    k_tan_elements<<<ge, kBlock, 0, c->stream>>>(c->d, t);
+    k_tan_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, t, dt, damp);
+    c->launches += 2;
+  }
+  return check_kernel(c, "tangent step");
+}
+
+int fw_tan_read(fw_ctx* c, float* dx, float* dv, int32_t on_device) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->tan.dx) return fail(c, FW_ERR_STATE, "fw_tan_read before fw_tan_begin");
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  k_tan_out<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->tan, c->N);
+  c->launches += 1;
+  if (dx) FW_CUDA(c, cudaMemcpyAsync(dx, c->tan.io_x, sizeof(float2) * c->N, k, c->stream));
+  if (dv) FW_CUDA(c, cudaMemcpyAsync(dv, c->tan.io_v, sizeof(float2) * c->N, k, c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   return FW_OK;
 }

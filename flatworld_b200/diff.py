@@ -28,8 +28,8 @@ from .world import PackedWorld, SceneLayout, build_native
 class DiffSim:
     """A single-scene rollout of ``n_steps`` substeps of ``dt`` with its adjoint."""
 
-    def __init__(self, domains, dt, n_steps, checkpoint_every=50, device=0):
-        self.layout = SceneLayout(domains, dt=dt, useAdapativeDT=False)
+    def __init__(self, domains, dt, n_steps, checkpoint_every=50, device=0, damping=0.0):
+        self.layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=False)
         self.packed = PackedWorld([self.layout])
         self.native = build_native(self.packed, device=device, path="gather")
         self.N, self.E = self.packed.N, self.packed.E
@@ -52,6 +52,19 @@ class DiffSim:
             self.native.step(n, self.dt)
         return self.native.read_nodes(_native.FW_FIELD_X, 0, self.N)
 
+    def jvp(self, young, v0, dE=None, dv0=None):
+        """Forward-mode derivative of the rollout: (x_T, dx_T) along the
+        moduli direction dE (per triangle) and velocity direction dv0."""
+        self.native.set_element_young(np.asarray(young, np.float32))
+        self.native.restore(0)
+        self.native.write_nodes(_native.FW_FIELD_V, 0, np.asarray(v0, np.float32).reshape(self.N, 2))
+        self.native.tan_begin(None, None if dv0 is None else np.asarray(dv0, np.float32).reshape(self.N, 2),
+                              None if dE is None else np.asarray(dE, np.float32))
+        self.native.tan_step(self.n_steps, self.dt)
+        x = self.native.read_nodes(_native.FW_FIELD_X, 0, self.N)
+        dx, _ = self.native.tan_read(self.N)
+        return x, dx
+
     def backward(self, xbar_T, vbar_T=None):
         """Reverse the last forward rollout from dL/dx_T (and dL/dv_T);
         returns (dL/dE per triangle, dL/dv0 per node, dL/dx0 per node)."""
@@ -72,7 +85,10 @@ try:
 
         @staticmethod
         def forward(ctx, young, v0, sim):
-            x = sim.forward(young.detach().cpu().numpy(), v0.detach().cpu().numpy())
+            ctx.young = young.detach().cpu().numpy()
+            ctx.v0 = v0.detach().cpu().numpy()
+            ctx.device = young.device
+            x = sim.forward(ctx.young, ctx.v0)
             ctx.sim = sim
             return torch.from_numpy(x).to(young.device)
 
@@ -81,6 +97,14 @@ try:
             eb, vb, _ = ctx.sim.backward(grad_x.detach().cpu().numpy())
             dev = grad_x.device
             return torch.from_numpy(eb).to(dev), torch.from_numpy(vb).to(dev), None
+
+        @staticmethod
+        def jvp(ctx, young_t, v0_t, sim_t):
+            """Forward-mode AD (torch.func.jvp / forward_ad) through the tangent."""
+            sim = ctx.sim
+            _, dx = sim.jvp(ctx.young, ctx.v0, None if young_t is None else young_t.detach().cpu().numpy(),
+                            None if v0_t is None else v0_t.detach().cpu().numpy())
+            return torch.from_numpy(dx).to(ctx.device)
 
 except ImportError:  # pragma: no cover
     FEMRollout = None

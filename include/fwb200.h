@@ -309,6 +309,19 @@ int fw_adj_seed(fw_ctx* ctx, const float* xbar, const float* vbar, int32_t on_de
 int fw_adj_segment(fw_ctx* ctx, int32_t n_steps, float dt);
 int fw_adj_read(fw_ctx* ctx, float* xbar, float* vbar, float* Ebar, int32_t on_device);
 
+/* Forward-mode derivative (tangent) of a rollout along (dx0, dv0, dE), carried
+ * with the substeps themselves on the same trajectory and gates as the
+ * adjoint; no reference counterpart.
+ *   fw_tan_begin(ctx, dx0, dv0, dE)  tangent of the current state (NULL = 0)
+ *   fw_tan_step(ctx, n, dt)          n substeps of dt, state and tangent
+ *   fw_tan_read(ctx, dx, dv)         tangent of positions and velocities
+ * <w, dx_T> equals the adjoint's <dL/dE, dE> + <dL/dv0, dv0> + <dL/dx0, dx0>
+ * for L = <w, x_T> up to rounding (the dot-product test of the adjoint).
+ * Same scope as the adjoint. */
+int fw_tan_begin(fw_ctx* ctx, const float* dx0, const float* dv0, const float* dE, int32_t on_device);
+int fw_tan_step(fw_ctx* ctx, int32_t n_steps, float dt);
+int fw_tan_read(fw_ctx* ctx, float* dx, float* dv, int32_t on_device);
+
 /* Library build identification string (arch, flags). */
 const char* fw_build_info(void);
 

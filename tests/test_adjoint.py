@@ -18,8 +18,8 @@ from tests import scenes
 pytestmark = pytest.mark.gpu
 
 
-def rollout64(domains_fn, young, v0, steps, dt):
-    o = oracle.OracleLoop(domains_fn(young), dt, useAdapativeDT=False, precision="f64", threads=8)
+def rollout64(domains_fn, young, v0, steps, dt, damping=0.0):
+    o = oracle.OracleLoop(domains_fn(young), dt, damping=damping, useAdapativeDT=False, precision="f64", threads=8)
     o.set_state(None, v0)
     o.advance(steps)
     return o.state()[0]
@@ -32,7 +32,7 @@ def perturbed(p0, d, eps):
     return hi, lo, (hi.astype(np.float64) - lo.astype(np.float64)) / (2.0 * eps)
 
 
-def directional_errors(sim, build, v0, steps, dt, seed_fn, loss_fn, n_dirs, seed, eps=1e-4):
+def directional_errors(sim, build, v0, steps, dt, seed_fn, loss_fn, n_dirs, seed, eps=1e-4, damping=0.0):
     """Relative error |adj - fd| / |fd| along random directions: n_dirs in
     the moduli (dE) and n_dirs in the initial velocities (dv), each checked
     on its own (a mixed direction's two parts can cancel, which magnifies
@@ -40,7 +40,7 @@ def directional_errors(sim, build, v0, steps, dt, seed_fn, loss_fn, n_dirs, seed
     the GPU rollout and from the FP64 oracle rollout of the unperturbed
     inputs."""
     x32 = sim.forward(sim.E0, v0)
-    x64 = rollout64(build, sim.E0, v0, steps, dt)
+    x64 = rollout64(build, sim.E0, v0, steps, dt, damping)
     eb, vb, _ = sim.backward(seed_fn(x32, x64))
     rng = np.random.default_rng(seed)
     errs = []
@@ -53,7 +53,8 @@ def directional_errors(sim, build, v0, steps, dt, seed_fn, loss_fn, n_dirs, seed
             vp, vm, dv = perturbed(v0, rng.standard_normal((sim.N, 2)), eps)
             Ep = Em = sim.E0
             adj = float(np.sum(vb.astype(np.float64) * dv))
-        fd = (loss_fn(rollout64(build, Ep, vp, steps, dt)) - loss_fn(rollout64(build, Em, vm, steps, dt))) / (2 * eps)
+        fd = (loss_fn(rollout64(build, Ep, vp, steps, dt, damping))
+              - loss_fn(rollout64(build, Em, vm, steps, dt, damping))) / (2 * eps)
         errs.append(abs(adj - fd) / max(abs(fd), 1e-30))
     return errs
 
@@ -106,6 +107,45 @@ def test_adjoint_of_linear_functional():
     errs = directional_errors(sim, build, v0, steps, dt, lambda *xs: w, lambda x: float(np.sum(w * x)), 2, seed=1)
     print("relative error of directional derivatives:", errs)
     assert max(errs) < 1e-3, errs
+
+
+def test_adjoint_with_damping_matches_fp64_central_differences():
+    """Velocity damping c enters the update as v' = v (1 - dt c / m) + dt f / m."""
+    dt, steps, c = 1e-4, 600, 0.05
+    build = lambda y=None: scenes.gradient_block_scene(fw, n=12, side=0.12, bottom=0.04, young=y, seed=4)  # noqa: E731
+    sim = DiffSim(build(), dt, steps, checkpoint_every=50, damping=c)
+    v0 = np.tile(np.array([0.0, -2.0], np.float32), (sim.N, 1))
+    w = np.random.default_rng(11).standard_normal((sim.N, 2))
+    errs = directional_errors(sim, build, v0, steps, dt, lambda *xs: w, lambda x: float(np.sum(w * x)), 2, seed=2,
+                              damping=c)
+    print("relative error of directional derivatives (damping):", errs)
+    assert max(errs) < 1e-3, errs
+
+
+@pytest.mark.parametrize("damping", [0.0, 0.05])
+def test_adjoint_is_the_transpose_of_the_tangent(damping):
+    """Dot-product test on one FP32 trajectory: for L = <w, x_T>, the adjoint's
+    <dL/dE, dE> + <dL/dv0, dv0> equals <w, dx_T> of the forward-mode tangent
+    along (dE, dv0) to rounding (1e-5 of the terms' magnitude), for
+    directions in E only, v0 only and both; with plane contact."""
+    dt, steps = 1e-4, 600
+    build = lambda y=None: scenes.gradient_block_scene(fw, n=12, side=0.12, bottom=0.04, young=y, seed=6)  # noqa: E731
+    sim = DiffSim(build(), dt, steps, checkpoint_every=50, damping=damping)
+    rng = np.random.default_rng(21)
+    v0 = (np.tile([0.0, -2.0], (sim.N, 1)) + 0.3 * rng.standard_normal((sim.N, 2))).astype(np.float32)
+    w = rng.standard_normal((sim.N, 2))
+    sim.forward(sim.E0, v0)
+    eb, vb, _ = sim.backward(w)
+    for kind in ("E", "v", "both"):
+        dE = (sim.E0 * rng.standard_normal(sim.E)).astype(np.float32) if kind != "v" else np.zeros(sim.E, np.float32)
+        dv = rng.standard_normal((sim.N, 2)).astype(np.float32) if kind != "E" else np.zeros((sim.N, 2), np.float32)
+        _, dx = sim.jvp(sim.E0, v0, dE, dv)
+        tangent = float(np.sum(w * dx.astype(np.float64)))
+        a_e = float(np.dot(eb.astype(np.float64), dE))
+        a_v = float(np.sum(vb.astype(np.float64) * dv))
+        err = abs(tangent - (a_e + a_v)) / (abs(a_e) + abs(a_v))
+        print(f"dot-product test ({kind}, damping {damping}): tangent {tangent:.9e} adjoint {a_e + a_v:.9e} rel {err:.2e}")
+        assert err < 1e-5, (kind, tangent, a_e + a_v)
 
 
 def test_checkpoint_interval_does_not_change_gradients():
