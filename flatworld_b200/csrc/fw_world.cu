@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
 // The node's own state, its CSR range and its first kNodeCorners corner
 // forces are loaded before the scene lookup, so one node waits on few
 // dependent loads; the corners are then summed in the same ascending order.
-constexpr int kNodeCorners = 8;
+constexpr int kNodeCorners = 6;  // an interior node of a structured triangulation has 6
 
 __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
   const uint32_t w = valid ? d.node_word[i] : 0u;
