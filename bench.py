@@ -328,6 +328,22 @@ def run_batched(args, rank, world, local):
                      "traffic_note": "DRAM bytes per substep scaled from an ncu capture of a 256-body batch"},
         "gpu_launches": launches, "clocks": clk.summary(),
     }
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        work, t_cpu, bodies = 0, 0.0, 0
+        for i in pick[:8]:  # a bounded sample: 8 of the same bodies, 100 substeps each
+            o = oracle.OracleLoop(scenes.ragged_batch_one(fw, int(i), seed=rank), 5e-5, useAdapativeDT=False,
+                                  precision="f32", threads=threads)
+            t1 = time.perf_counter()
+            o.advance(100)
+            t_cpu += time.perf_counter() - t1
+            work += o.E * 100
+            bodies += 1
+        line["cpu_baseline"] = {"value": work / t_cpu, "unit": "element-steps/s", "cores": threads, "kind": "port",
+                                "sample": f"{bodies} bodies of the batch x 100 substeps, FP32 C restatement of the "
+                                          f"reference scheme, {threads} threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -359,8 +375,10 @@ def run_served(args, rank, world, local):
     Server(lambda b: scenes.ragged_batch_one(fw, 10_000 + b), arena_nodes=200_000, arena_elems=400_000,
            arena_bodies=64, arena_scenes=64, device=local).run(warm, realtime=False)
     barrier(dist)
+    l0 = srv.arena.native.launch_count()
     with ClockSampler(local) as clk:
         out = srv.run(reqs, realtime=True)
+    launches = srv.arena.native.launch_count() - l0
     # capacity: the requests of the first 10 s all queued at t = 0 (a fresh server)
     cap_reqs = [r for r in reqs if r.arrival < 10.0]
     cap_srv = Server(lambda b: population[b], budget_bytes=150e9, device=local)
@@ -405,7 +423,7 @@ def run_served(args, rank, world, local):
                        "element_steps_per_s": fo["element_steps"] / fo["wall_s"],
                        "latency_ms": {"p50": percentile_ms(flat, 50) if len(flat) else None,
                                       "p99": percentile_ms(flat, 99) if len(flat) else None}},
-        "clocks": clk.summary(),
+        "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -678,9 +696,11 @@ def main():
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             rate, n = cpu_oracle_rate(fw, args.mesh, args.cpu_seconds, threads)
+            rate1, n1 = cpu_oracle_rate(fw, args.mesh, args.cpu_seconds / 2, 1)
             line["cpu_baseline"] = {"value": rate, "unit": "element-steps/s", "cores": threads, "kind": "port",
                                     "sample": f"{n} substeps of the same workload, FP32 C restatement of the "
-                                              f"reference scheme, {threads} threads"}
+                                              f"reference scheme, {threads} threads",
+                                    "one_thread": {"value": rate1, "sample": f"{n1} substeps, 1 thread"}}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
