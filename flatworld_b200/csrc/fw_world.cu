@@ -649,8 +649,10 @@ struct fw_ctx {
   std::vector<int32_t> cur_active;
   Dev d{};
   std::vector<void*> allocs;
-  // captured graphs of kGraphSteps substeps, keyed by (uniform flag, dt bits)
+  // captured step graphs, keyed by (uniform flag, substeps, dt bits); the
+  // adjoint's recompute / reverse graphs, keyed by (kind, substeps, dt bits)
   std::vector<std::pair<uint64_t, cudaGraphExec_t>> graphs;
+  std::vector<std::pair<uint64_t, cudaGraphExec_t>> adj_graphs;
   cudaStream_t graph_stream = nullptr;
   int grid_e = 1, grid_n = 1;
   int block_e = kBlock, block_n = kBlock, grid_e_cap = 0, sms = 148;
@@ -795,37 +797,59 @@ int launch_step(fw_ctx* c) {
 void drop_graphs(fw_ctx* c) {
   for (auto& g : c->graphs) cudaGraphExecDestroy(g.second);
   c->graphs.clear();
+  for (auto& g : c->adj_graphs) cudaGraphExecDestroy(g.second);
+  c->adj_graphs.clear();
 }
 
-int get_graph(fw_ctx* c, cudaGraphExec_t* out) {
+// A graph of the work `body` queues on the context stream, cached under key
+// in cache.  A graph holds the world descriptor and buffer addresses it was
+// captured with, so caches are dropped when those change.
+template <class Body>
+int cached_graph(fw_ctx* c, std::vector<std::pair<uint64_t, cudaGraphExec_t>>& cache, uint64_t key, Body body,
+                 cudaGraphExec_t* out) {
   if (c->graph_stream != c->stream) {
     drop_graphs(c);
     c->graph_stream = c->stream;
   }
-  uint32_t bits;
-  memcpy(&bits, &c->d.dt_uniform, sizeof(bits));
-  const uint64_t key = ((uint64_t)(c->d.uniform_dt ? 1 : 0) << 32) | (c->d.uniform_dt ? bits : 0u);
-  for (auto& g : c->graphs)
+  for (auto& g : cache)
     if (g.first == key) {
       *out = g.second;
       return FW_OK;
     }
-  if (c->graphs.size() >= 8) drop_graphs(c);
+  if (cache.size() >= 16) {
+    for (auto& g : cache) cudaGraphExecDestroy(g.second);
+    cache.clear();
+  }
   cudaGraph_t g = nullptr;
   FW_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int k = 0; k < kGraphSteps; ++k) {
-    k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
-    k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
-  }
+  body();
   cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
   if (ce != cudaSuccess) return fail(c, FW_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
   cudaGraphExec_t exec = nullptr;
   ce = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) return fail(c, FW_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
-  c->graphs.push_back({key, exec});
+  cache.push_back({key, exec});
   *out = exec;
   return FW_OK;
+}
+
+uint32_t float_bits(float v) {
+  uint32_t bits;
+  memcpy(&bits, &v, sizeof(bits));
+  return bits;
+}
+
+// Graph of n substeps (n <= kGraphSteps) of the gather step.
+int get_graph(fw_ctx* c, int n, cudaGraphExec_t* out) {
+  const uint64_t key = ((uint64_t)(c->d.uniform_dt ? 1 : 0) << 63) | ((uint64_t)n << 32) |
+                       (c->d.uniform_dt ? float_bits(c->d.dt_uniform) : 0u);
+  return cached_graph(c, c->graphs, key, [&] {
+    for (int k = 0; k < n; ++k) {
+      k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
+      k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+    }
+  }, out);
 }
 
 int launch_resident(fw_ctx* c, int n);
@@ -839,13 +863,20 @@ int run_steps(fw_ctx* c, int n) {
   c->host_counter += n;
   if (n >= kGraphSteps) {
     cudaGraphExec_t g = nullptr;
-    rc = get_graph(c, &g);
+    rc = get_graph(c, kGraphSteps, &g);
     if (rc) return rc;
     while (n >= kGraphSteps) {
       FW_CUDA(c, cudaGraphLaunch(g, c->stream));
       c->launches += 2 * kGraphSteps;
       n -= kGraphSteps;
     }
+  }
+  if (n >= 2) {  // the remainder as one graph too
+    cudaGraphExec_t g = nullptr;
+    if ((rc = get_graph(c, n, &g))) return rc;
+    FW_CUDA(c, cudaGraphLaunch(g, c->stream));
+    c->launches += 2 * n;
+    n = 0;
   }
   for (int k = 0; k < n && rc == FW_OK; ++k) rc = launch_step(c);
   return rc;
@@ -1844,8 +1875,9 @@ int fw_arena_scene_info(fw_ctx* c, int32_t s, int64_t* info) {
 
 int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* young, int32_t on_device) {
   if (!c || !young) return FW_ERR_ARG;
-  if (!c->finalized || c->arena || c->path != FW_PATH_GATHER)
-    return fail(c, FW_ERR_STATE, "fw_set_element_young needs a finalized world on the gather path");
+  // (the resident step loads the Lame constants at every launch, so both paths see the change)
+  if (!c->finalized || c->arena)
+    return fail(c, FW_ERR_STATE, "fw_set_element_young needs a finalized world (not an arena)");
   if (first < 0 || count < 0 || (int64_t)first + count > c->E) return fail(c, FW_ERR_ARG, "element range out of bounds");
   if (count == 0) return FW_OK;
   int rc;
@@ -1861,8 +1893,10 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
 
 int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
   if (!c) return FW_ERR_ARG;
-  if (!c->finalized || c->arena || c->path != FW_PATH_GATHER || c->S != 1)
-    return fail(c, FW_ERR_STATE, "the adjoint needs a finalized single-scene world on the gather path");
+  // The forward may run on either path (identical bits); the recompute and the
+  // reverse use the gather kernels and data, which every non-arena world has.
+  if (!c->finalized || c->arena || c->S != 1)
+    return fail(c, FW_ERR_STATE, "the adjoint needs a finalized single-scene world (not an arena)");
   if (max_segment_steps <= 0) return fail(c, FW_ERR_ARG, "max_segment_steps must be > 0");
   if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the adjoint covers Elastic and NeoHookean triangles (no J2)");
   for (const Pair& p : c->h_pairs)
@@ -1879,6 +1913,7 @@ int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
       return rc;
   }
   if (c->adj_cap < max_segment_steps) {
+    drop_graphs(c);  // graphs hold the old trajectory buffers
     if ((rc = dalloc(c, &a.traj, (size_t)max_segment_steps * c->N)) ||
         (rc = dalloc(c, &a.gates, (size_t)max_segment_steps * std::max(1, c->d.P))))
       return rc;
@@ -1911,27 +1946,39 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
   c->d.uniform_dt = 1;
   c->d.dt_uniform = dt;
   int rc;
+  const uint64_t key_lo = ((uint64_t)n_steps << 32) | float_bits(dt);
   // recompute the segment from the current state, recording positions and gates
-  for (int j = 0; j < n_steps; ++j) {
-    FW_CUDA(c, cudaMemcpyAsync(a.traj + (size_t)j * N, c->d.x, sizeof(float2) * N, cudaMemcpyDeviceToDevice, c->stream));
-    if ((rc = launch_step(c))) return rc;
-    c->host_counter += 1;
-    if (c->d.P > 0)
-      FW_CUDA(c, cudaMemcpyAsync(a.gates + (size_t)j * P, c->d.pair_active, sizeof(int32_t) * c->d.P,
-                                 cudaMemcpyDeviceToDevice, c->stream));
-  }
+  cudaGraphExec_t g_fwd = nullptr;
+  rc = cached_graph(c, c->adj_graphs, (1ull << 62) | key_lo, [&] {
+    for (int j = 0; j < n_steps; ++j) {
+      cudaMemcpyAsync(a.traj + (size_t)j * N, c->d.x, sizeof(float2) * N, cudaMemcpyDeviceToDevice, c->stream);
+      k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
+      k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+      if (c->d.P > 0)
+        cudaMemcpyAsync(a.gates + (size_t)j * P, c->d.pair_active, sizeof(int32_t) * c->d.P,
+                        cudaMemcpyDeviceToDevice, c->stream);
+    }
+  }, &g_fwd);
+  if (rc) return rc;
+  FW_CUDA(c, cudaGraphLaunch(g_fwd, c->stream));
+  c->host_counter += n_steps;
+  c->launches += 2 * n_steps;
   // (xb, vb) hold the adjoint of the segment's end state; the segment leaves
   // the adjoint of its start state there (the checkpoint it was restored from).
   const int gn = (N + kBlock - 1) / kBlock, ge = (E + kBlock - 1) / kBlock;
   const float damp = c->h_damp.empty() ? 0.0f : c->h_damp[0];
-  k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt, damp);  // force / velocity adjoints of the last substep
-  c->launches += 1;
-  for (int j = n_steps - 1; j >= 0; --j) {
-    const float2* x = a.traj + (size_t)j * N;
-    k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x);
-    k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt, damp, j > 0);
-    c->launches += 2;
-  }
+  cudaGraphExec_t g_rev = nullptr;
+  rc = cached_graph(c, c->adj_graphs, (2ull << 62) | key_lo, [&] {
+    k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt, damp);  // force / velocity adjoints of the last substep
+    for (int j = n_steps - 1; j >= 0; --j) {
+      const float2* x = a.traj + (size_t)j * N;
+      k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x);
+      k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt, damp, j > 0);
+    }
+  }, &g_rev);
+  if (rc) return rc;
+  FW_CUDA(c, cudaGraphLaunch(g_rev, c->stream));
+  c->launches += 1 + 2 * n_steps;
   return check_kernel(c, "adjoint segment");
 }
 
@@ -1951,8 +1998,8 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
 
 int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE, int32_t on_device) {
   if (!c) return FW_ERR_ARG;
-  if (!c->finalized || c->arena || c->path != FW_PATH_GATHER || c->S != 1)
-    return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world on the gather path");
+  if (!c->finalized || c->arena || c->S != 1)
+    return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world (not an arena)");
   if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the tangent covers Elastic and NeoHookean triangles (no J2)");
   for (const Pair& p : c->h_pairs)
     if (p.kind != fw::PAIR_PLANE) return fail(c, FW_ERR_ARG, "the tangent covers plane contact only");

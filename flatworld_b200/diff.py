@@ -6,7 +6,8 @@ modulus and initial velocities, by a hand-written adjoint of the FEM substep
     x_T = FEMRollout.apply(E, v0, sim)       # torch tensors, E per triangle, v0 per node
     loss = ((x_T - target) ** 2).sum(); loss.backward()   # E.grad, v0.grad
 
-Forward: the rollout runs on the GPU (gather path) and stores the state at
+Forward: the rollout runs on the GPU (the resident step when the mesh fits on
+chip, else the gather step) and stores the state at
 the start of every segment of ``checkpoint_every`` substeps (fw_snapshot).
 Backward: for each segment, last first, the checkpoint is restored, the
 segment is recomputed with its positions and broad-phase gates recorded, and
@@ -31,7 +32,10 @@ class DiffSim:
     def __init__(self, domains, dt, n_steps, checkpoint_every=50, device=0, damping=0.0):
         self.layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=False)
         self.packed = PackedWorld([self.layout])
-        self.native = build_native(self.packed, device=device, path="gather")
+        # forward on the resident step when the mesh fits on chip (one launch per
+        # segment); the adjoint recomputes segments with the gather kernels,
+        # which give the same bits
+        self.native = build_native(self.packed, device=device, path="auto")
         self.N, self.E = self.packed.N, self.packed.E
         self.dt = float(np.float32(dt))
         self.n_steps = int(n_steps)

@@ -290,7 +290,7 @@ int fw_arena_remove(fw_ctx* ctx, int32_t scene);
 int fw_arena_scene_info(fw_ctx* ctx, int32_t scene, int64_t* info);
 
 /* Differentiable form.  fw_set_element_young: new per-element Young's moduli
- * for elements [first, first+count) (Lame constants recomputed; gather path).
+ * for elements [first, first+count) (Lame constants recomputed; either step path).
  * The reference stores E per element (femspringmanager.py:584, 753) but has no
  * setter or adjoint.  Reverse pass of a rollout of dt-substeps:
  *   fw_adj_begin(ctx, K)      adjoint buffers for segments of up to K substeps
