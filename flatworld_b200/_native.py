@@ -80,6 +80,8 @@ _SIGNATURES = {
     "fw_read_reference_shape": (C.c_int, [_vp, _f32p, _f32p]),
     "fw_read_counters": (C.c_int, [_vp, _i64p]),
     "fw_energy": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "fw_scene_status": (C.c_int, [_vp, _vp, C.c_int32]),
+    "fw_clear_scene_status": (C.c_int, [_vp, C.c_int32]),
     "fw_launch_count": (C.c_int64, [_vp]),
     "fw_build_info": (C.c_char_p, []),
     "fw_step_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp,
@@ -351,6 +353,18 @@ class NativeWorld:
         out = np.zeros((n_scenes, 4), dtype=np.float64)
         self._check(self._L.fw_energy(self._h, out.ctypes.data_as(C.POINTER(C.c_double))), "fw_energy")
         return out
+
+    def scene_status(self, n_scenes: int, out=None, asynchronous=False):
+        """Per-scene non-finite flags (int32).  With asynchronous=True the copy
+        is only queued: pass pinned memory (e.g. a pinned torch tensor's numpy
+        view) and read it after the stream has passed this point."""
+        if out is None:
+            out = np.zeros((n_scenes,), dtype=np.int32)
+        self._check(self._L.fw_scene_status(self._h, out.ctypes.data, 1 if asynchronous else 0), "fw_scene_status")
+        return out
+
+    def clear_scene_status(self, scene: int = -1):
+        self._check(self._L.fw_clear_scene_status(self._h, int(scene)), "fw_clear_scene_status")
 
     def launch_count(self) -> int:
         return int(self._L.fw_launch_count(self._h))

@@ -223,6 +223,7 @@ __device__ __forceinline__ float2 res_node(const Dev& d, const ResSmem& s, const
     f.y += c.y;
   }
   fw::integrate_im((int)(w & fw::NODE_BC_MASK), f, s.m[i], s.im[i], s.bcv[i], dt, damp, x, v);
+  if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) d.scene_bad[0] = 1;  // one scene
   s.x[i] = x;
   s.v[i] = v;
   return x;

@@ -72,6 +72,7 @@ struct Dev {
   int32_t* scene_active;
   int32_t* scene_mode_req;
   int32_t* scene_mode;
+  int32_t* scene_bad;  // set to 1 when a node of the scene gets a non-finite position or velocity
   int32_t* aabb_ring;  // [2][B][4] ordered ints
   int N, E, B, S, P;
   int has_j2;
@@ -221,6 +222,7 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
     fw::integrate(bc, f, mass, bv, dt, damp, x, v);
     d.x[i] = x;
     d.v[i] = v;
+    if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) d.scene_bad[s] = 1;
   }
   // Per-body AABB of boundary nodes (femspringmanager.py:361-408).
   const unsigned full = 0xFFFFFFFFu;
@@ -1459,8 +1461,10 @@ int fw_finalize(fw_ctx* c) {
       (rc = upload(c, &d.occ, c->h_occ)) || (rc = dalloc(c, &d.scene_dt, S)) ||
       (rc = upload(c, &d.scene_damp, c->h_damp)) || (rc = dalloc(c, &d.scene_counter, S)) ||
       (rc = dalloc(c, &d.scene_active, S)) || (rc = dalloc(c, &d.scene_mode_req, S)) ||
-      (rc = dalloc(c, &d.scene_mode, S)) || (rc = dalloc(c, &d.aabb_ring, 8 * (size_t)B)))
+      (rc = dalloc(c, &d.scene_mode, S)) || (rc = dalloc(c, &d.aabb_ring, 8 * (size_t)B)) ||
+      (rc = dalloc(c, &d.scene_bad, S)))
     return rc;
+  FW_CUDA(c, cudaMemsetAsync(d.scene_bad, 0, sizeof(int32_t) * S, c->stream));
   FW_CUDA(c, cudaMemsetAsync(d.j2state, 0, sizeof(float4) * (has_j2 ? E : 1), c->stream));
   FW_CUDA(c, cudaMemsetAsync(d.pair_active, 0, sizeof(int32_t) * (pairs.empty() ? 1 : pairs.size()), c->stream));
   FW_CUDA(c, cudaMemsetAsync(d.scene_dt, 0, sizeof(float) * S, c->stream));
@@ -1620,8 +1624,9 @@ int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_b
       (rc = dalloc(c, &d.scene_counter, S)) || (rc = dalloc(c, &d.scene_active, S)) ||
       (rc = dalloc(c, &d.scene_mode_req, S)) || (rc = dalloc(c, &d.scene_mode, S)) ||
       (rc = dalloc(c, &d.aabb_ring, 8 * (size_t)B)) || (rc = dalloc(c, &c->a_young, E)) ||
-      (rc = dalloc(c, &c->a_poisson, E)) || (rc = dalloc(c, &c->a_rho, E)))
+      (rc = dalloc(c, &c->a_poisson, E)) || (rc = dalloc(c, &c->a_rho, E)) || (rc = dalloc(c, &d.scene_bad, S)))
     return rc;
+  FW_CUDA(c, cudaMemsetAsync(d.scene_bad, 0, sizeof(int32_t) * S, c->stream));
   c->chunk_cap = E / 32 + N / 32 + 2 * (int64_t)S + 16;
   if ((rc = dalloc(c, &c->d_echunks, c->chunk_cap)) || (rc = dalloc(c, &c->d_nchunks, c->chunk_cap))) return rc;
   std::vector<int32_t> dead(B, S - 1);
@@ -1786,7 +1791,8 @@ int fw_arena_commit(fw_ctx* c, int32_t* scene_out) {
   const float damp = c->h_damp.empty() ? 0.f : c->h_damp[0];
   const int32_t one = 1, zero = 0;
   if ((rc = up(d.scene_damp + s, &damp, sizeof(float))) || (rc = up(d.scene_counter + s, &zero, sizeof(int32_t))) ||
-      (rc = up(d.scene_mode_req + s, &one, sizeof(int32_t))) || (rc = up(d.scene_active + s, &one, sizeof(int32_t))))
+      (rc = up(d.scene_mode_req + s, &one, sizeof(int32_t))) || (rc = up(d.scene_active + s, &one, sizeof(int32_t))) ||
+      (rc = up(d.scene_bad + s, &zero, sizeof(int32_t))))
     return rc;
   const int e_lo = (int)a.e0, e_hi = (int)(a.e0 + Es), n_lo = (int)a.n0, n_hi = (int)(a.n0 + Ns);
   k_prepare_elements<<<(int)((Es + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->a_young + a.e0, c->a_poisson + a.e0,
@@ -1817,6 +1823,7 @@ int fw_arena_remove(fw_ctx* c, int32_t s) {
   const int32_t zero = 0;
   FW_CUDA(c, cudaMemcpyAsync(c->d.body_scene + a.b0, dead.data(), sizeof(int32_t) * a.nb, cudaMemcpyHostToDevice, c->stream));
   FW_CUDA(c, cudaMemcpyAsync(c->d.scene_active + s, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_bad + s, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   for (int64_t b = 0; b < a.nb; ++b) c->a_body_scene[a.b0 + b] = c->S - 1;
   c->fl_nodes.give(a.n0, a.nn);
@@ -2255,6 +2262,23 @@ int fw_energy(fw_ctx* c, double* out) {
     out[4 * sc + 2] += res[g].z;
     out[4 * sc + 3] += res[g].w;
   }
+  return FW_OK;
+}
+
+int fw_scene_status(fw_ctx* c, int32_t* bad, int32_t async) {
+  if (!c || !bad) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_scene_status before fw_finalize");
+  FW_CUDA(c, cudaMemcpyAsync(bad, c->d.scene_bad, sizeof(int32_t) * c->S, cudaMemcpyDeviceToHost, c->stream));
+  if (!async) FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
+int fw_clear_scene_status(fw_ctx* c, int32_t scene) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_clear_scene_status before fw_finalize");
+  if (scene < -1 || scene >= c->S) return fail(c, FW_ERR_ARG, "scene %d out of range", scene);
+  if (scene < 0) FW_CUDA(c, cudaMemsetAsync(c->d.scene_bad, 0, sizeof(int32_t) * c->S, c->stream));
+  else FW_CUDA(c, cudaMemsetAsync(c->d.scene_bad + scene, 0, sizeof(int32_t), c->stream));
   return FW_OK;
 }
 

@@ -124,11 +124,12 @@ def request_substeps(req, frame_dt, stable_time):
 
 
 class _Job:
-    __slots__ = ("req", "runs", "pos", "left", "start", "init")
+    __slots__ = ("req", "runs", "pos", "left", "start", "init", "failed")
 
     def __init__(self, req, frame_dt, stable_time, init=False):
         self.req = req
         self.init = init  # the body was just admitted: its first launch is the zero-dt construction step
+        self.failed = False  # its body's state turned non-finite before it was retired
         sub = frame_dt / request_substeps(req, frame_dt, stable_time)
         self.runs = substep_schedule(frame_dt, sub, sub, False)
         self.pos = 0
@@ -186,6 +187,7 @@ class Server:
         self.element_steps = 0
         self.admit_s = 0.0        # host time spent admitting new bodies
         self.last_admit_t = 0.0   # run clock of the last admission
+        self.evicted = 0          # bodies removed because their state turned non-finite
 
     def _admit(self, body, t0=None):
         """True if resident now; "new" if admitted by this call; False if it
@@ -242,10 +244,41 @@ class Server:
         dts = np.zeros(S, dtype=np.float32)
         inflight = collections.deque()
         done_at = {}
-        pending_done = []  # (event, [jobs finished in that call], start event, substeps)
+        failed = {}  # rid -> run clock when the request was failed (its body's state turned non-finite)
+        pending_done = []  # (event, [jobs finished in that call], start event, substeps, status slot)
+        # per-call copies of the non-finite flags, read when the call retires
+        ring = 2 * self.max_inflight + 4
+        status = torch.zeros((ring, S), dtype=torch.int32, pin_memory=True).numpy()
+        slot = 0
         t0 = time.perf_counter()
         n_sub = 0
         n_calls = 0
+
+        def evict(bad_scenes):
+            """Fail the requests of bodies whose state turned non-finite and
+            remove the bodies (a later request admits them afresh)."""
+            scene_body = {sc: b for b, sc in self.resident.items()}
+            now_ = time.perf_counter() - t0
+            for sc in bad_scenes:
+                body = scene_body.get(int(sc))
+                if body is None:
+                    continue
+                job = busy.pop(int(sc), None)
+                if job is not None:
+                    failed[job.req.rid] = now_
+                    busy_m[sc] = False
+                    busy_bodies.discard(body)
+                for r in queues[body]:
+                    failed[r.rid] = now_
+                queues[body].clear()
+                for entry in pending_done:  # finished in calls not yet retired: ran on the broken state
+                    for j in entry[1]:
+                        if j.req.body == body:
+                            j.failed = True
+                ready.discard(body)
+                self.release(body)  # waits for the stream, clears the flag
+                status[:, sc] = 0   # copies queued before the release must not flag the slot's next body
+                self.evicted += 1
         while arrivals or busy or ready or pending_done:
             now = time.perf_counter() - t0
             while arrivals and (not realtime or arrivals[0].arrival <= now):
@@ -274,7 +307,7 @@ class Server:
                 if not arrivals and not pending_done and ready:
                     raise RuntimeError("requests wait for bodies that cannot be admitted (arena or budget full)")
                 # nothing on the GPU: retire finished work, then wait for the next arrival
-                self._retire(pending_done, done_at, t0, block=True)
+                evict(self._retire(pending_done, done_at, failed, status, t0, block=True))
                 if arrivals and realtime:
                     time.sleep(max(0.0, arrivals[0].arrival - (time.perf_counter() - t0)))
                 continue
@@ -286,6 +319,7 @@ class Server:
             ev0 = torch.cuda.Event(enable_timing=True)
             ev0.record(self.stream)
             self.arena.native.step_served_n(dts, span)
+            self.arena.native.scene_status(S, out=status[slot], asynchronous=True)
             n_sub += span
             n_calls += 1
             self.element_steps += int(n_el[busy_m].sum()) * span - int(n_el[busy_m & init_m].sum())
@@ -308,31 +342,43 @@ class Server:
                     ready.add(body)
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(self.stream)
-            pending_done.append((ev, finished, ev0, span))
+            pending_done.append((ev, finished, ev0, span, slot))
+            slot = (slot + 1) % ring
             inflight.append(ev)
             if len(inflight) > self.max_inflight:
                 inflight.popleft().synchronize()
-            self._retire(pending_done, done_at, t0, block=False)
-        self._retire(pending_done, done_at, t0, block=True)
+            evict(self._retire(pending_done, done_at, failed, status, t0, block=False))
+        evict(self._retire(pending_done, done_at, failed, status, t0, block=True))
         wall = time.perf_counter() - t0
-        lat = np.array([done_at[r.rid] - r.arrival if realtime else done_at[r.rid] for r in requests])
+        ends = {**done_at, **failed}
+        lat = np.array([ends[r.rid] - r.arrival if realtime else ends[r.rid] for r in requests])
         return {"latency_s": lat, "wall_s": wall, "substeps": n_sub, "native_calls": n_calls,
+                "failed": sorted(failed), "evicted_bodies": self.evicted,
                 "element_steps": self.element_steps, "deferred_admissions": self.deferred_admissions,
                 "resident_bodies": len(self.resident), "used_bytes": self.used_bytes,
                 "admit_s": self.admit_s, "last_admit_t": self.last_admit_t}
 
-    def _retire(self, pending_done, done_at, t0, block):
+    def _retire(self, pending_done, done_at, failed, status, t0, block):
+        """Retire completed calls in order; returns the scenes whose state
+        turned non-finite in them (their finished requests count as failed)."""
+        bad = set()
         while pending_done:
-            ev, jobs, ev0, span = pending_done[0]
+            ev, jobs, ev0, span, slot = pending_done[0]
             if block:
                 ev.synchronize()
             elif not ev.query():
                 break
             t = time.perf_counter() - t0
+            flagged = set(np.nonzero(status[slot])[0].tolist())
+            bad |= flagged
             for j in jobs:
-                done_at[j.req.rid] = t
+                if j.failed or self.resident.get(j.req.body) in flagged:
+                    failed[j.req.rid] = t
+                else:
+                    done_at[j.req.rid] = t
             self.us_per_substep = 0.8 * self.us_per_substep + 0.2 * max(1.0, ev0.elapsed_time(ev) * 1e3 / span)
             pending_done.pop(0)
+        return bad
 
     def coords(self, body):
         return self.arena.coords(self.resident[body])

@@ -224,6 +224,17 @@ int fw_read_reference_shape(fw_ctx* ctx, float* area, float* jinv);
 /* Per-scene step counters (number of advance() calls since finalize). */
 int fw_read_counters(fw_ctx* ctx, int64_t* counters);
 
+/* Non-finite detection: bad[s] = 1 once a node of scene s got a NaN/inf
+ * position or velocity in a step (n_scenes entries; arena: max_scenes + 1).
+ * The step sets the flag and carries on -- scenes never exchange forces, so a
+ * broken scene cannot spoil the others; a request loop evicts it.  async = 1
+ * only queues the copy (bad must then be pinned host memory, valid once the
+ * stream reaches this point); async = 0 waits for it.  fw_clear_scene_status
+ * clears scene s (s = -1: all).  The reference has no such check (it raises
+ * only on buffer overflow, femspringmanager.py:708-730). */
+int fw_scene_status(fw_ctx* ctx, int32_t* bad, int32_t async);
+int fw_clear_scene_status(fw_ctx* ctx, int32_t scene);
+
 /* Total energy per scene, reduced in FP64 on the device (deterministic order):
  * out[4 s + 0..3] = kinetic, strain, external potential (gravity -m g.x or
  * constant nodal force -f.x), contact penalty (1/2 k sd^2 of every

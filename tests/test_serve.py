@@ -47,6 +47,42 @@ def test_served_results_equal_alone():
         assert np.array_equal(srv.arena.velocities(srv.resident[body]), v), body
 
 
+def exploding_body(i):
+    """A soft NeoHookean block thrown apart by random 50 m/s nodal velocities:
+    its triangles fold over (J <= 0) within a few substeps and the state turns
+    non-finite -- the same on the FP32 oracle."""
+    conn, coords = fw.structured_rectangle(12, 12, 0.12, 0.12, origin=(0.0, 0.0))
+    v0 = np.random.default_rng(5).normal(0.0, 50.0, size=coords.shape)
+    ics = [fw.InitialVel([k], v0[k]) for k in range(coords.shape[0])]
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.HyperElastic(1e4, 0.45, 1000.0)), [],
+                       initials=ics)
+    return [fem]
+
+
+def test_nonfinite_body_is_evicted_and_others_are_untouched():
+    """A body whose state turns NaN is flagged on the device, its requests fail,
+    it is removed from the arena, and the other bodies' results are the same
+    bits as alone."""
+    body_fn = lambda b: exploding_body(b) if b == 4 else small_body(b)  # noqa: E731
+    reqs = [Request(0.0, k, k % 5, 40) for k in range(15)]
+    srv = Server(body_fn, arena_nodes=60_000, arena_elems=120_000, arena_bodies=64, arena_scenes=64)
+    out = srv.run(reqs, realtime=False)
+    bad = {r.rid for r in reqs if r.body == 4}
+    assert set(out["failed"]) == bad
+    assert out["evicted_bodies"] == 1 and 4 not in srv.resident
+    for body in range(4):
+        x, v = alone(body, [r for r in reqs if r.body == body])
+        assert np.array_equal(srv.coords(body), x), body
+    # the flag itself, through the C ABI on a plain loop (both step paths)
+    for path in ("gather", "resident"):
+        lp = fw.ExplicitLoop(0.0, exploding_body(0), useAdapativeDT=True, path=path)
+        assert lp._native.scene_status(1)[0] == 0
+        lp.advance_n(200)
+        assert lp._native.scene_status(1)[0] == 1, path
+        lp._native.clear_scene_status(0)
+        assert lp._native.scene_status(1)[0] == 0
+
+
 def test_arena_reuses_ranges_after_remove():
     ar = Arena(40_000, 80_000, 16, 16, 16, 1 << 16, 1 << 20)
     a = ar.insert(small_body(0), dt=5e-5)
