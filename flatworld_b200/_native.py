@@ -28,6 +28,8 @@ FW_OPT_BLOCK_ELEMS = 2
 FW_OPT_BLOCK_NODES = 3
 FW_OPT_GRID_ELEMS = 4
 FW_OPT_RES_SYNC = 5
+FW_OPT_WAIT_LIMIT = 6
+FW_OPT_TEST_WITHHOLD = 7
 
 _lock = threading.Lock()
 _lib = None

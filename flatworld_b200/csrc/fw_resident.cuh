@@ -79,6 +79,8 @@ struct Res {
   unsigned long long* bll;  // [2][B][P][4] flag-in-data partial boxes (epoch << 32 | ordered int)
   int* bar;                 // arrivals counter (reset by the prologue)
   int* err;                 // != 0: a wait gave up
+  long long wait_limit;     // polls before a wait gives up (kPollLimit / kSpinLimit unless set)
+  int withhold_cta;         // test hook: this CTA skips its first publish (-1: none)
   int P, no_max, nh_max, ne_max, ncsr_max;
   int has_j2;
   int tab_h, tab_o;         // ground tables staged in shared memory (floats, bytes)
@@ -319,7 +321,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
             wx = ll_load(w);
             wy = ll_load(w + 1);
             if (ll_has(wx, want) && ll_has(wy, want)) break;
-            if ((++it & 1023) == 0 && (it > kPollLimit || *(volatile int*)r.err)) {
+            if ((++it & 1023) == 0 && (it > r.wait_limit || *(volatile int*)r.err)) {
               atomicExch(r.err, 1);
               s_abort = 1;
               break;
@@ -338,7 +340,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
             b2 = ll_load(w + 2);
             b3 = ll_load(w + 3);
             if (ll_has(b0, want) && ll_has(b1, want) && ll_has(b2, want) && ll_has(b3, want)) break;
-            if ((++it & 1023) == 0 && (it > kPollLimit || *(volatile int*)r.err)) {
+            if ((++it & 1023) == 0 && (it > r.wait_limit || *(volatile int*)r.err)) {
               atomicExch(r.err, 1);
               s_abort = 1;
               break;
@@ -356,7 +358,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           long long it = 0;
           const int target = r.P * k;
           while (ld_acquire(r.bar) < target) {
-            if (++it > kSpinLimit || *(volatile int*)r.err) {
+            if (++it > r.wait_limit || *(volatile int*)r.err) {
               atomicExch(r.err, 1);
               s_abort = 1;
               break;
@@ -407,7 +409,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           body = (int)(w >> fw::NODE_BODY_SHIFT);
           bnd = (w & fw::NODE_BOUNDARY) != 0;
           const int gid = s.gid[i];
-          if (gid < 0) {
+          if (gid < 0 && !(k == 0 && (int)blockIdx.x == r.withhold_cta)) {
             const size_t gi = (size_t)(gid & 0x7FFFFFFF);
             if (LL) {
               ll_store(dll + 2 * gi, ll_pack(ep_out, __float_as_uint(x.x)));
@@ -443,13 +445,14 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
         }
       }
       named_bar(1, FT);
+      const bool withhold = k == 0 && (int)blockIdx.x == r.withhold_cta;
       if (LL) {
-        if (t < 4 * B) {  // this CTA's partial box of body t / 4, component t % 4
+        if (t < 4 * B && !withhold) {  // this CTA's partial box of body t / 4, component t % 4
           unsigned long long* bdst = r.bll + ((size_t)((k + 1) & 1) * B * r.P + (size_t)(t >> 2) * r.P + blockIdx.x) * 4;
           ll_store(bdst + (t & 3), ll_pack(ep_out, (uint32_t)s_pbox[t]));
           s_pbox[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
         }
-      } else if (t == 0) {
+      } else if (t == 0 && !withhold) {
         cuda::atomic_ref<int, cuda::thread_scope_device> a(*r.bar);
         a.fetch_add(1, cuda::memory_order_release);
       }

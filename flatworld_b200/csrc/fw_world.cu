@@ -718,6 +718,8 @@ struct fw_ctx {
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
   int res_sync = 0;          // FW_OPT_RES_SYNC
+  int64_t wait_limit = 0;    // FW_OPT_WAIT_LIMIT (0: the built-in limits)
+  int withhold_cta = -1;     // FW_OPT_TEST_WITHHOLD
   // fw_energy scratch (plain cudaMalloc, freed in fw_destroy)
   EnergyChunk* d_echunk = nullptr;
   double4* d_epart = nullptr;
@@ -1101,6 +1103,8 @@ int launch_resident(fw_ctx* c, int n) {
   }
   uint32_t ep0 = c->res_epoch;
   c->res_epoch += (uint32_t)n + 1u;
+  c->res.wait_limit = c->wait_limit > 0 ? c->wait_limit : (ll ? kPollLimit : kSpinLimit);
+  c->res.withhold_cta = c->withhold_cta;
   k_res_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, ll ? 1 : 0);
   float dt = c->d.dt_uniform, damp = c->h_damp[0];
   void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&step0, (void*)&n, (void*)&dt, (void*)&damp, (void*)&ep0};
@@ -1540,6 +1544,14 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
       drop_graphs(c);
       return FW_OK;
     }
+    case FW_OPT_WAIT_LIMIT:
+      if (value < 0) return fail(c, FW_ERR_ARG, "FW_OPT_WAIT_LIMIT must be >= 0");
+      c->wait_limit = value;
+      return FW_OK;
+    case FW_OPT_TEST_WITHHOLD:
+      if (value < -1) return fail(c, FW_ERR_ARG, "FW_OPT_TEST_WITHHOLD must be >= -1");
+      c->withhold_cta = value;
+      return FW_OK;
     case FW_OPT_RES_SYNC: {
       if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_RES_SYNC after fw_finalize");
       if (value != 0 && value != 1) return fail(c, FW_ERR_ARG, "FW_OPT_RES_SYNC must be 0 or 1");

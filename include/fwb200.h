@@ -154,6 +154,14 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
  * 1 = arrival counter + release fence (any number of bodies).  Set before
  * fw_finalize.  Both give identical results. */
 #define FW_OPT_RES_SYNC 5
+/* FW_OPT_WAIT_LIMIT: polls a resident CTA makes before a cross-CTA wait gives
+ * up (0 = built-in: 2^22 flag-in-data, 2^26 counter); then the launch ends
+ * early and the next synchronising call returns FW_ERR_TIMEOUT.
+ * FW_OPT_TEST_WITHHOLD: test hook -- resident CTA n withholds its first
+ * publish, so the others' waits run out (-1 = off).  Both may be set at any
+ * time; they apply from the next launch. */
+#define FW_OPT_WAIT_LIMIT 6
+#define FW_OPT_TEST_WITHHOLD 7
 int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
 
 /* Checkpoint / resume: copy the whole step state (positions, velocities, J2
