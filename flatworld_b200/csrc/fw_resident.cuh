@@ -81,6 +81,9 @@ struct Res {
   int* err;                 // != 0: a wait gave up
   long long wait_limit;     // polls before a wait gives up (kPollLimit / kSpinLimit unless set)
   int withhold_cta;         // test hook: this CTA skips its first publish (-1: none)
+  float2* rec_x;            // if set: positions at the start of each substep, [nsteps][N] (adjoint recompute)
+  int* rec_gates;           // if set: broad-phase gates of each substep, [nsteps][rec_stride]
+  int rec_stride;
   int P, no_max, nh_max, ne_max, ncsr_max;
   int has_j2;
   int tab_h, tab_o;         // ground tables staged in shared memory (floats, bytes)
@@ -303,6 +306,8 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
   constexpr int FT = FRONT * 32;
   const bool front = t < FT;
   const int BT = T - FT, bt = t - FT;
+  if (r.rec_x)
+    for (int i = t; i < P.no; i += T) r.rec_x[s.gid[i] & 0x7FFFFFFF] = s.x[i];
   if (!front)
     for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
   const int g1_trips = (P.n_g1 + FT - 1) / FT;
@@ -383,6 +388,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           else
             bb = __ldcg(reinterpret_cast<const int4*>(r.aabb3 + ((size_t)(g % 3) * B + pr.body) * 4));
           s.gate[t] = fw::pair_gate(pr, fw::ord2f(bb.x), fw::ord2f(bb.y), fw::ord2f(bb.z), fw::ord2f(bb.w), g) ? 1 : 0;
+          if (r.rec_gates && blockIdx.x == 0) r.rec_gates[(size_t)k * r.rec_stride + t] = s.gate[t];
         }
         if (!LL && blockIdx.x == 0)
           for (int b = t; b < B; b += FT) aabb_reset(r.aabb3 + ((size_t)((g + 2) % 3) * B + b) * 4);
@@ -460,6 +466,8 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
       for (int i = P.n_g1 + bt; i < P.no; i += BT) res_node(d, s, heights, occ, i, dt, damp);
     }
     __syncthreads();  // every owned node of substep k is updated
+    if (r.rec_x && k + 1 < nsteps)  // owned positions stay as they are until the next CTA barrier
+      for (int i = t; i < P.no; i += T) r.rec_x[(size_t)(k + 1) * N + (s.gid[i] & 0x7FFFFFFF)] = s.x[i];
     if (!front && k + 1 < nsteps)
       for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
   }
@@ -473,6 +481,205 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
   if (r.has_j2)
     for (int q = t; q < P.ne; q += T)
       if ((s.conn[q].y >> 16) & kJ2Writer) d.j2state[r.eid[P.elem_off + q]] = s.j2[q];
+}
+
+// ------------------------------------------------------------------ resident adjoint
+// Reverse pass of one segment on the same patches (cooperative launch): the
+// adjoint state of the owned nodes (xb, vb, fb in FP64) and dL/dE of the
+// triangles whose first corner the patch owns stay in shared memory; the
+// positions of each substep come from the recorded trajectory.  Per reverse
+// substep the only cross-CTA traffic is the force adjoint of exported nodes,
+// published as flag-in-data words (each FP64 value as two 32-bit halves, each
+// with the epoch); halo membership is symmetric, so neighbours stay within one
+// substep of each other and two parity slots suffice.  The arithmetic and its
+// order are those of k_adj_prep / k_adj_elements / k_adj_nodes, so both
+// reverse passes give the same bits.
+struct ResAdjSmem {
+  double2* xb;
+  double2* vb;
+  double2* fb;  // owned, then halo
+  double* Eb;
+  float* yng;
+};
+
+__host__ __device__ inline size_t res_adj_layout(const Res& r, unsigned char* base, ResAdjSmem* s) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* p = base ? base + o : nullptr;
+    o += res_align(bytes);
+    return p;
+  };
+  ResAdjSmem t;
+  t.xb = (double2*)take(sizeof(double2) * r.no_max);
+  t.vb = (double2*)take(sizeof(double2) * r.no_max);
+  t.fb = (double2*)take(sizeof(double2) * (size_t)(r.no_max + r.nh_max));
+  t.Eb = (double*)take(sizeof(double) * r.ne_max);
+  t.yng = (float*)take(sizeof(float) * r.ne_max);
+  if (s) *s = t;
+  return o;
+}
+
+__device__ __forceinline__ void res_adj_prep(const ResSmem& s, const ResAdjSmem& q, int i, double h, double damp) {
+  const int bc = (int)(s.w[i] & fw::NODE_BC_MASK);
+  const double2 xb = q.xb[i], vb = q.vb[i];
+  const double2 vt = make_double2(vb.x + h * xb.x, vb.y + h * xb.y);
+  const bool vfixed = (bc & (fw::BC_U | fw::BC_V)) != 0;
+  const bool fdead = vfixed || (bc & fw::BC_A) != 0;
+  const double sc = h / (double)s.m[i];
+  const double keep = 1.0 - sc * damp;
+  q.fb[i] = fdead ? make_double2(0.0, 0.0) : make_double2(sc * vt.x, sc * vt.y);
+  q.vb[i] = vfixed ? make_double2(0.0, 0.0) : make_double2(keep * vt.x, keep * vt.y);
+}
+
+__device__ __forceinline__ uint32_t lo32(double v) { return (uint32_t)(__double_as_longlong(v) & 0xFFFFFFFFll); }
+__device__ __forceinline__ uint32_t hi32(double v) { return (uint32_t)((unsigned long long)__double_as_longlong(v) >> 32); }
+__device__ __forceinline__ double join64(uint32_t lo, uint32_t hi) {
+  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
+}
+
+__global__ void __launch_bounds__(kResThreads, 1)
+k_res_adj(Dev d, Res r, Adj a, const float2* __restrict__ rec_x, const int* __restrict__ rec_gates,
+          int gate_stride, unsigned long long* fll, int nsteps, float dt, float damp, uint32_t ep0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_abort;
+  ResSmem s;
+  const size_t base = res_layout(r, smem_raw, &s);
+  ResAdjSmem q;
+  res_adj_layout(r, smem_raw + base, &q);
+  const ResPatch P = r.patch[blockIdx.x];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int N = d.N;
+  // ---- load the patch and its adjoint state
+  for (int k = t; k < P.ne; k += T) {
+    const int e = r.eid[P.elem_off + k];
+    s.jinv[k] = d.jinv[e];
+    s.mat[k] = d.emat[e];
+    s.conn[k] = r.conn[P.elem_off + k];
+    q.yng[k] = a.young[e];
+    q.Eb[k] = ((s.conn[k].y >> 16) & kJ2Writer) ? a.Eb[e] : 0.0;
+  }
+  for (int i = t; i < P.no; i += T) {
+    const int g = r.nodes[P.node_off + i];
+    const int gi = g & 0x7FFFFFFF;
+    s.gid[i] = g;
+    s.m[i] = d.mass[gi];
+    s.w[i] = d.node_word[gi];
+    q.xb[i] = a.xb[gi];
+    q.vb[i] = a.vb[gi];
+  }
+  for (int i = t; i < P.nh; i += T) s.hidx[i] = r.halo[P.halo_off + i];
+  for (int i = t; i <= P.no; i += T) s.csrp[i] = (uint16_t)r.csr_ptr[P.csr_ptr_off + i];
+  for (int i = t; i < P.ncsr; i += T) s.csrs[i] = r.csr_slot[P.csr_off + i];
+  for (int i = t; i < d.P; i += T) s.pairs[i] = d.pairs[i];
+  for (int b = t; b < d.B; b += T) {
+    s.bpo[b] = d.body_pair_off[b];
+    s.bpc[b] = d.body_pair_cnt[b];
+  }
+  if (t == 0) s_abort = 0;
+  __syncthreads();
+  const double h = (double)dt, dmp = (double)damp;
+  for (int i = t; i < P.no; i += T) res_adj_prep(s, q, i, h, dmp);  // the segment's last substep
+  __syncthreads();
+  for (int rr = 0; rr < nsteps; ++rr) {
+    const int j = nsteps - 1 - rr;
+    const uint32_t ep = ep0 + (uint32_t)rr + 1u;
+    unsigned long long* slot = fll + (size_t)(rr & 1) * N * 4;
+    // publish the force adjoints others read; positions of substep j
+    for (int i = t; i < P.no; i += T) {
+      const int g = s.gid[i];
+      const int gi = g & 0x7FFFFFFF;
+      s.x[i] = rec_x[(size_t)j * N + gi];
+      if (g < 0) {
+        const double2 f = q.fb[i];
+        unsigned long long* w = slot + 4 * (size_t)gi;
+        ll_store(w, ll_pack(ep, lo32(f.x)));
+        ll_store(w + 1, ll_pack(ep, hi32(f.x)));
+        ll_store(w + 2, ll_pack(ep, lo32(f.y)));
+        ll_store(w + 3, ll_pack(ep, hi32(f.y)));
+      }
+    }
+    for (int k = t; k < P.nh; k += T) {
+      const int gi = s.hidx[k];
+      s.x[P.no + k] = rec_x[(size_t)j * N + gi];
+      const unsigned long long* w = slot + 4 * (size_t)gi;
+      unsigned long long w0, w1, w2, w3;
+      long long it = 0;
+      while (true) {
+        w0 = ll_load(w);
+        w1 = ll_load(w + 1);
+        w2 = ll_load(w + 2);
+        w3 = ll_load(w + 3);
+        if (ll_has(w0, ep) && ll_has(w1, ep) && ll_has(w2, ep) && ll_has(w3, ep)) break;
+        if ((++it & 1023) == 0 && (it > r.wait_limit || *(volatile int*)r.err)) {
+          atomicExch(r.err, 1);
+          s_abort = 1;
+          break;
+        }
+      }
+      q.fb[P.no + k] = make_double2(join64((uint32_t)w0, (uint32_t)w1), join64((uint32_t)w2, (uint32_t)w3));
+    }
+    __syncthreads();
+    if (s_abort) break;
+    // element Jacobian products with the force adjoints (as k_adj_elements)
+    for (int k = t; k < P.ne; k += T) {
+      const uint2 c = s.conn[k];
+      const int i0 = c.x & 0xFFFFu, i1 = c.x >> 16, i2 = c.y & 0xFFFFu;
+      const double2 b0 = q.fb[i0], b1 = q.fb[i1], b2 = q.fb[i2];
+      const float2 w0 = make_float2((float)b0.x, (float)b0.y), w1 = make_float2((float)b1.x, (float)b1.y),
+                   w2 = make_float2((float)b2.x, (float)b2.y);
+      const ElemMat m = s.mat[k];
+      fw::Dual f[6];
+      fw::element_forces_jvp(s.x[i0], s.x[i1], s.x[i2], w0, w1, w2, s.jinv[k], fw::elem_type(m.word), m.lam, m.mu,
+                             m.area, f);
+      s.f[3 * k] = make_float2(f[0].d, f[1].d);
+      s.f[3 * k + 1] = make_float2(f[2].d, f[3].d);
+      s.f[3 * k + 2] = make_float2(f[4].d, f[5].d);
+      if ((c.y >> 16) & kJ2Writer) {
+        const double dot = b0.x * f[0].v + b0.y * f[1].v + b1.x * f[2].v + b1.y * f[3].v + b2.x * f[4].v +
+                           b2.y * f[5].v;
+        q.Eb[k] += dot / (double)q.yng[k];
+      }
+    }
+    __syncthreads();
+    // xb += element VJPs + plane contact; then the previous substep's adjoints (as k_adj_nodes)
+    for (int i = t; i < P.no; i += T) {
+      double2 xb = q.xb[i];
+      const double2 fb = q.fb[i];
+      for (int k = s.csrp[i]; k < s.csrp[i + 1]; ++k) {
+        const float2 c = s.f[s.csrs[k]];
+        xb.x += c.x;
+        xb.y += c.y;
+      }
+      const uint32_t w = s.w[i];
+      if (w & fw::NODE_BOUNDARY) {
+        const int b = (int)(w >> fw::NODE_BODY_SHIFT);
+        const float2 xi = s.x[i];
+        for (int k = 0; k < s.bpc[b]; ++k) {
+          const int p = s.bpo[b] + k;
+          if (!rec_gates[(size_t)j * gate_stride + p]) continue;
+          const Pair& pr = s.pairs[p];
+          const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
+          if (pen < 0.0f) {
+            const double tt = -(double)pr.penalty * (pr.f[2] * fb.x + pr.f[3] * fb.y);
+            xb.x += tt * pr.f[2];
+            xb.y += tt * pr.f[3];
+          }
+        }
+      }
+      q.xb[i] = xb;
+      if (j > 0) res_adj_prep(s, q, i, h, dmp);
+    }
+    __syncthreads();
+  }
+  // ---- write the adjoint state back
+  __syncthreads();
+  for (int i = t; i < P.no; i += T) {
+    const int gi = s.gid[i] & 0x7FFFFFFF;
+    a.xb[gi] = q.xb[i];
+    a.vb[gi] = q.vb[i];
+  }
+  for (int k = t; k < P.ne; k += T)
+    if ((s.conn[k].y >> 16) & kJ2Writer) a.Eb[r.eid[P.elem_off + k]] = q.Eb[k];
 }
 
 using ResKernel = void (*)(Dev, Res, int, int, float, float, uint32_t);

@@ -713,6 +713,9 @@ struct fw_ctx {
   Adj adj{};
   int adj_cap = 0;  // steps per segment the trajectory buffer holds
   Tan tan{};
+  bool res_adj = false;            // the reverse pass runs resident (k_res_adj)
+  size_t res_adj_smem = 0;
+  unsigned long long* fll = nullptr;  // [2][N][4] flag-in-data force adjoints of the reverse pass
   float* d_poisson = nullptr;
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
@@ -1938,6 +1941,27 @@ int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
       return rc;
     c->adj_cap = max_segment_steps;
   }
+  // Resident reverse pass when the world runs resident and the adjoint state fits on chip too.
+  if (c->path == FW_PATH_RESIDENT && !c->res_adj) {
+    int optin = 0, sms = 148;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const size_t need = res_layout(c->res, nullptr, nullptr) + res_adj_layout(c->res, nullptr, nullptr);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_res_adj);
+    int per_sm = 0;
+    if ((long)need + (long)fa.sharedSizeBytes + 64 <= optin &&
+        cudaFuncSetAttribute(k_res_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - (int)fa.sharedSizeBytes) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_res_adj, kResThreads, need) == cudaSuccess &&
+        per_sm * sms >= c->res.P) {
+      if ((rc = dalloc(c, &c->fll, 8 * (size_t)c->N))) return rc;
+      FW_CUDA(c, cudaMemsetAsync(c->fll, 0, sizeof(unsigned long long) * 8 * (size_t)c->N, c->stream));
+      c->res_adj = true;
+      c->res_adj_smem = need;
+    }
+    cudaGetLastError();
+  }
   FW_CUDA(c, cudaMemsetAsync(a.Eb, 0, sizeof(double) * c->E, c->stream));
   FW_CUDA(c, cudaMemsetAsync(a.xb, 0, sizeof(double2) * c->N, c->stream));
   FW_CUDA(c, cudaMemsetAsync(a.vb, 0, sizeof(double2) * c->N, c->stream));
@@ -1965,6 +1989,35 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
   c->d.uniform_dt = 1;
   c->d.dt_uniform = dt;
   int rc;
+  if (c->res_adj) {
+    // recompute on the resident step, recording positions and gates, then the resident reverse
+    c->res.rec_x = a.traj;
+    c->res.rec_gates = a.gates;
+    c->res.rec_stride = P;
+    rc = launch_resident(c, n_steps);
+    c->res.rec_x = nullptr;
+    c->res.rec_gates = nullptr;
+    if (rc) return rc;
+    if (c->res_epoch > 0xF0000000u) {
+      FW_CUDA(c, cudaMemsetAsync(c->fll, 0, sizeof(unsigned long long) * 8 * (size_t)N, c->stream));
+      FW_CUDA(c, cudaMemsetAsync(c->res.xll, 0, sizeof(unsigned long long) * 4 * (size_t)N, c->stream));
+      FW_CUDA(c, cudaMemsetAsync(c->res.bll, 0, sizeof(unsigned long long) * 8 * (size_t)c->B * c->res.P,
+                                 c->stream));
+      c->res_epoch = 1;
+    }
+    uint32_t ep0 = c->res_epoch;
+    c->res_epoch += (uint32_t)n_steps + 1u;
+    float damp_f = c->h_damp.empty() ? 0.0f : c->h_damp[0];
+    int nn = n_steps, gs = P;
+    const float2* tx = a.traj;
+    const int* tg = a.gates;
+    void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&c->adj, (void*)&tx, (void*)&tg, (void*)&gs,
+                    (void*)&c->fll, (void*)&nn, (void*)&dt, (void*)&damp_f, (void*)&ep0};
+    FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_res_adj, dim3(c->res.P), dim3(kResThreads), args,
+                                           c->res_adj_smem, c->stream));
+    c->launches += 1;
+    return check_kernel(c, "resident adjoint segment");
+  }
   const uint64_t key_lo = ((uint64_t)n_steps << 32) | float_bits(dt);
   // recompute the segment from the current state, recording positions and gates
   cudaGraphExec_t g_fwd = nullptr;

@@ -29,13 +29,13 @@ from .world import PackedWorld, SceneLayout, build_native
 class DiffSim:
     """A single-scene rollout of ``n_steps`` substeps of ``dt`` with its adjoint."""
 
-    def __init__(self, domains, dt, n_steps, checkpoint_every=50, device=0, damping=0.0):
+    def __init__(self, domains, dt, n_steps, checkpoint_every=50, device=0, damping=0.0, path="auto"):
         self.layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=False)
         self.packed = PackedWorld([self.layout])
-        # forward on the resident step when the mesh fits on chip (one launch per
-        # segment); the adjoint recomputes segments with the gather kernels,
-        # which give the same bits
-        self.native = build_native(self.packed, device=device, path="auto")
+        # forward, recompute and reverse on the resident step when the mesh
+        # (and the adjoint state) fits on chip; otherwise on the gather step --
+        # the same bits either way
+        self.native = build_native(self.packed, device=device, path=path)
         self.N, self.E = self.packed.N, self.packed.E
         self.dt = float(np.float32(dt))
         self.n_steps = int(n_steps)

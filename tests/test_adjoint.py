@@ -148,6 +148,24 @@ def test_adjoint_is_the_transpose_of_the_tangent(damping):
         assert err < 1e-5, (kind, tangent, a_e + a_v)
 
 
+def test_resident_reverse_pass_equals_gather_reverse_pass():
+    """The resident recompute + reverse (one cooperative launch each per
+    segment) and the gather ones give the same bits, with contact and damping."""
+    dt, steps = 1e-4, 300
+    build = lambda: scenes.gradient_block_scene(fw, n=12, side=0.12, bottom=0.02, seed=8)  # noqa: E731
+    a = DiffSim(build(), dt, steps, checkpoint_every=50, damping=0.03)
+    b = DiffSim(build(), dt, steps, checkpoint_every=50, damping=0.03, path="gather")
+    assert a.native.get_path()[0] == 2 and b.native.get_path()[0] == 1
+    rng = np.random.default_rng(3)
+    v0 = (np.tile([0.0, -2.0], (a.N, 1)) + 0.3 * rng.standard_normal((a.N, 2))).astype(np.float32)
+    w = rng.standard_normal((a.N, 2)).astype(np.float32)
+    xa = a.forward(a.E0, v0)
+    xb_ = b.forward(b.E0, v0)
+    assert np.array_equal(xa, xb_)
+    for u, v in zip(a.backward(w), b.backward(w)):
+        assert np.array_equal(u, v)
+
+
 def test_checkpoint_interval_does_not_change_gradients():
     build = lambda: scenes.gradient_block_scene(fw, n=10, side=0.1, bottom=0.03, seed=2)  # noqa: E731
     a = DiffSim(build(), 1e-4, 300, checkpoint_every=50)
