@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--fifo-seconds", type=float, default=5.0, help="served: wall-time cap of the FIFO server")
     ap.add_argument("--scenes", type=int, default=2048, help="batched: number of bodies")
     ap.add_argument("--plain-sample", type=int, default=64, help="batched: bodies timed alone")
+    ap.add_argument("--batch-path", choices=["gather", "stream"], default="stream",
+                    help="batched: step implementation (same bits)")
     return ap.parse_args()
 
 
@@ -176,14 +178,15 @@ def ncu_traffic():
     return None
 
 
-def ncu_traffic_ratio_batched():
-    """DRAM bytes / algorithmic bytes of the gather kernels, measured by ncu on
-    a 256-body batch (per-triangle and per-node traffic do not depend on the
-    batch size, so the ratio scales to the full batch)."""
+def ncu_traffic_ratio_batched(step_path="gather"):
+    """DRAM bytes / algorithmic bytes of the batched step kernels, measured by
+    ncu on a 256-body batch (per-triangle and per-node traffic do not depend on
+    the batch size, so the ratio scales to the full batch)."""
     path = os.path.join(ROOT, "profiles", "traffic_batched.json")
     if os.path.exists(path):
         with open(path) as f:
-            return json.load(f).get("traffic_over_algorithmic")
+            d = json.load(f)
+        return d.get("stream_traffic_over_algorithmic") if step_path == "stream" else d.get("traffic_over_algorithmic")
     return None
 
 
@@ -257,7 +260,7 @@ def run_batched(args, rank, world, local):
     substeps = 100 * args.steps
     t0 = time.perf_counter()
     batch = scenes.ragged_batch(fw, args.scenes, seed=rank)
-    b = BatchedLoop(batch, dt=5e-5, useAdapativeDT=False, device=local)
+    b = BatchedLoop(batch, dt=5e-5, useAdapativeDT=False, device=local, path=args.batch_path)
     build_s = time.perf_counter() - t0
     tuned = autotune.tune_batched(b)
     stream = torch.cuda.Stream()
@@ -274,10 +277,28 @@ def run_batched(args, rank, world, local):
                 e_.record(stream)
             torch.cuda.synchronize()
         launches = b.launch_count() - l0
+        # ---- end to end: every body's positions and velocities in from pinned
+        # host memory, one step of 100 substeps, and back out
+        N = b.n_nodes
+        xh = torch.empty((N, 2), dtype=torch.float32, pin_memory=True)
+        vh = torch.empty((N, 2), dtype=torch.float32, pin_memory=True)
+        b._native.read_nodes_ptr(0, 0, N, xh.data_ptr())
+        b._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for s_, e_ in ev2:
+            s_.record(stream)
+            b._native.write_nodes_ptr(0, 0, N, xh.data_ptr())
+            b._native.write_nodes_ptr(1, 0, N, vh.data_ptr())
+            b.advance(100)
+            b._native.read_nodes_ptr(0, 0, N, xh.data_ptr())
+            b._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
+            e_.record(stream)
+        torch.cuda.synchronize()
     barrier(dist)
     lat = [s_.elapsed_time(e_) for s_, e_ in ev]
     E = b.n_elems
     work, ms = shard.aggregate(E * substeps, float(sum(lat)))
+    work_e2e, ms_e2e = shard.aggregate(E * 100 * args.steps, float(sum(s_.elapsed_time(e_) for s_, e_ in ev2)))
     finite = bool(np.isfinite(b.all_coords()).all())
     value = work / (ms / 1e3)
     # plain path: sample of the same bodies, one loop per body
@@ -314,18 +335,23 @@ def run_batched(args, rank, world, local):
         "config": {"workload": f"ragged batch of {args.scenes} bodies on voxel grids, dt 5e-5",
                    "elements": E, "nodes": b.n_nodes, "bodies": args.scenes, "substeps": substeps,
                    "step": "100 substeps", "l2": "working set larger than L2", "launch": tuned,
-                   "host_build_s": build_s, "state_finite": finite, "replicas": world},
+                   "host_build_s": build_s, "state_finite": finite, "replicas": world,
+                   "step_path": args.batch_path},
         "batched_vs_plain": {"plain_value": plain_value, "ratio": value / plain_value,
                              "plain_sample_bodies": len(pick),
                              "plain_p50_ms_per_substep": percentile_ms(plain_lat, 50)},
         "latency_ms_per_substep": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99),
                                    "p99.9": percentile_ms(lat, 99.9)},
-        "roofline": {"bound": "hbm", "kernel": "substep = k_elements + k_nodes", "achieved": achieved,
+        "roofline": {"bound": "hbm",
+                     "kernel": ("substep = k_control + k_stream" if args.batch_path == "stream"
+                                else "substep = k_elements + k_nodes"), "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": which,
                      "algorithmic_bytes_per_substep": bstep,
-                     "traffic": (None if ncu_traffic_ratio_batched() is None
-                                 else round(ncu_traffic_ratio_batched() * bstep)),
+                     "traffic": (None if ncu_traffic_ratio_batched(args.batch_path) is None
+                                 else round(ncu_traffic_ratio_batched(args.batch_path) * bstep)),
                      "traffic_note": "DRAM bytes per substep scaled from an ncu capture of a 256-body batch"},
+        "e2e": {"value": work_e2e / (ms_e2e / 1e3), "unit": "element-steps/s",
+                "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
         "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:

@@ -22,7 +22,8 @@ FW_FIELD_X0 = 3
 FW_PATH_AUTO = 0
 FW_PATH_GATHER = 1
 FW_PATH_RESIDENT = 2
-PATHS = {"auto": FW_PATH_AUTO, "gather": FW_PATH_GATHER, "resident": FW_PATH_RESIDENT}
+FW_PATH_STREAM = 3
+PATHS = {"auto": FW_PATH_AUTO, "gather": FW_PATH_GATHER, "resident": FW_PATH_RESIDENT, "stream": FW_PATH_STREAM}
 FW_OPT_FRONT_WARPS = 1
 FW_OPT_BLOCK_ELEMS = 2
 FW_OPT_BLOCK_NODES = 3

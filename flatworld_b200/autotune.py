@@ -64,8 +64,12 @@ def _time_steps(native, steps, dt, stream):
 
 
 def tune_batched(loop, blocks=(128, 256, 512), steps=16, use_cache=True):
-    """Pick the gather kernels' block sizes for ``loop`` (a BatchedLoop)."""
+    """Pick the gather kernels' block sizes for ``loop`` (a BatchedLoop).  The
+    stream path has a fixed launch shape (one 64-thread CTA per 64-node patch)."""
     import torch
+
+    if getattr(loop, "path", "gather") == "stream":
+        return {"path": "stream", "block_elems": 0, "block_nodes": 0, "candidates": []}
 
     key = f"batched|{_gpu_name(loop._native.device)}|N={loop.n_nodes}|E={loop.n_elems}|S={loop.S}"
     if use_cache:

@@ -31,10 +31,13 @@ class BatchedLoop:
         device: CUDA ordinal
         block_elems, block_nodes: launch shape of the step kernels (0: tuned
             default; see flatworld_b200.autotune)
+        path: "stream" (one patch-streaming kernel per substep, the faster one
+            for many small scenes) or "gather" (two kernels per substep through
+            a corner buffer, launch shape tunable); both give the same bits
     """
 
     def __init__(self, scenes, dt=0.0, useAdapativeDT=True, damping=0.0, device=0,
-                 block_elems=0, block_nodes=0):
+                 block_elems=0, block_nodes=0, path="stream"):
         S = len(scenes)
         dts = dt if np.iterable(dt) else [dt] * S
         ada = useAdapativeDT if np.iterable(useAdapativeDT) else [useAdapativeDT] * S
@@ -42,7 +45,8 @@ class BatchedLoop:
         self.layouts = [SceneLayout(d, dt=a, damping=c, useAdapativeDT=b)
                         for d, a, b, c in zip(scenes, dts, ada, damp)]
         self.packed = PackedWorld(self.layouts)
-        self._native = build_native(self.packed, device=device, path="gather")
+        self._native = build_native(self.packed, device=device, path=path)
+        self.path = path
         if block_elems or block_nodes:
             self.set_launch(block_elems, block_nodes)
         self.S = S

@@ -1,0 +1,224 @@
+// fw_stream.cuh -- patch-streaming substep for worlds of many scenes.
+//
+// Every body is cut into patches of at most kStreamNodes nodes (recursive
+// coordinate bisection).  One CTA per patch and substep: it gathers the
+// positions of its owned and halo nodes into shared memory, evaluates every
+// triangle touching an owned node (cut triangles are evaluated by each patch
+// that holds them) into shared corner forces, and updates its owned nodes --
+// contact, the corner forces in ascending element order, boundary conditions,
+// symplectic Euler, body boxes -- so corner forces never go to DRAM and one
+// kernel does the work of k_elements + k_nodes.  Other patches read halo
+// positions while a patch writes its own, so positions are double-buffered
+// (x_in -> x_out, the host swaps the buffers after each substep); so is the J2
+// state, which the patch owning a triangle's first corner writes.  The scene
+// control (modes, gates, counters, box slots) runs first in k_control, as in
+// block 0 of k_elements.  Same arithmetic in the same order as the gather step:
+// the results are the same bits.
+//
+// The kernel is bound by the latency of its dependent loads, not by DRAM
+// bandwidth, so the static data of a patch is stored in patch order
+// (StreamElem per patch triangle, StreamNode per owned node; built by
+// k_stream_elems / k_stream_nodes and rebuilt when a Young's modulus changes):
+// a record is one load at the CTA's own offset rather than an index load
+// followed by a dependent gather.  Small CTAs (64 threads) capped at 32
+// registers keep 32 CTAs on an SM, which hides the rest of that latency.
+#pragma once
+
+namespace {
+
+constexpr int kStreamNodes = 64;  // owned nodes per patch (and threads per CTA): small
+                                  // patches balance the ragged scenes over the SMs
+constexpr int kStreamThreads = 64;
+
+struct StreamPatch {
+  int node_off, no;  // owned nodes: nodes[node_off .. +no), ascending
+  int halo_off, nh;  // halo nodes: halo[halo_off .. +nh), ascending
+  int elem_off, ne;  // triangles touching an owned node: elem/eid/conn[elem_off .. +ne), ascending
+  int csrp_off;      // csrp[csrp_off .. +no+1): local corner-list offsets of the owned nodes
+  int csr_off;       // csrs[csr_off + csrp[..]]: 3 * local triangle + corner
+  int scene;
+  int pad[3];
+};
+
+// Static data of one patch triangle, in patch order.
+struct __align__(16) StreamElem {
+  ElemMat m;   // emat[e]
+  float4 ji;   // jinv[e]
+  uint2 conn;  // local corners: x = a | b << 16, y = c | writer << 16 (writer: this patch owns corner a)
+  int e;       // global triangle index (J2 state)
+  int pad;
+};
+
+// Static data of one owned node, in patch order.
+struct __align__(16) StreamNode {
+  uint32_t word;  // node_word[g]
+  float mass;     // mass[g]
+  float2 bcv;     // bcv[g]
+};
+
+struct StreamDev {
+  const StreamPatch* patch;
+  const int32_t* nodes;
+  const int32_t* halo;
+  const int32_t* eid;
+  const uint2* conn;        // x = a | b << 16, y = c | writer << 16 (local node ids)
+  const uint16_t* csrp;
+  const uint16_t* csrs;
+  int no_max, nh_max, ne_max;
+  StreamElem* elem;  // built from eid/conn by k_stream_elems
+  StreamNode* node;  // built from nodes by k_stream_nodes
+};
+
+__global__ void k_stream_nodes(Dev d, const int32_t* nodes, StreamNode* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int g = nodes[i];
+  StreamNode r;
+  r.word = d.node_word[g];
+  r.mass = d.mass[g];
+  r.bcv = d.bcv[g];
+  out[i] = r;
+}
+
+__global__ void k_stream_elems(Dev d, const int32_t* eid, const uint2* conn, StreamElem* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = eid[i];
+  StreamElem r;
+  r.m = d.emat[e];
+  r.ji = d.jinv[e];
+  r.conn = conn[i];
+  r.e = e;
+  r.pad = 0;
+  out[i] = r;
+}
+
+__global__ void k_control(Dev d) { step_control(d); }
+
+// One triangle of the patch (element_step on shared positions).
+__device__ __forceinline__ void stream_element(const Dev& d, const float2* sx, float2* sf, int q, int e, uint2 c,
+                                               ElemMat m, float4 ji, const float4* j2_in, float4* j2_out) {
+  float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float sy = 0.f, H = 0.f;
+  const bool mises = fw::elem_type(m.word) == fw::MAT_MISES;
+  if (mises) {
+    j2 = j2_in[e];
+    const float2 jp = d.j2par[e];
+    sy = jp.x;
+    H = jp.y;
+  }
+  float2 f1, f2, f3;
+  fw::element_forces(sx[c.x & 0xFFFFu], sx[c.x >> 16], sx[c.y & 0xFFFFu], ji, m, sy, H, j2, f1, f2, f3);
+  if (mises && (c.y >> 16)) j2_out[e] = j2;
+  sf[3 * q] = f1;
+  sf[3 * q + 1] = f2;
+  sf[3 * q + 2] = f3;
+}
+
+__global__ void __launch_bounds__(kStreamThreads, 32) k_stream(Dev d, StreamDev sd, const float2* __restrict__ x_in,
+                                                               float2* __restrict__ x_out, const float4* j2_in,
+                                                               float4* j2_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* sx = reinterpret_cast<float2*>(smem_raw);  // owned, then halo
+  float2* sf = sx + (sd.no_max + sd.nh_max);         // 3 per patch triangle
+  const StreamPatch P = sd.patch[blockIdx.x];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int mode = d.scene_mode[P.scene];
+  if (mode == fw::MODE_FROZEN) {  // keep the state: carry it into the other buffers
+    for (int i = t; i < P.no; i += T) {
+      const int g = sd.nodes[P.node_off + i];
+      x_out[g] = x_in[g];
+    }
+    if (d.has_j2)
+      for (int q = t; q < P.ne; q += T) {
+        const StreamElem& r = sd.elem[P.elem_off + q];
+        if (r.conn.y >> 16) j2_out[r.e] = j2_in[r.e];
+      }
+    return;
+  }
+  static_assert(kStreamThreads == kStreamNodes, "one owned node per thread");
+  // positions of the owned (one per thread) and halo nodes
+  const bool valid = t < P.no;
+  const int g = valid ? sd.nodes[P.node_off + t] : 0;
+  if (valid) sx[t] = x_in[g];
+  for (int h = t; h < P.nh; h += T) sx[P.no + h] = x_in[sd.halo[P.halo_off + h]];
+  __syncthreads();
+  // triangles (element_step)
+  for (int q = t; q < P.ne; q += T) {
+    const StreamElem r = sd.elem[P.elem_off + q];
+    stream_element(d, sx, sf, q, r.e, r.conn, r.m, r.ji, j2_in, j2_out);
+  }
+  __syncthreads();
+  // owned nodes (node_step)
+  const StreamNode nr = valid ? sd.node[P.node_off + t] : StreamNode{0u, 1.0f, make_float2(0.f, 0.f)};
+  const float2 v0 = valid ? d.v[g] : make_float2(0.f, 0.f);
+  const int k0 = valid ? sd.csrp[P.csrp_off + t] : 0, k1 = valid ? sd.csrp[P.csrp_off + t + 1] : 0;
+  float2 x = valid ? sx[t] : make_float2(0.f, 0.f);
+  const uint32_t w = nr.word;
+  const float mass = nr.mass;
+  const float2 bv0 = nr.bcv;
+  const int b = (int)(w >> fw::NODE_BODY_SHIFT);
+  bool bnd = false;
+  if (valid) {
+    float2 v = v0;
+    const int s = P.scene;
+    const float dt = mode == fw::MODE_INIT ? 0.0f : (d.uniform_dt ? d.dt_uniform : d.scene_dt[s]);
+    const float damp = mode == fw::MODE_INIT ? 0.0f : d.scene_damp[s];
+    float2 f = make_float2(0.f, 0.f);
+    bnd = (w & fw::NODE_BOUNDARY) != 0;
+    if (bnd && mode == fw::MODE_STEP) {
+      const int p0 = d.body_pair_off[b], pn = d.body_pair_cnt[b];
+      for (int k = 0; k < pn; ++k) {
+        if (!d.pair_active[p0 + k]) continue;
+        float2 cf;
+        if (fw::contact_force(d.pairs[p0 + k], d.heights, d.occ, x, v, dt, cf)) {
+          f.x += cf.x;
+          f.y += cf.y;
+        }
+      }
+    }
+    for (int k = k0; k < k1; ++k) {  // ascending element
+      const float2 cq = sf[sd.csrs[P.csr_off + k]];
+      f.x += cq.x;
+      f.y += cq.y;
+    }
+    const int bc = (int)(w & fw::NODE_BC_MASK);
+    const float2 bv = (bc & (fw::BC_A | fw::BC_GRAVITY | fw::BC_FORCE | fw::BC_V)) ? bv0 : make_float2(0.f, 0.f);
+    fw::integrate(bc, f, mass, bv, dt, damp, x, v);
+    x_out[g] = x;
+    d.v[g] = v;
+    if (!(isfinite(x.x) && isfinite(x.y) && isfinite(v.x) && isfinite(v.y))) d.scene_bad[s] = 1;
+  }
+  // per-body box of boundary nodes (as node_step)
+  const unsigned full = 0xFFFFFFFFu;
+  const unsigned mb = __ballot_sync(full, bnd);
+  if (mb == 0u) return;
+  const int leader = __ffs(mb) - 1;
+  const int bl = __shfl_sync(full, b, leader);
+  const bool uniform = __all_sync(full, !bnd || b == bl);
+  float lx = bnd ? x.x : 1e30f, ly = bnd ? x.y : 1e30f;
+  float hx = bnd ? x.x : -1e30f, hy = bnd ? x.y : -1e30f;
+  if (uniform) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lx = fminf(lx, __shfl_xor_sync(full, lx, o));
+      ly = fminf(ly, __shfl_xor_sync(full, ly, o));
+      hx = fmaxf(hx, __shfl_xor_sync(full, hx, o));
+      hy = fmaxf(hy, __shfl_xor_sync(full, hy, o));
+    }
+    if ((int)(t & 31) == leader) {
+      int* r = d.aabb_ring + ((size_t)(d.scene_counter[P.scene] & 1) * d.B + b) * 4;
+      atomicMin(r + 0, fw::f2ord(lx));
+      atomicMin(r + 1, fw::f2ord(ly));
+      atomicMax(r + 2, fw::f2ord(hx));
+      atomicMax(r + 3, fw::f2ord(hy));
+    }
+  } else if (bnd) {
+    int* r = d.aabb_ring + ((size_t)(d.scene_counter[P.scene] & 1) * d.B + b) * 4;
+    atomicMin(r + 0, fw::f2ord(lx));
+    atomicMin(r + 1, fw::f2ord(ly));
+    atomicMax(r + 2, fw::f2ord(hx));
+    atomicMax(r + 3, fw::f2ord(hy));
+  }
+}
+
+}  // namespace

@@ -43,6 +43,7 @@ constexpr int kGraphSteps = 32;
 
 struct Dev {
   float2* x;
+  float2* x_alt;       // stream path: the other position buffer (swapped every substep)
   float2* v;
   float2* x0;
   float2* bcv;
@@ -58,6 +59,7 @@ struct Dev {
   ElemMat* emat;
   float2* j2par;
   float4* j2state;
+  float4* j2_alt;      // stream path: the other J2 state buffer
   float* ndmass;
   int32_t* body_scene;
   int32_t* body_pair_off;
@@ -626,6 +628,7 @@ __global__ void k_energy_groups(const int* first, int n_groups, const double4* p
 }  // namespace
 
 #include "fw_resident.cuh"
+#include "fw_stream.cuh"
 
 // ------------------------------------------------------------------ context
 
@@ -713,6 +716,12 @@ struct fw_ctx {
   Adj adj{};
   int adj_cap = 0;  // steps per segment the trajectory buffer holds
   Tan tan{};
+  // stream path (FW_PATH_STREAM)
+  StreamDev sd{};
+  int st_P = 0;
+  size_t st_smem = 0;
+  float2* x_buf0 = nullptr;  // the position buffer allocated first (parity of the swaps)
+  int st_ne = 0, st_no = 0;  // patch triangles and owned nodes (record counts)
   bool res_adj = false;            // the reverse pass runs resident (k_res_adj)
   size_t res_adj_smem = 0;
   unsigned long long* fll = nullptr;  // [2][N][4] flag-in-data force adjoints of the reverse pass
@@ -863,10 +872,13 @@ int launch_resident(fw_ctx* c, int n);
 
 int rebuild_chunks(fw_ctx* c);
 
+int stream_steps(fw_ctx* c, int n);
+
 int run_steps(fw_ctx* c, int n) {
   int rc = FW_OK;
   if (c->arena && (rc = rebuild_chunks(c))) return rc;
   if (c->path == FW_PATH_RESIDENT && c->d.uniform_dt) return launch_resident(c, n);
+  if (c->path == FW_PATH_STREAM) return stream_steps(c, n);
   c->host_counter += n;
   if (n >= kGraphSteps) {
     cudaGraphExec_t g = nullptr;
@@ -889,6 +901,180 @@ int run_steps(fw_ctx* c, int n) {
   return rc;
 }
 
+
+// n substeps of the stream path: k_control + k_stream each, alternating the
+// position / J2 buffers; graphs of up to kGraphSteps substeps, cached per
+// (starting buffer, dt mode, dt, count).
+int stream_steps(fw_ctx* c, int n) {
+  c->host_counter += n;
+  while (n > 0) {
+    const int m = std::min(n, kGraphSteps);
+    const uint64_t parity = c->d.x == c->x_buf0 ? 0 : 1;
+    const uint64_t key = (1ull << 62) | (parity << 61) | ((uint64_t)(c->d.uniform_dt ? 1 : 0) << 60) |
+                         ((uint64_t)m << 32) | (c->d.uniform_dt ? float_bits(c->d.dt_uniform) : 0u);
+    cudaGraphExec_t g = nullptr;
+    int rc = cached_graph(c, c->graphs, key, [&] {
+      float2 *xa = c->d.x, *xb = c->d.x_alt;
+      float4 *ja = c->d.j2state, *jb = c->d.j2_alt;
+      for (int k = 0; k < m; ++k) {
+        k_control<<<1, kMaxBlock, 0, c->stream>>>(c->d);
+        k_stream<<<c->st_P, kStreamThreads, c->st_smem, c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
+        std::swap(xa, xb);
+        std::swap(ja, jb);
+      }
+    }, &g);
+    if (rc) return rc;
+    FW_CUDA(c, cudaGraphLaunch(g, c->stream));
+    c->launches += 2 * m;
+    if (m & 1) {
+      std::swap(c->d.x, c->d.x_alt);
+      std::swap(c->d.j2state, c->d.j2_alt);
+    }
+    n -= m;
+  }
+  return check_kernel(c, "stream step");
+}
+
+void rcb(const std::vector<float2>& x, std::vector<int>& idx, int lo, int hi, int p0, int np,
+         std::vector<int>& part);
+
+// (Re)build the patch-ordered records of the stream path from the element and
+// node arrays (after finalize, and after a Young's modulus changes).
+int stream_records(fw_ctx* c) {
+  if (c->st_ne > 0)
+    k_stream_elems<<<(c->st_ne + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.eid, c->sd.conn,
+                                                                               c->sd.elem, c->st_ne);
+  if (c->st_no > 0)
+    k_stream_nodes<<<(c->st_no + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.nodes, c->sd.node,
+                                                                               c->st_no);
+  c->launches += 2;
+  return check_kernel(c, "stream records");
+}
+
+// Patches of the stream path: each body cut into patches of at most
+// kStreamNodes nodes; per patch the owned nodes, the triangles touching them,
+// the halo nodes, local connectivity and the owned nodes' corner lists in the
+// global ascending-element order.
+int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<int32_t>& slot,
+                 const std::vector<float2>& x0, bool has_j2) {
+  const int N = c->N, E = c->E;
+  std::vector<int> part(N, -1), idx;
+  int P = 0;
+  for (int b = 0; b < c->B; ++b) {
+    const int n0 = c->h_noff[b], nn = c->h_ncnt[b];
+    if (nn <= 0) continue;
+    const int np = (nn + kStreamNodes - 1) / kStreamNodes;
+    idx.resize(nn);
+    for (int k = 0; k < nn; ++k) idx[k] = n0 + k;
+    rcb(x0, idx, 0, nn, P, np, part);
+    P += np;
+  }
+  std::vector<std::vector<int>> owned(P);
+  for (int i = 0; i < N; ++i) {
+    if (part[i] < 0) return fail(c, FW_ERR_ARG, "stream path: node %d belongs to no body", i);
+    owned[part[i]].push_back(i);
+  }
+  std::vector<int> node_scene(N, 0);
+  for (int b = 0; b < c->B; ++b)
+    for (int k = 0; k < c->h_ncnt[b]; ++k) node_scene[c->h_noff[b] + k] = c->h_scene[b];
+  std::vector<StreamPatch> patches(P);
+  std::vector<int32_t> rn, rh, re, rcp;
+  std::vector<uint2> rc;
+  std::vector<uint16_t> rcs;
+  std::vector<int> loc(N, -1), eloc(E, -1);
+  int no_max = 1, nh_max = 1, ne_max = 1;
+  for (int p = 0; p < P; ++p) {
+    const std::vector<int>& ow = owned[p];
+    if ((int)ow.size() > kStreamNodes) return fail(c, FW_ERR_ARG, "stream path: patch larger than %d nodes", kStreamNodes);
+    std::vector<int> tri;
+    for (int n : ow)
+      for (int k = off[n]; k < off[n + 1]; ++k) tri.push_back(slot[k] / 3);
+    std::sort(tri.begin(), tri.end());
+    tri.erase(std::unique(tri.begin(), tri.end()), tri.end());
+    std::vector<int> hal;
+    for (int e : tri)
+      for (int k = 0; k < 3; ++k) {
+        const int n = c->h_conn[3 * e + k];
+        if (part[n] != p) hal.push_back(n);
+      }
+    std::sort(hal.begin(), hal.end());
+    hal.erase(std::unique(hal.begin(), hal.end()), hal.end());
+    if (ow.size() + hal.size() >= 65536 || 3 * tri.size() >= 65536)
+      return fail(c, FW_ERR_ARG, "stream path: patch too large for 16-bit local indices");
+    StreamPatch& sp = patches[p];
+    sp.node_off = (int)rn.size();
+    sp.no = (int)ow.size();
+    sp.halo_off = (int)rh.size();
+    sp.nh = (int)hal.size();
+    sp.elem_off = (int)re.size();
+    sp.ne = (int)tri.size();
+    sp.csrp_off = (int)rcp.size();
+    sp.csr_off = (int)rcs.size();
+    sp.scene = node_scene[ow[0]];
+    for (int i = 0; i < sp.no; ++i) {
+      loc[ow[i]] = i;
+      rn.push_back(ow[i]);
+    }
+    for (int h = 0; h < sp.nh; ++h) {
+      loc[hal[h]] = sp.no + h;
+      rh.push_back(hal[h]);
+    }
+    for (int q = 0; q < sp.ne; ++q) {
+      const int e = tri[q];
+      eloc[e] = q;
+      re.push_back(e);
+      const uint32_t a = loc[c->h_conn[3 * e]], b = loc[c->h_conn[3 * e + 1]], cc = loc[c->h_conn[3 * e + 2]];
+      const uint32_t writer = part[c->h_conn[3 * e]] == p ? 1u : 0u;
+      rc.push_back(make_uint2(a | (b << 16), cc | (writer << 16)));
+    }
+    int cnt = 0;
+    for (int i = 0; i < sp.no; ++i) {
+      rcp.push_back((int32_t)cnt);
+      const int n = ow[i];
+      for (int k = off[n]; k < off[n + 1]; ++k) {
+        rcs.push_back((uint16_t)(3 * eloc[slot[k] / 3] + slot[k] % 3));
+        ++cnt;
+      }
+    }
+    rcp.push_back((int32_t)cnt);
+    if (cnt >= 65536) return fail(c, FW_ERR_ARG, "stream path: patch corner list too long");
+    for (int n : ow) loc[n] = -1;
+    for (int n : hal) loc[n] = -1;
+    for (int e : tri) eloc[e] = -1;
+    no_max = std::max(no_max, sp.no);
+    nh_max = std::max(nh_max, sp.nh);
+    ne_max = std::max(ne_max, sp.ne);
+  }
+  std::vector<uint16_t> rcp16(rcp.begin(), rcp.end());
+  int r;
+  StreamPatch* dp = nullptr;
+  int32_t *dn = nullptr, *dh = nullptr, *de = nullptr;
+  uint2* dc = nullptr;
+  uint16_t *dcp = nullptr, *dcs = nullptr;
+  if ((r = upload(c, &dp, patches)) || (r = upload(c, &dn, rn)) || (r = upload(c, &dh, rh)) ||
+      (r = upload(c, &de, re)) || (r = upload(c, &dc, rc)) || (r = upload(c, &dcp, rcp16)) ||
+      (r = upload(c, &dcs, rcs)) || (r = dalloc(c, &c->d.x_alt, N)) ||
+      (r = dalloc(c, &c->d.j2_alt, has_j2 ? E : 1)))
+    return r;
+  FW_CUDA(c, cudaMemcpyAsync(c->d.x_alt, c->d.x, sizeof(float2) * N, cudaMemcpyDeviceToDevice, c->stream));
+  if (has_j2)
+    FW_CUDA(c, cudaMemcpyAsync(c->d.j2_alt, c->d.j2state, sizeof(float4) * E, cudaMemcpyDeviceToDevice, c->stream));
+  StreamElem* dse = nullptr;
+  StreamNode* dsn = nullptr;
+  if ((r = dalloc(c, &dse, re.size())) || (r = dalloc(c, &dsn, rn.size()))) return r;
+  c->sd = StreamDev{dp, dn, dh, de, dc, dcp, dcs, no_max, nh_max, ne_max, dse, dsn};
+  c->st_ne = (int)re.size();
+  c->st_no = (int)rn.size();
+  if ((r = stream_records(c))) return r;
+  c->st_P = P;
+  c->st_smem = sizeof(float2) * (size_t)(no_max + nh_max) + sizeof(float2) * 3 * (size_t)ne_max;
+  c->x_buf0 = c->d.x;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if ((long)c->st_smem > optin) return fail(c, FW_ERR_ARG, "stream path: patch needs %zu B of shared memory", c->st_smem);
+  FW_CUDA(c, cudaFuncSetAttribute(k_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  return FW_OK;
+}
 
 void rcb(const std::vector<float2>& x, std::vector<int>& idx, int lo, int hi, int p0, int np,
          std::vector<int>& part) {
@@ -1495,7 +1681,11 @@ int fw_finalize(fw_ctx* c) {
   if ((rc = launch_step(c))) return rc;
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   c->path = FW_PATH_GATHER;
-  if (c->path_req != FW_PATH_GATHER) {
+  if (c->path_req == FW_PATH_STREAM) {
+    if ((rc = build_stream(c, off, slot, x0, has_j2))) return rc;
+    c->path = FW_PATH_STREAM;
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  } else if (c->path_req != FW_PATH_GATHER) {
     rc = build_resident(c, off, slot, x0, has_j2);
     if (rc < 0) return rc;
     if (rc == 0) {
@@ -1512,7 +1702,7 @@ int fw_finalize(fw_ctx* c) {
 int fw_set_path(fw_ctx* c, int32_t path, int32_t patches) {
   if (!c) return FW_ERR_ARG;
   if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_path after fw_finalize");
-  if (path != FW_PATH_AUTO && path != FW_PATH_GATHER && path != FW_PATH_RESIDENT)
+  if (path != FW_PATH_AUTO && path != FW_PATH_GATHER && path != FW_PATH_RESIDENT && path != FW_PATH_STREAM)
     return fail(c, FW_ERR_ARG, "fw_set_path: unknown path %d", path);
   if (patches < 0) return fail(c, FW_ERR_ARG, "fw_set_path: patches < 0");
   c->path_req = path;
@@ -1897,7 +2087,8 @@ int fw_arena_scene_info(fw_ctx* c, int32_t s, int64_t* info) {
 
 int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* young, int32_t on_device) {
   if (!c || !young) return FW_ERR_ARG;
-  // (the resident step loads the Lame constants at every launch, so both paths see the change)
+  // (the resident step loads the Lame constants at every launch; the stream path's
+  // patch records are rebuilt below)
   if (!c->finalized || c->arena)
     return fail(c, FW_ERR_STATE, "fw_set_element_young needs a finalized world (not an arena)");
   if (first < 0 || count < 0 || (int64_t)first + count > c->E) return fail(c, FW_ERR_ARG, "element range out of bounds");
@@ -1910,15 +2101,16 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
   k_set_young<<<(count + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, dst, c->d_poisson, first, first + count);
   c->launches += 1;
-  return check_kernel(c, "set young");
+  if ((rc = check_kernel(c, "set young"))) return rc;
+  return c->path == FW_PATH_STREAM ? stream_records(c) : FW_OK;
 }
 
 int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
   if (!c) return FW_ERR_ARG;
   // The forward may run on either path (identical bits); the recompute and the
   // reverse use the gather kernels and data, which every non-arena world has.
-  if (!c->finalized || c->arena || c->S != 1)
-    return fail(c, FW_ERR_STATE, "the adjoint needs a finalized single-scene world (not an arena)");
+  if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)
+    return fail(c, FW_ERR_STATE, "the adjoint needs a finalized single-scene world on the gather or resident path");
   if (max_segment_steps <= 0) return fail(c, FW_ERR_ARG, "max_segment_steps must be > 0");
   if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the adjoint covers Elastic and NeoHookean triangles (no J2)");
   for (const Pair& p : c->h_pairs)
@@ -2070,8 +2262,8 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
 
 int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE, int32_t on_device) {
   if (!c) return FW_ERR_ARG;
-  if (!c->finalized || c->arena || c->S != 1)
-    return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world (not an arena)");
+  if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)
+    return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world on the gather or resident path");
   if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the tangent covers Elastic and NeoHookean triangles (no J2)");
   for (const Pair& p : c->h_pairs)
     if (p.kind != fw::PAIR_PLANE) return fail(c, FW_ERR_ARG, "the tangent covers plane contact only");
@@ -2130,7 +2322,7 @@ int fw_tan_read(fw_ctx* c, float* dx, float* dv, int32_t on_device) {
 int fw_get_path(const fw_ctx* c, int32_t* path, int32_t* patches) {
   if (!c || !path) return FW_ERR_ARG;
   *path = c->finalized ? c->path : FW_PATH_AUTO;
-  if (patches) *patches = c->path == FW_PATH_RESIDENT ? c->res.P : 0;
+  if (patches) *patches = c->path == FW_PATH_RESIDENT ? c->res.P : (c->path == FW_PATH_STREAM ? c->st_P : 0);
   return FW_OK;
 }
 

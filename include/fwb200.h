@@ -63,6 +63,7 @@ extern "C" {
 #define FW_PATH_AUTO 0     /* resident when the world fits, else gather */
 #define FW_PATH_GATHER 1   /* two kernels per substep, any world */
 #define FW_PATH_RESIDENT 2 /* one persistent kernel per fw_step call */
+#define FW_PATH_STREAM 3   /* one patch-streaming kernel per substep (worlds of many scenes) */
 
 typedef struct fw_ctx fw_ctx;
 
@@ -172,7 +173,7 @@ int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
 int fw_snapshot(fw_ctx* ctx, int32_t slot);
 int fw_restore(fw_ctx* ctx, int32_t slot);
 
-/* Active path (FW_PATH_GATHER or FW_PATH_RESIDENT) and patch count. */
+/* Active path (FW_PATH_GATHER, FW_PATH_RESIDENT or FW_PATH_STREAM) and patch count. */
 int fw_get_path(const fw_ctx* ctx, int32_t* path, int32_t* patches);
 
 /* Advance every active scene by n_steps substeps of dt (float32), i.e. n_steps

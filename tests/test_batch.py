@@ -28,9 +28,10 @@ def small_batch(n=9, seed=7):
     return out
 
 
-def test_batched_equals_alone_and_oracle_fixed_dt():
+@pytest.mark.parametrize("path", ["gather", "stream"])
+def test_batched_equals_alone_and_oracle_fixed_dt(path):
     build = lambda: small_batch()  # noqa: E731
-    b = BatchedLoop(build(), dt=5e-5, useAdapativeDT=False)
+    b = BatchedLoop(build(), dt=5e-5, useAdapativeDT=False, path=path)
     b.advance(300)
     alone = build()
     for s, doms in enumerate(alone):
@@ -47,12 +48,14 @@ def test_batched_equals_alone_and_oracle_fixed_dt():
         assert np.array_equal(b.velocities(s).astype(np.float64), vo), s
 
 
-def test_batched_advance_with_time_per_scene_dt():
+@pytest.mark.parametrize("path", ["gather", "stream"])
+def test_batched_advance_with_time_per_scene_dt(path):
     """Adaptive dt differs per scene: each scene takes its own substeps (the
-    reference's own test scenes, each stable at its adaptive dt)."""
+    reference's own test scenes, each stable at its adaptive dt); finished
+    scenes freeze while the others go on."""
     build = lambda: [scenes.hf_disk_scene(fw), scenes.voxel_disk_scene(fw), scenes.plain_small_scene(fw),  # noqa: E731
                      [scenes.two_triangle_square(fw)]]
-    b = BatchedLoop(build(), useAdapativeDT=True)
+    b = BatchedLoop(build(), useAdapativeDT=True, path=path)
     assert len(set(np.round(b.dt, 12))) > 1
     for _ in range(2):
         b.advanceWithTime(FRAME)
@@ -66,8 +69,9 @@ def test_batched_advance_with_time_per_scene_dt():
         assert b.counters[s] == lp._counter_py
 
 
-def test_snapshot_restore_and_frozen_scenes():
-    b = BatchedLoop(small_batch(n=4), dt=5e-5, useAdapativeDT=False)
+@pytest.mark.parametrize("path", ["gather", "stream"])
+def test_snapshot_restore_and_frozen_scenes(path):
+    b = BatchedLoop(small_batch(n=4), dt=5e-5, useAdapativeDT=False, path=path)
     b.advance(50)
     b._native.snapshot(3)
     b.advance(60)
@@ -84,8 +88,8 @@ def test_snapshot_restore_and_frozen_scenes():
 
 def test_autotune_keeps_results(tmp_path, monkeypatch):
     monkeypatch.setenv("FLATWORLD_B200_CACHE", str(tmp_path))
-    a = BatchedLoop(small_batch(n=5), dt=5e-5, useAdapativeDT=False)
-    c = BatchedLoop(small_batch(n=5), dt=5e-5, useAdapativeDT=False)
+    a = BatchedLoop(small_batch(n=5), dt=5e-5, useAdapativeDT=False, path="gather")
+    c = BatchedLoop(small_batch(n=5), dt=5e-5, useAdapativeDT=False, path="gather")
     best = autotune.tune_batched(a, blocks=(128, 256), steps=4)
     assert best["block_elems"] in (128, 256) and len(best["candidates"]) == 4
     a.advance(100)
@@ -93,3 +97,20 @@ def test_autotune_keeps_results(tmp_path, monkeypatch):
     assert np.array_equal(a.all_coords(), c.all_coords())
     again = autotune.tune_batched(a, blocks=(128, 256), steps=4)
     assert again.get("cached")
+
+
+def test_stream_young_change_equals_gather():
+    """A Young's modulus change mid-run reaches the stream path's patch
+    records: both paths give the same bits afterwards."""
+    loops = [BatchedLoop(small_batch(n=4), dt=5e-5, useAdapativeDT=False, path=p) for p in ("gather", "stream")]
+    rng = np.random.default_rng(3)
+    young = None
+    for lp in loops:
+        lp.advance(50)
+        if young is None:
+            young = rng.uniform(5e3, 4e4, lp.n_elems).astype(np.float32)
+        lp._native.set_element_young(young)
+        lp.advance(100)
+    assert np.array_equal(loops[0].all_coords(), loops[1].all_coords())
+    assert not np.array_equal(loops[0].all_coords(), BatchedLoop(small_batch(n=4), dt=5e-5, useAdapativeDT=False,
+                                                                  path="stream").all_coords())

@@ -23,11 +23,12 @@ RTOL = 1e-5
 FRAME = 1.0 / 60.0
 
 
-@pytest.fixture(params=["gather", "resident", "resident-counter"])
+@pytest.fixture(params=["gather", "resident", "resident-counter", "stream"])
 def path(request):
-    """Every step implementation must meet the same bar: the gather path and
-    the resident path with either hand-off between CTAs (flag-in-data words,
-    the default for <= 8 bodies, or the arrival counter)."""
+    """Every step implementation must meet the same bar: the gather path, the
+    resident path with either hand-off between CTAs (flag-in-data words, the
+    default for <= 8 bodies, or the arrival counter) and the patch-streaming
+    path."""
     return request.param
 
 
