@@ -52,6 +52,11 @@ _SIGNATURES = {
     "fw_add_plane_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_float, C.c_float, C.c_float, C.c_float]),
     "fw_add_heightfield_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, _f32p, C.c_float, C.c_float, C.c_int32]),
     "fw_add_voxel_pair": (C.c_int, [_vp, C.c_int32, C.c_float, _f32p, _f32p, C.c_int32, C.c_int32, _i32p, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "fw_set_boundary_edges": (C.c_int, [_vp, C.c_int32, _i32p, _i32p, _i32p]),
+    "fw_set_flex_scene": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f32p]),
+    "fw_add_flex_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float]),
+    "fw_set_flex_clock": (C.c_int, [_vp, C.c_double]),
+    "fw_read_flex_state": (C.c_int, [_vp, _i32p, C.c_int32, _f32p]),
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
@@ -198,6 +203,30 @@ class NativeWorld:
         nx, ny = occ.shape
         self._check(self._L.fw_add_voxel_pair(self._h, body, penalty, lo[1], hi[1], nx, ny, o[1], float(lbx),
                                               float(lby), float(dx), float(dz)), "fw_add_voxel_pair")
+
+    def set_boundary_edges(self, edges, body_off, body_cnt):
+        e, o, c = _i(np.asarray(edges).reshape(-1)), _i(body_off), _i(body_cnt)
+        self._check(self._L.fw_set_boundary_edges(self._h, len(e[0]) // 2, e[1], o[1], c[1]), "fw_set_boundary_edges")
+
+    def set_flex_scene(self, scene, skip_bvh, dom_obj, dom_body, dom_box):
+        o, b, x = _i(dom_obj), _i(dom_body), _f(np.asarray(dom_box, np.float32).reshape(-1))
+        self._check(self._L.fw_set_flex_scene(self._h, int(scene), int(skip_bvh), len(o[0]), o[1], b[1], x[1]),
+                    "fw_set_flex_scene")
+
+    def add_flex_pair(self, body1, body2, penalty, friction):
+        self._check(self._L.fw_add_flex_pair(self._h, int(body1), int(body2), float(penalty), float(friction)),
+                    "fw_add_flex_pair")
+
+    def read_flex_state(self, n_items: int):
+        """(work-item edge caches int32[n_items], hash grid float32[8])."""
+        cache = np.zeros(max(n_items, 1), np.int32)
+        grid = np.zeros(8, np.float32)
+        self._check(self._L.fw_read_flex_state(self._h, cache.ctypes.data_as(_i32p), int(n_items),
+                                               grid.ctypes.data_as(_f32p)), "fw_read_flex_state")
+        return cache[:n_items], grid
+
+    def set_flex_clock(self, dt: float):
+        self._check(self._L.fw_set_flex_clock(self._h, float(dt)), "fw_set_flex_clock")
 
     def set_path(self, path: int, patches: int = 0):
         self._check(self._L.fw_set_path(self._h, int(path), int(patches)), "fw_set_path")

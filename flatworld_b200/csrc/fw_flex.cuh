@@ -1,0 +1,463 @@
+// fw_flex.cuh -- FEM-FEM penalty contact: the reference's ContactFlexFlex on
+// its spatial-hash path (flatworld/mixedcontact.py:886-1018, launched from
+// run_batched_contacts, mixedcontact.py:1662-1696).
+//
+// Work items (one per boundary node and contact pair side, built on the host
+// in the reference's order, mixedcontact.py:1876-1924) look for the boundary
+// edge of the other body that they penetrate: first the edge they hit last
+// time (the per-item cache), then every candidate the spatial hash returns
+// around the node.  The hash (flatworld/spatialmanager.py) is rebuilt on the
+// device whenever 1/500 s of simulated time has accumulated
+// (femspringmanager.py:1035-1039), from the boundary-edge boxes and the FEM
+// domain boxes of the end of the previous substep.  Its cells list their
+// elements in registration order -- what the reference's counting sort gives
+// when its atomic counters hand out indices in launch order -- so here the
+// cells are filled with atomics and then sorted.  Each work item keeps its own
+// candidate list (the reference's GPU launch shares one 512-entry list among
+// all items, spatialmanager.py:564 / mixedcontact.py:2545, a race; the serial
+// reading is the race-free one).
+//
+// A contact adds a force to the node and the reactions to the edge's two
+// nodes.  In the reference these are atomic_adds in work-item order; here each
+// node keeps a short list of (work item, force) entries, which k_nodes sorts
+// by work item and adds between the plane and the height-field / voxel
+// contact forces -- the reference's launch order -- so no float atomics are
+// needed and the sums repeat bit for bit.
+#pragma once
+
+namespace {
+
+constexpr int kFlexMaxQuery = 512;                   // SpatialHashManager max_query_results
+constexpr int kFlexMaxCells = 100000;                // SpatialHashManager max_cells
+constexpr int kFlexListCap = 16;                     // contributions one node takes per substep
+constexpr double kFlexRebuildInterval = 1.0 / 500.0; // FemSpringManager._sh_rebuild_interval
+constexpr int kFlexScanThreads = 1024;
+
+struct FlexGrid {
+  int tc, cnx, cny, npairs;
+  float olx, oly, gsx, gsy;
+  int estimate;  // ordered-int minimum of the element box diagonals
+  int rebuild;   // this substep rebuilds the hash
+  int err;       // bit 0: a node's contribution list overflowed
+  int pad;
+  double elapsed;   // simulated time since the last rebuild (float64, as the host's float)
+  double clock_dt;  // the substep's dt as the host's float64 holds it
+};
+
+struct FlexDev {
+  int n_items, n_pairs, n_fem, n_dom, skip_bvh, n_be, body0, scene;
+  int max_pairs;
+  float mpd;  // max(pow(100000.0f, 0.5f), 1.0f), evaluated on the host
+  const int32_t* item_node;
+  const int32_t* item_target;  // fem-local index of the body whose edges the item searches
+  const int32_t* item_pair;
+  const float* item_pen;
+  const float* item_fric;
+  int32_t* item_cache;  // boundary edge hit last time, or -1
+  const int2* pair_body;  // (domain1, domain2) global body ids
+  const int2* be;         // per boundary edge: its two global node ids
+  const int32_t* be_dom;  // per boundary edge: fem-local domain
+  const int32_t* be_off;  // per fem-local domain
+  const int32_t* be_cnt;
+  const int32_t* dom_obj;   // per domain of the scene: a broad-phase object (considerContact)
+  const int32_t* dom_body;  // per domain: global body id, or -1 for a ground
+  const float4* dom_box;    // per domain: a ground's static box
+  int32_t* pair_active;
+  int32_t* stamped;  // per fem-local index g: domain g is in a broad-phase pair this substep
+  FlexGrid* g;
+  float4* ebox;
+  int32_t* ecount;
+  int32_t* ebase;
+  int32_t* cell_count;
+  int32_t* cell_start;
+  int32_t* cell_end;
+  int32_t* cursor;
+  int32_t* sorted;
+};
+
+// wp.min / wp.max on floats: a < b ? a : b (first argument on ties)
+__device__ __forceinline__ float wmin(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float wmax(float a, float b) { return a > b ? a : b; }
+
+__device__ __forceinline__ bool flex_stepping(const Dev& d, int s) {
+  return d.scene_active[s] && !d.scene_mode_req[s];
+}
+
+__device__ __forceinline__ float4 ring_box(const Dev& d, int slot, int body) {
+  const int* r = d.aabb_ring + ((size_t)slot * d.B + body) * 4;
+  return make_float4(fw::ord2f(r[0]), fw::ord2f(r[1]), fw::ord2f(r[2]), fw::ord2f(r[3]));
+}
+
+// Broad-phase overlap of two leaf boxes, grown by 10% of their extent on the
+// steps the reference rebuilds its BVH (as fw::pair_gate).
+__device__ __forceinline__ bool flex_boxes_overlap(float4 a, float4 b, int counter) {
+  if (counter % 100 == 0) {
+    const float ax = 0.1f * (a.z - a.x), ay = 0.1f * (a.w - a.y);
+    const float bx = 0.1f * (b.z - b.x), by = 0.1f * (b.w - b.y);
+    a.x = a.x - ax; a.z = a.z + ax; a.y = a.y - ay; a.w = a.w + ay;
+    b.x = b.x - bx; b.z = b.z + bx; b.y = b.y - by; b.w = b.w + by;
+  }
+  return a.x <= b.z && a.z >= b.x && a.y <= b.w && a.w >= b.y;
+}
+
+__device__ __forceinline__ int flex_cell(float delta, float gs, int n) {
+  int c = (int)floorf(delta / gs);
+  c = c > 0 ? c : 0;
+  c = c < n - 1 ? c : n - 1;
+  return c;
+}
+
+// Per substep, before k_elements: scene mode, hash clock, pair activation
+// and the broad-phase domain stamps.  force != 0: the construction-time build
+// (explicitloop.py:383-385) -- rebuild, no contact.
+__global__ void k_flex_pre(Dev d, FlexDev f, int force) {
+  const int s = f.scene;
+  const bool step = !force && flex_stepping(d, s);
+  if (threadIdx.x == 0) {
+    int rb = force ? 1 : 0;
+    if (step) {  // maybe_rebuild_fem_spatial_hash(self.dt)
+      double e = f.g->elapsed + f.g->clock_dt;
+      if (e >= kFlexRebuildInterval) {
+        rb = 1;
+        e = 0.0;
+      }
+      f.g->elapsed = e;
+    }
+    f.g->rebuild = rb;
+    if (rb) f.g->estimate = fw::f2ord(1e30f);
+  }
+  if (!step) return;
+  const int k = d.scene_counter[s];
+  const int slot = k & 1;
+  // _activate_or_fill_pairs: every pair when the loop has no BVH, else BVH overlap
+  for (int p = threadIdx.x; p < f.n_pairs; p += blockDim.x) {
+    const int2 pb = f.pair_body[p];
+    f.pair_active[p] = f.skip_bvh ? 1 : (flex_boxes_overlap(ring_box(d, slot, pb.x), ring_box(d, slot, pb.y), k) ? 1 : 0);
+  }
+  // _scan_bvh_pairs_stamp_kernel: domain g (global index) is stamped when it
+  // is in some broad-phase pair; the contact kernel reads the stamp at the
+  // item's fem-local target index
+  for (int gi = threadIdx.x; gi < f.n_fem; gi += blockDim.x) {
+    int st = 0;
+    if (gi < f.n_dom && f.dom_obj[gi]) {
+      const float4 a = f.dom_body[gi] >= 0 ? ring_box(d, slot, f.dom_body[gi]) : f.dom_box[gi];
+      for (int h = 0; h < f.n_dom && !st; ++h) {
+        if (h == gi || !f.dom_obj[h]) continue;
+        const float4 b = f.dom_body[h] >= 0 ? ring_box(d, slot, f.dom_body[h]) : f.dom_box[h];
+        if (flex_boxes_overlap(a, b, k)) st = 1;
+      }
+    }
+    f.stamped[gi] = st;
+  }
+}
+
+// add_element for every boundary edge (registration index = edge index).
+__global__ void k_flex_boxes(Dev d, FlexDev f) {
+  if (!f.g->rebuild) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= f.n_be) return;
+  const int2 n = f.be[e];
+  const float2 a = d.x[n.x], b = d.x[n.y];
+  float lx = 1e30f, ly = 1e30f, ux = -1e30f, uy = -1e30f;
+  lx = wmin(lx, a.x); ly = wmin(ly, a.y); ux = wmax(ux, a.x); uy = wmax(uy, a.y);
+  lx = wmin(lx, b.x); ly = wmin(ly, b.y); ux = wmax(ux, b.x); uy = wmax(uy, b.y);
+  const float4 bb = make_float4(lx - 0.0f, ly - 0.0f, ux + 0.0f, uy + 0.0f);
+  f.ebox[e] = bb;
+  const float dx = bb.z - bb.x, dy = bb.w - bb.y;
+  atomicMin(&f.g->estimate, fw::f2ord(sqrtf(dx * dx + dy * dy)));
+}
+
+// The global box of the FEM domains (populate kernel) and _build_grid_kernel.
+__global__ void k_flex_grid(Dev d, FlexDev f) {
+  if (!f.g->rebuild || threadIdx.x != 0) return;
+  const int slot = d.scene_counter[f.scene] & 1;
+  float glx = 1e9f, gly = 1e9f, gux = -1e9f, guy = -1e9f;
+  for (int k = 0; k < f.n_fem; ++k) {
+    const float4 bb = ring_box(d, slot, f.body0 + k);
+    glx = wmin(glx, bb.x);
+    gly = wmin(gly, bb.y);
+    gux = wmax(gux, bb.z);
+    guy = wmax(guy, bb.w);
+  }
+  const float extent = wmax(gux - glx, guy - gly);
+  const float expand = extent * 0.01f + 0.0f;
+  glx = glx - expand;
+  gly = gly - expand;
+  gux = gux + expand;
+  guy = guy + expand;
+  float cell = fw::ord2f(f.g->estimate) * 1.5f;
+  const float exx = gux - glx, exy = guy - gly;
+  cell = wmax(cell, exx / f.mpd);
+  cell = wmax(cell, exy / f.mpd);
+  const float cs = cell + 1e-6f;
+  const int nx = (int)wmax(ceilf(exx / cs), 1.0f);
+  const int ny = (int)wmax(ceilf(exy / cs), 1.0f);
+  FlexGrid* g = f.g;
+  g->olx = glx;
+  g->oly = gly;
+  g->cnx = nx;
+  g->cny = ny;
+  g->gsx = exx / (float)nx;
+  g->gsy = exy / (float)ny;
+  const int total = nx * ny;
+  g->tc = total < kFlexMaxCells ? total : kFlexMaxCells;
+}
+
+__device__ __forceinline__ void flex_elem_cells(const FlexGrid& g, float4 eb, int& lx, int& ly, int& ux, int& uy) {
+  lx = flex_cell(eb.x - g.olx, g.gsx, g.cnx);
+  ly = flex_cell(eb.y - g.oly, g.gsy, g.cny);
+  ux = flex_cell(eb.z - g.olx, g.gsx, g.cnx);
+  uy = flex_cell(eb.w - g.oly, g.gsy, g.cny);
+}
+
+// Zero the cell counts; per element, how many (cell, element) pairs it makes.
+__global__ void k_flex_count(FlexDev f) {
+  if (!f.g->rebuild) return;
+  const FlexGrid g = *f.g;
+  const int stride = gridDim.x * blockDim.x;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.tc; c += stride) f.cell_count[c] = 0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.n_be; e += stride) {
+    int lx, ly, ux, uy, n = 0;
+    flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+    for (int ix = lx; ix <= ux; ++ix)
+      for (int iy = ly; iy <= uy; ++iy)
+        if (ix + iy * g.cnx < g.tc) ++n;
+    f.ecount[e] = n;
+  }
+}
+
+// Exclusive scan of n ints (one CTA of kFlexScanThreads); returns the total.
+// Each thread scans a contiguous chunk, the chunk sums are scanned in shared
+// memory.
+__device__ int flex_block_scan(const int32_t* in, int32_t* out, int n) {
+  __shared__ int part[kFlexScanThreads];
+  const int t = threadIdx.x;
+  const int chunk = (n + kFlexScanThreads - 1) / kFlexScanThreads;
+  const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
+  int sum = 0;
+  for (int i = lo; i < hi; ++i) sum += in[i];
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < kFlexScanThreads; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int i = lo; i < hi; ++i) {
+    const int v = in[i];
+    out[i] = run;
+    run += v;
+  }
+  return part[kFlexScanThreads - 1];
+}
+
+// Pair index of each element's first (cell, element) pair: the order of
+// _expand_pairs_kernel's atomic counter in launch order.
+__global__ void __launch_bounds__(kFlexScanThreads) k_flex_scan_elems(FlexDev f) {
+  if (!f.g->rebuild) return;
+  const int total = flex_block_scan(f.ecount, f.ebase, f.n_be);
+  if (threadIdx.x == 0) f.g->npairs = total;
+}
+
+// Cell counts of the pairs kept (pair index < max_pairs).
+__global__ void k_flex_cells(FlexDev f) {
+  if (!f.g->rebuild) return;
+  const FlexGrid g = *f.g;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= f.n_be) return;
+  int lx, ly, ux, uy, p = f.ebase[e];
+  flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+  for (int ix = lx; ix <= ux; ++ix)
+    for (int iy = ly; iy <= uy; ++iy) {
+      const int cid = ix + iy * g.cnx;
+      if (cid < g.tc) {
+        if (p < f.max_pairs) atomicAdd(&f.cell_count[cid], 1);
+        ++p;
+      }
+    }
+}
+
+__global__ void __launch_bounds__(kFlexScanThreads) k_flex_scan_cells(FlexDev f) {
+  if (!f.g->rebuild) return;
+  const int tc = f.g->tc;
+  flex_block_scan(f.cell_count, f.cell_start, tc);
+  __syncthreads();
+  for (int c = threadIdx.x; c < tc; c += blockDim.x) {
+    f.cursor[c] = f.cell_start[c];
+    f.cell_end[c] = f.cell_start[c] + f.cell_count[c];
+  }
+}
+
+__global__ void k_flex_fill(FlexDev f) {
+  if (!f.g->rebuild) return;
+  const FlexGrid g = *f.g;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= f.n_be) return;
+  int lx, ly, ux, uy, p = f.ebase[e];
+  flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+  for (int ix = lx; ix <= ux; ++ix)
+    for (int iy = ly; iy <= uy; ++iy) {
+      const int cid = ix + iy * g.cnx;
+      if (cid < g.tc) {
+        if (p < f.max_pairs) f.sorted[atomicAdd(&f.cursor[cid], 1)] = e;
+        ++p;
+      }
+    }
+}
+
+// Registration order inside every cell (insertion sort; cells hold few elements).
+__global__ void k_flex_sort(FlexDev f) {
+  if (!f.g->rebuild) return;
+  const int tc = f.g->tc;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < tc; c += gridDim.x * blockDim.x) {
+    const int lo = f.cell_start[c], hi = f.cell_end[c];
+    for (int i = lo + 1; i < hi; ++i) {
+      const int v = f.sorted[i];
+      int j = i - 1;
+      while (j >= lo && f.sorted[j] > v) {
+        f.sorted[j + 1] = f.sorted[j];
+        --j;
+      }
+      f.sorted[j + 1] = v;
+    }
+  }
+}
+
+// pointToEdgeContact + detectPointToMeshBoundary (contact_detection.py:15-92):
+// the penetration if |pen| < limit and the point projects inside the edge,
+// else 1e9; the weights either way.
+__device__ __forceinline__ float flex_detect(float2 p, float2 a, float2 b, float limit, float& nx, float& ny,
+                                             float& w0, float& w1) {
+  const float ex = b.x - a.x, ey = b.y - a.y;
+  const float len = sqrtf(ex * ex + ey * ey);
+  float pen = 1e9f, mx = 0.f, my = 0.f;
+  bool inside = false;
+  w0 = 0.f;
+  w1 = 0.f;
+  if (len > 1e-9f) {
+    const float dx = ex / len, dy = ey / len;
+    mx = dy;
+    my = -dx;
+    const float tx = p.x - a.x, ty = p.y - a.y;
+    float t = tx * dx + ty * dy;
+    t = t / len;
+    if (0.0f <= t && t <= 1.0f) {
+      inside = true;
+      pen = tx * mx + ty * my;
+      w0 = 1.0f - t;
+      w1 = t;
+    }
+  }
+  nx = 0.f;
+  ny = 0.f;
+  if (fabsf(pen) < limit && inside) {
+    nx = mx;
+    ny = my;
+    return pen;
+  }
+  return 1e9f;
+}
+
+__device__ __forceinline__ void flex_push(const Dev& d, FlexGrid* g, int node, int item, float2 force) {
+  const int slot = d.flex_slot[node];
+  const int j = atomicAdd(&d.flex_cnt[slot], 1);
+  if (j < kFlexListCap) {
+    d.flex_item[slot * kFlexListCap + j] = item;
+    d.flex_force[slot * kFlexListCap + j] = force;
+  } else {
+    atomicOr(&g->err, 1);
+  }
+}
+
+// _batched_flexflex_contact_kernel_sh, one thread per work item.
+__global__ void __launch_bounds__(128) k_flex_contact(Dev d, FlexDev f) {
+  const int it = blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= f.n_items || !flex_stepping(d, f.scene)) return;
+  if (!f.pair_active[f.item_pair[it]]) return;
+  const int target = f.item_target[it];
+  if (!f.skip_bvh && !f.stamped[target]) return;
+  const FlexGrid g = *f.g;
+  const int nid = f.item_node[it];
+  const int be_off = f.be_off[target], be_cnt = f.be_cnt[target];
+  const float2 p = d.x[nid], vp = d.v[nid];
+  const float pen_k = f.item_pen[it], fric = f.item_fric[it];
+  const float qbuf = wmax(wmax(1e-4f, wmax(g.gsx, g.gsy)), 0.016f);
+  float best = 1e9f, bnx = 0.f, bny = 0.f, bw0 = 0.f, bw1 = 0.f;
+  int bn0 = 0, bn1 = 0;
+  bool found = false;
+  const int cached = f.item_cache[it];
+  int cache_out = cached;
+  if (cached >= be_off && cached < be_off + be_cnt) {
+    const int2 n = f.be[cached];
+    const float2 a = d.x[n.x], b = d.x[n.y];
+    float lx = 1e30f, ly = 1e30f, ux = -1e30f, uy = -1e30f;
+    lx = wmin(lx, a.x); ly = wmin(ly, a.y); ux = wmax(ux, a.x); uy = wmax(uy, a.y);
+    lx = wmin(lx, b.x); ly = wmin(ly, b.y); ux = wmax(ux, b.x); uy = wmax(uy, b.y);
+    const float dx = ux - lx, dy = uy - ly;
+    const float margin = wmax(1e-4f, 1e-2f * sqrtf(dx * dx + dy * dy));
+    lx = lx - margin; ly = ly - margin; ux = ux + margin; uy = uy + margin;
+    const bool outside = wmin(p.x - lx, p.y - ly) < 0.0f || wmin(ux - p.x, uy - p.y) < 0.0f;
+    if (!outside) {
+      float nx, ny, w0, w1;
+      const float pen = flex_detect(p, a, b, margin, nx, ny, w0, w1);
+      if (pen < 1e-4f && fabsf(pen) < margin) {
+        best = pen; bnx = nx; bny = ny; bw0 = w0; bw1 = w1; bn0 = n.x; bn1 = n.y; found = true;
+      }
+    }
+  }
+  if (!found && g.tc > 0) {  // query_point_with_buffer, then every candidate in order
+    int cand[kFlexMaxQuery];
+    int num = 0;
+    const int lx = flex_cell(p.x - qbuf - g.olx, g.gsx, g.cnx), ly = flex_cell(p.y - qbuf - g.oly, g.gsy, g.cny);
+    const int ux = flex_cell(p.x + qbuf - g.olx, g.gsx, g.cnx), uy = flex_cell(p.y + qbuf - g.oly, g.gsy, g.cny);
+    for (int ix = lx; ix <= ux; ++ix)
+      for (int iy = ly; iy <= uy; ++iy) {
+        const int cid = ix + iy * g.cnx;
+        if (cid < 0 || cid >= g.tc) continue;
+        for (int q = f.cell_start[cid]; q < f.cell_end[cid]; ++q) {
+          const int e = f.sorted[q];
+          if (e < 0 || f.be_dom[e] != target) continue;
+          bool dup = false;
+          for (int k = 0; k < num; ++k) dup |= cand[k] == e;
+          if (!dup && num < kFlexMaxQuery) cand[num++] = e;
+        }
+      }
+    for (int j = 0; j < num; ++j) {
+      const int e = cand[j];
+      const int2 n = f.be[e];
+      float nx, ny, w0, w1;
+      const float pen = flex_detect(p, d.x[n.x], d.x[n.y], qbuf, nx, ny, w0, w1);
+      if (pen < best && pen < 1e-4f && fabsf(pen) < qbuf) {
+        best = pen; bnx = nx; bny = ny; bw0 = w0; bw1 = w1; bn0 = n.x; bn1 = n.y; found = true;
+        cache_out = e;
+      }
+    }
+  }
+  if (!found) cache_out = -1;
+  if (cache_out != cached) f.item_cache[it] = cache_out;
+  if (found && best < 0.0f) {
+    const float fx = -bnx * pen_k * best, fy = -bny * pen_k * best;
+    float tx = fx, ty = fy;
+    if (fric > 1e-9f) {
+      const float2 va = d.v[bn0], vb = d.v[bn1];
+      const float sx = va.x * bw0 + vb.x * bw1, sy = va.y * bw0 + vb.y * bw1;
+      const float rx = vp.x - sx, ry = vp.y - sy;
+      const float dn = rx * bnx + ry * bny;
+      const float gx = rx - dn * bnx, gy = ry - dn * bny;
+      const float tl = sqrtf(gx * gx + gy * gy);
+      if (tl > 1e-9f) {
+        const float ddx = -gx / tl, ddy = -gy / tl;
+        const float nl = sqrtf(fx * fx + fy * fy);
+        tx = tx + ddx * fric * nl;
+        ty = ty + ddy * fric * nl;
+      }
+    }
+    flex_push(d, f.g, nid, it, make_float2(tx, ty));
+    flex_push(d, f.g, bn0, it, make_float2(-(tx * bw0), -(ty * bw0)));
+    flex_push(d, f.g, bn1, it, make_float2(-(tx * bw1), -(ty * bw1)));
+  }
+}
+
+}  // namespace

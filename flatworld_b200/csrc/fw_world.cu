@@ -87,7 +87,21 @@ struct Dev {
   int n_e_chunks, n_n_chunks;
   const int2* e_chunks;  // (first element, count <= element block size)
   const int2* n_chunks;  // (first node, count <= node block size)
+  // FEM-FEM contact (fw_flex.cuh); flex_slot == nullptr when the world has none.
+  // Node i (if flex_slot[i] >= 0) receives this substep's contact forces as
+  // (work item, force) entries flex_item/flex_force[slot * kFlexListCap ..
+  // + flex_cnt[slot]), which node_step adds in work-item order.
+  int32_t* flex_slot;
+  int32_t* flex_cnt;
+  int32_t* flex_item;
+  float2* flex_force;
 };
+
+}  // namespace
+
+#include "fw_flex.cuh"
+
+namespace {
 
 // ------------------------------------------------------------------ kernels
 
@@ -166,11 +180,38 @@ __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) element_step(d, e);
 }
 
+// This substep's FEM-FEM contact forces on one node, in work-item order (the
+// reference adds them with atomic_add in launch order): the entries' item ids
+// are distinct, so each pass adds the entry with the next larger id.  The list
+// is emptied for the next substep.
+__device__ __forceinline__ void flex_add(const Dev& d, int slot, float2& f) {
+  const int n = min(d.flex_cnt[slot], kFlexListCap);
+  const int* items = d.flex_item + slot * kFlexListCap;
+  const float2* forces = d.flex_force + slot * kFlexListCap;
+  int last = -1;
+  for (int r = 0; r < n; ++r) {
+    int pick = 0, best = 0x7FFFFFFF;
+    for (int j = 0; j < n; ++j) {
+      const int w = items[j];
+      if (w > last && w < best) {
+        best = w;
+        pick = j;
+      }
+    }
+    const float2 c = forces[pick];
+    f.x += c.x;
+    f.y += c.y;
+    last = best;
+  }
+  d.flex_cnt[slot] = 0;
+}
+
 // The node's own state, its CSR range and its first kNodeCorners corner
 // forces are loaded before the scene lookup, so one node waits on few
 // dependent loads; the corners are then summed in the same ascending order.
 constexpr int kNodeCorners = 6;  // an interior node of a structured triangulation has 6
 
+template <bool FLEX>
 __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
   const uint32_t w = valid ? d.node_word[i] : 0u;
   float2 x = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f), bv0 = make_float2(0.f, 0.f);
@@ -199,7 +240,13 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
     bnd = (w & fw::NODE_BOUNDARY) != 0;
     if (bnd && mode == fw::MODE_STEP) {
       const int p0 = d.body_pair_off[b], pn = d.body_pair_cnt[b];
+      const int fs = FLEX ? d.flex_slot[i] : -1;
+      bool flex_done = !FLEX || fs < 0;
       for (int k = 0; k < pn; ++k) {
+        if (FLEX && !flex_done && d.pairs[p0 + k].kind != fw::PAIR_PLANE) {
+          flex_add(d, fs, f);  // FEM-FEM contact runs after the planes, before the height fields / voxels
+          flex_done = true;
+        }
         if (!d.pair_active[p0 + k]) continue;
         float2 cf;
         if (fw::contact_force(d.pairs[p0 + k], d.heights, d.occ, x, v, dt, cf)) {
@@ -207,6 +254,7 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
           f.y += cf.y;
         }
       }
+      if (FLEX && !flex_done) flex_add(d, fs, f);
     }
 #pragma unroll
     for (int u = 0; u < kNodeCorners; ++u)  // contiguous, ascending element
@@ -262,12 +310,19 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
   if (d.use_chunks) {
     for (int c = blockIdx.x; c < d.n_n_chunks; c += gridDim.x) {
       const int2 ch = d.n_chunks[c];
-      node_step(d, ch.x + (int)threadIdx.x, (int)threadIdx.x < ch.y);
+      node_step<false>(d, ch.x + (int)threadIdx.x, (int)threadIdx.x < ch.y);
     }
     return;
   }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  node_step(d, i, i < d.N);
+  node_step<false>(d, i, i < d.N);
+}
+
+// k_nodes of worlds with FEM-FEM contact: the node's contact forces from the
+// work items join its plane and ground contact forces in launch order.
+__global__ void __launch_bounds__(kMaxBlock) k_nodes_flex(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  node_step<true>(d, i, i < d.N);
 }
 
 // Reference-shape precompute, _prepare_fem_data_kernel
@@ -745,6 +800,20 @@ struct fw_ctx {
   size_t res_smem = 0;
   std::string res_reason;
   int64_t host_counter = 0;  // step counter of scene 0 (single-scene worlds)
+  // FEM-FEM contact (fw_flex.cuh): staging, then the device state
+  std::vector<int2> h_be;                   // boundary edges, global node ids
+  std::vector<int32_t> h_be_off, h_be_cnt;  // per body
+  struct FlexPair {
+    int b1, b2;
+    float pen, fric;
+  };
+  std::vector<FlexPair> h_flex;
+  int flex_scene = -1, flex_skip_bvh = 0;
+  std::vector<int32_t> h_dom_obj, h_dom_body;
+  std::vector<float4> h_dom_box;
+  bool has_flex = false;
+  FlexDev fx{};
+  double flex_clock = 0.0;  // host copy of the last fw_set_flex_clock value
 };
 
 namespace {
@@ -803,9 +872,36 @@ void set_grids(fw_ctx* c) {
   c->grid_n = std::max(1, (N + c->block_n - 1) / c->block_n);
 }
 
+// The FEM-FEM contact of one substep (force: the construction-time hash
+// build only): activation and hash clock, the hash rebuild (each kernel
+// returns at once unless the clock fired), the contact work items.
+void flex_launch(fw_ctx* c, int force) {
+  const FlexDev& f = c->fx;
+  const int eb = (f.n_be + kBlock - 1) / kBlock;
+  const int wide = 2 * c->sms;
+  k_flex_pre<<<1, 128, 0, c->stream>>>(c->d, f, force);
+  k_flex_boxes<<<eb, kBlock, 0, c->stream>>>(c->d, f);
+  k_flex_grid<<<1, 32, 0, c->stream>>>(c->d, f);
+  k_flex_count<<<wide, kBlock, 0, c->stream>>>(f);
+  k_flex_scan_elems<<<1, kFlexScanThreads, 0, c->stream>>>(f);
+  k_flex_cells<<<eb, kBlock, 0, c->stream>>>(f);
+  k_flex_scan_cells<<<1, kFlexScanThreads, 0, c->stream>>>(f);
+  k_flex_fill<<<eb, kBlock, 0, c->stream>>>(f);
+  k_flex_sort<<<wide, kBlock, 0, c->stream>>>(f);
+  c->launches += 9;
+  if (!force) {
+    k_flex_contact<<<(f.n_items + 127) / 128, 128, 0, c->stream>>>(c->d, f);
+    c->launches += 1;
+  }
+}
+
 int launch_step(fw_ctx* c) {
+  if (c->has_flex) flex_launch(c, 0);
   k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
-  k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+  if (c->has_flex)
+    k_nodes_flex<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+  else
+    k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
   c->launches += 2;
   return check_kernel(c, "step");
 }
@@ -860,12 +956,12 @@ uint32_t float_bits(float v) {
 int get_graph(fw_ctx* c, int n, cudaGraphExec_t* out) {
   const uint64_t key = ((uint64_t)(c->d.uniform_dt ? 1 : 0) << 63) | ((uint64_t)n << 32) |
                        (c->d.uniform_dt ? float_bits(c->d.dt_uniform) : 0u);
-  return cached_graph(c, c->graphs, key, [&] {
-    for (int k = 0; k < n; ++k) {
-      k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
-      k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
-    }
+  const int64_t before = c->launches;
+  const int rc = cached_graph(c, c->graphs, key, [&] {
+    for (int k = 0; k < n; ++k) launch_step(c);  // every launch of a substep, FEM-FEM contact included
   }, out);
+  c->launches = before;  // counted when the graph is launched
+  return rc;
 }
 
 int launch_resident(fw_ctx* c, int n);
@@ -886,7 +982,7 @@ int run_steps(fw_ctx* c, int n) {
     if (rc) return rc;
     while (n >= kGraphSteps) {
       FW_CUDA(c, cudaGraphLaunch(g, c->stream));
-      c->launches += 2 * kGraphSteps;
+      c->launches += (c->has_flex ? 12 : 2) * kGraphSteps;
       n -= kGraphSteps;
     }
   }
@@ -894,7 +990,7 @@ int run_steps(fw_ctx* c, int n) {
     cudaGraphExec_t g = nullptr;
     if ((rc = get_graph(c, n, &g))) return rc;
     FW_CUDA(c, cudaGraphLaunch(g, c->stream));
-    c->launches += 2 * n;
+    c->launches += (c->has_flex ? 12 : 2) * n;
     n = 0;
   }
   for (int k = 0; k < n && rc == FW_OK; ++k) rc = launch_step(c);
@@ -1309,6 +1405,14 @@ int launch_resident(fw_ctx* c, int n) {
 }
 
 int check_device_error(fw_ctx* c) {
+  if (c->has_flex) {
+    int ferr = 0;
+    FW_CUDA(c, cudaMemcpyAsync(&ferr, &c->fx.g->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (ferr & 1)
+      return fail(c, FW_ERR_ARG, "FEM-FEM contact: a node received more than %d contact forces in one substep",
+                  kFlexListCap);
+  }
   if (c->path != FW_PATH_RESIDENT) return FW_OK;
   int err = 0;
   FW_CUDA(c, cudaMemcpyAsync(&err, c->res.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1549,6 +1653,192 @@ int fw_add_voxel_pair(fw_ctx* c, int32_t body, float penalty, const float* lo, c
   return add_pair(c, p, lo, hi);
 }
 
+int fw_set_boundary_edges(fw_ctx* c, int32_t n_edges, const int32_t* edges, const int32_t* body_off,
+                          const int32_t* body_cnt) {
+  if (!c || n_edges < 0 || (n_edges && !edges) || !body_off || !body_cnt) return FW_ERR_ARG;
+  if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_set_boundary_edges after fw_finalize / on an arena");
+  if (c->B <= 0) return fail(c, FW_ERR_STATE, "fw_set_boundary_edges before fw_set_bodies");
+  for (int b = 0; b < c->B; ++b)
+    if (body_off[b] < 0 || body_cnt[b] < 0 || (int64_t)body_off[b] + body_cnt[b] > n_edges)
+      return fail(c, FW_ERR_ARG, "fw_set_boundary_edges: body %d range outside [0, %d)", b, n_edges);
+  c->h_be.resize(n_edges);
+  for (int k = 0; k < n_edges; ++k) c->h_be[k] = make_int2(edges[2 * k], edges[2 * k + 1]);
+  c->h_be_off.assign(body_off, body_off + c->B);
+  c->h_be_cnt.assign(body_cnt, body_cnt + c->B);
+  return FW_OK;
+}
+
+int fw_set_flex_scene(fw_ctx* c, int32_t scene, int32_t skip_bvh, int32_t n_domains, const int32_t* dom_obj,
+                      const int32_t* dom_body, const float* dom_box) {
+  if (!c || n_domains < 0 || (n_domains && (!dom_obj || !dom_body || !dom_box))) return FW_ERR_ARG;
+  if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_set_flex_scene after fw_finalize / on an arena");
+  c->flex_scene = scene;
+  c->flex_skip_bvh = skip_bvh ? 1 : 0;
+  c->h_dom_obj.assign(dom_obj, dom_obj + n_domains);
+  c->h_dom_body.assign(dom_body, dom_body + n_domains);
+  c->h_dom_box.resize(n_domains);
+  for (int g = 0; g < n_domains; ++g)
+    c->h_dom_box[g] = make_float4(dom_box[4 * g], dom_box[4 * g + 1], dom_box[4 * g + 2], dom_box[4 * g + 3]);
+  return FW_OK;
+}
+
+int fw_add_flex_pair(fw_ctx* c, int32_t body1, int32_t body2, float penalty, float friction) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_add_flex_pair after fw_finalize / on an arena");
+  if (body1 < 0 || body2 < 0 || body1 >= c->B || body2 >= c->B || body1 == body2)
+    return fail(c, FW_ERR_ARG, "fw_add_flex_pair: bodies %d, %d", body1, body2);
+  c->h_flex.push_back(fw_ctx::FlexPair{body1, body2, penalty, friction});
+  return FW_OK;
+}
+
+int fw_read_flex_state(fw_ctx* c, int32_t* item_cache, int32_t n_items, float* grid) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->has_flex) return fail(c, FW_ERR_STATE, "fw_read_flex_state: the world has no FEM-FEM contact");
+  if (n_items != c->fx.n_items) return fail(c, FW_ERR_ARG, "fw_read_flex_state: %d work items, not %d", c->fx.n_items, n_items);
+  FlexGrid g{};
+  if (item_cache)
+    FW_CUDA(c, cudaMemcpyAsync(item_cache, c->fx.item_cache, sizeof(int32_t) * n_items, cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(&g, c->fx.g, sizeof(FlexGrid), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (grid) {
+    int est = g.estimate >= 0 ? g.estimate : g.estimate ^ 0x7FFFFFFF;  // ordered int -> float bits
+    float estf;
+    memcpy(&estf, &est, sizeof(float));
+    const float v[8] = {(float)g.tc, (float)g.cnx, (float)g.cny, g.olx, g.oly, g.gsx, g.gsy, estf};
+    memcpy(grid, v, sizeof(v));
+  }
+  return FW_OK;
+}
+
+int fw_set_flex_clock(fw_ctx* c, double dt) {
+  if (!c) return FW_ERR_ARG;
+  c->flex_clock = dt;
+  if (c->has_flex)
+    FW_CUDA(c, cudaMemcpyAsync(&c->fx.g->clock_dt, &c->flex_clock, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return FW_OK;
+}
+
+// Device state of the FEM-FEM contact of a single-scene world: work items in
+// the reference's order (per pair: domain2's boundary nodes against domain1's
+// edges, then domain1's against domain2's; mixedcontact.py:1876-1924), the
+// spatial hash arrays sized as the reference sizes them
+// (femspringmanager.py:545-548: MAX_BOUNDARY_ELEMENTS; spatialmanager.py:520-525:
+// 3^2 pairs per element), and the per-node contribution lists.
+int build_flex(fw_ctx* c) {
+  const int B = c->B, N = c->N;
+  if (c->S != 1 || c->flex_scene != 0)
+    return fail(c, FW_ERR_ARG, "FEM-FEM contact: one scene per world (fw_set_flex_scene(ctx, 0, ...))");
+  if ((int)c->h_be_off.size() != B) return fail(c, FW_ERR_ARG, "FEM-FEM contact: fw_set_boundary_edges missing");
+  const int n_be = (int)c->h_be.size();
+  std::vector<int32_t> be_dom(std::max(n_be, 1), 0), be_off(B), be_cnt(B);
+  int run = 0;
+  for (int b = 0; b < B; ++b) {
+    if (c->h_be_off[b] != run) return fail(c, FW_ERR_ARG, "FEM-FEM contact: boundary edges must be stored body by body");
+    be_off[b] = c->h_be_off[b];
+    be_cnt[b] = c->h_be_cnt[b];
+    for (int k = 0; k < be_cnt[b]; ++k) {
+      const int2 e = c->h_be[run + k];
+      if (e.x < c->h_noff[b] || e.x >= c->h_noff[b] + c->h_ncnt[b] || e.y < c->h_noff[b] ||
+          e.y >= c->h_noff[b] + c->h_ncnt[b])
+        return fail(c, FW_ERR_ARG, "FEM-FEM contact: boundary edge %d leaves body %d", run + k, b);
+      be_dom[run + k] = b;
+    }
+    run += be_cnt[b];
+  }
+  if (run != n_be || n_be == 0) return fail(c, FW_ERR_ARG, "FEM-FEM contact: boundary edge counts do not add up");
+  const int n_dom = (int)c->h_dom_obj.size();
+  for (int g = 0; g < n_dom; ++g)
+    if (c->h_dom_body[g] >= B) return fail(c, FW_ERR_ARG, "FEM-FEM contact: domain %d names body %d", g, c->h_dom_body[g]);
+  std::vector<int32_t> item_node, item_target, item_pair;
+  std::vector<float> item_pen, item_fric;
+  std::vector<int2> pair_body;
+  std::vector<int32_t> slot(N, -1);
+  int n_slots = 0;
+  for (size_t p = 0; p < c->h_flex.size(); ++p) {
+    const fw_ctx::FlexPair& fp = c->h_flex[p];
+    pair_body.push_back(make_int2(fp.b1, fp.b2));
+    for (int side = 0; side < 2; ++side) {
+      const int src = side == 0 ? fp.b2 : fp.b1, dst = side == 0 ? fp.b1 : fp.b2;
+      for (int k = 0; k < c->h_bncnt[src]; ++k) {
+        const int n = c->h_bnodes[c->h_bnoff[src] + k];
+        item_node.push_back(n);
+        item_target.push_back(dst);
+        item_pair.push_back((int)p);
+        item_pen.push_back(fp.pen);
+        item_fric.push_back(fp.fric);
+        if (slot[n] < 0) slot[n] = n_slots++;
+      }
+    }
+  }
+  for (const int2& e : c->h_be)  // edge nodes receive the reactions
+    for (int n : {e.x, e.y})
+      if (slot[n] < 0) slot[n] = n_slots++;
+  const int n_items = (int)item_node.size();
+  const int max_nodes = std::max(N + 1024, 2048);
+  const int max_elements = std::max(n_be + 1024, max_nodes);
+  FlexDev f{};
+  f.n_items = n_items;
+  f.n_pairs = (int)pair_body.size();
+  f.n_fem = B;
+  f.n_dom = n_dom;
+  f.skip_bvh = c->flex_skip_bvh;
+  f.n_be = n_be;
+  f.body0 = 0;
+  f.scene = 0;
+  f.max_pairs = 9 * max_elements;
+  f.mpd = std::max(powf(100000.0f, 0.5f), 1.0f);
+  int rc;
+  int32_t *inode = nullptr, *itgt = nullptr, *ipair = nullptr, *icache = nullptr, *bdom = nullptr, *boff = nullptr,
+          *bcnt = nullptr, *dobj = nullptr, *dbody = nullptr, *pact = nullptr, *stamp = nullptr, *ecount = nullptr,
+          *ebase = nullptr, *ccount = nullptr, *cstart = nullptr, *cend = nullptr, *cursor = nullptr,
+          *sorted = nullptr, *dslot = nullptr, *dcnt = nullptr, *ditem = nullptr;
+  float *ipen = nullptr, *ifric = nullptr;
+  int2 *pbody = nullptr, *dbe = nullptr;
+  float4 *dbox = nullptr, *ebox = nullptr;
+  float2* dforce = nullptr;
+  FlexGrid* grid = nullptr;
+  std::vector<int32_t> minus1(std::max(n_items, 1), -1);
+  std::vector<float4> dom_box = c->h_dom_box;
+  std::vector<int32_t> dom_obj = c->h_dom_obj, dom_body = c->h_dom_body;
+  if (dom_obj.empty()) {
+    dom_obj.push_back(0);
+    dom_body.push_back(-1);
+    dom_box.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+  }
+  if ((rc = upload(c, &inode, item_node)) || (rc = upload(c, &itgt, item_target)) || (rc = upload(c, &ipair, item_pair)) ||
+      (rc = upload(c, &ipen, item_pen)) || (rc = upload(c, &ifric, item_fric)) || (rc = upload(c, &icache, minus1)) ||
+      (rc = upload(c, &pbody, pair_body)) || (rc = upload(c, &dbe, c->h_be)) || (rc = upload(c, &bdom, be_dom)) ||
+      (rc = upload(c, &boff, be_off)) || (rc = upload(c, &bcnt, be_cnt)) || (rc = upload(c, &dobj, dom_obj)) ||
+      (rc = upload(c, &dbody, dom_body)) || (rc = upload(c, &dbox, dom_box)) ||
+      (rc = dalloc(c, &pact, std::max(1, f.n_pairs))) || (rc = dalloc(c, &stamp, std::max(1, B))) ||
+      (rc = dalloc(c, &grid, 1)) || (rc = dalloc(c, &ebox, n_be)) || (rc = dalloc(c, &ecount, n_be)) ||
+      (rc = dalloc(c, &ebase, n_be)) || (rc = dalloc(c, &ccount, kFlexMaxCells)) ||
+      (rc = dalloc(c, &cstart, kFlexMaxCells)) || (rc = dalloc(c, &cend, kFlexMaxCells)) ||
+      (rc = dalloc(c, &cursor, kFlexMaxCells)) || (rc = dalloc(c, &sorted, f.max_pairs)) ||
+      (rc = upload(c, &dslot, slot)) || (rc = dalloc(c, &dcnt, std::max(1, n_slots))) ||
+      (rc = dalloc(c, &ditem, std::max(1, n_slots) * kFlexListCap)) ||
+      (rc = dalloc(c, &dforce, std::max(1, n_slots) * kFlexListCap)))
+    return rc;
+  FW_CUDA(c, cudaMemsetAsync(grid, 0, sizeof(FlexGrid), c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(&grid->clock_dt, &c->flex_clock, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(dcnt, 0, sizeof(int32_t) * std::max(1, n_slots), c->stream));
+  FW_CUDA(c, cudaMemsetAsync(cstart, 0, sizeof(int32_t) * kFlexMaxCells, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(cend, 0, sizeof(int32_t) * kFlexMaxCells, c->stream));
+  f.item_node = inode; f.item_target = itgt; f.item_pair = ipair; f.item_pen = ipen; f.item_fric = ifric;
+  f.item_cache = icache; f.pair_body = pbody; f.be = dbe; f.be_dom = bdom; f.be_off = boff; f.be_cnt = bcnt;
+  f.dom_obj = dobj; f.dom_body = dbody; f.dom_box = dbox; f.pair_active = pact; f.stamped = stamp; f.g = grid;
+  f.ebox = ebox; f.ecount = ecount; f.ebase = ebase; f.cell_count = ccount; f.cell_start = cstart;
+  f.cell_end = cend; f.cursor = cursor; f.sorted = sorted;
+  c->fx = f;
+  c->d.flex_slot = dslot;
+  c->d.flex_cnt = dcnt;
+  c->d.flex_item = ditem;
+  c->d.flex_force = dforce;
+  c->has_flex = true;
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  return FW_OK;
+}
+
 int fw_finalize(fw_ctx* c) {
   if (!c) return FW_ERR_ARG;
   if (c->finalized) return fail(c, FW_ERR_STATE, "fw_finalize called twice");
@@ -1677,10 +1967,24 @@ int fw_finalize(fw_ctx* c) {
   if ((rc = check_kernel(c, "prepare"))) return rc;
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
   set_grids(c);
+  if (!c->h_flex.empty()) {
+    if (c->path_req == FW_PATH_RESIDENT || c->path_req == FW_PATH_STREAM)
+      return fail(c, FW_ERR_ARG, "FEM-FEM contact runs on the gather path only");
+    if ((rc = build_flex(c))) return rc;
+  }
   // zero-dt construction step (setGlobalAABB -> substep(0, 0))
   if ((rc = launch_step(c))) return rc;
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (c->has_flex) {  // the initial FEM spatial hash (explicitloop.py:383-385)
+    flex_launch(c, 1);
+    if ((rc = check_kernel(c, "FEM-FEM hash"))) return rc;
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   c->path = FW_PATH_GATHER;
+  if (c->has_flex) {
+    c->finalized = true;
+    return FW_OK;
+  }
   if (c->path_req == FW_PATH_STREAM) {
     if ((rc = build_stream(c, off, slot, x0, has_j2))) return rc;
     c->path = FW_PATH_STREAM;
@@ -1757,6 +2061,8 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
 }
 
 int fw_snapshot(fw_ctx* c, int32_t slot) {
+  if (c && c->has_flex)
+    return fail(c, FW_ERR_STATE, "snapshots do not hold the FEM-FEM contact state (hash, element caches)");
   if (!c) return FW_ERR_ARG;
   if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_snapshot before fw_finalize");
   if (slot < 0 || slot >= 1024) return fail(c, FW_ERR_ARG, "fw_snapshot: slot outside [0, 1024)");
@@ -1782,6 +2088,8 @@ int fw_snapshot(fw_ctx* c, int32_t slot) {
 }
 
 int fw_restore(fw_ctx* c, int32_t slot) {
+  if (c && c->has_flex)
+    return fail(c, FW_ERR_STATE, "snapshots do not hold the FEM-FEM contact state (hash, element caches)");
   if (!c) return FW_ERR_ARG;
   if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_restore before fw_finalize");
   if (slot < 0 || slot >= (int)c->snaps.size() || !c->snaps[slot].valid)
@@ -2106,6 +2414,7 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
 }
 
 int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
+  if (c && c->has_flex) return fail(c, FW_ERR_STATE, "the adjoint does not cover FEM-FEM contact");
   if (!c) return FW_ERR_ARG;
   // The forward may run on either path (identical bits); the recompute and the
   // reverse use the gather kernels and data, which every non-arena world has.
@@ -2261,6 +2570,7 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
 }
 
 int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE, int32_t on_device) {
+  if (c && c->has_flex) return fail(c, FW_ERR_STATE, "the tangent does not cover FEM-FEM contact");
   if (!c) return FW_ERR_ARG;
   if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)
     return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world on the gather or resident path");

@@ -217,16 +217,27 @@ class ExplicitLoop:
         self.numContacts = len(layout.contacts)
         self._unbatched_contacts = layout.unbatched
         self._counter_py = 0
+        if layout.flex and self.ties:
+            raise NotImplementedError("tied FEM-FEM pairs (ExplicitLoop ties=...) are not part of flatworld_b200")
         self._packed = PackedWorld([layout])
         self._native = build_native(self._packed, device=device, path=path, patches=patches,
                                     front_warps=front_warps, res_sync=res_sync)
         self.path, self.patches = self._native.get_path()
         self.aabb = _AABBView(self)
         self.femSpringManager = FemSpringManager(self, self._packed, self._native, 0)
+        self._flex_clock = None
+
+    def _clock(self, dt: float):
+        """Hand the substep's float64 dt to the FEM-FEM hash-refresh clock
+        (femspringmanager.py:1035-1039 accumulates ``self.dt`` in float64)."""
+        if self._layout.flex and dt != self._flex_clock:
+            self._native.set_flex_clock(dt)
+            self._flex_clock = dt
 
     # ---- stepping
     def advance(self):
         """One substep of ``self.dt`` (explicitloop.py:473-555)."""
+        self._clock(self.dt)
         self._native.step(1, float(np.float32(self.dt)))
         self._counter_py += 1
 
@@ -234,6 +245,7 @@ class ExplicitLoop:
         """``n`` substeps of ``dt`` (default ``self.dt``) queued in one call."""
         if dt is not None:
             self.dt = dt
+        self._clock(self.dt)
         self._native.step(int(n), float(np.float32(self.dt)))
         self._counter_py += int(n)
 
@@ -244,6 +256,7 @@ class ExplicitLoop:
         total = 0
         for n, sub in runs:
             self.dt = sub
+            self._clock(sub)
             self._native.step(n, float(np.float32(sub)))
             self._counter_py += n
             total += n

@@ -44,25 +44,29 @@ def contact_stable_time(penalty: float, dom) -> float:
 
 @dataclass
 class ContactSpec:
-    kind: str  # "plane" | "heightfield" | "voxel"
-    fem: object
-    ground: object
+    kind: str  # "plane" | "heightfield" | "voxel" | "flex"
+    fem: object     # the FEM domain (for "flex": domain1, the later domain)
+    ground: object  # the ground (for "flex": domain2, the earlier FEM domain)
     pair_ids: tuple  # (later domain index, earlier domain index), explicitloop.py:275-276
     penalty: float
     stableTime: float
+    friction: float = 0.0
 
 
 def _contact_helper(di, dj, ctype, i, j):
-    """contactHelper (femcontact.py:283-303) restricted to the FEM-ground pairs."""
+    """contactHelper (femcontact.py:283-303) restricted to the FEM-ground and
+    FEM-FEM pairs."""
     kinds = {
         ContactType.FLEXANLAYTICAL: "plane",
         ContactType.FEXHEIGHTFIELD: "heightfield",
         ContactType.FLEXVOXELMAP: "voxel",
     }
     if ctype == ContactType.FLEXFLEX:
-        raise NotImplementedError(
-            "FEM-FEM contact (two FEM domains with considerContact=True in one loop) is outside "
-            "flatworld_b200's scope; set considerContact=False on the FEM domains that need not touch")
+        # ContactFlexFlex (femcontact.py:199-206): the smaller side penalty, the
+        # smaller side stable time; friction = max of the two (mixedcontact.py:1889)
+        pen = min(segment_penalty(di), segment_penalty(dj)) * 1.0
+        st = min(contact_stable_time(pen, di), contact_stable_time(pen, dj))
+        return ContactSpec("flex", di, dj, (i, j), pen, st, max(di.friction, dj.friction))
     if ctype not in kinds:
         return None
     fem, ground = (di, dj) if di.type == DomainType.FEM else (dj, di)
@@ -137,6 +141,11 @@ class SceneLayout:
             self.unbatched += vox
             vox = []
         self.pairs = anal + hf + vox
+        # FEM-FEM pairs in contact-creation order (mixedcontact.py:1869-1935); the
+        # loop skips the BVH (all of them stay active) when it has no ground
+        # contact at all (explicitloop.py:367-373)
+        self.flex = [c for c in contacts if c.kind == "flex"]
+        self.skip_bvh = not (anal or hf or vox or self.unbatched)
         self.n_nodes = sum(d.nnodes for d in self.fem)
         self.n_elems = sum(d.nelements for d in self.fem)
 
@@ -161,6 +170,7 @@ class PackedWorld:
         syv = np.zeros(E, np.float32)
         Hv = np.zeros(E, np.float32)
         noff, ncnt, eoff, ecnt, bscene, bnoff, bncnt, bnodes = [], [], [], [], [], [], [], []
+        beoff, becnt, bedges = [], [], []
         self.body_of = {}  # (scene idx, fem idx) -> global body id
         self.scene_bodies = []
         n0 = e0 = b0 = 0
@@ -209,6 +219,10 @@ class PackedWorld:
                 bn = n0 + np.asarray(mesh.boundaryNodes, dtype=np.int64)
                 bncnt.append(len(bn))
                 bnodes.append(bn)
+                beoff.append(sum(len(x) for x in bedges))
+                be = n0 + np.asarray(mesh.boundaryElements, dtype=np.int64).reshape(-1, 2)
+                becnt.append(len(be))
+                bedges.append(be)
                 n0 += nn
                 e0 += ne
             b0 += len(sc.fem)
@@ -223,8 +237,33 @@ class PackedWorld:
         self.bnoff = np.asarray(bnoff, np.int32)
         self.bncnt = np.asarray(bncnt, np.int32)
         self.bnodes = np.concatenate(bnodes).astype(np.int32) if bnodes else np.zeros(0, np.int32)
+        self.beoff = np.asarray(beoff, np.int32)
+        self.becnt = np.asarray(becnt, np.int32)
+        self.bedges = np.concatenate(bedges).astype(np.int32) if bedges else np.zeros((0, 2), np.int32)
         self.B = len(noff)
         self.S = len(scenes)
+
+    def flex_records(self):
+        """Per scene with FEM-FEM pairs: (scene, skip_bvh, dom_obj, dom_body,
+        dom_box, [(body1, body2, penalty f32, friction f32)])."""
+        out = []
+        for si, sc in enumerate(self.scenes):
+            if not sc.flex:
+                continue
+            fem_index = {id(d): k for k, d in enumerate(sc.fem)}
+            dom_obj = np.asarray([1 if d.considerContact else 0 for d in sc.domains], np.int32)
+            dom_body = np.asarray([self.body_of[(si, fem_index[id(d)])] if id(d) in fem_index else -1
+                                   for d in sc.domains], np.int32)
+            dom_box = np.zeros((len(sc.domains), 4), np.float32)
+            for g, d in enumerate(sc.domains):
+                if id(d) not in fem_index and d.considerContact:
+                    lo, hi = d.getBBox()
+                    dom_box[g, :2] = np.asarray(lo, np.float32).reshape(2)
+                    dom_box[g, 2:] = np.asarray(hi, np.float32).reshape(2)
+            pairs = [(self.body_of[(si, fem_index[id(c.fem)])], self.body_of[(si, fem_index[id(c.ground)])],
+                      np.float32(c.penalty), np.float32(c.friction)) for c in sc.flex]
+            out.append((si, sc.skip_bvh, dom_obj, dom_body, dom_box, pairs))
+        return out
 
     def pair_records(self):
         """(kind, body, penalty f32, gate lo, gate hi, ground) in launch order."""
@@ -272,6 +311,13 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
             nw.add_heightfield(body, pen, lo, hi, g.height, g.lb[0], g.ub[0], 1 if g.reverse else 0)
         else:
             nw.add_voxel(body, pen, lo, hi, np.asarray(g.occ, np.int32), g.lb[0], g.lb[1], g.dx, g.dz)
+    flex = packed.flex_records()
+    if flex:
+        nw.set_boundary_edges(packed.bedges, packed.beoff, packed.becnt)
+        for si, skip, obj, body, box, pairs in flex:
+            nw.set_flex_scene(si, skip, obj, body, box)
+            for b1, b2, pen, fric in pairs:
+                nw.add_flex_pair(b1, b2, pen, fric)
 
 
 def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):

@@ -122,6 +122,38 @@ int fw_add_voxel_pair(fw_ctx* ctx, int32_t body, float penalty, const float* gat
                       const float* gate_hi, int32_t nx, int32_t ny, const int32_t* occupancy,
                       float lb_x, float lb_y, float dx, float dz);
 
+/* FEM-FEM penalty contact (single-scene worlds, gather path).
+ * fw_set_boundary_edges: every body's boundary edges (2 global node ids each,
+ * in mesh order and orientation, mesh.py:53-71), stored body by body:
+ * body b's at edges[2*body_off[b] ..], body_cnt[b] of them.  Replaces the
+ * boundaryElements / domainBoundaryElemOffset packing, femspringmanager.py:783-799.
+ * fw_set_flex_scene: the loop's domains in loop order -- dom_obj[g] != 0 if
+ * domain g takes part in the broad phase (considerContact), dom_body[g] its
+ * body id (-1 for a ground), dom_box the ground's getBBox() (lo x, lo y, hi x,
+ * hi y); skip_bvh != 0 when the loop has no plane, height-field, voxel or
+ * unbatched ground contact (every FEM-FEM pair then stays active).  Replaces
+ * the BVH set-up and domain stamps, explicitloop.py:203-227, 362-373, 495-514.
+ * fw_add_flex_pair: one ContactFlexFlex (femcontact.py:199-206): body1 =
+ * domain1, body2 = domain2, penalty = float32 of min(2 K1, 2 K2), friction =
+ * max of the two domains'.  Work lists and the per-substep launch replace
+ * mixedcontact.py:1869-1935 and _batched_flexflex_contact_kernel_sh,
+ * mixedcontact.py:886-1018, with the spatial hash of spatialmanager.py.
+ * fw_set_flex_clock: the substep dt as the host's float64 holds it, which the
+ * hash-refresh clock accumulates (femspringmanager.py:1035-1039: rebuilt once
+ * 1/500 s has accumulated); call it before fw_step whenever dt changes. */
+int fw_set_boundary_edges(fw_ctx* ctx, int32_t n_edges, const int32_t* edges, const int32_t* body_off,
+                          const int32_t* body_cnt);
+int fw_set_flex_scene(fw_ctx* ctx, int32_t scene, int32_t skip_bvh, int32_t n_domains, const int32_t* dom_obj,
+                      const int32_t* dom_body, const float* dom_box);
+int fw_add_flex_pair(fw_ctx* ctx, int32_t body1, int32_t body2, float penalty, float friction);
+int fw_set_flex_clock(fw_ctx* ctx, double dt);
+/* The work items' edge caches (boundary edge index hit last substep, or -1;
+ * n_items must equal the world's count) and the spatial hash grid: tc, nx, ny,
+ * origin x, origin y, cell x, cell y, element-box diagonal minimum.  The
+ * reference keeps these in bc_flex_cache_elem and SpatialHashManager
+ * (mixedcontact.py:1915, spatialmanager.py:538-551); here for tests. */
+int fw_read_flex_state(fw_ctx* ctx, int32_t* item_cache, int32_t n_items, float* grid);
+
 /* Upload, precompute reference-shape data (area, Dm^-1, lumped mass, Lame
  * constants, node->element gather lists) and run the zero-dt step that the
  * reference runs at construction.

@@ -35,6 +35,13 @@
  *   flatworld/mixedcontact.py:1566-1643    heightfield / voxel contact kernels
  *   flatworld/mixedcontact.py:1654-1755    run_batched_contacts (launch order)
  *   flatworld/explicitloop.py:473-555      advance (contacts -> femStep)
+ *   flatworld/mixedcontact.py:886-1018     _batched_flexflex_contact_kernel_sh (FEM-FEM)
+ *   flatworld/mixedcontact.py:1654-1696    flex pair activation, hash refresh, launch
+ *   flatworld/explicitloop.py:495-514      BVH domain stamps (+ :451-463 scan kernel)
+ *   flatworld/contact_detection.py:15-92   pointToEdgeContact, detectPointToMeshBoundary
+ *   flatworld/spatialmanager.py:30-198     add_element, query_point_with_buffer
+ *   flatworld/spatialmanager.py:200-420, 613-712  hash build kernels, build()
+ *   flatworld/femspringmanager.py:1035-1063 + its populate kernel  FEM hash refresh
  *
  * Warp builtins (warp-lang, unpinned: requirements.txt `warp-lang>=1.7.0`) are
  * restated from their published definitions: mat22 @ mat22 and mat @ vec sum
@@ -100,6 +107,8 @@ static float or_logf(float x) {
 #define R_FLOOR floor
 #define R_ROUND round
 #define R_FABS fabs
+#define R_CEIL ceil
+#define R_POW pow
 #else
 #define R_SQRT sqrtf
 #if defined(USE_LIBM_LOG)
@@ -110,6 +119,8 @@ static float or_logf(float x) {
 #define R_FLOOR floorf
 #define R_ROUND roundf
 #define R_FABS fabsf
+#define R_CEIL ceilf
+#define R_POW powf
 #endif
 
 /* Bit constants: flatworld/definitions.py:96-104 */
@@ -159,6 +170,7 @@ typedef struct {
   /* CSR (node -> element corners, ascending element) for the threaded path */
   int32_t *csr_off, *csr_slot;
   REAL* corner; /* 6 per element */
+  struct or_flex* flex; /* FEM-FEM contact, NULL when the loop has none */
 } or_world;
 
 static REAL* dupf(const float* src, size_t n) {
@@ -431,9 +443,12 @@ static int pair_active(const or_world* w, const or_pair* c, long counter) {
   return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
 }
 
-static void contacts(or_world* w, REAL dt, long counter) {
+/* planes: the pairs of kind PAIR_PLANE (launched before FEM-FEM contact);
+ * otherwise the height-field and voxel pairs (launched after it). */
+static void contacts(or_world* w, REAL dt, long counter, int planes) {
   for (int pi = 0; pi < w->n_pairs; ++pi) {
     const or_pair* c = &w->pairs[pi];
+    if ((c->kind == PAIR_PLANE) != (planes != 0)) continue;
     if (!pair_active(w, c, counter)) continue;
     int off = w->bn_off[c->body], cnt = w->bn_cnt[c->body];
     for (int k = 0; k < cnt; ++k) {
@@ -617,6 +632,352 @@ static void par_for(or_world* w, int n, void (*fn)(or_world*, int, int, REAL, RE
   for (int t = 1; t < T; ++t) pthread_join(th[t], NULL);
 }
 
+/* ------------------------------------------------------- FEM-FEM contact
+ *
+ * One reference ExplicitLoop with ContactFlexFlex pairs.  Work items, in the
+ * reference's order (mixedcontact.py:1876-1924): per pair (contact-creation
+ * order) the boundary nodes of domain2 against domain1's boundary edges, then
+ * those of domain1 against domain2's.  The spatial hash and the contact kernel
+ * are restated with the serial semantics of Warp's CPU device: atomic counters
+ * hand out indices in launch order, so every hash cell lists its elements in
+ * registration order, and each work item's candidate list is its own (the
+ * reference's GPU launch shares one 512-entry candidate array among all work
+ * items, spatialmanager.py:564, mixedcontact.py:2545, which is a race; the
+ * serial semantics are the race-free reading).  Contact forces go to fext in
+ * work-item order: node, then the edge's two nodes (atomic_add in launch
+ * order). */
+#define FLEX_MAX_QUERY 512       /* SpatialHashManager max_query_results */
+#define FLEX_MAX_CELLS 100000    /* SpatialHashManager max_cells */
+
+typedef struct or_flex {
+  int n_items, n_pairs, n_fem, n_dom, skip_bvh;
+  int32_t *item_node, *item_target, *item_be_off, *item_be_cnt, *item_pair, *item_cache;
+  REAL *item_pen, *item_fric;
+  int32_t *pair_b1, *pair_b2; /* domain1, domain2 (fem-local = body index) */
+  int n_be;
+  int32_t *be;      /* 2 per boundary edge: global node ids */
+  int32_t *be_off, *be_cnt; /* per fem domain */
+  int32_t *dom_obj, *dom_body; /* per scene domain: BVH object?, body (or -1) */
+  REAL* dom_box;    /* 4 per domain: static box of a ground domain */
+  /* hash */
+  int max_elements, max_pairs;
+  int n_reg, tc, cnx, cny;
+  REAL estimate, olx, oly, gsx, gsy;
+  REAL* ebox;                 /* 4 per registered element */
+  int32_t *edom, *eid;        /* domain id, element id per registered element */
+  int32_t *pair_cell, *pair_elem, *sorted, *cell_count, *cell_offset, *cell_start, *cell_end;
+  int32_t cand[FLEX_MAX_QUERY];
+} or_flex;
+
+static REAL rmin(REAL a, REAL b) { return a < b ? a : b; }
+static REAL rmax(REAL a, REAL b) { return a > b ? a : b; }
+
+/* pointToEdgeContact (contact_detection.py:15-61) */
+static void point_edge(REAL px, REAL py, REAL ax, REAL ay, REAL bx, REAL by, REAL* pen, REAL* nx,
+                       REAL* ny, int* inside, REAL* w0, REAL* w1) {
+  REAL ex = bx - ax, ey = by - ay;
+  REAL len = R_SQRT(ex * ex + ey * ey);
+  *pen = (REAL)1e9;
+  *nx = 0;
+  *ny = 0;
+  *inside = 0;
+  *w0 = 0;
+  *w1 = 0;
+  if (len > (REAL)1e-9) {
+    REAL dx = ex / len, dy = ey / len;
+    *nx = dy;
+    *ny = -dx;
+    REAL tx = px - ax, ty = py - ay;
+    REAL t = tx * dx + ty * dy;
+    t = t / len;
+    if ((REAL)0.0 <= t && t <= (REAL)1.0) {
+      *inside = 1;
+      *pen = tx * *nx + ty * *ny;
+      *w0 = (REAL)1.0 - t;
+      *w1 = t;
+    }
+  }
+}
+
+/* detectPointToMeshBoundary (contact_detection.py:63-92): the penetration is
+ * kept only when |pen| < limit and the point projects inside the edge;
+ * the weights are pointToEdgeContact's either way. */
+static REAL detect_edge(const or_world* w, REAL px, REAL py, int e, REAL limit, REAL* nx, REAL* ny,
+                        REAL* w0, REAL* w1) {
+  const or_flex* f = w->flex;
+  int a = f->be[2 * e], b = f->be[2 * e + 1];
+  REAL pen, mx, my;
+  int inside;
+  point_edge(px, py, w->x[2 * a], w->x[2 * a + 1], w->x[2 * b], w->x[2 * b + 1], &pen, &mx, &my, &inside, w0, w1);
+  *nx = 0;
+  *ny = 0;
+  if (R_FABS(pen) < limit && inside) {
+    *nx = mx;
+    *ny = my;
+    return pen;
+  }
+  return (REAL)1e9;
+}
+
+static int cell_coord(REAL d, REAL gs, int n) {
+  int c = (int)R_FLOOR(d / gs);
+  c = c > 0 ? c : 0;
+  c = c < n - 1 ? c : n - 1;
+  return c;
+}
+
+/* FemSpringManager.populate_fem_spatial_hash(0.0) (femspringmanager.py:1041-1063,
+ * _populate_fem_spatial_hash_kernel) + SpatialHashManager.reset/build
+ * (spatialmanager.py:200-420, 613-712), serial. */
+void or_flex_rebuild(or_world* w) {
+  or_flex* f = w->flex;
+  if (!f) return;
+  f->n_reg = 0;
+  f->estimate = (REAL)1e30;
+  f->tc = 0;
+  REAL glx = (REAL)1e9, gly = (REAL)1e9, gux = (REAL)-1e9, guy = (REAL)-1e9;
+  for (int d = 0; d < f->n_fem; ++d) {
+    const REAL* bb = w->aabb + 4 * d;
+    glx = rmin(glx, bb[0]);
+    gly = rmin(gly, bb[1]);
+    gux = rmax(gux, bb[2]);
+    guy = rmax(guy, bb[3]);
+  }
+  REAL extent = rmax(gux - glx, guy - gly);
+  REAL expand = extent * (REAL)0.01 + (REAL)0.0;
+  glx = glx - expand;
+  gly = gly - expand;
+  gux = gux + expand;
+  guy = guy + expand;
+  for (int d = 0; d < f->n_fem; ++d)
+    for (int k = 0; k < f->be_cnt[d]; ++k) {
+      int e = f->be_off[d] + k;
+      REAL lx = (REAL)1e30, ly = (REAL)1e30, ux = (REAL)-1e30, uy = (REAL)-1e30;
+      for (int c = 0; c < 2; ++c) {
+        int nid = f->be[2 * e + c];
+        lx = rmin(lx, w->x[2 * nid]);
+        ly = rmin(ly, w->x[2 * nid + 1]);
+        ux = rmax(ux, w->x[2 * nid]);
+        uy = rmax(uy, w->x[2 * nid + 1]);
+      }
+      int idx = f->n_reg++;
+      if (idx < f->max_elements) {
+        f->edom[idx] = d;
+        f->eid[idx] = e;
+        REAL blx = lx - (REAL)0.0, bly = ly - (REAL)0.0, bux = ux + (REAL)0.0, buy = uy + (REAL)0.0;
+        f->ebox[4 * idx] = blx;
+        f->ebox[4 * idx + 1] = bly;
+        f->ebox[4 * idx + 2] = bux;
+        f->ebox[4 * idx + 3] = buy;
+        REAL ddx = bux - blx, ddy = buy - bly;
+        REAL diag = R_SQRT(ddx * ddx + ddy * ddy);
+        f->estimate = rmin(f->estimate, diag);
+      }
+    }
+  f->olx = glx;
+  f->oly = gly;
+  /* _build_grid_kernel */
+  REAL cell = f->estimate * (REAL)1.5;
+  REAL exx = gux - glx, exy = guy - gly;
+  REAL mpd = R_POW((REAL)FLEX_MAX_CELLS, (REAL)0.5);
+  mpd = rmax(mpd, (REAL)1.0);
+  cell = rmax(cell, exx / mpd);
+  cell = rmax(cell, exy / mpd);
+  REAL cs = cell + (REAL)1e-6;
+  int nx = (int)rmax(R_CEIL(exx / cs), (REAL)1.0);
+  int ny = (int)rmax(R_CEIL(exy / cs), (REAL)1.0);
+  f->cnx = nx;
+  f->cny = ny;
+  f->gsx = exx / (REAL)nx;
+  f->gsy = exy / (REAL)ny;
+  int total = nx * ny;
+  f->tc = total < FLEX_MAX_CELLS ? total : FLEX_MAX_CELLS;
+  int ne = f->n_reg;
+  if (ne == 0) return;
+  if (ne > f->max_elements) ne = f->max_elements;
+  /* _expand_pairs_kernel, serial */
+  int npairs = 0;
+  for (int i = 0; i < ne; ++i) {
+    const REAL* eb = f->ebox + 4 * i;
+    int lx = cell_coord(eb[0] - glx, f->gsx, nx), ly = cell_coord(eb[1] - gly, f->gsy, ny);
+    int ux = cell_coord(eb[2] - glx, f->gsx, nx), uy = cell_coord(eb[3] - gly, f->gsy, ny);
+    for (int ix = lx; ix <= ux; ++ix)
+      for (int iy = ly; iy <= uy; ++iy) {
+        int cid = ix + iy * nx;
+        if (cid < f->tc) {
+          int p = npairs++;
+          if (p < f->max_pairs) {
+            f->pair_cell[p] = cid;
+            f->pair_elem[p] = i;
+          }
+        }
+      }
+  }
+  int np_ = npairs < f->max_pairs ? npairs : f->max_pairs;
+  for (int c = 0; c < f->tc; ++c) f->cell_count[c] = 0;
+  for (int p = 0; p < np_; ++p) {
+    int cid = f->pair_cell[p];
+    if (0 <= cid && cid < f->tc) f->cell_count[cid] += 1;
+  }
+  if (f->tc > 0) {
+    f->cell_offset[0] = 0;
+    for (int c = 1; c < f->tc; ++c) f->cell_offset[c] = f->cell_offset[c - 1] + f->cell_count[c - 1];
+  }
+  for (int c = 0; c < f->tc; ++c) f->cell_count[c] = f->cell_offset[c];
+  for (int p = 0; p < np_; ++p) {
+    int cid = f->pair_cell[p];
+    if (0 <= cid && cid < f->tc) {
+      int dest = f->cell_count[cid]++;
+      if (dest < f->max_pairs) f->sorted[dest] = f->pair_elem[p];
+    }
+  }
+  for (int c = 0; c < f->tc; ++c) {
+    f->cell_start[c] = f->cell_offset[c];
+    f->cell_end[c] = f->cell_count[c];
+  }
+}
+
+/* query_point_with_buffer (spatialmanager.py:126-197) with this item's own
+ * candidate list. */
+static int flex_query(or_flex* f, REAL px, REAL py, REAL buf, int domain) {
+  int num = 0;
+  if (f->tc <= 0) return 0;
+  REAL qlx = px - buf, qly = py - buf, qux = px + buf, quy = py + buf;
+  int lx = cell_coord(qlx - f->olx, f->gsx, f->cnx), ly = cell_coord(qly - f->oly, f->gsy, f->cny);
+  int ux = cell_coord(qux - f->olx, f->gsx, f->cnx), uy = cell_coord(quy - f->oly, f->gsy, f->cny);
+  for (int ix = lx; ix <= ux; ++ix)
+    for (int iy = ly; iy <= uy; ++iy) {
+      int cid = ix + iy * f->cnx;
+      if (0 <= cid && cid < f->tc)
+        for (int p = f->cell_start[cid]; p < f->cell_end[cid]; ++p) {
+          int ei = f->sorted[p];
+          if (ei >= 0 && f->edom[ei] == domain) {
+            int id = f->eid[ei], dup = 0;
+            for (int k = 0; k < num; ++k)
+              if (f->cand[k] == id) dup = 1;
+            if (!dup && num < FLEX_MAX_QUERY) f->cand[num++] = id;
+          }
+        }
+    }
+  return num;
+}
+
+static int boxes_overlap(const REAL* a, const REAL* b, long counter) {
+  REAL alo[2] = {a[0], a[1]}, ahi[2] = {a[2], a[3]};
+  REAL blo[2] = {b[0], b[1]}, bhi[2] = {b[2], b[3]};
+  if (counter % 100 == 0) {
+    for (int k = 0; k < 2; ++k) {
+      REAL ba = (REAL)0.1 * (ahi[k] - alo[k]);
+      REAL bbuf = (REAL)0.1 * (bhi[k] - blo[k]);
+      alo[k] = alo[k] - ba;
+      ahi[k] = ahi[k] + ba;
+      blo[k] = blo[k] - bbuf;
+      bhi[k] = bhi[k] + bbuf;
+    }
+  }
+  return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
+}
+
+static const REAL* dom_box(const or_world* w, int g) {
+  const or_flex* f = w->flex;
+  return f->dom_body[g] >= 0 ? w->aabb + 4 * f->dom_body[g] : f->dom_box + 4 * g;
+}
+
+/* _batched_flexflex_contact_kernel_sh (mixedcontact.py:886-1018), serial.
+ * Pair activation (mixedcontact.py:1662-1665, 2282-2291): every pair when the
+ * loop skips the BVH (explicitloop.py:367-373), else the BVH overlap of the two
+ * domain boxes.  Domain mask (explicitloop.py:501-511, mixedcontact.py:925): a
+ * work item runs only if the domain whose GLOBAL index equals the item's target
+ * FEM-local index appears in some BVH pair this step -- the reference indexes
+ * the global stamp array with the FEM-local id; restated as written. */
+static void flex_contacts(or_world* w, long counter) {
+  or_flex* f = w->flex;
+  if (!f || f->n_items == 0) return;
+  int* active = (int*)malloc(sizeof(int) * (size_t)(f->n_pairs + 1));
+  int* stamped = (int*)malloc(sizeof(int) * (size_t)(f->n_fem + 1));
+  for (int p = 0; p < f->n_pairs; ++p)
+    active[p] = f->skip_bvh ? 1 : boxes_overlap(w->aabb + 4 * f->pair_b1[p], w->aabb + 4 * f->pair_b2[p], counter);
+  for (int g = 0; g < f->n_fem; ++g) {
+    stamped[g] = 0;
+    if (g < f->n_dom && f->dom_obj[g])
+      for (int h = 0; h < f->n_dom; ++h)
+        if (h != g && f->dom_obj[h] && boxes_overlap(dom_box(w, g), dom_box(w, h), counter)) stamped[g] = 1;
+  }
+  REAL qbuf = rmax(rmax((REAL)1e-4, rmax(f->gsx, f->gsy)), (REAL)0.016);
+  for (int it = 0; it < f->n_items; ++it) {
+    if (!active[f->item_pair[it]]) continue;
+    int target = f->item_target[it];
+    if (!f->skip_bvh && !stamped[target]) continue;
+    int nid = f->item_node[it];
+    int be_off = f->item_be_off[it], be_cnt = f->item_be_cnt[it];
+    REAL px = w->x[2 * nid], py = w->x[2 * nid + 1];
+    REAL vx = w->v[2 * nid], vy = w->v[2 * nid + 1];
+    REAL pen_k = f->item_pen[it], fric = f->item_fric[it];
+    REAL best = (REAL)1e9, bnx = 0, bny = 0, bw0 = 0, bw1 = 0;
+    int bn0 = 0, bn1 = 0, found = 0;
+    int cached = f->item_cache[it];
+    if (cached >= be_off && cached < be_off + be_cnt) {
+      int a = f->be[2 * cached], b = f->be[2 * cached + 1];
+      REAL lx = (REAL)1e30, ly = (REAL)1e30, ux = (REAL)-1e30, uy = (REAL)-1e30;
+      lx = rmin(lx, w->x[2 * a]); ly = rmin(ly, w->x[2 * a + 1]);
+      ux = rmax(ux, w->x[2 * a]); uy = rmax(uy, w->x[2 * a + 1]);
+      lx = rmin(lx, w->x[2 * b]); ly = rmin(ly, w->x[2 * b + 1]);
+      ux = rmax(ux, w->x[2 * b]); uy = rmax(uy, w->x[2 * b + 1]);
+      REAL dx = ux - lx, dy = uy - ly;
+      REAL margin = rmax((REAL)1e-4, (REAL)1e-2 * R_SQRT(dx * dx + dy * dy));
+      lx = lx - margin; ly = ly - margin; ux = ux + margin; uy = uy + margin;
+      int outside = rmin(px - lx, py - ly) < (REAL)0.0 || rmin(ux - px, uy - py) < (REAL)0.0;
+      if (!outside) {
+        REAL nx, ny, w0, w1;
+        REAL pen = detect_edge(w, px, py, cached, margin, &nx, &ny, &w0, &w1);
+        if (pen < (REAL)1e-4 && R_FABS(pen) < margin) {
+          best = pen; bnx = nx; bny = ny; bw0 = w0; bw1 = w1; bn0 = a; bn1 = b; found = 1;
+        }
+      }
+    }
+    if (!found) {
+      int n = flex_query(f, px, py, qbuf, target);
+      for (int j = 0; j < n; ++j) {
+        int e = f->cand[j];
+        REAL nx, ny, w0, w1;
+        REAL pen = detect_edge(w, px, py, e, qbuf, &nx, &ny, &w0, &w1);
+        if (pen < best && pen < (REAL)1e-4 && R_FABS(pen) < qbuf) {
+          best = pen; bnx = nx; bny = ny; bw0 = w0; bw1 = w1;
+          bn0 = f->be[2 * e]; bn1 = f->be[2 * e + 1]; found = 1;
+          f->item_cache[it] = e;
+        }
+      }
+    }
+    if (!found) f->item_cache[it] = -1;
+    if (found && best < (REAL)0.0) {
+      REAL fx = -bnx * pen_k * best, fy = -bny * pen_k * best;
+      REAL tx = fx, ty = fy;
+      if (fric > (REAL)1e-9) {
+        REAL sx = w->v[2 * bn0] * bw0 + w->v[2 * bn1] * bw1;
+        REAL sy = w->v[2 * bn0 + 1] * bw0 + w->v[2 * bn1 + 1] * bw1;
+        REAL rx = vx - sx, ry = vy - sy;
+        REAL dn = rx * bnx + ry * bny;
+        REAL gx = rx - dn * bnx, gy = ry - dn * bny;
+        REAL tl = R_SQRT(gx * gx + gy * gy);
+        if (tl > (REAL)1e-9) {
+          REAL dx = -gx / tl, dy = -gy / tl;
+          REAL nl = R_SQRT(fx * fx + fy * fy);
+          tx = tx + dx * fric * nl;
+          ty = ty + dy * fric * nl;
+        }
+      }
+      w->fext[2 * nid] += tx;
+      w->fext[2 * nid + 1] += ty;
+      w->fext[2 * bn0] += -(tx * bw0);
+      w->fext[2 * bn0 + 1] += -(ty * bw0);
+      w->fext[2 * bn1] += -(tx * bw1);
+      w->fext[2 * bn1 + 1] += -(ty * bw1);
+    }
+  }
+  free(active);
+  free(stamped);
+}
+
 /* ---------------------------------------------------------------- C API */
 
 or_world* or_create(int n_nodes, const float* x, const float* v, const int32_t* bc, const float* bcv,
@@ -709,6 +1070,96 @@ int or_add_voxel(or_world* w, int body, float penalty, const float* glb, const f
 
 void or_set_threads(or_world* w, int n) { w->n_threads = n < 1 ? 1 : n; }
 
+/* FEM-FEM contact set-up of one loop.  be: 2 global node ids per boundary
+ * edge, the edges of fem domain d at be[be_off[d] ..], in mesh order
+ * (mesh.py:53-71); dom_obj / dom_body / dom_box: per domain of the loop (in
+ * loop order) whether it is a BVH object (considerContact), its body (fem
+ * index, or -1 for a ground) and a ground's static box; skip_bvh: the loop has
+ * no plane, height-field, voxel or unbatched ground contact. */
+int or_set_flex(or_world* w, int n_be, const int32_t* be, const int32_t* be_off, const int32_t* be_cnt,
+                int n_dom, const int32_t* dom_obj, const int32_t* dom_body, const float* dom_box, int skip_bvh) {
+  or_flex* f = (or_flex*)calloc(1, sizeof(or_flex));
+  f->n_fem = w->n_bodies;
+  f->n_dom = n_dom;
+  f->skip_bvh = skip_bvh;
+  f->n_be = n_be;
+  f->be = dupi(be, 2 * (size_t)n_be);
+  f->be_off = dupi(be_off, w->n_bodies);
+  f->be_cnt = dupi(be_cnt, w->n_bodies);
+  f->dom_obj = dupi(dom_obj, n_dom);
+  f->dom_body = dupi(dom_body, n_dom);
+  f->dom_box = dupf(dom_box, 4 * (size_t)n_dom);
+  /* femspringmanager.py:545-548, spatialmanager.py:520-525 */
+  int max_nodes = w->n_nodes + 1024 > 2048 ? w->n_nodes + 1024 : 2048;
+  f->max_elements = n_be + 1024 > max_nodes ? n_be + 1024 : max_nodes;
+  f->max_pairs = f->max_elements * 9;
+  f->ebox = (REAL*)calloc(4 * (size_t)f->max_elements, sizeof(REAL));
+  f->edom = (int32_t*)calloc((size_t)f->max_elements, sizeof(int32_t));
+  f->eid = (int32_t*)calloc((size_t)f->max_elements, sizeof(int32_t));
+  f->pair_cell = (int32_t*)calloc((size_t)f->max_pairs, sizeof(int32_t));
+  f->pair_elem = (int32_t*)calloc((size_t)f->max_pairs, sizeof(int32_t));
+  f->sorted = (int32_t*)calloc((size_t)f->max_pairs, sizeof(int32_t));
+  f->cell_count = (int32_t*)calloc(FLEX_MAX_CELLS, sizeof(int32_t));
+  f->cell_offset = (int32_t*)calloc(FLEX_MAX_CELLS, sizeof(int32_t));
+  f->cell_start = (int32_t*)calloc(FLEX_MAX_CELLS, sizeof(int32_t));
+  f->cell_end = (int32_t*)calloc(FLEX_MAX_CELLS, sizeof(int32_t));
+  w->flex = f;
+  return 0;
+}
+
+/* One ContactFlexFlex pair (mixedcontact.py:1876-1924): domain1 = b1, domain2 =
+ * b2 (fem indices); work items for b2's boundary nodes against b1's edges,
+ * then b1's nodes against b2's edges. */
+int or_add_flex_pair(or_world* w, int b1, int b2, float penalty, float friction) {
+  or_flex* f = w->flex;
+  if (!f) return -1;
+  int p = f->n_pairs++;
+  f->pair_b1 = (int32_t*)realloc(f->pair_b1, sizeof(int32_t) * (size_t)f->n_pairs);
+  f->pair_b2 = (int32_t*)realloc(f->pair_b2, sizeof(int32_t) * (size_t)f->n_pairs);
+  f->pair_b1[p] = b1;
+  f->pair_b2[p] = b2;
+  int add = w->bn_cnt[b1] + w->bn_cnt[b2];
+  int n0 = f->n_items, n = n0 + add;
+  f->item_node = (int32_t*)realloc(f->item_node, sizeof(int32_t) * (size_t)n);
+  f->item_target = (int32_t*)realloc(f->item_target, sizeof(int32_t) * (size_t)n);
+  f->item_be_off = (int32_t*)realloc(f->item_be_off, sizeof(int32_t) * (size_t)n);
+  f->item_be_cnt = (int32_t*)realloc(f->item_be_cnt, sizeof(int32_t) * (size_t)n);
+  f->item_pair = (int32_t*)realloc(f->item_pair, sizeof(int32_t) * (size_t)n);
+  f->item_cache = (int32_t*)realloc(f->item_cache, sizeof(int32_t) * (size_t)n);
+  f->item_pen = (REAL*)realloc(f->item_pen, sizeof(REAL) * (size_t)n);
+  f->item_fric = (REAL*)realloc(f->item_fric, sizeof(REAL) * (size_t)n);
+  int k = n0;
+  for (int side = 0; side < 2; ++side) {
+    int src = side == 0 ? b2 : b1, dst = side == 0 ? b1 : b2;
+    for (int i = 0; i < w->bn_cnt[src]; ++i, ++k) {
+      f->item_node[k] = w->bnodes[w->bn_off[src] + i];
+      f->item_target[k] = dst;
+      f->item_be_off[k] = f->be_off[dst];
+      f->item_be_cnt[k] = f->be_cnt[dst];
+      f->item_pair[k] = p;
+      f->item_cache[k] = -1;
+      f->item_pen[k] = penalty;
+      f->item_fric[k] = friction;
+    }
+  }
+  f->n_items = n;
+  return p;
+}
+
+/* The hash grid: tc, nx, ny, origin x, origin y, cell x, cell y, estimate. */
+void or_get_flex_grid(const or_world* w, double* out) {
+  const or_flex* f = w->flex;
+  if (!f) return;
+  out[0] = f->tc; out[1] = f->cnx; out[2] = f->cny; out[3] = f->olx; out[4] = f->oly;
+  out[5] = f->gsx; out[6] = f->gsy; out[7] = f->estimate;
+}
+
+/* The per-item element cache (for tests). */
+void or_get_flex_cache(const or_world* w, int32_t* out) {
+  if (w->flex)
+    for (int i = 0; i < w->flex->n_items; ++i) out[i] = w->flex->item_cache[i];
+}
+
 /* One FemSpringManager.femStep plus, unless init_step, the contact launches of
  * ExplicitLoop.advance that precede it.  init_step reproduces the zero-dt step
  * setGlobalAABB runs at construction (femspringmanager.py:872-879). */
@@ -718,7 +1169,11 @@ void or_step(or_world* w, float dt_f, float damping_f, long counter, int init_st
   g_step_dt = dt;
   g_step_damping = damping;
   for (int i = 0; i < 2 * N; ++i) w->fext[i] = 0;
-  if (!init_step) contacts(w, dt, counter);
+  if (!init_step) {
+    contacts(w, dt, counter, 1);
+    flex_contacts(w, counter);
+    contacts(w, dt, counter, 0);
+  }
   if (w->n_threads <= 1) {
     REAL f[6];
     for (int e = 0; e < E; ++e) {
@@ -816,5 +1271,15 @@ void or_destroy(or_world* w) {
   }
   free(w->pairs);
   free(w->csr_off); free(w->csr_slot); free(w->corner);
+  if (w->flex) {
+    or_flex* f = w->flex;
+    free(f->item_node); free(f->item_target); free(f->item_be_off); free(f->item_be_cnt);
+    free(f->item_pair); free(f->item_cache); free(f->item_pen); free(f->item_fric);
+    free(f->pair_b1); free(f->pair_b2); free(f->be); free(f->be_off); free(f->be_cnt);
+    free(f->dom_obj); free(f->dom_body); free(f->dom_box); free(f->ebox); free(f->edom); free(f->eid);
+    free(f->pair_cell); free(f->pair_elem); free(f->sorted); free(f->cell_count); free(f->cell_offset);
+    free(f->cell_start); free(f->cell_end);
+    free(f);
+  }
   free(w);
 }

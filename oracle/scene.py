@@ -16,6 +16,11 @@ recomputed here with the reference's own loops:
   flatworld/grounddomain.py:54-70, heightfielddomain.py:26-27,190-194,
   voxeldomain.py:194-195                   broad-phase boxes
   flatworld/explicitloop.py:558-589        advanceWithTime substep loop
+  flatworld/femcontact.py:199-206          ContactFlexFlex penalty, stable time
+  flatworld/mixedcontact.py:1869-1935      FEM-FEM work items
+  flatworld/explicitloop.py:203-227, 362-373, 383-385  BVH objects, skip_bvh,
+                                           initial FEM spatial hash
+  flatworld/femspringmanager.py:523-524, 1035-1039  hash refresh every 1/500 s
 Domain objects are read through the reference's attribute names only
 (mesh.coords, mesh.connectivity, prop.mat, bcs, initials, point, normal,
 height, lb, ub, reverse, occ, nx, ny, dx, dz, considerContact, type, ...).
@@ -68,6 +73,11 @@ def _lib(precision: str):
         L.or_set_state.argtypes = [C.c_void_p, _f32p, _f32p]
         L.or_point_stress.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, _f32p, _f32p, C.c_float,
                                       _f64p, _f64p, _f64p]
+        L.or_set_flex.argtypes = [C.c_void_p, C.c_int, _i32p, _i32p, _i32p, C.c_int, _i32p, _i32p, _f32p, C.c_int]
+        L.or_add_flex_pair.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.or_flex_rebuild.argtypes = [C.c_void_p]
+        L.or_get_flex_cache.argtypes = [C.c_void_p, _i32p]
+        L.or_get_flex_grid.argtypes = [C.c_void_p, _f64p]
         L.or_destroy.argtypes = [C.c_void_p]
         L.or_log32.argtypes = [C.c_float]
         L.or_log32.restype = C.c_float
@@ -86,6 +96,20 @@ def _ip(a):
 
 
 # ---------------------------------------------------------------- host restatement
+
+def boundary_edges_literal(conns):
+    """mesh.py:53-71, loop for loop: edges seen once, in first-seen order and
+    orientation."""
+    edge_count = defaultdict(int)
+    for cell in np.asarray(conns).tolist():
+        for i in range(3):
+            v1, v2 = cell[i], cell[(i + 1) % 3]
+            if (v2, v1) in edge_count:
+                edge_count[(v2, v1)] += 1
+            else:
+                edge_count[(v1, v2)] += 1
+    return np.array([e for e, c in edge_count.items() if c == 1], dtype=np.int64).reshape(-1, 2)
+
 
 def boundary_nodes_literal(conns):
     """mesh.py:53-71 and 40-47, loop for loop."""
@@ -162,18 +186,16 @@ class OracleLoop:
                         continue
                     if ct in (RIGIDRIGID, RIGIDANLAYTICAL, ANALYTICALANALYTICAL):
                         continue
+                    if ct == FLEXFLEX:  # ContactFlexFlex(dom_i, dom_j): domain1 = i, domain2 = j
+                        pen = min(self._seg_penalty(di), self._seg_penalty(dj)) * 1.0
+                        st = min(self._contact_stable(pen, di, fem), self._contact_stable(pen, dj, fem))
+                        contacts.append((ct, di, dj, pen, st))
+                        continue
                     if ct not in (FLEXANLAYTICAL, FEXHEIGHTFIELD, FLEXVOXELMAP):
-                        if ct == FLEXFLEX:
-                            raise NotImplementedError("FEM-FEM contact is not restated")
                         continue
                     femd, gnd = (di, dj) if di.type == FEM else (dj, di)
-                    mat = femd.prop.mat
-                    nu = min(mat.nu, 0.4999)
-                    K = mat.E / (3.0 * (1.0 - 2.0 * nu))
-                    pen = 2.0 * 1.0 * K * 1.0
-                    Lc = self.char_len[fem.index(femd)]
-                    m_node = mat.rho * (Lc * Lc * 0.5) / 3.0
-                    contacts.append((ct, femd, gnd, pen, 0.9 * (m_node / pen) ** 0.5))
+                    pen = self._seg_penalty(femd) * 1.0
+                    contacts.append((ct, femd, gnd, pen, self._contact_stable(pen, femd, fem)))
         for c in contacts:
             stable = min(stable, c[4])
         self.stableTime = stable
@@ -248,9 +270,13 @@ class OracleLoop:
         anal = [c for c in contacts if c[0] == FLEXANLAYTICAL]
         hf = [c for c in contacts if c[0] == FEXHEIGHTFIELD]
         vox = [c for c in contacts if c[0] == FLEXVOXELMAP]
+        flex = [c for c in contacts if c[0] == FLEXFLEX]
+        unbatched = 0
         if len({id(c[2]) for c in hf}) > 1:
+            unbatched += len(hf)
             hf = []
         if len({id(c[2]) for c in vox}) > 1:
+            unbatched += len(vox)
             vox = []
         for ct, femd, g, pen, _ in anal + hf + vox:
             body = fem.index(femd)
@@ -269,9 +295,53 @@ class OracleLoop:
                 occ = _ip(np.asarray(g.occ, np.int32))
                 L.or_add_voxel(self._w, body, pen32, lo[1], hi[1], int(g.nx), int(g.ny), occ[1], float(g.lb[0]),
                                float(g.lb[1]), float(np.float32(g.dx)), float(np.float32(g.dz)))
+        self.flex = flex
+        if flex:
+            # boundary edges per fem domain, global node ids, mesh order
+            edges, be_off, be_cnt = [], [], []
+            for d, (n0, _) in zip(fem, self.node_ranges):
+                e = boundary_edges_literal(d.mesh.connectivity) + n0
+                be_off.append(sum(len(x) for x in edges))
+                be_cnt.append(len(e))
+                edges.append(e)
+            dom_obj = [1 if d.considerContact else 0 for d in domains]
+            dom_body = [fem.index(d) if d.type == FEM else -1 for d in domains]
+            dom_box = np.zeros((len(domains), 4), np.float32)
+            for i, d in enumerate(domains):
+                if d.type != FEM and d.considerContact:
+                    lo, hi = self._ground_box(d)
+                    dom_box[i, :2] = lo[0]
+                    dom_box[i, 2:] = hi[0]
+            skip_bvh = 1 if (len(anal) + len(hf) + len(vox) + unbatched) == 0 else 0
+            ea, eo, ec = _ip(np.concatenate(edges).reshape(-1)), _ip(be_off), _ip(be_cnt)
+            do, db, dbx = _ip(dom_obj), _ip(dom_body), _fp(dom_box)
+            self._keep += [ea, eo, ec, do, db, dbx]
+            L.or_set_flex(self._w, len(ea[0]) // 2, ea[1], eo[1], ec[1], len(domains), do[1], db[1], dbx[1], skip_bvh)
+            for _, d1, d2, pen, _ in flex:
+                fric = max(d1.friction, d2.friction)
+                L.or_add_flex_pair(self._w, fem.index(d1), fem.index(d2), float(np.float32(pen)),
+                                   float(np.float32(fric)))
+        self.sh_elapsed = 0.0
         self.counter = 0
         # setGlobalAABB -> substep(0.0, 0.0) (femspringmanager.py:872-879)
         L.or_step(self._w, 0.0, 0.0, 0, 1)
+        if flex:  # explicitloop.py:383-385: initial FEM spatial hash
+            L.or_flex_rebuild(self._w)
+
+    @staticmethod
+    def _seg_penalty(dom):
+        """femcontact.py:100-119, 2D: 2 K."""
+        mat = dom.prop.mat
+        nu = min(mat.nu, 0.4999)
+        K = mat.E / (3.0 * (1.0 - 2.0 * nu))
+        return 2.0 * 1.0 * K
+
+    def _contact_stable(self, pen, dom, fem):
+        """femcontact.py:121-141"""
+        mat = dom.prop.mat
+        Lc = self.char_len[fem.index(dom)]
+        m_node = mat.rho * (Lc * Lc * 0.5) / 3.0
+        return 0.9 * (m_node / pen) ** 0.5
 
     @staticmethod
     def _ground_box(g):
@@ -304,8 +374,26 @@ class OracleLoop:
     def advance(self, n: int = 1, dt: float | None = None):
         d = self.dt if dt is None else dt
         for _ in range(n):
+            if self.flex:  # maybe_rebuild_fem_spatial_hash(self.dt), femspringmanager.py:1035-1039
+                self.sh_elapsed += d
+                if self.sh_elapsed >= 1.0 / 500.0:
+                    self._L.or_flex_rebuild(self._w)
+                    self.sh_elapsed = 0.0
             self._L.or_step(self._w, float(np.float32(d)), float(np.float32(self.damping)), self.counter, 0)
             self.counter += 1
+
+    def flex_grid(self):
+        """The hash grid: tc, nx, ny, origin x, origin y, cell x, cell y, estimate."""
+        out = np.zeros(8)
+        self._L.or_get_flex_grid(self._w, out.ctypes.data_as(_f64p))
+        return out
+
+    def flex_cache(self):
+        """The work items' element caches (edge index, or -1)."""
+        n = sum(sum(len(boundary_nodes_literal(d.mesh.connectivity)) for d in (c[1], c[2])) for c in self.flex)
+        out = np.zeros(n, np.int32)
+        self._L.or_get_flex_cache(self._w, out.ctypes.data_as(_i32p))
+        return out
 
     def advance_with_time(self, frame_dt=1.0 / 60.0):
         remaining = float(frame_dt)

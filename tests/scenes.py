@@ -200,3 +200,52 @@ def gradient_block_scene(fw, n=64, side=0.4, bottom=0.5, young=None, v0=(0.0, -2
                        [fw.Gravity([0.0, -9.8])], initials=[fw.InitialVel("ALL", list(v0))])
     fem.elementYoung = lognormal_young(2 * n * n, seed=seed) if young is None else np.asarray(young, np.float32)
     return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), fem]
+
+
+# ---- FEM-FEM contact scenes
+
+def flex_circles(fw, contact=True):
+    """The reference's FEM-FEM scene (test2D/test_2Dfem_contact.py:14-26): two
+    16-segment circles of radius 0.1 at y = 0.5 and 0.8, pulled toward each
+    other by gravity +10 and -10, Elastic E = 2e4, nu = 0.2, rho = 40."""
+    msh = fw.FEMesher(2)
+    prop = fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0))
+    a = fw.FemDomain(msh.createCircle([0.5, 0.5], 0.1), prop, [fw.Gravity([0, 10.0])], considerContact=contact)
+    b = fw.FemDomain(msh.createCircle([0.5, 0.8], 0.1), prop, [fw.Gravity([0, -10.0])], considerContact=contact)
+    return [a, b]
+
+
+def flex_stack(fw):
+    """A circle resting on the ground plane and a NeoHookean circle with
+    friction 0.3 dropped onto it, slightly off centre (plane + FEM-FEM
+    contact, so the broad phase gates the FEM-FEM pair)."""
+    msh = fw.FEMesher(2)
+    g = fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0])
+    a = fw.FemDomain(msh.createCircle([0.5, 0.101], 0.1), fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)),
+                     [fw.Gravity([0, -10.0])])
+    b = fw.FemDomain(msh.createCircle([0.52, 0.35], 0.1), fw.SolidProp(fw.HyperElastic(E=2e4, nu=0.2, rho=40.0)),
+                     [fw.Gravity([0, -10.0])], friction=0.3)
+    return [g, a, b]
+
+
+def ccw_rectangle(fw, nx, ny, lx, ly, origin):
+    """structured_rectangle with counter-clockwise triangles, so boundary-edge
+    normals point outward as FEM-FEM contact expects."""
+    conn, coords = fw.structured_rectangle(nx, ny, lx, ly, origin=origin)
+    return fw.Mesh(2, np.ascontiguousarray(conn[:, [0, 2, 1]]), coords)
+
+
+def flex_blocks(fw):
+    """A 16 x 4 Elastic slab falling onto a rippled height field and an 8 x 8
+    NeoHookean block (friction 0.3, 0.3 m/s down) falling onto the slab;
+    height field + FEM-FEM contact.  Stable at a fixed dt of 0.3 x the loop's
+    adaptive dt (at the adaptive dt itself the two soft bodies' two-sided
+    penalty contact diverges, in the oracle as on the GPU)."""
+    xs = np.linspace(-0.2, 0.5, 64)
+    g = fw.HeightFieldDomain(2, (0.004 * np.sin(25 * xs)).astype(np.float32), [-0.2, -1.0], [0.5, 1.0])
+    a = fw.FemDomain(ccw_rectangle(fw, 16, 4, 0.2, 0.05, (0.0, 0.01)), fw.SolidProp(fw.Elastic(E=2e4, nu=0.3, rho=100.0)),
+                     [fw.Gravity([0.0, -9.8])])
+    b = fw.FemDomain(ccw_rectangle(fw, 8, 8, 0.08, 0.08, (0.05, 0.075)),
+                     fw.SolidProp(fw.HyperElastic(E=2e4, nu=0.3, rho=100.0)), [fw.Gravity([0.0, -9.8])],
+                     initials=[fw.InitialVel("ALL", [0.0, -0.3])], friction=0.3)
+    return [g, a, b]
