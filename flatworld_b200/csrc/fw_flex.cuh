@@ -35,6 +35,8 @@ constexpr int kFlexScanThreads = 1024;
 
 struct FlexGrid {
   int tc, cnx, cny, npairs;
+  int simple;  // every element sits in every cell of its box (no cell cap, no pair truncation)
+  int pad2[3];
   float olx, oly, gsx, gsy;
   int estimate;  // ordered-int minimum of the element box diagonals
   int rebuild;   // this substep rebuilds the hash
@@ -73,6 +75,10 @@ struct FlexDev {
   int32_t* cell_end;
   int32_t* cursor;
   int32_t* sorted;
+  int2* crange;  // (start, end) of cell (ix, iy) at ix * cny + iy: a column is contiguous
+  int2* ecell;   // per element: its lowest cell (ix, iy), clamped to the grid
+  int4* srec;    // per cell entry (cell order): element, its domain, its two nodes
+  int2* scell;   // per cell entry: the element's lowest cell
 };
 
 // wp.min / wp.max on floats: a < b ? a : b (first argument on ties)
@@ -109,8 +115,10 @@ __device__ __forceinline__ int flex_cell(float delta, float gs, int n) {
 
 // Per substep, before k_elements: scene mode, hash clock, pair activation
 // and the broad-phase domain stamps.  force != 0: the construction-time build
-// (explicitloop.py:383-385) -- rebuild, no contact.
+// (explicitloop.py:383-385) -- rebuild, no contact.  Dynamic shared memory:
+// (n_dom + n_fem) boxes -- every domain's, then every FEM body's.
 __global__ void k_flex_pre(Dev d, FlexDev f, int force) {
+  extern __shared__ float4 sbox[];
   const int s = f.scene;
   const bool step = !force && flex_stepping(d, s);
   if (threadIdx.x == 0) {
@@ -129,25 +137,31 @@ __global__ void k_flex_pre(Dev d, FlexDev f, int force) {
   if (!step) return;
   const int k = d.scene_counter[s];
   const int slot = k & 1;
+  float4* body_box = sbox + f.n_dom;
+  for (int g = threadIdx.x; g < f.n_dom; g += blockDim.x)
+    sbox[g] = f.dom_body[g] >= 0 ? ring_box(d, slot, f.dom_body[g]) : f.dom_box[g];
+  for (int b = threadIdx.x; b < f.n_fem; b += blockDim.x) body_box[b] = ring_box(d, slot, f.body0 + b);
+  __syncthreads();
   // _activate_or_fill_pairs: every pair when the loop has no BVH, else BVH overlap
   for (int p = threadIdx.x; p < f.n_pairs; p += blockDim.x) {
     const int2 pb = f.pair_body[p];
-    f.pair_active[p] = f.skip_bvh ? 1 : (flex_boxes_overlap(ring_box(d, slot, pb.x), ring_box(d, slot, pb.y), k) ? 1 : 0);
+    f.pair_active[p] = f.skip_bvh ? 1 : (flex_boxes_overlap(body_box[pb.x - f.body0], body_box[pb.y - f.body0], k) ? 1 : 0);
   }
   // _scan_bvh_pairs_stamp_kernel: domain g (global index) is stamped when it
   // is in some broad-phase pair; the contact kernel reads the stamp at the
-  // item's fem-local target index
-  for (int gi = threadIdx.x; gi < f.n_fem; gi += blockDim.x) {
-    int st = 0;
+  // item's fem-local target index.  One warp per g.
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int gi = warp; gi < f.n_fem; gi += nwarps) {
+    bool st = false;
     if (gi < f.n_dom && f.dom_obj[gi]) {
-      const float4 a = f.dom_body[gi] >= 0 ? ring_box(d, slot, f.dom_body[gi]) : f.dom_box[gi];
-      for (int h = 0; h < f.n_dom && !st; ++h) {
-        if (h == gi || !f.dom_obj[h]) continue;
-        const float4 b = f.dom_body[h] >= 0 ? ring_box(d, slot, f.dom_body[h]) : f.dom_box[h];
-        if (flex_boxes_overlap(a, b, k)) st = 1;
+      const float4 a = sbox[gi];
+      for (int h0 = 0; h0 < f.n_dom && !st; h0 += 32) {
+        const int h = h0 + lane;
+        const bool hit = h < f.n_dom && h != gi && f.dom_obj[h] && flex_boxes_overlap(a, sbox[h], k);
+        st = __any_sync(0xFFFFFFFFu, hit);
       }
     }
-    f.stamped[gi] = st;
+    if (lane == 0) f.stamped[gi] = st ? 1 : 0;
   }
 }
 
@@ -219,6 +233,7 @@ __global__ void k_flex_count(FlexDev f) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.n_be; e += stride) {
     int lx, ly, ux, uy, n = 0;
     flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+    f.ecell[e] = make_int2(lx, ly);
     for (int ix = lx; ix <= ux; ++ix)
       for (int iy = ly; iy <= uy; ++iy)
         if (ix + iy * g.cnx < g.tc) ++n;
@@ -258,7 +273,10 @@ __device__ int flex_block_scan(const int32_t* in, int32_t* out, int n) {
 __global__ void __launch_bounds__(kFlexScanThreads) k_flex_scan_elems(FlexDev f) {
   if (!f.g->rebuild) return;
   const int total = flex_block_scan(f.ecount, f.ebase, f.n_be);
-  if (threadIdx.x == 0) f.g->npairs = total;
+  if (threadIdx.x == 0) {
+    f.g->npairs = total;
+    f.g->simple = (f.g->tc == f.g->cnx * f.g->cny && total <= f.max_pairs) ? 1 : 0;
+  }
 }
 
 // Cell counts of the pairs kept (pair index < max_pairs).
@@ -322,6 +340,16 @@ __global__ void k_flex_sort(FlexDev f) {
       }
       f.sorted[j + 1] = v;
     }
+    if (f.g->simple) {  // then tc = cnx * cny <= kFlexMaxCells: the column index is in range
+      const int cnx = f.g->cnx, cny = f.g->cny;
+      f.crange[(c % cnx) * cny + c / cnx] = make_int2(lo, hi);
+      for (int i = lo; i < hi; ++i) {  // what the contact walk reads of each entry, in entry order
+        const int e = f.sorted[i];
+        const int2 n = f.be[e];
+        f.srec[i] = make_int4(e, f.be_dom[e], n.x, n.y);
+        f.scell[i] = f.ecell[e];
+      }
+    }
   }
 }
 
@@ -371,10 +399,31 @@ __device__ __forceinline__ void flex_push(const Dev& d, FlexGrid* g, int node, i
   }
 }
 
-// _batched_flexflex_contact_kernel_sh, one thread per work item.
-__global__ void __launch_bounds__(128) k_flex_contact(Dev d, FlexDev f) {
-  const int it = blockIdx.x * blockDim.x + threadIdx.x;
-  if (it >= f.n_items || !flex_stepping(d, f.scene)) return;
+// _batched_flexflex_contact_kernel_sh.  A work item's pair is active only
+// where two bodies meet, so few items run; to keep the SMs busy each item
+// gets kFlexLanes lanes.  The query walks cells ix-major then iy, each cell's
+// elements in order, strict < keeping the first minimum.  When every element
+// sits in every cell of its box (no cell cap, no pair truncation: g.simple),
+// an element is new at cell (ix, iy) exactly when that is the first cell of
+// its box inside the query window, so no candidate list is needed: the
+// window's cells are cut into kFlexLanes contiguous runs of the walk, each
+// lane keeps the first minimum of its run, and the group takes the smallest
+// penetration, ties to the lower lane (earlier in the walk) -- the serial
+// result.  Otherwise, or past the reference's 512 unique candidates, the walk
+// keeps the candidate list as written.
+constexpr int kFlexLanes = 8;
+constexpr int kFlexContactThreads = 128;
+
+struct FlexBest {
+  float pen, nx, ny, w0, w1;
+  int e, n0, n1;
+};
+
+__global__ void __launch_bounds__(kFlexContactThreads) k_flex_contact(Dev d, FlexDev f) {
+  const int it = (blockIdx.x * blockDim.x + threadIdx.x) / kFlexLanes;
+  const int sub = threadIdx.x % kFlexLanes;
+  const unsigned gmask = ((1u << kFlexLanes) - 1u) << ((threadIdx.x & 31) & ~(kFlexLanes - 1));
+  if (it >= f.n_items || !flex_stepping(d, f.scene)) return;  // uniform within the group
   if (!f.pair_active[f.item_pair[it]]) return;
   const int target = f.item_target[it];
   if (!f.skip_bvh && !f.stamped[target]) return;
@@ -408,33 +457,84 @@ __global__ void __launch_bounds__(128) k_flex_contact(Dev d, FlexDev f) {
     }
   }
   if (!found && g.tc > 0) {  // query_point_with_buffer, then every candidate in order
-    int cand[kFlexMaxQuery];
-    int num = 0;
     const int lx = flex_cell(p.x - qbuf - g.olx, g.gsx, g.cnx), ly = flex_cell(p.y - qbuf - g.oly, g.gsy, g.cny);
     const int ux = flex_cell(p.x + qbuf - g.olx, g.gsx, g.cnx), uy = flex_cell(p.y + qbuf - g.oly, g.gsy, g.cny);
-    for (int ix = lx; ix <= ux; ++ix)
-      for (int iy = ly; iy <= uy; ++iy) {
-        const int cid = ix + iy * g.cnx;
-        if (cid < 0 || cid >= g.tc) continue;
-        for (int q = f.cell_start[cid]; q < f.cell_end[cid]; ++q) {
-          const int e = f.sorted[q];
-          if (e < 0 || f.be_dom[e] != target) continue;
-          bool dup = false;
-          for (int k = 0; k < num; ++k) dup |= cand[k] == e;
-          if (!dup && num < kFlexMaxQuery) cand[num++] = e;
+    bool serial = !g.simple;
+    if (g.simple) {
+      const int h = uy - ly + 1, ncell = (ux - lx + 1) * h;
+      const int chunk = (ncell + kFlexLanes - 1) / kFlexLanes;
+      const int t1 = min(ncell, (sub + 1) * chunk);
+      FlexBest b{1e9f, 0.f, 0.f, 0.f, 0.f, -1, 0, 0};
+      int num = 0;
+      for (int t = min(ncell, sub * chunk); t < t1; ++t) {
+        const int ix = lx + t / h, iy = ly + t % h;
+        const int2 r = f.crange[ix * g.cny + iy];
+        for (int q = r.x; q < r.y; ++q) {
+          const int4 rec = f.srec[q];  // element, domain, nodes
+          if (rec.y != target) continue;
+          const int2 ec = f.scell[q];
+          if (ix != (lx > ec.x ? lx : ec.x) || iy != (ly > ec.y ? ly : ec.y)) continue;  // seen earlier
+          ++num;
+          float nx, ny, w0, w1;
+          const float pen = flex_detect(p, d.x[rec.z], d.x[rec.w], qbuf, nx, ny, w0, w1);
+          if (pen < b.pen && pen < 1e-4f && fabsf(pen) < qbuf) b = FlexBest{pen, nx, ny, w0, w1, rec.x, rec.z, rec.w};
         }
       }
-    for (int j = 0; j < num; ++j) {
-      const int e = cand[j];
-      const int2 n = f.be[e];
-      float nx, ny, w0, w1;
-      const float pen = flex_detect(p, d.x[n.x], d.x[n.y], qbuf, nx, ny, w0, w1);
-      if (pen < best && pen < 1e-4f && fabsf(pen) < qbuf) {
-        best = pen; bnx = nx; bny = ny; bw0 = w0; bw1 = w1; bn0 = n.x; bn1 = n.y; found = true;
-        cache_out = e;
+      for (int o = kFlexLanes / 2; o > 0; o >>= 1) num += __shfl_xor_sync(gmask, num, o);
+      if (num > kFlexMaxQuery) {
+        serial = true;  // the reference stops adding candidates at 512: walk as written
+      } else {
+        float wp = b.pen;
+        int wl = sub;
+        for (int o = kFlexLanes / 2; o > 0; o >>= 1) {  // min penetration, ties to the lower lane
+          const float op = __shfl_xor_sync(gmask, wp, o);
+          const int ol = __shfl_xor_sync(gmask, wl, o);
+          if (op < wp || (op == wp && ol < wl)) {
+            wp = op;
+            wl = ol;
+          }
+        }
+        const int src = (threadIdx.x & 31 & ~(kFlexLanes - 1)) + wl;
+        const int we = __shfl_sync(gmask, b.e, src);
+        const float pbest = __shfl_sync(gmask, b.pen, src), pnx = __shfl_sync(gmask, b.nx, src);
+        const float pny = __shfl_sync(gmask, b.ny, src), pw0 = __shfl_sync(gmask, b.w0, src);
+        const float pw1 = __shfl_sync(gmask, b.w1, src);
+        const int pn0 = __shfl_sync(gmask, b.n0, src), pn1 = __shfl_sync(gmask, b.n1, src);
+        if (we >= 0) {
+          best = pbest; bnx = pnx; bny = pny; bw0 = pw0; bw1 = pw1; bn0 = pn0; bn1 = pn1;
+          found = true;
+          cache_out = we;
+        }
+      }
+    }
+    if (serial) {  // every lane of the group walks the window (same result in each)
+      int cand[kFlexMaxQuery];
+      int num = 0;
+      for (int ix = lx; ix <= ux; ++ix)
+        for (int iy = ly; iy <= uy; ++iy) {
+          const int cid = ix + iy * g.cnx;
+          if (cid < 0 || cid >= g.tc) continue;
+          for (int q = f.cell_start[cid]; q < f.cell_end[cid]; ++q) {
+            const int e = f.sorted[q];
+            if (e < 0 || f.be_dom[e] != target) continue;
+            bool dup = false;
+            for (int k = 0; k < num; ++k) dup |= cand[k] == e;
+            if (!dup && num < kFlexMaxQuery) cand[num++] = e;
+          }
+        }
+      for (int j = 0; j < num; ++j) {
+        const int e = cand[j];
+        const int2 n = f.be[e];
+        float nx, ny, w0, w1;
+        const float pen = flex_detect(p, d.x[n.x], d.x[n.y], qbuf, nx, ny, w0, w1);
+        if (pen < best && pen < 1e-4f && fabsf(pen) < qbuf) {
+          best = pen; bnx = nx; bny = ny; bw0 = w0; bw1 = w1; bn0 = n.x; bn1 = n.y; found = true;
+          cache_out = e;
+        }
       }
     }
   }
+  if (sub != 0) return;
   if (!found) cache_out = -1;
   if (cache_out != cached) f.item_cache[it] = cache_out;
   if (found && best < 0.0f) {

@@ -813,6 +813,7 @@ struct fw_ctx {
   std::vector<float4> h_dom_box;
   bool has_flex = false;
   FlexDev fx{};
+  size_t flex_pre_smem = 0;  // k_flex_pre: (domains + FEM bodies) boxes
   double flex_clock = 0.0;  // host copy of the last fw_set_flex_clock value
 };
 
@@ -879,7 +880,7 @@ void flex_launch(fw_ctx* c, int force) {
   const FlexDev& f = c->fx;
   const int eb = (f.n_be + kBlock - 1) / kBlock;
   const int wide = 2 * c->sms;
-  k_flex_pre<<<1, 128, 0, c->stream>>>(c->d, f, force);
+  k_flex_pre<<<1, 512, c->flex_pre_smem, c->stream>>>(c->d, f, force);
   k_flex_boxes<<<eb, kBlock, 0, c->stream>>>(c->d, f);
   k_flex_grid<<<1, 32, 0, c->stream>>>(c->d, f);
   k_flex_count<<<wide, kBlock, 0, c->stream>>>(f);
@@ -890,7 +891,9 @@ void flex_launch(fw_ctx* c, int force) {
   k_flex_sort<<<wide, kBlock, 0, c->stream>>>(f);
   c->launches += 9;
   if (!force) {
-    k_flex_contact<<<(f.n_items + 127) / 128, 128, 0, c->stream>>>(c->d, f);
+    const int64_t threads = (int64_t)f.n_items * kFlexLanes;
+    k_flex_contact<<<(int)((threads + kFlexContactThreads - 1) / kFlexContactThreads), kFlexContactThreads, 0,
+                     c->stream>>>(c->d, f);
     c->launches += 1;
   }
 }
@@ -1792,6 +1795,8 @@ int build_flex(fw_ctx* c) {
           *bcnt = nullptr, *dobj = nullptr, *dbody = nullptr, *pact = nullptr, *stamp = nullptr, *ecount = nullptr,
           *ebase = nullptr, *ccount = nullptr, *cstart = nullptr, *cend = nullptr, *cursor = nullptr,
           *sorted = nullptr, *dslot = nullptr, *dcnt = nullptr, *ditem = nullptr;
+  int2 *crange = nullptr, *ecell = nullptr, *scell = nullptr;
+  int4* srec = nullptr;
   float *ipen = nullptr, *ifric = nullptr;
   int2 *pbody = nullptr, *dbe = nullptr;
   float4 *dbox = nullptr, *ebox = nullptr;
@@ -1815,6 +1820,8 @@ int build_flex(fw_ctx* c) {
       (rc = dalloc(c, &ebase, n_be)) || (rc = dalloc(c, &ccount, kFlexMaxCells)) ||
       (rc = dalloc(c, &cstart, kFlexMaxCells)) || (rc = dalloc(c, &cend, kFlexMaxCells)) ||
       (rc = dalloc(c, &cursor, kFlexMaxCells)) || (rc = dalloc(c, &sorted, f.max_pairs)) ||
+      (rc = dalloc(c, &crange, kFlexMaxCells)) || (rc = dalloc(c, &ecell, n_be)) ||
+      (rc = dalloc(c, &srec, f.max_pairs)) || (rc = dalloc(c, &scell, f.max_pairs)) ||
       (rc = upload(c, &dslot, slot)) || (rc = dalloc(c, &dcnt, std::max(1, n_slots))) ||
       (rc = dalloc(c, &ditem, std::max(1, n_slots) * kFlexListCap)) ||
       (rc = dalloc(c, &dforce, std::max(1, n_slots) * kFlexListCap)))
@@ -1828,7 +1835,15 @@ int build_flex(fw_ctx* c) {
   f.item_cache = icache; f.pair_body = pbody; f.be = dbe; f.be_dom = bdom; f.be_off = boff; f.be_cnt = bcnt;
   f.dom_obj = dobj; f.dom_body = dbody; f.dom_box = dbox; f.pair_active = pact; f.stamped = stamp; f.g = grid;
   f.ebox = ebox; f.ecount = ecount; f.ebase = ebase; f.cell_count = ccount; f.cell_start = cstart;
-  f.cell_end = cend; f.cursor = cursor; f.sorted = sorted;
+  f.cell_end = cend; f.cursor = cursor; f.sorted = sorted; f.crange = crange; f.ecell = ecell;
+  f.srec = srec; f.scell = scell;
+  c->flex_pre_smem = sizeof(float4) * (size_t)(std::max(n_dom, 1) + B);
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if ((long)c->flex_pre_smem > optin)
+    return fail(c, FW_ERR_ARG, "FEM-FEM contact: %d domains need %zu B of shared memory", n_dom, c->flex_pre_smem);
+  if (c->flex_pre_smem > 48 * 1024)
+    FW_CUDA(c, cudaFuncSetAttribute(k_flex_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->flex_pre_smem));
   c->fx = f;
   c->d.flex_slot = dslot;
   c->d.flex_cnt = dcnt;

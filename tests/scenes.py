@@ -249,3 +249,30 @@ def flex_blocks(fw):
                      fw.SolidProp(fw.HyperElastic(E=2e4, nu=0.3, rho=100.0)), [fw.Gravity([0.0, -9.8])],
                      initials=[fw.InitialVel("ALL", [0.0, -0.3])], friction=0.3)
     return [g, a, b]
+
+
+def ccw_disk(fw, cells, radius, centre):
+    """A disk meshed by mapping the counter-clockwise cells x cells square grid
+    onto the circle (elliptical grid mapping x sqrt(1 - y^2/2), y sqrt(1 - x^2/2)):
+    a round boundary of 4 cells edges without corners."""
+    conn, coords = fw.structured_rectangle(cells, cells, 2.0, 2.0, origin=(-1.0, -1.0))
+    u, v = coords[:, 0].astype(np.float64), coords[:, 1].astype(np.float64)
+    x = u * np.sqrt(np.maximum(0.0, 1.0 - 0.5 * v * v))
+    y = v * np.sqrt(np.maximum(0.0, 1.0 - 0.5 * u * u))
+    pts = np.stack([centre[0] + radius * x, centre[1] + radius * y], axis=1).astype(np.float32)
+    return fw.Mesh(2, np.ascontiguousarray(conn[:, [0, 2, 1]]), pts)
+
+
+def flex_pile(fw, cols=8, rows=8, cells=16, radius=0.025, gap=0.01, E=1e5, rho=1000.0):
+    """cols x rows disks (cells x cells mapped grid each) in a grid above the
+    ground plane y = 0, alternately Elastic and NeoHookean, friction 0.2,
+    every pair in FEM-FEM contact; the columns fall, land and stack."""
+    doms = [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0])]
+    pitch = 2 * radius + gap
+    for r in range(rows):
+        for c in range(cols):
+            k = r * cols + c
+            mat = (fw.Elastic if k % 2 == 0 else fw.HyperElastic)(E=E, nu=0.3, rho=rho)
+            mesh = ccw_disk(fw, cells, radius, (radius + c * pitch + 0.002 * (r % 2), radius + 0.002 + r * pitch))
+            doms.append(fw.FemDomain(mesh, fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])], friction=0.2))
+    return doms
