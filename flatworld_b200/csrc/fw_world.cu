@@ -365,6 +365,49 @@ __global__ void k_prepare_mass(Dev d, int n_lo, int n_hi) {
 
 // Lame constants of elements [e_lo, e_hi) from new Young's moduli (same
 // formula as k_prepare_elements).
+// Selective mass scaling, _mass_scaling_kernel (femspringmanager.py:139-196):
+// a triangle whose critical step 0.4 L_min / sqrt(E / rho) is below dt_target
+// gets the density that makes it dt_target, and its three nodes a third of
+// the added mass each.  The reference runs it on one thread in element order;
+// here k_mass_scale_elems finds each triangle's share and k_mass_scale_nodes
+// adds a node's shares in ascending element order (its CSR list), the same
+// additions in the same order.
+__global__ void k_mass_scale_elems(Dev d, const float* __restrict__ young, const float* __restrict__ rho,
+                                   float dt_target, float* __restrict__ dm, int32_t* __restrict__ hit) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.E) return;
+  const float2 a = d.x[d.conn[3 * e]], b = d.x[d.conn[3 * e + 1]], c = d.x[d.conn[3 * e + 2]];
+  const float e01x = b.x - a.x, e01y = b.y - a.y, e12x = c.x - b.x, e12y = c.y - b.y, e20x = a.x - c.x, e20y = a.y - c.y;
+  const float e01 = sqrtf(e01x * e01x + e01y * e01y), e12 = sqrtf(e12x * e12x + e12y * e12y);
+  const float e20 = sqrtf(e20x * e20x + e20y * e20y);
+  const float m12 = e12 < e20 ? e12 : e20;
+  const float L = e01 < m12 ? e01 : m12;
+  const float E = young[e], r = rho[e];
+  const float ce = sqrtf(E / r);
+  const float dt_elem = 0.4f * L / ce;
+  int h = 0;
+  float add = 0.0f;
+  if (dt_elem < dt_target && L > 1e-15f) {
+    const float q = dt_target / (0.4f * L);
+    const float rho_new = E * q * q;
+    add = (rho_new - r) * d.emat[e].area / 3.0f;
+    h = 1;
+  }
+  dm[e] = add;
+  hit[e] = h;
+}
+
+__global__ void k_mass_scale_nodes(Dev d, const float* __restrict__ dm, const int32_t* __restrict__ hit) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  float m = d.mass[i];
+  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
+    const int e = d.csr_slot[k] / 3;
+    if (hit[e]) m = m + dm[e];
+  }
+  d.mass[i] = m;
+}
+
 __global__ void k_set_young(Dev d, const float* __restrict__ young, const float* __restrict__ poisson,
                             int e_lo, int e_hi) {
   const int e = e_lo + blockIdx.x * blockDim.x + threadIdx.x;
@@ -1691,6 +1734,27 @@ int fw_add_flex_pair(fw_ctx* c, int32_t body1, int32_t body2, float penalty, flo
   if (body1 < 0 || body2 < 0 || body1 >= c->B || body2 >= c->B || body1 == body2)
     return fail(c, FW_ERR_ARG, "fw_add_flex_pair: bodies %d, %d", body1, body2);
   c->h_flex.push_back(fw_ctx::FlexPair{body1, body2, penalty, friction});
+  return FW_OK;
+}
+
+int fw_mass_scaling(fw_ctx* c, float dt_target) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_mass_scaling needs a finalized world (not an arena)");
+  if (!(dt_target > 0.0f)) return fail(c, FW_ERR_ARG, "fw_mass_scaling: dt_target must be > 0");
+  if ((int)c->h_E.size() != c->E || (int)c->h_rho.size() != c->E)
+    return fail(c, FW_ERR_STATE, "fw_mass_scaling: element materials are no longer staged");
+  float *young = nullptr, *rho = nullptr, *dm = nullptr;
+  int32_t* hit = nullptr;
+  int rc;
+  if ((rc = upload(c, &young, c->h_E)) || (rc = upload(c, &rho, c->h_rho)) || (rc = dalloc(c, &dm, c->E)) ||
+      (rc = dalloc(c, &hit, c->E)))
+    return rc;
+  k_mass_scale_elems<<<(c->E + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, young, rho, dt_target, dm, hit);
+  k_mass_scale_nodes<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, dm, hit);
+  c->launches += 2;
+  if ((rc = check_kernel(c, "mass scaling"))) return rc;
+  if (c->path == FW_PATH_STREAM && (rc = stream_records(c))) return rc;  // its node records hold the masses
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
   return FW_OK;
 }
 

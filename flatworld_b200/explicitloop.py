@@ -198,15 +198,14 @@ class ExplicitLoop:
                  front_warps=0, res_sync=0):
         if joints:
             raise NotImplementedError("joints belong to the rigid-body solver, outside flatworld_b200's scope")
-        if mass_scaling_dt > 0.0:
-            raise NotImplementedError("selective mass scaling is not part of flatworld_b200")
         self.domains = domains
         self.d = domains[0].d
         self.joints = joints
         self.ties = list(ties) if ties is not None else []
         self._max_domains = len(domains) + 10
         self.rigidManager = None
-        layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT)
+        layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT,
+                             mass_scaling_dt=mass_scaling_dt)
         self._layout = layout
         self.stableTime = layout.stableTime
         self.useAdapative = layout.useAdapative
@@ -222,6 +221,8 @@ class ExplicitLoop:
         self._packed = PackedWorld([layout])
         self._native = build_native(self._packed, device=device, path=path, patches=patches,
                                     front_warps=front_warps, res_sync=res_sync)
+        if layout.mass_scaling_dt > 0.0:  # applyMassScaling after setGlobalAABB (explicitloop.py:168-169)
+            self._native.mass_scaling(float(np.float32(layout.mass_scaling_dt)))
         self.path, self.patches = self._native.get_path()
         self.aabb = _AABBView(self)
         self.femSpringManager = FemSpringManager(self, self._packed, self._native, 0)

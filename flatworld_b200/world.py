@@ -77,7 +77,7 @@ def _contact_helper(di, dj, ctype, i, j):
 class SceneLayout:
     """Construction-time state of one scene (one reference ExplicitLoop)."""
 
-    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True):
+    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, mass_scaling_dt=0.0):
         for d in domains:
             if d.type not in _SUPPORTED:
                 raise NotImplementedError(
@@ -97,6 +97,11 @@ class SceneLayout:
         for d in self.fem:
             fsm_stable = min(d.stableTime, fsm_stable)
         stable = min(fsm_stable, stable)
+        # explicitloop.py:168-170: mass scaling lifts the bound to its target
+        # (contacts may lower it again below)
+        self.mass_scaling_dt = float(mass_scaling_dt)
+        if self.mass_scaling_dt > 0.0:
+            stable = max(stable, self.mass_scaling_dt)
         # explicitloop.py:237-277: O(D^2) pair loop over contact domains
         contacts = []
         contact_domains = [(i, d) for i, d in enumerate(domains) if d.considerContact]

@@ -147,6 +147,15 @@ int fw_set_flex_scene(fw_ctx* ctx, int32_t scene, int32_t skip_bvh, int32_t n_do
                       const int32_t* dom_body, const float* dom_box);
 int fw_add_flex_pair(fw_ctx* ctx, int32_t body1, int32_t body2, float penalty, float friction);
 int fw_set_flex_clock(fw_ctx* ctx, double dt);
+/* Selective mass scaling (ExplicitLoop(mass_scaling_dt=...)): every triangle
+ * whose critical step 0.4 L_min / sqrt(E / rho) is below dt_target adds
+ * (rho_new - rho) * area / 3 to each of its nodes, rho_new = E (dt_target /
+ * (0.4 L_min))^2, node by node in ascending element order.  Call once, right
+ * after fw_finalize, as the reference calls it right after setGlobalAABB.
+ * Replaces applyMassScaling / _mass_scaling_kernel, femspringmanager.py:139-196,
+ * explicitloop.py:168-170. */
+int fw_mass_scaling(fw_ctx* ctx, float dt_target);
+
 /* The work items' edge caches (boundary edge index hit last substep, or -1;
  * n_items must equal the world's count) and the spatial hash grid: tc, nx, ny,
  * origin x, origin y, cell x, cell y, element-box diagonal minimum.  The

@@ -1146,6 +1146,32 @@ int or_add_flex_pair(or_world* w, int b1, int b2, float penalty, float friction)
   return p;
 }
 
+/* _mass_scaling_kernel (femspringmanager.py:139-196), FEM triangles, serial in
+ * element order. */
+void or_mass_scaling(or_world* w, float dt_target_f) {
+  REAL dt_target = (REAL)dt_target_f;
+  for (int e = 0; e < w->n_elems; ++e) {
+    int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
+    REAL ax = w->x[2 * n1], ay = w->x[2 * n1 + 1], bx = w->x[2 * n2], by = w->x[2 * n2 + 1];
+    REAL cx = w->x[2 * n3], cy = w->x[2 * n3 + 1];
+    REAL e01x = bx - ax, e01y = by - ay, e12x = cx - bx, e12y = cy - by, e20x = ax - cx, e20y = ay - cy;
+    REAL e01 = R_SQRT(e01x * e01x + e01y * e01y), e12 = R_SQRT(e12x * e12x + e12y * e12y);
+    REAL e20 = R_SQRT(e20x * e20x + e20y * e20y);
+    REAL L = rmin(e01, rmin(e12, e20));
+    REAL E = w->E[e], rho = w->rho[e];
+    REAL ce = R_SQRT(E / rho);
+    REAL dt_elem = (REAL)0.4 * L / ce;
+    if (dt_elem < dt_target && L > (REAL)1e-15) {
+      REAL q = dt_target / ((REAL)0.4 * L);
+      REAL rho_new = E * q * q;
+      REAL dm = (rho_new - rho) * w->area[e] / (REAL)3.0;
+      w->mass[n1] = w->mass[n1] + dm;
+      w->mass[n2] = w->mass[n2] + dm;
+      w->mass[n3] = w->mass[n3] + dm;
+    }
+  }
+}
+
 /* The hash grid: tc, nx, ny, origin x, origin y, cell x, cell y, estimate. */
 void or_get_flex_grid(const or_world* w, double* out) {
   const or_flex* f = w->flex;

@@ -78,6 +78,7 @@ def _lib(precision: str):
         L.or_flex_rebuild.argtypes = [C.c_void_p]
         L.or_get_flex_cache.argtypes = [C.c_void_p, _i32p]
         L.or_get_flex_grid.argtypes = [C.c_void_p, _f64p]
+        L.or_mass_scaling.argtypes = [C.c_void_p, C.c_float]
         L.or_destroy.argtypes = [C.c_void_p]
         L.or_log32.argtypes = [C.c_float]
         L.or_log32.restype = C.c_float
@@ -159,7 +160,8 @@ def log32(x, precision="f32"):
 class OracleLoop:
     """CPU restatement of one reference ExplicitLoop over FEM + ground domains."""
 
-    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, precision="f32", threads=1):
+    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, precision="f32", threads=1,
+                 mass_scaling_dt=0.0):
         self.precision = precision
         L = self._L = _lib(precision)
         self.domains = list(domains)
@@ -174,6 +176,8 @@ class OracleLoop:
         for d, Lc in zip(fem, self.char_len):
             fsm = min(0.4 * Lc / (d.prop.mat.E / d.prop.mat.rho) ** 0.5, fsm)
         stable = min(fsm, stable)
+        if mass_scaling_dt > 0.0:  # explicitloop.py:168-170
+            stable = max(stable, mass_scaling_dt)
         # --- contacts (explicitloop.py:237-277; femcontact.py:155-197)
         contacts = []
         cds = [(i, d) for i, d in enumerate(domains) if d.considerContact]
@@ -325,6 +329,8 @@ class OracleLoop:
         self.counter = 0
         # setGlobalAABB -> substep(0.0, 0.0) (femspringmanager.py:872-879)
         L.or_step(self._w, 0.0, 0.0, 0, 1)
+        if mass_scaling_dt > 0.0:  # applyMassScaling right after setGlobalAABB
+            L.or_mass_scaling(self._w, float(np.float32(mass_scaling_dt)))
         if flex:  # explicitloop.py:383-385: initial FEM spatial hash
             L.or_flex_rebuild(self._w)
 
