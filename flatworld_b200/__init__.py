@@ -10,7 +10,7 @@ C ABI (include/fwb200.h); there is no CPU fallback.
 from .bcs import (EnforceAcc, EnforceRotAcc, EnforceRotVel, EnforceVel, Fixed, FixedAll, Force, Gravity,
                   InitialVel, Torque)
 from .definitions import *  # noqa: F401,F403
-from .domains import FemDomain, GroundDomain, HeightFieldDomain, VoxelGridDomain
+from .domains import FemDomain, GroundDomain, HeightFieldDomain, SpringMassDomain, VoxelGridDomain
 from .explicitloop import ExplicitLoop, FemSpringManager
 from .femesher import FEMesher
 from .materials import J2, Elastic, HyperElastic, MisesPlastic, NeoHookean, SolidProp
@@ -35,7 +35,6 @@ PrismaticJoint = _out_of_scope("PrismaticJoint", _RIGID)
 RevoluteJoint = _out_of_scope("RevoluteJoint", _RIGID)
 SphericalJoint = _out_of_scope("SphericalJoint", _RIGID)
 WeldJoint = _out_of_scope("WeldJoint", _RIGID)
-SpringMassDomain = _out_of_scope("SpringMassDomain", _RIGID)
 InitialAngVel = _out_of_scope("InitialAngVel", _RIGID)
 
 __version__ = "0.1.0"

@@ -57,6 +57,7 @@ _SIGNATURES = {
     "fw_add_flex_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float]),
     "fw_set_flex_clock": (C.c_int, [_vp, C.c_double]),
     "fw_mass_scaling": (C.c_int, [_vp, C.c_float]),
+    "fw_set_spring_bodies": (C.c_int, [_vp, C.c_int32, _i32p, _f32p]),
     "fw_read_flex_state": (C.c_int, [_vp, _i32p, C.c_int32, _f32p]),
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
@@ -225,6 +226,10 @@ class NativeWorld:
         self._check(self._L.fw_read_flex_state(self._h, cache.ctypes.data_as(_i32p), int(n_items),
                                                grid.ctypes.data_as(_f32p)), "fw_read_flex_state")
         return cache[:n_items], grid
+
+    def set_spring_bodies(self, bodies, node_mass):
+        b, m = _i(bodies), _f(node_mass)
+        self._check(self._L.fw_set_spring_bodies(self._h, len(b[0]), b[1], m[1]), "fw_set_spring_bodies")
 
     def mass_scaling(self, dt_target: float):
         self._check(self._L.fw_mass_scaling(self._h, float(dt_target)), "fw_mass_scaling")

@@ -24,6 +24,7 @@ constexpr uint32_t NODE_BC_MASK = 0x1FFu;
 constexpr uint32_t NODE_BOUNDARY = 0x200u;
 constexpr int NODE_BODY_SHIFT = 10;
 
+constexpr int MAT_SPRING = 0;  // a 2-node spring of a spring-mass domain (elemType 0 in the reference)
 constexpr int MAT_ELASTIC = 1;
 constexpr int MAT_NEOHOOKEAN = 2;
 constexpr int MAT_MISES = 3;

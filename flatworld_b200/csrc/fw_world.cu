@@ -149,6 +149,21 @@ __device__ __forceinline__ void element_step(const Dev& d, int e) {
     const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
     const int s = d.body_scene[fw::elem_body(m.word)];
     if (!d.scene_active[s]) return;
+    if (fw::elem_type(m.word) == fw::MAT_SPRING) {  // _spring_force_kernel, femspringmanager.py:283-312
+      const float2 va = d.v[c0], vb = d.v[c1];
+      const float xx = a.x - b.x, xy = a.y - b.y;
+      const float lnew = sqrtf(xx * xx + xy * xy);
+      const float dx = xx / lnew, dy = xy / lnew;
+      const float sc = m.lam * (lnew / m.area - 1.0f);  // stiffness x strain; area holds the rest length
+      float fx = sc * dx, fy = sc * dy;
+      const float vx = va.x - vb.x, vy = va.y - vb.y;
+      const float dmp = m.mu * (vx * dx + vy * dy);  // mu holds the damping
+      fx = fx + dmp * dx;
+      fy = fy + dmp * dy;
+      d.corner[q0] = make_float2(-fx, -fy);
+      d.corner[q1] = make_float2(fx, fy);
+      return;
+    }
     float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
     float sy = 0.f, H = 0.f;
     const bool mises = fw::elem_type(m.word) == fw::MAT_MISES;
@@ -333,6 +348,16 @@ __global__ void k_prepare_elements(Dev d, const float* __restrict__ young,
                                    const float* __restrict__ rho, int e_lo, int e_hi) {
   const int e = e_lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= e_hi) return;
+  if (fw::elem_type(d.emat[e].word) == fw::MAT_SPRING) {  // addSpringDomain (femspringmanager.py:848-861)
+    ElemMat m = d.emat[e];
+    m.area = rho[e - e_lo];     // rest length
+    m.lam = young[e - e_lo];    // spring stiffness
+    m.mu = poisson[e - e_lo];   // damping
+    d.emat[e] = m;
+    d.jinv[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+    d.ndmass[e] = 0.0f;         // the nodes carry the domain's mass
+    return;
+  }
   const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
   const float2 a = d.x0[c0], b = d.x0[c1], c = d.x0[c2];
   const float j00 = a.x - c.x, j01 = b.x - c.x, j10 = a.y - c.y, j11 = b.y - c.y;
@@ -363,8 +388,6 @@ __global__ void k_prepare_mass(Dev d, int n_lo, int n_hi) {
   d.mass[i] = m;
 }
 
-// Lame constants of elements [e_lo, e_hi) from new Young's moduli (same
-// formula as k_prepare_elements).
 // Selective mass scaling, _mass_scaling_kernel (femspringmanager.py:139-196):
 // a triangle whose critical step 0.4 L_min / sqrt(E / rho) is below dt_target
 // gets the density that makes it dt_target, and its three nodes a third of
@@ -376,6 +399,11 @@ __global__ void k_mass_scale_elems(Dev d, const float* __restrict__ young, const
                                    float dt_target, float* __restrict__ dm, int32_t* __restrict__ hit) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.E) return;
+  if (fw::elem_type(d.emat[e].word) == fw::MAT_SPRING) {  // springs: the node pass
+    dm[e] = 0.0f;
+    hit[e] = 0;
+    return;
+  }
   const float2 a = d.x[d.conn[3 * e]], b = d.x[d.conn[3 * e + 1]], c = d.x[d.conn[3 * e + 2]];
   const float e01x = b.x - a.x, e01y = b.y - a.y, e12x = c.x - b.x, e12y = c.y - b.y, e20x = a.x - c.x, e20y = a.y - c.y;
   const float e01 = sqrtf(e01x * e01x + e01y * e01y), e12 = sqrtf(e12x * e12x + e12y * e12y);
@@ -397,17 +425,27 @@ __global__ void k_mass_scale_elems(Dev d, const float* __restrict__ young, const
   hit[e] = h;
 }
 
-__global__ void k_mass_scale_nodes(Dev d, const float* __restrict__ dm, const int32_t* __restrict__ hit) {
+__global__ void k_mass_scale_nodes(Dev d, const float* __restrict__ dm, const int32_t* __restrict__ hit,
+                                   float dt_target) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.N) return;
   float m = d.mass[i];
-  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
+  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {  // triangles first (the reference's first loop)
     const int e = d.csr_slot[k] / 3;
     if (hit[e]) m = m + dm[e];
+  }
+  for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {  // then springs: at least 4 k dt^2 (its second loop)
+    const int e = d.csr_slot[k] / 3;
+    const ElemMat em = d.emat[e];
+    if (fw::elem_type(em.word) != fw::MAT_SPRING) continue;
+    const float m_min = 4.0f * em.lam * dt_target * dt_target;
+    if (m < m_min) m = m_min;
   }
   d.mass[i] = m;
 }
 
+// Lame constants of elements [e_lo, e_hi) from new Young's moduli (same
+// formula as k_prepare_elements).
 __global__ void k_set_young(Dev d, const float* __restrict__ young, const float* __restrict__ poisson,
                             int e_lo, int e_hi) {
   const int e = e_lo + blockIdx.x * blockDim.x + threadIdx.x;
@@ -636,6 +674,11 @@ __device__ double elem_energy(const Dev& d, int e) {
   const ElemMat m = d.emat[e];
   const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
   const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
+  if (fw::elem_type(m.word) == fw::MAT_SPRING) {  // k L0 / 2 (l / L0 - 1)^2, whose l-derivative is the spring force
+    const double dx = (double)a.x - b.x, dy = (double)a.y - b.y;
+    const double st = sqrt(dx * dx + dy * dy) / (double)m.area - 1.0;
+    return 0.5 * (double)m.lam * (double)m.area * st * st;
+  }
   const float4 ji = d.jinv[e];
   const double j00 = (double)a.x - (double)c.x, j01 = (double)b.x - (double)c.x;
   const double j10 = (double)a.y - (double)c.y, j11 = (double)b.y - (double)c.y;
@@ -858,6 +901,9 @@ struct fw_ctx {
   FlexDev fx{};
   size_t flex_pre_smem = 0;  // k_flex_pre: (domains + FEM bodies) boxes
   double flex_clock = 0.0;  // host copy of the last fw_set_flex_clock value
+  // spring-mass domains: per body its node mass (0: an FEM body)
+  std::vector<float> h_spring_mass;
+  bool has_springs = false;
 };
 
 namespace {
@@ -1592,8 +1638,10 @@ int fw_set_elements(fw_ctx* c, int32_t n, const int32_t* conn, const int32_t* ma
   if (hardening) c->h_H.assign(hardening, hardening + n);
   for (int e = 0; e < n; ++e) {
     const int t = c->h_type[e];
-    if (t != fw::MAT_ELASTIC && t != fw::MAT_NEOHOOKEAN && t != fw::MAT_MISES)
+    if (t != fw::MAT_SPRING && t != fw::MAT_ELASTIC && t != fw::MAT_NEOHOOKEAN && t != fw::MAT_MISES)
       return fail(c, FW_ERR_ARG, "element %d: unknown material type %d", e, t);
+    if (t == fw::MAT_SPRING && c->arena)
+      return fail(c, FW_ERR_ARG, "element %d: spring-mass domains are not served from an arena", e);
   }
   return FW_OK;
 }
@@ -1613,6 +1661,7 @@ int fw_set_bodies(fw_ctx* c, int32_t nb, const int32_t* noff, const int32_t* ncn
   c->h_eoff.assign(eoff, eoff + nb);
   c->h_ecnt.assign(ecnt, ecnt + nb);
   c->h_scene.assign(scene, scene + nb);
+  c->h_spring_mass.assign(nb, 0.0f);
   c->h_bnoff.assign(bnoff, bnoff + nb);
   c->h_bncnt.assign(bncnt, bncnt + nb);
   c->h_bnodes.assign(bnodes, bnodes + (n_bnodes > 0 ? n_bnodes : 0));
@@ -1750,7 +1799,7 @@ int fw_mass_scaling(fw_ctx* c, float dt_target) {
       (rc = dalloc(c, &hit, c->E)))
     return rc;
   k_mass_scale_elems<<<(c->E + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, young, rho, dt_target, dm, hit);
-  k_mass_scale_nodes<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, dm, hit);
+  k_mass_scale_nodes<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, dm, hit, dt_target);
   c->launches += 2;
   if ((rc = check_kernel(c, "mass scaling"))) return rc;
   if (c->path == FW_PATH_STREAM && (rc = stream_records(c))) return rc;  // its node records hold the masses
@@ -1774,6 +1823,19 @@ int fw_read_flex_state(fw_ctx* c, int32_t* item_cache, int32_t n_items, float* g
     const float v[8] = {(float)g.tc, (float)g.cnx, (float)g.cny, g.olx, g.oly, g.gsx, g.gsy, estf};
     memcpy(grid, v, sizeof(v));
   }
+  return FW_OK;
+}
+
+int fw_set_spring_bodies(fw_ctx* c, int32_t n, const int32_t* bodies, const float* node_mass) {
+  if (!c || n < 0 || (n && (!bodies || !node_mass))) return FW_ERR_ARG;
+  if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_set_spring_bodies after fw_finalize / on an arena");
+  if ((int)c->h_spring_mass.size() != c->B) return fail(c, FW_ERR_STATE, "fw_set_spring_bodies before fw_set_bodies");
+  for (int k = 0; k < n; ++k) {
+    if (bodies[k] < 0 || bodies[k] >= c->B) return fail(c, FW_ERR_ARG, "fw_set_spring_bodies: body %d", bodies[k]);
+    if (!(node_mass[k] > 0.0f)) return fail(c, FW_ERR_ARG, "fw_set_spring_bodies: node mass must be > 0");
+    c->h_spring_mass[bodies[k]] = node_mass[k];
+  }
+  c->has_springs = n > 0;
   return FW_OK;
 }
 
@@ -1946,8 +2008,15 @@ int fw_finalize(fw_ctx* c) {
     if (node_body[i] < 0) return fail(c, FW_ERR_ARG, "node %d belongs to no body", i);
   for (int e = 0; e < E; ++e) {
     if (elem_body[e] < 0) return fail(c, FW_ERR_ARG, "element %d belongs to no body", e);
+    const bool spring = c->h_type[e] == fw::MAT_SPRING;
+    if (spring != (c->h_spring_mass[elem_body[e]] > 0.0f))
+      return fail(c, FW_ERR_ARG, "element %d: springs (type 0) belong to spring-mass bodies, triangles to FEM bodies", e);
     for (int k = 0; k < 3; ++k) {
       const int n = c->h_conn[3 * e + k];
+      if (spring && k == 2) {
+        if (n != -1) return fail(c, FW_ERR_ARG, "spring %d: third node id must be -1", e);
+        continue;
+      }
       if (n < 0 || n >= N) return fail(c, FW_ERR_ARG, "element %d: node id %d outside [0, %d)", e, n, N);
       if (node_body[n] != elem_body[e])
         return fail(c, FW_ERR_ARG, "element %d references node %d of another body", e, n);
@@ -1978,13 +2047,18 @@ int fw_finalize(fw_ctx* c) {
   // CSR node -> (element, corner), ascending element
   std::vector<int32_t> off(N + 1, 0), slot(3 * (size_t)E);
   for (int e = 0; e < E; ++e)
-    for (int k = 0; k < 3; ++k) off[c->h_conn[3 * e + k] + 1]++;
+    for (int k = 0; k < 3; ++k)
+      if (c->h_conn[3 * e + k] >= 0) off[c->h_conn[3 * e + k] + 1]++;
   for (int i = 0; i < N; ++i) off[i + 1] += off[i];
   std::vector<int32_t> cpos(3 * (size_t)E);
   {
     std::vector<int32_t> fill(off.begin(), off.end() - 1);
     for (int e = 0; e < E; ++e)
       for (int k = 0; k < 3; ++k) {
+        if (c->h_conn[3 * e + k] < 0) {  // a spring's missing third corner: never written
+          cpos[3 * (size_t)e + k] = cpos[3 * (size_t)e + k - 1];
+          continue;
+        }
         const int32_t at = fill[c->h_conn[3 * e + k]]++;
         slot[at] = 3 * e + k;
         cpos[3 * (size_t)e + k] = at;
@@ -1999,6 +2073,11 @@ int fw_finalize(fw_ctx* c) {
     j2par[e] = make_float2(c->h_sy[e], c->h_H[e]);
     has_j2 |= c->h_type[e] == fw::MAT_MISES;
   }
+  // device connectivity: a spring's missing third node repeats its second, so
+  // loads that every element issues stay in bounds
+  std::vector<int32_t> conn_dev(c->h_conn);
+  for (int e = 0; e < E; ++e)
+    if (conn_dev[3 * (size_t)e + 2] < 0) conn_dev[3 * (size_t)e + 2] = conn_dev[3 * (size_t)e + 1];
   std::vector<float2> x0(N), bcv(N), v0(N);
   for (int i = 0; i < N; ++i) {
     x0[i] = make_float2(c->h_x[2 * i], c->h_x[2 * i + 1]);
@@ -2013,7 +2092,7 @@ int fw_finalize(fw_ctx* c) {
       (rc = upload(c, &d.bcv, bcv)) || (rc = upload(c, &d.node_word, word)) ||
       (rc = dalloc(c, &d.mass, N)) || (rc = upload(c, &d.csr_off, off)) ||
       (rc = upload(c, &d.csr_slot, slot)) || (rc = upload(c, &d.corner_pos, cpos)) ||
-      (rc = upload(c, &d.conn, c->h_conn)) ||
+      (rc = upload(c, &d.conn, conn_dev)) ||
       (rc = dalloc(c, &d.jinv, E)) || (rc = upload(c, &d.emat, emat)) ||
       (rc = upload(c, &d.j2par, j2par)) || (rc = dalloc(c, &d.j2state, has_j2 ? E : 1)) ||
       (rc = dalloc(c, &d.ndmass, E)) || (rc = dalloc(c, &d.corner, 3 * (size_t)E)) ||
@@ -2044,8 +2123,20 @@ int fw_finalize(fw_ctx* c) {
   k_prepare_mass<<<(N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(d, 0, N);
   c->launches += 2;
   if ((rc = check_kernel(c, "prepare"))) return rc;
+  if (c->has_springs) {  // a spring-mass domain's nodes carry its mass (femspringmanager.py:844-845)
+    std::vector<float> sm(N);
+    FW_CUDA(c, cudaMemcpyAsync(sm.data(), d.mass, sizeof(float) * N, cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < B; ++b)
+      if (c->h_spring_mass[b] > 0.0f)
+        for (int k = 0; k < c->h_ncnt[b]; ++k) sm[c->h_noff[b] + k] = c->h_spring_mass[b];
+    FW_CUDA(c, cudaMemcpyAsync(d.mass, sm.data(), sizeof(float) * N, cudaMemcpyHostToDevice, c->stream));
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
   set_grids(c);
+  if (c->has_springs && (c->path_req == FW_PATH_RESIDENT || c->path_req == FW_PATH_STREAM))
+    return fail(c, FW_ERR_ARG, "spring-mass domains run on the gather path only");
   if (!c->h_flex.empty()) {
     if (c->path_req == FW_PATH_RESIDENT || c->path_req == FW_PATH_STREAM)
       return fail(c, FW_ERR_ARG, "FEM-FEM contact runs on the gather path only");
@@ -2060,7 +2151,7 @@ int fw_finalize(fw_ctx* c) {
     FW_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   c->path = FW_PATH_GATHER;
-  if (c->has_flex) {
+  if (c->has_flex || c->has_springs) {
     c->finalized = true;
     return FW_OK;
   }
@@ -2479,6 +2570,7 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
   if (!c->finalized || c->arena)
     return fail(c, FW_ERR_STATE, "fw_set_element_young needs a finalized world (not an arena)");
   if (first < 0 || count < 0 || (int64_t)first + count > c->E) return fail(c, FW_ERR_ARG, "element range out of bounds");
+  if (c->has_springs) return fail(c, FW_ERR_STATE, "fw_set_element_young: the world has spring-mass domains");
   if (count == 0) return FW_OK;
   int rc;
   if (!c->d_poisson && (rc = upload(c, &c->d_poisson, c->h_nu))) return rc;
@@ -2493,7 +2585,8 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
 }
 
 int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
-  if (c && c->has_flex) return fail(c, FW_ERR_STATE, "the adjoint does not cover FEM-FEM contact");
+  if (c && (c->has_flex || c->has_springs))
+    return fail(c, FW_ERR_STATE, "the adjoint covers FEM triangles without FEM-FEM contact");
   if (!c) return FW_ERR_ARG;
   // The forward may run on either path (identical bits); the recompute and the
   // reverse use the gather kernels and data, which every non-arena world has.
@@ -2649,7 +2742,8 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
 }
 
 int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE, int32_t on_device) {
-  if (c && c->has_flex) return fail(c, FW_ERR_STATE, "the tangent does not cover FEM-FEM contact");
+  if (c && (c->has_flex || c->has_springs))
+    return fail(c, FW_ERR_STATE, "the tangent covers FEM triangles without FEM-FEM contact");
   if (!c) return FW_ERR_ARG;
   if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)
     return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world on the gather or resident path");

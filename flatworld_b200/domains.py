@@ -265,3 +265,47 @@ class VoxelGridDomain(DomainBase):
         verts = np.stack([p0, p1], axis=1).reshape(-1, 2)
         edges = np.arange(2 * len(p0), dtype=np.int32).reshape(-1, 2)
         return verts, edges
+
+
+class SpringMassDomain(DomainBase):
+    """A spring-mass network (reference: flatworld/springmass.py:6-73): nodes
+    of equal mass joined by 2-node springs.  prop = [stiffness, damping, node
+    mass]; rest lengths are the float32 norms of the initial edge vectors."""
+
+    def __init__(self, d, coords, conns, prop=[100.0, 1.0, 1.0], bcs=[], considerContact=True,
+                 considerGroundContact=True, initials=[], friction=0.0):
+        if d != 2:
+            raise NotImplementedError("flatworld_b200 implements 2D spring-mass domains only")
+        self.d = d
+        self.prop = prop
+        self.bcs = bcs
+        self.initials = initials
+        self.friction = friction
+        self.considerContact = considerContact
+        self.considerGroundContact = considerGroundContact
+        self.type = DomainType.SPRINGMASS
+        self.spring, self.damping, self.mass = prop
+        self.massInv = 1.0 / self.mass
+        self.coords = np.array(coords, dtype=np.float32)
+        self.connectivity = np.array(conns, dtype=np.int32)
+        self.nnodes = coords.shape[0]
+        self.nelements = conns.shape[0]
+        ab = self.coords[self.connectivity[:, 0]] - self.coords[self.connectivity[:, 1]]
+        self.restLength = np.array([np.linalg.norm(v) for v in ab], dtype=np.float32)  # springmass.py:43-49
+        self.stableTime = 0.5 * np.sqrt(self.mass / self.spring)  # springmass.py:38
+        self.category_bits = COLLISION_CATEGORY_FEM
+        self.collide_bits = COLLISION_MASK_ALL
+        self.femManager = None
+        self.domainIdx = None
+
+    def attach(self, femManager, domainIdx):
+        self.femManager = femManager
+        self.domainIdx = domainIdx
+
+    def getBBox(self):
+        if self.femManager is not None:
+            return self.femManager.body_aabb(self.domainIdx)
+        return np.min(self.coords, axis=0), np.max(self.coords, axis=0)
+
+    def getCurrentCoords(self):
+        return self.femManager.body_coords(self.domainIdx)

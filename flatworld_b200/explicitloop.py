@@ -72,9 +72,10 @@ class FemSpringManager:
         self._ne = int(sum(int(packed.ecnt[b]) for b in bodies))
         sc = packed.scenes[scene]
         self.domains = sc.fem
-        self.domainMeshes = [d.mesh for d in sc.fem]
+        self.domainMeshes = [getattr(d, "mesh", None) for d in sc.fem]
         self.d = 2
-        nb = sum(d.mesh.numBoundNodes for d in sc.fem)
+        nbound = [d.mesh.numBoundNodes if d.type == DomainType.FEM else d.nnodes for d in sc.fem]
+        nb = sum(nbound)
         self.MAX_NODES = max(self._nn + 1024, 2048)
         self.MAX_ELEMENTS = max(self._ne + 2048, 4096)
         self.MAX_BOUNDARY_NODES = max(nb + 1024, self.MAX_NODES)
@@ -84,19 +85,20 @@ class FemSpringManager:
         i32 = np.int32
         self.totalNodes = _HostArray(np.array([self._nn], i32))
         self.totalElements = _HostArray(np.array([self._ne], i32))
-        self.totalFEMElements = _HostArray(np.array([self._ne], i32))
-        self.totalFEMNodes = _HostArray(np.array([self._nn], i32))
-        self.numFemDomains = _HostArray(np.array([len(bodies)], i32))
-        self.numSpringDomains = _HostArray(np.array([0], i32))
+        n_fem = sum(1 for d in sc.fem if d.type == DomainType.FEM)
+        self.totalFEMElements = _HostArray(np.array([sum(d.nelements for d in sc.fem if d.type == DomainType.FEM)], i32))
+        self.totalFEMNodes = _HostArray(np.array([sum(d.nnodes for d in sc.fem if d.type == DomainType.FEM)], i32))
+        self.numFemDomains = _HostArray(np.array([n_fem], i32))
+        self.numSpringDomains = _HostArray(np.array([len(bodies) - n_fem], i32))
         pad = lambda a, n, dt: np.concatenate([a, np.zeros((n - len(a),) + a.shape[1:], dt)])  # noqa: E731
         md = max(len(bodies), 128)
         self.domainNodeOffset = _HostArray(pad(packed.noff[bodies] - self._n0, md, i32))
         self.domainNodeCount = _HostArray(pad(packed.ncnt[bodies], md, i32))
         self.domainElemOffset = _HostArray(pad(packed.eoff[bodies] - self._e0, md, i32))
         self.domainElemCount = _HostArray(pad(packed.ecnt[bodies], md, i32))
-        bnoff = np.concatenate([[0], np.cumsum([d.mesh.numBoundNodes for d in sc.fem])[:-1]]).astype(i32)
+        bnoff = np.concatenate([[0], np.cumsum(nbound)[:-1]]).astype(i32)
         self.domainBoundaryNodeOffset = _HostArray(pad(bnoff, md, i32))
-        self.domainBoundaryNodeCount = _HostArray(pad(np.array([d.mesh.numBoundNodes for d in sc.fem], i32), md, i32))
+        self.domainBoundaryNodeCount = _HostArray(pad(np.array(nbound, i32), md, i32))
         bn = np.concatenate([packed.bnodes[packed.bnoff[b]:packed.bnoff[b] + packed.bncnt[b]] for b in bodies]) - self._n0
         self.boundaryNodes = _HostArray(pad(bn.astype(i32), self.MAX_BOUNDARY_NODES, i32))
         ids = [loop.domains.index(d) for d in sc.fem]
@@ -176,7 +178,7 @@ class _AABBView:
         out = np.zeros((lp._max_domains, 2, 2), np.float32)
         boxes = lp._native.read_aabb(lp._packed.B)
         for i, d in enumerate(lp.domains):
-            if d.type == DomainType.FEM:
+            if d.type in (DomainType.FEM, DomainType.SPRINGMASS):
                 k = lp._packed.scenes[0].fem.index(d)
                 b = lp._packed.scene_bodies[0][k]
                 out[i, 0] = boxes[b, :2]

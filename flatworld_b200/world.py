@@ -20,7 +20,10 @@ import numpy as np
 from . import _native
 from .definitions import ContactType, DomainType
 
-_SUPPORTED = (DomainType.FEM, DomainType.ANALYTICAL, DomainType.HEIGHTFIELD, DomainType.VOXELMAP)
+_SUPPORTED = (DomainType.FEM, DomainType.SPRINGMASS, DomainType.ANALYTICAL, DomainType.HEIGHTFIELD,
+              DomainType.VOXELMAP)
+_BODY_TYPES = (DomainType.FEM, DomainType.SPRINGMASS)
+_SPRING_PENALTY_SCALE = 100.0  # femcontact.py:209, 246, 259, 272
 
 
 def bulk_modulus(mat) -> float:
@@ -54,8 +57,22 @@ class ContactSpec:
 
 
 def _contact_helper(di, dj, ctype, i, j):
-    """contactHelper (femcontact.py:283-303) restricted to the FEM-ground and
-    FEM-FEM pairs."""
+    """contactHelper (femcontact.py:283-303) restricted to the FEM-ground,
+    FEM-FEM and spring-mass pairs."""
+    if ctype in (ContactType.ANALYTICALSPRING, ContactType.SPRINGHEIGHTFIELD):
+        # ContactSpringAnalytical / ContactSpringHeightField (femcontact.py:251-280):
+        # penalty 100 k, stable time 0.5 sqrt(m / penalty)
+        spring, ground = (di, dj) if di.type == DomainType.SPRINGMASS else (dj, di)
+        pen = spring.spring * _SPRING_PENALTY_SCALE
+        kind = "plane" if ctype == ContactType.ANALYTICALSPRING else "heightfield"
+        return ContactSpec(kind, spring, ground, (i, j), pen, 0.5 * (spring.mass / pen) ** 0.5)
+    if ctype == ContactType.FLEXSPRING:
+        # ContactSpringFlex (femcontact.py:207-220): a reference contact the loop
+        # never executes (it lands in the unbatched list); it bounds the stable
+        # time and keeps the broad phase on
+        spring, femd = (di, dj) if di.type == DomainType.SPRINGMASS else (dj, di)
+        pen = min(spring.spring, segment_penalty(femd)) * _SPRING_PENALTY_SCALE
+        return ContactSpec("spring-fem", spring, femd, (i, j), pen, contact_stable_time(pen, femd))
     kinds = {
         ContactType.FLEXANLAYTICAL: "plane",
         ContactType.FEXHEIGHTFIELD: "heightfield",
@@ -83,9 +100,15 @@ class SceneLayout:
                 raise NotImplementedError(
                     f"domain type {d.type} (rigid bodies, springs) is outside flatworld_b200's scope")
         self.domains = list(domains)
-        self.fem = [d for d in domains if d.type == DomainType.FEM]
+        # the bodies: FEM and spring-mass domains in loop order (FemSpringManager.domains)
+        self.fem = [d for d in domains if d.type in _BODY_TYPES]
         if not self.fem:
-            raise ValueError("a scene needs at least one FemDomain")
+            raise ValueError("a scene needs at least one FemDomain or SpringMassDomain")
+        kinds = [d.type for d in self.fem]
+        if DomainType.SPRINGMASS in kinds and DomainType.FEM in kinds[kinds.index(DomainType.SPRINGMASS):]:
+            raise NotImplementedError(
+                "a SpringMassDomain before a FemDomain: the reference's kernels take the first "
+                "totalFEMElements elements as triangles (femspringmanager.py:231, 297), so list FEM domains first")
         self.damping = float(damping)
         self.useAdapative = bool(useAdapativeDT)
         # explicitloop.py:145-170: 1.0, capped by the rigid manager's 1e-3 when an
@@ -105,7 +128,7 @@ class SceneLayout:
         # explicitloop.py:237-277: O(D^2) pair loop over contact domains
         contacts = []
         contact_domains = [(i, d) for i, d in enumerate(domains) if d.considerContact]
-        if any(d.type == DomainType.FEM for d in domains if d.considerContact):
+        if any(d.type in _BODY_TYPES for d in domains if d.considerContact):
             for a, (i, di) in enumerate(contact_domains):
                 for b in range(a):
                     j, dj = contact_domains[b]
@@ -134,7 +157,7 @@ class SceneLayout:
         anal = [c for c in contacts if c.kind == "plane"]
         hf = [c for c in contacts if c.kind == "heightfield"]
         vox = [c for c in contacts if c.kind == "voxel"]
-        self.unbatched = []
+        self.unbatched = [c for c in contacts if c.kind == "spring-fem"]
         if len({id(c.ground) for c in hf}) > 1:
             warnings.warn("more than one HeightFieldDomain in a loop: like the reference, height-field "
                           "contact is not executed for any of them", RuntimeWarning)
@@ -176,24 +199,39 @@ class PackedWorld:
         Hv = np.zeros(E, np.float32)
         noff, ncnt, eoff, ecnt, bscene, bnoff, bncnt, bnodes = [], [], [], [], [], [], [], []
         beoff, becnt, bedges = [], [], []
+        spring_bodies = []
         self.body_of = {}  # (scene idx, fem idx) -> global body id
         self.scene_bodies = []
         n0 = e0 = b0 = 0
         for si, sc in enumerate(scenes):
             bodies = []
             for fi, dom in enumerate(sc.fem):
-                mesh = dom.mesh
-                nn, ne = mesh.numNodes, mesh.numElements
-                coords[n0:n0 + nn] = np.asarray(mesh.coords, dtype=np.float32)[:, :2]
-                conn[e0:e0 + ne] = np.asarray(mesh.connectivity, dtype=np.int64)[:, :3] + n0
-                mat = dom.prop.getMaterial()
-                mtype[e0:e0 + ne] = int(mat.type)
-                ey = getattr(dom, "elementYoung", None)  # optional per-element E (else the material's)
-                Ev[e0:e0 + ne] = float(mat.E) if ey is None else np.asarray(ey, np.float32).reshape(ne)
-                nuv[e0:e0 + ne] = float(mat.nu)
-                rhov[e0:e0 + ne] = float(mat.rho)
-                syv[e0:e0 + ne] = float(getattr(mat, "sigma_y", 0.0))
-                Hv[e0:e0 + ne] = float(getattr(mat, "H", 0.0))
+                spring = dom.type == DomainType.SPRINGMASS
+                if spring:
+                    # addSpringDomain (femspringmanager.py:815-870): 2-node springs,
+                    # type 0; stiffness, damping and rest length ride in E, nu, rho
+                    nn, ne = dom.nnodes, dom.nelements
+                    coords[n0:n0 + nn] = np.asarray(dom.coords, dtype=np.float32)[:, :2]
+                    conn[e0:e0 + ne, :2] = np.asarray(dom.connectivity, dtype=np.int64)[:, :2] + n0
+                    conn[e0:e0 + ne, 2] = -1
+                    mtype[e0:e0 + ne] = 0
+                    Ev[e0:e0 + ne] = float(dom.spring)
+                    nuv[e0:e0 + ne] = float(dom.damping)
+                    rhov[e0:e0 + ne] = dom.restLength
+                    spring_bodies.append((b0 + fi, float(np.float32(dom.mass))))
+                else:
+                    mesh = dom.mesh
+                    nn, ne = mesh.numNodes, mesh.numElements
+                    coords[n0:n0 + nn] = np.asarray(mesh.coords, dtype=np.float32)[:, :2]
+                    conn[e0:e0 + ne] = np.asarray(mesh.connectivity, dtype=np.int64)[:, :3] + n0
+                    mat = dom.prop.getMaterial()
+                    mtype[e0:e0 + ne] = int(mat.type)
+                    ey = getattr(dom, "elementYoung", None)  # optional per-element E (else the material's)
+                    Ev[e0:e0 + ne] = float(mat.E) if ey is None else np.asarray(ey, np.float32).reshape(ne)
+                    nuv[e0:e0 + ne] = float(mat.nu)
+                    rhov[e0:e0 + ne] = float(mat.rho)
+                    syv[e0:e0 + ne] = float(getattr(mat, "sigma_y", 0.0))
+                    Hv[e0:e0 + ne] = float(getattr(mat, "H", 0.0))
                 # processConditions (femspringmanager.py:660-705)
                 for bc in dom.bcs:
                     t, nodes, values = bc.processData()
@@ -221,11 +259,13 @@ class PackedWorld:
                 ecnt.append(ne)
                 bscene.append(si)
                 bnoff.append(sum(len(x) for x in bnodes))
-                bn = n0 + np.asarray(mesh.boundaryNodes, dtype=np.int64)
+                # a spring domain's contact work items and box cover all its nodes
+                bn = n0 + (np.arange(nn, dtype=np.int64) if spring else np.asarray(mesh.boundaryNodes, dtype=np.int64))
                 bncnt.append(len(bn))
                 bnodes.append(bn)
                 beoff.append(sum(len(x) for x in bedges))
-                be = n0 + np.asarray(mesh.boundaryElements, dtype=np.int64).reshape(-1, 2)
+                be = (np.zeros((0, 2), np.int64) if spring
+                      else n0 + np.asarray(mesh.boundaryElements, dtype=np.int64).reshape(-1, 2))
                 becnt.append(len(be))
                 bedges.append(be)
                 n0 += nn
@@ -242,6 +282,7 @@ class PackedWorld:
         self.bnoff = np.asarray(bnoff, np.int32)
         self.bncnt = np.asarray(bncnt, np.int32)
         self.bnodes = np.concatenate(bnodes).astype(np.int32) if bnodes else np.zeros(0, np.int32)
+        self.spring_bodies = spring_bodies  # (body id, node mass f32)
         self.beoff = np.asarray(beoff, np.int32)
         self.becnt = np.asarray(becnt, np.int32)
         self.bedges = np.concatenate(bedges).astype(np.int32) if bedges else np.zeros((0, 2), np.int32)
@@ -308,6 +349,9 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
     nw.set_elements(packed.conn, packed.mtype, packed.Ev, packed.nuv, packed.rhov, packed.syv, packed.Hv)
     nw.set_bodies(packed.noff, packed.ncnt, packed.eoff, packed.ecnt, packed.bscene, packed.bnoff,
                   packed.bncnt, packed.bnodes)
+    if packed.spring_bodies:
+        nw.set_spring_bodies(np.asarray([b for b, _ in packed.spring_bodies], np.int32),
+                             np.asarray([m for _, m in packed.spring_bodies], np.float32))
     nw.set_scenes(np.asarray([s.damping for s in packed.scenes], np.float32))
     for kind, body, pen, lo, hi, g in packed.pair_records():
         if kind == "plane":

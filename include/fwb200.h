@@ -147,11 +147,25 @@ int fw_set_flex_scene(fw_ctx* ctx, int32_t scene, int32_t skip_bvh, int32_t n_do
                       const int32_t* dom_body, const float* dom_box);
 int fw_add_flex_pair(fw_ctx* ctx, int32_t body1, int32_t body2, float penalty, float friction);
 int fw_set_flex_clock(fw_ctx* ctx, double dt);
+/* Spring-mass domains (SpringMassDomain, femspringmanager.py:815-870): the
+ * listed bodies are spring-mass bodies whose nodes each carry node_mass (the
+ * domain's prop[2]).  Their elements are 2-node springs given to
+ * fw_set_elements as type 0 with the third node id -1, young = stiffness
+ * (prop[0]), poisson = damping (prop[1]) and density = rest length; the
+ * force is _spring_force_kernel's (femspringmanager.py:283-312), added after
+ * the triangles' as the reference launches it.  Pass every node of a spring
+ * body as its boundary nodes (its contact work items and box cover all of
+ * them, mixedcontact.py:1822-1829).  Call after fw_set_bodies.  Gather path
+ * only. */
+int fw_set_spring_bodies(fw_ctx* ctx, int32_t n, const int32_t* bodies, const float* node_mass);
+
 /* Selective mass scaling (ExplicitLoop(mass_scaling_dt=...)): every triangle
  * whose critical step 0.4 L_min / sqrt(E / rho) is below dt_target adds
  * (rho_new - rho) * area / 3 to each of its nodes, rho_new = E (dt_target /
  * (0.4 L_min))^2, node by node in ascending element order.  Call once, right
  * after fw_finalize, as the reference calls it right after setGlobalAABB.
+ * Spring nodes are then raised to at least 4 k dt_target^2 (the kernel's second
+ * loop).
  * Replaces applyMassScaling / _mass_scaling_kernel, femspringmanager.py:139-196,
  * explicitloop.py:168-170. */
 int fw_mass_scaling(fw_ctx* ctx, float dt_target);

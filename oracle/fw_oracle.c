@@ -131,6 +131,7 @@ static float or_logf(float x) {
 #define BC_GRAVITY 0x10
 
 /* MaterialType: flatworld/definitions.py:80-83 */
+#define MAT_SPRING 0 /* a 2-node spring of a spring-mass domain (elemType 0) */
 #define MAT_ELASTIC 1
 #define MAT_NEOHOOKEAN 2
 #define MAT_MISES 3
@@ -188,6 +189,11 @@ static int32_t* dupi(const int32_t* src, size_t n) {
 static void prepare(or_world* w) {
   for (int i = 0; i < w->n_nodes; ++i) w->mass[i] = 0;
   for (int e = 0; e < w->n_elems; ++e) {
+    if (w->type[e] == MAT_SPRING) { /* addSpringDomain: elemVolume = rest length (rho slot) */
+      w->area[e] = w->rho[e];
+      for (int k = 0; k < 4; ++k) w->jinv[4 * e + k] = 0;
+      continue;
+    }
     int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
     REAL j00 = w->x[2 * n1] - w->x[2 * n3], j01 = w->x[2 * n2] - w->x[2 * n3];
     REAL j10 = w->x[2 * n1 + 1] - w->x[2 * n3 + 1], j11 = w->x[2 * n2 + 1] - w->x[2 * n3 + 1];
@@ -292,6 +298,20 @@ static void stress(const or_world* w, int e, REAL F00, REAL F01, REAL F10, REAL 
 /* _fem_internal_force_kernel (femspringmanager.py:217-280): writes the three
  * corner forces -(B^T S)*A of element e into out[6] and updates J2 state. */
 static void element_force(or_world* w, int e, REAL* out) {
+  if (w->type[e] == MAT_SPRING) { /* _spring_force_kernel (femspringmanager.py:283-312) */
+    int a = w->conn[3 * e], b = w->conn[3 * e + 1];
+    REAL xx = w->x[2 * a] - w->x[2 * b], xy = w->x[2 * a + 1] - w->x[2 * b + 1];
+    REAL lnew = R_SQRT(xx * xx + xy * xy);
+    REAL dx = xx / lnew, dy = xy / lnew;
+    REAL sc = w->E[e] * (lnew / w->area[e] - (REAL)1.0);
+    REAL fx = sc * dx, fy = sc * dy;
+    REAL vx = w->v[2 * a] - w->v[2 * b], vy = w->v[2 * a + 1] - w->v[2 * b + 1];
+    REAL dmp = w->nu[e] * (vx * dx + vy * dy); /* nu slot: damping */
+    fx = fx + dmp * dx;
+    fy = fy + dmp * dy;
+    out[0] = -fx; out[1] = -fy; out[2] = fx; out[3] = fy; out[4] = 0; out[5] = 0;
+    return;
+  }
   int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
   const REAL* x = w->x;
   REAL j00 = x[2 * n1] - x[2 * n3], j01 = x[2 * n2] - x[2 * n3];
@@ -565,12 +585,14 @@ static void build_csr(or_world* w) {
   w->csr_slot = (int32_t*)malloc(sizeof(int32_t) * (3 * (size_t)E + 1));
   w->corner = (REAL*)malloc(sizeof(REAL) * (6 * (size_t)E + 1));
   for (int e = 0; e < E; ++e)
-    for (int c = 0; c < 3; ++c) w->csr_off[w->conn[3 * e + c] + 1]++;
+    for (int c = 0; c < 3; ++c)
+      if (w->conn[3 * e + c] >= 0) w->csr_off[w->conn[3 * e + c] + 1]++;
   for (int i = 0; i < N; ++i) w->csr_off[i + 1] += w->csr_off[i];
   int32_t* fill = (int32_t*)malloc(sizeof(int32_t) * ((size_t)N + 1));
   for (int i = 0; i < N; ++i) fill[i] = w->csr_off[i];
   for (int e = 0; e < E; ++e)
-    for (int c = 0; c < 3; ++c) w->csr_slot[fill[w->conn[3 * e + c]]++] = 3 * e + c;
+    for (int c = 0; c < 3; ++c)
+      if (w->conn[3 * e + c] >= 0) w->csr_slot[fill[w->conn[3 * e + c]]++] = 3 * e + c;
   free(fill);
 }
 
@@ -1151,6 +1173,7 @@ int or_add_flex_pair(or_world* w, int b1, int b2, float penalty, float friction)
 void or_mass_scaling(or_world* w, float dt_target_f) {
   REAL dt_target = (REAL)dt_target_f;
   for (int e = 0; e < w->n_elems; ++e) {
+    if (w->type[e] == MAT_SPRING) continue;
     int n1 = w->conn[3 * e], n2 = w->conn[3 * e + 1], n3 = w->conn[3 * e + 2];
     REAL ax = w->x[2 * n1], ay = w->x[2 * n1 + 1], bx = w->x[2 * n2], by = w->x[2 * n2 + 1];
     REAL cx = w->x[2 * n3], cy = w->x[2 * n3 + 1];
@@ -1170,6 +1193,20 @@ void or_mass_scaling(or_world* w, float dt_target_f) {
       w->mass[n3] = w->mass[n3] + dm;
     }
   }
+  for (int e = 0; e < w->n_elems; ++e) { /* springs: at least 4 k dt^2 per node */
+    if (w->type[e] != MAT_SPRING) continue;
+    REAL m_min = (REAL)4.0 * w->E[e] * dt_target * dt_target;
+    for (int k = 0; k < 2; ++k) {
+      int nid = w->conn[3 * e + k];
+      if (w->mass[nid] < m_min) w->mass[nid] = m_min;
+    }
+  }
+}
+
+/* A spring-mass body's nodes (its boundary-node list: all of them) carry its
+ * node mass (femspringmanager.py:844-845). */
+void or_set_spring_mass(or_world* w, int body, float mass) {
+  for (int k = 0; k < w->bn_cnt[body]; ++k) w->mass[w->bnodes[w->bn_off[body] + k]] = (REAL)mass;
 }
 
 /* The hash grid: tc, nx, ny, origin x, origin y, cell x, cell y, estimate. */
@@ -1209,8 +1246,10 @@ void or_step(or_world* w, float dt_f, float damping_f, long counter, int init_st
       w->fext[2 * n1 + 1] += f[1];
       w->fext[2 * n2] += f[2];
       w->fext[2 * n2 + 1] += f[3];
-      w->fext[2 * n3] += f[4];
-      w->fext[2 * n3 + 1] += f[5];
+      if (n3 >= 0) {  /* a spring has two nodes */
+        w->fext[2 * n3] += f[4];
+        w->fext[2 * n3 + 1] += f[5];
+      }
     }
     for (int i = 0; i < N; ++i) integrate_node(w, i, dt, damping);
   } else {

@@ -39,6 +39,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # flatworld/definitions.py
 FEM, ANALYTICAL, RIGID, SPRINGMASS, HEIGHTFIELD, VOXELMAP = 0b10, 0b1, 0b100, 0b1000, 0b100000, 0b1000000
 FLEXANLAYTICAL, FLEXFLEX, FEXHEIGHTFIELD, FLEXVOXELMAP = 0b11, 0b10, 0b100010, 0b1000010
+FLEXSPRING, ANALYTICALSPRING, SPRINGHEIGHTFIELD = 0b1010, 0b1001, 0b101000
 RIGIDRIGID, RIGIDANLAYTICAL, ANALYTICALANALYTICAL = 0b100, 0b101, 0b1
 
 _LIBS = {}
@@ -79,6 +80,7 @@ def _lib(precision: str):
         L.or_get_flex_cache.argtypes = [C.c_void_p, _i32p]
         L.or_get_flex_grid.argtypes = [C.c_void_p, _f64p]
         L.or_mass_scaling.argtypes = [C.c_void_p, C.c_float]
+        L.or_set_spring_mass.argtypes = [C.c_void_p, C.c_int, C.c_float]
         L.or_destroy.argtypes = [C.c_void_p]
         L.or_log32.argtypes = [C.c_float]
         L.or_log32.restype = C.c_float
@@ -165,23 +167,28 @@ class OracleLoop:
         self.precision = precision
         L = self._L = _lib(precision)
         self.domains = list(domains)
-        fem = [d for d in domains if d.type == FEM]
+        # bodies: FEM and spring-mass domains in loop order (FemSpringManager.domains)
+        fem = [d for d in domains if d.type in (FEM, SPRINGMASS)]
         self.fem = fem
         # --- stable time (explicitloop.py:145-170, femdomain.py:24)
         stable = 1.0
         if any(d.type in (RIGID, ANALYTICAL) for d in domains):
             stable = min(1.0 / 1000.0, stable)
-        self.char_len = [char_length_literal(d.mesh.connectivity, d.mesh.coords) for d in fem]
+        self.char_len = [char_length_literal(d.mesh.connectivity, d.mesh.coords) if d.type == FEM else 0.0
+                         for d in fem]
         fsm = 1.0
         for d, Lc in zip(fem, self.char_len):
-            fsm = min(0.4 * Lc / (d.prop.mat.E / d.prop.mat.rho) ** 0.5, fsm)
+            if d.type == FEM:
+                fsm = min(0.4 * Lc / (d.prop.mat.E / d.prop.mat.rho) ** 0.5, fsm)
+            else:  # springmass.py:38
+                fsm = min(0.5 * np.sqrt(d.mass / d.spring), fsm)
         stable = min(fsm, stable)
         if mass_scaling_dt > 0.0:  # explicitloop.py:168-170
             stable = max(stable, mass_scaling_dt)
         # --- contacts (explicitloop.py:237-277; femcontact.py:155-197)
         contacts = []
         cds = [(i, d) for i, d in enumerate(domains) if d.considerContact]
-        if any(d.type == FEM for d in domains if d.considerContact):
+        if any(d.type in (FEM, SPRINGMASS) for d in domains if d.considerContact):
             for a, (i, di) in enumerate(cds):
                 for b in range(a):
                     j, dj = cds[b]
@@ -189,6 +196,17 @@ class OracleLoop:
                     if di.category_bits & dj.collide_bits == 0 or di.collide_bits & dj.category_bits == 0:
                         continue
                     if ct in (RIGIDRIGID, RIGIDANLAYTICAL, ANALYTICALANALYTICAL):
+                        continue
+                    if ct in (ANALYTICALSPRING, SPRINGHEIGHTFIELD):  # femcontact.py:251-280
+                        spr, gnd = (di, dj) if di.type == SPRINGMASS else (dj, di)
+                        pen = spr.spring * 100.0
+                        contacts.append((FLEXANLAYTICAL if ct == ANALYTICALSPRING else FEXHEIGHTFIELD, spr, gnd, pen,
+                                         0.5 * (spr.mass / pen) ** 0.5))
+                        continue
+                    if ct == FLEXSPRING:  # femcontact.py:207-220: never executed (unbatched), bounds dt
+                        spr, fd = (di, dj) if di.type == SPRINGMASS else (dj, di)
+                        pen = min(spr.spring, self._seg_penalty(fd)) * 100.0
+                        contacts.append((FLEXSPRING, spr, fd, pen, self._contact_stable(pen, fd, fem)))
                         continue
                     if ct == FLEXFLEX:  # ContactFlexFlex(dom_i, dom_j): domain1 = i, domain2 = j
                         pen = min(self._seg_penalty(di), self._seg_penalty(dj)) * 1.0
@@ -213,7 +231,37 @@ class OracleLoop:
         bn_off, bn_cnt, bnodes = [], [], []
         off = 0
         self.node_ranges = []
+        spring_mass = []
         for d in fem:
+            if d.type == SPRINGMASS:  # addSpringDomain (femspringmanager.py:815-870)
+                nn = d.nnodes
+                xs.append(np.asarray(d.coords, dtype=np.float32)[:, :2])
+                v = np.zeros((nn, 2), np.float32)
+                bits = np.zeros(nn, np.int64)
+                vals = np.zeros((nn, 2), np.float32)
+                self._conditions(d, nn, v, bits, vals)
+                vs.append(v)
+                bcs.append(bits)
+                bcv.append(vals)
+                cn = np.full((d.nelements, 3), -1, np.int64)
+                cn[:, :2] = np.asarray(d.connectivity, np.int64)[:, :2] + off
+                conns.append(cn)
+                ne = d.nelements
+                types.append(np.zeros(ne))
+                Es.append(np.full(ne, float(d.spring), np.float32))
+                nus.append(np.full(ne, float(d.damping), np.float32))
+                ab = np.asarray(d.coords, np.float32)[d.connectivity[:, 0]] - np.asarray(d.coords, np.float32)[d.connectivity[:, 1]]
+                rhos.append(np.array([np.linalg.norm(r) for r in ab], dtype=np.float32))  # rest lengths
+                sys_.append(np.zeros(ne, np.float32))
+                Hs.append(np.zeros(ne, np.float32))
+                bn = np.arange(nn, dtype=np.int64) + off
+                bn_off.append(sum(len(x) for x in bnodes))
+                bn_cnt.append(len(bn))
+                bnodes.append(bn)
+                spring_mass.append((len(self.node_ranges), float(np.float32(d.mass))))
+                self.node_ranges.append((off, nn))
+                off += nn
+                continue
             m = d.mesh
             nn = m.numNodes
             c = np.asarray(m.coords, dtype=np.float32)[:, :2]
@@ -221,25 +269,7 @@ class OracleLoop:
             v = np.zeros((nn, 2), np.float32)
             bits = np.zeros(nn, np.int64)
             vals = np.zeros((nn, 2), np.float32)
-            for bc in d.bcs:
-                t, nodes, values = bc.processData()
-                if values is None:
-                    values = [0.0] * d.d
-                if nodes is None:
-                    nodes = range(nn)
-                for idx in nodes:
-                    nd = int(idx)
-                    bits[nd] |= int(t)
-                    vals[nd, 0] = float(values[0])
-                    vals[nd, 1] = float(values[1])
-            for ic in d.initials:
-                vx, vy = float(ic.vel[0]), float(ic.vel[1])
-                if getattr(ic, "is_all_nodes", False):
-                    v[:, 0] = vx
-                    v[:, 1] = vy
-                else:
-                    for nid in np.asarray(ic.nds):
-                        v[int(nid)] = (vx, vy)
+            self._conditions(d, nn, v, bits, vals)
             vs.append(v)
             bcs.append(bits)
             bcv.append(vals)
@@ -270,12 +300,14 @@ class OracleLoop:
                               k[7][1], k[8][1], k[9][1], k[10][1], len(fem), k[11][1], k[12][1], len(k[13][0]),
                               k[13][1])
         L.or_set_threads(self._w, int(threads))
+        for body, mass in spring_mass:
+            L.or_set_spring_mass(self._w, body, mass)
         # --- work lists in launch order (mixedcontact.py:1794-2261)
         anal = [c for c in contacts if c[0] == FLEXANLAYTICAL]
         hf = [c for c in contacts if c[0] == FEXHEIGHTFIELD]
         vox = [c for c in contacts if c[0] == FLEXVOXELMAP]
         flex = [c for c in contacts if c[0] == FLEXFLEX]
-        unbatched = 0
+        unbatched = sum(1 for c in contacts if c[0] == FLEXSPRING)
         if len({id(c[2]) for c in hf}) > 1:
             unbatched += len(hf)
             hf = []
@@ -304,15 +336,16 @@ class OracleLoop:
             # boundary edges per fem domain, global node ids, mesh order
             edges, be_off, be_cnt = [], [], []
             for d, (n0, _) in zip(fem, self.node_ranges):
-                e = boundary_edges_literal(d.mesh.connectivity) + n0
+                e = (boundary_edges_literal(d.mesh.connectivity) + n0 if d.type == FEM
+                     else np.zeros((0, 2), np.int64))
                 be_off.append(sum(len(x) for x in edges))
                 be_cnt.append(len(e))
                 edges.append(e)
             dom_obj = [1 if d.considerContact else 0 for d in domains]
-            dom_body = [fem.index(d) if d.type == FEM else -1 for d in domains]
+            dom_body = [fem.index(d) if d.type in (FEM, SPRINGMASS) else -1 for d in domains]
             dom_box = np.zeros((len(domains), 4), np.float32)
             for i, d in enumerate(domains):
-                if d.type != FEM and d.considerContact:
+                if d.type not in (FEM, SPRINGMASS) and d.considerContact:
                     lo, hi = self._ground_box(d)
                     dom_box[i, :2] = lo[0]
                     dom_box[i, 2:] = hi[0]
@@ -333,6 +366,30 @@ class OracleLoop:
             L.or_mass_scaling(self._w, float(np.float32(mass_scaling_dt)))
         if flex:  # explicitloop.py:383-385: initial FEM spatial hash
             L.or_flex_rebuild(self._w)
+
+    @staticmethod
+    def _conditions(d, nn, v, bits, vals):
+        """processConditions (femspringmanager.py:660-705) and initial velocities
+        (initialconditions.py:31-50) of one body, loop for loop."""
+        for bc in d.bcs:
+            t, nodes, values = bc.processData()
+            if values is None:
+                values = [0.0] * d.d
+            if nodes is None:
+                nodes = range(nn)
+            for idx in nodes:
+                nd = int(idx)
+                bits[nd] |= int(t)
+                vals[nd, 0] = float(values[0])
+                vals[nd, 1] = float(values[1])
+        for ic in d.initials:
+            vx, vy = float(ic.vel[0]), float(ic.vel[1])
+            if getattr(ic, "is_all_nodes", False):
+                v[:, 0] = vx
+                v[:, 1] = vy
+            else:
+                for nid in np.asarray(ic.nds):
+                    v[int(nid)] = (vx, vy)
 
     @staticmethod
     def _seg_penalty(dom):
