@@ -45,6 +45,10 @@ class BatchedLoop:
         self.layouts = [SceneLayout(d, dt=a, damping=c, useAdapativeDT=b)
                         for d, a, b, c in zip(scenes, dts, ada, damp)]
         self.packed = PackedWorld(self.layouts)
+        if path == "stream" and self.packed.spring_bodies:
+            path = "gather"  # the patch-streaming step covers triangles only
+        if any(lay.flex for lay in self.layouts):
+            raise NotImplementedError("FEM-FEM contact runs in single-scene loops (ExplicitLoop) only")
         self._native = build_native(self.packed, device=device, path=path)
         self.path = path
         if block_elems or block_nodes:
