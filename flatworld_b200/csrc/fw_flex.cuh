@@ -35,8 +35,9 @@ constexpr int kFlexScanThreads = 1024;
 
 struct FlexGrid {
   int tc, cnx, cny, npairs;
-  int simple;  // every element sits in every cell of its box (no cell cap, no pair truncation)
-  int pad2[3];
+  int simple;    // every element sits in every cell of its box (no cell cap, no pair truncation)
+  int n_active;  // work items of active (pair, side) segments this substep
+  int pad2[2];
   float olx, oly, gsx, gsy;
   int estimate;  // ordered-int minimum of the element box diagonals
   int rebuild;   // this substep rebuilds the hash
@@ -79,6 +80,9 @@ struct FlexDev {
   int2* ecell;   // per element: its lowest cell (ix, iy), clamped to the grid
   int4* srec;    // per cell entry (cell order): element, its domain, its two nodes
   int2* scell;   // per cell entry: the element's lowest cell
+  int n_seg;            // (pair, side) segments of consecutive work items
+  const int4* seg;      // per segment: first item, item count, pair, target body
+  int32_t* seg_off;     // [n_seg + 1]: exclusive scan of the active segments' item counts
 };
 
 // wp.min / wp.max on floats: a < b ? a : b (first argument on ties)
@@ -113,6 +117,33 @@ __device__ __forceinline__ int flex_cell(float delta, float gs, int n) {
   return c;
 }
 
+// Exclusive scan of n ints (one CTA of kFlexScanThreads); returns the total.
+// Each thread scans a contiguous chunk, the chunk sums are scanned in shared
+// memory.
+__device__ int flex_block_scan(const int32_t* in, int32_t* out, int n) {
+  __shared__ int part[kFlexScanThreads];
+  const int t = threadIdx.x;
+  const int chunk = (n + kFlexScanThreads - 1) / kFlexScanThreads;
+  const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
+  int sum = 0;
+  for (int i = lo; i < hi; ++i) sum += in[i];
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < kFlexScanThreads; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int i = lo; i < hi; ++i) {
+    const int v = in[i];
+    out[i] = run;
+    run += v;
+  }
+  return part[kFlexScanThreads - 1];
+}
+
 // Per substep, before k_elements: scene mode, hash clock, pair activation
 // and the broad-phase domain stamps.  force != 0: the construction-time build
 // (explicitloop.py:383-385) -- rebuild, no contact.  Dynamic shared memory:
@@ -133,6 +164,7 @@ __global__ void k_flex_pre(Dev d, FlexDev f, int force) {
     }
     f.g->rebuild = rb;
     if (rb) f.g->estimate = fw::f2ord(1e30f);
+    if (!step) f.g->n_active = 0;
   }
   if (!step) return;
   const int k = d.scene_counter[s];
@@ -162,6 +194,21 @@ __global__ void k_flex_pre(Dev d, FlexDev f, int force) {
       }
     }
     if (lane == 0) f.stamped[gi] = st ? 1 : 0;
+  }
+  __syncthreads();
+  // the work items that run: the (pair, side) segments whose pair is active
+  // and whose target is stamped (or every one when the loop has no BVH),
+  // compacted so the contact kernel visits nothing else
+  for (int q = threadIdx.x; q < f.n_seg; q += blockDim.x) {
+    const int4 sg = f.seg[q];
+    const bool on = f.pair_active[sg.z] && (f.skip_bvh || f.stamped[sg.w]);
+    f.seg_off[q] = on ? sg.y : 0;
+  }
+  __syncthreads();
+  const int total = flex_block_scan(f.seg_off, f.seg_off, f.n_seg);
+  if (threadIdx.x == 0) {
+    f.seg_off[f.n_seg] = total;
+    f.g->n_active = total;
   }
 }
 
@@ -239,33 +286,6 @@ __global__ void k_flex_count(FlexDev f) {
         if (ix + iy * g.cnx < g.tc) ++n;
     f.ecount[e] = n;
   }
-}
-
-// Exclusive scan of n ints (one CTA of kFlexScanThreads); returns the total.
-// Each thread scans a contiguous chunk, the chunk sums are scanned in shared
-// memory.
-__device__ int flex_block_scan(const int32_t* in, int32_t* out, int n) {
-  __shared__ int part[kFlexScanThreads];
-  const int t = threadIdx.x;
-  const int chunk = (n + kFlexScanThreads - 1) / kFlexScanThreads;
-  const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
-  int sum = 0;
-  for (int i = lo; i < hi; ++i) sum += in[i];
-  part[t] = sum;
-  __syncthreads();
-  for (int o = 1; o < kFlexScanThreads; o <<= 1) {
-    const int v = t >= o ? part[t - o] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
-  }
-  int run = part[t] - sum;
-  for (int i = lo; i < hi; ++i) {
-    const int v = in[i];
-    out[i] = run;
-    run += v;
-  }
-  return part[kFlexScanThreads - 1];
 }
 
 // Pair index of each element's first (cell, element) pair: the order of
@@ -419,15 +439,8 @@ struct FlexBest {
   int e, n0, n1;
 };
 
-__global__ void __launch_bounds__(kFlexContactThreads) k_flex_contact(Dev d, FlexDev f) {
-  const int it = (blockIdx.x * blockDim.x + threadIdx.x) / kFlexLanes;
-  const int sub = threadIdx.x % kFlexLanes;
-  const unsigned gmask = ((1u << kFlexLanes) - 1u) << ((threadIdx.x & 31) & ~(kFlexLanes - 1));
-  if (it >= f.n_items || !flex_stepping(d, f.scene)) return;  // uniform within the group
-  if (!f.pair_active[f.item_pair[it]]) return;
-  const int target = f.item_target[it];
-  if (!f.skip_bvh && !f.stamped[target]) return;
-  const FlexGrid g = *f.g;
+__device__ __forceinline__ void flex_item(const Dev& d, const FlexDev& f, const FlexGrid& g, int it, int target,
+                                          int sub, unsigned gmask) {
   const int nid = f.item_node[it];
   const int be_off = f.be_off[target], be_cnt = f.be_cnt[target];
   const float2 p = d.x[nid], vp = d.v[nid];
@@ -557,6 +570,26 @@ __global__ void __launch_bounds__(kFlexContactThreads) k_flex_contact(Dev d, Fle
     flex_push(d, f.g, nid, it, make_float2(tx, ty));
     flex_push(d, f.g, bn0, it, make_float2(-(tx * bw0), -(ty * bw0)));
     flex_push(d, f.g, bn1, it, make_float2(-(tx * bw1), -(ty * bw1)));
+  }
+}
+
+// Each group of kFlexLanes lanes takes active work items in turn (grid
+// stride over the compacted list): the item's segment by binary search over
+// the segment offsets, then flex_item.
+__global__ void __launch_bounds__(kFlexContactThreads) k_flex_contact(Dev d, FlexDev f) {
+  const int sub = threadIdx.x % kFlexLanes;
+  const unsigned gmask = ((1u << kFlexLanes) - 1u) << ((threadIdx.x & 31) & ~(kFlexLanes - 1));
+  const FlexGrid g = *f.g;
+  const int groups = gridDim.x * (blockDim.x / kFlexLanes);
+  for (int a = blockIdx.x * (blockDim.x / kFlexLanes) + threadIdx.x / kFlexLanes; a < g.n_active; a += groups) {
+    int lo = 0, hi = f.n_seg - 1;  // the last segment whose offset is <= a (the active one of a run)
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (f.seg_off[mid] <= a) lo = mid;
+      else hi = mid - 1;
+    }
+    const int4 sg = f.seg[lo];
+    flex_item(d, f, g, sg.x + (a - f.seg_off[lo]), sg.w, sub, gmask);
   }
 }
 

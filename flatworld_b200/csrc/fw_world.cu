@@ -969,7 +969,7 @@ void flex_launch(fw_ctx* c, int force) {
   const FlexDev& f = c->fx;
   const int eb = (f.n_be + kBlock - 1) / kBlock;
   const int wide = 2 * c->sms;
-  k_flex_pre<<<1, 512, c->flex_pre_smem, c->stream>>>(c->d, f, force);
+  k_flex_pre<<<1, kFlexScanThreads, c->flex_pre_smem, c->stream>>>(c->d, f, force);
   k_flex_boxes<<<eb, kBlock, 0, c->stream>>>(c->d, f);
   k_flex_grid<<<1, 32, 0, c->stream>>>(c->d, f);
   k_flex_count<<<wide, kBlock, 0, c->stream>>>(f);
@@ -981,8 +981,8 @@ void flex_launch(fw_ctx* c, int force) {
   c->launches += 9;
   if (!force) {
     const int64_t threads = (int64_t)f.n_items * kFlexLanes;
-    k_flex_contact<<<(int)((threads + kFlexContactThreads - 1) / kFlexContactThreads), kFlexContactThreads, 0,
-                     c->stream>>>(c->d, f);
+    const int blocks = (int)std::min<int64_t>((threads + kFlexContactThreads - 1) / kFlexContactThreads, 8 * c->sms);
+    k_flex_contact<<<blocks, kFlexContactThreads, 0, c->stream>>>(c->d, f);
     c->launches += 1;
   }
 }
@@ -1881,6 +1881,7 @@ int build_flex(fw_ctx* c) {
   std::vector<int32_t> item_node, item_target, item_pair;
   std::vector<float> item_pen, item_fric;
   std::vector<int2> pair_body;
+  std::vector<int4> segs;  // (first item, count, pair, target)
   std::vector<int32_t> slot(N, -1);
   int n_slots = 0;
   for (size_t p = 0; p < c->h_flex.size(); ++p) {
@@ -1888,6 +1889,7 @@ int build_flex(fw_ctx* c) {
     pair_body.push_back(make_int2(fp.b1, fp.b2));
     for (int side = 0; side < 2; ++side) {
       const int src = side == 0 ? fp.b2 : fp.b1, dst = side == 0 ? fp.b1 : fp.b2;
+      segs.push_back(make_int4((int)item_node.size(), c->h_bncnt[src], (int)p, dst));
       for (int k = 0; k < c->h_bncnt[src]; ++k) {
         const int n = c->h_bnodes[c->h_bnoff[src] + k];
         item_node.push_back(n);
@@ -1922,7 +1924,8 @@ int build_flex(fw_ctx* c) {
           *ebase = nullptr, *ccount = nullptr, *cstart = nullptr, *cend = nullptr, *cursor = nullptr,
           *sorted = nullptr, *dslot = nullptr, *dcnt = nullptr, *ditem = nullptr;
   int2 *crange = nullptr, *ecell = nullptr, *scell = nullptr;
-  int4* srec = nullptr;
+  int4 *srec = nullptr, *dseg = nullptr;
+  int32_t* dsegoff = nullptr;
   float *ipen = nullptr, *ifric = nullptr;
   int2 *pbody = nullptr, *dbe = nullptr;
   float4 *dbox = nullptr, *ebox = nullptr;
@@ -1948,6 +1951,7 @@ int build_flex(fw_ctx* c) {
       (rc = dalloc(c, &cursor, kFlexMaxCells)) || (rc = dalloc(c, &sorted, f.max_pairs)) ||
       (rc = dalloc(c, &crange, kFlexMaxCells)) || (rc = dalloc(c, &ecell, n_be)) ||
       (rc = dalloc(c, &srec, f.max_pairs)) || (rc = dalloc(c, &scell, f.max_pairs)) ||
+      (rc = upload(c, &dseg, segs)) || (rc = dalloc(c, &dsegoff, segs.size() + 1)) ||
       (rc = upload(c, &dslot, slot)) || (rc = dalloc(c, &dcnt, std::max(1, n_slots))) ||
       (rc = dalloc(c, &ditem, std::max(1, n_slots) * kFlexListCap)) ||
       (rc = dalloc(c, &dforce, std::max(1, n_slots) * kFlexListCap)))
@@ -1963,6 +1967,7 @@ int build_flex(fw_ctx* c) {
   f.ebox = ebox; f.ecount = ecount; f.ebase = ebase; f.cell_count = ccount; f.cell_start = cstart;
   f.cell_end = cend; f.cursor = cursor; f.sorted = sorted; f.crange = crange; f.ecell = ecell;
   f.srec = srec; f.scell = scell;
+  f.n_seg = (int)segs.size(); f.seg = dseg; f.seg_off = dsegoff;
   c->flex_pre_smem = sizeof(float4) * (size_t)(std::max(n_dom, 1) + B);
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
