@@ -693,10 +693,10 @@ def run_flex(args, rank, world, local):
                    "step": "100 substeps", "l2": "working set smaller than L2 (small meshes)",
                    "host_build_s": build_s, "state_finite": finite, "replicas": world, "path": "gather"},
         "latency_ms_per_step": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99)},
-        "roofline": {"bound": "hbm", "kernel": "substep = FEM-FEM contact (10 kernels) + k_elements + k_nodes_flex",
+        "roofline": {"bound": "hbm", "kernel": "substep = k_flex_pre + k_flex_contact + k_elements + k_nodes_flex",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": which,
                      "algorithmic_bytes_per_substep": bstep, "traffic": None,
-                     "note": "latency-bound: a substep is 12 short dependent launches over a world of ~1 MB of state"},
+                     "note": "latency-bound: a substep is 4 dependent launches over a world of ~1 MB of state"},
         "e2e": {"value": work_e2e / (ms_e2e / 1e3), "unit": "element-steps/s",
                 "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
         "gpu_launches": launches, "clocks": clk.summary(),

@@ -123,6 +123,7 @@ __device__ __forceinline__ int flex_cell(float delta, float gs, int n) {
 __device__ int flex_block_scan(const int32_t* in, int32_t* out, int n) {
   __shared__ int part[kFlexScanThreads];
   const int t = threadIdx.x;
+  __syncthreads();  // a previous call's readers of part[] are done
   const int chunk = (n + kFlexScanThreads - 1) / kFlexScanThreads;
   const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
   int sum = 0;
@@ -144,12 +145,160 @@ __device__ int flex_block_scan(const int32_t* in, int32_t* out, int n) {
   return part[kFlexScanThreads - 1];
 }
 
-// Per substep, before k_elements: scene mode, hash clock, pair activation
-// and the broad-phase domain stamps.  force != 0: the construction-time build
-// (explicitloop.py:383-385) -- rebuild, no contact.  Dynamic shared memory:
-// (n_dom + n_fem) boxes -- every domain's, then every FEM body's.
-__global__ void k_flex_pre(Dev d, FlexDev f, int force) {
+__device__ __forceinline__ void flex_elem_cells(const FlexGrid& g, float4 eb, int& lx, int& ly, int& ux, int& uy) {
+  lx = flex_cell(eb.x - g.olx, g.gsx, g.cnx);
+  ly = flex_cell(eb.y - g.oly, g.gsy, g.cny);
+  ux = flex_cell(eb.z - g.olx, g.gsx, g.cnx);
+  uy = flex_cell(eb.w - g.oly, g.gsy, g.cny);
+}
+
+// The spatial-hash rebuild, by the whole block, phase after phase:
+// populate_fem_spatial_hash + SpatialHashManager.build (femspringmanager.py:
+// 1041-1063; spatialmanager.py:200-420, 613-712).  Registration index =
+// boundary-edge index.  The (cell, element) pairs get the pair indices of
+// _expand_pairs_kernel's counter in launch order (a scan of the per-element
+// counts), so the reference's MAX_PAIRS truncation is reproduced; cells are
+// filled with atomics and then sorted, giving each cell its elements in
+// registration order.
+__device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
+  const int t = threadIdx.x, T = blockDim.x;
+  // add_element for every boundary edge
+  for (int e = t; e < f.n_be; e += T) {
+    const int2 n = f.be[e];
+    const float2 a = d.x[n.x], b = d.x[n.y];
+    float lx = 1e30f, ly = 1e30f, ux = -1e30f, uy = -1e30f;
+    lx = wmin(lx, a.x); ly = wmin(ly, a.y); ux = wmax(ux, a.x); uy = wmax(uy, a.y);
+    lx = wmin(lx, b.x); ly = wmin(ly, b.y); ux = wmax(ux, b.x); uy = wmax(uy, b.y);
+    const float4 bb = make_float4(lx - 0.0f, ly - 0.0f, ux + 0.0f, uy + 0.0f);
+    f.ebox[e] = bb;
+    const float dx = bb.z - bb.x, dy = bb.w - bb.y;
+    atomicMin(&f.g->estimate, fw::f2ord(sqrtf(dx * dx + dy * dy)));
+  }
+  __syncthreads();
+  // the global box of the FEM domains (populate kernel) and _build_grid_kernel
+  if (t == 0) {
+    const int slot = d.scene_counter[f.scene] & 1;
+    float glx = 1e9f, gly = 1e9f, gux = -1e9f, guy = -1e9f;
+    for (int k = 0; k < f.n_fem; ++k) {
+      const float4 bb = ring_box(d, slot, f.body0 + k);
+      glx = wmin(glx, bb.x);
+      gly = wmin(gly, bb.y);
+      gux = wmax(gux, bb.z);
+      guy = wmax(guy, bb.w);
+    }
+    const float extent = wmax(gux - glx, guy - gly);
+    const float expand = extent * 0.01f + 0.0f;
+    glx = glx - expand;
+    gly = gly - expand;
+    gux = gux + expand;
+    guy = guy + expand;
+    float cell = fw::ord2f(f.g->estimate) * 1.5f;
+    const float exx = gux - glx, exy = guy - gly;
+    cell = wmax(cell, exx / f.mpd);
+    cell = wmax(cell, exy / f.mpd);
+    const float cs = cell + 1e-6f;
+    const int nx = (int)wmax(ceilf(exx / cs), 1.0f);
+    const int ny = (int)wmax(ceilf(exy / cs), 1.0f);
+    FlexGrid* g = f.g;
+    g->olx = glx;
+    g->oly = gly;
+    g->cnx = nx;
+    g->cny = ny;
+    g->gsx = exx / (float)nx;
+    g->gsy = exy / (float)ny;
+    const int total = nx * ny;
+    g->tc = total < kFlexMaxCells ? total : kFlexMaxCells;
+  }
+  __syncthreads();
+  FlexGrid g = *f.g;
+  // zero the cell counts; per element its lowest cell and how many pairs it makes
+  for (int c = t; c < g.tc; c += T) f.cell_count[c] = 0;
+  for (int e = t; e < f.n_be; e += T) {
+    int lx, ly, ux, uy, n = 0;
+    flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+    f.ecell[e] = make_int2(lx, ly);
+    for (int ix = lx; ix <= ux; ++ix)
+      for (int iy = ly; iy <= uy; ++iy)
+        if (ix + iy * g.cnx < g.tc) ++n;
+    f.ecount[e] = n;
+  }
+  __syncthreads();
+  const int npairs = flex_block_scan(f.ecount, f.ebase, f.n_be);
+  if (t == 0) {
+    f.g->npairs = npairs;
+    f.g->simple = (g.tc == g.cnx * g.cny && npairs <= f.max_pairs) ? 1 : 0;
+  }
+  __syncthreads();  // every chunk of ebase is written
+  // counts of the pairs kept (pair index < max_pairs)
+  for (int e = t; e < f.n_be; e += T) {
+    int lx, ly, ux, uy, p = f.ebase[e];
+    flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+    for (int ix = lx; ix <= ux; ++ix)
+      for (int iy = ly; iy <= uy; ++iy) {
+        const int cid = ix + iy * g.cnx;
+        if (cid < g.tc) {
+          if (p < f.max_pairs) atomicAdd(&f.cell_count[cid], 1);
+          ++p;
+        }
+      }
+  }
+  __syncthreads();
+  flex_block_scan(f.cell_count, f.cell_start, g.tc);
+  __syncthreads();
+  for (int c = t; c < g.tc; c += T) {
+    f.cursor[c] = f.cell_start[c];
+    f.cell_end[c] = f.cell_start[c] + f.cell_count[c];
+  }
+  __syncthreads();
+  for (int e = t; e < f.n_be; e += T) {
+    int lx, ly, ux, uy, p = f.ebase[e];
+    flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
+    for (int ix = lx; ix <= ux; ++ix)
+      for (int iy = ly; iy <= uy; ++iy) {
+        const int cid = ix + iy * g.cnx;
+        if (cid < g.tc) {
+          if (p < f.max_pairs) f.sorted[atomicAdd(&f.cursor[cid], 1)] = e;
+          ++p;
+        }
+      }
+  }
+  __syncthreads();
+  const bool simple = f.g->simple != 0;
+  // registration order inside every cell (insertion sort; cells hold few
+  // elements), then what the contact walk reads of each entry
+  for (int c = t; c < g.tc; c += T) {
+    const int lo = f.cell_start[c], hi = f.cell_end[c];
+    for (int i = lo + 1; i < hi; ++i) {
+      const int v = f.sorted[i];
+      int j = i - 1;
+      while (j >= lo && f.sorted[j] > v) {
+        f.sorted[j + 1] = f.sorted[j];
+        --j;
+      }
+      f.sorted[j + 1] = v;
+    }
+    if (simple) {  // then tc = cnx * cny <= kFlexMaxCells: the column index is in range
+      f.crange[(c % g.cnx) * g.cny + c / g.cnx] = make_int2(lo, hi);
+      for (int i = lo; i < hi; ++i) {
+        const int e = f.sorted[i];
+        const int2 n = f.be[e];
+        f.srec[i] = make_int4(e, f.be_dom[e], n.x, n.y);
+        f.scell[i] = f.ecell[e];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Per substep, before k_elements, one block: the hash clock and, when it
+// fires, the rebuild (flex_rebuild); pair activation, the broad-phase domain
+// stamps, and the compacted list of work items that run.  force != 0: the
+// construction-time build (explicitloop.py:383-385) -- rebuild, no contact.
+// Dynamic shared memory: (n_dom + n_fem) boxes -- every domain's, then every
+// FEM body's.
+__global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f, int force) {
   extern __shared__ float4 sbox[];
+  __shared__ int s_rebuild;
   const int s = f.scene;
   const bool step = !force && flex_stepping(d, s);
   if (threadIdx.x == 0) {
@@ -165,7 +314,10 @@ __global__ void k_flex_pre(Dev d, FlexDev f, int force) {
     f.g->rebuild = rb;
     if (rb) f.g->estimate = fw::f2ord(1e30f);
     if (!step) f.g->n_active = 0;
+    s_rebuild = rb;
   }
+  __syncthreads();
+  if (s_rebuild) flex_rebuild(d, f);
   if (!step) return;
   const int k = d.scene_counter[s];
   const int slot = k & 1;
@@ -209,167 +361,6 @@ __global__ void k_flex_pre(Dev d, FlexDev f, int force) {
   if (threadIdx.x == 0) {
     f.seg_off[f.n_seg] = total;
     f.g->n_active = total;
-  }
-}
-
-// add_element for every boundary edge (registration index = edge index).
-__global__ void k_flex_boxes(Dev d, FlexDev f) {
-  if (!f.g->rebuild) return;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= f.n_be) return;
-  const int2 n = f.be[e];
-  const float2 a = d.x[n.x], b = d.x[n.y];
-  float lx = 1e30f, ly = 1e30f, ux = -1e30f, uy = -1e30f;
-  lx = wmin(lx, a.x); ly = wmin(ly, a.y); ux = wmax(ux, a.x); uy = wmax(uy, a.y);
-  lx = wmin(lx, b.x); ly = wmin(ly, b.y); ux = wmax(ux, b.x); uy = wmax(uy, b.y);
-  const float4 bb = make_float4(lx - 0.0f, ly - 0.0f, ux + 0.0f, uy + 0.0f);
-  f.ebox[e] = bb;
-  const float dx = bb.z - bb.x, dy = bb.w - bb.y;
-  atomicMin(&f.g->estimate, fw::f2ord(sqrtf(dx * dx + dy * dy)));
-}
-
-// The global box of the FEM domains (populate kernel) and _build_grid_kernel.
-__global__ void k_flex_grid(Dev d, FlexDev f) {
-  if (!f.g->rebuild || threadIdx.x != 0) return;
-  const int slot = d.scene_counter[f.scene] & 1;
-  float glx = 1e9f, gly = 1e9f, gux = -1e9f, guy = -1e9f;
-  for (int k = 0; k < f.n_fem; ++k) {
-    const float4 bb = ring_box(d, slot, f.body0 + k);
-    glx = wmin(glx, bb.x);
-    gly = wmin(gly, bb.y);
-    gux = wmax(gux, bb.z);
-    guy = wmax(guy, bb.w);
-  }
-  const float extent = wmax(gux - glx, guy - gly);
-  const float expand = extent * 0.01f + 0.0f;
-  glx = glx - expand;
-  gly = gly - expand;
-  gux = gux + expand;
-  guy = guy + expand;
-  float cell = fw::ord2f(f.g->estimate) * 1.5f;
-  const float exx = gux - glx, exy = guy - gly;
-  cell = wmax(cell, exx / f.mpd);
-  cell = wmax(cell, exy / f.mpd);
-  const float cs = cell + 1e-6f;
-  const int nx = (int)wmax(ceilf(exx / cs), 1.0f);
-  const int ny = (int)wmax(ceilf(exy / cs), 1.0f);
-  FlexGrid* g = f.g;
-  g->olx = glx;
-  g->oly = gly;
-  g->cnx = nx;
-  g->cny = ny;
-  g->gsx = exx / (float)nx;
-  g->gsy = exy / (float)ny;
-  const int total = nx * ny;
-  g->tc = total < kFlexMaxCells ? total : kFlexMaxCells;
-}
-
-__device__ __forceinline__ void flex_elem_cells(const FlexGrid& g, float4 eb, int& lx, int& ly, int& ux, int& uy) {
-  lx = flex_cell(eb.x - g.olx, g.gsx, g.cnx);
-  ly = flex_cell(eb.y - g.oly, g.gsy, g.cny);
-  ux = flex_cell(eb.z - g.olx, g.gsx, g.cnx);
-  uy = flex_cell(eb.w - g.oly, g.gsy, g.cny);
-}
-
-// Zero the cell counts; per element, how many (cell, element) pairs it makes.
-__global__ void k_flex_count(FlexDev f) {
-  if (!f.g->rebuild) return;
-  const FlexGrid g = *f.g;
-  const int stride = gridDim.x * blockDim.x;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.tc; c += stride) f.cell_count[c] = 0;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.n_be; e += stride) {
-    int lx, ly, ux, uy, n = 0;
-    flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
-    f.ecell[e] = make_int2(lx, ly);
-    for (int ix = lx; ix <= ux; ++ix)
-      for (int iy = ly; iy <= uy; ++iy)
-        if (ix + iy * g.cnx < g.tc) ++n;
-    f.ecount[e] = n;
-  }
-}
-
-// Pair index of each element's first (cell, element) pair: the order of
-// _expand_pairs_kernel's atomic counter in launch order.
-__global__ void __launch_bounds__(kFlexScanThreads) k_flex_scan_elems(FlexDev f) {
-  if (!f.g->rebuild) return;
-  const int total = flex_block_scan(f.ecount, f.ebase, f.n_be);
-  if (threadIdx.x == 0) {
-    f.g->npairs = total;
-    f.g->simple = (f.g->tc == f.g->cnx * f.g->cny && total <= f.max_pairs) ? 1 : 0;
-  }
-}
-
-// Cell counts of the pairs kept (pair index < max_pairs).
-__global__ void k_flex_cells(FlexDev f) {
-  if (!f.g->rebuild) return;
-  const FlexGrid g = *f.g;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= f.n_be) return;
-  int lx, ly, ux, uy, p = f.ebase[e];
-  flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
-  for (int ix = lx; ix <= ux; ++ix)
-    for (int iy = ly; iy <= uy; ++iy) {
-      const int cid = ix + iy * g.cnx;
-      if (cid < g.tc) {
-        if (p < f.max_pairs) atomicAdd(&f.cell_count[cid], 1);
-        ++p;
-      }
-    }
-}
-
-__global__ void __launch_bounds__(kFlexScanThreads) k_flex_scan_cells(FlexDev f) {
-  if (!f.g->rebuild) return;
-  const int tc = f.g->tc;
-  flex_block_scan(f.cell_count, f.cell_start, tc);
-  __syncthreads();
-  for (int c = threadIdx.x; c < tc; c += blockDim.x) {
-    f.cursor[c] = f.cell_start[c];
-    f.cell_end[c] = f.cell_start[c] + f.cell_count[c];
-  }
-}
-
-__global__ void k_flex_fill(FlexDev f) {
-  if (!f.g->rebuild) return;
-  const FlexGrid g = *f.g;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= f.n_be) return;
-  int lx, ly, ux, uy, p = f.ebase[e];
-  flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
-  for (int ix = lx; ix <= ux; ++ix)
-    for (int iy = ly; iy <= uy; ++iy) {
-      const int cid = ix + iy * g.cnx;
-      if (cid < g.tc) {
-        if (p < f.max_pairs) f.sorted[atomicAdd(&f.cursor[cid], 1)] = e;
-        ++p;
-      }
-    }
-}
-
-// Registration order inside every cell (insertion sort; cells hold few elements).
-__global__ void k_flex_sort(FlexDev f) {
-  if (!f.g->rebuild) return;
-  const int tc = f.g->tc;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < tc; c += gridDim.x * blockDim.x) {
-    const int lo = f.cell_start[c], hi = f.cell_end[c];
-    for (int i = lo + 1; i < hi; ++i) {
-      const int v = f.sorted[i];
-      int j = i - 1;
-      while (j >= lo && f.sorted[j] > v) {
-        f.sorted[j + 1] = f.sorted[j];
-        --j;
-      }
-      f.sorted[j + 1] = v;
-    }
-    if (f.g->simple) {  // then tc = cnx * cny <= kFlexMaxCells: the column index is in range
-      const int cnx = f.g->cnx, cny = f.g->cny;
-      f.crange[(c % cnx) * cny + c / cnx] = make_int2(lo, hi);
-      for (int i = lo; i < hi; ++i) {  // what the contact walk reads of each entry, in entry order
-        const int e = f.sorted[i];
-        const int2 n = f.be[e];
-        f.srec[i] = make_int4(e, f.be_dom[e], n.x, n.y);
-        f.scell[i] = f.ecell[e];
-      }
-    }
   }
 }
 

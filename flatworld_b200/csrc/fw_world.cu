@@ -963,22 +963,12 @@ void set_grids(fw_ctx* c) {
 }
 
 // The FEM-FEM contact of one substep (force: the construction-time hash
-// build only): activation and hash clock, the hash rebuild (each kernel
-// returns at once unless the clock fired), the contact work items.
+// build only): k_flex_pre (hash clock, the rebuild when it fires, activation,
+// the active work items), then the contact work items.
 void flex_launch(fw_ctx* c, int force) {
   const FlexDev& f = c->fx;
-  const int eb = (f.n_be + kBlock - 1) / kBlock;
-  const int wide = 2 * c->sms;
   k_flex_pre<<<1, kFlexScanThreads, c->flex_pre_smem, c->stream>>>(c->d, f, force);
-  k_flex_boxes<<<eb, kBlock, 0, c->stream>>>(c->d, f);
-  k_flex_grid<<<1, 32, 0, c->stream>>>(c->d, f);
-  k_flex_count<<<wide, kBlock, 0, c->stream>>>(f);
-  k_flex_scan_elems<<<1, kFlexScanThreads, 0, c->stream>>>(f);
-  k_flex_cells<<<eb, kBlock, 0, c->stream>>>(f);
-  k_flex_scan_cells<<<1, kFlexScanThreads, 0, c->stream>>>(f);
-  k_flex_fill<<<eb, kBlock, 0, c->stream>>>(f);
-  k_flex_sort<<<wide, kBlock, 0, c->stream>>>(f);
-  c->launches += 9;
+  c->launches += 1;
   if (!force) {
     const int64_t threads = (int64_t)f.n_items * kFlexLanes;
     const int blocks = (int)std::min<int64_t>((threads + kFlexContactThreads - 1) / kFlexContactThreads, 8 * c->sms);
@@ -1074,7 +1064,7 @@ int run_steps(fw_ctx* c, int n) {
     if (rc) return rc;
     while (n >= kGraphSteps) {
       FW_CUDA(c, cudaGraphLaunch(g, c->stream));
-      c->launches += (c->has_flex ? 12 : 2) * kGraphSteps;
+      c->launches += (c->has_flex ? 4 : 2) * kGraphSteps;
       n -= kGraphSteps;
     }
   }
@@ -1082,7 +1072,7 @@ int run_steps(fw_ctx* c, int n) {
     cudaGraphExec_t g = nullptr;
     if ((rc = get_graph(c, n, &g))) return rc;
     FW_CUDA(c, cudaGraphLaunch(g, c->stream));
-    c->launches += (c->has_flex ? 12 : 2) * n;
+    c->launches += (c->has_flex ? 4 : 2) * n;
     n = 0;
   }
   for (int k = 0; k < n && rc == FW_OK; ++k) rc = launch_step(c);
