@@ -128,3 +128,19 @@ def test_gpu_mass_scaling_with_springs():
         o.advance_with_time(FRAME)
         xo, _, _ = o.state()
         assert np.array_equal(lp.femSpringManager.coords.numpy()[:n].astype(np.float64), xo), f
+
+
+@pytest.mark.gpu
+def test_gpu_batched_spring_scenes_equal_alone():
+    """A BatchedLoop of spring scenes steps on the gather path; each scene
+    equals the same scene stepped alone."""
+    from flatworld_b200.batch import BatchedLoop
+
+    builds = [bcs_scene, lambda: grid_scene(20), mixed_scene]
+    b = BatchedLoop([f() for f in builds], dt=2e-4, useAdapativeDT=False)
+    b.advance(150)
+    for s, f in enumerate(builds):
+        lp = fw.ExplicitLoop(2e-4, f(), useAdapativeDT=False)
+        lp.advance_n(150)
+        n = len(b.coords(s))
+        assert np.array_equal(b.coords(s), lp.femSpringManager.coords.numpy()[:n]), s
