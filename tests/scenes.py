@@ -276,3 +276,14 @@ def flex_pile(fw, cols=8, rows=8, cells=16, radius=0.025, gap=0.01, E=1e5, rho=1
             mesh = ccw_disk(fw, cells, radius, (radius + c * pitch + 0.002 * (r % 2), radius + 0.002 + r * pitch))
             doms.append(fw.FemDomain(mesh, fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])], friction=0.2))
     return doms
+
+
+def flex_stamp_quirk(fw):
+    """A ground plane far below (never in a broad-phase pair) as domain 0, then
+    two circles pulled together (tests/scenes.flex_circles).  The reference
+    reads the broad-phase stamp of the FEM-FEM item's target at its FEM-local
+    index (mixedcontact.py:925) in an array indexed by global domain index
+    (explicitloop.py:451-463): items targeting the first circle (FEM-local 0)
+    read the far plane's stamp and never run; items targeting the second read
+    the first circle's and do."""
+    return [fw.GroundDomain(2, [0.0, -5.0], [0.0, 1.0])] + flex_circles(fw)

@@ -71,6 +71,22 @@ def test_oracle_circles_no_deep_penetration():
     assert worst < 0.005, worst
 
 
+def test_oracle_stamp_quirk_one_sided():
+    """With the far plane as domain 0, only the items whose target is the second
+    circle (FEM-local 1) ever find an edge."""
+    doms = scenes.flex_stamp_quirk(fw)
+    o = oracle.OracleLoop(doms, useAdapativeDT=True)
+    n_b = len(oracle.scene.boundary_nodes_literal(doms[2].mesh.connectivity))
+    hit = np.zeros(len(o.flex_cache()), bool)
+    for f in range(10):
+        o.advance_with_time(FRAME)
+        hit |= o.flex_cache() >= 0
+    # pair (domain1 = second circle, domain2 = first): items 0..n_b-1 are the first
+    # circle's nodes against the second's edges (target FEM-local 1), the rest target FEM-local 0
+    n_a = len(hit) - n_b
+    assert hit[:n_a].any() and not hit[n_a:].any()
+
+
 def test_layout_matches_oracle():
     """Stable dt, pair order, penalty and friction of the host layout equal the
     oracle's literal restatement."""
@@ -84,9 +100,9 @@ def test_layout_matches_oracle():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,frames", [("circles", 24), ("stack", 40)])
+@pytest.mark.parametrize("name,frames", [("circles", 24), ("stack", 40), ("stamp-quirk", 16)])
 def test_gpu_equals_oracle_frames(name, frames):
-    build = {"circles": scenes.flex_circles, "stack": scenes.flex_stack}[name]
+    build = {"circles": scenes.flex_circles, "stack": scenes.flex_stack, "stamp-quirk": scenes.flex_stamp_quirk}[name]
     lp = fw.ExplicitLoop(0.0, build(fw), useAdapativeDT=True)
     assert lp.path == 1  # FEM-FEM contact runs on the gather path
     o = oracle.OracleLoop(build(fw), useAdapativeDT=True)
@@ -102,6 +118,8 @@ def test_gpu_equals_oracle_frames(name, frames):
         assert np.array_equal(v, vo), (name, f)
         touched |= bool((o.flex_cache() >= 0).any())
     assert touched
+    cache, _ = lp._native.read_flex_state(len(o.flex_cache()))
+    assert np.array_equal(cache, o.flex_cache())  # every work item's edge cache, too
 
 
 @pytest.mark.gpu
