@@ -56,6 +56,7 @@ _SIGNATURES = {
     "fw_set_flex_scene": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f32p]),
     "fw_add_flex_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float]),
     "fw_set_flex_clock": (C.c_int, [_vp, C.c_double]),
+    "fw_set_flex_clocks": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "fw_mass_scaling": (C.c_int, [_vp, C.c_float]),
     "fw_set_spring_bodies": (C.c_int, [_vp, C.c_int32, _i32p, _f32p]),
     "fw_read_flex_state": (C.c_int, [_vp, _i32p, C.c_int32, _f32p]),
@@ -233,6 +234,12 @@ class NativeWorld:
 
     def mass_scaling(self, dt_target: float):
         self._check(self._L.fw_mass_scaling(self._h, float(dt_target)), "fw_mass_scaling")
+
+    def set_flex_clocks(self, dt):
+        """Per scene: the substep dt in float64 (FEM-FEM hash clock)."""
+        a = np.ascontiguousarray(dt, dtype=np.float64)
+        self._check(self._L.fw_set_flex_clocks(self._h, a.ctypes.data_as(C.POINTER(C.c_double))),
+                    "fw_set_flex_clocks")
 
     def set_flex_clock(self, dt: float):
         self._check(self._L.fw_set_flex_clock(self._h, float(dt)), "fw_set_flex_clock")

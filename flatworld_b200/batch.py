@@ -45,10 +45,9 @@ class BatchedLoop:
         self.layouts = [SceneLayout(d, dt=a, damping=c, useAdapativeDT=b)
                         for d, a, b, c in zip(scenes, dts, ada, damp)]
         self.packed = PackedWorld(self.layouts)
-        if path == "stream" and self.packed.spring_bodies:
-            path = "gather"  # the patch-streaming step covers triangles only
-        if any(lay.flex for lay in self.layouts):
-            raise NotImplementedError("FEM-FEM contact runs in single-scene loops (ExplicitLoop) only")
+        self._has_flex = any(lay.flex for lay in self.layouts)
+        if path == "stream" and (self.packed.spring_bodies or self._has_flex):
+            path = "gather"  # the patch-streaming step covers triangles without FEM-FEM contact
         self._native = build_native(self.packed, device=device, path=path)
         self.path = path
         if block_elems or block_nodes:
@@ -87,8 +86,15 @@ class BatchedLoop:
             self._native.set_active(active)
             self._active = active.copy()
 
+    def _clocks(self, dt):
+        """The FEM-FEM hash clocks accumulate each scene's float64 dt
+        (femspringmanager.py:1035-1039)."""
+        if self._has_flex:
+            self._native.set_flex_clocks(np.asarray(dt, np.float64))
+
     def advance(self, n: int = 1):
         """n substeps of every active scene, each with its own dt."""
+        self._clocks(self.dt)
         d32 = self.dt.astype(np.float32)
         if np.all(d32 == d32[0]):
             self._native.step(int(n), float(d32[0]))
@@ -110,12 +116,15 @@ class BatchedLoop:
             if not live:
                 break
             dts = np.zeros(self.S, dtype=np.float32)
+            dts64 = np.zeros(self.S, dtype=np.float64)
             act = np.zeros(self.S, dtype=np.int32)
             for s in live:
                 dts[s] = np.float32(runs[s][pos[s]][1])
+                dts64[s] = runs[s][pos[s]][1]
                 act[s] = 1
             n = min(left[s] for s in live)
             self._set_active(act)
+            self._clocks(dts64)
             self._native.step_scenes(n, dts)
             for s in live:
                 self.counters[s] += n

@@ -41,32 +41,49 @@ struct FlexGrid {
   float olx, oly, gsx, gsy;
   int estimate;  // ordered-int minimum of the element box diagonals
   int rebuild;   // this substep rebuilds the hash
-  int err;       // bit 0: a node's contribution list overflowed
-  int pad;
+  int pad[2];
   double elapsed;   // simulated time since the last rebuild (float64, as the host's float)
-  double clock_dt;  // the substep's dt as the host's float64 holds it
 };
 
+// One scene with FEM-FEM contact: where its part of every array starts.
+struct FlexScene {
+  int scene, body0, n_fem;       // the scene and its bodies (FEM-local index = body - body0)
+  int dom_off, n_dom, skip_bvh;  // its domains (dom_obj / dom_body / dom_box)
+  int pair_off, n_pairs;         // its ContactFlexFlex pairs
+  int seg_base, n_seg;           // its (pair, side) segments; seg_off holds n_seg + 1 entries at seg_base + k
+  int be0, n_be;                 // its boundary edges (registration order)
+  int max_pairs, pair_base;      // its (cell, element) pair capacity and slot base
+  int cell_base, pad;            // its cells: k * kFlexMaxCells
+};
+
+// The FEM-FEM state of a world; a kernel works on one scene's view of it
+// (flex_view): the scalars are that scene's, the per-scene pointers start at
+// its part.  Items, pairs' body ids, nodes, bodies and boundary edges keep
+// global indices.
 struct FlexDev {
-  int n_items, n_pairs, n_fem, n_dom, skip_bvh, n_be, body0, scene;
+  int n_items, n_fs;
+  int n_pairs, n_fem, n_dom, skip_bvh, n_be, be0, body0, scene;  // the view's scene
   int max_pairs;
   float mpd;  // max(pow(100000.0f, 0.5f), 1.0f), evaluated on the host
+  const FlexScene* sc;
+  const double* clock_dt;  // per FEM-FEM scene: its substep dt as the host's float64 holds it
+  int* err;                // bit 0: a node's contribution list overflowed
   const int32_t* item_node;
-  const int32_t* item_target;  // fem-local index of the body whose edges the item searches
+  const int32_t* item_target;  // the body whose edges the item searches
   const int32_t* item_pair;
   const float* item_pen;
   const float* item_fric;
   int32_t* item_cache;  // boundary edge hit last time, or -1
   const int2* pair_body;  // (domain1, domain2) global body ids
   const int2* be;         // per boundary edge: its two global node ids
-  const int32_t* be_dom;  // per boundary edge: fem-local domain
-  const int32_t* be_off;  // per fem-local domain
+  const int32_t* be_dom;  // per boundary edge: its body
+  const int32_t* be_off;  // per body: its first boundary edge
   const int32_t* be_cnt;
   const int32_t* dom_obj;   // per domain of the scene: a broad-phase object (considerContact)
   const int32_t* dom_body;  // per domain: global body id, or -1 for a ground
   const float4* dom_box;    // per domain: a ground's static box
   int32_t* pair_active;
-  int32_t* stamped;  // per fem-local index g: domain g is in a broad-phase pair this substep
+  int32_t* stamped;  // at body0 + g: the scene's domain g is in a broad-phase pair this substep
   FlexGrid* g;
   float4* ebox;
   int32_t* ecount;
@@ -78,12 +95,27 @@ struct FlexDev {
   int32_t* sorted;
   int2* crange;  // (start, end) of cell (ix, iy) at ix * cny + iy: a column is contiguous
   int2* ecell;   // per element: its lowest cell (ix, iy), clamped to the grid
-  int4* srec;    // per cell entry (cell order): element, its domain, its two nodes
+  int4* srec;    // per cell entry (cell order): element, its body, its two nodes
   int2* scell;   // per cell entry: the element's lowest cell
   int n_seg;            // (pair, side) segments of consecutive work items
-  const int4* seg;      // per segment: first item, item count, pair, target body
+  const int4* seg;      // per segment: first item, item count, pair (in the scene), target body
   int32_t* seg_off;     // [n_seg + 1]: exclusive scan of the active segments' item counts
 };
+
+__device__ __forceinline__ FlexDev flex_view(const FlexDev& f0, int k) {
+  const FlexScene c = f0.sc[k];
+  FlexDev f = f0;
+  f.scene = c.scene; f.body0 = c.body0; f.n_fem = c.n_fem; f.n_dom = c.n_dom; f.skip_bvh = c.skip_bvh;
+  f.n_pairs = c.n_pairs; f.n_seg = c.n_seg; f.be0 = c.be0; f.n_be = c.n_be; f.max_pairs = c.max_pairs;
+  f.dom_obj += c.dom_off; f.dom_body += c.dom_off; f.dom_box += c.dom_off;
+  f.pair_body += c.pair_off; f.pair_active += c.pair_off;
+  f.g += k;
+  f.cell_count += c.cell_base; f.cell_start += c.cell_base; f.cell_end += c.cell_base;
+  f.cursor += c.cell_base; f.crange += c.cell_base;
+  f.sorted += c.pair_base; f.srec += c.pair_base; f.scell += c.pair_base;
+  f.seg += c.seg_base; f.seg_off += c.seg_base + k;
+  return f;
+}
 
 // wp.min / wp.max on floats: a < b ? a : b (first argument on ties)
 __device__ __forceinline__ float wmin(float a, float b) { return a < b ? a : b; }
@@ -162,8 +194,9 @@ __device__ __forceinline__ void flex_elem_cells(const FlexGrid& g, float4 eb, in
 // registration order.
 __device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
   const int t = threadIdx.x, T = blockDim.x;
+  const int e0 = f.be0, e1 = f.be0 + f.n_be;
   // add_element for every boundary edge
-  for (int e = t; e < f.n_be; e += T) {
+  for (int e = e0 + t; e < e1; e += T) {
     const int2 n = f.be[e];
     const float2 a = d.x[n.x], b = d.x[n.y];
     float lx = 1e30f, ly = 1e30f, ux = -1e30f, uy = -1e30f;
@@ -213,7 +246,7 @@ __device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
   FlexGrid g = *f.g;
   // zero the cell counts; per element its lowest cell and how many pairs it makes
   for (int c = t; c < g.tc; c += T) f.cell_count[c] = 0;
-  for (int e = t; e < f.n_be; e += T) {
+  for (int e = e0 + t; e < e1; e += T) {
     int lx, ly, ux, uy, n = 0;
     flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
     f.ecell[e] = make_int2(lx, ly);
@@ -223,14 +256,14 @@ __device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
     f.ecount[e] = n;
   }
   __syncthreads();
-  const int npairs = flex_block_scan(f.ecount, f.ebase, f.n_be);
+  const int npairs = flex_block_scan(f.ecount + e0, f.ebase + e0, f.n_be);
   if (t == 0) {
     f.g->npairs = npairs;
     f.g->simple = (g.tc == g.cnx * g.cny && npairs <= f.max_pairs) ? 1 : 0;
   }
   __syncthreads();  // every chunk of ebase is written
   // counts of the pairs kept (pair index < max_pairs)
-  for (int e = t; e < f.n_be; e += T) {
+  for (int e = e0 + t; e < e1; e += T) {
     int lx, ly, ux, uy, p = f.ebase[e];
     flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
     for (int ix = lx; ix <= ux; ++ix)
@@ -250,7 +283,7 @@ __device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
     f.cell_end[c] = f.cell_start[c] + f.cell_count[c];
   }
   __syncthreads();
-  for (int e = t; e < f.n_be; e += T) {
+  for (int e = e0 + t; e < e1; e += T) {
     int lx, ly, ux, uy, p = f.ebase[e];
     flex_elem_cells(g, f.ebox[e], lx, ly, ux, uy);
     for (int ix = lx; ix <= ux; ++ix)
@@ -296,15 +329,16 @@ __device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
 // construction-time build (explicitloop.py:383-385) -- rebuild, no contact.
 // Dynamic shared memory: (n_dom + n_fem) boxes -- every domain's, then every
 // FEM body's.
-__global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f, int force) {
+__global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f0, int force) {
   extern __shared__ float4 sbox[];
   __shared__ int s_rebuild;
+  const FlexDev f = flex_view(f0, blockIdx.x);  // one block per scene with FEM-FEM contact
   const int s = f.scene;
   const bool step = !force && flex_stepping(d, s);
   if (threadIdx.x == 0) {
     int rb = force ? 1 : 0;
     if (step) {  // maybe_rebuild_fem_spatial_hash(self.dt)
-      double e = f.g->elapsed + f.g->clock_dt;
+      double e = f.g->elapsed + f.clock_dt[blockIdx.x];
       if (e >= kFlexRebuildInterval) {
         rb = 1;
         e = 0.0;
@@ -345,7 +379,7 @@ __global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f,
         st = __any_sync(0xFFFFFFFFu, hit);
       }
     }
-    if (lane == 0) f.stamped[gi] = st ? 1 : 0;
+    if (lane == 0) f.stamped[f.body0 + gi] = st ? 1 : 0;
   }
   __syncthreads();
   // the work items that run: the (pair, side) segments whose pair is active
@@ -399,14 +433,14 @@ __device__ __forceinline__ float flex_detect(float2 p, float2 a, float2 b, float
   return 1e9f;
 }
 
-__device__ __forceinline__ void flex_push(const Dev& d, FlexGrid* g, int node, int item, float2 force) {
+__device__ __forceinline__ void flex_push(const Dev& d, int* err, int node, int item, float2 force) {
   const int slot = d.flex_slot[node];
   const int j = atomicAdd(&d.flex_cnt[slot], 1);
   if (j < kFlexListCap) {
     d.flex_item[slot * kFlexListCap + j] = item;
     d.flex_force[slot * kFlexListCap + j] = force;
   } else {
-    atomicOr(&g->err, 1);
+    atomicOr(err, 1);
   }
 }
 
@@ -558,16 +592,17 @@ __device__ __forceinline__ void flex_item(const Dev& d, const FlexDev& f, const 
         ty = ty + ddy * fric * nl;
       }
     }
-    flex_push(d, f.g, nid, it, make_float2(tx, ty));
-    flex_push(d, f.g, bn0, it, make_float2(-(tx * bw0), -(ty * bw0)));
-    flex_push(d, f.g, bn1, it, make_float2(-(tx * bw1), -(ty * bw1)));
+    flex_push(d, f.err, nid, it, make_float2(tx, ty));
+    flex_push(d, f.err, bn0, it, make_float2(-(tx * bw0), -(ty * bw0)));
+    flex_push(d, f.err, bn1, it, make_float2(-(tx * bw1), -(ty * bw1)));
   }
 }
 
 // Each group of kFlexLanes lanes takes active work items in turn (grid
 // stride over the compacted list): the item's segment by binary search over
 // the segment offsets, then flex_item.
-__global__ void __launch_bounds__(kFlexContactThreads) k_flex_contact(Dev d, FlexDev f) {
+__global__ void __launch_bounds__(kFlexContactThreads) k_flex_contact(Dev d, FlexDev f0) {
+  const FlexDev f = flex_view(f0, blockIdx.y);  // blockIdx.y: the scene
   const int sub = threadIdx.x % kFlexLanes;
   const unsigned gmask = ((1u << kFlexLanes) - 1u) << ((threadIdx.x & 31) & ~(kFlexLanes - 1));
   const FlexGrid g = *f.g;

@@ -894,13 +894,20 @@ struct fw_ctx {
     float pen, fric;
   };
   std::vector<FlexPair> h_flex;
-  int flex_scene = -1, flex_skip_bvh = 0;
-  std::vector<int32_t> h_dom_obj, h_dom_body;
-  std::vector<float4> h_dom_box;
+  struct FlexSceneHost {
+    int skip_bvh = 0;
+    std::vector<int32_t> dom_obj, dom_body;
+    std::vector<float4> dom_box;
+  };
+  std::map<int, FlexSceneHost> h_flex_scene;  // scene -> its domains (fw_set_flex_scene)
+  std::vector<int> flex_scene_of;              // per FEM-FEM scene (kernel order): the scene
   bool has_flex = false;
   FlexDev fx{};
   size_t flex_pre_smem = 0;  // k_flex_pre: (domains + FEM bodies) boxes
-  double flex_clock = 0.0;  // host copy of the last fw_set_flex_clock value
+  std::vector<double> flex_clock;  // per FEM-FEM scene: the float64 substep dt (host copy)
+  double flex_clock_all = 0.0;     // fw_set_flex_clock before fw_finalize
+  double* d_flex_clock = nullptr;
+  int* d_flex_err = nullptr;
   // spring-mass domains: per body its node mass (0: an FEM body)
   std::vector<float> h_spring_mass;
   bool has_springs = false;
@@ -967,12 +974,13 @@ void set_grids(fw_ctx* c) {
 // the active work items), then the contact work items.
 void flex_launch(fw_ctx* c, int force) {
   const FlexDev& f = c->fx;
-  k_flex_pre<<<1, kFlexScanThreads, c->flex_pre_smem, c->stream>>>(c->d, f, force);
+  k_flex_pre<<<f.n_fs, kFlexScanThreads, c->flex_pre_smem, c->stream>>>(c->d, f, force);
   c->launches += 1;
   if (!force) {
     const int64_t threads = (int64_t)f.n_items * kFlexLanes;
-    const int blocks = (int)std::min<int64_t>((threads + kFlexContactThreads - 1) / kFlexContactThreads, 8 * c->sms);
-    k_flex_contact<<<blocks, kFlexContactThreads, 0, c->stream>>>(c->d, f);
+    const int64_t want = (threads + kFlexContactThreads - 1) / kFlexContactThreads;
+    const int bx = (int)std::max<int64_t>(1, std::min<int64_t>(want, 8 * c->sms) / f.n_fs);
+    k_flex_contact<<<dim3(bx, f.n_fs), kFlexContactThreads, 0, c->stream>>>(c->d, f);
     c->launches += 1;
   }
 }
@@ -1489,7 +1497,7 @@ int launch_resident(fw_ctx* c, int n) {
 int check_device_error(fw_ctx* c) {
   if (c->has_flex) {
     int ferr = 0;
-    FW_CUDA(c, cudaMemcpyAsync(&ferr, &c->fx.g->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(c, cudaMemcpyAsync(&ferr, c->d_flex_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     FW_CUDA(c, cudaStreamSynchronize(c->stream));
     if (ferr & 1)
       return fail(c, FW_ERR_ARG, "FEM-FEM contact: a node received more than %d contact forces in one substep",
@@ -1757,13 +1765,14 @@ int fw_set_flex_scene(fw_ctx* c, int32_t scene, int32_t skip_bvh, int32_t n_doma
                       const int32_t* dom_body, const float* dom_box) {
   if (!c || n_domains < 0 || (n_domains && (!dom_obj || !dom_body || !dom_box))) return FW_ERR_ARG;
   if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_set_flex_scene after fw_finalize / on an arena");
-  c->flex_scene = scene;
-  c->flex_skip_bvh = skip_bvh ? 1 : 0;
-  c->h_dom_obj.assign(dom_obj, dom_obj + n_domains);
-  c->h_dom_body.assign(dom_body, dom_body + n_domains);
-  c->h_dom_box.resize(n_domains);
+  if (scene < 0) return fail(c, FW_ERR_ARG, "fw_set_flex_scene: scene %d", scene);
+  fw_ctx::FlexSceneHost& h = c->h_flex_scene[scene];
+  h.skip_bvh = skip_bvh ? 1 : 0;
+  h.dom_obj.assign(dom_obj, dom_obj + n_domains);
+  h.dom_body.assign(dom_body, dom_body + n_domains);
+  h.dom_box.resize(n_domains);
   for (int g = 0; g < n_domains; ++g)
-    c->h_dom_box[g] = make_float4(dom_box[4 * g], dom_box[4 * g + 1], dom_box[4 * g + 2], dom_box[4 * g + 3]);
+    h.dom_box[g] = make_float4(dom_box[4 * g], dom_box[4 * g + 1], dom_box[4 * g + 2], dom_box[4 * g + 3]);
   return FW_OK;
 }
 
@@ -1804,7 +1813,7 @@ int fw_read_flex_state(fw_ctx* c, int32_t* item_cache, int32_t n_items, float* g
   FlexGrid g{};
   if (item_cache)
     FW_CUDA(c, cudaMemcpyAsync(item_cache, c->fx.item_cache, sizeof(int32_t) * n_items, cudaMemcpyDeviceToHost, c->stream));
-  FW_CUDA(c, cudaMemcpyAsync(&g, c->fx.g, sizeof(FlexGrid), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(&g, c->fx.g, sizeof(FlexGrid), cudaMemcpyDeviceToHost, c->stream));  // the first FEM-FEM scene
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
   if (grid) {
     int est = g.estimate >= 0 ? g.estimate : g.estimate ^ 0x7FFFFFFF;  // ordered int -> float bits
@@ -1831,22 +1840,32 @@ int fw_set_spring_bodies(fw_ctx* c, int32_t n, const int32_t* bodies, const floa
 
 int fw_set_flex_clock(fw_ctx* c, double dt) {
   if (!c) return FW_ERR_ARG;
-  c->flex_clock = dt;
+  for (double& v : c->flex_clock) v = dt;
+  c->flex_clock_all = dt;
   if (c->has_flex)
-    FW_CUDA(c, cudaMemcpyAsync(&c->fx.g->clock_dt, &c->flex_clock, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    FW_CUDA(c, cudaMemcpyAsync(c->d_flex_clock, c->flex_clock.data(), sizeof(double) * c->flex_clock.size(),
+                               cudaMemcpyHostToDevice, c->stream));
   return FW_OK;
 }
 
-// Device state of the FEM-FEM contact of a single-scene world: work items in
-// the reference's order (per pair: domain2's boundary nodes against domain1's
-// edges, then domain1's against domain2's; mixedcontact.py:1876-1924), the
-// spatial hash arrays sized as the reference sizes them
-// (femspringmanager.py:545-548: MAX_BOUNDARY_ELEMENTS; spatialmanager.py:520-525:
-// 3^2 pairs per element), and the per-node contribution lists.
+int fw_set_flex_clocks(fw_ctx* c, const double* dt) {
+  if (!c || !dt) return FW_ERR_ARG;
+  if (!c->has_flex) return fail(c, FW_ERR_STATE, "fw_set_flex_clocks: no FEM-FEM contact (or before fw_finalize)");
+  for (size_t k = 0; k < c->flex_clock.size(); ++k) c->flex_clock[k] = dt[c->flex_scene_of[k]];
+  FW_CUDA(c, cudaMemcpyAsync(c->d_flex_clock, c->flex_clock.data(), sizeof(double) * c->flex_clock.size(),
+                             cudaMemcpyHostToDevice, c->stream));
+  return FW_OK;
+}
+
+// Device state of the FEM-FEM contact: per scene with ContactFlexFlex pairs,
+// its work items in the reference's order (per pair: domain2's boundary nodes
+// against domain1's edges, then domain1's against domain2's;
+// mixedcontact.py:1876-1924), its spatial hash arrays sized as the reference
+// sizes them for that loop (femspringmanager.py:545-548 MAX_BOUNDARY_ELEMENTS;
+// spatialmanager.py:520-525: 3^2 pairs per element, 100000 cells), and the
+// per-node contribution lists.
 int build_flex(fw_ctx* c) {
   const int B = c->B, N = c->N;
-  if (c->S != 1 || c->flex_scene != 0)
-    return fail(c, FW_ERR_ARG, "FEM-FEM contact: one scene per world (fw_set_flex_scene(ctx, 0, ...))");
   if ((int)c->h_be_off.size() != B) return fail(c, FW_ERR_ARG, "FEM-FEM contact: fw_set_boundary_edges missing");
   const int n_be = (int)c->h_be.size();
   std::vector<int32_t> be_dom(std::max(n_be, 1), 0), be_off(B), be_cnt(B);
@@ -1865,104 +1884,155 @@ int build_flex(fw_ctx* c) {
     run += be_cnt[b];
   }
   if (run != n_be || n_be == 0) return fail(c, FW_ERR_ARG, "FEM-FEM contact: boundary edge counts do not add up");
-  const int n_dom = (int)c->h_dom_obj.size();
-  for (int g = 0; g < n_dom; ++g)
-    if (c->h_dom_body[g] >= B) return fail(c, FW_ERR_ARG, "FEM-FEM contact: domain %d names body %d", g, c->h_dom_body[g]);
+  // bodies of each scene (contiguous, in body order)
+  std::vector<int> s_b0(c->S, -1), s_nb(c->S, 0);
+  for (int b = 0; b < B; ++b) {
+    const int sc = c->h_scene[b];
+    if (s_b0[sc] < 0) s_b0[sc] = b;
+    if (s_b0[sc] + s_nb[sc] != b) return fail(c, FW_ERR_ARG, "FEM-FEM contact: a scene's bodies must be contiguous");
+    ++s_nb[sc];
+  }
+  // pairs grouped by scene, creation order kept within a scene
+  std::map<int, std::vector<int>> pairs_of;
+  for (size_t p = 0; p < c->h_flex.size(); ++p) {
+    const fw_ctx::FlexPair& fp = c->h_flex[p];
+    if (c->h_scene[fp.b1] != c->h_scene[fp.b2]) return fail(c, FW_ERR_ARG, "FEM-FEM pair %zu joins two scenes", p);
+    pairs_of[c->h_scene[fp.b1]].push_back((int)p);
+  }
   std::vector<int32_t> item_node, item_target, item_pair;
   std::vector<float> item_pen, item_fric;
   std::vector<int2> pair_body;
-  std::vector<int4> segs;  // (first item, count, pair, target)
+  std::vector<int4> segs;  // (first item, count, pair in its scene, target)
+  std::vector<FlexScene> scs;
+  std::vector<int32_t> dom_obj, dom_body;
+  std::vector<float4> dom_box;
   std::vector<int32_t> slot(N, -1);
-  int n_slots = 0;
-  for (size_t p = 0; p < c->h_flex.size(); ++p) {
-    const fw_ctx::FlexPair& fp = c->h_flex[p];
-    pair_body.push_back(make_int2(fp.b1, fp.b2));
-    for (int side = 0; side < 2; ++side) {
-      const int src = side == 0 ? fp.b2 : fp.b1, dst = side == 0 ? fp.b1 : fp.b2;
-      segs.push_back(make_int4((int)item_node.size(), c->h_bncnt[src], (int)p, dst));
-      for (int k = 0; k < c->h_bncnt[src]; ++k) {
-        const int n = c->h_bnodes[c->h_bnoff[src] + k];
-        item_node.push_back(n);
-        item_target.push_back(dst);
-        item_pair.push_back((int)p);
-        item_pen.push_back(fp.pen);
-        item_fric.push_back(fp.fric);
-        if (slot[n] < 0) slot[n] = n_slots++;
+  int n_slots = 0, pair_base = 0, max_dom_fem = 1;
+  c->flex_scene_of.clear();
+  for (auto& kv : pairs_of) {
+    const int sc = kv.first;
+    auto it = c->h_flex_scene.find(sc);
+    if (it == c->h_flex_scene.end()) return fail(c, FW_ERR_ARG, "FEM-FEM contact: fw_set_flex_scene missing for scene %d", sc);
+    const fw_ctx::FlexSceneHost& h = it->second;
+    FlexScene fsd{};
+    fsd.scene = sc;
+    fsd.body0 = s_b0[sc];
+    fsd.n_fem = s_nb[sc];
+    fsd.dom_off = (int)dom_obj.size();
+    fsd.n_dom = (int)h.dom_obj.size();
+    fsd.skip_bvh = h.skip_bvh;
+    for (int g = 0; g < fsd.n_dom; ++g) {
+      const int db = h.dom_body[g];
+      if (db >= 0 && (db < fsd.body0 || db >= fsd.body0 + fsd.n_fem))
+        return fail(c, FW_ERR_ARG, "FEM-FEM contact: scene %d domain %d names body %d of another scene", sc, g, db);
+      dom_obj.push_back(h.dom_obj[g]);
+      dom_body.push_back(db);
+      dom_box.push_back(h.dom_box[g]);
+    }
+    fsd.pair_off = (int)pair_body.size();
+    fsd.n_pairs = (int)kv.second.size();
+    fsd.seg_base = (int)segs.size();
+    int scene_nodes = 0;
+    for (int b = fsd.body0; b < fsd.body0 + fsd.n_fem; ++b) scene_nodes += c->h_ncnt[b];
+    fsd.be0 = be_off[fsd.body0];
+    fsd.n_be = 0;
+    for (int b = fsd.body0; b < fsd.body0 + fsd.n_fem; ++b) fsd.n_be += be_cnt[b];
+    const int max_nodes = std::max(scene_nodes + 1024, 2048);
+    const int max_elements = std::max(fsd.n_be + 1024, max_nodes);
+    fsd.max_pairs = 9 * max_elements;
+    fsd.pair_base = pair_base;
+    pair_base += fsd.max_pairs;
+    fsd.cell_base = (int)scs.size() * kFlexMaxCells;
+    for (int lp = 0; lp < fsd.n_pairs; ++lp) {
+      const fw_ctx::FlexPair& fp = c->h_flex[kv.second[lp]];
+      pair_body.push_back(make_int2(fp.b1, fp.b2));
+      for (int side = 0; side < 2; ++side) {
+        const int src = side == 0 ? fp.b2 : fp.b1, dst = side == 0 ? fp.b1 : fp.b2;
+        segs.push_back(make_int4((int)item_node.size(), c->h_bncnt[src], lp, dst));
+        for (int k = 0; k < c->h_bncnt[src]; ++k) {
+          const int n = c->h_bnodes[c->h_bnoff[src] + k];
+          item_node.push_back(n);
+          item_target.push_back(dst);
+          item_pair.push_back(fsd.pair_off + lp);
+          item_pen.push_back(fp.pen);
+          item_fric.push_back(fp.fric);
+          if (slot[n] < 0) slot[n] = n_slots++;
+        }
       }
     }
+    fsd.n_seg = (int)segs.size() - fsd.seg_base;
+    for (int k = fsd.be0; k < fsd.be0 + fsd.n_be; ++k)  // edge nodes receive the reactions
+      for (int n : {c->h_be[k].x, c->h_be[k].y})
+        if (slot[n] < 0) slot[n] = n_slots++;
+    max_dom_fem = std::max(max_dom_fem, fsd.n_dom + fsd.n_fem);
+    scs.push_back(fsd);
+    c->flex_scene_of.push_back(sc);
   }
-  for (const int2& e : c->h_be)  // edge nodes receive the reactions
-    for (int n : {e.x, e.y})
-      if (slot[n] < 0) slot[n] = n_slots++;
+  const int n_fs = (int)scs.size();
   const int n_items = (int)item_node.size();
-  const int max_nodes = std::max(N + 1024, 2048);
-  const int max_elements = std::max(n_be + 1024, max_nodes);
   FlexDev f{};
   f.n_items = n_items;
-  f.n_pairs = (int)pair_body.size();
-  f.n_fem = B;
-  f.n_dom = n_dom;
-  f.skip_bvh = c->flex_skip_bvh;
-  f.n_be = n_be;
-  f.body0 = 0;
-  f.scene = 0;
-  f.max_pairs = 9 * max_elements;
+  f.n_fs = n_fs;
   f.mpd = std::max(powf(100000.0f, 0.5f), 1.0f);
-  int rc;
-  int32_t *inode = nullptr, *itgt = nullptr, *ipair = nullptr, *icache = nullptr, *bdom = nullptr, *boff = nullptr,
-          *bcnt = nullptr, *dobj = nullptr, *dbody = nullptr, *pact = nullptr, *stamp = nullptr, *ecount = nullptr,
-          *ebase = nullptr, *ccount = nullptr, *cstart = nullptr, *cend = nullptr, *cursor = nullptr,
-          *sorted = nullptr, *dslot = nullptr, *dcnt = nullptr, *ditem = nullptr;
-  int2 *crange = nullptr, *ecell = nullptr, *scell = nullptr;
-  int4 *srec = nullptr, *dseg = nullptr;
-  int32_t* dsegoff = nullptr;
-  float *ipen = nullptr, *ifric = nullptr;
-  int2 *pbody = nullptr, *dbe = nullptr;
-  float4 *dbox = nullptr, *ebox = nullptr;
-  float2* dforce = nullptr;
-  FlexGrid* grid = nullptr;
-  std::vector<int32_t> minus1(std::max(n_items, 1), -1);
-  std::vector<float4> dom_box = c->h_dom_box;
-  std::vector<int32_t> dom_obj = c->h_dom_obj, dom_body = c->h_dom_body;
+  c->flex_clock.assign(n_fs, c->flex_clock_all);
   if (dom_obj.empty()) {
     dom_obj.push_back(0);
     dom_body.push_back(-1);
     dom_box.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
   }
+  std::vector<int32_t> minus1(std::max(n_items, 1), -1);
+  // each scene's seg_off has n_seg + 1 entries: seg_base + k
+  const size_t n_segoff = segs.size() + (size_t)n_fs;
+  int rc;
+  int32_t *inode = nullptr, *itgt = nullptr, *ipair = nullptr, *icache = nullptr, *bdom = nullptr, *boff = nullptr,
+          *bcnt = nullptr, *dobj = nullptr, *dbody = nullptr, *pact = nullptr, *stamp = nullptr, *ecount = nullptr,
+          *ebase = nullptr, *ccount = nullptr, *cstart = nullptr, *cend = nullptr, *cursor = nullptr,
+          *sorted = nullptr, *dslot = nullptr, *dcnt = nullptr, *ditem = nullptr, *dsegoff = nullptr;
+  float *ipen = nullptr, *ifric = nullptr;
+  int2 *pbody = nullptr, *dbe = nullptr, *crange = nullptr, *ecell = nullptr, *scell = nullptr;
+  int4 *srec = nullptr, *dseg = nullptr;
+  float4 *dbox = nullptr, *ebox = nullptr;
+  float2* dforce = nullptr;
+  FlexGrid* grid = nullptr;
+  FlexScene* dsc = nullptr;
+  const size_t cells = (size_t)n_fs * kFlexMaxCells;
   if ((rc = upload(c, &inode, item_node)) || (rc = upload(c, &itgt, item_target)) || (rc = upload(c, &ipair, item_pair)) ||
       (rc = upload(c, &ipen, item_pen)) || (rc = upload(c, &ifric, item_fric)) || (rc = upload(c, &icache, minus1)) ||
       (rc = upload(c, &pbody, pair_body)) || (rc = upload(c, &dbe, c->h_be)) || (rc = upload(c, &bdom, be_dom)) ||
       (rc = upload(c, &boff, be_off)) || (rc = upload(c, &bcnt, be_cnt)) || (rc = upload(c, &dobj, dom_obj)) ||
-      (rc = upload(c, &dbody, dom_body)) || (rc = upload(c, &dbox, dom_box)) ||
-      (rc = dalloc(c, &pact, std::max(1, f.n_pairs))) || (rc = dalloc(c, &stamp, std::max(1, B))) ||
-      (rc = dalloc(c, &grid, 1)) || (rc = dalloc(c, &ebox, n_be)) || (rc = dalloc(c, &ecount, n_be)) ||
-      (rc = dalloc(c, &ebase, n_be)) || (rc = dalloc(c, &ccount, kFlexMaxCells)) ||
-      (rc = dalloc(c, &cstart, kFlexMaxCells)) || (rc = dalloc(c, &cend, kFlexMaxCells)) ||
-      (rc = dalloc(c, &cursor, kFlexMaxCells)) || (rc = dalloc(c, &sorted, f.max_pairs)) ||
-      (rc = dalloc(c, &crange, kFlexMaxCells)) || (rc = dalloc(c, &ecell, n_be)) ||
-      (rc = dalloc(c, &srec, f.max_pairs)) || (rc = dalloc(c, &scell, f.max_pairs)) ||
-      (rc = upload(c, &dseg, segs)) || (rc = dalloc(c, &dsegoff, segs.size() + 1)) ||
+      (rc = upload(c, &dbody, dom_body)) || (rc = upload(c, &dbox, dom_box)) || (rc = upload(c, &dsc, scs)) ||
+      (rc = dalloc(c, &pact, std::max<size_t>(1, pair_body.size()))) || (rc = dalloc(c, &stamp, B)) ||
+      (rc = dalloc(c, &grid, n_fs)) || (rc = dalloc(c, &ebox, n_be)) || (rc = dalloc(c, &ecount, n_be)) ||
+      (rc = dalloc(c, &ebase, n_be)) || (rc = dalloc(c, &ccount, cells)) || (rc = dalloc(c, &cstart, cells)) ||
+      (rc = dalloc(c, &cend, cells)) || (rc = dalloc(c, &cursor, cells)) || (rc = dalloc(c, &crange, cells)) ||
+      (rc = dalloc(c, &sorted, (size_t)pair_base)) || (rc = dalloc(c, &srec, (size_t)pair_base)) ||
+      (rc = dalloc(c, &scell, (size_t)pair_base)) || (rc = dalloc(c, &ecell, n_be)) ||
+      (rc = upload(c, &dseg, segs)) || (rc = dalloc(c, &dsegoff, n_segoff)) ||
       (rc = upload(c, &dslot, slot)) || (rc = dalloc(c, &dcnt, std::max(1, n_slots))) ||
       (rc = dalloc(c, &ditem, std::max(1, n_slots) * kFlexListCap)) ||
-      (rc = dalloc(c, &dforce, std::max(1, n_slots) * kFlexListCap)))
+      (rc = dalloc(c, &dforce, std::max(1, n_slots) * kFlexListCap)) || (rc = dalloc(c, &c->d_flex_clock, n_fs)) ||
+      (rc = dalloc(c, &c->d_flex_err, 1)))
     return rc;
-  FW_CUDA(c, cudaMemsetAsync(grid, 0, sizeof(FlexGrid), c->stream));
-  FW_CUDA(c, cudaMemcpyAsync(&grid->clock_dt, &c->flex_clock, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(grid, 0, sizeof(FlexGrid) * n_fs, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(c->d_flex_err, 0, sizeof(int), c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(c->d_flex_clock, c->flex_clock.data(), sizeof(double) * n_fs, cudaMemcpyHostToDevice,
+                             c->stream));
   FW_CUDA(c, cudaMemsetAsync(dcnt, 0, sizeof(int32_t) * std::max(1, n_slots), c->stream));
-  FW_CUDA(c, cudaMemsetAsync(cstart, 0, sizeof(int32_t) * kFlexMaxCells, c->stream));
-  FW_CUDA(c, cudaMemsetAsync(cend, 0, sizeof(int32_t) * kFlexMaxCells, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(cstart, 0, sizeof(int32_t) * cells, c->stream));
+  FW_CUDA(c, cudaMemsetAsync(cend, 0, sizeof(int32_t) * cells, c->stream));
   f.item_node = inode; f.item_target = itgt; f.item_pair = ipair; f.item_pen = ipen; f.item_fric = ifric;
   f.item_cache = icache; f.pair_body = pbody; f.be = dbe; f.be_dom = bdom; f.be_off = boff; f.be_cnt = bcnt;
   f.dom_obj = dobj; f.dom_body = dbody; f.dom_box = dbox; f.pair_active = pact; f.stamped = stamp; f.g = grid;
   f.ebox = ebox; f.ecount = ecount; f.ebase = ebase; f.cell_count = ccount; f.cell_start = cstart;
   f.cell_end = cend; f.cursor = cursor; f.sorted = sorted; f.crange = crange; f.ecell = ecell;
   f.srec = srec; f.scell = scell;
-  f.n_seg = (int)segs.size(); f.seg = dseg; f.seg_off = dsegoff;
-  c->flex_pre_smem = sizeof(float4) * (size_t)(std::max(n_dom, 1) + B);
+  f.seg = dseg; f.seg_off = dsegoff;
+  f.sc = dsc; f.clock_dt = c->d_flex_clock; f.err = c->d_flex_err;
+  c->flex_pre_smem = sizeof(float4) * (size_t)max_dom_fem;
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if ((long)c->flex_pre_smem > optin)
-    return fail(c, FW_ERR_ARG, "FEM-FEM contact: %d domains need %zu B of shared memory", n_dom, c->flex_pre_smem);
+    return fail(c, FW_ERR_ARG, "FEM-FEM contact: a scene's domains need %zu B of shared memory", c->flex_pre_smem);
   if (c->flex_pre_smem > 48 * 1024)
     FW_CUDA(c, cudaFuncSetAttribute(k_flex_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->flex_pre_smem));
   c->fx = f;

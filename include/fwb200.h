@@ -122,12 +122,13 @@ int fw_add_voxel_pair(fw_ctx* ctx, int32_t body, float penalty, const float* gat
                       const float* gate_hi, int32_t nx, int32_t ny, const int32_t* occupancy,
                       float lb_x, float lb_y, float dx, float dz);
 
-/* FEM-FEM penalty contact (single-scene worlds, gather path).
+/* FEM-FEM penalty contact (gather path; any number of scenes, each with its
+ * own spatial hash).
  * fw_set_boundary_edges: every body's boundary edges (2 global node ids each,
  * in mesh order and orientation, mesh.py:53-71), stored body by body:
  * body b's at edges[2*body_off[b] ..], body_cnt[b] of them.  Replaces the
  * boundaryElements / domainBoundaryElemOffset packing, femspringmanager.py:783-799.
- * fw_set_flex_scene: the loop's domains in loop order -- dom_obj[g] != 0 if
+ * fw_set_flex_scene (once per scene that has FEM-FEM pairs): the loop's domains in loop order -- dom_obj[g] != 0 if
  * domain g takes part in the broad phase (considerContact), dom_body[g] its
  * body id (-1 for a ground), dom_box the ground's getBBox() (lo x, lo y, hi x,
  * hi y); skip_bvh != 0 when the loop has no plane, height-field, voxel or
@@ -147,6 +148,10 @@ int fw_set_flex_scene(fw_ctx* ctx, int32_t scene, int32_t skip_bvh, int32_t n_do
                       const int32_t* dom_body, const float* dom_box);
 int fw_add_flex_pair(fw_ctx* ctx, int32_t body1, int32_t body2, float penalty, float friction);
 int fw_set_flex_clock(fw_ctx* ctx, double dt);
+/* The same per scene (dt[scene], one entry per scene of the world; scenes
+ * without FEM-FEM contact are ignored), for worlds whose scenes step with their
+ * own dt (batched advanceWithTime).  After fw_finalize. */
+int fw_set_flex_clocks(fw_ctx* ctx, const double* dt);
 /* Spring-mass domains (SpringMassDomain, femspringmanager.py:815-870): the
  * listed bodies are spring-mass bodies whose nodes each carry node_mass (the
  * domain's prop[2]).  Their elements are 2-node springs given to

@@ -151,3 +151,22 @@ def test_gpu_flex_world_limits():
     lp = fw.ExplicitLoop(0.0, scenes.flex_circles(fw), useAdapativeDT=True)
     with pytest.raises(RuntimeError, match="FEM-FEM"):
         lp._native.snapshot(0)
+
+
+@pytest.mark.gpu
+def test_gpu_batched_flex_scenes_equal_alone():
+    """FEM-FEM scenes batched with others (each scene its own spatial hash,
+    clock and broad phase; per-scene dt schedules): every scene equals the same
+    scene in its own loop, frame after frame."""
+    from flatworld_b200.batch import BatchedLoop
+
+    builds = [scenes.flex_circles, scenes.flex_stack, scenes.flex_stamp_quirk, scenes.plain_small_scene]
+    b = BatchedLoop([f(fw) for f in builds], useAdapativeDT=True)
+    assert len(set(np.round(b.dt, 12))) > 1
+    alone = [fw.ExplicitLoop(0.0, f(fw), useAdapativeDT=True) for f in builds]
+    for frame in range(8):
+        b.advanceWithTime(FRAME)
+        for s, lp in enumerate(alone):
+            lp.advanceWithTime(FRAME)
+            n = len(b.coords(s))
+            assert np.array_equal(b.coords(s), lp.femSpringManager.coords.numpy()[:n]), (frame, s)
