@@ -1969,6 +1969,8 @@ int build_flex(fw_ctx* c) {
     c->flex_scene_of.push_back(sc);
   }
   const int n_fs = (int)scs.size();
+  if (n_fs > 65535)  // the contact launch puts the scenes in gridDim.y
+    return fail(c, FW_ERR_ARG, "FEM-FEM contact: %d scenes with FEM-FEM pairs in one world, at most 65535", n_fs);
   const int n_items = (int)item_node.size();
   FlexDev f{};
   f.n_items = n_items;
