@@ -2,19 +2,22 @@
 
 Drop-in for the FEM path of FlatWorld (``from flatworld import ...``):
 FemDomain / SolidProp(Elastic | HyperElastic | MisesPlastic) /
-GroundDomain | HeightFieldDomain | VoxelGridDomain / ExplicitLoop.
+GroundDomain | HeightFieldDomain | VoxelGridDomain / ExplicitLoop, plus
+FEM-FEM contact, SpringMassDomain, and rigid primitives (RigidBodyDomain with
+BallRigid | BoxRigid | CapsuleRigid) in contact with FEM bodies.
 The step runs as hand-written CUDA kernels for sm_100a (libfwb200.so) behind a
 C ABI (include/fwb200.h); there is no CPU fallback.
 """
 
 from .bcs import (EnforceAcc, EnforceRotAcc, EnforceRotVel, EnforceVel, Fixed, FixedAll, Force, Gravity,
-                  InitialVel, Torque)
+                  InitialAngVel, InitialVel, Torque)
 from .definitions import *  # noqa: F401,F403
 from .domains import FemDomain, GroundDomain, HeightFieldDomain, SpringMassDomain, VoxelGridDomain
 from .explicitloop import ExplicitLoop, FemSpringManager
 from .femesher import FEMesher
 from .materials import J2, Elastic, HyperElastic, MisesPlastic, NeoHookean, SolidProp
 from .mesh import Mesh, structured_rectangle
+from .rigid import BallRigid, BoxRigid, CapsuleRigid, MeshRigid, RigidBodyDomain, RigidType, Transform
 
 
 def _out_of_scope(name, why):
@@ -24,17 +27,10 @@ def _out_of_scope(name, why):
     return type(name, (), {"__init__": _raise})
 
 
-_RIGID = "rigid bodies, joints and springs are solved by the reference's rigid/spring managers"
-RigidBodyDomain = _out_of_scope("RigidBodyDomain", _RIGID)
-BallRigid = _out_of_scope("BallRigid", _RIGID)
-BoxRigid = _out_of_scope("BoxRigid", _RIGID)
-CapsuleRigid = _out_of_scope("CapsuleRigid", _RIGID)
-MeshRigid = _out_of_scope("MeshRigid", _RIGID)
-Transform = _out_of_scope("Transform", _RIGID)
-PrismaticJoint = _out_of_scope("PrismaticJoint", _RIGID)
-RevoluteJoint = _out_of_scope("RevoluteJoint", _RIGID)
-SphericalJoint = _out_of_scope("SphericalJoint", _RIGID)
-WeldJoint = _out_of_scope("WeldJoint", _RIGID)
-InitialAngVel = _out_of_scope("InitialAngVel", _RIGID)
+_JOINTS = "joints are solved by the reference's rigid-body constraint solver"
+PrismaticJoint = _out_of_scope("PrismaticJoint", _JOINTS)
+RevoluteJoint = _out_of_scope("RevoluteJoint", _JOINTS)
+SphericalJoint = _out_of_scope("SphericalJoint", _JOINTS)
+WeldJoint = _out_of_scope("WeldJoint", _JOINTS)
 
 __version__ = "0.1.0"

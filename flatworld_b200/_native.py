@@ -60,6 +60,10 @@ _SIGNATURES = {
     "fw_mass_scaling": (C.c_int, [_vp, C.c_float]),
     "fw_set_spring_bodies": (C.c_int, [_vp, C.c_int32, _i32p, _f32p]),
     "fw_read_flex_state": (C.c_int, [_vp, _i32p, C.c_int32, _f32p]),
+    "fw_set_rigids": (C.c_int, [_vp, C.c_int32, _f32p, _i32p, C.c_int32, _f32p]),
+    "fw_add_rigid_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32]),
+    "fw_set_rigid_clock": (C.c_int, [_vp, C.c_int32, C.c_float, C.c_float]),
+    "fw_read_rigids": (C.c_int, [_vp, _f32p, _i32p]),
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
@@ -231,6 +235,29 @@ class NativeWorld:
     def set_spring_bodies(self, bodies, node_mass):
         b, m = _i(bodies), _f(node_mass)
         self._check(self._L.fw_set_spring_bodies(self._h, len(b[0]), b[1], m[1]), "fw_set_spring_bodies")
+
+    def set_rigids(self, params, ints, grounds):
+        """params float32[n, 16], ints int32[n, 3], grounds float32[g, 5]."""
+        p = _f(np.asarray(params, np.float32).reshape(-1))
+        i = _i(np.asarray(ints, np.int32).reshape(-1))
+        g = _f(np.asarray(grounds, np.float32).reshape(-1))
+        self._check(self._L.fw_set_rigids(self._h, len(i[0]) // 3, p[1], i[1], len(g[0]) // 5, g[1]),
+                    "fw_set_rigids")
+
+    def add_rigid_pair(self, body, rigid, penalty, friction, skip_bvh):
+        self._check(self._L.fw_add_rigid_pair(self._h, int(body), int(rigid), float(penalty), float(friction),
+                                              int(skip_bvh)), "fw_add_rigid_pair")
+
+    def set_rigid_clock(self, every: int, dt: float, damping: float):
+        self._check(self._L.fw_set_rigid_clock(self._h, int(every), float(dt), float(damping)), "fw_set_rigid_clock")
+
+    def read_rigids(self, n: int):
+        """(float32[n, 12] per rigid: center, angle, V, angular velocity, U, box lb, ub; flags)."""
+        out = np.zeros((max(n, 1), 12), np.float32)
+        flags = np.zeros(1, np.int32)
+        self._check(self._L.fw_read_rigids(self._h, out.ctypes.data_as(_f32p), flags.ctypes.data_as(_i32p)),
+                    "fw_read_rigids")
+        return out[:n], int(flags[0])
 
     def mass_scaling(self, dt_target: float):
         self._check(self._L.fw_mass_scaling(self._h, float(dt_target)), "fw_mass_scaling")

@@ -126,3 +126,19 @@ class InitialVel:
             self.nds = np.asarray(nds, dtype=np.int32)
         self.vel = np.asarray(vel, dtype=np.float32)
         self.type = VTYPE
+
+
+class InitialAngVel:
+    """Initial angular velocity of a rigid body (reference:
+    initialconditions.py:53-73); ``nds == "ALL"`` applies it to every index."""
+
+    def __init__(self, nds, ang_vel, ref_point=None):
+        if isinstance(nds, str) and nds == "ALL":
+            self.is_all_nodes = True
+            self.nds = None
+        else:
+            self.is_all_nodes = False
+            self.nds = np.asarray(nds, dtype=np.int32)
+        self.ang_vel = np.asarray(ang_vel, dtype=np.float32)
+        self.ref_point = np.asarray(ref_point, dtype=np.float32) if ref_point is not None else None
+        self.type = ROTVTYPE

@@ -189,9 +189,8 @@ __device__ __forceinline__ void element_forces(float2 a, float2 b, float2 c, flo
 
 // Broad-phase gate of one pair (bvh.py:40-46 test; 10% grown boxes on the
 // rebuild steps counter % 100 == 0, bvh.py:321-342; raw boxes otherwise).
-__device__ __forceinline__ bool pair_gate(const Pair& p, float alx, float aly, float ahx,
-                                          float ahy, int counter) {
-  float blx = p.glo[0], bly = p.glo[1], bhx = p.ghi[0], bhy = p.ghi[1];
+__device__ __forceinline__ bool box_gate(float alx, float aly, float ahx, float ahy, float blx, float bly,
+                                         float bhx, float bhy, int counter) {
   if (counter % 100 == 0) {
     const float ax = 0.1f * (ahx - alx), ay = 0.1f * (ahy - aly);
     const float bx = 0.1f * (bhx - blx), by = 0.1f * (bhy - bly);
@@ -199,6 +198,11 @@ __device__ __forceinline__ bool pair_gate(const Pair& p, float alx, float aly, f
     blx = blx - bx; bhx = bhx + bx; bly = bly - by; bhy = bhy + by;
   }
   return alx <= bhx && ahx >= blx && aly <= bhy && ahy >= bly;
+}
+
+__device__ __forceinline__ bool pair_gate(const Pair& p, float alx, float aly, float ahx,
+                                          float ahy, int counter) {
+  return box_gate(alx, aly, ahx, ahy, p.glo[0], p.glo[1], p.ghi[0], p.ghi[1], counter);
 }
 
 // Penalty force of one pair on one boundary node; returns false when the node

@@ -30,10 +30,12 @@
 
 #include "../../include/fwb200.h"
 #include "fw_device.cuh"
+#include "fw_rigid.cuh"
 #include "fw_adjoint.cuh"
 
 using fw::ElemMat;
 using fw::Pair;
+using fw::Rigid;
 
 namespace {
 
@@ -95,6 +97,12 @@ struct Dev {
   int32_t* flex_cnt;
   int32_t* flex_item;
   float2* flex_force;
+  // FEM-rigid contact (fw_rigid.cuh); rig == nullptr when the world has none.
+  // A rigid pair's work item for node i is ritem[pair.n0 + bslot[i]]
+  // (bslot: the node's index in its body's boundary node list).
+  Rigid* rig;
+  float4* ritem;
+  int32_t* bslot;
 };
 
 }  // namespace
@@ -120,6 +128,12 @@ __device__ void step_control(const Dev& d) {
     if (d.scene_mode[s] != fw::MODE_STEP) continue;
     const int k = d.scene_counter[s];
     const int* r = d.aabb_ring + ((size_t)(k & 1) * d.B + pr.body) * 4;
+    if (pr.kind == fw::PAIR_RIGID) {  // the rigid's current box; plain overlap when the loop skips the BVH
+      const Rigid& g = d.rig[pr.table];
+      d.pair_active[p] = fw::box_gate(fw::ord2f(r[0]), fw::ord2f(r[1]), fw::ord2f(r[2]), fw::ord2f(r[3]),
+                                      g.lb[0], g.lb[1], g.ub[0], g.ub[1], pr.n1 ? 1 : k) ? 1 : 0;
+      continue;
+    }
     d.pair_active[p] = fw::pair_gate(pr, fw::ord2f(r[0]), fw::ord2f(r[1]), fw::ord2f(r[2]),
                                      fw::ord2f(r[3]), k) ? 1 : 0;
   }
@@ -226,7 +240,7 @@ __device__ __forceinline__ void flex_add(const Dev& d, int slot, float2& f) {
 // dependent loads; the corners are then summed in the same ascending order.
 constexpr int kNodeCorners = 6;  // an interior node of a structured triangulation has 6
 
-template <bool FLEX>
+template <bool FLEX, bool RIGID>
 __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
   const uint32_t w = valid ? d.node_word[i] : 0u;
   float2 x = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f), bv0 = make_float2(0.f, 0.f);
@@ -261,6 +275,14 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
         if (FLEX && !flex_done && d.pairs[p0 + k].kind != fw::PAIR_PLANE) {
           flex_add(d, fs, f);  // FEM-FEM contact runs after the planes, before the height fields / voxels
           flex_done = true;
+        }
+        if (RIGID && d.pairs[p0 + k].kind == fw::PAIR_RIGID) {
+          const Pair& pr = d.pairs[p0 + k];
+          const float4 rec = d.pair_active[p0 + k]
+                                 ? fw::rigid_item(d.rig[pr.table], pr.table, pr.penalty, pr.f[0], x, v, dt, f)
+                                 : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+          d.ritem[pr.n0 + d.bslot[i]] = rec;
+          continue;
         }
         if (!d.pair_active[p0 + k]) continue;
         float2 cf;
@@ -325,19 +347,82 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes(Dev d) {
   if (d.use_chunks) {
     for (int c = blockIdx.x; c < d.n_n_chunks; c += gridDim.x) {
       const int2 ch = d.n_chunks[c];
-      node_step<false>(d, ch.x + (int)threadIdx.x, (int)threadIdx.x < ch.y);
+      node_step<false, false>(d, ch.x + (int)threadIdx.x, (int)threadIdx.x < ch.y);
     }
     return;
   }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  node_step<false>(d, i, i < d.N);
+  node_step<false, false>(d, i, i < d.N);
 }
 
 // k_nodes of worlds with FEM-FEM contact: the node's contact forces from the
 // work items join its plane and ground contact forces in launch order.
 __global__ void __launch_bounds__(kMaxBlock) k_nodes_flex(Dev d) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  node_step<true>(d, i, i < d.N);
+  node_step<true, false>(d, i, i < d.N);
+}
+
+// k_nodes of worlds with FEM-rigid contact (FLEX: FEM-FEM contact as well).
+template <bool FLEX>
+__global__ void __launch_bounds__(kMaxBlock) k_nodes_rigid(Dev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  node_step<FLEX, true>(d, i, i < d.N);
+}
+
+// The rigid side of a substep (single-scene worlds), one warp: the work
+// items' reactions added to their rigids' accumulators in item order (lanes
+// stage 32 records at a time, lane 0 adds them), then the rigid counter and,
+// on the substeps of the schedule, the rigid update (fw_rigid.cuh).
+struct RigidDev {
+  Rigid* rig;
+  int n;
+  float4* gbox;
+  int* gkind;
+  int n_ground;
+  float4* item;
+  int n_items;
+  const fw::RigidClock* clock;
+  int* count;
+  int* err;
+};
+
+__global__ void __launch_bounds__(32) k_rigid(Dev d, RigidDev r) {
+  if (d.scene_mode[0] != fw::MODE_STEP) return;
+  __shared__ float4 buf[32];
+  const int lane = threadIdx.x;
+  for (int base = 0; base < r.n_items; base += 32) {
+    const int it = base + lane;
+    buf[lane] = it < r.n_items ? r.item[it] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    __syncwarp();
+    if (lane == 0) {
+      const int m = min(32, r.n_items - base);
+      for (int j = 0; j < m; ++j) {
+        const float4 q = buf[j];
+        const int g = __float_as_int(q.w);
+        if (g < 0) continue;
+        Rigid& rg = r.rig[g];
+        rg.acc[0] = rg.acc[0] + q.x;
+        rg.acc[1] = rg.acc[1] + q.y;
+        rg.accw = rg.accw + q.z;
+      }
+    }
+    __syncwarp();
+  }
+  if (lane != 0) return;
+  const fw::RigidClock ck = *r.clock;
+  const int cnt = *r.count + 1;
+  *r.count = cnt;
+  if (ck.every < 1 || cnt % ck.every != 0) return;
+  fw::rigid_update(r.rig, r.n, r.gbox, r.gkind, r.n_ground, ck.dt, ck.damping, r.err);
+}
+
+// Rotation cache and boxes of the rigids at construction
+// (precompute_rigid_transforms + updateBBox, explicitloop.py:198-201).
+__global__ void k_rigid_init(Rigid* rig, int n) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  fw::rigid_rot(rig[a]);
+  fw::rigid_aabb(rig[a]);
 }
 
 // Reference-shape precompute, _prepare_fem_data_kernel
@@ -722,6 +807,13 @@ __device__ void node_energy(const Dev& d, int i, double& ke, double& ext, double
     for (int q = 0; q < d.body_pair_cnt[b]; ++q) {
       const Pair& pr = d.pairs[d.body_pair_off[b] + q];
       float2 f;
+      if (pr.kind == fw::PAIR_RIGID) {  // the normal penalty force of the primitive
+        float nx, ny, cx, cy;
+        const Rigid& g = d.rig[pr.table];
+        const float depth = fw::rigid_detect(g, x.x, x.y, nx, ny, cx, cy) - 1e-4f;
+        if (depth < 0.0f) pen += 0.5 * (double)pr.penalty * (double)depth * (double)depth;
+        continue;
+      }
       if (fw::contact_force(pr, d.heights, d.occ, x, make_float2(0.f, 0.f), 0.f, f))
         pen += 0.5 * ((double)f.x * f.x + (double)f.y * f.y) / (double)pr.penalty;
     }
@@ -911,6 +1003,13 @@ struct fw_ctx {
   // spring-mass domains: per body its node mass (0: an FEM body)
   std::vector<float> h_spring_mass;
   bool has_springs = false;
+  // rigid primitives (fw_rigid.cuh): staging, then the device state
+  std::vector<Rigid> h_rigid;
+  std::vector<float4> h_gbox;
+  std::vector<int> h_gkind;
+  bool rigid_set = false, has_rigid = false;
+  RigidDev rd{};
+  fw::RigidClock* d_rclock = nullptr;
 };
 
 namespace {
@@ -985,13 +1084,24 @@ void flex_launch(fw_ctx* c, int force) {
   }
 }
 
+// Kernel launches of one gather-path substep.
+int step_launches(const fw_ctx* c) { return 2 + (c->has_flex ? 2 : 0) + (c->has_rigid ? 1 : 0); }
+
 int launch_step(fw_ctx* c) {
   if (c->has_flex) flex_launch(c, 0);
   k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
-  if (c->has_flex)
+  if (c->has_rigid) {
+    if (c->has_flex)
+      k_nodes_rigid<true><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+    else
+      k_nodes_rigid<false><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+    k_rigid<<<1, 32, 0, c->stream>>>(c->d, c->rd);
+    c->launches += 1;
+  } else if (c->has_flex) {
     k_nodes_flex<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
-  else
+  } else {
     k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+  }
   c->launches += 2;
   return check_kernel(c, "step");
 }
@@ -1072,7 +1182,7 @@ int run_steps(fw_ctx* c, int n) {
     if (rc) return rc;
     while (n >= kGraphSteps) {
       FW_CUDA(c, cudaGraphLaunch(g, c->stream));
-      c->launches += (c->has_flex ? 4 : 2) * kGraphSteps;
+      c->launches += step_launches(c) * kGraphSteps;
       n -= kGraphSteps;
     }
   }
@@ -1080,7 +1190,7 @@ int run_steps(fw_ctx* c, int n) {
     cudaGraphExec_t g = nullptr;
     if ((rc = get_graph(c, n, &g))) return rc;
     FW_CUDA(c, cudaGraphLaunch(g, c->stream));
-    c->launches += (c->has_flex ? 4 : 2) * n;
+    c->launches += step_launches(c) * n;
     n = 0;
   }
   for (int k = 0; k < n && rc == FW_OK; ++k) rc = launch_step(c);
@@ -1503,6 +1613,15 @@ int check_device_error(fw_ctx* c) {
       return fail(c, FW_ERR_ARG, "FEM-FEM contact: a node received more than %d contact forces in one substep",
                   kFlexListCap);
   }
+  if (c->has_rigid) {
+    int rerr = 0;
+    FW_CUDA(c, cudaMemcpyAsync(&rerr, c->rd.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (rerr & 1)
+      return fail(c, FW_ERR_UNSUPPORTED,
+                  "a rigid body's box met a ground's or another contact rigid's: rigid-rigid and rigid-ground "
+                  "contact (the reference's constraint solve) are outside this library");
+  }
   if (c->path != FW_PATH_RESIDENT) return FW_OK;
   int err = 0;
   FW_CUDA(c, cudaMemcpyAsync(&err, c->res.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1838,6 +1957,83 @@ int fw_set_spring_bodies(fw_ctx* c, int32_t n, const int32_t* bodies, const floa
   return FW_OK;
 }
 
+int fw_set_rigids(fw_ctx* c, int32_t n, const float* params, const int32_t* ints, int32_t n_ground,
+                  const float* grounds) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_set_rigids after fw_finalize");
+  if (c->arena) return fail(c, FW_ERR_STATE, "rigid bodies are not part of arena (served) worlds");
+  if (n < 0 || n_ground < 0 || (n > 0 && (!params || !ints)) || (n_ground > 0 && !grounds))
+    return fail(c, FW_ERR_ARG, "fw_set_rigids: bad sizes or pointers");
+  c->h_rigid.assign(n, Rigid{});
+  for (int a = 0; a < n; ++a) {
+    const float* q = params + 16 * (size_t)a;
+    Rigid& g = c->h_rigid[a];
+    g.type = ints[3 * a];
+    g.bc = ints[3 * a + 1];
+    g.in_contact = ints[3 * a + 2];
+    if (g.type != fw::RIGID_BALL && g.type != fw::RIGID_BOX && g.type != fw::RIGID_CAPSULE)
+      return fail(c, FW_ERR_ARG, "rigid %d: type %d is not a ball, box or capsule", a, g.type);
+    g.c[0] = q[0]; g.c[1] = q[1]; g.prim[0] = q[2]; g.prim[1] = q[3];
+    g.radius = q[4]; g.quat = q[5]; g.mass = q[6]; g.inertia = q[7];
+    g.V[0] = q[8]; g.V[1] = q[9]; g.W = q[10];
+    g.bcT[0] = q[11]; g.bcT[1] = q[12]; g.bcG[0] = q[13]; g.bcG[1] = q[14]; g.bcR = q[15];
+  }
+  c->h_gbox.resize(n_ground);
+  c->h_gkind.resize(n_ground);
+  for (int k = 0; k < n_ground; ++k) {
+    const float* q = grounds + 5 * (size_t)k;
+    if (q[0] != 0.0f && q[0] != 1.0f) return fail(c, FW_ERR_ARG, "ground %d: kind must be 0 (plane) or 1 (box)", k);
+    c->h_gkind[k] = (int)q[0];
+    c->h_gbox[k] = make_float4(q[1], q[2], q[3], q[4]);
+  }
+  c->rigid_set = true;
+  return FW_OK;
+}
+
+int fw_add_rigid_pair(fw_ctx* c, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->rigid_set) return fail(c, FW_ERR_STATE, "fw_add_rigid_pair before fw_set_rigids");
+  if (rigid < 0 || rigid >= (int)c->h_rigid.size())
+    return fail(c, FW_ERR_ARG, "rigid pair: rigid %d outside [0, %d)", rigid, (int)c->h_rigid.size());
+  Pair p{};
+  p.kind = fw::PAIR_RIGID;
+  p.body = body;
+  p.penalty = penalty;
+  p.table = rigid;
+  p.n1 = skip_bvh ? 1 : 0;
+  p.f[0] = friction;
+  const float zero[2] = {0.0f, 0.0f};
+  return add_pair(c, p, zero, zero);
+}
+
+int fw_set_rigid_clock(fw_ctx* c, int32_t every, float dt, float damping) {
+  if (!c) return FW_ERR_ARG;
+  if (every < 1) return fail(c, FW_ERR_ARG, "fw_set_rigid_clock: every must be >= 1");
+  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_set_rigid_clock: no FEM-rigid contact (or before fw_finalize)");
+  const fw::RigidClock ck{every, dt, damping, 0};
+  FW_CUDA(c, cudaMemcpyAsync(c->d_rclock, &ck, sizeof(ck), cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));  // ck lives on this stack frame
+  return FW_OK;
+}
+
+int fw_read_rigids(fw_ctx* c, float* out, int32_t* flags) {
+  if (!c || !out) return FW_ERR_ARG;
+  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_read_rigids: no FEM-rigid contact (or before fw_finalize)");
+  std::vector<Rigid> h(c->rd.n);
+  int err = 0;
+  FW_CUDA(c, cudaMemcpyAsync(h.data(), c->rd.rig, sizeof(Rigid) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaMemcpyAsync(&err, c->rd.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (size_t a = 0; a < h.size(); ++a) {
+    const Rigid& g = h[a];
+    float* o = out + 12 * a;
+    o[0] = g.c[0]; o[1] = g.c[1]; o[2] = g.quat; o[3] = g.V[0]; o[4] = g.V[1]; o[5] = g.W;
+    o[6] = g.U[0]; o[7] = g.U[1]; o[8] = g.lb[0]; o[9] = g.lb[1]; o[10] = g.ub[0]; o[11] = g.ub[1];
+  }
+  if (flags) *flags = err;
+  return FW_OK;
+}
+
 int fw_set_flex_clock(fw_ctx* c, double dt) {
   if (!c) return FW_ERR_ARG;
   for (double& v : c->flex_clock) v = dt;
@@ -2107,6 +2303,16 @@ int fw_finalize(fw_ctx* c) {
   std::vector<Pair> pairs = c->h_pairs;
   for (const Pair& p : pairs)
     if (p.body >= B) return fail(c, FW_ERR_ARG, "contact pair: body %d >= %d", p.body, B);
+  int n_ritems = 0;  // FEM-rigid work items: per rigid pair (added order) its body's boundary nodes
+  for (Pair& p : pairs)
+    if (p.kind == fw::PAIR_RIGID) {
+      if (p.table < 0 || p.table >= (int)c->h_rigid.size())
+        return fail(c, FW_ERR_ARG, "rigid pair: rigid %d outside [0, %d)", p.table, (int)c->h_rigid.size());
+      p.n0 = n_ritems;
+      n_ritems += c->h_bncnt[p.body];
+    }
+  c->has_rigid = !c->h_rigid.empty();
+  if (c->has_rigid && S != 1) return fail(c, FW_ERR_ARG, "FEM-rigid contact: single-scene worlds only");
   std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& a, const Pair& b) { return a.body < b.body; });
   std::vector<int32_t> poff(B, 0), pcnt(B, 0);
   for (size_t k = 0; k < pairs.size(); ++k) pcnt[pairs[k].body]++;
@@ -2209,6 +2415,33 @@ int fw_finalize(fw_ctx* c) {
       return fail(c, FW_ERR_ARG, "FEM-FEM contact runs on the gather path only");
     if ((rc = build_flex(c))) return rc;
   }
+  if (c->has_rigid) {
+    if (c->path_req == FW_PATH_RESIDENT || c->path_req == FW_PATH_STREAM)
+      return fail(c, FW_ERR_ARG, "FEM-rigid contact runs on the gather path only");
+    std::vector<int32_t> bslot(N, 0);
+    for (int b = 0; b < B; ++b)
+      for (int k = 0; k < c->h_bncnt[b]; ++k) bslot[c->h_bnodes[c->h_bnoff[b] + k]] = k;
+    RigidDev& r = c->rd;
+    r.n = (int)c->h_rigid.size();
+    r.n_ground = (int)c->h_gbox.size();
+    r.n_items = n_ritems;
+    fw::RigidClock ck{1, 0.0f, 0.0f, 0};
+    if ((rc = upload(c, &r.rig, c->h_rigid)) || (rc = upload(c, &d.bslot, bslot)) ||
+        (rc = dalloc(c, &r.item, (size_t)n_ritems)) || (rc = upload(c, &r.gbox, c->h_gbox)) ||
+        (rc = upload(c, &r.gkind, c->h_gkind)) ||
+        (rc = dalloc(c, &c->d_rclock, 1)) || (rc = dalloc(c, &r.count, 1)) || (rc = dalloc(c, &r.err, 1)))
+      return rc;
+    FW_CUDA(c, cudaMemcpyAsync(c->d_rclock, &ck, sizeof(ck), cudaMemcpyHostToDevice, c->stream));
+    FW_CUDA(c, cudaMemsetAsync(r.count, 0, sizeof(int), c->stream));
+    FW_CUDA(c, cudaMemsetAsync(r.err, 0, sizeof(int), c->stream));
+    r.clock = c->d_rclock;
+    d.rig = r.rig;
+    d.ritem = r.item;
+    k_rigid_init<<<(r.n + 127) / 128, 128, 0, c->stream>>>(r.rig, r.n);
+    c->launches += 1;
+    if ((rc = check_kernel(c, "rigid init"))) return rc;
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   // zero-dt construction step (setGlobalAABB -> substep(0, 0))
   if ((rc = launch_step(c))) return rc;
   FW_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -2218,7 +2451,7 @@ int fw_finalize(fw_ctx* c) {
     FW_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   c->path = FW_PATH_GATHER;
-  if (c->has_flex || c->has_springs) {
+  if (c->has_flex || c->has_springs || c->has_rigid) {
     c->finalized = true;
     return FW_OK;
   }
@@ -2298,6 +2531,7 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
 }
 
 int fw_snapshot(fw_ctx* c, int32_t slot) {
+  if (c && c->has_rigid) return fail(c, FW_ERR_STATE, "snapshots do not hold the rigid bodies' state");
   if (c && c->has_flex)
     return fail(c, FW_ERR_STATE, "snapshots do not hold the FEM-FEM contact state (hash, element caches)");
   if (!c) return FW_ERR_ARG;
@@ -2325,6 +2559,7 @@ int fw_snapshot(fw_ctx* c, int32_t slot) {
 }
 
 int fw_restore(fw_ctx* c, int32_t slot) {
+  if (c && c->has_rigid) return fail(c, FW_ERR_STATE, "snapshots do not hold the rigid bodies' state");
   if (c && c->has_flex)
     return fail(c, FW_ERR_STATE, "snapshots do not hold the FEM-FEM contact state (hash, element caches)");
   if (!c) return FW_ERR_ARG;
@@ -2652,7 +2887,7 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
 }
 
 int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
-  if (c && (c->has_flex || c->has_springs))
+  if (c && (c->has_flex || c->has_springs || c->has_rigid))
     return fail(c, FW_ERR_STATE, "the adjoint covers FEM triangles without FEM-FEM contact");
   if (!c) return FW_ERR_ARG;
   // The forward may run on either path (identical bits); the recompute and the
@@ -2809,7 +3044,7 @@ int fw_adj_read(fw_ctx* c, float* xbar, float* vbar, float* Ebar, int32_t on_dev
 }
 
 int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE, int32_t on_device) {
-  if (c && (c->has_flex || c->has_springs))
+  if (c && (c->has_flex || c->has_springs || c->has_rigid))
     return fail(c, FW_ERR_STATE, "the tangent covers FEM triangles without FEM-FEM contact");
   if (!c) return FW_ERR_ARG;
   if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)

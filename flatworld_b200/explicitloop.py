@@ -177,8 +177,13 @@ class _AABBView:
         lp = self._loop
         out = np.zeros((lp._max_domains, 2, 2), np.float32)
         boxes = lp._native.read_aabb(lp._packed.B)
+        rig = lp._rigid_state() if lp._layout.rigids else None
         for i, d in enumerate(lp.domains):
-            if d.type in (DomainType.FEM, DomainType.SPRINGMASS):
+            if d.type == DomainType.RIGID:
+                k = lp._layout.rigids.index(d)
+                out[i, 0] = rig[k, 8:10]
+                out[i, 1] = rig[k, 10:12]
+            elif d.type in (DomainType.FEM, DomainType.SPRINGMASS):
                 k = lp._packed.scenes[0].fem.index(d)
                 b = lp._packed.scene_bodies[0][k]
                 out[i, 0] = boxes[b, :2]
@@ -190,6 +195,48 @@ class _AABBView:
         return out
 
 
+class RigidManager:
+    """Read-only view of the rigid bodies of a loop with the reference's names
+    (rigidmanager.py:1410-1790): stableTime (1e-3), numRigids, and the state
+    arrays rigidParams (center, primary), quat, V, RotV, U read from the GPU."""
+
+    stableTime = 1.0 / 1000.0
+
+    def __init__(self, loop):
+        self._loop = loop
+        self.numRigids = len(loop._layout.rigids)
+        self.needUpdate = self.numRigids > 0
+        self._prim = [np.asarray(loop._packed.rigid_records()[0][k, 2:4]) for k in range(self.numRigids)]
+
+    def _col(self, sl):
+        return _HostArray(self._loop._rigid_state()[:, sl].copy())
+
+    @property
+    def rigidParams(self):
+        st = self._loop._rigid_state()
+        out = np.zeros((self.numRigids, 2, 2), np.float32)
+        out[:, 0] = st[:, 0:2]
+        for k, p in enumerate(self._prim):
+            out[k, 1] = p
+        return _HostArray(out)
+
+    @property
+    def quat(self):
+        return self._col(2)
+
+    @property
+    def V(self):
+        return self._col(slice(3, 5))
+
+    @property
+    def RotV(self):
+        return self._col(5)
+
+    @property
+    def U(self):
+        return self._col(slice(6, 8))
+
+
 class ExplicitLoop:
     """Explicit dynamics driver with the reference's constructor and stepping
     API (explicitloop.py:72-85, 473-589)."""
@@ -199,7 +246,10 @@ class ExplicitLoop:
                  mass_scaling_dt=0.0, max_contact_velocity=50.0, device=0, path="auto", patches=0,
                  front_warps=0, res_sync=0):
         if joints:
-            raise NotImplementedError("joints belong to the rigid-body solver, outside flatworld_b200's scope")
+            raise NotImplementedError("joints belong to the rigid-body constraint solver, outside flatworld_b200")
+        if not considerRigidRigidContact and any(d.type == DomainType.RIGID for d in domains):
+            raise NotImplementedError("considerRigidRigidContact=False with rigid bodies: flatworld_b200 runs "
+                                      "FEM-rigid contact with the reference's default broad phase only")
         self.domains = domains
         self.d = domains[0].d
         self.joints = joints
@@ -218,8 +268,9 @@ class ExplicitLoop:
         self.numContacts = len(layout.contacts)
         self._unbatched_contacts = layout.unbatched
         self._counter_py = 0
-        if layout.flex and self.ties:
-            raise NotImplementedError("tied FEM-FEM pairs (ExplicitLoop ties=...) are not part of flatworld_b200")
+        if (layout.flex or layout.rigids) and self.ties:
+            raise NotImplementedError("tied FEM-FEM / FEM-rigid pairs (ExplicitLoop ties=...) are not part of "
+                                      "flatworld_b200")
         self._packed = PackedWorld([layout])
         self._native = build_native(self._packed, device=device, path=path, patches=patches,
                                     front_warps=front_warps, res_sync=res_sync)
@@ -229,13 +280,34 @@ class ExplicitLoop:
         self.aabb = _AABBView(self)
         self.femSpringManager = FemSpringManager(self, self._packed, self._native, 0)
         self._flex_clock = None
+        self._rigid_clock = None
+        if layout.rigids:
+            self.rigidManager = RigidManager(self)
+            self.rigid_update_times = 0
+            for k, d in enumerate(layout.rigids):
+                d.attach(self, k)
 
     def _clock(self, dt: float):
         """Hand the substep's float64 dt to the FEM-FEM hash-refresh clock
-        (femspringmanager.py:1035-1039 accumulates ``self.dt`` in float64)."""
+        (femspringmanager.py:1035-1039 accumulates ``self.dt`` in float64) and
+        to the rigid schedule: the rigids move every N = max(1, 1e-3 // dt)
+        substeps by N * dt (explicitloop.py:533-538)."""
         if self._layout.flex and dt != self._flex_clock:
             self._native.set_flex_clock(dt)
             self._flex_clock = dt
+        if self._layout.rigids and dt != self._rigid_clock:
+            every = max(1, RigidManager.stableTime // dt)
+            self._native.set_rigid_clock(int(every), float(np.float32(every * dt)),
+                                         float(np.float32(self.damping)))
+            self._rigid_clock = dt
+
+    def _rigid_state(self):
+        """float32[numRigids, 12]: center, angle, V, angular velocity, U, box."""
+        st, flags = self._native.read_rigids(len(self._layout.rigids))
+        if flags & 1:
+            raise RuntimeError("a rigid body met a ground or another contact rigid: rigid-rigid and "
+                               "rigid-ground contact (the reference's constraint solve) are outside flatworld_b200")
+        return st
 
     # ---- stepping
     def advance(self):
@@ -243,6 +315,8 @@ class ExplicitLoop:
         self._clock(self.dt)
         self._native.step(1, float(np.float32(self.dt)))
         self._counter_py += 1
+        if self._layout.rigids:
+            self.rigid_update_times += 1
 
     def advance_n(self, n: int, dt: float | None = None):
         """``n`` substeps of ``dt`` (default ``self.dt``) queued in one call."""
@@ -251,6 +325,8 @@ class ExplicitLoop:
         self._clock(self.dt)
         self._native.step(int(n), float(np.float32(self.dt)))
         self._counter_py += int(n)
+        if self._layout.rigids:
+            self.rigid_update_times += int(n)
 
     def advanceWithTime(self, frame_dt: float = 1.0 / 60.0, verbose: bool = False):
         """Advance by exactly ``frame_dt`` of simulated time in substeps of at
@@ -263,6 +339,8 @@ class ExplicitLoop:
             self._native.step(n, float(np.float32(sub)))
             self._counter_py += n
             total += n
+        if self._layout.rigids:
+            self.rigid_update_times += total
         if verbose:
             print(f"Completed {total} substeps for {frame_dt} seconds of simulation time.")
 

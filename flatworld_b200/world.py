@@ -18,10 +18,13 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from .definitions import ContactType, DomainType
+from .definitions import (ATYPE, FORCETYPE, GRAVITY, ROTATYPE, ROTVTYPE, RTYPE, TORQUETYPE, UTYPE, VTYPE,
+                          ContactType, DomainType)
+from .rigid import RigidType
 
 _SUPPORTED = (DomainType.FEM, DomainType.SPRINGMASS, DomainType.ANALYTICAL, DomainType.HEIGHTFIELD,
-              DomainType.VOXELMAP)
+              DomainType.VOXELMAP, DomainType.RIGID)
+_GROUND_TYPES = (DomainType.ANALYTICAL, DomainType.HEIGHTFIELD, DomainType.VOXELMAP)
 _BODY_TYPES = (DomainType.FEM, DomainType.SPRINGMASS)
 _SPRING_PENALTY_SCALE = 100.0  # femcontact.py:209, 246, 259, 272
 
@@ -47,7 +50,7 @@ def contact_stable_time(penalty: float, dom) -> float:
 
 @dataclass
 class ContactSpec:
-    kind: str  # "plane" | "heightfield" | "voxel" | "flex"
+    kind: str  # "plane" | "heightfield" | "voxel" | "flex" | "rigid" | "spring-fem"
     fem: object     # the FEM domain (for "flex": domain1, the later domain)
     ground: object  # the ground (for "flex": domain2, the earlier FEM domain)
     pair_ids: tuple  # (later domain index, earlier domain index), explicitloop.py:275-276
@@ -58,7 +61,16 @@ class ContactSpec:
 
 def _contact_helper(di, dj, ctype, i, j):
     """contactHelper (femcontact.py:283-303) restricted to the FEM-ground,
-    FEM-FEM and spring-mass pairs."""
+    FEM-FEM, FEM-rigid and spring-mass pairs."""
+    if ctype == ContactType.RIGIDSPRING:
+        raise NotImplementedError("spring-mass domains against rigid bodies (ContactSpringRigid) are outside "
+                                  "flatworld_b200; set considerContact=False on one of them")
+    if ctype == ContactType.FLEXRIGID:
+        # ContactFlexRigid (femcontact.py:173-179): the FEM side's penalty and
+        # stable time; friction = the rigid's (mixedcontact.py:1992)
+        fem, rig = (di, dj) if di.type == DomainType.FEM else (dj, di)
+        pen = segment_penalty(fem)
+        return ContactSpec("rigid", fem, rig, (i, j), pen, contact_stable_time(pen, fem), float(rig.friction))
     if ctype in (ContactType.ANALYTICALSPRING, ContactType.SPRINGHEIGHTFIELD):
         # ContactSpringAnalytical / ContactSpringHeightField (femcontact.py:251-280):
         # penalty 100 k, stable time 0.5 sqrt(m / penalty)
@@ -97,8 +109,7 @@ class SceneLayout:
     def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, mass_scaling_dt=0.0):
         for d in domains:
             if d.type not in _SUPPORTED:
-                raise NotImplementedError(
-                    f"domain type {d.type} (rigid bodies, springs) is outside flatworld_b200's scope")
+                raise NotImplementedError(f"domain type {d.type} is outside flatworld_b200's scope")
         self.domains = list(domains)
         # the bodies: FEM and spring-mass domains in loop order (FemSpringManager.domains)
         self.fem = [d for d in domains if d.type in _BODY_TYPES]
@@ -168,12 +179,20 @@ class SceneLayout:
                           "is not executed for any of them", RuntimeWarning)
             self.unbatched += vox
             vox = []
-        self.pairs = anal + hf + vox
+        # FEM-rigid pairs run after FEM-FEM contact, before the height field
+        # (mixedcontact.py:1697-1715), in contact order
+        rig = [c for c in contacts if c.kind == "rigid"]
+        self.pairs = anal + rig + hf + vox
+        # RigidManager: rigid bodies in domain order (rigidmanager.py:2448-2480)
+        self.rigids = [d for d in domains if d.type == DomainType.RIGID]
+        self.grounds = [d for d in domains if d.type in _GROUND_TYPES]
         # FEM-FEM pairs in contact-creation order (mixedcontact.py:1869-1935); the
-        # loop skips the BVH (all of them stay active) when it has no ground
-        # contact at all (explicitloop.py:367-373)
+        # loop skips the BVH (all pairs stay active / plain box tests) when it has
+        # no ground contact and at most one contact rigid (explicitloop.py:362-373)
         self.flex = [c for c in contacts if c.kind == "flex"]
-        self.skip_bvh = not (anal or hf or vox or self.unbatched)
+        rigid_needs_bvh = sum(1 for d in self.rigids if d.considerContact) > 1
+        no_bvh = len(contact_domains) <= 1  # explicitloop.py:222-228: no broad phase object
+        self.skip_bvh = no_bvh or not (anal or hf or vox or self.unbatched or rigid_needs_bvh)
         self.n_nodes = sum(d.nnodes for d in self.fem)
         self.n_elems = sum(d.nelements for d in self.fem)
 
@@ -289,6 +308,24 @@ class PackedWorld:
         self.B = len(noff)
         self.S = len(scenes)
 
+    def rigid_records(self):
+        """Per rigid of the (single) scene: float32[16] and int32[3] for
+        fw_set_rigids, plus the static grounds float32[g, 5]."""
+        params, ints, boxes = [], [], []
+        for sc in self.scenes:
+            for dom in sc.rigids:
+                p, i = rigid_record(dom)
+                params.append(p)
+                ints.append(i)
+            for g in sc.grounds:  # plane: kind 0, point, normal; height field / voxel grid: kind 1, box
+                if g.type == DomainType.ANALYTICAL:
+                    boxes.append([0.0, *np.asarray(g.point, np.float32)[:2], *np.asarray(g.normal, np.float32)[:2]])
+                else:
+                    lo, hi = g.getBBox()
+                    boxes.append([1.0, *np.asarray(lo, np.float32).reshape(2), *np.asarray(hi, np.float32).reshape(2)])
+        as2 = lambda a, w, dt: np.asarray(a, dt).reshape(-1, w)  # noqa: E731
+        return as2(params, 16, np.float32), as2(ints, 3, np.int32), as2(boxes, 5, np.float32)
+
     def flex_records(self):
         """Per scene with FEM-FEM pairs: (scene, skip_bvh, dom_obj, dom_body,
         dom_box, [(body1, body2, penalty f32, friction f32)])."""
@@ -318,6 +355,10 @@ class PackedWorld:
             fem_index = {id(d): k for k, d in enumerate(sc.fem)}
             for c in sc.pairs:
                 body = self.body_of[(si, fem_index[id(c.fem)])]
+                if c.kind == "rigid":  # the gate box is the rigid's current one, on the device
+                    rid = next(k for k, d in enumerate(sc.rigids) if d is c.ground)
+                    out.append((c.kind, body, np.float32(c.penalty), rid, np.float32(c.friction), sc.skip_bvh))
+                    continue
                 lo, hi = c.ground.getBBox()
                 out.append((c.kind, body, np.float32(c.penalty), np.asarray(lo, np.float32),
                             np.asarray(hi, np.float32), c.ground))
@@ -353,8 +394,12 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
         nw.set_spring_bodies(np.asarray([b for b, _ in packed.spring_bodies], np.int32),
                              np.asarray([m for _, m in packed.spring_bodies], np.float32))
     nw.set_scenes(np.asarray([s.damping for s in packed.scenes], np.float32))
+    if any(sc.rigids for sc in packed.scenes):
+        nw.set_rigids(*packed.rigid_records())
     for kind, body, pen, lo, hi, g in packed.pair_records():
-        if kind == "plane":
+        if kind == "rigid":  # (rigid index, friction, skip_bvh) in the box slots
+            nw.add_rigid_pair(body, lo, pen, hi, 1 if g else 0)
+        elif kind == "plane":
             nw.add_plane(body, pen, lo, hi, g.point, g.normal)
         elif kind == "heightfield":
             nw.add_heightfield(body, pen, lo, hi, g.height, g.lb[0], g.ub[0], 1 if g.reverse else 0)
@@ -367,6 +412,75 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
             nw.set_flex_scene(si, skip, obj, body, box)
             for b1, b2, pen, fric in pairs:
                 nw.add_flex_pair(b1, b2, pen, fric)
+
+
+def _as_float(v) -> float:
+    """rigidmanager.py:77-81: the first element of a sequence, else float(v)."""
+    if hasattr(v, "__len__") and not isinstance(v, (str, bytes)):
+        return float(np.asarray(v, dtype=np.float32).reshape(-1)[0])
+    return float(v)
+
+
+def _as_vec2(v):
+    a = np.asarray(v, dtype=np.float32).reshape(-1)
+    return float(a[0]), (float(a[1]) if a.size > 1 else 0.0)
+
+
+def rigid_record(dom):
+    """One rigid as RigidManager stores it: RigidBodyDomain.attach (initial
+    conditions, rigiddomain.py:118-124), packRigidParams (rigidmanager.py:
+    2250-2400) and processConditions / _addBcValue (2527-2567), in that order.
+    Returns float32[16] (center, primary, radius, angle, mass, inertia, V,
+    angular velocity, BC translation value, gravity, BC rotation value) and
+    int32[3] (type, BC bits, considerContact)."""
+    r = dom.rigid
+    f = np.zeros(16, np.float32)
+    for ic in dom.initials:
+        ids = [0] if getattr(ic, "is_all_nodes", False) else [int(n) for n in np.asarray(ic.nds).reshape(-1)]
+        if ids != [0]:
+            raise NotImplementedError("a rigid body's initial condition must name index 0 (or 'ALL')")
+        if ic.type in (VTYPE, ATYPE):
+            f[8], f[9] = _as_vec2(ic.vel)
+        else:
+            f[10] = _as_float(ic.ang_vel)
+    ref = np.asarray(r.getRefPoint(), np.float32).reshape(-1)
+    f[0], f[1] = _as_vec2(ref)
+    f[6] = _as_float(r.mass)
+    if r.rtype == RigidType.BALL:
+        f[4] = _as_float(r.getRadius())
+    elif r.rtype == RigidType.BOX:
+        f[2], f[3] = _as_vec2(r.getPrimary())
+    elif r.rtype == RigidType.CAPSULE:
+        f[2], f[3] = _as_vec2(r.getPrimary() - r.getRefPoint())
+        f[4] = _as_float(r.getRadius())
+    f[5] = _as_float(r.angle)
+    f[7] = float(r.inertia_body)
+    bits = 0
+    for bc in dom.bcs:
+        t, _, value = bc.processData()
+        t = int(t)
+        bits |= t
+        if t == UTYPE:
+            f[11:13] = 0.0
+            f[6] = 1e10
+        elif t == RTYPE:
+            f[11:13] = 0.0
+            f[6] = 1e10
+            f[7] = 1e10
+            f[15] = 0.0
+        elif t == VTYPE:
+            f[11], f[12] = _as_vec2(value)
+            f[6] = 1e10
+        elif t == ROTVTYPE:
+            f[15] = _as_float(value)
+            f[7] = 1e10
+        elif t in (ROTATYPE, TORQUETYPE):
+            f[15] = _as_float(value)
+        elif t == GRAVITY:
+            f[13], f[14] = _as_vec2(value)
+        else:  # ATYPE, FORCETYPE
+            f[11], f[12] = _as_vec2(value)
+    return f, np.array([int(r.rtype), bits, 1 if dom.considerContact else 0], np.int32)
 
 
 def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):

@@ -39,6 +39,7 @@ extern "C" {
 #define FW_ERR_TIMEOUT -4   /* a bounded device wait gave up */
 #define FW_ERR_NONFINITE -5 /* a NaN/inf was found in the state */
 #define FW_ERR_STATE -6     /* call out of order (e.g. step before finalize) */
+#define FW_ERR_UNSUPPORTED -7 /* the world reached a state outside the library (rigid-rigid / rigid-ground contact) */
 
 /* Node boundary-condition bits: same values as the reference's
  * flatworld/definitions.py:96-104. */
@@ -181,6 +182,43 @@ int fw_mass_scaling(fw_ctx* ctx, float dt_target);
  * reference keeps these in bc_flex_cache_elem and SpatialHashManager
  * (mixedcontact.py:1915, spatialmanager.py:538-551); here for tests. */
 int fw_read_flex_state(fw_ctx* ctx, int32_t* item_cache, int32_t n_items, float* grid);
+
+/* Rigid primitives touching FEM bodies (RigidBodyDomain with BallRigid /
+ * BoxRigid / CapsuleRigid), before fw_finalize, single-scene worlds, gather
+ * path.  Per rigid 16 floats -- center x, y; primary x, y (box: full extents;
+ * capsule: lower end minus center); radius; angle; mass; inertia; velocity x,
+ * y; angular velocity; BC translation value x, y; gravity x, y; BC rotation
+ * value -- and 3 ints: RigidType (1 ball, 2 box, 8 capsule), BC bits
+ * (definitions.py:96-104) and considerContact.  grounds: 5 floats per ground
+ * domain -- kind 0 (plane): point x, y, normal x, y; kind 1 (height field,
+ * voxel grid): box lb x, y, ub x, y.  A rigid that comes within 0.01 of a
+ * ground (20x the reference's rigid-ground contact margin) or of another
+ * contact rigid's box at an update makes the next synchronising call return
+ * FW_ERR_UNSUPPORTED.
+ * Replaces RigidManager.processDomains_ / packRigidParams / processConditions
+ * and precompute_rigid_transforms + updateBBox, rigidmanager.py:2448-2598,
+ * 4001-4015, 4643-4662, explicitloop.py:198-201. */
+int fw_set_rigids(fw_ctx* ctx, int32_t n, const float* params, const int32_t* ints, int32_t n_ground,
+                  const float* grounds);
+/* One FEM-rigid pair (ContactFlexRigid, femcontact.py:173-179): the body's
+ * boundary nodes against the rigid, penalty 2K of the body, the rigid's
+ * friction; skip_bvh: the loop activates the pair by plain box overlap
+ * (mixedcontact.py:1697-1713, 474-492) instead of the broad phase.  Add in the
+ * reference's launch order: plane pairs, rigid pairs (contact order), height
+ * field, voxel.  Replaces _build_batched_contacts' rigid work lists and
+ * _batched_rigid_prim_kernel, mixedcontact.py:1963-2130, 1026-1115. */
+int fw_add_rigid_pair(fw_ctx* ctx, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh);
+/* The rigid update schedule of the coming substeps: the rigids move every
+ * `every` substeps by dt (the reference's N = max(1, 1e-3 // dt) and N * dt,
+ * explicitloop.py:533-538, computed by the caller from its float64 dt), with
+ * the loop's damping.  After fw_finalize. */
+int fw_set_rigid_clock(fw_ctx* ctx, int32_t every, float dt, float damping);
+/* Per rigid 12 floats: center x, y, angle, velocity x, y, angular velocity,
+ * displacement x, y, box lb x, y, ub x, y; *flags (may be NULL): bit 0 set
+ * once a rigid met a ground or another rigid.  The reference's
+ * getCurrentRefPoint / getCurrentRefAngles / getCurrentVelocity / getBBox,
+ * rigiddomain.py:128-155. */
+int fw_read_rigids(fw_ctx* ctx, float* out, int32_t* flags);
 
 /* Upload, precompute reference-shape data (area, Dm^-1, lumped mass, Lame
  * constants, node->element gather lists) and run the zero-dt step that the

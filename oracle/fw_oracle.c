@@ -172,6 +172,7 @@ typedef struct {
   int32_t *csr_off, *csr_slot;
   REAL* corner; /* 6 per element */
   struct or_flex* flex; /* FEM-FEM contact, NULL when the loop has none */
+  struct or_rigids* rig; /* rigid primitives, NULL when the loop has none */
 } or_world;
 
 static REAL* dupf(const float* src, size_t n) {
@@ -1000,6 +1001,339 @@ static void flex_contacts(or_world* w, long counter) {
   free(stamped);
 }
 
+/* ------------------------------------------------ FEM-rigid (primitives) */
+
+/* sin and cos of the FP32 builds, from IEEE + - * only, so that the CUDA
+ * kernels evaluating the same operations in the same order give the same bits
+ * (the reference's wp.sin / wp.cos are the platform's; any accurate pair is a
+ * faithful reading).  Method: Cody-Waite reduction x = k pi/2 + r with pi/2
+ * split into 1.5703125 + 0x1.fb4p-12 + 0x1.4442d2p-24 (the first two short
+ * enough that k times them is exact for |k| < 2^13), then the Taylor series of
+ * sin through r^9 and of cos through r^10 on |r| <= pi/4 (truncation error
+ * below 2e-9), and the quadrant k mod 4. */
+static void or_sincosf(float x, float* s_out, float* c_out) {
+  const float k = floorf(x * 0.63661975f + 0.5f);
+  const float r = ((x - k * 1.5703125f) - k * 4.837512969970703125e-4f) - k * 0x1.4442d2p-24f;
+  const float z = r * r;
+  const float sp = -1.0f / 6.0f + z * (1.0f / 120.0f + z * (-1.0f / 5040.0f + z * (1.0f / 362880.0f)));
+  const float sr = r + r * z * sp;
+  const float cp = -0.5f + z * (1.0f / 24.0f + z * (-1.0f / 720.0f + z * (1.0f / 40320.0f + z * (-1.0f / 3628800.0f))));
+  const float cr = 1.0f + z * cp;
+  const int q = ((int)k) & 3;
+  *s_out = q == 0 ? sr : q == 1 ? cr : q == 2 ? -sr : -cr;
+  *c_out = q == 0 ? cr : q == 1 ? -sr : q == 2 ? -cr : sr;
+}
+
+static void r_sincos(REAL x, REAL* s, REAL* c) {
+#if defined(REAL_IS_DOUBLE)
+  *s = sin(x);
+  *c = cos(x);
+#else
+  or_sincosf(x, s, c);
+#endif
+}
+
+/* RigidType (flatworld/definitions.py:50-53) */
+#define RIGID_BALL 1
+#define RIGID_BOX 2
+#define RIGID_CAPSULE 8
+/* rigid BC bits (definitions.py:96-104) */
+#define RBC_U 0x1
+#define RBC_V 0x2
+#define RBC_A 0x4
+#define RBC_FORCE 0x8
+#define RBC_GRAVITY 0x10
+#define RBC_R 0x20
+#define RBC_ROTV 0x40
+#define RBC_ROTA 0x80
+#define RBC_TORQUE 0x100
+
+typedef struct {
+  int type, bc, in_contact;
+  REAL c[2], prim[2], radius, quat, mass, inertia;
+  REAL V[2], W, bcT[2], bcG[2], bcR, U[2];
+  REAL rot[4]; /* cached_rotation_matrix (row-major), refreshed by the velocity pass */
+  REAL acc[2], accw;
+  REAL lb[2], ub[2];
+} or_rigid;
+
+typedef struct or_rigids {
+  int n, n_ground, err;
+  or_rigid* r;
+  REAL* gbox;  /* static grounds, 4 per ground: plane p x, y, n x, y or box lb x, y, ub x, y */
+  int* gkind; /* 0: plane, 1: box (height field, voxel grid) */
+  /* work items, reference order: per rigid pair its FEM body's boundary nodes */
+  int n_rp;
+  int *rp_body, *rp_rigid, *rp_skip;
+  REAL *rp_pen, *rp_fric;
+} or_rigids;
+
+/* cal2DRotationMat (flatworld/utils.py:7-11): [[c, -s], [s, c]]. */
+static void rot_of(REAL theta, REAL* m) {
+  REAL s, c;
+  r_sincos(theta, &s, &c);
+  m[0] = c; m[1] = -s; m[2] = s; m[3] = c;
+}
+
+/* _write_primitive_aabb (rigidmanager.py:766-794) with getBallBBox,
+ * getBoxBBox, getCapsuleBBox (utils.py:235-300). */
+static void rigid_aabb(or_rigid* g) {
+  const REAL* m = g->rot;
+  if (g->type == RIGID_BALL) {
+    g->lb[0] = g->c[0] - g->radius; g->lb[1] = g->c[1] - g->radius;
+    g->ub[0] = g->c[0] + g->radius; g->ub[1] = g->c[1] + g->radius;
+  } else if (g->type == RIGID_BOX) {
+    const REAL ex = g->prim[0], ey = g->prim[1];
+    REAL px[4], py[4];
+    const REAL vx[4] = {ex, ex, ex, -ex}, vy[4] = {ey, -ey, ey, ey};
+    const REAL sc[4] = {(REAL)-0.5, (REAL)0.5, (REAL)0.5, (REAL)0.5};
+    for (int k = 0; k < 4; ++k) {
+      const REAL rx = m[0] * vx[k] + m[1] * vy[k], ry = m[2] * vx[k] + m[3] * vy[k];
+      px[k] = g->c[0] + sc[k] * rx;
+      py[k] = g->c[1] + sc[k] * ry;
+    }
+    g->lb[0] = rmin(rmin(px[0], px[1]), rmin(px[2], px[3]));
+    g->lb[1] = rmin(rmin(py[0], py[1]), rmin(py[2], py[3]));
+    g->ub[0] = rmax(rmax(px[0], px[1]), rmax(px[2], px[3]));
+    g->ub[1] = rmax(rmax(py[0], py[1]), rmax(py[2], py[3]));
+  } else if (g->type == RIGID_CAPSULE) {
+    const REAL ax = g->prim[0], ay = g->prim[1];
+    const REAL alen = R_SQRT(ax * ax + ay * ay);
+    const REAL d0 = ax / alen, d1 = ay / alen;
+    const REAL dx = m[0] * d0 + m[1] * d1, dy = m[2] * d0 + m[3] * d1;
+    const REAL p0x = g->c[0] - dx * alen, p0y = g->c[1] - dy * alen;
+    const REAL p1x = g->c[0] + dx * alen, p1y = g->c[1] + dy * alen;
+    const REAL perp0 = g->radius * R_SQRT(rmax((REAL)0.0, (REAL)1.0 - dx * dx)), axial0 = g->radius * R_FABS(dx);
+    const REAL perp1 = g->radius * R_SQRT(rmax((REAL)0.0, (REAL)1.0 - dy * dy)), axial1 = g->radius * R_FABS(dy);
+    g->lb[0] = rmin(p0x, p1x) - perp0 - axial0;
+    g->lb[1] = rmin(p0y, p1y) - perp1 - axial1;
+    g->ub[0] = rmax(p0x, p1x) + perp0 + axial0;
+    g->ub[1] = rmax(p0y, p1y) + perp1 + axial1;
+  }
+}
+
+/* detectPointToPrimitive (contact_detection.py:148-190) with sphereSDFQuery,
+ * capsuleSDFQuery, obbSDFQuery and calMinDisNode2Segment (utils.py:34-145). */
+static REAL detect_prim(const or_rigid* g, REAL px, REAL py, REAL* nx, REAL* ny, REAL* cx, REAL* cy) {
+  REAL pen = (REAL)1e9, n0 = 0, n1 = 0;
+  const REAL* m = g->rot;
+  if (g->type == RIGID_BALL) {
+    const REAL qx = px - g->c[0], qy = py - g->c[1];
+    const REAL len = R_SQRT(qx * qx + qy * qy);
+    pen = len - g->radius;
+    const REAL dn = rmax(len, (REAL)1e-9);
+    n0 = qx / dn;
+    n1 = qy / dn;
+  } else if (g->type == RIGID_BOX) {
+    const REAL hx = (REAL)0.5 * g->prim[0], hy = (REAL)0.5 * g->prim[1];
+    const REAL wx = px - g->c[0], wy = py - g->c[1];
+    const REAL lx = m[0] * wx + m[2] * wy, ly = m[1] * wx + m[3] * wy; /* transpose(rot) @ w */
+    const REAL sd0 = lx - hx, sd1 = -lx - hx, sd2 = ly - hy, sd3 = -ly - hy;
+    REAL best = (REAL)-1e9, ln0 = 0, ln1 = 0;
+    if (sd0 > best) { best = sd0; ln0 = 1; ln1 = 0; }
+    if (sd1 > best) { best = sd1; ln0 = -1; ln1 = 0; }
+    if (sd2 > best) { best = sd2; ln0 = 0; ln1 = 1; }
+    if (sd3 > best) { best = sd3; ln0 = 0; ln1 = -1; }
+    if (sd0 > 0 || sd1 > 0 || sd2 > 0 || sd3 > 0) {
+      REAL qx = lx, qy = ly;
+      if (lx < -hx) qx = -hx; else if (lx > hx) qx = hx;
+      if (ly < -hy) qy = -hy; else if (ly > hy) qy = hy;
+      const REAL ddx = lx - qx, ddy = ly - qy;
+      const REAL dist = R_SQRT(ddx * ddx + ddy * ddy);
+      if (dist > (REAL)1e-9) { ln0 = ddx / dist; ln1 = ddy / dist; }
+      best = dist;
+    }
+    pen = best;
+    n0 = m[0] * ln0 + m[1] * ln1;
+    n1 = m[2] * ln0 + m[3] * ln1;
+  } else if (g->type == RIGID_CAPSULE) {
+    const REAL lcx = g->c[0] + (m[0] * g->prim[0] + m[1] * g->prim[1]);
+    const REAL lcy = g->c[1] + (m[2] * g->prim[0] + m[3] * g->prim[1]);
+    const REAL qx = (REAL)2.0 * g->c[0] - lcx, qy = (REAL)2.0 * g->c[1] - lcy;
+    const REAL apx = px - lcx, apy = py - lcy, abx = qx - lcx, aby = qy - lcy;
+    const REAL ab2 = abx * abx + aby * aby;
+    REAL t = (apx * abx + apy * aby) / ab2;
+    t = rmax((REAL)0.0, rmin((REAL)1.0, t));
+    const REAL clx = lcx + t * abx, cly = lcy + t * aby;
+    const REAL ex = px - clx, ey = py - cly;
+    const REAL dist = R_SQRT(ex * ex + ey * ey);
+    pen = dist - g->radius;
+    const REAL dn = rmax(dist, (REAL)1e-9);
+    n0 = ex / dn;
+    n1 = ey / dn;
+  }
+  *nx = n0;
+  *ny = n1;
+  *cx = px;
+  *cy = py;
+  if (pen < (REAL)0.0) {
+    *cx = px - n0 * pen;
+    *cy = py - n1 * pen;
+  }
+  return pen;
+}
+
+/* Gate of a FEM-rigid pair: the broad phase on the FEM body's box and the
+ * rigid's current box (bvh.py rules as pair_active), or the plain box overlap
+ * of _activate_pairs_by_aabb_kernel (mixedcontact.py:474-492) when the loop
+ * skips the BVH. */
+static int rigid_pair_active(const or_world* w, int body, const or_rigid* g, int skip, long counter) {
+  const REAL* bb = w->aabb + 4 * body;
+  REAL alo[2] = {bb[0], bb[1]}, ahi[2] = {bb[2], bb[3]};
+  REAL blo[2] = {g->lb[0], g->lb[1]}, bhi[2] = {g->ub[0], g->ub[1]};
+  if (!skip && counter % 100 == 0) {
+    for (int k = 0; k < 2; ++k) {
+      REAL ba = (REAL)0.1 * (ahi[k] - alo[k]);
+      REAL bbuf = (REAL)0.1 * (bhi[k] - blo[k]);
+      alo[k] = alo[k] - ba; ahi[k] = ahi[k] + ba;
+      blo[k] = blo[k] - bbuf; bhi[k] = bhi[k] + bbuf;
+    }
+  }
+  return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
+}
+
+/* _batched_rigid_prim_kernel (mixedcontact.py:1026-1115), untied branch, its
+ * work items serially in order; the reaction impulse and torque of each hit
+ * are added to the rigid's accumulators in that order. */
+static void rigid_contacts(or_world* w, REAL dt, long counter) {
+  or_rigids* R = w->rig;
+  if (!R) return;
+  for (int pi = 0; pi < R->n_rp; ++pi) {
+    or_rigid* g = &R->r[R->rp_rigid[pi]];
+    const int body = R->rp_body[pi];
+    if (!rigid_pair_active(w, body, g, R->rp_skip[pi], counter)) continue;
+    const REAL k = R->rp_pen[pi], mu = R->rp_fric[pi];
+    const int off = w->bn_off[body], cnt = w->bn_cnt[body];
+    for (int q = 0; q < cnt; ++q) {
+      const int nid = w->bnodes[off + q];
+      const REAL px = w->x[2 * nid], py = w->x[2 * nid + 1];
+      if (rmin(px - g->lb[0], py - g->lb[1]) < (REAL)0.0 || rmin(g->ub[0] - px, g->ub[1] - py) < (REAL)0.0) continue;
+      REAL nx, ny, cx, cy;
+      const REAL pen = detect_prim(g, px, py, &nx, &ny, &cx, &cy);
+      const REAL gx = g->ub[0] - g->lb[0], gy = g->ub[1] - g->lb[1];
+      const REAL margin = R_SQRT(gx * gx + gy * gy) * (REAL)0.5;
+      if (!(pen < margin)) continue;
+      const REAL depth = pen - (REAL)1e-4;
+      if (!(depth < (REAL)0.0)) continue;
+      const REAL fnx = -nx * k * depth, fny = -ny * k * depth;
+      REAL tx = fnx, ty = fny;
+      if (mu > (REAL)1e-9) {
+        const REAL rx = cx - g->c[0], ry = cy - g->c[1];
+        const REAL svx = g->V[0] + -g->W * ry, svy = g->V[1] + g->W * rx;
+        const REAL relx = w->v[2 * nid] - svx, rely = w->v[2 * nid + 1] - svy;
+        const REAL rn = relx * nx + rely * ny;
+        const REAL tgx = relx - rn * nx, tgy = rely - rn * ny;
+        const REAL tlen = R_SQRT(tgx * tgx + tgy * tgy);
+        if (tlen > (REAL)1e-9) {
+          const REAL dx = -tgx / tlen, dy = -tgy / tlen;
+          const REAL fn = R_SQRT(fnx * fnx + fny * fny);
+          tx = tx + dx * mu * fn;
+          ty = ty + dy * mu * fn;
+        }
+      }
+      w->fext[2 * nid] += tx;
+      w->fext[2 * nid + 1] += ty;
+      g->acc[0] += -tx * dt;
+      g->acc[1] += -ty * dt;
+      const REAL lx = cx - g->c[0], ly = cy - g->c[1];
+      const REAL fx = -tx, fy = -ty;
+      g->accw += (lx * fy - ly * fx) * dt;
+    }
+  }
+}
+
+/* Clearance below which a rigid counts as meeting a ground or another rigid:
+ * 20x the reference's speculative rigid-ground contact margin (0.0005,
+ * rigidmanager.py:3257), so that every state where the reference's constraint
+ * solve could see a contact row is flagged. */
+#define RIGID_CLEARANCE 0.01
+
+/* The rigid bodies' part of RigidManager.substep (rigidmanager.py:2102-2197)
+ * for worlds without rigid-rigid / rigid-ground contact and joints (no
+ * constraint solve): _rigid_step_wp (832-891) then _update_u_and_bbox_wp
+ * (894-964).  A rigid within RIGID_CLEARANCE of a ground plane (its box's
+ * support point, as _detect_analytical_prim_contacts_wp's early out measures
+ * it, rigidmanager.py:1127-1136), of a height-field / voxel box, or of another
+ * contact rigid's box sets the error flag: such a world needs the solver. */
+void or_rigid_update(or_world* w, float dt_f, float damping_f) {
+  or_rigids* R = w->rig;
+  if (!R) return;
+  const REAL dt = (REAL)dt_f, damping = (REAL)damping_f, cl = (REAL)RIGID_CLEARANCE;
+  for (int a = 0; a < R->n; ++a) {
+    const or_rigid* g = &R->r[a];
+    for (int q = 0; q < R->n_ground; ++q) {
+      const REAL* b = R->gbox + 4 * q;
+      if (R->gkind[q] == 0) {
+        const REAL sx = b[2] < 0 ? g->ub[0] : g->lb[0], sy = b[3] < 0 ? g->ub[1] : g->lb[1];
+        if ((sx - b[0]) * b[2] + (sy - b[1]) * b[3] <= cl) R->err = 1;
+      } else if (g->lb[0] - cl <= b[2] && g->ub[0] + cl >= b[0] && g->lb[1] - cl <= b[3] && g->ub[1] + cl >= b[1]) {
+        R->err = 1;
+      }
+    }
+    for (int q = a + 1; q < R->n; ++q) {
+      const or_rigid* h = &R->r[q];
+      if (g->in_contact && h->in_contact && g->lb[0] - cl <= h->ub[0] && g->ub[0] + cl >= h->lb[0] &&
+          g->lb[1] - cl <= h->ub[1] && g->ub[1] + cl >= h->lb[1])
+        R->err = 1;
+    }
+  }
+  for (int a = 0; a < R->n; ++a) { /* _rigid_step_wp */
+    or_rigid* g = &R->r[a];
+    rot_of(g->quat, g->rot);
+    if (g->bc & RBC_A) {
+      g->acc[0] = 0; g->acc[1] = 0;
+    } else {
+      if (g->bc & RBC_GRAVITY) {
+        g->acc[0] = g->acc[0] + g->mass * g->bcG[0] * dt;
+        g->acc[1] = g->acc[1] + g->mass * g->bcG[1] * dt;
+      }
+      if (g->bc & RBC_FORCE) {
+        g->acc[0] = g->acc[0] + g->bcT[0] * dt;
+        g->acc[1] = g->acc[1] + g->bcT[1] * dt;
+      }
+    }
+    if (g->bc & RBC_ROTA) g->accw = 0;
+    else if (g->bc & RBC_TORQUE) g->accw = g->accw + g->bcR * dt;
+    g->V[0] = g->V[0] + g->acc[0] / g->mass;
+    g->V[1] = g->V[1] + g->acc[1] / g->mass;
+    g->W = g->W + g->accw / (g->inertia + (REAL)1e-6);
+    const REAL damp = rmax((REAL)0.0, (REAL)1.0 - damping * dt);
+    g->V[0] = g->V[0] * damp;
+    g->V[1] = g->V[1] * damp;
+    g->W = g->W * damp;
+  }
+  for (int a = 0; a < R->n; ++a) {
+    or_rigid* g = &R->r[a];
+    if (g->bc & RBC_A) {
+      g->V[0] = g->V[0] + g->bcT[0] * dt;
+      g->V[1] = g->V[1] + g->bcT[1] * dt;
+    }
+    if (g->bc & RBC_ROTA) g->W = g->W + g->bcR * dt;
+  }
+  for (int a = 0; a < R->n; ++a) { /* _update_u_and_bbox_wp */
+    or_rigid* g = &R->r[a];
+    if (g->bc & RBC_V) {
+      g->V[0] = g->bcT[0]; g->V[1] = g->bcT[1];
+    } else if (g->bc & RBC_U) {
+      g->V[0] = 0; g->V[1] = 0;
+    } else if (g->bc & RBC_R) {
+      g->V[0] = 0; g->V[1] = 0;
+      g->W = 0;
+    }
+    if (g->bc & RBC_ROTV) g->W = g->bcR;
+    const REAL dux = g->V[0] * dt, duy = g->V[1] * dt;
+    g->U[0] = g->U[0] + dux; g->U[1] = g->U[1] + duy;
+    g->c[0] = g->c[0] + dux; g->c[1] = g->c[1] + duy;
+    g->quat = g->quat + g->W * dt;
+    if (g->quat > (REAL)3.141592653589793) g->quat = g->quat - (REAL)2.0 * (REAL)3.141592653589793;
+    else if (g->quat < (REAL)-3.141592653589793) g->quat = g->quat + (REAL)2.0 * (REAL)3.141592653589793;
+  }
+  for (int a = 0; a < R->n; ++a) {
+    R->r[a].acc[0] = 0; R->r[a].acc[1] = 0; R->r[a].accw = 0;
+  }
+  for (int a = 0; a < R->n; ++a) rigid_aabb(&R->r[a]);
+}
+
 /* ---------------------------------------------------------------- C API */
 
 or_world* or_create(int n_nodes, const float* x, const float* v, const int32_t* bc, const float* bcv,
@@ -1235,6 +1569,7 @@ void or_step(or_world* w, float dt_f, float damping_f, long counter, int init_st
   if (!init_step) {
     contacts(w, dt, counter, 1);
     flex_contacts(w, counter);
+    rigid_contacts(w, dt, counter); /* mixedcontact.py:1697-1715: after FEM-FEM, before height fields */
     contacts(w, dt, counter, 0);
   }
   if (w->n_threads <= 1) {
@@ -1324,6 +1659,73 @@ void or_point_stress(int type, float E, float nu, float sy, float H, const float
 /* The oracle's FP32 log, exported for its accuracy test. */
 float or_log32(float x) { return R_LOG(x); }
 
+/* Rigid primitives (RigidManager.packRigidParams / processConditions,
+ * rigidmanager.py:2250-2400, 2527-2567): per rigid 16 floats (center x, y,
+ * primary x, y, radius, angle, mass, inertia, V x, y, angular velocity, BC
+ * translation value x, y, gravity x, y, BC rotation value) and 3 ints (type,
+ * BC bits, considerContact); the static grounds, 5 floats each (kind 0 plane:
+ * p x, y, n x, y; kind 1 box: lb x, y, ub x, y).  The
+ * rotation cache and boxes are set as precompute_rigid_transforms + updateBBox
+ * do at loop construction (explicitloop.py:198-201). */
+int or_set_rigids(or_world* w, int n, const float* f, const int32_t* iv, int n_ground, const float* grounds) {
+  or_rigids* R = (or_rigids*)calloc(1, sizeof(or_rigids));
+  R->n = n;
+  R->r = (or_rigid*)calloc((size_t)(n ? n : 1), sizeof(or_rigid));
+  for (int a = 0; a < n; ++a) {
+    or_rigid* g = &R->r[a];
+    const float* q = f + 16 * a;
+    g->type = iv[3 * a]; g->bc = iv[3 * a + 1]; g->in_contact = iv[3 * a + 2];
+    g->c[0] = q[0]; g->c[1] = q[1]; g->prim[0] = q[2]; g->prim[1] = q[3];
+    g->radius = q[4]; g->quat = q[5]; g->mass = q[6]; g->inertia = q[7];
+    g->V[0] = q[8]; g->V[1] = q[9]; g->W = q[10];
+    g->bcT[0] = q[11]; g->bcT[1] = q[12]; g->bcG[0] = q[13]; g->bcG[1] = q[14]; g->bcR = q[15];
+    rot_of(g->quat, g->rot);
+    rigid_aabb(g);
+  }
+  R->n_ground = n_ground;
+  R->gbox = (REAL*)calloc(4 * (size_t)(n_ground ? n_ground : 1), sizeof(REAL));
+  R->gkind = (int*)calloc((size_t)(n_ground ? n_ground : 1), sizeof(int));
+  for (int q = 0; q < n_ground; ++q) {
+    R->gkind[q] = (int)grounds[5 * q];
+    for (int k = 0; k < 4; ++k) R->gbox[4 * q + k] = grounds[5 * q + 1 + k];
+  }
+  w->rig = R;
+  return 0;
+}
+
+/* One FEM-rigid pair (its work items: the body's boundary nodes), added in
+ * the reference's rigid-contact order (mixedcontact.py:1987-2030). */
+int or_add_rigid_pair(or_world* w, int body, int rigid, float penalty, float friction, int skip_bvh) {
+  or_rigids* R = w->rig;
+  if (!R || rigid < 0 || rigid >= R->n || body < 0 || body >= w->n_bodies) return -1;
+  const int k = R->n_rp++;
+  R->rp_body = (int*)realloc(R->rp_body, sizeof(int) * R->n_rp);
+  R->rp_rigid = (int*)realloc(R->rp_rigid, sizeof(int) * R->n_rp);
+  R->rp_skip = (int*)realloc(R->rp_skip, sizeof(int) * R->n_rp);
+  R->rp_pen = (REAL*)realloc(R->rp_pen, sizeof(REAL) * R->n_rp);
+  R->rp_fric = (REAL*)realloc(R->rp_fric, sizeof(REAL) * R->n_rp);
+  R->rp_body[k] = body; R->rp_rigid[k] = rigid; R->rp_skip[k] = skip_bvh;
+  R->rp_pen[k] = penalty; R->rp_fric[k] = friction;
+  return 0;
+}
+
+/* Per rigid 12 doubles: center x, y, angle, V x, y, angular velocity, U x, y,
+ * box lb x, y, ub x, y.  Returns the error flag of the update pass. */
+int or_get_rigids(const or_world* w, double* out) {
+  const or_rigids* R = w->rig;
+  if (!R) return 0;
+  for (int a = 0; a < R->n; ++a) {
+    const or_rigid* g = &R->r[a];
+    double* o = out + 12 * a;
+    o[0] = g->c[0]; o[1] = g->c[1]; o[2] = g->quat; o[3] = g->V[0]; o[4] = g->V[1]; o[5] = g->W;
+    o[6] = g->U[0]; o[7] = g->U[1]; o[8] = g->lb[0]; o[9] = g->lb[1]; o[10] = g->ub[0]; o[11] = g->ub[1];
+  }
+  return R->err;
+}
+
+void or_sincos32(float x, float* s, float* c) { or_sincosf(x, s, c); }
+
+
 void or_destroy(or_world* w) {
   if (!w) return;
   free(w->x); free(w->v); free(w->u); free(w->fext); free(w->mass); free(w->bc); free(w->bcv);
@@ -1336,6 +1738,12 @@ void or_destroy(or_world* w) {
   }
   free(w->pairs);
   free(w->csr_off); free(w->csr_slot); free(w->corner);
+  if (w->rig) {
+    or_rigids* R = w->rig;
+    free(R->r); free(R->gbox); free(R->gkind); free(R->rp_body); free(R->rp_rigid); free(R->rp_skip); free(R->rp_pen);
+    free(R->rp_fric);
+    free(R);
+  }
   if (w->flex) {
     or_flex* f = w->flex;
     free(f->item_node); free(f->item_target); free(f->item_be_off); free(f->item_be_cnt);

@@ -21,6 +21,11 @@ recomputed here with the reference's own loops:
   flatworld/explicitloop.py:203-227, 362-373, 383-385  BVH objects, skip_bvh,
                                            initial FEM spatial hash
   flatworld/femspringmanager.py:523-524, 1035-1039  hash refresh every 1/500 s
+  flatworld/femcontact.py:173-179          ContactFlexRigid penalty, stable time
+  flatworld/mixedcontact.py:1963-2054      FEM-rigid work items (friction of the rigid)
+  flatworld/rigiddomain.py:118-124, rigidmanager.py:2250-2400, 2448-2567
+                                           rigid packing, BCs, initial conditions
+  flatworld/explicitloop.py:533-538        rigid update every max(1, 1e-3 // dt) substeps
 Domain objects are read through the reference's attribute names only
 (mesh.coords, mesh.connectivity, prop.mat, bcs, initials, point, normal,
 height, lb, ub, reverse, occ, nx, ny, dx, dz, considerContact, type, ...).
@@ -40,6 +45,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 FEM, ANALYTICAL, RIGID, SPRINGMASS, HEIGHTFIELD, VOXELMAP = 0b10, 0b1, 0b100, 0b1000, 0b100000, 0b1000000
 FLEXANLAYTICAL, FLEXFLEX, FEXHEIGHTFIELD, FLEXVOXELMAP = 0b11, 0b10, 0b100010, 0b1000010
 FLEXSPRING, ANALYTICALSPRING, SPRINGHEIGHTFIELD = 0b1010, 0b1001, 0b101000
+FLEXRIGID = 0b110
 RIGIDRIGID, RIGIDANLAYTICAL, ANALYTICALANALYTICAL = 0b100, 0b101, 0b1
 
 _LIBS = {}
@@ -84,6 +90,12 @@ def _lib(precision: str):
         L.or_destroy.argtypes = [C.c_void_p]
         L.or_log32.argtypes = [C.c_float]
         L.or_log32.restype = C.c_float
+        L.or_set_rigids.argtypes = [C.c_void_p, C.c_int, _f32p, _i32p, C.c_int, _f32p]
+        L.or_add_rigid_pair.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int]
+        L.or_rigid_update.argtypes = [C.c_void_p, C.c_float, C.c_float]
+        L.or_get_rigids.argtypes = [C.c_void_p, _f64p]
+        L.or_get_rigids.restype = C.c_int
+        L.or_sincos32.argtypes = [C.c_float, _f32p, _f32p]
         _LIBS[name] = L
     return _LIBS[name]
 
@@ -159,6 +171,13 @@ def log32(x, precision="f32"):
     return float(_lib(precision).or_log32(float(x)))
 
 
+def sincos32(x):
+    """The FP32 (sin, cos) the oracle and the CUDA rigid update use."""
+    sv, cv = C.c_float(), C.c_float()
+    _lib("f32").or_sincos32(float(x), C.byref(sv), C.byref(cv))
+    return sv.value, cv.value
+
+
 class OracleLoop:
     """CPU restatement of one reference ExplicitLoop over FEM + ground domains."""
 
@@ -207,6 +226,11 @@ class OracleLoop:
                         spr, fd = (di, dj) if di.type == SPRINGMASS else (dj, di)
                         pen = min(spr.spring, self._seg_penalty(fd)) * 100.0
                         contacts.append((FLEXSPRING, spr, fd, pen, self._contact_stable(pen, fd, fem)))
+                        continue
+                    if ct == FLEXRIGID:  # ContactFlexRigid: domain1 = the FEM side
+                        femd, rig = (di, dj) if di.type == FEM else (dj, di)
+                        pen = self._seg_penalty(femd) * 1.0
+                        contacts.append((ct, femd, rig, pen, self._contact_stable(pen, femd, fem)))
                         continue
                     if ct == FLEXFLEX:  # ContactFlexFlex(dom_i, dom_j): domain1 = i, domain2 = j
                         pen = min(self._seg_penalty(di), self._seg_penalty(dj)) * 1.0
@@ -332,6 +356,33 @@ class OracleLoop:
                 L.or_add_voxel(self._w, body, pen32, lo[1], hi[1], int(g.nx), int(g.ny), occ[1], float(g.lb[0]),
                                float(g.lb[1]), float(np.float32(g.dx)), float(np.float32(g.dz)))
         self.flex = flex
+        # explicitloop.py:222-228, 362-373: no broad phase with <= 1 contact
+        # domain; it is skipped without ground contact and with <= 1 contact rigid
+        rigid_doms = [d for d in domains if d.type == RIGID]
+        rigid_needs_bvh = sum(1 for d in rigid_doms if d.considerContact) > 1
+        no_bvh = len(cds) <= 1
+        skip_bvh = 1 if (no_bvh or ((len(anal) + len(hf) + len(vox) + unbatched) == 0 and not rigid_needs_bvh)) else 0
+        self.rigids = rigid_doms
+        self.rigid_update_times = 0
+        if rigid_doms:
+            prm = np.zeros((len(rigid_doms), 16), np.float32)
+            ivs = np.zeros((len(rigid_doms), 3), np.int32)
+            for a, d in enumerate(rigid_doms):
+                self._pack_rigid(d, prm[a], ivs[a])
+            gb = []
+            for g in domains:  # plane (kind 0): point, normal; height field / voxel (kind 1): its box
+                if g.type == ANALYTICAL:
+                    gb.append([0.0, *np.asarray(g.point, np.float32)[:2], *np.asarray(g.normal, np.float32)[:2]])
+                elif g.type in (HEIGHTFIELD, VOXELMAP):
+                    gb.append([1.0, *self._ground_box(g)[0][0], *self._ground_box(g)[1][0]])
+            gbox = _fp(np.asarray(gb, np.float32).reshape(-1, 5))
+            rp, ri = _fp(prm), _ip(ivs)
+            self._keep += [rp, ri, gbox]
+            L.or_set_rigids(self._w, len(rigid_doms), rp[1], ri[1], len(gb), gbox[1])
+            for ct, femd, rig, pen, _ in contacts:
+                if ct == FLEXRIGID:
+                    L.or_add_rigid_pair(self._w, fem.index(femd), rigid_doms.index(rig), float(np.float32(pen)),
+                                        float(np.float32(rig.friction)), skip_bvh)
         if flex:
             # boundary edges per fem domain, global node ids, mesh order
             edges, be_off, be_cnt = [], [], []
@@ -349,7 +400,6 @@ class OracleLoop:
                     lo, hi = self._ground_box(d)
                     dom_box[i, :2] = lo[0]
                     dom_box[i, 2:] = hi[0]
-            skip_bvh = 1 if (len(anal) + len(hf) + len(vox) + unbatched) == 0 else 0
             ea, eo, ec = _ip(np.concatenate(edges).reshape(-1)), _ip(be_off), _ip(be_cnt)
             do, db, dbx = _ip(dom_obj), _ip(dom_body), _fp(dom_box)
             self._keep += [ea, eo, ec, do, db, dbx]
@@ -390,6 +440,64 @@ class OracleLoop:
             else:
                 for nid in np.asarray(ic.nds):
                     v[int(nid)] = (vx, vy)
+
+    @staticmethod
+    def _pack_rigid(d, f, iv):
+        """One rigid, in the reference's order: attach's initial conditions
+        (rigiddomain.py:118-124), packRigidParams (rigidmanager.py:2250-2400),
+        then each BC through _addBcValue (2527-2553)."""
+        def first(v):
+            if hasattr(v, "__len__") and not isinstance(v, (str, bytes)):
+                return float(np.asarray(v, dtype=np.float32).reshape(-1)[0])
+            return float(v)
+
+        def vec2(v):
+            a = np.asarray(v, dtype=np.float32).reshape(-1)
+            return (float(a[0]), float(a[1]) if a.size > 1 else 0.0)
+
+        r = d.rigid
+        for ic in d.initials:
+            if ic.type in (0b10, 0b100):  # VTYPE, ATYPE: V[offset]
+                f[8], f[9] = vec2(ic.vel)
+            else:  # RotV[offset]
+                f[10] = first(ic.ang_vel)
+        ref = r.getRefPoint()
+        f[0], f[1] = vec2(ref)
+        f[6] = first(r.mass)
+        if r.rtype == 0b1:  # BALL
+            f[4] = first(r.getRadius())
+        elif r.rtype == 0b10:  # BOX
+            f[2], f[3] = vec2(r.getPrimary())
+        elif r.rtype == 0b1000:  # CAPSULE
+            f[2], f[3] = vec2(r.getPrimary() - ref)
+            f[4] = first(r.getRadius())
+        f[5] = first(r.angle)
+        f[7] = first(r.inertia_body)
+        bits = 0
+        for bc in d.bcs:
+            t, _, value = bc.processData()
+            bits |= int(t)
+            if t == 0b1:  # UTYPE
+                f[11], f[12] = 0.0, 0.0
+                f[6] = 1e10
+            elif t == 0b100000:  # RTYPE
+                f[11], f[12] = 0.0, 0.0
+                f[6] = 1e10
+                f[7] = 1e10
+                f[15] = 0.0
+            elif t == 0b10:  # VTYPE
+                f[11], f[12] = vec2(value)
+                f[6] = 1e10
+            elif t == 0b1000000:  # ROTVTYPE
+                f[15] = first(value)
+                f[7] = 1e10
+            elif t in (0b10000000, 0b100000000):  # ROTATYPE, TORQUETYPE
+                f[15] = first(value)
+            elif t == 0b10000:  # GRAVITY
+                f[13], f[14] = vec2(value)
+            else:
+                f[11], f[12] = vec2(value)
+        iv[0], iv[1], iv[2] = int(r.rtype), bits, 1 if d.considerContact else 0
 
     @staticmethod
     def _seg_penalty(dom):
@@ -444,6 +552,11 @@ class OracleLoop:
                     self.sh_elapsed = 0.0
             self._L.or_step(self._w, float(np.float32(d)), float(np.float32(self.damping)), self.counter, 0)
             self.counter += 1
+            if self.rigids:  # explicitloop.py:533-538
+                every = max(1, 1.0e-3 // d)
+                self.rigid_update_times += 1
+                if self.rigid_update_times % every == 0:
+                    self._L.or_rigid_update(self._w, float(np.float32(every * d)), float(np.float32(self.damping)))
 
     def flex_grid(self):
         """The hash grid: tc, nx, ny, origin x, origin y, cell x, cell y, estimate."""
@@ -491,6 +604,13 @@ class OracleLoop:
         eq = np.zeros(self.E)
         self._L.or_get_plastic(self._w, ep.ctypes.data_as(_f64p), eq.ctypes.data_as(_f64p))
         return ep, eq
+
+    def rigid_state(self):
+        """(float64[n, 12] per rigid: center, angle, V, angular velocity, U,
+        box lb, ub; error flag)."""
+        out = np.zeros((max(len(self.rigids), 1), 12))
+        err = self._L.or_get_rigids(self._w, out.ctypes.data_as(_f64p))
+        return out[:len(self.rigids)], err
 
     def aabb(self):
         out = np.zeros((len(self.fem), 4))

@@ -287,3 +287,44 @@ def flex_stamp_quirk(fw):
     read the far plane's stamp and never run; items targeting the second read
     the first circle's and do."""
     return [fw.GroundDomain(2, [0.0, -5.0], [0.0, 1.0])] + flex_circles(fw)
+
+
+def rigid_fixed_ball(fw):
+    """The reference's FEM-rigid scene (test2D/test_2Dfemcontact_types.py:26-38):
+    an Elastic circle of radius 0.05 at (0.5, 0.6) falling under gravity 10
+    onto a fixed BallRigid of radius 0.15 at (0.5, 0.3), ground plane y = 0."""
+    mesh = fw.FEMesher(2).createCircle([0.5, 0.6], 0.05)
+    fem = fw.FemDomain(mesh, fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)), [fw.Gravity([0, -10.0])])
+    rigid = fw.RigidBodyDomain(fw.BallRigid(2, [0.5, 0.3], 0.15, 100.0), [fw.FixedAll([0])], considerContact=True)
+    ground = fw.GroundDomain(2, [0, 0.0], [0, 1])
+    return [fem, rigid, ground]
+
+
+def rigid_block(fw, nx=16, ny=4, w=0.4, h=0.1, y0=0.0, mat=None):
+    conn, coords = fw.structured_rectangle(nx, ny, w, h, origin=(0.3, y0))
+    mat = mat or fw.Elastic(E=5e4, nu=0.3, rho=100.0)
+    return fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])])
+
+
+def rigid_pusher(fw):
+    """A box driven at constant velocity and spin (EnforceVel + EnforceRotVel)
+    sweeping across the top of an FEM block (0.4 x 0.2) that rests on the
+    ground, with friction 0.3 (the rigid's), plus a free capsule (gravity, no
+    BCs) dropped onto the block's far end: FEM-rigid contact with both
+    BC-driven and free rigids, friction, and reaction impulses.  The rigids
+    stay clear of the ground plane's box (y <= 0.1)."""
+    block = rigid_block(fw, nx=16, ny=8, h=0.2)
+    box = fw.RigidBodyDomain(fw.BoxRigid(2, [0.25, 0.262], [0.08, 0.1], [0.3], 5.0),
+                             [fw.EnforceVel([0], [0.6, -0.05]), fw.EnforceRotVel([0], 2.0)], friction=0.3)
+    cap = fw.RigidBodyDomain(fw.CapsuleRigid(2, [0.55, 0.26], [0.65, 0.28], [0.0], 0.02, 2.0),
+                             [fw.Gravity([0.0, -9.8])], friction=0.1)
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), block, box, cap]
+
+
+def rigid_free_ball(fw):
+    """A free ball (gravity, initial spin) dropped onto an FEM block resting on
+    the ground: its fall is stopped by the reaction impulses alone."""
+    block = rigid_block(fw, nx=20, ny=5, w=0.4, h=0.2, y0=0.0, mat=fw.HyperElastic(E=4e4, nu=0.3, rho=80.0))
+    ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.5, 0.32], 0.06, 2.0), [fw.Gravity([0.0, -9.8])],
+                              initials=[fw.InitialAngVel([0], 3.0)], friction=0.2)
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), block, ball]

@@ -1,0 +1,171 @@
+"""Rigid primitives in contact with FEM bodies (RigidBodyDomain with BallRigid /
+BoxRigid / CapsuleRigid; the reference's _batched_rigid_prim_kernel,
+mixedcontact.py:1026-1115, and RigidManager.substep without a constraint
+solve, rigidmanager.py:832-964, 2102-2197).
+
+CPU: the oracle reproduces the reference's FEM-rigid scene
+(test2D/test_2Dfemcontact_types.py:26-38: an FEM circle dropped on a fixed
+ball stays on it, mean y > 0.2), a free ball is stopped by an FEM block
+through the reaction impulses alone, the host's packing of rigids and pairs
+equals the oracle's, the FP32 sin/cos is accurate, and scenes outside the
+scope are refused.  GPU: the CUDA path gives the oracle's bits for the FEM
+nodes and for every rigid's state, frame after frame, and raises when a rigid
+meets the ground."""
+
+import numpy as np
+import pytest
+
+import flatworld_b200 as fw
+import oracle
+from flatworld_b200.world import PackedWorld, SceneLayout
+from oracle.scene import OracleLoop, sincos32
+from tests import scenes
+
+FRAME = 1.0 / 60.0
+
+
+def test_oracle_sincos_accuracy():
+    """The FP32 sin / cos of the rigid rotation (Cody-Waite reduction + Taylor)
+    within 2 ulp of 1 on [-8 pi, 8 pi] and exact at 0."""
+    xs = np.concatenate([np.linspace(-8 * np.pi, 8 * np.pi, 20001), [0.0, np.pi / 2, -np.pi, 1e-6, -3.0]])
+    worst = 0.0
+    for x in xs.astype(np.float32):
+        s, c = sincos32(float(x))
+        worst = max(worst, abs(s - np.sin(np.float64(x))), abs(c - np.cos(np.float64(x))))
+    assert worst < 2 * 2.0 ** -23, worst
+    assert sincos32(0.0) == (0.0, 1.0)
+
+
+def test_oracle_fem_rests_on_fixed_ball():
+    """test2D/test_2Dfemcontact_types.py:26-38 (60 frames, mean y > 0.2); the
+    circle settles on top of the ball (centre about r_ball + r_fem above it)."""
+    o = OracleLoop(scenes.rigid_fixed_ball(fw), useAdapativeDT=True)
+    for _ in range(60):
+        o.advance_with_time(FRAME)
+    x, _, _ = o.state()
+    st, err = o.rigid_state()
+    assert err == 0
+    assert np.mean(x[:, 1]) > 0.2
+    assert abs(x[:, 1].mean() - (0.3 + 0.15 + 0.05)) < 0.02
+    assert np.array_equal(st[0, :2], [np.float32(0.5), np.float32(0.3)])  # FixedAll: the ball never moves
+
+
+def test_oracle_free_ball_stopped_by_reactions():
+    """A free ball (gravity 9.8, spin 3 rad/s) on an FEM block: the FEM-rigid
+    reactions stop its fall; it then rattles on the block (undamped penalty
+    contact, as in the reference) with its centre about one radius above the
+    block's top, and rolls (friction turns its spin into travel)."""
+    o = OracleLoop(scenes.rigid_free_ball(fw), useAdapativeDT=True)
+    ys = []
+    for f in range(60):
+        o.advance_with_time(FRAME)
+        st, err = o.rigid_state()
+        assert err == 0
+        if f >= 20:
+            ys.append(st[0, 1])
+    assert 0.24 < min(ys) and max(ys) < 0.30, (min(ys), max(ys))
+    assert abs(st[0, 4]) < 1.0
+    assert st[0, 0] < 0.49 and st[0, 2] > 0.5  # rolled to the left, turned
+
+
+def test_oracle_flags_rigid_near_ground():
+    """A rigid falling toward the ground plane sets the error flag: rigid-ground
+    contact belongs to the constraint solver."""
+    doms = scenes.rigid_fixed_ball(fw)
+    doms[1] = fw.RigidBodyDomain(fw.BallRigid(2, [0.2, 0.3], 0.05, 1.0), [fw.Gravity([0, -10.0])])
+    o = OracleLoop(doms, useAdapativeDT=True)
+    for _ in range(30):
+        o.advance_with_time(FRAME)
+    assert o.rigid_state()[1] == 1
+
+
+def test_layout_matches_oracle():
+    """Stable dt, pair order and penalties, skip_bvh and the rigid records of
+    the host equal the oracle's restatement."""
+    for build in (scenes.rigid_fixed_ball, scenes.rigid_pusher, scenes.rigid_free_ball):
+        lay = SceneLayout(build(fw), useAdapativeDT=True)
+        o = OracleLoop(build(fw), useAdapativeDT=True)
+        assert lay.stableTime == o.stableTime, build.__name__
+        rig = [c for c in lay.pairs if c.kind == "rigid"]
+        orc = [c for c in o.contacts if c[0] == 0b110]
+        assert len(rig) == len(orc) > 0
+        for a, b in zip(rig, orc):
+            assert np.float32(a.penalty) == np.float32(b[3])
+            assert lay.rigids.index(a.ground) == o.rigids.index(b[2])
+        params, ints, grounds = PackedWorld([lay]).rigid_records()
+        for k, d in enumerate(lay.rigids):
+            f = np.zeros(16, np.float32)
+            iv = np.zeros(3, np.int32)
+            OracleLoop._pack_rigid(d, f, iv)
+            assert np.array_equal(params[k], f) and np.array_equal(ints[k], iv), (build.__name__, k)
+        assert grounds.shape == (1, 5) and grounds[0, 0] == 0.0
+    # FEM + one rigid, no ground: the loop skips the broad phase (plain box test)
+    assert SceneLayout([scenes.rigid_fixed_ball(fw)[i] for i in (0, 1)], useAdapativeDT=True).skip_bvh
+    assert not SceneLayout(scenes.rigid_fixed_ball(fw), useAdapativeDT=True).skip_bvh
+
+
+def test_out_of_scope_refused():
+    with pytest.raises(NotImplementedError):
+        fw.MeshRigid(2, None, 0.0, 1.0)
+    with pytest.raises(NotImplementedError):
+        fw.RevoluteJoint()
+    net = fw.SpringMassDomain(2, np.array([[0.0, 0.5], [0.1, 0.5]], np.float32), np.array([[0, 1]], np.int32),
+                              [10.0, 1.0, 1.0], [])
+    ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.5, 0.3], 0.1, 1.0))
+    with pytest.raises(NotImplementedError):
+        SceneLayout([net, ball])
+    with pytest.raises(NotImplementedError):
+        fw.ExplicitLoop(0.0, scenes.rigid_fixed_ball(fw), considerRigidRigidContact=False)
+
+
+def _compare(lp, o, n, tag):
+    xo, vo, _ = o.state()
+    assert np.array_equal(lp.femSpringManager.coords.numpy()[:n].astype(np.float64), xo), tag
+    assert np.array_equal(lp.femSpringManager.V.numpy()[:n].astype(np.float64), vo), tag
+    st, err = o.rigid_state()
+    assert err == 0, tag
+    assert np.array_equal(lp._rigid_state().astype(np.float64), st), tag
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,frames", [("fixed-ball", 40), ("pusher", 14), ("free-ball", 40)])
+def test_gpu_equals_oracle_frames(name, frames):
+    build = {"fixed-ball": scenes.rigid_fixed_ball, "pusher": scenes.rigid_pusher,
+             "free-ball": scenes.rigid_free_ball}[name]
+    lp = fw.ExplicitLoop(0.0, build(fw), useAdapativeDT=True)
+    assert lp.path == 1  # FEM-rigid contact runs on the gather path
+    o = oracle.OracleLoop(build(fw), useAdapativeDT=True)
+    for f in range(frames):
+        lp.advanceWithTime(FRAME)
+        o.advance_with_time(FRAME)
+        _compare(lp, o, o.N, (name, f))
+    lp.synchronize()
+    if name == "fixed-ball":
+        assert np.mean(lp.femSpringManager.coords.numpy()[:o.N, 1]) > 0.2
+    d = lp._layout.rigids[-1]
+    assert np.array_equal(d.getCurrentRefPoint(), lp._rigid_state()[-1, :2])
+
+
+@pytest.mark.gpu
+def test_gpu_equals_oracle_fixed_dt_advance():
+    """advance() at a fixed dt whose rigid schedule is N = 1e-3 // dt = 6."""
+    dt = 1.6e-4
+    lp = fw.ExplicitLoop(dt, scenes.rigid_free_ball(fw), useAdapativeDT=False)
+    o = oracle.OracleLoop(scenes.rigid_free_ball(fw), dt=dt, useAdapativeDT=False)
+    for k in range(8):
+        lp.advance_n(97)
+        o.advance(97)
+        _compare(lp, o, o.N, k)
+
+
+@pytest.mark.gpu
+def test_gpu_rigid_near_ground_raises():
+    doms = scenes.rigid_fixed_ball(fw)
+    doms[1] = fw.RigidBodyDomain(fw.BallRigid(2, [0.2, 0.3], 0.05, 1.0), [fw.Gravity([0, -10.0])])
+    lp = fw.ExplicitLoop(0.0, doms, useAdapativeDT=True)
+    for _ in range(30):
+        lp.advanceWithTime(FRAME)
+    with pytest.raises(RuntimeError, match="rigid"):
+        lp.synchronize()
+    with pytest.raises(RuntimeError):
+        lp._native.snapshot(0)
