@@ -42,6 +42,9 @@
  *   flatworld/spatialmanager.py:30-198     add_element, query_point_with_buffer
  *   flatworld/spatialmanager.py:200-420, 613-712  hash build kernels, build()
  *   flatworld/femspringmanager.py:1035-1063 + its populate kernel  FEM hash refresh
+ *   flatworld/mixedcontact.py:1026-1115     _batched_rigid_prim_kernel (FEM-rigid, untied)
+ *   flatworld/contact_detection.py:148-190, utils.py:7-145, 235-300  primitive SDFs, boxes
+ *   flatworld/rigidmanager.py:766-794, 832-964  rigid boxes, _rigid_step_wp, _update_u_and_bbox_wp
  *
  * Warp builtins (warp-lang, unpinned: requirements.txt `warp-lang>=1.7.0`) are
  * restated from their published definitions: mat22 @ mat22 and mat @ vec sum
