@@ -44,7 +44,10 @@ def parse():
     ap.add_argument("--mesh", type=int, default=256, help="quads per side of the large mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--workload", choices=["plain_large", "batched", "served", "adjoint", "flex"], default="plain_large")
+    ap.add_argument("--workload", choices=["plain_large", "batched", "served", "adjoint", "flex", "rigid"],
+                    default="plain_large")
+    ap.add_argument("--rigid-mesh", type=int, default=256,
+                    help="rigid: quads along the slab (and a quarter of that across)")
     ap.add_argument("--flex-side", type=int, default=12, help="flex: disks per row and column of the pile")
     ap.add_argument("--flex-scenes", type=int, default=1,
                     help="flex: > 1 batches that many independent 3 x 3 piles (BatchedLoop) instead of one pile")
@@ -724,6 +727,115 @@ def run_flex(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_rigid(args, rank, world, local):
+    """FEM-rigid contact: a NeoHookean slab of --rigid-mesh x --rigid-mesh/4
+    quads on a ground plane, with 12 BC-driven ball / box / capsule rigids
+    pressing into its top (tests/scenes.py rigid_row): per substep the plane
+    items, 12 x (slab boundary nodes) FEM-rigid items with their reactions,
+    and the rigid update every max(1, 1e-3 // dt) substeps.  Adaptive dt; a
+    step is 100 substeps."""
+    import torch
+
+    import flatworld_b200 as fw
+    from tests import scenes
+
+    torch.cuda.set_device(local)
+    dist = dist_init(world, local)
+    nx = args.rigid_mesh
+    build = lambda: scenes.rigid_row(fw, nx, max(4, nx // 4))  # noqa: E731
+    t0 = time.perf_counter()
+    loop = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, device=local)
+    build_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    loop._native.set_stream(stream.cuda_stream)
+    pk = loop._packed
+    N, E = pk.N, pk.E
+    n_rigid = len(loop._layout.rigids)
+    n_items = n_rigid * int(pk.bncnt[0])
+    dt = loop.dt
+    per = 100
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            loop.advance_n(per)
+        torch.cuda.synchronize()
+        barrier(dist)
+        l0 = loop.launch_count()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with ClockSampler(local) as clk:
+            for s_, e_ in ev:
+                s_.record(stream)
+                loop.advance_n(per)
+                e_.record(stream)
+            torch.cuda.synchronize()
+        launches = loop.launch_count() - l0
+        # ---- end to end: positions and velocities in from pinned host memory, a step, and out
+        xh = torch.empty((N, 2), dtype=torch.float32, pin_memory=True)
+        vh = torch.empty((N, 2), dtype=torch.float32, pin_memory=True)
+        loop._native.read_nodes_ptr(0, 0, N, xh.data_ptr())
+        loop._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for s_, e_ in ev2:
+            s_.record(stream)
+            loop._native.write_nodes_ptr(0, 0, N, xh.data_ptr())
+            loop._native.write_nodes_ptr(1, 0, N, vh.data_ptr())
+            loop.advance_n(per)
+            loop._native.read_nodes_ptr(0, 0, N, xh.data_ptr())
+            loop._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
+            e_.record(stream)
+        torch.cuda.synchronize()
+    barrier(dist)
+    loop.synchronize()  # raises if a rigid met the ground or another rigid
+    rig = loop._rigid_state()
+    lat = [s_.elapsed_time(e_) for s_, e_ in ev]
+    work, ms = shard.aggregate(E * per * args.steps, float(sum(lat)))
+    work_e2e, ms_e2e = shard.aggregate(E * per * args.steps, float(sum(s_.elapsed_time(e_) for s_, e_ in ev2)))
+    finite = bool(np.isfinite(loop.femSpringManager.coords.numpy()[:N]).all())
+    value = work / (ms / 1e3)
+    bstep = algorithmic_bytes_per_substep(N, E, 0, int(pk.bncnt[0]) + n_items, 0)
+    achieved = bstep / (ms / 1e3 / (per * args.steps)) / 1e9
+    peak, which = peaks()
+    line = {
+        "metric": "FEM element-steps/s (FEM-rigid contact)", "value": value, "unit": "element-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (slab and a row of rigid primitives)",
+        "config": {"workload": f"NeoHookean slab {nx}x{max(4, nx // 4)} quads on a plane, 12 BC-driven "
+                               f"ball / box / capsule rigids pressing into it",
+                   "elements": E, "nodes": N, "rigids": n_rigid, "rigid_work_items": n_items, "dt": dt,
+                   "rigid_update_every": int(max(1, 1e-3 // dt)), "step": "100 substeps",
+                   "l2": "working set smaller than L2", "host_build_s": build_s, "state_finite": finite,
+                   "rigid_x_range_at_end": [float(rig[:, 0].min()), float(rig[:, 0].max())],
+                   "replicas": world, "path": "gather"},
+        "latency_ms_per_step": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99)},
+        "roofline": {"bound": "hbm", "kernel": "substep = k_elements + k_nodes_rigid + k_rigid",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": which,
+                     "algorithmic_bytes_per_substep": bstep, "traffic": None,
+                     "note": "latency-bound: 3 dependent launches per substep over ~1 MB of state"},
+        "e2e": {"value": work_e2e / (ms_e2e / 1e3), "unit": "element-steps/s",
+                "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        o = oracle.OracleLoop(build(), useAdapativeDT=True, precision="f32", threads=threads)
+        o.advance(20)
+        t1 = time.perf_counter()
+        n_cpu = 3000
+        o.advance(n_cpu)
+        t_cpu = time.perf_counter() - t1
+        line["cpu_baseline"] = {"value": E * n_cpu / t_cpu, "unit": "element-steps/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"{n_cpu} substeps of the same scene, FP32 C restatement ({threads} "
+                                          f"threads for the element / node work, FEM-rigid contact and the "
+                                          f"rigid update serial as in the reference's CPU device)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def run_flex_batched(args, rank, world, local):
     """FEM-FEM contact, batched: --flex-scenes independent piles of 3 x 3
     touching disks (as the flex workload) in one BatchedLoop, each scene with
@@ -810,6 +922,9 @@ def main():
         return
     if args.workload == "adjoint":
         run_adjoint(args, rank, world, local)
+        return
+    if args.workload == "rigid":
+        run_rigid(args, rank, world, local)
         return
     if args.workload == "flex":
         if args.flex_scenes > 1:

@@ -80,7 +80,7 @@ struct FlexDev {
   const int32_t* be_off;  // per body: its first boundary edge
   const int32_t* be_cnt;
   const int32_t* dom_obj;   // per domain of the scene: a broad-phase object (considerContact)
-  const int32_t* dom_body;  // per domain: global body id, or -1 for a ground
+  const int32_t* dom_body;  // per domain: global body id, -1 for a ground, -2 - r for rigid r
   const float4* dom_box;    // per domain: a ground's static box
   int32_t* pair_active;
   int32_t* stamped;  // at body0 + g: the scene's domain g is in a broad-phase pair this substep
@@ -124,6 +124,9 @@ __device__ __forceinline__ float wmax(float a, float b) { return a > b ? a : b; 
 __device__ __forceinline__ bool flex_stepping(const Dev& d, int s) {
   return d.scene_active[s] && !d.scene_mode_req[s];
 }
+
+// A rigid domain's current box (lb x, y, ub x, y), as the broad phase sees it.
+__device__ __forceinline__ float4 rigid_box(const Rigid& g) { return make_float4(g.lb[0], g.lb[1], g.ub[0], g.ub[1]); }
 
 __device__ __forceinline__ float4 ring_box(const Dev& d, int slot, int body) {
   const int* r = d.aabb_ring + ((size_t)slot * d.B + body) * 4;
@@ -357,7 +360,9 @@ __global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f0
   const int slot = k & 1;
   float4* body_box = sbox + f.n_dom;
   for (int g = threadIdx.x; g < f.n_dom; g += blockDim.x)
-    sbox[g] = f.dom_body[g] >= 0 ? ring_box(d, slot, f.dom_body[g]) : f.dom_box[g];
+    sbox[g] = f.dom_body[g] >= 0    ? ring_box(d, slot, f.dom_body[g])
+              : f.dom_body[g] <= -2 ? rigid_box(d.rig[-2 - f.dom_body[g]])
+                                    : f.dom_box[g];
   for (int b = threadIdx.x; b < f.n_fem; b += blockDim.x) body_box[b] = ring_box(d, slot, f.body0 + b);
   __syncthreads();
   // _activate_or_fill_pairs: every pair when the loop has no BVH, else BVH overlap

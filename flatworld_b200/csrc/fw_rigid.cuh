@@ -239,7 +239,8 @@ constexpr float kRigidClearance = 0.01f;
 // _detect_analytical_prim_contacts_wp's early out measures it,
 // rigidmanager.py:1127-1136), of a height-field / voxel box (gkind 1), or of
 // another contact rigid's box sets bit 0 of *err: the reference would solve
-// that contact, this library does not.
+// that contact, this library does not.  So does a rigid whose state is no
+// longer finite.
 __device__ __forceinline__ void rigid_update(Rigid* rig, int n, const float4* gbox, const int* gkind,
                                              int n_ground, float dt, float damping, int* err) {
   const float cl = kRigidClearance;
@@ -247,19 +248,21 @@ __device__ __forceinline__ void rigid_update(Rigid* rig, int n, const float4* gb
     const Rigid& g = rig[a];
     for (int q = 0; q < n_ground; ++q) {
       const float4 b = gbox[q];
+      // written as "not clear", so that a non-finite box is flagged too
       if (gkind[q] == 0) {
         const float sx = b.z < 0.0f ? g.ub[0] : g.lb[0], sy = b.w < 0.0f ? g.ub[1] : g.lb[1];
-        if ((sx - b.x) * b.z + (sy - b.y) * b.w <= cl) *err |= 1;
-      } else if (g.lb[0] - cl <= b.z && g.ub[0] + cl >= b.x && g.lb[1] - cl <= b.w && g.ub[1] + cl >= b.y) {
+        if (!((sx - b.x) * b.z + (sy - b.y) * b.w > cl)) *err |= 1;
+      } else if (!(g.lb[0] - cl > b.z || g.ub[0] + cl < b.x || g.lb[1] - cl > b.w || g.ub[1] + cl < b.y)) {
         *err |= 1;
       }
     }
     for (int q = a + 1; q < n; ++q) {
       const Rigid& h = rig[q];
-      if (g.in_contact && h.in_contact && g.lb[0] - cl <= h.ub[0] && g.ub[0] + cl >= h.lb[0] &&
-          g.lb[1] - cl <= h.ub[1] && g.ub[1] + cl >= h.lb[1])
+      if (g.in_contact && h.in_contact &&
+          !(g.lb[0] - cl > h.ub[0] || g.ub[0] + cl < h.lb[0] || g.lb[1] - cl > h.ub[1] || g.ub[1] + cl < h.lb[1]))
         *err |= 1;
     }
+    if (!(fabsf(g.c[0]) < 1e30f && fabsf(g.c[1]) < 1e30f && fabsf(g.quat) < 1e30f)) *err |= 1;
   }
   for (int a = 0; a < n; ++a) {  // _rigid_step_wp
     Rigid& g = rig[a];

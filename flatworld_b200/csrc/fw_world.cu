@@ -369,10 +369,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes_rigid(Dev d) {
   node_step<FLEX, true>(d, i, i < d.N);
 }
 
-// The rigid side of a substep (single-scene worlds), one warp: the work
-// items' reactions added to their rigids' accumulators in item order (lanes
-// stage 32 records at a time, lane 0 adds them), then the rigid counter and,
-// on the substeps of the schedule, the rigid update (fw_rigid.cuh).
+// The rigid side of a substep (single-scene worlds): one warp per rigid adds
+// its work items' reactions to its accumulators in work-item order (its
+// pairs in pair order, each pair's items in boundary-node order: lanes load
+// 128 records at a time, and every lane adds the hits in ascending lane order
+// through shuffles, so the sum is a serial run of the reference's atomic
+// adds); then thread 0 counts the substep and, on the substeps of the
+// schedule, runs the rigid update (fw_rigid.cuh).
 struct RigidDev {
   Rigid* rig;
   int n;
@@ -381,34 +384,53 @@ struct RigidDev {
   int n_ground;
   float4* item;
   int n_items;
+  int* rp_off;   // per rigid: its pairs' item ranges rp_rng[rp_off[g] .. rp_off[g + 1])
+  int2* rp_rng;  // (first item, item count), pair order
   const fw::RigidClock* clock;
   int* count;
   int* err;
 };
 
-__global__ void __launch_bounds__(32) k_rigid(Dev d, RigidDev r) {
+constexpr int kRigidThreads = 1024;
+
+__global__ void __launch_bounds__(kRigidThreads) k_rigid(Dev d, RigidDev r) {
   if (d.scene_mode[0] != fw::MODE_STEP) return;
-  __shared__ float4 buf[32];
-  const int lane = threadIdx.x;
-  for (int base = 0; base < r.n_items; base += 32) {
-    const int it = base + lane;
-    buf[lane] = it < r.n_items ? r.item[it] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-    __syncwarp();
-    if (lane == 0) {
-      const int m = min(32, r.n_items - base);
-      for (int j = 0; j < m; ++j) {
-        const float4 q = buf[j];
-        const int g = __float_as_int(q.w);
-        if (g < 0) continue;
-        Rigid& rg = r.rig[g];
-        rg.acc[0] = rg.acc[0] + q.x;
-        rg.acc[1] = rg.acc[1] + q.y;
-        rg.accw = rg.accw + q.z;
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  const float4 none = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+  for (int g = warp; g < r.n; g += n_warps) {
+    Rigid& rg = r.rig[g];
+    float ax = rg.acc[0], ay = rg.acc[1], aw = rg.accw;
+    for (int q = r.rp_off[g]; q < r.rp_off[g + 1]; ++q) {
+      const int2 rng = r.rp_rng[q];
+      for (int base = 0; base < rng.y; base += 128) {
+        float4 rec[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int it = base + 32 * u + lane;
+          rec[u] = it < rng.y ? r.item[rng.x + it] : none;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          unsigned m = __ballot_sync(full, __float_as_int(rec[u].w) >= 0);
+          while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            ax = ax + __shfl_sync(full, rec[u].x, l);
+            ay = ay + __shfl_sync(full, rec[u].y, l);
+            aw = aw + __shfl_sync(full, rec[u].z, l);
+          }
+        }
       }
     }
-    __syncwarp();
+    if (lane == 0) {
+      rg.acc[0] = ax;
+      rg.acc[1] = ay;
+      rg.accw = aw;
+    }
   }
-  if (lane != 0) return;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   const fw::RigidClock ck = *r.clock;
   const int cnt = *r.count + 1;
   *r.count = cnt;
@@ -1095,7 +1117,7 @@ int launch_step(fw_ctx* c) {
       k_nodes_rigid<true><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
     else
       k_nodes_rigid<false><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
-    k_rigid<<<1, 32, 0, c->stream>>>(c->d, c->rd);
+    k_rigid<<<1, 32 * std::min(32, std::max(1, c->rd.n)), 0, c->stream>>>(c->d, c->rd);
     c->launches += 1;
   } else if (c->has_flex) {
     k_nodes_flex<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
@@ -1619,8 +1641,9 @@ int check_device_error(fw_ctx* c) {
     FW_CUDA(c, cudaStreamSynchronize(c->stream));
     if (rerr & 1)
       return fail(c, FW_ERR_UNSUPPORTED,
-                  "a rigid body's box met a ground's or another contact rigid's: rigid-rigid and rigid-ground "
-                  "contact (the reference's constraint solve) are outside this library");
+                  "a rigid body came within 0.01 of a ground or of another contact rigid (rigid-rigid and "
+                  "rigid-ground contact, the reference's constraint solve, are outside this library), or its "
+                  "state is no longer finite");
   }
   if (c->path != FW_PATH_RESIDENT) return FW_OK;
   int err = 0;
@@ -2421,6 +2444,21 @@ int fw_finalize(fw_ctx* c) {
     std::vector<int32_t> bslot(N, 0);
     for (int b = 0; b < B; ++b)
       for (int k = 0; k < c->h_bncnt[b]; ++k) bslot[c->h_bnodes[c->h_bnoff[b] + k]] = k;
+    // per rigid, its pairs' item ranges in pair (= item) order; `pairs` is
+    // grouped by body by now, so order the rigid pairs by first item again
+    std::vector<Pair> rpairs;
+    for (const Pair& p : pairs)
+      if (p.kind == fw::PAIR_RIGID) rpairs.push_back(p);
+    std::sort(rpairs.begin(), rpairs.end(), [](const Pair& a, const Pair& b) { return a.n0 < b.n0; });
+    const int nr = (int)c->h_rigid.size();
+    std::vector<int32_t> rp_off(nr + 1, 0);
+    for (const Pair& p : rpairs) rp_off[p.table + 1]++;
+    for (int g = 0; g < nr; ++g) rp_off[g + 1] += rp_off[g];
+    std::vector<int2> rp_rng(std::max(1, rp_off[nr]));
+    {
+      std::vector<int32_t> fill(rp_off.begin(), rp_off.end() - 1);
+      for (const Pair& p : rpairs) rp_rng[fill[p.table]++] = make_int2(p.n0, c->h_bncnt[p.body]);
+    }
     RigidDev& r = c->rd;
     r.n = (int)c->h_rigid.size();
     r.n_ground = (int)c->h_gbox.size();
@@ -2428,7 +2466,8 @@ int fw_finalize(fw_ctx* c) {
     fw::RigidClock ck{1, 0.0f, 0.0f, 0};
     if ((rc = upload(c, &r.rig, c->h_rigid)) || (rc = upload(c, &d.bslot, bslot)) ||
         (rc = dalloc(c, &r.item, (size_t)n_ritems)) || (rc = upload(c, &r.gbox, c->h_gbox)) ||
-        (rc = upload(c, &r.gkind, c->h_gkind)) ||
+        (rc = upload(c, &r.gkind, c->h_gkind)) || (rc = upload(c, &r.rp_off, rp_off)) ||
+        (rc = upload(c, &r.rp_rng, rp_rng)) ||
         (rc = dalloc(c, &c->d_rclock, 1)) || (rc = dalloc(c, &r.count, 1)) || (rc = dalloc(c, &r.err, 1)))
       return rc;
     FW_CUDA(c, cudaMemcpyAsync(c->d_rclock, &ck, sizeof(ck), cudaMemcpyHostToDevice, c->stream));

@@ -305,8 +305,9 @@ class ExplicitLoop:
         """float32[numRigids, 12]: center, angle, V, angular velocity, U, box."""
         st, flags = self._native.read_rigids(len(self._layout.rigids))
         if flags & 1:
-            raise RuntimeError("a rigid body met a ground or another contact rigid: rigid-rigid and "
-                               "rigid-ground contact (the reference's constraint solve) are outside flatworld_b200")
+            raise RuntimeError("a rigid body came within 0.01 of a ground or another contact rigid (rigid-rigid "
+                               "and rigid-ground contact, the reference's constraint solve, are outside "
+                               "flatworld_b200), or its state is no longer finite")
         return st
 
     # ---- stepping

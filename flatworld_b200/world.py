@@ -335,11 +335,13 @@ class PackedWorld:
                 continue
             fem_index = {id(d): k for k, d in enumerate(sc.fem)}
             dom_obj = np.asarray([1 if d.considerContact else 0 for d in sc.domains], np.int32)
-            dom_body = np.asarray([self.body_of[(si, fem_index[id(d)])] if id(d) in fem_index else -1
+            rig_index = {id(d): k for k, d in enumerate(sc.rigids)}
+            dom_body = np.asarray([self.body_of[(si, fem_index[id(d)])] if id(d) in fem_index
+                                   else (-2 - rig_index[id(d)] if id(d) in rig_index else -1)
                                    for d in sc.domains], np.int32)
             dom_box = np.zeros((len(sc.domains), 4), np.float32)
-            for g, d in enumerate(sc.domains):
-                if id(d) not in fem_index and d.considerContact:
+            for g, d in enumerate(sc.domains):  # grounds: static boxes; bodies, rigids: boxes on the device
+                if id(d) not in fem_index and id(d) not in rig_index and d.considerContact:
                     lo, hi = d.getBBox()
                     dom_box[g, :2] = np.asarray(lo, np.float32).reshape(2)
                     dom_box[g, 2:] = np.asarray(hi, np.float32).reshape(2)

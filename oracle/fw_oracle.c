@@ -904,8 +904,11 @@ static int boxes_overlap(const REAL* a, const REAL* b, long counter) {
   return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
 }
 
+static const REAL* rigid_domain_box(const or_world* w, int r); /* a rigid's current box (below) */
+
 static const REAL* dom_box(const or_world* w, int g) {
   const or_flex* f = w->flex;
+  if (f->dom_body[g] <= -2) return rigid_domain_box(w, -2 - f->dom_body[g]);
   return f->dom_body[g] >= 0 ? w->aabb + 4 * f->dom_body[g] : f->dom_box + 4 * g;
 }
 
@@ -1058,6 +1061,7 @@ typedef struct {
   REAL rot[4]; /* cached_rotation_matrix (row-major), refreshed by the velocity pass */
   REAL acc[2], accw;
   REAL lb[2], ub[2];
+  REAL box[4]; /* lb x, y, ub x, y: the rigid's box as a broad-phase domain box */
 } or_rigid;
 
 typedef struct or_rigids {
@@ -1070,6 +1074,8 @@ typedef struct or_rigids {
   int *rp_body, *rp_rigid, *rp_skip;
   REAL *rp_pen, *rp_fric;
 } or_rigids;
+
+static const REAL* rigid_domain_box(const or_world* w, int r) { return w->rig->r[r].box; }
 
 /* cal2DRotationMat (flatworld/utils.py:7-11): [[c, -s], [s, c]]. */
 static void rot_of(REAL theta, REAL* m) {
@@ -1113,6 +1119,7 @@ static void rigid_aabb(or_rigid* g) {
     g->ub[0] = rmax(p0x, p1x) + perp0 + axial0;
     g->ub[1] = rmax(p0y, p1y) + perp1 + axial1;
   }
+  g->box[0] = g->lb[0]; g->box[1] = g->lb[1]; g->box[2] = g->ub[0]; g->box[3] = g->ub[1];
 }
 
 /* detectPointToPrimitive (contact_detection.py:148-190) with sphereSDFQuery,
@@ -1266,19 +1273,22 @@ void or_rigid_update(or_world* w, float dt_f, float damping_f) {
     const or_rigid* g = &R->r[a];
     for (int q = 0; q < R->n_ground; ++q) {
       const REAL* b = R->gbox + 4 * q;
+      /* written as "not clear", so that a non-finite box is flagged too */
       if (R->gkind[q] == 0) {
         const REAL sx = b[2] < 0 ? g->ub[0] : g->lb[0], sy = b[3] < 0 ? g->ub[1] : g->lb[1];
-        if ((sx - b[0]) * b[2] + (sy - b[1]) * b[3] <= cl) R->err = 1;
-      } else if (g->lb[0] - cl <= b[2] && g->ub[0] + cl >= b[0] && g->lb[1] - cl <= b[3] && g->ub[1] + cl >= b[1]) {
+        if (!((sx - b[0]) * b[2] + (sy - b[1]) * b[3] > cl)) R->err = 1;
+      } else if (!(g->lb[0] - cl > b[2] || g->ub[0] + cl < b[0] || g->lb[1] - cl > b[3] || g->ub[1] + cl < b[1])) {
         R->err = 1;
       }
     }
     for (int q = a + 1; q < R->n; ++q) {
       const or_rigid* h = &R->r[q];
-      if (g->in_contact && h->in_contact && g->lb[0] - cl <= h->ub[0] && g->ub[0] + cl >= h->lb[0] &&
-          g->lb[1] - cl <= h->ub[1] && g->ub[1] + cl >= h->lb[1])
+      if (g->in_contact && h->in_contact &&
+          !(g->lb[0] - cl > h->ub[0] || g->ub[0] + cl < h->lb[0] || g->lb[1] - cl > h->ub[1] ||
+            g->ub[1] + cl < h->lb[1]))
         R->err = 1;
     }
+    if (!(R_FABS(g->c[0]) < (REAL)1e30 && R_FABS(g->c[1]) < (REAL)1e30 && R_FABS(g->quat) < (REAL)1e30)) R->err = 1;
   }
   for (int a = 0; a < R->n; ++a) { /* _rigid_step_wp */
     or_rigid* g = &R->r[a];

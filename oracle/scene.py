@@ -393,10 +393,12 @@ class OracleLoop:
                 be_cnt.append(len(e))
                 edges.append(e)
             dom_obj = [1 if d.considerContact else 0 for d in domains]
-            dom_body = [fem.index(d) if d.type in (FEM, SPRINGMASS) else -1 for d in domains]
+            # bodies by index, rigids as -2 - rigid index (their boxes move), grounds -1
+            dom_body = [fem.index(d) if d.type in (FEM, SPRINGMASS) else
+                        (-2 - rigid_doms.index(d) if d.type == RIGID else -1) for d in domains]
             dom_box = np.zeros((len(domains), 4), np.float32)
             for i, d in enumerate(domains):
-                if d.type not in (FEM, SPRINGMASS) and d.considerContact:
+                if d.type not in (FEM, SPRINGMASS, RIGID) and d.considerContact:
                     lo, hi = self._ground_box(d)
                     dom_box[i, :2] = lo[0]
                     dom_box[i, 2:] = hi[0]

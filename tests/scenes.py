@@ -328,3 +328,44 @@ def rigid_free_ball(fw):
     ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.5, 0.32], 0.06, 2.0), [fw.Gravity([0.0, -9.8])],
                               initials=[fw.InitialAngVel([0], 3.0)], friction=0.2)
     return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), block, ball]
+
+
+def rigid_row(fw, nx=128, ny=32, n_rigid=12):
+    """A NeoHookean slab (1.0 x 0.25, nx x ny quads) on the ground plane under
+    gravity, with a row of n_rigid BC-driven primitives touching its top
+    (0.5 mm deep at the start), 0.08 apart, cycled: balls rolling right at
+    0.05 m/s (EnforceVel, friction 0.2), fixed box indenters (FixedAll) and
+    capsules spinning in place at 1 rad/s (Fixed + EnforceRotVel, friction
+    0.1), which press deeper as they turn.  BC-driven rigids keep their
+    clearances, so the scene runs for as long as a benchmark needs."""
+    conn, coords = fw.structured_rectangle(nx, ny, 1.0, 0.25, origin=(0.0, 0.0))
+    slab = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.HyperElastic(E=1e5, nu=0.3, rho=500.0)),
+                        [fw.Gravity([0.0, -9.8])])
+    doms = [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), slab]
+    for k in range(n_rigid):
+        x = 0.06 + 0.08 * k
+        if k % 3 == 0:
+            r = fw.RigidBodyDomain(fw.BallRigid(2, [x, 0.2745], 0.025, 0.5), [fw.EnforceVel([0], [0.05, 0.0])],
+                                   friction=0.2)
+        elif k % 3 == 1:
+            r = fw.RigidBodyDomain(fw.BoxRigid(2, [x, 0.2745], [0.04, 0.05], [0.0], 1.0), [fw.FixedAll([0])])
+        else:
+            r = fw.RigidBodyDomain(fw.CapsuleRigid(2, [x - 0.02, 0.2695], [x + 0.02, 0.2695], [0.0], 0.02, 0.5),
+                                   [fw.Fixed([0]), fw.EnforceRotVel([0], 1.0)], friction=0.1)
+        doms.append(r)
+    return doms
+
+
+def rigid_shared(fw, mass=20.0):
+    """A free box (gravity) lying across two FEM blocks that stand on the
+    ground 5 cm apart: one rigid in two FEM-rigid pairs (its reactions summed
+    over both pairs in pair order), next to the blocks' own FEM-FEM pair."""
+    def block(x0, mat):
+        conn, coords = fw.structured_rectangle(12, 6, 0.3, 0.15, origin=(x0, 0.0))
+        return fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])])
+
+    a = block(0.1, fw.Elastic(E=6e4, nu=0.3, rho=100.0))
+    b = block(0.45, fw.HyperElastic(E=4e4, nu=0.25, rho=120.0))
+    box = fw.RigidBodyDomain(fw.BoxRigid(2, [0.425, 0.1795], [0.5, 0.06], [0.02], mass), [fw.Gravity([0.0, -9.8])],
+                             friction=0.15)
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), a, b, box]

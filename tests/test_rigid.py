@@ -68,6 +68,27 @@ def test_oracle_free_ball_stopped_by_reactions():
     assert st[0, 0] < 0.49 and st[0, 2] > 0.5  # rolled to the left, turned
 
 
+def test_oracle_box_across_two_blocks():
+    """One rigid in two pairs: the box rests across both blocks (reactions
+    from both), level within a few degrees, clear of the ground."""
+    o = OracleLoop(scenes.rigid_shared(fw), useAdapativeDT=True)
+    for _ in range(40):
+        o.advance_with_time(FRAME)
+    st, err = o.rigid_state()
+    assert err == 0
+    assert abs(st[0, 1] - (0.15 + 0.03)) < 0.01 and abs(st[0, 2]) < 0.1, st[0]
+
+
+def test_oracle_flags_unstable_rigid():
+    """The same box at 1.5 kg is too light for the rigid update interval (its
+    contact frequency times N dt nears 1): it blows up, as the reference's
+    scheme would, and the non-finite state is flagged rather than reported."""
+    o = OracleLoop(scenes.rigid_shared(fw, mass=1.5), useAdapativeDT=True)
+    for _ in range(40):
+        o.advance_with_time(FRAME)
+    assert o.rigid_state()[1] == 1
+
+
 def test_oracle_flags_rigid_near_ground():
     """A rigid falling toward the ground plane sets the error flag: rigid-ground
     contact belongs to the constraint solver."""
@@ -128,10 +149,10 @@ def _compare(lp, o, n, tag):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,frames", [("fixed-ball", 40), ("pusher", 14), ("free-ball", 40)])
+@pytest.mark.parametrize("name,frames", [("fixed-ball", 40), ("pusher", 14), ("free-ball", 40), ("shared", 30)])
 def test_gpu_equals_oracle_frames(name, frames):
     build = {"fixed-ball": scenes.rigid_fixed_ball, "pusher": scenes.rigid_pusher,
-             "free-ball": scenes.rigid_free_ball}[name]
+             "free-ball": scenes.rigid_free_ball, "shared": scenes.rigid_shared}[name]
     lp = fw.ExplicitLoop(0.0, build(fw), useAdapativeDT=True)
     assert lp.path == 1  # FEM-rigid contact runs on the gather path
     o = oracle.OracleLoop(build(fw), useAdapativeDT=True)
