@@ -369,3 +369,21 @@ def rigid_shared(fw, mass=20.0):
     box = fw.RigidBodyDomain(fw.BoxRigid(2, [0.425, 0.1795], [0.5, 0.06], [0.02], mass), [fw.Gravity([0.0, -9.8])],
                              friction=0.15)
     return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), a, b, box]
+
+
+def rigid_bcs(fw):
+    """The remaining rigid BCs over an FEM slab (0.9 x 0.1) on the ground: a
+    ball under gravity pushed sideways by a Force and turned by a Torque, a
+    box driven down into the slab by EnforceAcc, and a capsule held by Fixed
+    and spun up by EnforceRotAcc, with loop damping 0.5."""
+    conn, coords = fw.structured_rectangle(36, 4, 0.9, 0.1, origin=(0.05, 0.0))
+    slab = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.Elastic(E=8e4, nu=0.3, rho=200.0)),
+                        [fw.Gravity([0.0, -9.8])])
+    ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.2, 0.14], 0.03, 4.0),
+                              [fw.Gravity([0.0, -9.8]), fw.Force([0], [0.5, 0.0]), fw.Torque([0], 0.01)],
+                              friction=0.2)
+    box = fw.RigidBodyDomain(fw.BoxRigid(2, [0.5, 0.1205], [0.06, 0.04], [0.1], 2.0),
+                             [fw.EnforceAcc([0], [0.0, -0.5])], friction=0.1)
+    cap = fw.RigidBodyDomain(fw.CapsuleRigid(2, [0.76, 0.1195], [0.84, 0.1195], [0.0], 0.02, 1.0),
+                             [fw.Fixed([0]), fw.EnforceRotAcc([0], 5.0)], friction=0.3)
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), slab, ball, box, cap]

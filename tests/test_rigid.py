@@ -79,6 +79,21 @@ def test_oracle_box_across_two_blocks():
     assert abs(st[0, 1] - (0.15 + 0.03)) < 0.01 and abs(st[0, 2]) < 0.1, st[0]
 
 
+def test_oracle_rigid_bcs():
+    """EnforceAcc zeroes the contact impulse (the box moves straight down at
+    the enforced acceleration, slowed only by damping); Fixed keeps the capsule
+    in place while EnforceRotAcc spins it up (angle near a t^2 / 2)."""
+    o = OracleLoop(scenes.rigid_bcs(fw), useAdapativeDT=True, damping=0.5)
+    st0, _ = o.rigid_state()
+    for _ in range(24):
+        o.advance_with_time(FRAME)
+    st, err = o.rigid_state()
+    assert err == 0
+    assert st[1, 0] == st0[1, 0] and st[1, 3] == 0.0 and -0.2 < st[1, 4] < -0.17
+    assert np.array_equal(st[2, :2], st0[2, :2])
+    assert 0.3 < st[2, 2] < 0.42 and st[2, 5] > 0.0
+
+
 def test_oracle_flags_unstable_rigid():
     """The same box at 1.5 kg is too light for the rigid update interval (its
     contact frequency times N dt nears 1): it blows up, as the reference's
@@ -165,6 +180,17 @@ def test_gpu_equals_oracle_frames(name, frames):
         assert np.mean(lp.femSpringManager.coords.numpy()[:o.N, 1]) > 0.2
     d = lp._layout.rigids[-1]
     assert np.array_equal(d.getCurrentRefPoint(), lp._rigid_state()[-1, :2])
+
+
+@pytest.mark.gpu
+def test_gpu_equals_oracle_bcs_damping():
+    """Force, Torque, EnforceAcc, Fixed + EnforceRotAcc and loop damping."""
+    lp = fw.ExplicitLoop(0.0, scenes.rigid_bcs(fw), useAdapativeDT=True, damping=0.5)
+    o = oracle.OracleLoop(scenes.rigid_bcs(fw), useAdapativeDT=True, damping=0.5)
+    for f in range(24):
+        lp.advanceWithTime(FRAME)
+        o.advance_with_time(FRAME)
+        _compare(lp, o, o.N, f)
 
 
 @pytest.mark.gpu
