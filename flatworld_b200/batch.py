@@ -44,6 +44,8 @@ class BatchedLoop:
         damp = damping if np.iterable(damping) else [damping] * S
         self.layouts = [SceneLayout(d, dt=a, damping=c, useAdapativeDT=b)
                         for d, a, b, c in zip(scenes, dts, ada, damp)]
+        if any(lay.rigids for lay in self.layouts):
+            raise NotImplementedError("rigid bodies run in a single-scene ExplicitLoop only, not in a BatchedLoop")
         self.packed = PackedWorld(self.layouts)
         self._has_flex = any(lay.flex for lay in self.layouts)
         if path == "stream" and (self.packed.spring_bodies or self._has_flex):

@@ -62,6 +62,8 @@ class Arena:
 
     def insert(self, domains, dt=0.0, useAdapativeDT=False, damping=0.0) -> int:
         layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT)
+        if layout.rigids:
+            raise NotImplementedError("rigid bodies run in a single-scene ExplicitLoop only, not in served worlds")
         stage(self.native, PackedWorld([layout]))
         s = self.native.arena_commit()
         self.layouts[s] = layout

@@ -152,6 +152,13 @@ def test_out_of_scope_refused():
         SceneLayout([net, ball])
     with pytest.raises(NotImplementedError):
         fw.ExplicitLoop(0.0, scenes.rigid_fixed_ball(fw), considerRigidRigidContact=False)
+    from flatworld_b200.batch import BatchedLoop
+    from flatworld_b200.diff import DiffSim
+
+    with pytest.raises(NotImplementedError):
+        BatchedLoop([scenes.rigid_fixed_ball(fw)])
+    with pytest.raises(NotImplementedError):
+        DiffSim(scenes.rigid_fixed_ball(fw), 1e-4, 10)
 
 
 def _compare(lp, o, n, tag):
