@@ -63,6 +63,7 @@ _SIGNATURES = {
     "fw_set_rigids": (C.c_int, [_vp, C.c_int32, _f32p, _i32p, C.c_int32, _f32p]),
     "fw_add_rigid_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32]),
     "fw_set_rigid_clock": (C.c_int, [_vp, C.c_int32, C.c_float, C.c_float]),
+    "fw_set_rigid_clocks": (C.c_int, [_vp, _i32p, _f32p, _f32p]),
     "fw_read_rigids": (C.c_int, [_vp, _f32p, _i32p]),
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
@@ -237,11 +238,11 @@ class NativeWorld:
         self._check(self._L.fw_set_spring_bodies(self._h, len(b[0]), b[1], m[1]), "fw_set_spring_bodies")
 
     def set_rigids(self, params, ints, grounds):
-        """params float32[n, 16], ints int32[n, 3], grounds float32[g, 5]."""
+        """params float32[n, 16], ints int32[n, 4], grounds float32[g, 6]."""
         p = _f(np.asarray(params, np.float32).reshape(-1))
         i = _i(np.asarray(ints, np.int32).reshape(-1))
         g = _f(np.asarray(grounds, np.float32).reshape(-1))
-        self._check(self._L.fw_set_rigids(self._h, len(i[0]) // 3, p[1], i[1], len(g[0]) // 5, g[1]),
+        self._check(self._L.fw_set_rigids(self._h, len(i[0]) // 4, p[1], i[1], len(g[0]) // 6, g[1]),
                     "fw_set_rigids")
 
     def add_rigid_pair(self, body, rigid, penalty, friction, skip_bvh):
@@ -250,6 +251,11 @@ class NativeWorld:
 
     def set_rigid_clock(self, every: int, dt: float, damping: float):
         self._check(self._L.fw_set_rigid_clock(self._h, int(every), float(dt), float(damping)), "fw_set_rigid_clock")
+
+    def set_rigid_clocks(self, every, dt, damping):
+        """Per scene: update interval, rigid dt and damping."""
+        e, t, m = _i(every), _f(dt), _f(damping)
+        self._check(self._L.fw_set_rigid_clocks(self._h, e[1], t[1], m[1]), "fw_set_rigid_clocks")
 
     def read_rigids(self, n: int):
         """(float32[n, 12] per rigid: center, angle, V, angular velocity, U, box lb, ub; flags)."""

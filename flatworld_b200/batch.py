@@ -44,12 +44,11 @@ class BatchedLoop:
         damp = damping if np.iterable(damping) else [damping] * S
         self.layouts = [SceneLayout(d, dt=a, damping=c, useAdapativeDT=b)
                         for d, a, b, c in zip(scenes, dts, ada, damp)]
-        if any(lay.rigids for lay in self.layouts):
-            raise NotImplementedError("rigid bodies run in a single-scene ExplicitLoop only, not in a BatchedLoop")
         self.packed = PackedWorld(self.layouts)
         self._has_flex = any(lay.flex for lay in self.layouts)
-        if path == "stream" and (self.packed.spring_bodies or self._has_flex):
-            path = "gather"  # the patch-streaming step covers triangles without FEM-FEM contact
+        self._has_rigid = any(lay.rigids for lay in self.layouts)
+        if path == "stream" and (self.packed.spring_bodies or self._has_flex or self._has_rigid):
+            path = "gather"  # the patch-streaming step covers triangles without FEM-FEM / FEM-rigid contact
         self._native = build_native(self.packed, device=device, path=path)
         self.path = path
         if block_elems or block_nodes:
@@ -90,9 +89,16 @@ class BatchedLoop:
 
     def _clocks(self, dt):
         """The FEM-FEM hash clocks accumulate each scene's float64 dt
-        (femspringmanager.py:1035-1039)."""
+        (femspringmanager.py:1035-1039); each scene's rigids move every
+        N = max(1, 1e-3 // dt) substeps by N * dt (explicitloop.py:533-538)."""
         if self._has_flex:
             self._native.set_flex_clocks(np.asarray(dt, np.float64))
+        if self._has_rigid:
+            every = [int(max(1, 1.0e-3 // float(t))) if t > 0 else 1 for t in dt]
+            rdt = [float(np.float32(e * float(t))) for e, t in zip(every, dt)]
+            damp = [float(np.float32(lay.damping)) for lay in self.layouts]
+            self._native.set_rigid_clocks(np.asarray(every, np.int32), np.asarray(rdt, np.float32),
+                                          np.asarray(damp, np.float32))
 
     def advance(self, n: int = 1):
         """n substeps of every active scene, each with its own dt."""
@@ -147,6 +153,19 @@ class BatchedLoop:
         n0 = int(self.packed.noff[bodies[0]])
         nn = int(sum(int(self.packed.ncnt[b]) for b in bodies))
         return n0, nn
+
+    def rigid_state(self, s):
+        """float32[rigids of scene s, 12]: center, angle, V, angular velocity,
+        U, box (the RigidBodyDomain getters' values)."""
+        n = len(self.layouts[s].rigids)
+        if n == 0:
+            return np.zeros((0, 12), np.float32)
+        st, flags = self._native.read_rigids(sum(len(lay.rigids) for lay in self.layouts))
+        if flags & 1:
+            raise RuntimeError("a rigid body came within 0.01 of a ground or another contact rigid, or its state "
+                               "is no longer finite")
+        r0 = self.packed.rigid_offsets()[s]
+        return st[r0:r0 + n]
 
     def coords(self, s):
         n0, nn = self._node_range(s)

@@ -43,8 +43,14 @@ struct __align__(16) Rigid {
   int type, bc, in_contact;
   float rot[4];                // cached_rotation_matrix, row-major
   float lb[2], ub[2];          // the rigid's box (aabb[domain])
+  int scene, pad[3];           // the scene (loop) the rigid belongs to
 };
-static_assert(sizeof(Rigid) == 128, "Rigid record is 128 bytes");
+static_assert(sizeof(Rigid) == 144, "Rigid record is 144 bytes");
+
+// The rigids and grounds of one scene: rig[r0, r0 + rn), grounds [g0, g0 + gn).
+struct RigidScene {
+  int scene, r0, rn, g0, gn, pad[3];
+};
 
 // Schedule of the rigid update (host-computed from the float64 substep dt,
 // explicitloop.py:535-538): every `every` substeps, with dt = every * dt.

@@ -369,13 +369,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes_rigid(Dev d) {
   node_step<FLEX, true>(d, i, i < d.N);
 }
 
-// The rigid side of a substep (single-scene worlds): one warp per rigid adds
+// The rigid side of a substep: one warp per rigid of a stepping scene adds
 // its work items' reactions to its accumulators in work-item order (its
 // pairs in pair order, each pair's items in boundary-node order: lanes load
 // 128 records at a time, and every lane adds the hits in ascending lane order
 // through shuffles, so the sum is a serial run of the reference's atomic
-// adds); then thread 0 counts the substep and, on the substeps of the
-// schedule, runs the rigid update (fw_rigid.cuh).
+// adds); then one thread per scene with rigids counts the substep and, on the
+// substeps of that scene's schedule, runs its rigid update (fw_rigid.cuh).
 struct RigidDev {
   Rigid* rig;
   int n;
@@ -386,20 +386,22 @@ struct RigidDev {
   int n_items;
   int* rp_off;   // per rigid: its pairs' item ranges rp_rng[rp_off[g] .. rp_off[g + 1])
   int2* rp_rng;  // (first item, item count), pair order
-  const fw::RigidClock* clock;
-  int* count;
+  fw::RigidScene* rs;  // the scenes with rigids
+  int n_rs;
+  const fw::RigidClock* clock;  // per scene
+  int* count;                   // per scene: the reference's rigid_update_times
   int* err;
 };
 
 constexpr int kRigidThreads = 1024;
 
 __global__ void __launch_bounds__(kRigidThreads) k_rigid(Dev d, RigidDev r) {
-  if (d.scene_mode[0] != fw::MODE_STEP) return;
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
   const float4 none = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
   for (int g = warp; g < r.n; g += n_warps) {
     Rigid& rg = r.rig[g];
+    if (d.scene_mode[rg.scene] != fw::MODE_STEP) continue;
     float ax = rg.acc[0], ay = rg.acc[1], aw = rg.accw;
     for (int q = r.rp_off[g]; q < r.rp_off[g + 1]; ++q) {
       const int2 rng = r.rp_rng[q];
@@ -430,12 +432,15 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(Dev d, RigidDev r) {
     }
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
-  const fw::RigidClock ck = *r.clock;
-  const int cnt = *r.count + 1;
-  *r.count = cnt;
-  if (ck.every < 1 || cnt % ck.every != 0) return;
-  fw::rigid_update(r.rig, r.n, r.gbox, r.gkind, r.n_ground, ck.dt, ck.damping, r.err);
+  for (int k = threadIdx.x; k < r.n_rs; k += blockDim.x) {
+    const fw::RigidScene rs = r.rs[k];
+    if (d.scene_mode[rs.scene] != fw::MODE_STEP) continue;
+    const fw::RigidClock ck = r.clock[rs.scene];
+    const int cnt = r.count[rs.scene] + 1;
+    r.count[rs.scene] = cnt;
+    if (ck.every < 1 || cnt % ck.every != 0) continue;
+    fw::rigid_update(r.rig + rs.r0, rs.rn, r.gbox + rs.g0, r.gkind + rs.g0, rs.gn, ck.dt, ck.damping, r.err);
+  }
 }
 
 // Rotation cache and boxes of the rigids at construction
@@ -1028,7 +1033,7 @@ struct fw_ctx {
   // rigid primitives (fw_rigid.cuh): staging, then the device state
   std::vector<Rigid> h_rigid;
   std::vector<float4> h_gbox;
-  std::vector<int> h_gkind;
+  std::vector<int> h_gkind, h_gscene;
   bool rigid_set = false, has_rigid = false;
   RigidDev rd{};
   fw::RigidClock* d_rclock = nullptr;
@@ -1991,9 +1996,10 @@ int fw_set_rigids(fw_ctx* c, int32_t n, const float* params, const int32_t* ints
   for (int a = 0; a < n; ++a) {
     const float* q = params + 16 * (size_t)a;
     Rigid& g = c->h_rigid[a];
-    g.type = ints[3 * a];
-    g.bc = ints[3 * a + 1];
-    g.in_contact = ints[3 * a + 2];
+    g.type = ints[4 * a];
+    g.bc = ints[4 * a + 1];
+    g.in_contact = ints[4 * a + 2];
+    g.scene = ints[4 * a + 3];
     if (g.type != fw::RIGID_BALL && g.type != fw::RIGID_BOX && g.type != fw::RIGID_CAPSULE)
       return fail(c, FW_ERR_ARG, "rigid %d: type %d is not a ball, box or capsule", a, g.type);
     g.c[0] = q[0]; g.c[1] = q[1]; g.prim[0] = q[2]; g.prim[1] = q[3];
@@ -2003,11 +2009,13 @@ int fw_set_rigids(fw_ctx* c, int32_t n, const float* params, const int32_t* ints
   }
   c->h_gbox.resize(n_ground);
   c->h_gkind.resize(n_ground);
+  c->h_gscene.resize(n_ground);
   for (int k = 0; k < n_ground; ++k) {
-    const float* q = grounds + 5 * (size_t)k;
+    const float* q = grounds + 6 * (size_t)k;
     if (q[0] != 0.0f && q[0] != 1.0f) return fail(c, FW_ERR_ARG, "ground %d: kind must be 0 (plane) or 1 (box)", k);
     c->h_gkind[k] = (int)q[0];
     c->h_gbox[k] = make_float4(q[1], q[2], q[3], q[4]);
+    c->h_gscene[k] = (int)q[5];
   }
   c->rigid_set = true;
   return FW_OK;
@@ -2029,19 +2037,31 @@ int fw_add_rigid_pair(fw_ctx* c, int32_t body, int32_t rigid, float penalty, flo
   return add_pair(c, p, zero, zero);
 }
 
-int fw_set_rigid_clock(fw_ctx* c, int32_t every, float dt, float damping) {
-  if (!c) return FW_ERR_ARG;
-  if (every < 1) return fail(c, FW_ERR_ARG, "fw_set_rigid_clock: every must be >= 1");
-  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_set_rigid_clock: no FEM-rigid contact (or before fw_finalize)");
-  const fw::RigidClock ck{every, dt, damping, 0};
-  FW_CUDA(c, cudaMemcpyAsync(c->d_rclock, &ck, sizeof(ck), cudaMemcpyHostToDevice, c->stream));
+int fw_set_rigid_clocks(fw_ctx* c, const int32_t* every, const float* dt, const float* damping) {
+  if (!c || !every || !dt || !damping) return FW_ERR_ARG;
+  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_set_rigid_clocks: no rigid bodies (or before fw_finalize)");
+  std::vector<fw::RigidClock> ck(c->S);
+  for (int s = 0; s < c->S; ++s) {
+    if (every[s] < 1) return fail(c, FW_ERR_ARG, "fw_set_rigid_clocks: every[%d] must be >= 1", s);
+    ck[s] = fw::RigidClock{every[s], dt[s], damping[s], 0};
+  }
+  FW_CUDA(c, cudaMemcpyAsync(c->d_rclock, ck.data(), sizeof(fw::RigidClock) * ck.size(), cudaMemcpyHostToDevice,
+                             c->stream));
   FW_CUDA(c, cudaStreamSynchronize(c->stream));  // ck lives on this stack frame
   return FW_OK;
 }
 
+int fw_set_rigid_clock(fw_ctx* c, int32_t every, float dt, float damping) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_set_rigid_clock: no rigid bodies (or before fw_finalize)");
+  const std::vector<int32_t> e(c->S, every);
+  const std::vector<float> t(c->S, dt), m(c->S, damping);
+  return fw_set_rigid_clocks(c, e.data(), t.data(), m.data());
+}
+
 int fw_read_rigids(fw_ctx* c, float* out, int32_t* flags) {
   if (!c || !out) return FW_ERR_ARG;
-  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_read_rigids: no FEM-rigid contact (or before fw_finalize)");
+  if (!c->has_rigid) return fail(c, FW_ERR_STATE, "fw_read_rigids: no rigid bodies (or before fw_finalize)");
   std::vector<Rigid> h(c->rd.n);
   int err = 0;
   FW_CUDA(c, cudaMemcpyAsync(h.data(), c->rd.rig, sizeof(Rigid) * h.size(), cudaMemcpyDeviceToHost, c->stream));
@@ -2335,7 +2355,6 @@ int fw_finalize(fw_ctx* c) {
       n_ritems += c->h_bncnt[p.body];
     }
   c->has_rigid = !c->h_rigid.empty();
-  if (c->has_rigid && S != 1) return fail(c, FW_ERR_ARG, "FEM-rigid contact: single-scene worlds only");
   std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& a, const Pair& b) { return a.body < b.body; });
   std::vector<int32_t> poff(B, 0), pcnt(B, 0);
   for (size_t k = 0; k < pairs.size(); ++k) pcnt[pairs[k].body]++;
@@ -2459,19 +2478,35 @@ int fw_finalize(fw_ctx* c) {
       std::vector<int32_t> fill(rp_off.begin(), rp_off.end() - 1);
       for (const Pair& p : rpairs) rp_rng[fill[p.table]++] = make_int2(p.n0, c->h_bncnt[p.body]);
     }
+    // the scenes with rigids: their rigids and grounds, each a contiguous range
+    std::vector<fw::RigidScene> rs;
+    for (int a = 0, q = 0; a < nr;) {
+      const int sc = c->h_rigid[a].scene;
+      if (sc < 0 || sc >= S) return fail(c, FW_ERR_ARG, "rigid %d: scene %d outside [0, %d)", a, sc, S);
+      if (!rs.empty() && sc <= rs.back().scene)
+        return fail(c, FW_ERR_ARG, "rigids must be grouped by scene in ascending scene order");
+      fw::RigidScene e{sc, a, 0, 0, 0, {0, 0, 0}};
+      while (a < nr && c->h_rigid[a].scene == sc) ++a, ++e.rn;
+      while (q < (int)c->h_gscene.size() && c->h_gscene[q] < sc) ++q;
+      e.g0 = q;
+      while (q < (int)c->h_gscene.size() && c->h_gscene[q] == sc) ++q, ++e.gn;
+      rs.push_back(e);
+    }
+    for (size_t k = 1; k < c->h_gscene.size(); ++k)
+      if (c->h_gscene[k] < c->h_gscene[k - 1]) return fail(c, FW_ERR_ARG, "grounds must be grouped by scene");
     RigidDev& r = c->rd;
     r.n = (int)c->h_rigid.size();
     r.n_ground = (int)c->h_gbox.size();
     r.n_items = n_ritems;
-    fw::RigidClock ck{1, 0.0f, 0.0f, 0};
+    r.n_rs = (int)rs.size();
+    std::vector<fw::RigidClock> ck(S, fw::RigidClock{1, 0.0f, 0.0f, 0});
     if ((rc = upload(c, &r.rig, c->h_rigid)) || (rc = upload(c, &d.bslot, bslot)) ||
         (rc = dalloc(c, &r.item, (size_t)n_ritems)) || (rc = upload(c, &r.gbox, c->h_gbox)) ||
         (rc = upload(c, &r.gkind, c->h_gkind)) || (rc = upload(c, &r.rp_off, rp_off)) ||
-        (rc = upload(c, &r.rp_rng, rp_rng)) ||
-        (rc = dalloc(c, &c->d_rclock, 1)) || (rc = dalloc(c, &r.count, 1)) || (rc = dalloc(c, &r.err, 1)))
+        (rc = upload(c, &r.rp_rng, rp_rng)) || (rc = upload(c, &r.rs, rs)) ||
+        (rc = upload(c, &c->d_rclock, ck)) || (rc = dalloc(c, &r.count, S)) || (rc = dalloc(c, &r.err, 1)))
       return rc;
-    FW_CUDA(c, cudaMemcpyAsync(c->d_rclock, &ck, sizeof(ck), cudaMemcpyHostToDevice, c->stream));
-    FW_CUDA(c, cudaMemsetAsync(r.count, 0, sizeof(int), c->stream));
+    FW_CUDA(c, cudaMemsetAsync(r.count, 0, sizeof(int) * S, c->stream));
     FW_CUDA(c, cudaMemsetAsync(r.err, 0, sizeof(int), c->stream));
     r.clock = c->d_rclock;
     d.rig = r.rig;

@@ -309,22 +309,35 @@ class PackedWorld:
         self.S = len(scenes)
 
     def rigid_records(self):
-        """Per rigid of the (single) scene: float32[16] and int32[3] for
-        fw_set_rigids, plus the static grounds float32[g, 5]."""
+        """Per rigid, scene-major: float32[16] and int32[4] (type, BC bits,
+        considerContact, scene) for fw_set_rigids; per ground of a scene with
+        rigids: float32[6] (kind, point + normal or box, scene)."""
         params, ints, boxes = [], [], []
-        for sc in self.scenes:
+        for si, sc in enumerate(self.scenes):
+            if not sc.rigids:
+                continue
             for dom in sc.rigids:
                 p, i = rigid_record(dom)
                 params.append(p)
-                ints.append(i)
+                ints.append([*i, si])
             for g in sc.grounds:  # plane: kind 0, point, normal; height field / voxel grid: kind 1, box
                 if g.type == DomainType.ANALYTICAL:
-                    boxes.append([0.0, *np.asarray(g.point, np.float32)[:2], *np.asarray(g.normal, np.float32)[:2]])
+                    boxes.append([0.0, *np.asarray(g.point, np.float32)[:2], *np.asarray(g.normal, np.float32)[:2],
+                                  si])
                 else:
                     lo, hi = g.getBBox()
-                    boxes.append([1.0, *np.asarray(lo, np.float32).reshape(2), *np.asarray(hi, np.float32).reshape(2)])
+                    boxes.append([1.0, *np.asarray(lo, np.float32).reshape(2), *np.asarray(hi, np.float32).reshape(2),
+                                  si])
         as2 = lambda a, w, dt: np.asarray(a, dt).reshape(-1, w)  # noqa: E731
-        return as2(params, 16, np.float32), as2(ints, 3, np.int32), as2(boxes, 5, np.float32)
+        return as2(params, 16, np.float32), as2(ints, 4, np.int32), as2(boxes, 6, np.float32)
+
+    def rigid_offsets(self):
+        """Index of each scene's first rigid in the world's rigid list."""
+        off, n = [], 0
+        for sc in self.scenes:
+            off.append(n)
+            n += len(sc.rigids)
+        return off
 
     def flex_records(self):
         """Per scene with FEM-FEM pairs: (scene, skip_bvh, dom_obj, dom_body,
@@ -335,7 +348,7 @@ class PackedWorld:
                 continue
             fem_index = {id(d): k for k, d in enumerate(sc.fem)}
             dom_obj = np.asarray([1 if d.considerContact else 0 for d in sc.domains], np.int32)
-            rig_index = {id(d): k for k, d in enumerate(sc.rigids)}
+            rig_index = {id(d): self.rigid_offsets()[si] + k for k, d in enumerate(sc.rigids)}
             dom_body = np.asarray([self.body_of[(si, fem_index[id(d)])] if id(d) in fem_index
                                    else (-2 - rig_index[id(d)] if id(d) in rig_index else -1)
                                    for d in sc.domains], np.int32)
@@ -353,12 +366,13 @@ class PackedWorld:
     def pair_records(self):
         """(kind, body, penalty f32, gate lo, gate hi, ground) in launch order."""
         out = []
+        r_off = self.rigid_offsets()
         for si, sc in enumerate(self.scenes):
             fem_index = {id(d): k for k, d in enumerate(sc.fem)}
             for c in sc.pairs:
                 body = self.body_of[(si, fem_index[id(c.fem)])]
                 if c.kind == "rigid":  # the gate box is the rigid's current one, on the device
-                    rid = next(k for k, d in enumerate(sc.rigids) if d is c.ground)
+                    rid = r_off[si] + next(k for k, d in enumerate(sc.rigids) if d is c.ground)
                     out.append((c.kind, body, np.float32(c.penalty), rid, np.float32(c.friction), sc.skip_bvh))
                     continue
                 lo, hi = c.ground.getBBox()

@@ -184,14 +184,15 @@ int fw_mass_scaling(fw_ctx* ctx, float dt_target);
 int fw_read_flex_state(fw_ctx* ctx, int32_t* item_cache, int32_t n_items, float* grid);
 
 /* Rigid primitives touching FEM bodies (RigidBodyDomain with BallRigid /
- * BoxRigid / CapsuleRigid), before fw_finalize, single-scene worlds, gather
- * path.  Per rigid 16 floats -- center x, y; primary x, y (box: full extents;
- * capsule: lower end minus center); radius; angle; mass; inertia; velocity x,
- * y; angular velocity; BC translation value x, y; gravity x, y; BC rotation
- * value -- and 3 ints: RigidType (1 ball, 2 box, 8 capsule), BC bits
- * (definitions.py:96-104) and considerContact.  grounds: 5 floats per ground
- * domain -- kind 0 (plane): point x, y, normal x, y; kind 1 (height field,
- * voxel grid): box lb x, y, ub x, y.  A rigid that comes within 0.01 of a
+ * BoxRigid / CapsuleRigid), before fw_finalize, gather path.  Per rigid 16
+ * floats -- center x, y; primary x, y (box: full extents; capsule: lower end
+ * minus center); radius; angle; mass; inertia; velocity x, y; angular
+ * velocity; BC translation value x, y; gravity x, y; BC rotation value -- and
+ * 4 ints: RigidType (1 ball, 2 box, 8 capsule), BC bits (definitions.py:
+ * 96-104), considerContact, scene; rigids grouped by scene in ascending order.
+ * grounds: 6 floats per ground domain -- kind 0 (plane): point x, y, normal
+ * x, y; kind 1 (height field, voxel grid): box lb x, y, ub x, y; then its
+ * scene (grouped by scene too).  A rigid that comes within 0.01 of a
  * ground (20x the reference's rigid-ground contact margin) or of another
  * contact rigid's box at an update makes the next synchronising call return
  * FW_ERR_UNSUPPORTED.
@@ -211,8 +212,10 @@ int fw_add_rigid_pair(fw_ctx* ctx, int32_t body, int32_t rigid, float penalty, f
 /* The rigid update schedule of the coming substeps: the rigids move every
  * `every` substeps by dt (the reference's N = max(1, 1e-3 // dt) and N * dt,
  * explicitloop.py:533-538, computed by the caller from its float64 dt), with
- * the loop's damping.  After fw_finalize. */
+ * the loop's damping; every scene alike, or per scene (arrays of one entry per
+ * scene of the world).  After fw_finalize. */
 int fw_set_rigid_clock(fw_ctx* ctx, int32_t every, float dt, float damping);
+int fw_set_rigid_clocks(fw_ctx* ctx, const int32_t* every, const float* dt, const float* damping);
 /* Per rigid 12 floats: center x, y, angle, velocity x, y, angular velocity,
  * displacement x, y, box lb x, y, ub x, y; *flags (may be NULL): bit 0 set
  * once a rigid met a ground or another rigid.  The reference's

@@ -10,7 +10,7 @@ through the reaction impulses alone, the host's packing of rigids and pairs
 equals the oracle's, the FP32 sin/cos is accurate, and scenes outside the
 scope are refused.  GPU: the CUDA path gives the oracle's bits for the FEM
 nodes and for every rigid's state, frame after frame, and raises when a rigid
-meets the ground."""
+meets the ground; batched rigid scenes equal the same scenes alone."""
 
 import numpy as np
 import pytest
@@ -133,8 +133,8 @@ def test_layout_matches_oracle():
             f = np.zeros(16, np.float32)
             iv = np.zeros(3, np.int32)
             OracleLoop._pack_rigid(d, f, iv)
-            assert np.array_equal(params[k], f) and np.array_equal(ints[k], iv), (build.__name__, k)
-        assert grounds.shape == (1, 5) and grounds[0, 0] == 0.0
+            assert np.array_equal(params[k], f) and np.array_equal(ints[k, :3], iv), (build.__name__, k)
+        assert grounds.shape == (1, 6) and grounds[0, 0] == 0.0
     # FEM + one rigid, no ground: the loop skips the broad phase (plain box test)
     assert SceneLayout([scenes.rigid_fixed_ball(fw)[i] for i in (0, 1)], useAdapativeDT=True).skip_bvh
     assert not SceneLayout(scenes.rigid_fixed_ball(fw), useAdapativeDT=True).skip_bvh
@@ -152,11 +152,8 @@ def test_out_of_scope_refused():
         SceneLayout([net, ball])
     with pytest.raises(NotImplementedError):
         fw.ExplicitLoop(0.0, scenes.rigid_fixed_ball(fw), considerRigidRigidContact=False)
-    from flatworld_b200.batch import BatchedLoop
     from flatworld_b200.diff import DiffSim
 
-    with pytest.raises(NotImplementedError):
-        BatchedLoop([scenes.rigid_fixed_ball(fw)])
     with pytest.raises(NotImplementedError):
         DiffSim(scenes.rigid_fixed_ball(fw), 1e-4, 10)
 
@@ -198,6 +195,30 @@ def test_gpu_equals_oracle_bcs_damping():
         lp.advanceWithTime(FRAME)
         o.advance_with_time(FRAME)
         _compare(lp, o, o.N, f)
+
+
+@pytest.mark.gpu
+def test_gpu_batched_rigid_scenes_equal_alone():
+    """Scenes with rigids batched with each other and with a plain scene (each
+    scene its own rigid clock, counter and clearance check; per-scene dt and
+    damping): every scene's nodes and rigids equal the same scene in its own
+    loop, frame after frame."""
+    from flatworld_b200.batch import BatchedLoop
+
+    builds = [scenes.rigid_fixed_ball, scenes.plain_small_scene, scenes.rigid_free_ball, scenes.rigid_bcs,
+              scenes.rigid_shared]
+    damp = [0.0, 0.0, 0.0, 0.5, 0.0]
+    b = BatchedLoop([f(fw) for f in builds], useAdapativeDT=True, damping=damp)
+    assert len(set(np.round(b.dt, 12))) > 1
+    alone = [fw.ExplicitLoop(0.0, f(fw), useAdapativeDT=True, damping=c) for f, c in zip(builds, damp)]
+    for frame in range(10):
+        b.advanceWithTime(FRAME)
+        for s, lp in enumerate(alone):
+            lp.advanceWithTime(FRAME)
+            n = len(b.coords(s))
+            assert np.array_equal(b.coords(s), lp.femSpringManager.coords.numpy()[:n]), (frame, s)
+            if lp._layout.rigids:
+                assert np.array_equal(b.rigid_state(s), lp._rigid_state()), (frame, s)
 
 
 @pytest.mark.gpu
