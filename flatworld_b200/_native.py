@@ -64,6 +64,7 @@ _SIGNATURES = {
     "fw_add_rigid_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32]),
     "fw_set_rigid_clock": (C.c_int, [_vp, C.c_int32, C.c_float, C.c_float]),
     "fw_set_rigid_clocks": (C.c_int, [_vp, _i32p, _f32p, _f32p]),
+    "fw_gate_by_rigid": (C.c_int, [_vp, C.c_int32]),
     "fw_read_rigids": (C.c_int, [_vp, _f32p, _i32p]),
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
@@ -238,7 +239,7 @@ class NativeWorld:
         self._check(self._L.fw_set_spring_bodies(self._h, len(b[0]), b[1], m[1]), "fw_set_spring_bodies")
 
     def set_rigids(self, params, ints, grounds):
-        """params float32[n, 16], ints int32[n, 4], grounds float32[g, 6]."""
+        """params float32[n, 20], ints int32[n, 4], grounds float32[g, 6]."""
         p = _f(np.asarray(params, np.float32).reshape(-1))
         i = _i(np.asarray(ints, np.int32).reshape(-1))
         g = _f(np.asarray(grounds, np.float32).reshape(-1))
@@ -251,6 +252,9 @@ class NativeWorld:
 
     def set_rigid_clock(self, every: int, dt: float, damping: float):
         self._check(self._L.fw_set_rigid_clock(self._h, int(every), float(dt), float(damping)), "fw_set_rigid_clock")
+
+    def gate_by_rigid(self, entry: int):
+        self._check(self._L.fw_gate_by_rigid(self._h, int(entry)), "fw_gate_by_rigid")
 
     def set_rigid_clocks(self, every, dt, damping):
         """Per scene: update interval, rigid dt and damping."""

@@ -46,7 +46,7 @@ class BatchedLoop:
                         for d, a, b, c in zip(scenes, dts, ada, damp)]
         self.packed = PackedWorld(self.layouts)
         self._has_flex = any(lay.flex for lay in self.layouts)
-        self._has_rigid = any(lay.rigids for lay in self.layouts)
+        self._has_rigid = any(lay.entries for lay in self.layouts)
         if path == "stream" and (self.packed.spring_bodies or self._has_flex or self._has_rigid):
             path = "gather"  # the patch-streaming step covers triangles without FEM-FEM / FEM-rigid contact
         self._native = build_native(self.packed, device=device, path=path)
@@ -160,7 +160,7 @@ class BatchedLoop:
         n = len(self.layouts[s].rigids)
         if n == 0:
             return np.zeros((0, 12), np.float32)
-        st, flags = self._native.read_rigids(sum(len(lay.rigids) for lay in self.layouts))
+        st, flags = self._native.read_rigids(sum(len(lay.entries) for lay in self.layouts))
         if flags & 1:
             raise RuntimeError("a rigid body came within 0.01 of a ground or another contact rigid, or its state "
                                "is no longer finite")

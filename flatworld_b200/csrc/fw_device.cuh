@@ -48,7 +48,8 @@ struct __align__(16) Pair {
   // plane: p.x, p.y, n.x, n.y.  heightfield: lb.x, ub.x.
   // voxel: lb.x, lb.y, dx, dz.
   float f[4];
-  int pad[2];
+  int gate;  // 0: the static box above gates the pair; e + 1: the current box of rigid entry e
+  int pad;
 };
 static_assert(sizeof(Pair) == 64, "Pair record is 64 bytes");
 

@@ -26,6 +26,10 @@ constexpr int PAIR_RIGID = 3;
 constexpr int RIGID_BALL = 1;
 constexpr int RIGID_BOX = 2;
 constexpr int RIGID_CAPSULE = 8;
+// An analytical entry of the rigid manager (a ground plane, height field or
+// voxel grid of a loop where some ground plane has BCs): it moves with its BCs
+// and its broad-phase box follows, rigidmanager.py:2486-2517, 832-964.
+constexpr int RIGID_ANALYTICAL = 64;
 
 // Rigid BC bits (flatworld/definitions.py:96-104)
 constexpr int RBC_U = 0x1, RBC_V = 0x2, RBC_A = 0x4, RBC_FORCE = 0x8, RBC_GRAVITY = 0x10;
@@ -93,10 +97,22 @@ __device__ __forceinline__ void rigid_rot(Rigid& g) {
   g.rot[3] = c;
 }
 
-// _write_primitive_aabb with getBallBBox / getBoxBBox / getCapsuleBBox.
+// _write_primitive_aabb with getBallBBox / getBoxBBox / getCapsuleBBox; for an
+// analytical entry the moving-plane box of _update_u_and_bbox_wp
+// (rigidmanager.py:950-964): +-100 along the tangent, +-0.1 along the rotated
+// normal (a height field's or voxel grid's entry has zero point and normal).
 __device__ __forceinline__ void rigid_aabb(Rigid& g) {
   const float* m = g.rot;
-  if (g.type == RIGID_BALL) {
+  if (g.type == RIGID_ANALYTICAL) {
+    const float nx = m[0] * g.prim[0] + m[1] * g.prim[1], ny = m[2] * g.prim[0] + m[3] * g.prim[1];
+    const float tx = -ny, ty = nx;
+    const float lox = g.c[0] - tx * 100.0f - nx * 0.1f, loy = g.c[1] - ty * 100.0f - ny * 0.1f;
+    const float hix = g.c[0] + tx * 100.0f + nx * 0.1f, hiy = g.c[1] + ty * 100.0f + ny * 0.1f;
+    g.lb[0] = rmin(lox, hix);
+    g.lb[1] = rmin(loy, hiy);
+    g.ub[0] = rmax(lox, hix);
+    g.ub[1] = rmax(loy, hiy);
+  } else if (g.type == RIGID_BALL) {
     g.lb[0] = g.c[0] - g.radius;
     g.lb[1] = g.c[1] - g.radius;
     g.ub[0] = g.c[0] + g.radius;
@@ -252,6 +268,7 @@ __device__ __forceinline__ void rigid_update(Rigid* rig, int n, const float4* gb
   const float cl = kRigidClearance;
   for (int a = 0; a < n; ++a) {
     const Rigid& g = rig[a];
+    if (g.type == RIGID_ANALYTICAL) continue;  // not a rigid body
     for (int q = 0; q < n_ground; ++q) {
       const float4 b = gbox[q];
       // written as "not clear", so that a non-finite box is flagged too
@@ -264,7 +281,7 @@ __device__ __forceinline__ void rigid_update(Rigid* rig, int n, const float4* gb
     }
     for (int q = a + 1; q < n; ++q) {
       const Rigid& h = rig[q];
-      if (g.in_contact && h.in_contact &&
+      if (h.type != RIGID_ANALYTICAL && g.in_contact && h.in_contact &&
           !(g.lb[0] - cl > h.ub[0] || g.ub[0] + cl < h.lb[0] || g.lb[1] - cl > h.ub[1] || g.ub[1] + cl < h.lb[1]))
         *err |= 1;
     }
@@ -273,6 +290,7 @@ __device__ __forceinline__ void rigid_update(Rigid* rig, int n, const float4* gb
   for (int a = 0; a < n; ++a) {  // _rigid_step_wp
     Rigid& g = rig[a];
     rigid_rot(g);
+    if (g.type == RIGID_ANALYTICAL) continue;  // the impulse pass covers the rigid bodies only
     if (g.bc & RBC_A) {
       g.acc[0] = 0.0f;
       g.acc[1] = 0.0f;

@@ -134,6 +134,12 @@ __device__ void step_control(const Dev& d) {
                                       g.lb[0], g.lb[1], g.ub[0], g.ub[1], pr.n1 ? 1 : k) ? 1 : 0;
       continue;
     }
+    if (pr.gate > 0) {  // a ground of a loop with a moving plane: its entry's current box
+      const Rigid& g = d.rig[pr.gate - 1];
+      d.pair_active[p] = fw::box_gate(fw::ord2f(r[0]), fw::ord2f(r[1]), fw::ord2f(r[2]), fw::ord2f(r[3]),
+                                      g.lb[0], g.lb[1], g.ub[0], g.ub[1], k) ? 1 : 0;
+      continue;
+    }
     d.pair_active[p] = fw::pair_gate(pr, fw::ord2f(r[0]), fw::ord2f(r[1]), fw::ord2f(r[2]),
                                      fw::ord2f(r[3]), k) ? 1 : 0;
   }
@@ -449,7 +455,7 @@ __global__ void k_rigid_init(Rigid* rig, int n) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   fw::rigid_rot(rig[a]);
-  fw::rigid_aabb(rig[a]);
+  if (rig[a].type != fw::RIGID_ANALYTICAL) fw::rigid_aabb(rig[a]);  // an analytical entry starts at getBBox()
 }
 
 // Reference-shape precompute, _prepare_fem_data_kernel
@@ -1994,18 +2000,20 @@ int fw_set_rigids(fw_ctx* c, int32_t n, const float* params, const int32_t* ints
     return fail(c, FW_ERR_ARG, "fw_set_rigids: bad sizes or pointers");
   c->h_rigid.assign(n, Rigid{});
   for (int a = 0; a < n; ++a) {
-    const float* q = params + 16 * (size_t)a;
+    const float* q = params + 20 * (size_t)a;
     Rigid& g = c->h_rigid[a];
     g.type = ints[4 * a];
     g.bc = ints[4 * a + 1];
     g.in_contact = ints[4 * a + 2];
     g.scene = ints[4 * a + 3];
-    if (g.type != fw::RIGID_BALL && g.type != fw::RIGID_BOX && g.type != fw::RIGID_CAPSULE)
-      return fail(c, FW_ERR_ARG, "rigid %d: type %d is not a ball, box or capsule", a, g.type);
+    if (g.type != fw::RIGID_BALL && g.type != fw::RIGID_BOX && g.type != fw::RIGID_CAPSULE &&
+        g.type != fw::RIGID_ANALYTICAL)
+      return fail(c, FW_ERR_ARG, "rigid %d: type %d is not a ball, box, capsule or analytical entry", a, g.type);
     g.c[0] = q[0]; g.c[1] = q[1]; g.prim[0] = q[2]; g.prim[1] = q[3];
     g.radius = q[4]; g.quat = q[5]; g.mass = q[6]; g.inertia = q[7];
     g.V[0] = q[8]; g.V[1] = q[9]; g.W = q[10];
     g.bcT[0] = q[11]; g.bcT[1] = q[12]; g.bcG[0] = q[13]; g.bcG[1] = q[14]; g.bcR = q[15];
+    g.lb[0] = q[16]; g.lb[1] = q[17]; g.ub[0] = q[18]; g.ub[1] = q[19];  // an analytical entry's first box
   }
   c->h_gbox.resize(n_ground);
   c->h_gkind.resize(n_ground);
@@ -2035,6 +2043,17 @@ int fw_add_rigid_pair(fw_ctx* c, int32_t body, int32_t rigid, float penalty, flo
   p.f[0] = friction;
   const float zero[2] = {0.0f, 0.0f};
   return add_pair(c, p, zero, zero);
+}
+
+int fw_gate_by_rigid(fw_ctx* c, int32_t entry) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized) return fail(c, FW_ERR_STATE, "fw_gate_by_rigid after fw_finalize");
+  if (c->h_pairs.empty() || c->h_pairs.back().kind == fw::PAIR_RIGID)
+    return fail(c, FW_ERR_STATE, "fw_gate_by_rigid: the last pair added is not a ground pair");
+  if (entry < 0 || entry >= (int)c->h_rigid.size())
+    return fail(c, FW_ERR_ARG, "fw_gate_by_rigid: entry %d outside [0, %d)", entry, (int)c->h_rigid.size());
+  c->h_pairs.back().gate = entry + 1;
+  return FW_OK;
 }
 
 int fw_set_rigid_clocks(fw_ctx* c, const int32_t* every, const float* dt, const float* damping) {

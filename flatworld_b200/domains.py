@@ -65,15 +65,14 @@ class FemDomain(DomainBase):
 
 
 class GroundDomain(DomainBase):
-    """Static ground plane through ``point`` with unit ``normal``
-    (reference: flatworld/grounddomain.py:18-77)."""
+    """Ground plane through ``point`` with unit ``normal`` (reference:
+    flatworld/grounddomain.py:18-77).  With BCs (e.g. ``Fixed([0])``,
+    ``EnforceVel``) the rigid manager moves it; as in the reference, FEM bodies
+    keep contacting the plane of construction time, while the broad-phase
+    boxes of the loop's grounds follow the moving entry."""
 
     def __init__(self, d, point, normal, bcs=[], considerContact=True, considerGroundContact=True,
                  initials=[]):
-        if len(bcs) > 0 or len(initials) > 0:
-            raise NotImplementedError(
-                "GroundDomain with bcs/initials is a moving rigid plane, driven by the rigid-body "
-                "solver; flatworld_b200 implements static grounds only")
         self.d = d
         self.point = np.asarray(point, dtype=np.float32)
         n = np.asarray(normal, dtype=np.float32)
@@ -89,10 +88,23 @@ class GroundDomain(DomainBase):
         self.category_bits = COLLISION_CATEGORY_GROUND
         self.collide_bits = COLLISION_MASK_ALL
 
+    def attach(self, loop, entry):
+        """A loop with a moving plane holds this ground as rigid-manager entry ``entry``."""
+        self._loop = loop
+        self._entry = int(entry)
+
     def getCurrentRefPoint(self):
+        if getattr(self, "_loop", None) is not None:
+            return self._loop._entry_state()[self._entry, 0:2].astype(np.float32)
         return self.point.copy()
 
     def getCurrentNormal(self):
+        """The normal rotated by the entry's angle (grounddomain.py:47-51)."""
+        if getattr(self, "_loop", None) is not None:
+            a = float(self._loop._entry_state()[self._entry, 2])
+            c, s = np.float32(np.cos(a)), np.float32(np.sin(a))
+            n = self.normal.astype(np.float32)
+            return np.array([c * n[0] - s * n[1], s * n[0] + c * n[1]], dtype=np.float32)
         return self.normal.astype(np.float32)
 
     def getBBox(self):

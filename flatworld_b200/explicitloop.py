@@ -177,12 +177,12 @@ class _AABBView:
         lp = self._loop
         out = np.zeros((lp._max_domains, 2, 2), np.float32)
         boxes = lp._native.read_aabb(lp._packed.B)
-        rig = lp._rigid_state() if lp._layout.rigids else None
+        ent = lp._entry_state() if lp._layout.entries else None
         for i, d in enumerate(lp.domains):
-            if d.type == DomainType.RIGID:
-                k = lp._layout.rigids.index(d)
-                out[i, 0] = rig[k, 8:10]
-                out[i, 1] = rig[k, 10:12]
+            if ent is not None and any(d is e for e in lp._layout.entries):
+                k = next(j for j, e in enumerate(lp._layout.entries) if e is d)
+                out[i, 0] = ent[k, 8:10]
+                out[i, 1] = ent[k, 10:12]
             elif d.type in (DomainType.FEM, DomainType.SPRINGMASS):
                 k = lp._packed.scenes[0].fem.index(d)
                 b = lp._packed.scene_bodies[0][k]
@@ -205,7 +205,9 @@ class RigidManager:
     def __init__(self, loop):
         self._loop = loop
         self.numRigids = len(loop._layout.rigids)
-        self.needUpdate = self.numRigids > 0
+        self.numAnalytical = len(loop._layout.grounds)
+        self.movingAnalytical = loop._layout.moving
+        self.needUpdate = len(loop._layout.entries) > 0
         self._prim = [np.asarray(loop._packed.rigid_records()[0][k, 2:4]) for k in range(self.numRigids)]
 
     def _col(self, sl):
@@ -281,11 +283,12 @@ class ExplicitLoop:
         self.femSpringManager = FemSpringManager(self, self._packed, self._native, 0)
         self._flex_clock = None
         self._rigid_clock = None
-        if layout.rigids:
+        if layout.entries:  # rigid bodies, or the analytical entries of a loop with a moving plane
             self.rigidManager = RigidManager(self)
             self.rigid_update_times = 0
-            for k, d in enumerate(layout.rigids):
-                d.attach(self, k)
+            for k, d in enumerate(layout.entries):
+                if d.type in (DomainType.RIGID, DomainType.ANALYTICAL):  # height fields / voxel grids keep no state
+                    d.attach(self, k)
 
     def _clock(self, dt: float):
         """Hand the substep's float64 dt to the FEM-FEM hash-refresh clock
@@ -295,7 +298,7 @@ class ExplicitLoop:
         if self._layout.flex and dt != self._flex_clock:
             self._native.set_flex_clock(dt)
             self._flex_clock = dt
-        if self._layout.rigids and dt != self._rigid_clock:
+        if self._layout.entries and dt != self._rigid_clock:
             every = max(1, RigidManager.stableTime // dt)
             self._native.set_rigid_clock(int(every), float(np.float32(every * dt)),
                                          float(np.float32(self.damping)))
@@ -303,7 +306,12 @@ class ExplicitLoop:
 
     def _rigid_state(self):
         """float32[numRigids, 12]: center, angle, V, angular velocity, U, box."""
-        st, flags = self._native.read_rigids(len(self._layout.rigids))
+        return self._entry_state()[:len(self._layout.rigids)]
+
+    def _entry_state(self):
+        """float32[entries, 12]: the rigids, then the analytical entries of a
+        loop with a moving plane."""
+        st, flags = self._native.read_rigids(len(self._layout.entries))
         if flags & 1:
             raise RuntimeError("a rigid body came within 0.01 of a ground or another contact rigid (rigid-rigid "
                                "and rigid-ground contact, the reference's constraint solve, are outside "
@@ -316,7 +324,7 @@ class ExplicitLoop:
         self._clock(self.dt)
         self._native.step(1, float(np.float32(self.dt)))
         self._counter_py += 1
-        if self._layout.rigids:
+        if self._layout.entries:
             self.rigid_update_times += 1
 
     def advance_n(self, n: int, dt: float | None = None):
@@ -326,7 +334,7 @@ class ExplicitLoop:
         self._clock(self.dt)
         self._native.step(int(n), float(np.float32(self.dt)))
         self._counter_py += int(n)
-        if self._layout.rigids:
+        if self._layout.entries:
             self.rigid_update_times += int(n)
 
     def advanceWithTime(self, frame_dt: float = 1.0 / 60.0, verbose: bool = False):
@@ -340,7 +348,7 @@ class ExplicitLoop:
             self._native.step(n, float(np.float32(sub)))
             self._counter_py += n
             total += n
-        if self._layout.rigids:
+        if self._layout.entries:
             self.rigid_update_times += total
         if verbose:
             print(f"Completed {total} substeps for {frame_dt} seconds of simulation time.")

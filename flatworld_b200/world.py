@@ -186,6 +186,14 @@ class SceneLayout:
         # RigidManager: rigid bodies in domain order (rigidmanager.py:2448-2480)
         self.rigids = [d for d in domains if d.type == DomainType.RIGID]
         self.grounds = [d for d in domains if d.type in _GROUND_TYPES]
+        # a ground plane with BCs makes the rigid manager move its analytical
+        # entries (planes, height fields, voxel grids, in domain order) and
+        # recompute their broad-phase boxes (rigidmanager.py:2510-2517, 2580-2586)
+        self.moving = any(d.type == DomainType.ANALYTICAL and len(d.bcs) > 0 for d in domains)
+        if self.moving and self.rigids:
+            raise NotImplementedError("a ground plane with BCs together with rigid bodies: the clearance check "
+                                      "of the rigids against a moving plane is not part of flatworld_b200")
+        self.entries = self.rigids + (self.grounds if self.moving else [])
         # FEM-FEM pairs in contact-creation order (mixedcontact.py:1869-1935); the
         # loop skips the BVH (all pairs stay active / plain box tests) when it has
         # no ground contact and at most one contact rigid (explicitloop.py:362-373)
@@ -314,12 +322,18 @@ class PackedWorld:
         rigids: float32[6] (kind, point + normal or box, scene)."""
         params, ints, boxes = [], [], []
         for si, sc in enumerate(self.scenes):
-            if not sc.rigids:
+            if not sc.entries:
                 continue
             for dom in sc.rigids:
                 p, i = rigid_record(dom)
                 params.append(p)
                 ints.append([*i, si])
+            for g in (sc.grounds if sc.moving else []):
+                p, i = analytical_record(g)
+                params.append(p)
+                ints.append([*i, si])
+            if not sc.rigids:
+                continue
             for g in sc.grounds:  # plane: kind 0, point, normal; height field / voxel grid: kind 1, box
                 if g.type == DomainType.ANALYTICAL:
                     boxes.append([0.0, *np.asarray(g.point, np.float32)[:2], *np.asarray(g.normal, np.float32)[:2],
@@ -329,15 +343,27 @@ class PackedWorld:
                     boxes.append([1.0, *np.asarray(lo, np.float32).reshape(2), *np.asarray(hi, np.float32).reshape(2),
                                   si])
         as2 = lambda a, w, dt: np.asarray(a, dt).reshape(-1, w)  # noqa: E731
-        return as2(params, 16, np.float32), as2(ints, 4, np.int32), as2(boxes, 6, np.float32)
+        return as2(params, 20, np.float32), as2(ints, 4, np.int32), as2(boxes, 6, np.float32)
 
     def rigid_offsets(self):
-        """Index of each scene's first rigid in the world's rigid list."""
+        """Index of each scene's first entry (rigids, then the analytical
+        entries of a loop with a moving plane) in the world's entry list."""
         off, n = [], 0
         for sc in self.scenes:
             off.append(n)
-            n += len(sc.rigids)
+            n += len(sc.entries)
         return off
+
+    def ground_gate_entries(self):
+        """Per pair of pair_records(): the entry whose current box gates it
+        (a ground pair of a loop with a moving plane), else -1."""
+        out = []
+        r_off = self.rigid_offsets()
+        for si, sc in enumerate(self.scenes):
+            for c in sc.pairs:
+                moving_ground = sc.moving and c.kind != "rigid"
+                out.append(r_off[si] + sc.entries.index(c.ground) if moving_ground else -1)
+        return out
 
     def flex_records(self):
         """Per scene with FEM-FEM pairs: (scene, skip_bvh, dom_obj, dom_body,
@@ -348,7 +374,7 @@ class PackedWorld:
                 continue
             fem_index = {id(d): k for k, d in enumerate(sc.fem)}
             dom_obj = np.asarray([1 if d.considerContact else 0 for d in sc.domains], np.int32)
-            rig_index = {id(d): self.rigid_offsets()[si] + k for k, d in enumerate(sc.rigids)}
+            rig_index = {id(d): self.rigid_offsets()[si] + k for k, d in enumerate(sc.entries)}
             dom_body = np.asarray([self.body_of[(si, fem_index[id(d)])] if id(d) in fem_index
                                    else (-2 - rig_index[id(d)] if id(d) in rig_index else -1)
                                    for d in sc.domains], np.int32)
@@ -410,17 +436,20 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
         nw.set_spring_bodies(np.asarray([b for b, _ in packed.spring_bodies], np.int32),
                              np.asarray([m for _, m in packed.spring_bodies], np.float32))
     nw.set_scenes(np.asarray([s.damping for s in packed.scenes], np.float32))
-    if any(sc.rigids for sc in packed.scenes):
+    if any(sc.entries for sc in packed.scenes):
         nw.set_rigids(*packed.rigid_records())
-    for kind, body, pen, lo, hi, g in packed.pair_records():
+    for (kind, body, pen, lo, hi, g), gate in zip(packed.pair_records(), packed.ground_gate_entries()):
         if kind == "rigid":  # (rigid index, friction, skip_bvh) in the box slots
             nw.add_rigid_pair(body, lo, pen, hi, 1 if g else 0)
-        elif kind == "plane":
+            continue
+        if kind == "plane":  # the plane of construction time, also when it moves (mixedcontact.py:1815-1818)
             nw.add_plane(body, pen, lo, hi, g.point, g.normal)
         elif kind == "heightfield":
             nw.add_heightfield(body, pen, lo, hi, g.height, g.lb[0], g.ub[0], 1 if g.reverse else 0)
         else:
             nw.add_voxel(body, pen, lo, hi, np.asarray(g.occ, np.int32), g.lb[0], g.lb[1], g.dx, g.dz)
+        if gate >= 0:
+            nw.gate_by_rigid(gate)
     flex = packed.flex_records()
     if flex:
         nw.set_boundary_edges(packed.bedges, packed.beoff, packed.becnt)
@@ -446,11 +475,11 @@ def rigid_record(dom):
     """One rigid as RigidManager stores it: RigidBodyDomain.attach (initial
     conditions, rigiddomain.py:118-124), packRigidParams (rigidmanager.py:
     2250-2400) and processConditions / _addBcValue (2527-2567), in that order.
-    Returns float32[16] (center, primary, radius, angle, mass, inertia, V,
-    angular velocity, BC translation value, gravity, BC rotation value) and
-    int32[3] (type, BC bits, considerContact)."""
+    Returns float32[20] (center, primary, radius, angle, mass, inertia, V,
+    angular velocity, BC translation value, gravity, BC rotation value, 4
+    unused) and int32[3] (type, BC bits, considerContact)."""
     r = dom.rigid
-    f = np.zeros(16, np.float32)
+    f = np.zeros(20, np.float32)
     for ic in dom.initials:
         ids = [0] if getattr(ic, "is_all_nodes", False) else [int(n) for n in np.asarray(ic.nds).reshape(-1)]
         if ids != [0]:
@@ -471,8 +500,39 @@ def rigid_record(dom):
         f[4] = _as_float(r.getRadius())
     f[5] = _as_float(r.angle)
     f[7] = float(r.inertia_body)
+    bits = _rigid_bcs(dom.bcs, f)
+    return f, np.array([int(r.rtype), bits, 1 if dom.considerContact else 0], np.int32)
+
+
+def analytical_record(g):
+    """The rigid manager's entry for a ground of a loop with a moving plane
+    (processDomains_, rigidmanager.py:2486-2517; GroundDomain.attach's initial
+    conditions; processConditions): a plane's point and normal as its center
+    and primary vector (zero for a height field or voxel grid, whose entries
+    the reference never fills), mass 1e10, its BCs, and its getBBox() as the
+    first broad-phase box."""
+    f = np.zeros(20, np.float32)
+    if g.type == DomainType.ANALYTICAL:
+        f[0], f[1] = _as_vec2(g.point)
+        f[2], f[3] = _as_vec2(g.normal)
+    f[6] = 1e10
+    for ic in getattr(g, "initials", []):
+        if ic.type in (VTYPE, ATYPE):
+            f[8], f[9] = _as_vec2(ic.vel)
+        else:
+            f[10] = _as_float(ic.ang_vel)
+    bits = _rigid_bcs(getattr(g, "bcs", []), f)
+    lo, hi = g.getBBox()
+    f[16], f[17] = _as_vec2(lo)
+    f[18], f[19] = _as_vec2(hi)
+    return f, np.array([64, bits, 1 if g.considerContact else 0], np.int32)
+
+
+def _rigid_bcs(bcs, f):
+    """processConditions -> _addBcValue (rigidmanager.py:2527-2553) on one
+    entry's record; returns its BC bits."""
     bits = 0
-    for bc in dom.bcs:
+    for bc in bcs:
         t, _, value = bc.processData()
         t = int(t)
         bits |= t
@@ -496,7 +556,7 @@ def rigid_record(dom):
             f[13], f[14] = _as_vec2(value)
         else:  # ATYPE, FORCETYPE
             f[11], f[12] = _as_vec2(value)
-    return f, np.array([int(r.rtype), bits, 1 if dom.considerContact else 0], np.int32)
+    return bits
 
 
 def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):

@@ -184,12 +184,15 @@ int fw_mass_scaling(fw_ctx* ctx, float dt_target);
 int fw_read_flex_state(fw_ctx* ctx, int32_t* item_cache, int32_t n_items, float* grid);
 
 /* Rigid primitives touching FEM bodies (RigidBodyDomain with BallRigid /
- * BoxRigid / CapsuleRigid), before fw_finalize, gather path.  Per rigid 16
- * floats -- center x, y; primary x, y (box: full extents; capsule: lower end
- * minus center); radius; angle; mass; inertia; velocity x, y; angular
- * velocity; BC translation value x, y; gravity x, y; BC rotation value -- and
- * 4 ints: RigidType (1 ball, 2 box, 8 capsule), BC bits (definitions.py:
- * 96-104), considerContact, scene; rigids grouped by scene in ascending order.
+ * BoxRigid / CapsuleRigid) and the rigid manager's analytical entries of
+ * loops with a moving ground plane, before fw_finalize, gather path.  Per
+ * entry 20 floats -- center x, y; primary x, y (box: full extents; capsule:
+ * lower end minus center; analytical: the plane normal); radius; angle; mass;
+ * inertia; velocity x, y; angular velocity; BC translation value x, y;
+ * gravity x, y; BC rotation value; an analytical entry's first box lb x, y,
+ * ub x, y -- and 4 ints: type (1 ball, 2 box, 8 capsule, 64 analytical), BC
+ * bits (definitions.py:96-104), considerContact, scene; grouped by scene in
+ * ascending order.
  * grounds: 6 floats per ground domain -- kind 0 (plane): point x, y, normal
  * x, y; kind 1 (height field, voxel grid): box lb x, y, ub x, y; then its
  * scene (grouped by scene too).  A rigid that comes within 0.01 of a
@@ -209,6 +212,13 @@ int fw_set_rigids(fw_ctx* ctx, int32_t n, const float* params, const int32_t* in
  * field, voxel.  Replaces _build_batched_contacts' rigid work lists and
  * _batched_rigid_prim_kernel, mixedcontact.py:1963-2130, 1026-1115. */
 int fw_add_rigid_pair(fw_ctx* ctx, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh);
+/* The last ground pair added (plane, height field, voxel) is gated by the
+ * current box of analytical entry `entry` (fw_set_rigids) instead of its
+ * static box: in a loop where some ground plane has BCs, every ground's
+ * broad-phase box follows the rigid manager (rigidmanager.py:950-964), while
+ * the contact itself keeps the plane of construction time
+ * (mixedcontact.py:1815-1818). */
+int fw_gate_by_rigid(fw_ctx* ctx, int32_t entry);
 /* The rigid update schedule of the coming substeps: the rigids move every
  * `every` substeps by dt (the reference's N = max(1, 1e-3 // dt) and N * dt,
  * explicitloop.py:533-538, computed by the caller from its float64 dt), with

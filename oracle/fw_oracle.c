@@ -146,6 +146,7 @@ static float or_logf(float x) {
 typedef struct {
   int kind;
   int body;
+  int entry; /* >= 0: gated by that rigid manager entry's current box (a loop with a moving plane) */
   REAL penalty;
   REAL glb[2], gub[2]; /* ground getBBox(), gate box */
   /* plane */
@@ -450,10 +451,16 @@ static REAL voxel_signed(const or_pair* c, REAL px, REAL py, REAL* nx_out, REAL*
  * overlap (bvh.py:40-46 inclusive test).  On steps with counter % 100 == 0 the
  * tree is rebuilt from boxes grown by 10% of their extent (bvh.py:321-342); on
  * the other steps the leaves are refit to the raw boxes (bvh.py:393-416). */
+static const REAL* rigid_domain_box(const or_world* w, int r); /* a rigid manager entry's current box */
+
 static int pair_active(const or_world* w, const or_pair* c, long counter) {
   const REAL* bb = w->aabb + 4 * c->body;
   REAL alo[2] = {bb[0], bb[1]}, ahi[2] = {bb[2], bb[3]};
   REAL blo[2] = {c->glb[0], c->glb[1]}, bhi[2] = {c->gub[0], c->gub[1]};
+  if (c->entry >= 0) {
+    const REAL* e = rigid_domain_box(w, c->entry);
+    blo[0] = e[0]; blo[1] = e[1]; bhi[0] = e[2]; bhi[1] = e[3];
+  }
   if (counter % 100 == 0) {
     for (int k = 0; k < 2; ++k) {
       REAL ba = (REAL)0.1 * (ahi[k] - alo[k]);
@@ -904,8 +911,6 @@ static int boxes_overlap(const REAL* a, const REAL* b, long counter) {
   return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
 }
 
-static const REAL* rigid_domain_box(const or_world* w, int r); /* a rigid's current box (below) */
-
 static const REAL* dom_box(const or_world* w, int g) {
   const or_flex* f = w->flex;
   if (f->dom_body[g] <= -2) return rigid_domain_box(w, -2 - f->dom_body[g]);
@@ -1039,10 +1044,13 @@ static void r_sincos(REAL x, REAL* s, REAL* c) {
 #endif
 }
 
-/* RigidType (flatworld/definitions.py:50-53) */
+/* RigidType (flatworld/definitions.py:50-53); 64: an analytical entry of the
+ * rigid manager (ground plane, height field, voxel grid) in a loop where some
+ * ground plane has BCs (rigidmanager.py:2486-2517) */
 #define RIGID_BALL 1
 #define RIGID_BOX 2
 #define RIGID_CAPSULE 8
+#define RIGID_ANALYTICAL 64
 /* rigid BC bits (definitions.py:96-104) */
 #define RBC_U 0x1
 #define RBC_V 0x2
@@ -1088,7 +1096,14 @@ static void rot_of(REAL theta, REAL* m) {
  * getBoxBBox, getCapsuleBBox (utils.py:235-300). */
 static void rigid_aabb(or_rigid* g) {
   const REAL* m = g->rot;
-  if (g->type == RIGID_BALL) {
+  if (g->type == RIGID_ANALYTICAL) { /* _update_u_and_bbox_wp's moving-plane box (rigidmanager.py:950-964) */
+    const REAL nx = m[0] * g->prim[0] + m[1] * g->prim[1], ny = m[2] * g->prim[0] + m[3] * g->prim[1];
+    const REAL tx = -ny, ty = nx;
+    const REAL lox = g->c[0] - tx * (REAL)100.0 - nx * (REAL)0.1, loy = g->c[1] - ty * (REAL)100.0 - ny * (REAL)0.1;
+    const REAL hix = g->c[0] + tx * (REAL)100.0 + nx * (REAL)0.1, hiy = g->c[1] + ty * (REAL)100.0 + ny * (REAL)0.1;
+    g->lb[0] = rmin(lox, hix); g->lb[1] = rmin(loy, hiy);
+    g->ub[0] = rmax(lox, hix); g->ub[1] = rmax(loy, hiy);
+  } else if (g->type == RIGID_BALL) {
     g->lb[0] = g->c[0] - g->radius; g->lb[1] = g->c[1] - g->radius;
     g->ub[0] = g->c[0] + g->radius; g->ub[1] = g->c[1] + g->radius;
   } else if (g->type == RIGID_BOX) {
@@ -1271,6 +1286,7 @@ void or_rigid_update(or_world* w, float dt_f, float damping_f) {
   const REAL dt = (REAL)dt_f, damping = (REAL)damping_f, cl = (REAL)RIGID_CLEARANCE;
   for (int a = 0; a < R->n; ++a) {
     const or_rigid* g = &R->r[a];
+    if (g->type == RIGID_ANALYTICAL) continue; /* not a rigid body */
     for (int q = 0; q < R->n_ground; ++q) {
       const REAL* b = R->gbox + 4 * q;
       /* written as "not clear", so that a non-finite box is flagged too */
@@ -1283,7 +1299,7 @@ void or_rigid_update(or_world* w, float dt_f, float damping_f) {
     }
     for (int q = a + 1; q < R->n; ++q) {
       const or_rigid* h = &R->r[q];
-      if (g->in_contact && h->in_contact &&
+      if (h->type != RIGID_ANALYTICAL && g->in_contact && h->in_contact &&
           !(g->lb[0] - cl > h->ub[0] || g->ub[0] + cl < h->lb[0] || g->lb[1] - cl > h->ub[1] ||
             g->ub[1] + cl < h->lb[1]))
         R->err = 1;
@@ -1293,6 +1309,7 @@ void or_rigid_update(or_world* w, float dt_f, float damping_f) {
   for (int a = 0; a < R->n; ++a) { /* _rigid_step_wp */
     or_rigid* g = &R->r[a];
     rot_of(g->quat, g->rot);
+    if (g->type == RIGID_ANALYTICAL) continue; /* the impulse pass covers the rigid bodies only */
     if (g->bc & RBC_A) {
       g->acc[0] = 0; g->acc[1] = 0;
     } else {
@@ -1392,7 +1409,15 @@ static or_pair* new_pair(or_world* w) {
   w->pairs = (or_pair*)realloc(w->pairs, sizeof(or_pair) * (size_t)(w->n_pairs + 1));
   or_pair* c = &w->pairs[w->n_pairs++];
   memset(c, 0, sizeof(*c));
+  c->entry = -1;
   return c;
+}
+
+/* The last ground pair added is gated by rigid manager entry `entry`'s box. */
+int or_gate_by_rigid(or_world* w, int entry) {
+  if (w->n_pairs == 0) return -1;
+  w->pairs[w->n_pairs - 1].entry = entry;
+  return 0;
 }
 
 /* Pairs must be added in launch order: planes, then heightfields, then voxels
@@ -1673,9 +1698,10 @@ void or_point_stress(int type, float E, float nu, float sy, float H, const float
 float or_log32(float x) { return R_LOG(x); }
 
 /* Rigid primitives (RigidManager.packRigidParams / processConditions,
- * rigidmanager.py:2250-2400, 2527-2567): per rigid 16 floats (center x, y,
+ * rigidmanager.py:2250-2400, 2527-2567): per entry 20 floats (center x, y,
  * primary x, y, radius, angle, mass, inertia, V x, y, angular velocity, BC
- * translation value x, y, gravity x, y, BC rotation value) and 3 ints (type,
+ * translation value x, y, gravity x, y, BC rotation value, an analytical
+ * entry's first box) and 3 ints (type,
  * BC bits, considerContact); the static grounds, 5 floats each (kind 0 plane:
  * p x, y, n x, y; kind 1 box: lb x, y, ub x, y).  The
  * rotation cache and boxes are set as precompute_rigid_transforms + updateBBox
@@ -1686,14 +1712,19 @@ int or_set_rigids(or_world* w, int n, const float* f, const int32_t* iv, int n_g
   R->r = (or_rigid*)calloc((size_t)(n ? n : 1), sizeof(or_rigid));
   for (int a = 0; a < n; ++a) {
     or_rigid* g = &R->r[a];
-    const float* q = f + 16 * a;
+    const float* q = f + 20 * a;
     g->type = iv[3 * a]; g->bc = iv[3 * a + 1]; g->in_contact = iv[3 * a + 2];
     g->c[0] = q[0]; g->c[1] = q[1]; g->prim[0] = q[2]; g->prim[1] = q[3];
     g->radius = q[4]; g->quat = q[5]; g->mass = q[6]; g->inertia = q[7];
     g->V[0] = q[8]; g->V[1] = q[9]; g->W = q[10];
     g->bcT[0] = q[11]; g->bcT[1] = q[12]; g->bcG[0] = q[13]; g->bcG[1] = q[14]; g->bcR = q[15];
     rot_of(g->quat, g->rot);
-    rigid_aabb(g);
+    if (g->type == RIGID_ANALYTICAL) { /* an analytical entry starts at getBBox() */
+      g->lb[0] = q[16]; g->lb[1] = q[17]; g->ub[0] = q[18]; g->ub[1] = q[19];
+      g->box[0] = q[16]; g->box[1] = q[17]; g->box[2] = q[18]; g->box[3] = q[19];
+    } else {
+      rigid_aabb(g);
+    }
   }
   R->n_ground = n_ground;
   R->gbox = (REAL*)calloc(4 * (size_t)(n_ground ? n_ground : 1), sizeof(REAL));

@@ -96,6 +96,7 @@ def _lib(precision: str):
         L.or_get_rigids.argtypes = [C.c_void_p, _f64p]
         L.or_get_rigids.restype = C.c_int
         L.or_sincos32.argtypes = [C.c_float, _f32p, _f32p]
+        L.or_gate_by_rigid.argtypes = [C.c_void_p, C.c_int]
         _LIBS[name] = L
     return _LIBS[name]
 
@@ -338,6 +339,16 @@ class OracleLoop:
         if len({id(c[2]) for c in vox}) > 1:
             unbatched += len(vox)
             vox = []
+        # a ground plane with BCs: the rigid manager moves its analytical entries
+        # (planes, height fields, voxel grids, in domain order), and every
+        # ground pair is gated by its entry's current box (rigidmanager.py:
+        # 2486-2517, 2580-2586, 950-964); the contact keeps the first plane
+        rigid_doms = [d for d in domains if d.type == RIGID]
+        grounds = [d for d in domains if d.type in (ANALYTICAL, HEIGHTFIELD, VOXELMAP)]
+        self.moving = any(d.type == ANALYTICAL and len(d.bcs) > 0 for d in domains)
+        if self.moving and rigid_doms:
+            raise NotImplementedError("a moving ground plane together with rigid bodies")
+        entries = rigid_doms + (grounds if self.moving else [])
         for ct, femd, g, pen, _ in anal + hf + vox:
             body = fem.index(femd)
             lo, hi = self._ground_box(g)
@@ -355,20 +366,25 @@ class OracleLoop:
                 occ = _ip(np.asarray(g.occ, np.int32))
                 L.or_add_voxel(self._w, body, pen32, lo[1], hi[1], int(g.nx), int(g.ny), occ[1], float(g.lb[0]),
                                float(g.lb[1]), float(np.float32(g.dx)), float(np.float32(g.dz)))
+            if self.moving:
+                L.or_gate_by_rigid(self._w, entries.index(g))
         self.flex = flex
         # explicitloop.py:222-228, 362-373: no broad phase with <= 1 contact
         # domain; it is skipped without ground contact and with <= 1 contact rigid
-        rigid_doms = [d for d in domains if d.type == RIGID]
         rigid_needs_bvh = sum(1 for d in rigid_doms if d.considerContact) > 1
         no_bvh = len(cds) <= 1
         skip_bvh = 1 if (no_bvh or ((len(anal) + len(hf) + len(vox) + unbatched) == 0 and not rigid_needs_bvh)) else 0
         self.rigids = rigid_doms
+        self.entries = entries
         self.rigid_update_times = 0
-        if rigid_doms:
-            prm = np.zeros((len(rigid_doms), 16), np.float32)
-            ivs = np.zeros((len(rigid_doms), 3), np.int32)
-            for a, d in enumerate(rigid_doms):
-                self._pack_rigid(d, prm[a], ivs[a])
+        if entries:
+            prm = np.zeros((len(entries), 20), np.float32)
+            ivs = np.zeros((len(entries), 3), np.int32)
+            for a, d in enumerate(entries):
+                if d.type == RIGID:
+                    self._pack_rigid(d, prm[a], ivs[a])
+                else:
+                    self._pack_analytical(d, prm[a], ivs[a])
             gb = []
             for g in domains:  # plane (kind 0): point, normal; height field / voxel (kind 1): its box
                 if g.type == ANALYTICAL:
@@ -378,7 +394,7 @@ class OracleLoop:
             gbox = _fp(np.asarray(gb, np.float32).reshape(-1, 5))
             rp, ri = _fp(prm), _ip(ivs)
             self._keep += [rp, ri, gbox]
-            L.or_set_rigids(self._w, len(rigid_doms), rp[1], ri[1], len(gb), gbox[1])
+            L.or_set_rigids(self._w, len(entries), rp[1], ri[1], len(gb), gbox[1])
             for ct, femd, rig, pen, _ in contacts:
                 if ct == FLEXRIGID:
                     L.or_add_rigid_pair(self._w, fem.index(femd), rigid_doms.index(rig), float(np.float32(pen)),
@@ -394,11 +410,13 @@ class OracleLoop:
                 edges.append(e)
             dom_obj = [1 if d.considerContact else 0 for d in domains]
             # bodies by index, rigids as -2 - rigid index (their boxes move), grounds -1
+            in_entries = lambda d: any(d is e for e in entries)  # noqa: E731
             dom_body = [fem.index(d) if d.type in (FEM, SPRINGMASS) else
-                        (-2 - rigid_doms.index(d) if d.type == RIGID else -1) for d in domains]
+                        (-2 - next(k for k, e in enumerate(entries) if e is d) if in_entries(d) else -1)
+                        for d in domains]
             dom_box = np.zeros((len(domains), 4), np.float32)
             for i, d in enumerate(domains):
-                if d.type not in (FEM, SPRINGMASS, RIGID) and d.considerContact:
+                if d.type not in (FEM, SPRINGMASS) and not in_entries(d) and d.considerContact:
                     lo, hi = self._ground_box(d)
                     dom_box[i, :2] = lo[0]
                     dom_box[i, 2:] = hi[0]
@@ -443,6 +461,62 @@ class OracleLoop:
                 for nid in np.asarray(ic.nds):
                     v[int(nid)] = (vx, vy)
 
+    def _pack_analytical(self, g, f, iv):
+        """A ground's rigid-manager entry: processDomains_ (rigidmanager.py:
+        2486-2517: mass 1e10, a plane's point and normal in rigidParams),
+        GroundDomain.attach's initial velocity, then _addBcValue per BC; its
+        first broad-phase box is its getBBox()."""
+        if g.type == ANALYTICAL:
+            f[0], f[1] = float(np.float32(g.point[0])), float(np.float32(g.point[1]))
+            f[2], f[3] = float(np.float32(g.normal[0])), float(np.float32(g.normal[1]))
+        f[6] = 1e10
+        for ic in g.initials:
+            a = np.asarray(ic.vel, np.float32).reshape(-1)
+            f[8], f[9] = float(a[0]), float(a[1]) if a.size > 1 else 0.0
+        lo, hi = self._ground_box(g)
+        f[16], f[17] = lo[0]
+        f[18], f[19] = hi[0]
+        self._bc_bits(g.bcs, f, iv)
+        iv[0], iv[2] = 64, 1 if g.considerContact else 0
+
+    @staticmethod
+    def _bc_bits(bcs, f, iv):
+        """_addBcValue (rigidmanager.py:2527-2553) for each BC, in order."""
+        def first(v):
+            if hasattr(v, "__len__") and not isinstance(v, (str, bytes)):
+                return float(np.asarray(v, dtype=np.float32).reshape(-1)[0])
+            return float(v)
+
+        def vec2(v):
+            a = np.asarray(v, dtype=np.float32).reshape(-1)
+            return (float(a[0]), float(a[1]) if a.size > 1 else 0.0)
+
+        bits = 0
+        for bc in bcs:
+            t, _, value = bc.processData()
+            bits |= int(t)
+            if t == 0b1:  # UTYPE
+                f[11], f[12] = 0.0, 0.0
+                f[6] = 1e10
+            elif t == 0b100000:  # RTYPE
+                f[11], f[12] = 0.0, 0.0
+                f[6] = 1e10
+                f[7] = 1e10
+                f[15] = 0.0
+            elif t == 0b10:  # VTYPE
+                f[11], f[12] = vec2(value)
+                f[6] = 1e10
+            elif t == 0b1000000:  # ROTVTYPE
+                f[15] = first(value)
+                f[7] = 1e10
+            elif t in (0b10000000, 0b100000000):  # ROTATYPE, TORQUETYPE
+                f[15] = first(value)
+            elif t == 0b10000:  # GRAVITY
+                f[13], f[14] = vec2(value)
+            else:
+                f[11], f[12] = vec2(value)
+        iv[1] = bits
+
     @staticmethod
     def _pack_rigid(d, f, iv):
         """One rigid, in the reference's order: attach's initial conditions
@@ -475,31 +549,8 @@ class OracleLoop:
             f[4] = first(r.getRadius())
         f[5] = first(r.angle)
         f[7] = first(r.inertia_body)
-        bits = 0
-        for bc in d.bcs:
-            t, _, value = bc.processData()
-            bits |= int(t)
-            if t == 0b1:  # UTYPE
-                f[11], f[12] = 0.0, 0.0
-                f[6] = 1e10
-            elif t == 0b100000:  # RTYPE
-                f[11], f[12] = 0.0, 0.0
-                f[6] = 1e10
-                f[7] = 1e10
-                f[15] = 0.0
-            elif t == 0b10:  # VTYPE
-                f[11], f[12] = vec2(value)
-                f[6] = 1e10
-            elif t == 0b1000000:  # ROTVTYPE
-                f[15] = first(value)
-                f[7] = 1e10
-            elif t in (0b10000000, 0b100000000):  # ROTATYPE, TORQUETYPE
-                f[15] = first(value)
-            elif t == 0b10000:  # GRAVITY
-                f[13], f[14] = vec2(value)
-            else:
-                f[11], f[12] = vec2(value)
-        iv[0], iv[1], iv[2] = int(r.rtype), bits, 1 if d.considerContact else 0
+        OracleLoop._bc_bits(d.bcs, f, iv)
+        iv[0], iv[2] = int(r.rtype), 1 if d.considerContact else 0
 
     @staticmethod
     def _seg_penalty(dom):
@@ -554,7 +605,7 @@ class OracleLoop:
                     self.sh_elapsed = 0.0
             self._L.or_step(self._w, float(np.float32(d)), float(np.float32(self.damping)), self.counter, 0)
             self.counter += 1
-            if self.rigids:  # explicitloop.py:533-538
+            if self.entries:  # explicitloop.py:533-538
                 every = max(1, 1.0e-3 // d)
                 self.rigid_update_times += 1
                 if self.rigid_update_times % every == 0:
@@ -610,9 +661,15 @@ class OracleLoop:
     def rigid_state(self):
         """(float64[n, 12] per rigid: center, angle, V, angular velocity, U,
         box lb, ub; error flag)."""
-        out = np.zeros((max(len(self.rigids), 1), 12))
+        st, err = self.entry_state()
+        return st[:len(self.rigids)], err
+
+    def entry_state(self):
+        """The same for every rigid-manager entry (rigids, then the analytical
+        entries of a loop with a moving plane)."""
+        out = np.zeros((max(len(self.entries), 1), 12))
         err = self._L.or_get_rigids(self._w, out.ctypes.data_as(_f64p))
-        return out[:len(self.rigids)], err
+        return out[:len(self.entries)], err
 
     def aabb(self):
         out = np.zeros((len(self.fem), 4))

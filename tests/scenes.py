@@ -387,3 +387,28 @@ def rigid_bcs(fw):
     cap = fw.RigidBodyDomain(fw.CapsuleRigid(2, [0.76, 0.1195], [0.84, 0.1195], [0.0], 0.02, 1.0),
                              [fw.Fixed([0]), fw.EnforceRotAcc([0], 5.0)], friction=0.3)
     return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), slab, ball, box, cap]
+
+
+def ground_circle(fw, bcs=None, plane_y=0.3):
+    """The reference's FEM-analytical scene (test2D/test_2Dfem_contact.py,
+    test_2Dfemanalytic_contact.py): an Elastic circle of radius 0.1 at
+    (0.5, 0.5) under gravity 10 over the plane y = plane_y; ``bcs`` on the
+    ground (the reference's example scripts often fix it: [Fixed([0])])."""
+    mesh = fw.FEMesher(2).createCircle([0.5, 0.5], 0.1)
+    fem = fw.FemDomain(mesh, fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)), [fw.Gravity([0, -10.0])])
+    return [fw.GroundDomain(2, [0.0, plane_y], [0.0, 1.0], bcs or []), fem]
+
+
+def fixed_ground_heightfield(fw, fixed=True):
+    """A circle dropped on a height-field bowl, with a ground plane far below;
+    the plane fixed by a BC or not.  With the BC the rigid manager recomputes
+    every ground's broad-phase box each update, and the height field's entry
+    (whose point and normal the reference never fills) collapses to the
+    origin, so the circle falls through the bowl onto the plane."""
+    x = np.linspace(0.0, 1.0, 64)
+    h = (0.3 + 0.4 * (x - 0.5) ** 2).astype(np.float32)
+    hf = fw.HeightFieldDomain(2, h, [0.0, 0.0], [1.0, 1.0])
+    mesh = fw.FEMesher(2).createCircle([0.5, 0.55], 0.08)
+    fem = fw.FemDomain(mesh, fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)), [fw.Gravity([0, -10.0])])
+    ground = fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0], [fw.Fixed([0])] if fixed else [])
+    return [ground, hf, fem]

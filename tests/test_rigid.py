@@ -130,7 +130,7 @@ def test_layout_matches_oracle():
             assert lay.rigids.index(a.ground) == o.rigids.index(b[2])
         params, ints, grounds = PackedWorld([lay]).rigid_records()
         for k, d in enumerate(lay.rigids):
-            f = np.zeros(16, np.float32)
+            f = np.zeros(20, np.float32)
             iv = np.zeros(3, np.int32)
             OracleLoop._pack_rigid(d, f, iv)
             assert np.array_equal(params[k], f) and np.array_equal(ints[k, :3], iv), (build.__name__, k)
@@ -244,3 +244,67 @@ def test_gpu_rigid_near_ground_raises():
         lp.synchronize()
     with pytest.raises(RuntimeError):
         lp._native.snapshot(0)
+
+
+# ---- ground planes with BCs (the rigid manager's moving analytical entries)
+
+def test_oracle_fixed_ground_equals_static():
+    """A ground with Fixed([0]) (common in the reference's example scripts)
+    gives the same bits as a static one while the body stays within the
+    moving-plane boxes' +-100 span."""
+    a = OracleLoop(scenes.ground_circle(fw), useAdapativeDT=True)
+    b = OracleLoop(scenes.ground_circle(fw, [fw.Fixed([0])]), useAdapativeDT=True)
+    for _ in range(60):
+        a.advance_with_time(FRAME)
+        b.advance_with_time(FRAME)
+    assert np.array_equal(a.state()[0], b.state()[0])
+    st, err = b.entry_state()
+    assert err == 0 and np.allclose(st[0, 8:12], [-100.0, 0.2, 100.0, 0.4])  # box now +-100 x +-0.1
+
+
+def test_oracle_moving_plane_moves_gates_not_contact():
+    """EnforceVel moves the plane's entry (and its broad-phase box) down at
+    0.5 m/s; the contact keeps the plane of construction time, so once the
+    box has left the body, the body falls through y = 0.3
+    (mixedcontact.py:1815-1818 copy the plane at build time)."""
+    m = OracleLoop(scenes.ground_circle(fw, [fw.EnforceVel([0], [0.0, -0.5])]), useAdapativeDT=True)
+    for _ in range(30):
+        m.advance_with_time(FRAME)
+    st, err = m.entry_state()
+    assert err == 0 and abs(st[0, 1] - (0.3 - 0.5 * 30 * FRAME)) < 0.02  # whole rigid updates of N dt
+    assert m.state()[0][:, 1].min() < 0.25
+
+
+def test_oracle_fixed_ground_collapses_heightfield_box():
+    """With a plane under BCs the height field's entry box becomes the origin
+    point after the first update and the circle falls through the bowl onto
+    the plane (without the BC it rests in the bowl)."""
+    runs = {}
+    for fixed in (False, True):
+        o = OracleLoop(scenes.fixed_ground_heightfield(fw, fixed), useAdapativeDT=True)
+        for _ in range(60):
+            o.advance_with_time(FRAME)
+        runs[fixed] = o
+    assert runs[False].state()[0][:, 1].min() > 0.3
+    assert runs[True].state()[0][:, 1].min() < 0.2
+    assert np.array_equal(runs[True].entry_state()[0][1, 8:12], [0.0, 0.0, 0.0, 0.0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,frames", [("fixed", 40), ("moving", 30), ("hf", 40)])
+def test_gpu_moving_ground_equals_oracle(name, frames):
+    build = {"fixed": lambda: scenes.ground_circle(fw, [fw.Fixed([0])]),
+             "moving": lambda: scenes.ground_circle(fw, [fw.EnforceVel([0], [0.0, -0.5])]),
+             "hf": lambda: scenes.fixed_ground_heightfield(fw, True)}[name]
+    lp = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True)
+    o = oracle.OracleLoop(build(), useAdapativeDT=True)
+    n = o.N
+    for f in range(frames):
+        lp.advanceWithTime(FRAME)
+        o.advance_with_time(FRAME)
+        xo, vo, _ = o.state()
+        assert np.array_equal(lp.femSpringManager.coords.numpy()[:n].astype(np.float64), xo), (name, f)
+        assert np.array_equal(lp.femSpringManager.V.numpy()[:n].astype(np.float64), vo), (name, f)
+        assert np.array_equal(lp._entry_state().astype(np.float64), o.entry_state()[0]), (name, f)
+    g = lp.domains[0]
+    assert np.array_equal(g.getCurrentRefPoint(), lp._entry_state()[0, :2])
