@@ -31,8 +31,9 @@ class DiffSim:
 
     def __init__(self, domains, dt, n_steps, checkpoint_every=50, device=0, damping=0.0, path="auto"):
         self.layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=False)
-        if self.layout.rigids:
-            raise NotImplementedError("the adjoint covers FEM triangles; rigid bodies are not differentiated")
+        if self.layout.entries:
+            raise NotImplementedError("the adjoint covers FEM triangles; rigid bodies and ground planes with BCs "
+                                      "are not differentiated")
         self.packed = PackedWorld([self.layout])
         # forward, recompute and reverse on the resident step when the mesh
         # (and the adjoint state) fits on chip; otherwise on the gather step --

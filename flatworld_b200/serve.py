@@ -62,8 +62,9 @@ class Arena:
 
     def insert(self, domains, dt=0.0, useAdapativeDT=False, damping=0.0) -> int:
         layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT)
-        if layout.rigids:
-            raise NotImplementedError("rigid bodies run in a single-scene ExplicitLoop only, not in served worlds")
+        if layout.entries:
+            raise NotImplementedError("rigid bodies and ground planes with BCs run in an ExplicitLoop or "
+                                      "BatchedLoop, not in served worlds")
         stage(self.native, PackedWorld([layout]))
         s = self.native.arena_commit()
         self.layouts[s] = layout
