@@ -70,6 +70,11 @@ def tune_batched(loop, blocks=(128, 256, 512), steps=16, use_cache=True):
 
     if getattr(loop, "path", "gather") == "stream":
         return {"path": "stream", "block_elems": 0, "block_nodes": 0, "candidates": []}
+    if getattr(loop, "_has_flex", False) or getattr(loop, "_has_rigid", False):
+        # candidates are timed from one snapshot, which holds neither the FEM-FEM
+        # contact state nor the rigid bodies: keep the default launch shape
+        return {"path": loop.path, "block_elems": 0, "block_nodes": 0, "candidates": [],
+                "skipped": "snapshots hold no FEM-FEM contact or rigid-body state"}
 
     key = f"batched|{_gpu_name(loop._native.device)}|N={loop.n_nodes}|E={loop.n_elems}|S={loop.S}"
     if use_cache:
