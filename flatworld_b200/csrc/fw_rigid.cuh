@@ -47,7 +47,9 @@ struct __align__(16) Rigid {
   int type, bc, in_contact;
   float rot[4];                // cached_rotation_matrix, row-major
   float lb[2], ub[2];          // the rigid's box (aabb[domain])
-  int scene, pad[3];           // the scene (loop) the rigid belongs to
+  int scene;                   // the scene (loop) the rigid belongs to
+  int rs;                      // that scene's index in the list of scenes with rigids
+  int pad[2];
 };
 static_assert(sizeof(Rigid) == 144, "Rigid record is 144 bytes");
 

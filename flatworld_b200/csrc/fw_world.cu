@@ -380,8 +380,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_nodes_rigid(Dev d) {
 // pairs in pair order, each pair's items in boundary-node order: lanes load
 // 128 records at a time, and every lane adds the hits in ascending lane order
 // through shuffles, so the sum is a serial run of the reference's atomic
-// adds); then one thread per scene with rigids counts the substep and, on the
-// substeps of that scene's schedule, runs its rigid update (fw_rigid.cuh).
+// adds).  Then each stepping scene's substep is counted and, on the substeps
+// of its schedule, its rigid update runs (fw_rigid.cuh): after a barrier, one
+// thread per scene, when all rigids fit in one block; otherwise by the warp
+// that finishes the scene's last rigid (a per-scene arrival count after a
+// fence).  The update reads only finished accumulators either way.
 struct RigidDev {
   Rigid* rig;
   int n;
@@ -394,20 +397,33 @@ struct RigidDev {
   int2* rp_rng;  // (first item, item count), pair order
   fw::RigidScene* rs;  // the scenes with rigids
   int n_rs;
+  int* done;           // per scene with rigids: warps finished this substep
   const fw::RigidClock* clock;  // per scene
   int* count;                   // per scene: the reference's rigid_update_times
   int* err;
 };
 
-constexpr int kRigidThreads = 1024;
+constexpr int kRigidThreads = 256;   // grid launch: 8 rigids per block
+constexpr int kRigidOneBlock = 1024;  // up to 32 rigids: one block, scenes updated after a barrier
 
-__global__ void __launch_bounds__(kRigidThreads) k_rigid(Dev d, RigidDev r) {
+// The counter and, when due, the rigid update of scene-with-rigids k.
+__device__ __forceinline__ void rigid_scene_update(const RigidDev& r, int k) {
+  const fw::RigidScene rs = r.rs[k];
+  const fw::RigidClock ck = r.clock[rs.scene];
+  const int cnt = r.count[rs.scene] + 1;
+  r.count[rs.scene] = cnt;
+  if (ck.every < 1 || cnt % ck.every != 0) return;
+  fw::rigid_update(r.rig + rs.r0, rs.rn, r.gbox + rs.g0, r.gkind + rs.g0, rs.gn, ck.dt, ck.damping, r.err);
+}
+
+__global__ void __launch_bounds__(kRigidOneBlock) k_rigid(Dev d, RigidDev r) {
   const unsigned full = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
   const float4 none = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-  for (int g = warp; g < r.n; g += n_warps) {
+  const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const bool live = g < r.n && d.scene_mode[r.rig[min(g, r.n - 1)].scene] == fw::MODE_STEP;
+  if (live) {
     Rigid& rg = r.rig[g];
-    if (d.scene_mode[rg.scene] != fw::MODE_STEP) continue;
     float ax = rg.acc[0], ay = rg.acc[1], aw = rg.accw;
     for (int q = r.rp_off[g]; q < r.rp_off[g + 1]; ++q) {
       const int2 rng = r.rp_rng[q];
@@ -437,16 +453,20 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid(Dev d, RigidDev r) {
       rg.accw = aw;
     }
   }
-  __syncthreads();
-  for (int k = threadIdx.x; k < r.n_rs; k += blockDim.x) {
-    const fw::RigidScene rs = r.rs[k];
-    if (d.scene_mode[rs.scene] != fw::MODE_STEP) continue;
-    const fw::RigidClock ck = r.clock[rs.scene];
-    const int cnt = r.count[rs.scene] + 1;
-    r.count[rs.scene] = cnt;
-    if (ck.every < 1 || cnt % ck.every != 0) continue;
-    fw::rigid_update(r.rig + rs.r0, rs.rn, r.gbox + rs.g0, r.gkind + rs.g0, rs.gn, ck.dt, ck.damping, r.err);
+  if (gridDim.x == 1) {  // every rigid in this block: a barrier, then one thread per scene
+    __syncthreads();
+    for (int k = threadIdx.x; k < r.n_rs; k += blockDim.x)
+      if (d.scene_mode[r.rs[k].scene] == fw::MODE_STEP) rigid_scene_update(r, k);
+    return;
   }
+  // grid: the warp that finishes a scene's last rigid runs that scene's update
+  if (!live || lane != 0) return;
+  __threadfence();
+  const int k = r.rig[g].rs;
+  if (atomicAdd(r.done + k, 1) + 1 != r.rs[k].rn) return;
+  __threadfence();
+  r.done[k] = 0;
+  rigid_scene_update(r, k);
 }
 
 // Rotation cache and boxes of the rigids at construction
@@ -1128,7 +1148,10 @@ int launch_step(fw_ctx* c) {
       k_nodes_rigid<true><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
     else
       k_nodes_rigid<false><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
-    k_rigid<<<1, 32 * std::min(32, std::max(1, c->rd.n)), 0, c->stream>>>(c->d, c->rd);
+    if (c->rd.n <= kRigidOneBlock / 32)
+      k_rigid<<<1, 32 * c->rd.n, 0, c->stream>>>(c->d, c->rd);
+    else
+      k_rigid<<<(c->rd.n + kRigidThreads / 32 - 1) / (kRigidThreads / 32), kRigidThreads, 0, c->stream>>>(c->d, c->rd);
     c->launches += 1;
   } else if (c->has_flex) {
     k_nodes_flex<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
@@ -2505,7 +2528,7 @@ int fw_finalize(fw_ctx* c) {
       if (!rs.empty() && sc <= rs.back().scene)
         return fail(c, FW_ERR_ARG, "rigids must be grouped by scene in ascending scene order");
       fw::RigidScene e{sc, a, 0, 0, 0, {0, 0, 0}};
-      while (a < nr && c->h_rigid[a].scene == sc) ++a, ++e.rn;
+      while (a < nr && c->h_rigid[a].scene == sc) c->h_rigid[a].rs = (int)rs.size(), ++a, ++e.rn;
       while (q < (int)c->h_gscene.size() && c->h_gscene[q] < sc) ++q;
       e.g0 = q;
       while (q < (int)c->h_gscene.size() && c->h_gscene[q] == sc) ++q, ++e.gn;
@@ -2523,9 +2546,11 @@ int fw_finalize(fw_ctx* c) {
         (rc = dalloc(c, &r.item, (size_t)n_ritems)) || (rc = upload(c, &r.gbox, c->h_gbox)) ||
         (rc = upload(c, &r.gkind, c->h_gkind)) || (rc = upload(c, &r.rp_off, rp_off)) ||
         (rc = upload(c, &r.rp_rng, rp_rng)) || (rc = upload(c, &r.rs, rs)) ||
-        (rc = upload(c, &c->d_rclock, ck)) || (rc = dalloc(c, &r.count, S)) || (rc = dalloc(c, &r.err, 1)))
+        (rc = upload(c, &c->d_rclock, ck)) || (rc = dalloc(c, &r.count, S)) || (rc = dalloc(c, &r.err, 1)) ||
+        (rc = dalloc(c, &r.done, rs.size())))
       return rc;
     FW_CUDA(c, cudaMemsetAsync(r.count, 0, sizeof(int) * S, c->stream));
+    FW_CUDA(c, cudaMemsetAsync(r.done, 0, sizeof(int) * rs.size(), c->stream));
     FW_CUDA(c, cudaMemsetAsync(r.err, 0, sizeof(int), c->stream));
     r.clock = c->d_rclock;
     d.rig = r.rig;

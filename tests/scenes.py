@@ -330,14 +330,15 @@ def rigid_free_ball(fw):
     return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), block, ball]
 
 
-def rigid_row(fw, nx=128, ny=32, n_rigid=12):
+def rigid_row(fw, nx=128, ny=32, n_rigid=12, ball_speed=0.05):
     """A NeoHookean slab (1.0 x 0.25, nx x ny quads) on the ground plane under
     gravity, with a row of n_rigid BC-driven primitives touching its top
     (0.5 mm deep at the start), 0.08 apart, cycled: balls rolling right at
-    0.05 m/s (EnforceVel, friction 0.2), fixed box indenters (FixedAll) and
-    capsules spinning in place at 1 rad/s (Fixed + EnforceRotVel, friction
-    0.1), which press deeper as they turn.  BC-driven rigids keep their
-    clearances, so the scene runs for as long as a benchmark needs."""
+    ball_speed m/s (EnforceVel, friction 0.2), fixed box indenters (FixedAll)
+    and capsules spinning in place at 1 rad/s (Fixed + EnforceRotVel,
+    friction 0.1), which press deeper as they turn.  BC-driven rigids keep
+    their clearances (a ball reaches the next box after about 0.035 /
+    ball_speed s), so the scene runs for as long as a benchmark needs."""
     conn, coords = fw.structured_rectangle(nx, ny, 1.0, 0.25, origin=(0.0, 0.0))
     slab = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.HyperElastic(E=1e5, nu=0.3, rho=500.0)),
                         [fw.Gravity([0.0, -9.8])])
@@ -345,7 +346,7 @@ def rigid_row(fw, nx=128, ny=32, n_rigid=12):
     for k in range(n_rigid):
         x = 0.06 + 0.08 * k
         if k % 3 == 0:
-            r = fw.RigidBodyDomain(fw.BallRigid(2, [x, 0.2745], 0.025, 0.5), [fw.EnforceVel([0], [0.05, 0.0])],
+            r = fw.RigidBodyDomain(fw.BallRigid(2, [x, 0.2745], 0.025, 0.5), [fw.EnforceVel([0], [ball_speed, 0.0])],
                                    friction=0.2)
         elif k % 3 == 1:
             r = fw.RigidBodyDomain(fw.BoxRigid(2, [x, 0.2745], [0.04, 0.05], [0.0], 1.0), [fw.FixedAll([0])])

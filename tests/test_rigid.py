@@ -201,13 +201,15 @@ def test_gpu_equals_oracle_bcs_damping():
 def test_gpu_batched_rigid_scenes_equal_alone():
     """Scenes with rigids batched with each other and with a plain scene (each
     scene its own rigid clock, counter and clearance check; per-scene dt and
-    damping): every scene's nodes and rigids equal the same scene in its own
-    loop, frame after frame."""
+    damping; 42 rigids, more than one block of the rigid kernel holds, so the
+    scene updates run from the last warp of each scene): every scene's nodes
+    and rigids equal the same scene in its own loop, frame after frame."""
     from flatworld_b200.batch import BatchedLoop
 
+    row = lambda f: scenes.rigid_row(f, 32, 8, ball_speed=0.01)  # noqa: E731  (12 rigids each)
     builds = [scenes.rigid_fixed_ball, scenes.plain_small_scene, scenes.rigid_free_ball, scenes.rigid_bcs,
-              scenes.rigid_shared]
-    damp = [0.0, 0.0, 0.0, 0.5, 0.0]
+              scenes.rigid_shared, row, row, row]
+    damp = [0.0, 0.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0]
     b = BatchedLoop([f(fw) for f in builds], useAdapativeDT=True, damping=damp)
     assert len(set(np.round(b.dt, 12))) > 1
     alone = [fw.ExplicitLoop(0.0, f(fw), useAdapativeDT=True, damping=c) for f, c in zip(builds, damp)]
