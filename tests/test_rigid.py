@@ -135,6 +135,19 @@ def test_layout_matches_oracle():
             OracleLoop._pack_rigid(d, f, iv)
             assert np.array_equal(params[k], f) and np.array_equal(ints[k, :3], iv), (build.__name__, k)
         assert grounds.shape == (1, 6) and grounds[0, 0] == 0.0
+    # every rigid BC kind, and a moving ground's analytical entries (plane + the
+    # entries a height field gets), packed as the oracle packs them
+    for doms in (scenes.rigid_bcs(fw), scenes.ground_circle(fw, [fw.EnforceVel([0], [0.1, -0.2])]),
+                 scenes.fixed_ground_heightfield(fw, True)):
+        lay = SceneLayout(doms, useAdapativeDT=True)
+        o = OracleLoop(doms, useAdapativeDT=True)
+        params, ints, _ = PackedWorld([lay]).rigid_records()
+        assert len(lay.entries) == len(o.entries) == len(params)
+        for k, d in enumerate(lay.entries):
+            f = np.zeros(20, np.float32)
+            iv = np.zeros(3, np.int32)
+            (OracleLoop._pack_rigid(d, f, iv) if d.type == fw.DomainType.RIGID else o._pack_analytical(d, f, iv))
+            assert np.array_equal(params[k], f) and np.array_equal(ints[k, :3], iv), k
     # FEM + one rigid, no ground: the loop skips the broad phase (plain box test)
     assert SceneLayout([scenes.rigid_fixed_ball(fw)[i] for i in (0, 1)], useAdapativeDT=True).skip_bvh
     assert not SceneLayout(scenes.rigid_fixed_ball(fw), useAdapativeDT=True).skip_bvh
