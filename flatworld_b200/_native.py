@@ -61,7 +61,7 @@ _SIGNATURES = {
     "fw_set_spring_bodies": (C.c_int, [_vp, C.c_int32, _i32p, _f32p]),
     "fw_read_flex_state": (C.c_int, [_vp, _i32p, C.c_int32, _f32p]),
     "fw_set_rigids": (C.c_int, [_vp, C.c_int32, _f32p, _i32p, C.c_int32, _f32p]),
-    "fw_add_rigid_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32]),
+    "fw_add_rigid_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32, C.c_int32]),
     "fw_set_rigid_clock": (C.c_int, [_vp, C.c_int32, C.c_float, C.c_float]),
     "fw_set_rigid_clocks": (C.c_int, [_vp, _i32p, _f32p, _f32p]),
     "fw_gate_by_rigid": (C.c_int, [_vp, C.c_int32]),
@@ -246,9 +246,9 @@ class NativeWorld:
         self._check(self._L.fw_set_rigids(self._h, len(i[0]) // 4, p[1], i[1], len(g[0]) // 6, g[1]),
                     "fw_set_rigids")
 
-    def add_rigid_pair(self, body, rigid, penalty, friction, skip_bvh):
+    def add_rigid_pair(self, body, rigid, penalty, friction, skip_bvh, tied=0):
         self._check(self._L.fw_add_rigid_pair(self._h, int(body), int(rigid), float(penalty), float(friction),
-                                              int(skip_bvh)), "fw_add_rigid_pair")
+                                              int(skip_bvh), int(tied)), "fw_add_rigid_pair")
 
     def set_rigid_clock(self, every: int, dt: float, damping: float):
         self._check(self._L.fw_set_rigid_clock(self._h, int(every), float(dt), float(damping)), "fw_set_rigid_clock")

@@ -49,7 +49,7 @@ struct __align__(16) Pair {
   // voxel: lb.x, lb.y, dx, dz.
   float f[4];
   int gate;  // 0: the static box above gates the pair; e + 1: the current box of rigid entry e
-  int pad;
+  int pad;   // rigid pairs: 1 when the pair is tied
 };
 static_assert(sizeof(Pair) == 64, "Pair record is 64 bytes");
 

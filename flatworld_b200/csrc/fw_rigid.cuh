@@ -216,9 +216,11 @@ __device__ __forceinline__ float rigid_detect(const Rigid& g, float px, float py
 
 // One FEM-rigid work item of one node: adds the contact force to f and
 // returns the reaction record (impulse x, y, torque, rigid index bits; rigid
-// -1 when the item does not touch).  mixedcontact.py:1054-1115.
-__device__ __forceinline__ float4 rigid_item(const Rigid& g, int rigid, float penalty, float mu, float2 x,
-                                             float2 v, float dt, float2& f) {
+// -1 when the item does not touch).  mixedcontact.py:1054-1115; a tied pair
+// (ExplicitLoop ties) pulls the node to the contact point with no offset and
+// no friction (1073-1087).
+__device__ __forceinline__ float4 rigid_item(const Rigid& g, int rigid, float penalty, float mu, bool tied,
+                                             float2 x, float2 v, float dt, float2& f) {
   const float4 none = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
   if (rmin(x.x - g.lb[0], x.y - g.lb[1]) < 0.0f || rmin(g.ub[0] - x.x, g.ub[1] - x.y) < 0.0f) return none;
   float nx, ny, cx, cy;
@@ -226,6 +228,15 @@ __device__ __forceinline__ float4 rigid_item(const Rigid& g, int rigid, float pe
   const float gx = g.ub[0] - g.lb[0], gy = g.ub[1] - g.lb[1];
   const float margin = sqrtf(gx * gx + gy * gy) * 0.5f;
   if (!(pen < margin)) return none;
+  if (tied) {
+    const float mx = cx - x.x, my = cy - x.y;
+    const float px = penalty * mx, py = penalty * my;
+    f.x += px;
+    f.y += py;
+    const float lx = cx - g.c[0], ly = cy - g.c[1];
+    const float fx = -px, fy = -py;
+    return make_float4(-px * dt, -py * dt, (lx * fy - ly * fx) * dt, __int_as_float(rigid));
+  }
   const float depth = pen - 1e-4f;
   if (!(depth < 0.0f)) return none;
   const float fnx = -nx * penalty * depth, fny = -ny * penalty * depth;

@@ -285,7 +285,8 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
         if (RIGID && d.pairs[p0 + k].kind == fw::PAIR_RIGID) {
           const Pair& pr = d.pairs[p0 + k];
           const float4 rec = d.pair_active[p0 + k]
-                                 ? fw::rigid_item(d.rig[pr.table], pr.table, pr.penalty, pr.f[0], x, v, dt, f)
+                                 ? fw::rigid_item(d.rig[pr.table], pr.table, pr.penalty, pr.f[0], pr.pad != 0, x,
+                                                  v, dt, f)
                                  : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
           d.ritem[pr.n0 + d.bslot[i]] = rec;
           continue;
@@ -2052,7 +2053,8 @@ int fw_set_rigids(fw_ctx* c, int32_t n, const float* params, const int32_t* ints
   return FW_OK;
 }
 
-int fw_add_rigid_pair(fw_ctx* c, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh) {
+int fw_add_rigid_pair(fw_ctx* c, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh,
+                      int32_t tied) {
   if (!c) return FW_ERR_ARG;
   if (!c->rigid_set) return fail(c, FW_ERR_STATE, "fw_add_rigid_pair before fw_set_rigids");
   if (rigid < 0 || rigid >= (int)c->h_rigid.size())
@@ -2063,6 +2065,7 @@ int fw_add_rigid_pair(fw_ctx* c, int32_t body, int32_t rigid, float penalty, flo
   p.penalty = penalty;
   p.table = rigid;
   p.n1 = skip_bvh ? 1 : 0;
+  p.pad = tied ? 1 : 0;  // a tied pair (rigid pairs only)
   p.f[0] = friction;
   const float zero[2] = {0.0f, 0.0f};
   return add_pair(c, p, zero, zero);

@@ -259,7 +259,7 @@ class ExplicitLoop:
         self._max_domains = len(domains) + 10
         self.rigidManager = None
         layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT,
-                             mass_scaling_dt=mass_scaling_dt)
+                             mass_scaling_dt=mass_scaling_dt, ties=self.ties)
         self._layout = layout
         self.stableTime = layout.stableTime
         self.useAdapative = layout.useAdapative
@@ -270,9 +270,6 @@ class ExplicitLoop:
         self.numContacts = len(layout.contacts)
         self._unbatched_contacts = layout.unbatched
         self._counter_py = 0
-        if (layout.flex or layout.rigids) and self.ties:
-            raise NotImplementedError("tied FEM-FEM / FEM-rigid pairs (ExplicitLoop ties=...) are not part of "
-                                      "flatworld_b200")
         self._packed = PackedWorld([layout])
         self._native = build_native(self._packed, device=device, path=path, patches=patches,
                                     front_warps=front_warps, res_sync=res_sync)

@@ -57,6 +57,7 @@ class ContactSpec:
     penalty: float
     stableTime: float
     friction: float = 0.0
+    tied: bool = False  # named in ExplicitLoop(ties=...) (explicitloop.py:265-270)
 
 
 def _contact_helper(di, dj, ctype, i, j):
@@ -106,7 +107,7 @@ def _contact_helper(di, dj, ctype, i, j):
 class SceneLayout:
     """Construction-time state of one scene (one reference ExplicitLoop)."""
 
-    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, mass_scaling_dt=0.0):
+    def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, mass_scaling_dt=0.0, ties=None):
         for d in domains:
             if d.type not in _SUPPORTED:
                 raise NotImplementedError(f"domain type {d.type} is outside flatworld_b200's scope")
@@ -156,6 +157,22 @@ class SceneLayout:
                     spec = _contact_helper(di, dj, ctype, i, j)
                     if spec is not None:
                         contacts.append(spec)
+        # ties (explicitloop.py:400-439): (domain, domain) index pairs, negative
+        # indices counted from the end; unresolvable entries are ignored
+        tie_pairs = set()
+        for t in (ties or []):
+            if not isinstance(t, (tuple, list)) or len(t) != 2:
+                continue
+            a, b = t
+            if not isinstance(a, (int, np.integer)) or not isinstance(b, (int, np.integer)):
+                continue
+            ia, ib = int(a) + (len(domains) if a < 0 else 0), int(b) + (len(domains) if b < 0 else 0)
+            if 0 <= ia < len(domains) and 0 <= ib < len(domains) and ia != ib:
+                tie_pairs.add((min(ia, ib), max(ia, ib)))
+        for c in contacts:
+            c.tied = (min(c.pair_ids), max(c.pair_ids)) in tie_pairs
+            if c.tied and c.kind == "flex":
+                raise NotImplementedError("tied FEM-FEM pairs (ExplicitLoop ties=...) are not part of flatworld_b200")
         self.contacts = contacts
         for c in contacts:  # explicitloop.py:313-315
             stable = min(stable, c.stableTime)
@@ -399,7 +416,8 @@ class PackedWorld:
                 body = self.body_of[(si, fem_index[id(c.fem)])]
                 if c.kind == "rigid":  # the gate box is the rigid's current one, on the device
                     rid = r_off[si] + next(k for k, d in enumerate(sc.rigids) if d is c.ground)
-                    out.append((c.kind, body, np.float32(c.penalty), rid, np.float32(c.friction), sc.skip_bvh))
+                    out.append((c.kind, body, np.float32(c.penalty), rid, np.float32(c.friction),
+                                (sc.skip_bvh, c.tied)))
                     continue
                 lo, hi = c.ground.getBBox()
                 out.append((c.kind, body, np.float32(c.penalty), np.asarray(lo, np.float32),
@@ -439,8 +457,8 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
     if any(sc.entries for sc in packed.scenes):
         nw.set_rigids(*packed.rigid_records())
     for (kind, body, pen, lo, hi, g), gate in zip(packed.pair_records(), packed.ground_gate_entries()):
-        if kind == "rigid":  # (rigid index, friction, skip_bvh) in the box slots
-            nw.add_rigid_pair(body, lo, pen, hi, 1 if g else 0)
+        if kind == "rigid":  # (rigid index, friction, (skip_bvh, tied)) in the box and ground slots
+            nw.add_rigid_pair(body, lo, pen, hi, 1 if g[0] else 0, 1 if g[1] else 0)
             continue
         if kind == "plane":  # the plane of construction time, also when it moves (mixedcontact.py:1815-1818)
             nw.add_plane(body, pen, lo, hi, g.point, g.normal)

@@ -207,11 +207,14 @@ int fw_set_rigids(fw_ctx* ctx, int32_t n, const float* params, const int32_t* in
 /* One FEM-rigid pair (ContactFlexRigid, femcontact.py:173-179): the body's
  * boundary nodes against the rigid, penalty 2K of the body, the rigid's
  * friction; skip_bvh: the loop activates the pair by plain box overlap
- * (mixedcontact.py:1697-1713, 474-492) instead of the broad phase.  Add in the
+ * (mixedcontact.py:1697-1713, 474-492) instead of the broad phase; tied: a
+ * pair named in ExplicitLoop(ties=...), which pulls each node to its contact
+ * point without the 1e-4 offset or friction.  Add in the
  * reference's launch order: plane pairs, rigid pairs (contact order), height
  * field, voxel.  Replaces _build_batched_contacts' rigid work lists and
  * _batched_rigid_prim_kernel, mixedcontact.py:1963-2130, 1026-1115. */
-int fw_add_rigid_pair(fw_ctx* ctx, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh);
+int fw_add_rigid_pair(fw_ctx* ctx, int32_t body, int32_t rigid, float penalty, float friction, int32_t skip_bvh,
+                      int32_t tied);
 /* The last ground pair added (plane, height field, voxel) is gated by the
  * current box of analytical entry `entry` (fw_set_rigids) instead of its
  * static box: in a loop where some ground plane has BCs, every ground's

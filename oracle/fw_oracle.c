@@ -1079,7 +1079,7 @@ typedef struct or_rigids {
   int* gkind; /* 0: plane, 1: box (height field, voxel grid) */
   /* work items, reference order: per rigid pair its FEM body's boundary nodes */
   int n_rp;
-  int *rp_body, *rp_rigid, *rp_skip;
+  int *rp_body, *rp_rigid, *rp_skip, *rp_tied;
   REAL *rp_pen, *rp_fric;
 } or_rigids;
 
@@ -1217,9 +1217,10 @@ static int rigid_pair_active(const or_world* w, int body, const or_rigid* g, int
   return alo[0] <= bhi[0] && ahi[0] >= blo[0] && alo[1] <= bhi[1] && ahi[1] >= blo[1];
 }
 
-/* _batched_rigid_prim_kernel (mixedcontact.py:1026-1115), untied branch, its
- * work items serially in order; the reaction impulse and torque of each hit
- * are added to the rigid's accumulators in that order. */
+/* _batched_rigid_prim_kernel (mixedcontact.py:1026-1115), its work items
+ * serially in order; the reaction impulse and torque of each hit are added to
+ * the rigid's accumulators in that order.  A tied pair pulls the node to the
+ * contact point with no offset and no friction (1073-1087). */
 static void rigid_contacts(or_world* w, REAL dt, long counter) {
   or_rigids* R = w->rig;
   if (!R) return;
@@ -1238,6 +1239,17 @@ static void rigid_contacts(or_world* w, REAL dt, long counter) {
       const REAL gx = g->ub[0] - g->lb[0], gy = g->ub[1] - g->lb[1];
       const REAL margin = R_SQRT(gx * gx + gy * gy) * (REAL)0.5;
       if (!(pen < margin)) continue;
+      if (R->rp_tied[pi]) {
+        const REAL tx = k * (cx - px), ty = k * (cy - py);
+        w->fext[2 * nid] += tx;
+        w->fext[2 * nid + 1] += ty;
+        g->acc[0] += -tx * dt;
+        g->acc[1] += -ty * dt;
+        const REAL lx = cx - g->c[0], ly = cy - g->c[1];
+        const REAL fx = -tx, fy = -ty;
+        g->accw += (lx * fy - ly * fx) * dt;
+        continue;
+      }
       const REAL depth = pen - (REAL)1e-4;
       if (!(depth < (REAL)0.0)) continue;
       const REAL fnx = -nx * k * depth, fny = -ny * k * depth;
@@ -1739,16 +1751,17 @@ int or_set_rigids(or_world* w, int n, const float* f, const int32_t* iv, int n_g
 
 /* One FEM-rigid pair (its work items: the body's boundary nodes), added in
  * the reference's rigid-contact order (mixedcontact.py:1987-2030). */
-int or_add_rigid_pair(or_world* w, int body, int rigid, float penalty, float friction, int skip_bvh) {
+int or_add_rigid_pair(or_world* w, int body, int rigid, float penalty, float friction, int skip_bvh, int tied) {
   or_rigids* R = w->rig;
   if (!R || rigid < 0 || rigid >= R->n || body < 0 || body >= w->n_bodies) return -1;
   const int k = R->n_rp++;
   R->rp_body = (int*)realloc(R->rp_body, sizeof(int) * R->n_rp);
   R->rp_rigid = (int*)realloc(R->rp_rigid, sizeof(int) * R->n_rp);
   R->rp_skip = (int*)realloc(R->rp_skip, sizeof(int) * R->n_rp);
+  R->rp_tied = (int*)realloc(R->rp_tied, sizeof(int) * R->n_rp);
   R->rp_pen = (REAL*)realloc(R->rp_pen, sizeof(REAL) * R->n_rp);
   R->rp_fric = (REAL*)realloc(R->rp_fric, sizeof(REAL) * R->n_rp);
-  R->rp_body[k] = body; R->rp_rigid[k] = rigid; R->rp_skip[k] = skip_bvh;
+  R->rp_body[k] = body; R->rp_rigid[k] = rigid; R->rp_skip[k] = skip_bvh; R->rp_tied[k] = tied;
   R->rp_pen[k] = penalty; R->rp_fric[k] = friction;
   return 0;
 }
@@ -1784,7 +1797,7 @@ void or_destroy(or_world* w) {
   free(w->csr_off); free(w->csr_slot); free(w->corner);
   if (w->rig) {
     or_rigids* R = w->rig;
-    free(R->r); free(R->gbox); free(R->gkind); free(R->rp_body); free(R->rp_rigid); free(R->rp_skip); free(R->rp_pen);
+    free(R->r); free(R->gbox); free(R->gkind); free(R->rp_body); free(R->rp_rigid); free(R->rp_skip); free(R->rp_tied); free(R->rp_pen);
     free(R->rp_fric);
     free(R);
   }

@@ -91,7 +91,7 @@ def _lib(precision: str):
         L.or_log32.argtypes = [C.c_float]
         L.or_log32.restype = C.c_float
         L.or_set_rigids.argtypes = [C.c_void_p, C.c_int, _f32p, _i32p, C.c_int, _f32p]
-        L.or_add_rigid_pair.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int]
+        L.or_add_rigid_pair.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int]
         L.or_rigid_update.argtypes = [C.c_void_p, C.c_float, C.c_float]
         L.or_get_rigids.argtypes = [C.c_void_p, _f64p]
         L.or_get_rigids.restype = C.c_int
@@ -183,7 +183,7 @@ class OracleLoop:
     """CPU restatement of one reference ExplicitLoop over FEM + ground domains."""
 
     def __init__(self, domains, dt=0.0, damping=0.0, useAdapativeDT=True, precision="f32", threads=1,
-                 mass_scaling_dt=0.0):
+                 mass_scaling_dt=0.0, ties=None):
         self.precision = precision
         L = self._L = _lib(precision)
         self.domains = list(domains)
@@ -395,10 +395,19 @@ class OracleLoop:
             rp, ri = _fp(prm), _ip(ivs)
             self._keep += [rp, ri, gbox]
             L.or_set_rigids(self._w, len(entries), rp[1], ri[1], len(gb), gbox[1])
+            # _parse_tie_entry / _is_tie_pair (explicitloop.py:400-439)
+            tie_set = set()
+            for t in (ties or []):
+                if isinstance(t, (tuple, list)) and len(t) == 2 and all(isinstance(v, (int, np.integer)) for v in t):
+                    a, b = (int(v) + (len(domains) if v < 0 else 0) for v in t)
+                    if 0 <= a < len(domains) and 0 <= b < len(domains) and a != b:
+                        tie_set.add((min(a, b), max(a, b)))
+            dom_index = lambda d: next(k for k, e in enumerate(domains) if e is d)  # noqa: E731
             for ct, femd, rig, pen, _ in contacts:
                 if ct == FLEXRIGID:
+                    ij = tuple(sorted((dom_index(femd), dom_index(rig))))
                     L.or_add_rigid_pair(self._w, fem.index(femd), rigid_doms.index(rig), float(np.float32(pen)),
-                                        float(np.float32(rig.friction)), skip_bvh)
+                                        float(np.float32(rig.friction)), skip_bvh, 1 if ij in tie_set else 0)
         if flex:
             # boundary edges per fem domain, global node ids, mesh order
             edges, be_off, be_cnt = [], [], []

@@ -323,3 +323,35 @@ def test_gpu_moving_ground_equals_oracle(name, frames):
         assert np.array_equal(lp._entry_state().astype(np.float64), o.entry_state()[0]), (name, f)
     g = lp.domains[0]
     assert np.array_equal(g.getCurrentRefPoint(), lp._entry_state()[0, :2])
+
+
+# ---- tied FEM-rigid pairs (ExplicitLoop ties=...)
+
+def test_oracle_tied_pair():
+    """A tied pair (explicitloop.py:265-270) takes the tied branch of the
+    rigid kernel: the node is pulled to its contact point with no 1e-4 offset
+    and no friction (mixedcontact.py:1073-1087).  The circle still rests on
+    the ball, on a trajectory of its own; negative indices name domains from
+    the end, and the host marks the same pair."""
+    free = OracleLoop(scenes.rigid_fixed_ball(fw), useAdapativeDT=True)
+    tied = OracleLoop(scenes.rigid_fixed_ball(fw), useAdapativeDT=True, ties=[(0, -2)])
+    for _ in range(40):
+        free.advance_with_time(FRAME)
+        tied.advance_with_time(FRAME)
+    xf, xt = free.state()[0], tied.state()[0]
+    assert not np.array_equal(xf, xt) and xt[:, 1].mean() > 0.45
+    lay = SceneLayout(scenes.rigid_fixed_ball(fw), useAdapativeDT=True, ties=[(0, -2)])
+    assert [c.tied for c in lay.pairs if c.kind == "rigid"] == [True]
+    assert [c.tied for c in SceneLayout(scenes.rigid_fixed_ball(fw), ties=[(0, 2)]).pairs if c.kind == "rigid"] == [False]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,ties,frames", [("fixed-ball", [(0, 1)], 30), ("pusher", [(1, 2), (1, 3)], 14)])
+def test_gpu_tied_equals_oracle(name, ties, frames):
+    build = {"fixed-ball": scenes.rigid_fixed_ball, "pusher": scenes.rigid_pusher}[name]
+    lp = fw.ExplicitLoop(0.0, build(fw), useAdapativeDT=True, ties=ties)
+    o = oracle.OracleLoop(build(fw), useAdapativeDT=True, ties=ties)
+    for f in range(frames):
+        lp.advanceWithTime(FRAME)
+        o.advance_with_time(FRAME)
+        _compare(lp, o, o.N, (name, f))
