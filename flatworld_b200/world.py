@@ -64,8 +64,12 @@ def _contact_helper(di, dj, ctype, i, j):
     """contactHelper (femcontact.py:283-303) restricted to the FEM-ground,
     FEM-FEM, FEM-rigid and spring-mass pairs."""
     if ctype == ContactType.RIGIDSPRING:
-        raise NotImplementedError("spring-mass domains against rigid bodies (ContactSpringRigid) are outside "
-                                  "flatworld_b200; set considerContact=False on one of them")
+        # ContactSpringRigid (femcontact.py:243-253): penalty 100 k, stable time
+        # 0.5 sqrt(m / penalty); every spring node is a work item of the rigid
+        # kernel (mixedcontact.py:2006-2018), friction the rigid's
+        spring, rig = (di, dj) if di.type == DomainType.SPRINGMASS else (dj, di)
+        pen = spring.spring * _SPRING_PENALTY_SCALE
+        return ContactSpec("rigid", spring, rig, (i, j), pen, 0.5 * (spring.mass / pen) ** 0.5, float(rig.friction))
     if ctype == ContactType.FLEXRIGID:
         # ContactFlexRigid (femcontact.py:173-179): the FEM side's penalty and
         # stable time; friction = the rigid's (mixedcontact.py:1992)

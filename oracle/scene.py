@@ -228,6 +228,11 @@ class OracleLoop:
                         pen = min(spr.spring, self._seg_penalty(fd)) * 100.0
                         contacts.append((FLEXSPRING, spr, fd, pen, self._contact_stable(pen, fd, fem)))
                         continue
+                    if ct == 0b1100:  # ContactSpringRigid (femcontact.py:243-253): every spring node an item
+                        spr, rig = (di, dj) if di.type == SPRINGMASS else (dj, di)
+                        pen = spr.spring * 100.0
+                        contacts.append((FLEXRIGID, spr, rig, pen, 0.5 * (spr.mass / pen) ** 0.5))
+                        continue
                     if ct == FLEXRIGID:  # ContactFlexRigid: domain1 = the FEM side
                         femd, rig = (di, dj) if di.type == FEM else (dj, di)
                         pen = self._seg_penalty(femd) * 1.0

@@ -413,3 +413,27 @@ def fixed_ground_heightfield(fw, fixed=True):
     fem = fw.FemDomain(mesh, fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)), [fw.Gravity([0, -10.0])])
     ground = fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0], [fw.Fixed([0])] if fixed else [])
     return [ground, hf, fem]
+
+
+def rigid_spring_net(fw):
+    """A spring net (6 x 6 cells of the reference's spring-grid pattern)
+    dropped onto a fixed box, next to an FEM block that a free ball lands on:
+    spring-rigid pairs (every spring node an item, penalty 100 k) beside
+    FEM-rigid ones.  No ground, so the broad phase is skipped."""
+    n, dx = 6, 0.03
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    coords = (np.stack([dx * ii, dx * jj], axis=-1).reshape(-1, 2) + np.float32([0.1, 0.42])).astype(np.float32)
+    conn = []
+    for i in range(n):
+        for j in range(n):
+            a, b, c = i * (n + 1) + j, i * (n + 1) + j + 1, (i + 1) * (n + 1) + j
+            conn += [[a, b], [b, c], [c, a]]
+    net = fw.SpringMassDomain(2, coords, np.asarray(conn, np.int32), [400.0, 0.5, 0.01], [fw.Gravity([0.0, -9.8])])
+    conn2, coords2 = fw.structured_rectangle(8, 4, 0.2, 0.1, origin=(0.5, 0.3))
+    block = fw.FemDomain(fw.Mesh(2, conn2, coords2), fw.SolidProp(fw.Elastic(E=3e4, nu=0.3, rho=100.0)),
+                         [fw.Fixed(list(range(9)))])
+    box = fw.RigidBodyDomain(fw.BoxRigid(2, [0.19, 0.36], [0.3, 0.1], [0.0], 5.0), [fw.FixedAll([0])],
+                             friction=0.2)
+    ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.6, 0.44], 0.04, 1.0), [fw.Gravity([0.0, -9.8])])
+    return [block, net, box, ball]
+

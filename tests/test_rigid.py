@@ -158,11 +158,6 @@ def test_out_of_scope_refused():
         fw.MeshRigid(2, None, 0.0, 1.0)
     with pytest.raises(NotImplementedError):
         fw.RevoluteJoint()
-    net = fw.SpringMassDomain(2, np.array([[0.0, 0.5], [0.1, 0.5]], np.float32), np.array([[0, 1]], np.int32),
-                              [10.0, 1.0, 1.0], [])
-    ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.5, 0.3], 0.1, 1.0))
-    with pytest.raises(NotImplementedError):
-        SceneLayout([net, ball])
     with pytest.raises(NotImplementedError):
         fw.ExplicitLoop(0.0, scenes.rigid_fixed_ball(fw), considerRigidRigidContact=False)
     from flatworld_b200.diff import DiffSim
@@ -355,3 +350,32 @@ def test_gpu_tied_equals_oracle(name, ties, frames):
         lp.advanceWithTime(FRAME)
         o.advance_with_time(FRAME)
         _compare(lp, o, o.N, (name, f))
+
+
+def test_oracle_spring_net_rests_on_box():
+    """Spring-rigid pairs (femcontact.py:243-253): penalty 100 k, stable time
+    0.5 sqrt(m / penalty), every spring node a work item; the net lands on the
+    fixed box and stays above it, while the ball lands on the FEM block."""
+    doms = scenes.rigid_spring_net(fw)
+    lay = SceneLayout(doms, useAdapativeDT=True)
+    o = OracleLoop(scenes.rigid_spring_net(fw), useAdapativeDT=True)
+    assert lay.stableTime == o.stableTime
+    assert [c.kind for c in lay.pairs] == ["rigid"] * 4  # block and net, each against box and ball
+    for _ in range(30):
+        o.advance_with_time(FRAME)
+    x, _, _ = o.state()
+    n_block = doms[0].nnodes
+    assert x[n_block:, 1].min() > 0.41 - 0.01  # the box top is at 0.41
+    st, err = o.rigid_state()
+    assert err == 0 and abs(st[1, 1] - (0.4 + 0.04)) < 0.01  # the ball on the block top
+
+
+@pytest.mark.gpu
+def test_gpu_spring_rigid_equals_oracle():
+    lp = fw.ExplicitLoop(0.0, scenes.rigid_spring_net(fw), useAdapativeDT=True)
+    o = oracle.OracleLoop(scenes.rigid_spring_net(fw), useAdapativeDT=True)
+    for f in range(24):
+        lp.advanceWithTime(FRAME)
+        o.advance_with_time(FRAME)
+        _compare(lp, o, o.N, f)
+
