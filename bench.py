@@ -536,8 +536,11 @@ def run_adjoint(args, rank, world, local):
     l0 = sim.native.launch_count()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     walls = []
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     with ClockSampler(local) as clk:
         for a, b, c in ev:
+            with torch.cuda.stream(stream):
+                flush.zero_()  # between timed iterations, on the stream the rollout runs on
             w0 = time.perf_counter()
             a.record(stream)
             x = sim.forward(sim.E0, v0)
@@ -578,7 +581,7 @@ def run_adjoint(args, rank, world, local):
         "config": {"workload": "differentiable 64x64-quad NeoHookean block, 2000 substeps dt 1e-4, K=50",
                    "elements": sim.E, "nodes": sim.N, "substeps": steps, "checkpoint_every": K,
                    "min_height_m": low, "contact": bool(low < 0.0),
-                   "l2": "working set (8192 triangles) fits in L2; latency-bound rollout"},
+                   "l2": "flushed between rollouts (256 MiB write)"},
         "adjoint": {"forward_ms": float(np.median(fwd_ms)), "backward_ms": float(np.median(bwd_ms)),
                     "forward_element_steps_per_s": sim.E * steps / (np.median(fwd_ms) / 1e3),
                     "backward_over_forward": float(np.median(bwd_ms) / np.median(fwd_ms)),
@@ -633,6 +636,7 @@ def run_flex(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     dist = dist_init(world, local)
     side = args.flex_side
     build = lambda: scenes.flex_pile(fw, side, side, gap=0.0)  # noqa: E731  (touching: contact from the start)
@@ -655,6 +659,7 @@ def run_flex(args, rank, world, local):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         with ClockSampler(local) as clk:
             for s_, e_ in ev:
+                flush.zero_()
                 s_.record(stream)
                 loop.advance_n(per)
                 e_.record(stream)
@@ -671,6 +676,7 @@ def run_flex(args, rank, world, local):
         loop._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
         ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for s_, e_ in ev2:
+            flush.zero_()
             s_.record(stream)
             loop._native.write_nodes_ptr(0, 0, N, xh.data_ptr())
             loop._native.write_nodes_ptr(1, 0, N, vh.data_ptr())
@@ -697,7 +703,7 @@ def run_flex(args, rank, world, local):
         "config": {"workload": f"pile of {side * side} touching disks with FEM-FEM contact on a plane, dt 0.5 x adaptive",
                    "elements": E, "nodes": N, "bodies": side * side, "flex_pairs": side * side * (side * side - 1) // 2,
                    "flex_work_items": n_items, "items_with_contact_at_end": in_contact, "dt": dt,
-                   "step": "100 substeps", "l2": "working set smaller than L2 (small meshes)",
+                   "step": "100 substeps", "l2": "flushed between steps (256 MiB write)",
                    "host_build_s": build_s, "state_finite": finite, "replicas": world, "path": "gather"},
         "latency_ms_per_step": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99)},
         "roofline": {"bound": "hbm", "kernel": "substep = k_flex_pre + k_flex_contact + k_elements + k_nodes_flex",
@@ -742,6 +748,7 @@ def run_rigid(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     dist = dist_init(world, local)
     nx = args.rigid_mesh
     build = lambda: scenes.rigid_row(fw, nx, max(4, nx // 4))  # noqa: E731
@@ -765,6 +772,7 @@ def run_rigid(args, rank, world, local):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         with ClockSampler(local) as clk:
             for s_, e_ in ev:
+                flush.zero_()
                 s_.record(stream)
                 loop.advance_n(per)
                 e_.record(stream)
@@ -777,6 +785,7 @@ def run_rigid(args, rank, world, local):
         loop._native.read_nodes_ptr(1, 0, N, vh.data_ptr())
         ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for s_, e_ in ev2:
+            flush.zero_()
             s_.record(stream)
             loop._native.write_nodes_ptr(0, 0, N, xh.data_ptr())
             loop._native.write_nodes_ptr(1, 0, N, vh.data_ptr())
@@ -805,7 +814,7 @@ def run_rigid(args, rank, world, local):
                                f"ball / box / capsule rigids pressing into it",
                    "elements": E, "nodes": N, "rigids": n_rigid, "rigid_work_items": n_items, "dt": dt,
                    "rigid_update_every": int(max(1, 1e-3 // dt)), "step": "100 substeps",
-                   "l2": "working set smaller than L2", "host_build_s": build_s, "state_finite": finite,
+                   "l2": "flushed between steps (256 MiB write)", "host_build_s": build_s, "state_finite": finite,
                    "rigid_x_range_at_end": [float(rig[:, 0].min()), float(rig[:, 0].max())],
                    "replicas": world, "path": "gather"},
         "latency_ms_per_step": {"p50": percentile_ms(lat, 50), "p99": percentile_ms(lat, 99)},
@@ -853,6 +862,7 @@ def run_rigid_batched(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     dist = dist_init(world, local)
     build = lambda: scenes.rigid_row(fw, 32, 8, ball_speed=0.01)  # noqa: E731  (clearances last the whole run)
     dt = SceneLayout(build(), useAdapativeDT=True).dt
@@ -873,6 +883,7 @@ def run_rigid_batched(args, rank, world, local):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         with ClockSampler(local) as clk:
             for s_, e_ in ev:
+                flush.zero_()
                 s_.record(stream)
                 b.advance(per)
                 e_.record(stream)
@@ -900,7 +911,7 @@ def run_rigid_batched(args, rank, world, local):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (slabs and rows of rigid primitives)",
         "config": {"workload": f"{K} slabs of 32 x 8 quads with 12 BC-driven rigids each, FEM-rigid contact",
-                   "elements": E, "scenes": K, "rigids": 12 * K, "dt": dt, "step": "100 substeps",
+                   "elements": E, "scenes": K, "rigids": 12 * K, "dt": dt, "step": "100 substeps", "l2": "flushed between steps (256 MiB write)",
                    "host_build_s": build_s, "path": "gather",
                    "state_finite": bool(np.isfinite(b.all_coords()).all())},
         "batched_vs_plain": {"plain_value": plain_value, "ratio": value / plain_value,
@@ -927,6 +938,7 @@ def run_flex_batched(args, rank, world, local):
     from tests import scenes
 
     torch.cuda.set_device(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
     dist = dist_init(world, local)
     build = lambda: scenes.flex_pile(fw, 3, 3, gap=0.0)  # noqa: E731
     dt = 0.5 * SceneLayout(build(), useAdapativeDT=True).dt
@@ -947,6 +959,7 @@ def run_flex_batched(args, rank, world, local):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         with ClockSampler(local) as clk:
             for s_, e_ in ev:
+                flush.zero_()
                 s_.record(stream)
                 b.advance(per)
                 e_.record(stream)
@@ -973,7 +986,7 @@ def run_flex_batched(args, rank, world, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded piles of disks)",
         "config": {"workload": f"{K} piles of 3 x 3 touching disks, FEM-FEM contact, dt 0.5 x adaptive",
-                   "elements": E, "scenes": K, "step": "100 substeps", "host_build_s": build_s, "path": "gather",
+                   "elements": E, "scenes": K, "step": "100 substeps", "l2": "flushed between steps (256 MiB write)", "host_build_s": build_s, "path": "gather",
                    "state_finite": bool(np.isfinite(b.all_coords()).all())},
         "batched_vs_plain": {"plain_value": plain_value, "ratio": value / plain_value,
                              "plain": "the same pile alone in an ExplicitLoop"},
