@@ -612,9 +612,10 @@ def run_adjoint(args, rank, world, local):
                                           f"takes 2 x {n_params} of them"}
         line["fd_check"] = {
             "directions": args.fd_directions, "eps": 1e-4,
-            "max_rel_err_dE": max(e[0] for e in errs["E"]), "max_rel_err_dv0": max(e[0] for e in errs["v"]),
-            "max_rel_err_dE_fp64_seed": max(e[1] for e in errs["E"]),
-            "max_rel_err_dv0_fp64_seed": max(e[1] for e in errs["v"]),
+            "max_rel_err_dE": max((e[0] for e in errs["E"]), default=None),
+            "max_rel_err_dv0": max((e[0] for e in errs["v"]), default=None),
+            "max_rel_err_dE_fp64_seed": max((e[1] for e in errs["E"]), default=None),
+            "max_rel_err_dv0_fp64_seed": max((e[1] for e in errs["v"]), default=None),
             "median_rel_err": float(np.median([e[0] for k in errs for e in errs[k]]))}
     if rank == 0:
         print(json.dumps(line), flush=True)
