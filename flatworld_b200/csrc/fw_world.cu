@@ -276,6 +276,7 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
     if (bnd && mode == fw::MODE_STEP) {
       const int p0 = d.body_pair_off[b], pn = d.body_pair_cnt[b];
       const int fs = FLEX ? d.flex_slot[i] : -1;
+      const int bs = RIGID ? d.bslot[i] : 0;  // this node's slot in its body's boundary list
       bool flex_done = !FLEX || fs < 0;
       for (int k = 0; k < pn; ++k) {
         if (FLEX && !flex_done && d.pairs[p0 + k].kind != fw::PAIR_PLANE) {
@@ -284,11 +285,12 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
         }
         if (RIGID && d.pairs[p0 + k].kind == fw::PAIR_RIGID) {
           const Pair& pr = d.pairs[p0 + k];
+          const int slot = pr.n0 + bs;
           const float4 rec = d.pair_active[p0 + k]
                                  ? fw::rigid_item(d.rig[pr.table], pr.table, pr.penalty, pr.f[0], pr.pad != 0, x,
                                                   v, dt, f)
                                  : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-          d.ritem[pr.n0 + d.bslot[i]] = rec;
+          d.ritem[slot] = rec;
           continue;
         }
         if (!d.pair_active[p0 + k]) continue;
