@@ -437,3 +437,39 @@ def rigid_spring_net(fw):
     ball = fw.RigidBodyDomain(fw.BallRigid(2, [0.6, 0.44], 0.04, 1.0), [fw.Gravity([0.0, -9.8])])
     return [block, net, box, ball]
 
+
+
+def plain_small_low_scene(fw, seed=0):
+    """The plain small body (64 x 16 jittered quads, Elastic, gravity (0, -1))
+    placed 5 mm above the ground plane y = 0 and moving down at 0.5 m/s, so
+    that plane contact starts within the first 100 substeps of 1e-4."""
+    conn, coords = fw.structured_rectangle(64, 16, 1.0, 0.25, origin=(0.0, 0.005), jitter=0.1, seed=seed)
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0)),
+                       [fw.Gravity([0.0, -1.0])], initials=[fw.InitialVel("ALL", [0.0, -0.5])])
+    ground = fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0])
+    return [ground, fem]
+
+
+def j2_block_scene(fw):
+    """A J2 (MisesPlastic) block, 24 x 12 jittered quads, thrown at the ground
+    plane at (0.3, -2) m/s under gravity 9.8; it yields on impact."""
+    conn, coords = fw.structured_rectangle(24, 12, 0.4, 0.2, origin=(0.1, 0.05), jitter=0.1, seed=3)
+    mat = fw.MisesPlastic(E=1e5, nu=0.3, rho=100.0, sigma_y=2e3, H=1e3)
+    fem = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(mat), [fw.Gravity([0.0, -9.8])],
+                       initials=[fw.InitialVel("ALL", [0.3, -2.0])])
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), fem]
+
+
+def bcs_scene(fw):
+    """test2D/test_2Dfem_bcs.py: two-triangle squares under Force + Fixed,
+    EnforceVel + Fixed, EnforceAcc + Fixed, and an initial velocity."""
+    conn = np.array([[0, 1, 3], [0, 3, 2]], dtype=np.int32)
+    c = np.array([[0.5, 0.5], [0.7, 0.5], [0.5, 0.7], [0.7, 0.7]], dtype=np.float32)
+    prop = fw.SolidProp(fw.Elastic(E=2e4, nu=0.2, rho=40.0))
+    d0 = fw.FemDomain(fw.Mesh(2, conn, c), prop, [fw.Force([0, 1], [0, -100.0]), fw.Fixed([2, 3])], False)
+    d1 = fw.FemDomain(fw.Mesh(2, conn, c + 0.25), prop, [fw.EnforceVel([0, 1], [0, -1.0]), fw.Fixed([2, 3])],
+                      False)
+    d2 = fw.FemDomain(fw.Mesh(2, conn, c - 0.25), prop, [fw.EnforceAcc([0, 1], [0, -10.0]), fw.Fixed([2, 3])],
+                      False)
+    d3 = fw.FemDomain(fw.Mesh(2, conn, c + 0.5), prop, [], False, initials=[fw.InitialVel([0, 1], [0, -1.0])])
+    return [d0, d1, d2, d3]
