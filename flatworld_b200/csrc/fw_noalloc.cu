@@ -38,7 +38,7 @@ constexpr int kMaxDevices = 64;
 std::mutex g_na_mutex;
 float2* g_na_addr[kMaxDevices] = {nullptr};
 
-__global__ void k_na_elements(int E, const float2* __restrict__ x, const int32_t* __restrict__ conn,
+__global__ void k_na_elements(int N, int E, const float2* __restrict__ x, const int32_t* __restrict__ conn,
                               const float4* __restrict__ jinv, const float4* __restrict__ emat,
                               float4* __restrict__ j2_state, const float2* __restrict__ j2_param,
                               float2* __restrict__ corners) {
@@ -49,20 +49,30 @@ __global__ void k_na_elements(int E, const float2* __restrict__ x, const int32_t
   m.area = mm.x;
   m.lam = mm.y;
   m.mu = mm.z;
-  m.word = (int)mm.w & 3;
-  const float2 a = x[conn[3 * e]], b = x[conn[3 * e + 1]], c = x[conn[3 * e + 2]];
-  float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
-  float sy = 0.f, H = 0.f;
-  // J2 state is read and stored only when the caller passed the arrays
-  const bool mises = fw::elem_type(m.word) == fw::MAT_MISES && j2_state != nullptr && j2_param != nullptr;
-  if (mises) {
-    j2 = j2_state[e];
-    sy = j2_param[e].x;
-    H = j2_param[e].y;
+  const int type = (int)mm.w;
+  m.word = type & 3;
+  const int n0 = conn[3 * e], n1 = conn[3 * e + 1], n2 = conn[3 * e + 2];
+  // Only triangles (types 1-3) with node ids inside [0, N) are evaluated; any
+  // other record (a spring, type 0, has no third node) adds no force and
+  // reads nothing out of bounds.
+  const bool valid = type >= 1 && type <= 3 && (unsigned)n0 < (unsigned)N && (unsigned)n1 < (unsigned)N &&
+                     (unsigned)n2 < (unsigned)N;
+  float2 f1 = make_float2(0.f, 0.f), f2 = f1, f3 = f1;
+  if (valid) {
+    const float2 a = x[n0], b = x[n1], c = x[n2];
+    float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
+    // J2 triangles without state arrays never yield: an infinite yield stress
+    // keeps the radial return off, so they respond with the elastic trial stress.
+    float sy = __int_as_float(0x7f800000), H = 0.f;
+    const bool mises = fw::elem_type(m.word) == fw::MAT_MISES && j2_state != nullptr;
+    if (mises) {
+      j2 = j2_state[e];
+      sy = j2_param[e].x;
+      H = j2_param[e].y;
+    }
+    fw::element_forces(a, b, c, jinv[e], m, sy, H, j2, f1, f2, f3);
+    if (mises) j2_state[e] = j2;
   }
-  float2 f1, f2, f3;
-  fw::element_forces(a, b, c, jinv[e], m, sy, H, j2, f1, f2, f3);
-  if (mises) j2_state[e] = j2;
   corners[3 * e] = f1;
   corners[3 * e + 1] = f2;
   corners[3 * e + 2] = f3;
@@ -110,9 +120,25 @@ extern "C" int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps
     return na_error(err, err_len, FW_ERR_ARG, "fw_step_noalloc: need n_nodes > 0, n_elems > 0, n_steps >= 0");
   if (!x || !v || !node_bc || !bc_values || !mass || !conn || !jinv || !elem_mat || !csr_off || !csr_slot)
     return na_error(err, err_len, FW_ERR_ARG, "fw_step_noalloc: a required device pointer is NULL");
+  if ((j2_state == nullptr) != (j2_param == nullptr))
+    return na_error(err, err_len, FW_ERR_ARG,
+                    "fw_step_noalloc: j2_state and j2_param must both be given or both be NULL");
+  {
+    // An error left by earlier work of the caller is reported as such, not as
+    // a failure of this call's launches (and is left in place for the caller).
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+      char msg[200];
+      snprintf(msg, sizeof(msg), "fw_step_noalloc: a CUDA error was pending before the call: %s",
+               cudaGetErrorString(pending));
+      return na_error(err, err_len, FW_ERR_CUDA, msg);
+    }
+  }
   // Set-up, once per device: the device address of the scratch array.  In host
   // code the array's name is a host-side stand-in, not a device address, so it
   // must be resolved with cudaGetSymbolAddress while that device is current.
+  // The address is cached for the life of the process: after cudaDeviceReset
+  // the module may be loaded elsewhere, so calls after a reset are unsupported.
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return na_error(err, err_len, FW_ERR_CUDA, "fw_step_noalloc: no current CUDA device");
@@ -134,7 +160,7 @@ extern "C" int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps
   cudaStream_t s = (cudaStream_t)stream;
   const int ge = (n_elems + kNaBlock - 1) / kNaBlock, gn = (n_nodes + kNaBlock - 1) / kNaBlock;
   for (int k = 0; k < n_steps; ++k) {
-    k_na_elements<<<ge, kNaBlock, 0, s>>>(n_elems, reinterpret_cast<const float2*>(x), conn,
+    k_na_elements<<<ge, kNaBlock, 0, s>>>(n_nodes, n_elems, reinterpret_cast<const float2*>(x), conn,
                                           reinterpret_cast<const float4*>(jinv),
                                           reinterpret_cast<const float4*>(elem_mat),
                                           reinterpret_cast<float4*>(j2_state),
@@ -142,12 +168,14 @@ extern "C" int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps
     k_na_nodes<<<gn, kNaBlock, 0, s>>>(n_nodes, reinterpret_cast<float2*>(x), reinterpret_cast<float2*>(v),
                                        node_bc, reinterpret_cast<const float2*>(bc_values), mass, csr_off,
                                        csr_slot, corners, dt, damping);
-  }
-  const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    char msg[200];
-    snprintf(msg, sizeof(msg), "fw_step_noalloc: launch failed: %s", cudaGetErrorString(e));
-    return na_error(err, err_len, FW_ERR_CUDA, msg);
+    if (k == 0 || k == n_steps - 1) {  // launch errors: after the first pair, and at the end
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        char msg[200];
+        snprintf(msg, sizeof(msg), "fw_step_noalloc: launch failed: %s", cudaGetErrorString(e));
+        return na_error(err, err_len, FW_ERR_CUDA, msg);
+      }
+    }
   }
   return FW_OK;
 }

@@ -383,18 +383,27 @@ int64_t fw_launch_count(const fw_ctx* ctx);
  *   x, v        [2*n_nodes]  positions / velocities, updated in place
  *   node_bc     [n_nodes]    OR of FW_BC_*;  bc_values [2*n_nodes];  mass [n_nodes]
  *   conn        [3*n_elems]  node ids;  jinv [4*n_elems] row-major Dm^-1
- *   elem_mat    [4*n_elems]  rest area, lambda, mu, material type (1, 2, 3 as float)
+ *   elem_mat    [4*n_elems]  rest area, lambda, mu, material type (1, 2, 3 as float);
+ *               a record of any other type (e.g. a spring, type 0) or with a
+ *               node id outside [0, n_nodes) adds no force and is never read
+ *               beyond its own fields
  *   j2_state    [4*n_elems]  eps_p (3) + eqps, updated; j2_param [2*n_elems]
- *               (yield stress, hardening).  Both may be NULL when no triangle
- *               is J2; J2 triangles then run with zero plastic state.
+ *               (yield stress, hardening).  Give both or neither (one NULL
+ *               and the other not is FW_ERR_ARG).  With both NULL, J2
+ *               triangles never yield: they respond with the elastic trial
+ *               stress on zero plastic strain, and no state is stored.
  *   csr_off     [n_nodes+1], csr_slot [3*n_elems]  node -> (3*e + corner),
  *               ascending e within a node
  * The scratch (one float2 per corner) is a fixed array inside the library:
  * at most FW_NOALLOC_MAX_ELEMS triangles (3 MiB, held by every GPU that loads
  * the library); larger meshes are rejected with FW_ERR_ARG.  The first call on
- * a device looks the array's address up (cudaGetSymbolAddress); make that first
- * call before any stream capture.  All calls share the array, so calls that
- * overlap on the GPU race.  Work is queued on `stream` (NULL: legacy default).
+ * a device looks the array's address up (cudaGetSymbolAddress) and caches it;
+ * make that first call before any stream capture.  Calls after a
+ * cudaDeviceReset of that device in the same process are not supported (the
+ * cached address is not looked up again).  All calls share the array, so calls
+ * that overlap on the GPU race.  A CUDA error pending before the call is
+ * reported (FW_ERR_CUDA, left in place) and nothing is launched.  Work is
+ * queued on `stream` (NULL: legacy default).
  * err/err_len: optional buffer for the error text. */
 #define FW_NOALLOC_MAX_ELEMS 131072
 int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps, float dt, float damping,
