@@ -1813,3 +1813,299 @@ void or_destroy(or_world* w) {
   }
   free(w);
 }
+
+/* ======================================================================
+ * Adjoint of the substep (reverse mode), restated in REAL arithmetic.  Test
+ * infrastructure for the differentiable form: the FP64 build gives the exact
+ * derivative of the FP64 trajectory, which the tests compare with FP64
+ * central differences (the formula check) and with the CUDA adjoint (whose
+ * remaining distance is the FP32 trajectory's own rounding).
+ *
+ * Forward substep of node i (femspringmanager.py:315-358, mixedcontact.py):
+ *   f  = contact(x, v) + sum_e f_e(x, state_e; E_e) [+ gravity / nodal force]
+ *   v' = v + dt (f - c v) / m     (enforced / fixed velocity: v' = bc)
+ *   x' = x + dt v'
+ * J2 triangles also update their plastic state: state' = g_e(x, state_e; E_e).
+ * Reverse, from the adjoints (xb', vb', sb') of (x', v', state'):
+ *   vt = vb' + dt xb'
+ *   fb = (dt / m) vt          (0 for fixed / enforced-velocity / prescribed-
+ *                              acceleration nodes)
+ *   vb = (1 - dt c / m) vt + (d contact / d v)^T fb      (0 when v' is fixed)
+ *   xb = xb' + sum_e (d f_e / d x)^T fb + (d contact / d x)^T fb
+ *        + sum_e (d g_e / d x)^T sb'
+ *   sb = sum (d f_e / d state)^T fb + (d g_e / d state)^T sb'
+ *   Eb += (d f_e / d E)^T fb + (d g_e / d E)^T sb'
+ * Every local Jacobian is taken column by column in forward mode (dual
+ * numbers) through the same formulas as element_force / stress / contacts
+ * above, so the derivative is that of this very code.  The broad-phase gates,
+ * the contact branches, the height-field sample / normal indices, the voxel
+ * cell and face, and the J2 yield branch are piecewise constant and are taken
+ * from the recorded forward pass.
+ * ====================================================================== */
+typedef struct {
+  REAL v, d;
+} dual;
+static dual D(REAL v, REAL d) { dual r = {v, d}; return r; }
+static dual dc(REAL v) { return D(v, 0); }
+static dual dadd(dual a, dual b) { return D(a.v + b.v, a.d + b.d); }
+static dual dsub(dual a, dual b) { return D(a.v - b.v, a.d - b.d); }
+static dual dneg(dual a) { return D(-a.v, -a.d); }
+static dual dmul(dual a, dual b) { return D(a.v * b.v, a.d * b.v + a.v * b.d); }
+static dual ddiv(dual a, dual b) {
+  REAL q = a.v / b.v;
+  return D(q, (a.d - q * b.d) / b.v);
+}
+static dual dlog_(dual a) { return D(R_LOG(a.v), a.d / a.v); }
+static dual dsqrt_(dual a) {
+  REAL s = R_SQRT(a.v);
+  return D(s, s > 0 ? a.d / ((REAL)2.0 * s) : (REAL)0.0);
+}
+
+/* element_force + stress in dual numbers: X[6] corner positions, S[4] J2 state
+ * (eps_p Voigt, eqps), E Young's modulus -> F[6] corner forces, SN[4] new state. */
+static void element_dual(const or_world* w, int e, const dual* X, const dual* S, dual E, dual* F, dual* SN) {
+  dual nu = dc(w->nu[e]);
+  dual one = dc(1), two = dc(2), half = dc((REAL)0.5);
+  dual lam = ddiv(dmul(E, nu), dmul(dadd(one, nu), dsub(one, dmul(two, nu))));
+  dual mu = ddiv(E, dmul(two, dadd(one, nu)));
+  dual j00 = dsub(X[0], X[4]), j01 = dsub(X[2], X[4]);
+  dual j10 = dsub(X[1], X[5]), j11 = dsub(X[3], X[5]);
+  const REAL* ji = w->jinv + 4 * e;
+  dual F00 = dadd(dmul(j00, dc(ji[0])), dmul(j01, dc(ji[2])));
+  dual F01 = dadd(dmul(j00, dc(ji[1])), dmul(j01, dc(ji[3])));
+  dual F10 = dadd(dmul(j10, dc(ji[0])), dmul(j11, dc(ji[2])));
+  dual F11 = dadd(dmul(j10, dc(ji[1])), dmul(j11, dc(ji[3])));
+  REAL d00 = ji[0], d01 = ji[1], d10 = ji[2], d11 = ji[3];
+  REAL d20 = -ji[0] - ji[2], d21 = -ji[1] - ji[3];
+  dual C00 = dadd(dmul(F00, F00), dmul(F10, F10));
+  dual C01 = dadd(dmul(F00, F01), dmul(F10, F11));
+  dual C11 = dadd(dmul(F01, F01), dmul(F11, F11));
+  dual e00 = dmul(half, dsub(C00, one)), e01 = dmul(half, C01), e11 = dmul(half, dsub(C11, one));
+  dual s0, s1, s2;
+  for (int k = 0; k < 4; ++k) SN[k] = S[k];
+  int t = w->type[e];
+  if (t == MAT_MISES) {
+    dual t0 = dsub(e00, S[0]), t1 = dsub(e11, S[1]), t2 = dsub(e01, S[2]);
+    dual tr = dadd(t0, t1);
+    dual tm = dmul(two, mu);
+    s0 = dadd(dmul(lam, tr), dmul(tm, t0));
+    s1 = dadd(dmul(lam, tr), dmul(tm, t1));
+    s2 = dmul(tm, t2);
+    dual p = ddiv(dadd(s0, s1), dc(3));
+    dual q0 = dsub(s0, p), q1 = dsub(s1, p), q2 = s2;
+    dual vm = dsqrt_(dadd(dsub(dadd(dmul(q0, q0), dmul(q1, q1)), dmul(q0, q1)), dmul(dc(3), dmul(q2, q2))));
+    dual f = dsub(vm, dadd(dc(w->sy[e]), dmul(dc(w->H[e]), S[3])));
+    if (f.v > (REAL)0.0) {
+      dual dg = ddiv(f, dadd(dmul(dc(3), mu), dc(w->H[e])));
+      SN[3] = dadd(S[3], dg);
+      dual scale = dsub(one, ddiv(dmul(dmul(dc(3), mu), dg), vm));
+      s0 = dadd(dmul(q0, scale), p);
+      s1 = dadd(dmul(q1, scale), p);
+      s2 = dmul(q2, scale);
+      SN[0] = dadd(S[0], dmul(dg, ddiv(q0, vm)));
+      SN[1] = dadd(S[1], dmul(dg, ddiv(q1, vm)));
+      SN[2] = dadd(S[2], dmul(dg, ddiv(q2, vm)));
+    }
+  } else if (t == MAT_ELASTIC) {
+    dual lt = dmul(lam, dadd(e00, e11));
+    dual tm = dmul(two, mu);
+    s0 = dadd(lt, dmul(tm, e00));
+    s1 = dadd(lt, dmul(tm, e11));
+    s2 = dmul(tm, e01);
+  } else {  /* NeoHookean */
+    dual cdet = dsub(dmul(C00, C11), dmul(C01, C01));
+    dual r = ddiv(one, cdet);
+    dual i00 = dmul(C11, r), i01 = dneg(dmul(C01, r)), i11 = dmul(C00, r);
+    dual J = dsub(dmul(F00, F11), dmul(F01, F10));
+    dual c = dsub(dmul(lam, dlog_(J)), mu);
+    s0 = dadd(dmul(c, i00), mu);
+    s1 = dadd(dmul(c, i11), mu);
+    s2 = dmul(c, i01);
+  }
+  dual B[3][6];
+  B[0][0] = dmul(dc(d00), F00); B[0][1] = dmul(dc(d00), F10);
+  B[1][0] = dmul(dc(d01), F01); B[1][1] = dmul(dc(d01), F11);
+  B[2][0] = dadd(dmul(dc(d01), F00), dmul(dc(d00), F01)); B[2][1] = dadd(dmul(dc(d00), F11), dmul(dc(d01), F10));
+  B[0][2] = dmul(dc(d10), F00); B[0][3] = dmul(dc(d10), F10);
+  B[1][2] = dmul(dc(d11), F01); B[1][3] = dmul(dc(d11), F11);
+  B[2][2] = dadd(dmul(dc(d11), F00), dmul(dc(d10), F01)); B[2][3] = dadd(dmul(dc(d10), F11), dmul(dc(d11), F10));
+  B[0][4] = dmul(dc(d20), F00); B[0][5] = dmul(dc(d20), F10);
+  B[1][4] = dmul(dc(d21), F01); B[1][5] = dmul(dc(d21), F11);
+  B[2][4] = dadd(dmul(dc(d21), F00), dmul(dc(d20), F01)); B[2][5] = dadd(dmul(dc(d20), F11), dmul(dc(d21), F10));
+  dual a = dc(w->area[e]);
+  for (int r = 0; r < 6; ++r) {
+    dual fi = dadd(dadd(dmul(B[0][r], s0), dmul(B[1][r], s1)), dmul(B[2][r], s2));
+    F[r] = dneg(dmul(fi, a));
+  }
+}
+
+/* contact force of pair c on a node at (px, py) with velocity (vx, vy), dual. */
+static int contact_dual(const or_pair* c, REAL dt, dual px, dual py, dual vx, dual vy, dual* fx, dual* fy) {
+  dual k = dc(c->penalty);
+  if (c->kind == PAIR_PLANE) {
+    dual pen = dadd(dmul(dsub(px, dc(c->p[0])), dc(c->n[0])), dmul(dsub(py, dc(c->p[1])), dc(c->n[1])));
+    if (!(pen.v < (REAL)0.0)) return 0;
+    *fx = dneg(dmul(dmul(dc(c->n[0]), k), pen));
+    *fy = dneg(dmul(dmul(dc(c->n[1]), k), pen));
+    return 1;
+  }
+  REAL n0, n1;
+  dual sd;
+  if (c->kind == PAIR_HEIGHTFIELD) {
+    REAL sg = hf_signed(c, px.v, py.v, &n0, &n1);
+    if (!(sg < (REAL)0.0)) return 0;
+    /* the interpolated height h(x) is the only x-dependent part of sd */
+    REAL span = c->hubx - c->hlbx;
+    dual u = dc(0);
+    if (span > (REAL)1e-12) u = ddiv(dsub(px, dc(c->hlbx)), dc(span));
+    if (u.v < (REAL)0.0) u = dc(0);
+    if (u.v > (REAL)1.0) u = dc(1);
+    int nx = c->hnx;
+    dual s = dmul(u, dc((REAL)(nx - 1)));
+    int i0 = (int)R_FLOOR(s.v);
+    int i1 = i0 + 1;
+    if (i1 >= nx) i1 = nx - 1;
+    if (i0 < 0) i0 = 0;
+    dual t = dsub(s, dc((REAL)i0));
+    dual h = dadd(dc(c->h[i0]), dmul(dc(c->h[i1] - c->h[i0]), t));
+    sd = dadd(dmul(dsub(px, px), dc(n0)), dmul(dsub(py, h), dc(n1)));
+    *fx = dmul(dmul(dc(-n0), k), sd);
+    *fy = dmul(dmul(dc(-n1), k), sd);
+  } else {
+    REAL s = voxel_signed(c, px.v, py.v, &n0, &n1);
+    if (!(s < (REAL)0.0)) return 0;
+    /* sd = -(distance to the chosen face): linear in the position */
+    dual pd = (n0 != 0) ? px : py;
+    REAL nn = (n0 != 0) ? n0 : n1;
+    REAL face = (n0 != 0 ? px.v : py.v) + nn * (-s); /* face coordinate */
+    sd = dmul(dc(nn), dsub(pd, dc(face)));
+    dual pen = dneg(sd);
+    *fx = dmul(dmul(dc(n0), k), pen);
+    *fy = dmul(dmul(dc(n1), k), pen);
+  }
+  dual vn = dadd(dmul(vx, dc(n0)), dmul(vy, dc(n1)));
+  if (vn.v < (REAL)0.0) {
+    *fx = dadd(*fx, dmul(dmul(dmul(dmul(dc(-n0), dc((REAL)0.5)), k), vn), dc(dt)));
+    *fy = dadd(*fy, dmul(dmul(dmul(dmul(dc(-n1), dc((REAL)0.5)), k), vn), dc(dt)));
+  }
+  return 1;
+}
+
+/* Reverse-mode derivative of n substeps of dt from the current state (which
+ * the call advances, like n forward substeps).  xbar_T / vbar_T (2N, NULL =
+ * 0) seed the adjoint of the final positions / velocities; the outputs are
+ * dL/dx0, dL/dv0 (2N) and dL/dE (E).  Returns -1 for worlds this restatement
+ * does not cover (FEM-FEM contact, rigids, springs). */
+int or_adjoint(or_world* w, int n, float dt_f, float damping_f, long counter0, const double* xbar_T,
+               const double* vbar_T, double* xbar0, double* vbar0, double* Ebar) {
+  if (w->flex || w->rig) return -1;
+  int N = w->n_nodes, E = w->n_elems, P = w->n_pairs;
+  for (int e = 0; e < E; ++e)
+    if (w->type[e] == MAT_SPRING) return -1;
+  REAL dt = (REAL)dt_f, damping = (REAL)damping_f;
+  size_t n2 = 2 * (size_t)N;
+  REAL* xs = (REAL*)malloc(sizeof(REAL) * n2 * (size_t)(n > 0 ? n : 1));
+  REAL* vs = (REAL*)malloc(sizeof(REAL) * n2 * (size_t)(n > 0 ? n : 1));
+  int has_j2 = 0;
+  for (int e = 0; e < E; ++e) has_j2 |= w->type[e] == MAT_MISES;
+  REAL* ss = (REAL*)malloc(sizeof(REAL) * 4 * (size_t)(has_j2 ? E : 1) * (size_t)(n > 0 ? n : 1));
+  char* gates = (char*)malloc((size_t)(P > 0 ? P : 1) * (size_t)(n > 0 ? n : 1));
+  for (int j = 0; j < n; ++j) {
+    memcpy(xs + n2 * j, w->x, sizeof(REAL) * n2);
+    memcpy(vs + n2 * j, w->v, sizeof(REAL) * n2);
+    for (int e = 0; has_j2 && e < E; ++e) {
+      REAL* s = ss + 4 * ((size_t)E * j + e);
+      s[0] = w->epsp[3 * e]; s[1] = w->epsp[3 * e + 1]; s[2] = w->epsp[3 * e + 2]; s[3] = w->eqps[e];
+    }
+    for (int p = 0; p < P; ++p) gates[(size_t)P * j + p] = (char)pair_active(w, &w->pairs[p], counter0 + j);
+    or_step(w, dt_f, damping_f, counter0 + j, 0);
+  }
+  double* xb = (double*)calloc(n2, sizeof(double));
+  double* vb = (double*)calloc(n2, sizeof(double));
+  double* fb = (double*)calloc(n2, sizeof(double));
+  double* sb = (double*)calloc(4 * (size_t)E + 1, sizeof(double));
+  double* sbn = (double*)calloc(4 * (size_t)E + 1, sizeof(double));
+  for (size_t i = 0; i < n2; ++i) {
+    xb[i] = xbar_T ? xbar_T[i] : 0.0;
+    vb[i] = vbar_T ? vbar_T[i] : 0.0;
+  }
+  for (int e = 0; e < E; ++e) Ebar[e] = 0.0;
+  for (int j = n - 1; j >= 0; --j) {
+    const REAL* x = xs + n2 * j;
+    const REAL* v = vs + n2 * j;
+    /* node adjoints through v' and x' */
+    for (int i = 0; i < N; ++i) {
+      int bc = w->bc[i];
+      int vfixed = (bc & (BC_U | BC_V)) != 0;
+      int fdead = vfixed || (bc & BC_A) != 0;
+      double sc = (double)dt / (double)w->mass[i];
+      double keep = 1.0 - sc * (double)damping;
+      for (int k = 0; k < 2; ++k) {
+        double vt = vb[2 * i + k] + (double)dt * xb[2 * i + k];
+        fb[2 * i + k] = fdead ? 0.0 : sc * vt;
+        vb[2 * i + k] = vfixed ? 0.0 : keep * vt;
+      }
+    }
+    /* elements: column by column of the local Jacobian */
+    for (int e = 0; e < E; ++e) {
+      int nd[3] = {w->conn[3 * e], w->conn[3 * e + 1], w->conn[3 * e + 2]};
+      int j2 = w->type[e] == MAT_MISES;
+      static const REAL s_zero[4] = {0, 0, 0, 0};
+      const REAL* s0 = j2 ? ss + 4 * ((size_t)E * j + e) : s_zero;
+      double outb[10];
+      for (int r = 0; r < 6; ++r) outb[r] = fb[2 * nd[r / 2] + (r & 1)];
+      for (int k = 0; k < 4; ++k) outb[6 + k] = j2 ? sb[4 * e + k] : 0.0;
+      int nin = j2 ? 11 : 7; /* 6 positions, [4 state], E */
+      for (int col = 0; col < nin; ++col) {
+        dual X[6], S[4], Fo[6], SN[4];
+        for (int r = 0; r < 6; ++r) X[r] = D(x[2 * nd[r / 2] + (r & 1)], col == r ? 1 : 0);
+        for (int k = 0; k < 4; ++k) S[k] = D(s0[k], (j2 && col == 6 + k) ? 1 : 0);
+        dual Ed = D(w->E[e], col == nin - 1 ? 1 : 0);
+        element_dual(w, e, X, S, Ed, Fo, SN);
+        double dot = 0.0;
+        for (int r = 0; r < 6; ++r) dot += outb[r] * (double)Fo[r].d;
+        if (j2)
+          for (int k = 0; k < 4; ++k) dot += outb[6 + k] * (double)SN[k].d;
+        if (col < 6) xb[2 * nd[col / 2] + (col & 1)] += dot;
+        else if (col < nin - 1) sbn[4 * e + (col - 6)] = dot;
+        else Ebar[e] += dot;
+      }
+    }
+    for (int e = 0; e < 4 * E; ++e) sb[e] = sbn[e];
+    /* contacts (gated as in the forward pass) */
+    for (int p = 0; p < P; ++p) {
+      if (!gates[(size_t)P * j + p]) continue;
+      const or_pair* c = &w->pairs[p];
+      for (int k = 0; k < w->bn_cnt[c->body]; ++k) {
+        int i = w->bnodes[w->bn_off[c->body] + k];
+        for (int col = 0; col < 4; ++col) {
+          dual px = D(x[2 * i], col == 0), py = D(x[2 * i + 1], col == 1);
+          dual vx = D(v[2 * i], col == 2), vy = D(v[2 * i + 1], col == 3);
+          dual fx, fy;
+          if (!contact_dual(c, dt, px, py, vx, vy, &fx, &fy)) break;
+          double dot = fb[2 * i] * (double)fx.d + fb[2 * i + 1] * (double)fy.d;
+          if (col < 2) xb[2 * i + col] += dot;
+          else vb[2 * i + col - 2] += dot;
+        }
+      }
+    }
+  }
+  for (size_t i = 0; i < n2; ++i) {
+    xbar0[i] = xb[i];
+    vbar0[i] = vb[i];
+  }
+  free(xs); free(vs); free(ss); free(gates); free(xb); free(vb); free(fb); free(sb); free(sbn);
+  return 0;
+}
+
+/* FP64 inputs for central differences: Young's modulus per element and the
+ * node state, set without a float32 round trip (the FP64 build keeps them). */
+void or_set_young64(or_world* w, const double* E) {
+  for (int e = 0; e < w->n_elems; ++e) w->E[e] = (REAL)E[e];
+}
+void or_set_state64(or_world* w, const double* x, const double* v) {
+  for (int i = 0; i < 2 * w->n_nodes; ++i) {
+    if (x) w->x[i] = (REAL)x[i];
+    if (v) w->v[i] = (REAL)v[i];
+  }
+}

@@ -97,6 +97,11 @@ def _lib(precision: str):
         L.or_get_rigids.restype = C.c_int
         L.or_sincos32.argtypes = [C.c_float, _f32p, _f32p]
         L.or_gate_by_rigid.argtypes = [C.c_void_p, C.c_int]
+        L.or_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_long, _f64p, _f64p, _f64p, _f64p,
+                                 _f64p]
+        L.or_adjoint.restype = C.c_int
+        L.or_set_young64.argtypes = [C.c_void_p, _f64p]
+        L.or_set_state64.argtypes = [C.c_void_p, _f64p, _f64p]
         _LIBS[name] = L
     return _LIBS[name]
 
@@ -658,6 +663,36 @@ class OracleLoop:
         xa = _fp(x) if x is not None else (None, None)
         va = _fp(v) if v is not None else (None, None)
         self._L.or_set_state(self._w, xa[1], va[1])
+
+    def adjoint(self, n: int, xbar=None, vbar=None, dt: float | None = None):
+        """Reverse-mode derivative of the next n substeps (the loop advances
+        over them): from the adjoints of the final positions / velocities
+        (N x 2, None = 0) to dL/dx0, dL/dv0 (N x 2) and dL/dE (per element).
+        The FP64 build gives the exact derivative of the FP64 trajectory."""
+        d = self.dt if dt is None else dt
+        xt = None if xbar is None else np.ascontiguousarray(xbar, np.float64)
+        vt = None if vbar is None else np.ascontiguousarray(vbar, np.float64)
+        xb = np.zeros((self.N, 2))
+        vb = np.zeros((self.N, 2))
+        eb = np.zeros(self.E)
+        p = lambda a: None if a is None else a.ctypes.data_as(_f64p)  # noqa: E731
+        rc = self._L.or_adjoint(self._w, int(n), float(np.float32(d)), float(np.float32(self.damping)),
+                                self.counter, p(xt), p(vt), p(xb), p(vb), p(eb))
+        if rc != 0:
+            raise NotImplementedError("oracle adjoint: FEM-FEM contact, rigids and springs are not covered")
+        self.counter += int(n)
+        return xb, vb, eb
+
+    def set_young64(self, young):
+        """Per-element Young's modulus in FP64 (no float32 rounding)."""
+        y = np.ascontiguousarray(young, np.float64)
+        self._L.or_set_young64(self._w, y.ctypes.data_as(_f64p))
+
+    def set_state64(self, x=None, v=None):
+        xa = None if x is None else np.ascontiguousarray(x, np.float64)
+        va = None if v is None else np.ascontiguousarray(v, np.float64)
+        self._L.or_set_state64(self._w, None if xa is None else xa.ctypes.data_as(_f64p),
+                               None if va is None else va.ctypes.data_as(_f64p))
 
     def prepared(self):
         m = np.zeros(self.N)
