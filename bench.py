@@ -147,7 +147,7 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.05)
+            time.sleep(0.005)  # 5 ms: several samples even in a timed region of ~40 ms
 
     def __enter__(self):
         if self._ok:
@@ -222,24 +222,27 @@ def run_reference(args, rank, world):
     import oracle
 
     o = oracle.OracleLoop(workload(fw, args.mesh), 0.0, useAdapativeDT=True, precision="f32", threads=threads)
-    sample = 50  # substeps per bench step: a bounded sample of one frame
+    # one bench step = advanceWithTime(1/60), the same frame of substeps the GPU arm times
     for _ in range(args.warmup):
-        o.advance(sample)
+        o.advance_with_time(FRAME)
+    c0 = o.counter
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        o.advance(sample)
+        o.advance_with_time(FRAME)
     el = time.perf_counter() - t0
-    value = o.E * sample * args.steps / el
+    sample = (o.counter - c0) // args.steps
+    value = o.E * (o.counter - c0) / el
     line = {
         "impl": "reference", "metric": "FEM element-steps/s", "value": value, "unit": "element-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"plain large single mesh {args.mesh}x{args.mesh} quads, NeoHookean, height field",
-                   "elements": o.E, "nodes": o.N, "substeps_per_step": sample, "dt": o.dt},
+                   "elements": o.E, "nodes": o.N, "step": "advanceWithTime(1/60)", "substeps_per_step": sample,
+                   "dt": o.stableTime},
         "cpu_baseline": {"value": value, "unit": "element-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} substeps per step x {args.steps} steps of the workload, FP32 C "
-                                   f"restatement of the reference scheme, {threads} threads"},
+                         "sample": f"{args.steps} steps of advanceWithTime(1/60) ({sample} substeps each) of the "
+                                   f"workload, FP32 C restatement of the reference scheme, {threads} threads"},
         "e2e": {"value": value, "unit": "element-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -1112,7 +1115,9 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": which, "algorithmic_bytes_per_substep": bstep,
                          "us_per_substep": per_sub_s * 1e6,
-                         "traffic": traffic},
+                         "traffic": traffic,
+                         "traffic_from": "profiles/traffic_plain_large.json (ncu capture of this workload, "
+                                         "committed; not measured in this run)"},
             "e2e": {"value": e2e, "unit": "element-steps/s", "h2d_bytes_per_step": 2 * N * 8,
                     "d2h_bytes_per_step": 2 * N * 8},
             "gpu_launches": launches,
