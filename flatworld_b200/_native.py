@@ -55,6 +55,7 @@ _SIGNATURES = {
     "fw_set_boundary_edges": (C.c_int, [_vp, C.c_int32, _i32p, _i32p, _i32p]),
     "fw_set_flex_scene": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f32p]),
     "fw_add_flex_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float]),
+    "fw_tie_flex_pair": (C.c_int, [_vp, C.c_int32]),
     "fw_set_flex_clock": (C.c_int, [_vp, C.c_double]),
     "fw_set_flex_clocks": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "fw_mass_scaling": (C.c_int, [_vp, C.c_float]),
@@ -99,6 +100,8 @@ _SIGNATURES = {
     "fw_energy": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "fw_scene_status": (C.c_int, [_vp, _vp, C.c_int32]),
     "fw_clear_scene_status": (C.c_int, [_vp, C.c_int32]),
+    "fw_set_cfl_monitor": (C.c_int, [_vp, _vp]),
+    "fw_read_cfl": (C.c_int, [_vp, _vp, C.c_int32]),
     "fw_launch_count": (C.c_int64, [_vp]),
     "fw_build_info": (C.c_char_p, []),
     "fw_step_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, _vp, _vp, _vp, _vp, _vp,
@@ -225,6 +228,9 @@ class NativeWorld:
     def add_flex_pair(self, body1, body2, penalty, friction):
         self._check(self._L.fw_add_flex_pair(self._h, int(body1), int(body2), float(penalty), float(friction)),
                     "fw_add_flex_pair")
+
+    def tie_flex_pair(self, pair):
+        self._check(self._L.fw_tie_flex_pair(self._h, int(pair)), "fw_tie_flex_pair")
 
     def read_flex_state(self, n_items: int):
         """(work-item edge caches int32[n_items], hash grid float32[8])."""
@@ -446,6 +452,20 @@ class NativeWorld:
         if out is None:
             out = np.zeros((n_scenes,), dtype=np.int32)
         self._check(self._L.fw_scene_status(self._h, out.ctypes.data, 1 if asynchronous else 0), "fw_scene_status")
+        return out
+
+    def set_cfl_monitor(self, coef_per_body):
+        """Turn the CFL monitor on with 0.4 / sqrt(E / rho) per body (None: off)."""
+        if coef_per_body is None:
+            self._check(self._L.fw_set_cfl_monitor(self._h, None), "fw_set_cfl_monitor")
+            return
+        c = np.ascontiguousarray(coef_per_body, np.float32)
+        self._check(self._L.fw_set_cfl_monitor(self._h, c.ctypes.data), "fw_set_cfl_monitor")
+
+    def read_cfl(self, n_scenes: int, reset: bool = True):
+        """Smallest current-shape stable time per scene since the last reset."""
+        out = np.zeros((n_scenes,), dtype=np.float32)
+        self._check(self._L.fw_read_cfl(self._h, out.ctypes.data, 1 if reset else 0), "fw_read_cfl")
         return out
 
     def clear_scene_status(self, scene: int = -1):

@@ -41,7 +41,8 @@ struct FlexGrid {
   float olx, oly, gsx, gsy;
   int estimate;  // ordered-int minimum of the element box diagonals
   int rebuild;   // this substep rebuilds the hash
-  int pad[2];
+  int tie_init;  // the scene's tied work items have looked for their edges (first substep)
+  int pad;
   double elapsed;   // simulated time since the last rebuild (float64, as the host's float)
 };
 
@@ -54,6 +55,7 @@ struct FlexScene {
   int be0, n_be;                 // its boundary edges (registration order)
   int max_pairs, pair_base;      // its (cell, element) pair capacity and slot base
   int cell_base, pad;            // its cells: k * kFlexMaxCells
+  int n_tied, n_untied;          // its work items of tied / untied pairs
 };
 
 // The FEM-FEM state of a world; a kernel works on one scene's view of it
@@ -100,6 +102,14 @@ struct FlexDev {
   int n_seg;            // (pair, side) segments of consecutive work items
   const int4* seg;      // per segment: first item, item count, pair (in the scene), target body
   int32_t* seg_off;     // [n_seg + 1]: exclusive scan of the active segments' item counts
+  // tied pairs (ExplicitLoop(ties=...)): per pair, and per work item the edge
+  // it found at the first substep (-1: none), its weights and normal gap
+  const int32_t* pair_tied;
+  int32_t* tie_elem;
+  float* tie_w0;
+  float* tie_w1;
+  float* tie_gap;
+  int n_tied, n_untied;  // the view's scene
 };
 
 __device__ __forceinline__ FlexDev flex_view(const FlexDev& f0, int k) {
@@ -108,7 +118,8 @@ __device__ __forceinline__ FlexDev flex_view(const FlexDev& f0, int k) {
   f.scene = c.scene; f.body0 = c.body0; f.n_fem = c.n_fem; f.n_dom = c.n_dom; f.skip_bvh = c.skip_bvh;
   f.n_pairs = c.n_pairs; f.n_seg = c.n_seg; f.be0 = c.be0; f.n_be = c.n_be; f.max_pairs = c.max_pairs;
   f.dom_obj += c.dom_off; f.dom_body += c.dom_off; f.dom_box += c.dom_off;
-  f.pair_body += c.pair_off; f.pair_active += c.pair_off;
+  f.pair_body += c.pair_off; f.pair_active += c.pair_off; f.pair_tied += c.pair_off;
+  f.n_tied = c.n_tied; f.n_untied = c.n_untied;
   f.g += k;
   f.cell_count += c.cell_base; f.cell_start += c.cell_base; f.cell_end += c.cell_base;
   f.cursor += c.cell_base; f.crange += c.cell_base;
@@ -326,6 +337,8 @@ __device__ void flex_rebuild(const Dev& d, const FlexDev& f) {
   __syncthreads();
 }
 
+__device__ void flex_ties(const Dev& d, const FlexDev& f);
+
 // Per substep, before k_elements, one block: the hash clock and, when it
 // fires, the rebuild (flex_rebuild); pair activation, the broad-phase domain
 // stamps, and the compacted list of work items that run.  force != 0: the
@@ -340,7 +353,10 @@ __global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f0
   const bool step = !force && flex_stepping(d, s);
   if (threadIdx.x == 0) {
     int rb = force ? 1 : 0;
-    if (step) {  // maybe_rebuild_fem_spatial_hash(self.dt)
+    // maybe_rebuild_fem_spatial_hash(self.dt), called while untied work items
+    // remain or the tied ones have not looked for their edges yet
+    // (mixedcontact.py:1667-1678)
+    if (step && (f.n_untied > 0 || (f.n_tied > 0 && !f.g->tie_init))) {
       double e = f.g->elapsed + f.clock_dt[blockIdx.x];
       if (e >= kFlexRebuildInterval) {
         rb = 1;
@@ -392,7 +408,7 @@ __global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f0
   // compacted so the contact kernel visits nothing else
   for (int q = threadIdx.x; q < f.n_seg; q += blockDim.x) {
     const int4 sg = f.seg[q];
-    const bool on = f.pair_active[sg.z] && (f.skip_bvh || f.stamped[sg.w]);
+    const bool on = !f.pair_tied[sg.z] && f.pair_active[sg.z] && (f.skip_bvh || f.stamped[sg.w]);
     f.seg_off[q] = on ? sg.y : 0;
   }
   __syncthreads();
@@ -401,6 +417,7 @@ __global__ void __launch_bounds__(kFlexScanThreads) k_flex_pre(Dev d, FlexDev f0
     f.seg_off[f.n_seg] = total;
     f.g->n_active = total;
   }
+  if (f.n_tied > 0) flex_ties(d, f);
 }
 
 // pointToEdgeContact + detectPointToMeshBoundary (contact_detection.py:15-92):
@@ -447,6 +464,115 @@ __device__ __forceinline__ void flex_push(const Dev& d, int* err, int node, int 
   } else {
     atomicOr(err, 1);
   }
+}
+
+// Tied pairs (mixedcontact.py:1680-1690).  At the scene's first substep every
+// tied work item looks for the boundary edge of its target nearest to its node
+// (_initialize_fem_fem_ties_once_kernel, mixedcontact.py:686-771: the hash
+// query with a buffer of max(1e-4, cell size, 0.001), the smallest |pen|
+// inside it) and keeps the edge, the weights of the foot point and the gap
+// along the edge normal; every substep a penalty spring then pulls the node to
+// that point (_apply_fem_fem_ties_fixed_kernel, mixedcontact.py:774-809), with
+// the reactions on the edge's nodes.  The reference launches the ties before
+// the contact kernel, which skips tied items: tie entries carry the work item
+// as their key, contact entries n_items + work item, so each node adds its tie
+// forces first.
+__device__ __forceinline__ float2 flex_tie_point(const Dev& d, int2 n, float w0, float w1) {
+  const float2 a = d.x[n.x], b = d.x[n.y];
+  float x = 0.0f, y = 0.0f;
+  x = x + a.x * w0;
+  y = y + a.y * w0;
+  x = x + b.x * w1;
+  y = y + b.y * w1;
+  return make_float2(x, y);
+}
+
+__device__ __forceinline__ float2 flex_tie_normal(const Dev& d, int2 n) {
+  const float2 a = d.x[n.x], b = d.x[n.y];
+  const float ex = b.x - a.x, ey = b.y - a.y;
+  const float el = sqrtf(ex * ex + ey * ey);
+  float tx = 1.0f, ty = 0.0f;
+  if (el > 1e-10f) {
+    tx = ex / el;
+    ty = ey / el;
+  }
+  return make_float2(-ty, tx);
+}
+
+__device__ void flex_tie_resolve(const Dev& d, const FlexDev& f, const FlexGrid& g, int it, int target) {
+  if (g.tc <= 0) return;
+  const int nid = f.item_node[it];
+  const float2 p = d.x[nid];
+  const float qbuf = wmax(wmax(1e-4f, wmax(g.gsx, g.gsy)), 0.001f);
+  const int lx = flex_cell(p.x - qbuf - g.olx, g.gsx, g.cnx), ly = flex_cell(p.y - qbuf - g.oly, g.gsy, g.cny);
+  const int ux = flex_cell(p.x + qbuf - g.olx, g.gsx, g.cnx), uy = flex_cell(p.y + qbuf - g.oly, g.gsy, g.cny);
+  int cand[kFlexMaxQuery];
+  int num = 0;
+  for (int ix = lx; ix <= ux; ++ix)
+    for (int iy = ly; iy <= uy; ++iy) {
+      const int cid = ix + iy * g.cnx;
+      if (cid < 0 || cid >= g.tc) continue;
+      for (int q = f.cell_start[cid]; q < f.cell_end[cid]; ++q) {
+        const int e = f.sorted[q];
+        if (e < 0 || f.be_dom[e] != target) continue;
+        bool dup = false;
+        for (int k = 0; k < num; ++k) dup |= cand[k] == e;
+        if (!dup && num < kFlexMaxQuery) cand[num++] = e;
+      }
+    }
+  float best = 1e9f, bw0 = 0.f, bw1 = 0.f;
+  int be = -1;
+  for (int j = 0; j < num; ++j) {
+    const int e = cand[j];
+    const int2 n = f.be[e];
+    float nx, ny, w0, w1;
+    const float pen = flex_detect(p, d.x[n.x], d.x[n.y], qbuf, nx, ny, w0, w1);
+    if (fabsf(pen) < fabsf(best) && fabsf(pen) < qbuf) {
+      bw0 = w0;
+      bw1 = w1;
+      be = e;
+      best = pen;
+    }
+  }
+  if (be < 0) return;
+  const int2 n = f.be[be];
+  const float2 cp = flex_tie_point(d, n, bw0, bw1);
+  const float gx = p.x - cp.x, gy = p.y - cp.y;
+  const float2 nn = flex_tie_normal(d, n);
+  f.tie_elem[it] = be;
+  f.tie_w0[it] = bw0;
+  f.tie_w1[it] = bw1;
+  f.tie_gap[it] = gx * nn.x + gy * nn.y;
+}
+
+__device__ void flex_ties(const Dev& d, const FlexDev& f) {
+  __syncthreads();  // the hash (if rebuilt) and the grid are final
+  const bool init = f.g->tie_init == 0;
+  const FlexGrid g = *f.g;
+  __syncthreads();  // every thread has read tie_init
+  for (int q = 0; q < f.n_seg; ++q) {
+    const int4 sg = f.seg[q];
+    if (!f.pair_tied[sg.z]) continue;
+    for (int it = sg.x + threadIdx.x; it < sg.x + sg.y; it += blockDim.x) {
+      if (init && f.tie_elem[it] < 0) flex_tie_resolve(d, f, g, it, sg.w);
+      const int e = f.tie_elem[it];
+      if (e < 0) continue;
+      const int nid = f.item_node[it];
+      const int2 n = f.be[e];
+      const float w0 = f.tie_w0[it], w1 = f.tie_w1[it], gap = f.tie_gap[it], k = f.item_pen[it];
+      const float2 cp = flex_tie_point(d, n, w0, w1);
+      const float2 nn = flex_tie_normal(d, n);
+      const float2 x = d.x[nid];
+      const float tx = cp.x + gap * nn.x, ty = cp.y + gap * nn.y;
+      const float mx = tx - x.x, my = ty - x.y;
+      const float fx = k * mx, fy = k * my;
+      flex_push(d, f.err, nid, it, make_float2(fx, fy));
+      flex_push(d, f.err, n.x, it, make_float2(-(fx * w0), -(fy * w0)));
+      flex_push(d, f.err, n.y, it, make_float2(-(fx * w1), -(fy * w1)));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && init) f.g->tie_init = 1;
 }
 
 // _batched_flexflex_contact_kernel_sh.  A work item's pair is active only
@@ -597,9 +723,10 @@ __device__ __forceinline__ void flex_item(const Dev& d, const FlexDev& f, const 
         ty = ty + ddy * fric * nl;
       }
     }
-    flex_push(d, f.err, nid, it, make_float2(tx, ty));
-    flex_push(d, f.err, bn0, it, make_float2(-(tx * bw0), -(ty * bw0)));
-    flex_push(d, f.err, bn1, it, make_float2(-(tx * bw1), -(ty * bw1)));
+    const int key = f.n_items + it;  // after every tie entry of the node
+    flex_push(d, f.err, nid, key, make_float2(tx, ty));
+    flex_push(d, f.err, bn0, key, make_float2(-(tx * bw0), -(ty * bw0)));
+    flex_push(d, f.err, bn1, key, make_float2(-(tx * bw1), -(ty * bw1)));
   }
 }
 

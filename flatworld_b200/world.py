@@ -175,8 +175,6 @@ class SceneLayout:
                 tie_pairs.add((min(ia, ib), max(ia, ib)))
         for c in contacts:
             c.tied = (min(c.pair_ids), max(c.pair_ids)) in tie_pairs
-            if c.tied and c.kind == "flex":
-                raise NotImplementedError("tied FEM-FEM pairs (ExplicitLoop ties=...) are not part of flatworld_b200")
         self.contacts = contacts
         for c in contacts:  # explicitloop.py:313-315
             stable = min(stable, c.stableTime)
@@ -337,6 +335,18 @@ class PackedWorld:
         self.B = len(noff)
         self.S = len(scenes)
 
+    def cfl_coefficients(self):
+        """Per body, 0.4 / sqrt(E / rho) of its material (the factor of the
+        reference's FemDomain.stableTime = 0.4 * L_min / sqrt(E / rho),
+        femdomain.py:24), float32; 0 for spring-mass domains."""
+        out = np.zeros(self.B, np.float32)
+        for si, sc in enumerate(self.scenes):
+            for fi, dom in enumerate(sc.fem):
+                if dom.type == DomainType.FEM:
+                    mat = dom.prop.getMaterial()
+                    out[self.body_of[(si, fi)]] = 0.4 / (float(mat.E) / float(mat.rho)) ** 0.5
+        return out
+
     def rigid_records(self):
         """Per rigid, scene-major: float32[16] and int32[4] (type, BC bits,
         considerContact, scene) for fw_set_rigids; per ground of a scene with
@@ -388,7 +398,7 @@ class PackedWorld:
 
     def flex_records(self):
         """Per scene with FEM-FEM pairs: (scene, skip_bvh, dom_obj, dom_body,
-        dom_box, [(body1, body2, penalty f32, friction f32)])."""
+        dom_box, [(body1, body2, penalty f32, friction f32, tied)])."""
         out = []
         for si, sc in enumerate(self.scenes):
             if not sc.flex:
@@ -406,7 +416,7 @@ class PackedWorld:
                     dom_box[g, :2] = np.asarray(lo, np.float32).reshape(2)
                     dom_box[g, 2:] = np.asarray(hi, np.float32).reshape(2)
             pairs = [(self.body_of[(si, fem_index[id(c.fem)])], self.body_of[(si, fem_index[id(c.ground)])],
-                      np.float32(c.penalty), np.float32(c.friction)) for c in sc.flex]
+                      np.float32(c.penalty), np.float32(c.friction), bool(c.tied)) for c in sc.flex]
             out.append((si, sc.skip_bvh, dom_obj, dom_body, dom_box, pairs))
         return out
 
@@ -475,10 +485,14 @@ def stage(nw: _native.NativeWorld, packed: PackedWorld):
     flex = packed.flex_records()
     if flex:
         nw.set_boundary_edges(packed.bedges, packed.beoff, packed.becnt)
+        n_flex = 0
         for si, skip, obj, body, box, pairs in flex:
             nw.set_flex_scene(si, skip, obj, body, box)
-            for b1, b2, pen, fric in pairs:
+            for b1, b2, pen, fric, tied in pairs:
                 nw.add_flex_pair(b1, b2, pen, fric)
+                if tied:
+                    nw.tie_flex_pair(n_flex)
+                n_flex += 1
 
 
 def _as_float(v) -> float:

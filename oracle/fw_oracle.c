@@ -700,6 +700,10 @@ typedef struct or_flex {
   int32_t *edom, *eid;        /* domain id, element id per registered element */
   int32_t *pair_cell, *pair_elem, *sorted, *cell_count, *cell_offset, *cell_start, *cell_end;
   int32_t cand[FLEX_MAX_QUERY];
+  /* tied pairs (ExplicitLoop(ties=...)): per work item */
+  int32_t *item_tied, *tie_resolved, *tie_elem;
+  REAL *tie_w0, *tie_w1, *tie_gap;
+  int n_tied, tie_initialized;
 } or_flex;
 
 static REAL rmin(REAL a, REAL b) { return a < b ? a : b; }
@@ -924,9 +928,101 @@ static const REAL* dom_box(const or_world* w, int g) {
  * work item runs only if the domain whose GLOBAL index equals the item's target
  * FEM-local index appears in some BVH pair this step -- the reference indexes
  * the global stamp array with the FEM-local id; restated as written. */
+/* _eval_fixed_tie_point and _fem_fem_tie_elem_normal (mixedcontact.py:136-163). */
+static void tie_point(const or_world* w, int e, REAL w0, REAL w1, REAL* cx, REAL* cy) {
+  const or_flex* f = w->flex;
+  int a = f->be[2 * e], b = f->be[2 * e + 1];
+  REAL x = 0, y = 0;
+  x = x + w->x[2 * a] * w0;
+  y = y + w->x[2 * a + 1] * w0;
+  x = x + w->x[2 * b] * w1;
+  y = y + w->x[2 * b + 1] * w1;
+  *cx = x;
+  *cy = y;
+}
+static void tie_normal(const or_world* w, int e, REAL* nx, REAL* ny) {
+  const or_flex* f = w->flex;
+  int a = f->be[2 * e], b = f->be[2 * e + 1];
+  REAL ex = w->x[2 * b] - w->x[2 * a], ey = w->x[2 * b + 1] - w->x[2 * a + 1];
+  REAL el = R_SQRT(ex * ex + ey * ey);
+  REAL tx = 1, ty = 0;
+  if (el > (REAL)1e-10) {
+    tx = ex / el;
+    ty = ey / el;
+  }
+  *nx = -ty;
+  *ny = tx;
+}
+
+/* Tied pairs (mixedcontact.py:1680-1690): once, at the first substep, every
+ * tied work item finds the boundary edge of its target domain nearest to its
+ * node (_initialize_fem_fem_ties_once_kernel, mixedcontact.py:686-771) and
+ * keeps its edge, weights and normal gap; then, every substep, a penalty
+ * spring pulls the node to that point of the edge, with the reactions on the
+ * edge's nodes (_apply_fem_fem_ties_fixed_kernel, mixedcontact.py:774-809).
+ * Launched before the contact kernel, which skips tied items. */
+static void flex_ties(or_world* w) {
+  or_flex* f = w->flex;
+  if (!f->tie_initialized) {
+    REAL qbuf = rmax(rmax((REAL)1e-4, rmax(f->gsx, f->gsy)), (REAL)0.001);
+    for (int it = 0; it < f->n_items; ++it) {
+      if (!f->item_tied[it] || f->tie_resolved[it]) continue;
+      int nid = f->item_node[it];
+      REAL px = w->x[2 * nid], py = w->x[2 * nid + 1];
+      REAL best = (REAL)1e9, bw0 = 0, bw1 = 0;
+      int be = -1, found = 0;
+      int n = flex_query(f, px, py, qbuf, f->item_target[it]);
+      for (int j = 0; j < n; ++j) {
+        int e = f->cand[j];
+        REAL nx, ny, w0, w1;
+        REAL pen = detect_edge(w, px, py, e, qbuf, &nx, &ny, &w0, &w1);
+        if (R_FABS(pen) < R_FABS(best) && R_FABS(pen) < qbuf) {
+          bw0 = w0;
+          bw1 = w1;
+          found = 1;
+          be = e;
+          best = pen;
+        }
+      }
+      if (found) {
+        REAL cx, cy, nx, ny;
+        tie_point(w, be, bw0, bw1, &cx, &cy);
+        REAL gx = px - cx, gy = py - cy;
+        tie_normal(w, be, &nx, &ny);
+        f->tie_resolved[it] = 1;
+        f->tie_elem[it] = be;
+        f->tie_w0[it] = bw0;
+        f->tie_w1[it] = bw1;
+        f->tie_gap[it] = gx * nx + gy * ny;
+      }
+    }
+    f->tie_initialized = 1;
+  }
+  for (int it = 0; it < f->n_items; ++it) {
+    if (!f->item_tied[it] || !f->tie_resolved[it]) continue;
+    int nid = f->item_node[it], e = f->tie_elem[it];
+    REAL w0 = f->tie_w0[it], w1 = f->tie_w1[it], gap = f->tie_gap[it], k = f->item_pen[it];
+    REAL cx, cy, nx, ny;
+    tie_point(w, e, w0, w1, &cx, &cy);
+    tie_normal(w, e, &nx, &ny);
+    REAL tx = cx + gap * nx, ty = cy + gap * ny;
+    REAL mx = tx - w->x[2 * nid], my = ty - w->x[2 * nid + 1];
+    REAL fx = k * mx, fy = k * my;
+    int a = f->be[2 * e], b = f->be[2 * e + 1];
+    w->fext[2 * nid] += fx;
+    w->fext[2 * nid + 1] += fy;
+    w->fext[2 * a] += -(fx * w0);
+    w->fext[2 * a + 1] += -(fy * w0);
+    w->fext[2 * b] += -(fx * w1);
+    w->fext[2 * b + 1] += -(fy * w1);
+  }
+}
+
 static void flex_contacts(or_world* w, long counter) {
   or_flex* f = w->flex;
   if (!f || f->n_items == 0) return;
+  if (f->n_tied > 0) flex_ties(w);
+  if (f->n_tied == f->n_items) return; /* the contact kernel runs only for untied items */
   int* active = (int*)malloc(sizeof(int) * (size_t)(f->n_pairs + 1));
   int* stamped = (int*)malloc(sizeof(int) * (size_t)(f->n_fem + 1));
   for (int p = 0; p < f->n_pairs; ++p)
@@ -939,6 +1035,7 @@ static void flex_contacts(or_world* w, long counter) {
   }
   REAL qbuf = rmax(rmax((REAL)1e-4, rmax(f->gsx, f->gsy)), (REAL)0.016);
   for (int it = 0; it < f->n_items; ++it) {
+    if (f->item_tied[it]) continue;
     if (!active[f->item_pair[it]]) continue;
     int target = f->item_target[it];
     if (!f->skip_bvh && !stamped[target]) continue;
@@ -1534,6 +1631,18 @@ int or_add_flex_pair(or_world* w, int b1, int b2, float penalty, float friction)
   f->item_cache = (int32_t*)realloc(f->item_cache, sizeof(int32_t) * (size_t)n);
   f->item_pen = (REAL*)realloc(f->item_pen, sizeof(REAL) * (size_t)n);
   f->item_fric = (REAL*)realloc(f->item_fric, sizeof(REAL) * (size_t)n);
+  f->item_tied = (int32_t*)realloc(f->item_tied, sizeof(int32_t) * (size_t)n);
+  f->tie_resolved = (int32_t*)realloc(f->tie_resolved, sizeof(int32_t) * (size_t)n);
+  f->tie_elem = (int32_t*)realloc(f->tie_elem, sizeof(int32_t) * (size_t)n);
+  f->tie_w0 = (REAL*)realloc(f->tie_w0, sizeof(REAL) * (size_t)n);
+  f->tie_w1 = (REAL*)realloc(f->tie_w1, sizeof(REAL) * (size_t)n);
+  f->tie_gap = (REAL*)realloc(f->tie_gap, sizeof(REAL) * (size_t)n);
+  for (int i = n0; i < n; ++i) {
+    f->item_tied[i] = 0;
+    f->tie_resolved[i] = 0;
+    f->tie_elem[i] = -1;
+    f->tie_w0[i] = f->tie_w1[i] = f->tie_gap[i] = 0;
+  }
   int k = n0;
   for (int side = 0; side < 2; ++side) {
     int src = side == 0 ? b2 : b1, dst = side == 0 ? b1 : b2;
@@ -1550,6 +1659,26 @@ int or_add_flex_pair(or_world* w, int b1, int b2, float penalty, float friction)
   }
   f->n_items = n;
   return p;
+}
+
+/* Mark the work items of flex pair p tied (explicitloop.py:265-270: the pair
+ * is named in ExplicitLoop(ties=...)). */
+int or_set_flex_pair_tied(or_world* w, int p, int tied) {
+  or_flex* f = w->flex;
+  if (!f || p < 0 || p >= f->n_pairs) return -1;
+  for (int i = 0; i < f->n_items; ++i)
+    if (f->item_pair[i] == p && f->item_tied[i] != (tied != 0)) {
+      f->item_tied[i] = tied != 0;
+      f->n_tied += tied ? 1 : -1;
+    }
+  return 0;
+}
+int or_flex_counts(const or_world* w, int32_t* out) {
+  const or_flex* f = w->flex;
+  out[0] = f ? f->n_items : 0;
+  out[1] = f ? f->n_tied : 0;
+  out[2] = f ? f->tie_initialized : 0;
+  return 0;
 }
 
 /* _mass_scaling_kernel (femspringmanager.py:139-196), FEM triangles, serial in
@@ -1807,6 +1936,7 @@ void or_destroy(or_world* w) {
     free(f->item_pair); free(f->item_cache); free(f->item_pen); free(f->item_fric);
     free(f->pair_b1); free(f->pair_b2); free(f->be); free(f->be_off); free(f->be_cnt);
     free(f->dom_obj); free(f->dom_body); free(f->dom_box); free(f->ebox); free(f->edom); free(f->eid);
+    free(f->item_tied); free(f->tie_resolved); free(f->tie_elem); free(f->tie_w0); free(f->tie_w1); free(f->tie_gap);
     free(f->pair_cell); free(f->pair_elem); free(f->sorted); free(f->cell_count); free(f->cell_offset);
     free(f->cell_start); free(f->cell_end);
     free(f);

@@ -82,6 +82,8 @@ def _lib(precision: str):
                                       _f64p, _f64p, _f64p]
         L.or_set_flex.argtypes = [C.c_void_p, C.c_int, _i32p, _i32p, _i32p, C.c_int, _i32p, _i32p, _f32p, C.c_int]
         L.or_add_flex_pair.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.or_set_flex_pair_tied.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.or_flex_counts.argtypes = [C.c_void_p, _i32p]
         L.or_flex_rebuild.argtypes = [C.c_void_p]
         L.or_get_flex_cache.argtypes = [C.c_void_p, _i32p]
         L.or_get_flex_grid.argtypes = [C.c_void_p, _f64p]
@@ -443,10 +445,20 @@ class OracleLoop:
             do, db, dbx = _ip(dom_obj), _ip(dom_body), _fp(dom_box)
             self._keep += [ea, eo, ec, do, db, dbx]
             L.or_set_flex(self._w, len(ea[0]) // 2, ea[1], eo[1], ec[1], len(domains), do[1], db[1], dbx[1], skip_bvh)
+            # _parse_tie_entry / _is_tie_pair (explicitloop.py:400-439): integer domain pairs
+            flex_ties = set()
+            for t in (ties or []):
+                if isinstance(t, (tuple, list)) and len(t) == 2 and all(isinstance(v, (int, np.integer)) for v in t):
+                    a, b = (int(v) + (len(domains) if v < 0 else 0) for v in t)
+                    if 0 <= a < len(domains) and 0 <= b < len(domains) and a != b:
+                        flex_ties.add((min(a, b), max(a, b)))
+            gidx = lambda d: next(k for k, e in enumerate(domains) if e is d)  # noqa: E731
             for _, d1, d2, pen, _ in flex:
                 fric = max(d1.friction, d2.friction)
-                L.or_add_flex_pair(self._w, fem.index(d1), fem.index(d2), float(np.float32(pen)),
-                                   float(np.float32(fric)))
+                p = L.or_add_flex_pair(self._w, fem.index(d1), fem.index(d2), float(np.float32(pen)),
+                                       float(np.float32(fric)))
+                if tuple(sorted((gidx(d1), gidx(d2)))) in flex_ties:
+                    L.or_set_flex_pair_tied(self._w, p, 1)
         self.sh_elapsed = 0.0
         self.counter = 0
         # setGlobalAABB -> substep(0.0, 0.0) (femspringmanager.py:872-879)
@@ -617,11 +629,16 @@ class OracleLoop:
     def advance(self, n: int = 1, dt: float | None = None):
         d = self.dt if dt is None else dt
         for _ in range(n):
-            if self.flex:  # maybe_rebuild_fem_spatial_hash(self.dt), femspringmanager.py:1035-1039
-                self.sh_elapsed += d
-                if self.sh_elapsed >= 1.0 / 500.0:
-                    self._L.or_flex_rebuild(self._w)
-                    self.sh_elapsed = 0.0
+            if self.flex:
+                # maybe_rebuild_fem_spatial_hash(self.dt) (femspringmanager.py:1035-1039), called
+                # while untied items remain or the ties are not yet initialised (mixedcontact.py:1667-1678)
+                cnt = np.zeros(3, np.int32)
+                self._L.or_flex_counts(self._w, cnt.ctypes.data_as(_i32p))
+                if cnt[1] < cnt[0] or (cnt[1] > 0 and not cnt[2]):
+                    self.sh_elapsed += d
+                    if self.sh_elapsed >= 1.0 / 500.0:
+                        self._L.or_flex_rebuild(self._w)
+                        self.sh_elapsed = 0.0
             self._L.or_step(self._w, float(np.float32(d)), float(np.float32(self.damping)), self.counter, 0)
             self.counter += 1
             if self.entries:  # explicitloop.py:533-538

@@ -50,7 +50,10 @@ CASES = {
     "nh_heightfield32": ("plain_large_scene", {"n": 32, "hf_offset": 0.17}, 0.0, True, ("steps", 3000, 250)),
     "j2_block": ("j2_block_scene", {}, 5e-5, False, ("steps", 4000, 400)),
     "bcs": ("bcs_scene", {}, 0.0, True, ("frames", 60, 10)),
+    "tied_slabs": ("tied_slabs_scene", {}, 1.25e-5, False, ("steps", 3000, 300)),
 }
+# ExplicitLoop keyword arguments beyond dt / useAdapativeDT, per case
+LOOP_KW = {"tied_slabs": {"ties": [(0, 1)]}}
 
 
 def reference_api():
@@ -84,7 +87,8 @@ def run_case(name: str) -> str:
     quiet = io.StringIO()
     t0 = time.time()
     with contextlib.redirect_stdout(quiet):
-        loop = rf.ExplicitLoop(dt, getattr(scenes, builder)(ns, **kw), useAdapativeDT=adaptive)
+        loop = rf.ExplicitLoop(dt, getattr(scenes, builder)(ns, **kw), useAdapativeDT=adaptive,
+                               **LOOP_KW.get(name, {}))
     dt0 = float(loop.dt)  # advanceWithTime changes loop.dt (its last substep is the remainder)
     fsm = loop.femSpringManager
     n = int(fsm.totalNodes.numpy()[0])

@@ -473,3 +473,25 @@ def bcs_scene(fw):
                       False)
     d3 = fw.FemDomain(fw.Mesh(2, conn, c + 0.5), prop, [], False, initials=[fw.InitialVel([0, 1], [0, -1.0])])
     return [d0, d1, d2, d3]
+
+
+def tied_slabs_scene(fw, disk=True):
+    """Two slabs glued by a tie (ExplicitLoop(ties=[(0, 1)])): a 16 x 4 Elastic
+    cantilever clamped at its left end, and an 8 x 4 NeoHookean slab resting on
+    its top face, sliding sideways at 0.2 m/s, held by the tie; both under
+    gravity.  With ``disk``, a free Elastic disk drops onto the upper slab:
+    untied FEM-FEM contact in the same loop, so nodes of the upper slab take
+    tie and contact forces in one substep.  Stable at a fixed dt of 1.25e-5
+    (half the loop's adaptive dt; at the adaptive dt the soft bodies' penalty
+    contact diverges, in the oracle as in the reference's scheme)."""
+    a = fw.FemDomain(ccw_rectangle(fw, 16, 4, 0.2, 0.05, (0.0, 0.01)), fw.SolidProp(fw.Elastic(E=5e4, nu=0.3, rho=100.0)),
+                     [fw.Gravity([0.0, -9.8]), fw.Fixed(list(range(5)))])
+    b = fw.FemDomain(ccw_rectangle(fw, 8, 4, 0.1, 0.05, (0.06, 0.06)),
+                     fw.SolidProp(fw.HyperElastic(E=5e4, nu=0.3, rho=100.0)), [fw.Gravity([0.0, -9.8])],
+                     initials=[fw.InitialVel("ALL", [0.2, 0.0])])
+    doms = [a, b]
+    if disk:
+        c = fw.FemDomain(ccw_disk(fw, 8, 0.02, (0.1, 0.14)), fw.SolidProp(fw.Elastic(E=5e4, nu=0.3, rho=100.0)),
+                         [fw.Gravity([0.0, -9.8])], initials=[fw.InitialVel("ALL", [0.0, -0.5])])
+        doms.append(c)
+    return doms

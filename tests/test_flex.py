@@ -170,3 +170,44 @@ def test_gpu_batched_flex_scenes_equal_alone():
             lp.advanceWithTime(FRAME)
             n = len(b.coords(s))
             assert np.array_equal(b.coords(s), lp.femSpringManager.coords.numpy()[:n]), (frame, s)
+
+
+def test_oracle_tied_pair_holds_the_slabs_together():
+    """ExplicitLoop(ties=[(0, 1)]): the upper slab slides at 0.2 m/s over the
+    cantilever; tied, its bottom face stays on the cantilever's top face
+    (within 2 mm); untied, it slides on by more than 5 mm in the same 3000
+    substeps."""
+    doms = scenes.tied_slabs_scene(fw)
+    n_a, n_b = doms[0].mesh.numNodes, doms[1].mesh.numNodes
+    out = {}
+    for ties in ([(0, 1)], None):
+        o = oracle.OracleLoop(scenes.tied_slabs_scene(fw), 1.25e-5, useAdapativeDT=False, ties=ties)
+        x0, _, _ = o.state()
+        o.advance(3000)
+        x, _, _ = o.state()
+        out[bool(ties)] = (x0, x)
+    x0, x = out[True]
+    a_top = np.arange(4, n_a, 5)  # node i * 5 + 4: the cantilever's top row (ny = 4)
+    b_bot = n_a + np.arange(0, n_b, 5)  # the upper slab's bottom row
+    shift_tied = float(np.abs((x[b_bot, 0] - x0[b_bot, 0]) - (x[a_top[4:13], 0] - x0[a_top[4:13], 0])).max())
+    x0u, xu = out[False]
+    shift_free = float(((xu[b_bot, 0] - x0u[b_bot, 0]) - (xu[a_top[4:13], 0] - x0u[a_top[4:13], 0])).mean())
+    assert shift_tied < 2e-3, shift_tied
+    assert shift_free > 5e-3, shift_free
+
+
+@pytest.mark.gpu
+def test_gpu_tied_pairs_equal_oracle():
+    """Tied pair plus untied FEM-FEM contact in one loop: the GPU gives the
+    oracle's bits every 300 substeps (the ties resolve at the first substep,
+    tie forces come before contact forces on every node)."""
+    lp = fw.ExplicitLoop(1.25e-5, scenes.tied_slabs_scene(fw), useAdapativeDT=False, ties=[(0, 1)])
+    o = oracle.OracleLoop(scenes.tied_slabs_scene(fw), 1.25e-5, useAdapativeDT=False, ties=[(0, 1)])
+    n = o.N
+    for k in range(10):
+        lp.advance_n(300)
+        o.advance(300)
+        xo, vo, _ = o.state()
+        assert np.array_equal(lp.femSpringManager.coords.numpy()[:n].astype(np.float64), xo), k
+        assert np.array_equal(lp.femSpringManager.V.numpy()[:n].astype(np.float64), vo), k
+

@@ -24,7 +24,7 @@ import pytest
 import flatworld_b200 as fw
 import oracle
 from tests import scenes
-from tests.golden.make_golden import CASES, FRAME
+from tests.golden.make_golden import CASES, FRAME, LOOP_KW
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 RTOL = 1e-5
@@ -47,7 +47,8 @@ def rel_linf(a, b):
 def run_oracle(name, precision):
     """Yield (mark, x, v, oracle) at the fixture's snapshots."""
     builder, kw, dt, adaptive, (mode, total, every) = CASES[name]
-    o = oracle.OracleLoop(getattr(scenes, builder)(fw, **kw), dt, useAdapativeDT=adaptive, precision=precision)
+    o = oracle.OracleLoop(getattr(scenes, builder)(fw, **kw), dt, useAdapativeDT=adaptive, precision=precision,
+                          **LOOP_KW.get(name, {}))
     yield 0, None, None, o
     for k in range(1, total + 1):
         if mode == "steps":

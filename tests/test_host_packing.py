@@ -85,14 +85,15 @@ def test_unbatched_second_heightfield_drops_hf_contact():
 
 def test_fem_fem_pairs_are_built():
     """Two contact-enabled FEM domains make one ContactFlexFlex pair (domain1 =
-    the later one); without ground contact the broad phase is skipped; tied
-    FEM-FEM pairs are refused; considerContact=False makes no pair."""
+    the later one); without ground contact the broad phase is skipped; a pair
+    named in ties= is marked tied; considerContact=False makes no pair."""
     a = scenes.two_triangle_square(fw)
     b = scenes.two_triangle_square(fw)
     lay = SceneLayout([a, b])
     assert len(lay.flex) == 1 and lay.flex[0].fem is b and lay.flex[0].ground is a
     assert lay.skip_bvh
-    with pytest.raises(NotImplementedError):
-        fw.ExplicitLoop(0.0, [a, b], ties=[(0, 1)])
+    assert not lay.flex[0].tied
+    assert SceneLayout([a, b], ties=[(0, 1)]).flex[0].tied
+    assert not SceneLayout([a, b], ties=[(0, 2)]).flex[0].tied  # unresolvable entries are ignored
     lay = SceneLayout([fw.FemDomain(a.mesh, a.prop, a.bcs, False), fw.FemDomain(b.mesh, b.prop, b.bcs, False)])
     assert not lay.flex
