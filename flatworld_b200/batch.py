@@ -183,5 +183,16 @@ class BatchedLoop:
         kinetic, strain, external potential, contact penalty."""
         return self._native.energy(len(self.packed.scenes))
 
+    def enable_cfl_monitor(self, on: bool = True):
+        """Per-scene stable time of the current (deformed) shapes, reduced on
+        the GPU in the element step (gather path; see
+        ExplicitLoop.enable_cfl_monitor).  dt is not changed."""
+        self._native.set_cfl_monitor(self.packed.cfl_coefficients() if on else None)
+
+    def currentStableTimes(self, reset: bool = True):
+        """float32[S]: each scene's smallest current-shape stable time since
+        the last reset (+inf for scenes that did not step)."""
+        return self._native.read_cfl(self.S, reset)
+
     def launch_count(self):
         return self._native.launch_count()

@@ -52,6 +52,13 @@ constexpr int kResMaxPairs = 64;
 constexpr long long kSpinLimit = 1ll << 26;
 constexpr long long kPollLimit = 1ll << 22;  // flag-in-data polls (each one an L2 round trip)
 constexpr int kLLMaxBodies = 8;
+// Flag-in-data partial boxes: a ring of kBoxRing substep slots.  CTAs read
+// everyone's partial boxes only when a gate cannot be decided locally, plus
+// once every kBoxSync substeps; that periodic exchange bounds how far apart
+// CTAs can run to kBoxSync substeps, so a ring of 2 * kBoxSync slots is never
+// overwritten before every reader is done with it.
+constexpr int kBoxSync = 64;
+constexpr int kBoxRing = 2 * kBoxSync;
 constexpr int kResTableBytes = 48 * 1024;
 
 struct ResPatch {
@@ -76,12 +83,13 @@ struct Res {
   float2* xpub;             // [2][N] published positions (counter mode)
   int* aabb3;               // [3][B][4] ordered-int body boxes (flag-in-data mode: [B][4] start box)
   unsigned long long* xll;  // [2][N][2] flag-in-data positions (epoch << 32 | float bits)
-  unsigned long long* bll;  // [2][B][P][4] flag-in-data partial boxes (epoch << 32 | ordered int)
+  unsigned long long* bll;  // [kBoxRing][B][P][4] flag-in-data partial boxes (epoch << 32 | ordered int)
   int* bar;                 // arrivals counter (reset by the prologue)
   int* err;                 // != 0: a wait gave up
   long long wait_limit;     // polls before a wait gives up (kPollLimit / kSpinLimit unless set)
   int withhold_cta;         // test hook: this CTA skips its first publish (-1: none)
   float2* rec_x;            // if set: positions at the start of each substep, [nsteps][N] (adjoint recompute)
+  float2* rec_v;            // if set: velocities at the start of each substep, [nsteps][N]
   int* rec_gates;           // if set: broad-phase gates of each substep, [nsteps][rec_stride]
   int rec_stride;
   int P, no_max, nh_max, ne_max, ncsr_max;
@@ -203,6 +211,29 @@ __device__ __forceinline__ void aabb_reset(int* r) {
   r[3] = fw::f2ord(-1e30f);
 }
 
+// Can pair p add a force to any node inside box [lo, hi]?  False only when
+// that is impossible whatever the gate (a margin covers the rounding of the
+// contact arithmetic): the plane's penetration is positive at every corner;
+// the box lies wholly above a height field's gate box (below it when the
+// field is reversed), where the signed distance to the curve is positive; the
+// box misses a voxel grid's cells.  An empty box (no boundary node of the
+// pair's body in this patch) cannot be reached either.
+__device__ __forceinline__ bool pair_reachable(const Pair& p, float lx, float ly, float hx, float hy) {
+  if (!(lx <= hx && ly <= hy)) return !(lx > hx || ly > hy);  // empty box (identity) -> false; NaN -> true
+  if (p.kind == fw::PAIR_PLANE) {
+    const double px = p.f[0], py = p.f[1], nx = p.f[2], ny = p.f[3];
+    const double cx = nx >= 0.0 ? lx : hx, cy = ny >= 0.0 ? ly : hy;  // corner of least penetration
+    const double pen = (cx - px) * nx + (cy - py) * ny;
+    const double mag = 1.0 + fabs((double)lx) + fabs((double)ly) + fabs((double)hx) + fabs((double)hy) +
+                       fabs(px) + fabs(py);
+    return !(pen > 1e-5 * mag);
+  }
+  if (p.kind == fw::PAIR_HEIGHTFIELD) return p.n1 == 1 ? !(hy < p.glo[1]) : !(ly > p.ghi[1]);
+  const double lbx = p.f[0], lby = p.f[1], dx = p.f[2], dz = p.f[3];
+  const double ex = (double)p.n0 * dx * (1.0 + 1e-4), ey = (double)p.n1 * dz * (1.0 + 1e-4);
+  return !(hx < lbx || hy < lby || lx - lbx > ex || ly - lby > ey);
+}
+
 // Update one owned node (shared-memory state) for the current substep.
 __device__ __forceinline__ float2 res_node(const Dev& d, const ResSmem& s, const float* heights,
                                            const int8_t* occ, int i, float dt, float damp) {
@@ -252,6 +283,8 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
   __shared__ int s_abort;
   __shared__ int s_box[LL ? 4 * kLLMaxBodies : 1];   // reduced body boxes (ordered ints)
   __shared__ int s_pbox[LL ? 4 * kLLMaxBodies : 1];  // this CTA's partial boxes
+  __shared__ int s_lbox[LL ? 4 * kLLMaxBodies : 1];  // the same, as of the end of the previous substep
+  __shared__ int s_need;                              // a gate needs everyone's boxes this substep
   ResSmem s;
   res_layout(r, smem_raw, &s);
   const ResPatch P = r.patch[blockIdx.x];
@@ -298,6 +331,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
     const int ident = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
     s_box[t] = ident;
     s_pbox[t] = ident;
+    s_lbox[t] = ident;
   }
   const float* heights = r.tab_h ? s.heights : d.heights;
   const int8_t* occ = r.tab_o ? s.occ : d.occ;
@@ -307,7 +341,10 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
   const bool front = t < FT;
   const int BT = T - FT, bt = t - FT;
   if (r.rec_x)
-    for (int i = t; i < P.no; i += T) r.rec_x[s.gid[i] & 0x7FFFFFFF] = s.x[i];
+    for (int i = t; i < P.no; i += T) {
+      r.rec_x[s.gid[i] & 0x7FFFFFFF] = s.x[i];
+      r.rec_v[s.gid[i] & 0x7FFFFFFF] = s.v[i];
+    }
   if (!front)
     for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
   const int g1_trips = (P.n_g1 + FT - 1) / FT;
@@ -334,28 +371,52 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           }
           s.x[P.no + i] = make_float2(__uint_as_float((uint32_t)wx), __uint_as_float((uint32_t)wy));
         }
-        const unsigned long long* bsrc = r.bll + (size_t)(k & 1) * B * r.P * 4;
-        for (int j = t; j < B * r.P; j += FT) {
-          const unsigned long long* w = bsrc + (size_t)j * 4;
-          unsigned long long b0, b1, b2, b3;
-          long long it = 0;
-          while (true) {
-            b0 = ll_load(w);
-            b1 = ll_load(w + 1);
-            b2 = ll_load(w + 2);
-            b3 = ll_load(w + 3);
-            if (ll_has(b0, want) && ll_has(b1, want) && ll_has(b2, want) && ll_has(b3, want)) break;
-            if ((++it & 1023) == 0 && (it > r.wait_limit || *(volatile int*)r.err)) {
-              atomicExch(r.err, 1);
-              s_abort = 1;
-              break;
-            }
+        // Gates decided from this patch's own boundary nodes where that is
+        // exact: the body box contains the patch's partial box, so a partial
+        // box that meets the ground box proves the gate on (on the 10%-growth
+        // substeps too: growth only enlarges both boxes); and a pair that can
+        // reach none of the patch's nodes changes no force here, on or off.
+        // Otherwise (and every kBoxSync substeps, and while gates are being
+        // recorded) the patch reads every CTA's partial box.
+        if (t == 0) s_need = (k % kBoxSync == 0 || r.rec_gates != nullptr) ? 1 : 0;
+        named_bar(1, FT);
+        if (t < d.P) {
+          const Pair& pr = s.pairs[t];
+          const int* lb = s_lbox + 4 * pr.body;
+          const float lx = fw::ord2f(lb[0]), ly = fw::ord2f(lb[1]), hx = fw::ord2f(lb[2]), hy = fw::ord2f(lb[3]);
+          if (lx <= pr.ghi[0] && hx >= pr.glo[0] && ly <= pr.ghi[1] && hy >= pr.glo[1]) {
+            s.gate[t] = 1;
+          } else if (!pair_reachable(pr, lx, ly, hx, hy)) {
+            s.gate[t] = 0;
+          } else {
+            s_need = 1;
           }
-          int* bx = s_box + 4 * (j / r.P);
-          atomicMin(bx + 0, (int)(uint32_t)b0);
-          atomicMin(bx + 1, (int)(uint32_t)b1);
-          atomicMax(bx + 2, (int)(uint32_t)b2);
-          atomicMax(bx + 3, (int)(uint32_t)b3);
+        }
+        named_bar(1, FT);
+        if (s_need && !s_abort) {
+          const unsigned long long* bsrc = r.bll + (size_t)(k % kBoxRing) * B * r.P * 4;
+          for (int j = t; j < B * r.P; j += FT) {
+            const unsigned long long* w = bsrc + (size_t)j * 4;
+            unsigned long long b0, b1, b2, b3;
+            long long it = 0;
+            while (true) {
+              b0 = ll_load(w);
+              b1 = ll_load(w + 1);
+              b2 = ll_load(w + 2);
+              b3 = ll_load(w + 3);
+              if (ll_has(b0, want) && ll_has(b1, want) && ll_has(b2, want) && ll_has(b3, want)) break;
+              if ((++it & 1023) == 0 && (it > r.wait_limit || *(volatile int*)r.err)) {
+                atomicExch(r.err, 1);
+                s_abort = 1;
+                break;
+              }
+            }
+            int* bx = s_box + 4 * (j / r.P);
+            atomicMin(bx + 0, (int)(uint32_t)b0);
+            atomicMin(bx + 1, (int)(uint32_t)b1);
+            atomicMax(bx + 2, (int)(uint32_t)b2);
+            atomicMax(bx + 3, (int)(uint32_t)b3);
+          }
         }
         named_bar(1, FT);
       } else if (k > 0) {
@@ -378,7 +439,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
         }
       }
       if (!s_abort) {
-        if (t < d.P) {
+        if (t < d.P && (!LL || k == 0 || s_need)) {
           const Pair& pr = s.pairs[t];
           int4 bb;
           if (LL)
@@ -454,8 +515,12 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
       const bool withhold = k == 0 && (int)blockIdx.x == r.withhold_cta;
       if (LL) {
         if (t < 4 * B && !withhold) {  // this CTA's partial box of body t / 4, component t % 4
-          unsigned long long* bdst = r.bll + ((size_t)((k + 1) & 1) * B * r.P + (size_t)(t >> 2) * r.P + blockIdx.x) * 4;
+          unsigned long long* bdst =
+              r.bll + ((size_t)((k + 1) % kBoxRing) * B * r.P + (size_t)(t >> 2) * r.P + blockIdx.x) * 4;
           ll_store(bdst + (t & 3), ll_pack(ep_out, (uint32_t)s_pbox[t]));
+        }
+        if (t < 4 * B) {
+          s_lbox[t] = s_pbox[t];
           s_pbox[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
         }
       } else if (t == 0 && !withhold) {
@@ -467,7 +532,10 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
     }
     __syncthreads();  // every owned node of substep k is updated
     if (r.rec_x && k + 1 < nsteps)  // owned positions stay as they are until the next CTA barrier
-      for (int i = t; i < P.no; i += T) r.rec_x[(size_t)(k + 1) * N + (s.gid[i] & 0x7FFFFFFF)] = s.x[i];
+      for (int i = t; i < P.no; i += T) {
+        r.rec_x[(size_t)(k + 1) * N + (s.gid[i] & 0x7FFFFFFF)] = s.x[i];
+        r.rec_v[(size_t)(k + 1) * N + (s.gid[i] & 0x7FFFFFFF)] = s.v[i];
+      }
     if (!front && k + 1 < nsteps)
       for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
   }
@@ -538,7 +606,8 @@ __device__ __forceinline__ double join64(uint32_t lo, uint32_t hi) {
 }
 
 __global__ void __launch_bounds__(kResThreads, 1)
-k_res_adj(Dev d, Res r, Adj a, const float2* __restrict__ rec_x, const int* __restrict__ rec_gates,
+k_res_adj(Dev d, Res r, Adj a, const float2* __restrict__ rec_x, const float2* __restrict__ rec_v,
+          const int* __restrict__ rec_gates,
           int gate_stride, unsigned long long* fll, int nsteps, float dt, float damp, uint32_t ep0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_abort;
@@ -653,18 +722,14 @@ k_res_adj(Dev d, Res r, Adj a, const float2* __restrict__ rec_x, const int* __re
       const uint32_t w = s.w[i];
       if (w & fw::NODE_BOUNDARY) {
         const int b = (int)(w >> fw::NODE_BODY_SHIFT);
-        const float2 xi = s.x[i];
+        const float2 xi = s.x[i], vi = rec_v[(size_t)j * N + (s.gid[i] & 0x7FFFFFFF)];
+        double2 vb = q.vb[i];
         for (int k = 0; k < s.bpc[b]; ++k) {
           const int p = s.bpo[b] + k;
           if (!rec_gates[(size_t)j * gate_stride + p]) continue;
-          const Pair& pr = s.pairs[p];
-          const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
-          if (pen < 0.0f) {
-            const double tt = -(double)pr.penalty * (pr.f[2] * fb.x + pr.f[3] * fb.y);
-            xb.x += tt * pr.f[2];
-            xb.y += tt * pr.f[3];
-          }
+          fw::contact_vjp(s.pairs[p], d.heights, d.occ, xi, vi, dt, fb, xb, vb);
         }
+        q.vb[i] = vb;
       }
       q.xb[i] = xb;
       if (j > 0) res_adj_prep(s, q, i, h, dmp);
@@ -724,14 +789,14 @@ __global__ void k_res_epilogue(Dev d, Res r, int step0, int nsteps) {
 }
 
 // Flag-in-data variant: the final boxes are the reduction of the partial
-// boxes of the last substep (slot nsteps & 1); the launch has completed, so
-// plain loads see them.
+// boxes of the last substep (ring slot nsteps % kBoxRing); the launch has
+// completed, so plain loads see them.
 __global__ void k_res_epilogue_ll(Dev d, Res r, int step0, int nsteps) {
   __shared__ int box[4 * kLLMaxBodies];
   const int B = d.B, t = threadIdx.x;
   if (t < 4 * B) box[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
   __syncthreads();
-  const unsigned long long* src = r.bll + (size_t)(nsteps & 1) * B * r.P * 4;
+  const unsigned long long* src = r.bll + (size_t)(nsteps % kBoxRing) * B * r.P * 4;
   for (int j = t; j < B * r.P; j += blockDim.x) {
     const unsigned long long* w = src + (size_t)j * 4;
     int* bx = box + 4 * (j / r.P);

@@ -103,6 +103,12 @@ struct Dev {
   Rigid* rig;
   float4* ritem;
   int32_t* bslot;
+  // CFL monitor (cfl_ord == nullptr: off): per scene, the smallest current-
+  // shape stable time 0.4 L / c of its triangles since the last read, as the
+  // int bits of a non-negative float (int order = float order); body_cfl =
+  // 0.4 / sqrt(E / rho) per body (0 for spring domains: not monitored).
+  int32_t* cfl_ord;
+  float* body_cfl;
 };
 
 }  // namespace
@@ -160,7 +166,7 @@ __device__ void step_control(const Dev& d) {
 
 // Loads that depend only on the triangle index are issued before the scene
 // check, so the gather of corner positions does not wait for it.
-__device__ __forceinline__ void element_step(const Dev& d, int e) {
+__device__ __forceinline__ float element_step(const Dev& d, int e) {
   {
     const ElemMat m = d.emat[e];
     const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
@@ -168,7 +174,7 @@ __device__ __forceinline__ void element_step(const Dev& d, int e) {
     const int q0 = d.corner_pos[3 * e], q1 = d.corner_pos[3 * e + 1], q2 = d.corner_pos[3 * e + 2];
     const float2 a = d.x[c0], b = d.x[c1], c = d.x[c2];
     const int s = d.body_scene[fw::elem_body(m.word)];
-    if (!d.scene_active[s]) return;
+    if (!d.scene_active[s]) return __int_as_float(0x7f800000);
     if (fw::elem_type(m.word) == fw::MAT_SPRING) {  // _spring_force_kernel, femspringmanager.py:283-312
       const float2 va = d.v[c0], vb = d.v[c1];
       const float xx = a.x - b.x, xy = a.y - b.y;
@@ -182,7 +188,7 @@ __device__ __forceinline__ void element_step(const Dev& d, int e) {
       fy = fy + dmp * dy;
       d.corner[q0] = make_float2(-fx, -fy);
       d.corner[q1] = make_float2(fx, fy);
-      return;
+      return __int_as_float(0x7f800000);
     }
     float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
     float sy = 0.f, H = 0.f;
@@ -199,7 +205,24 @@ __device__ __forceinline__ void element_step(const Dev& d, int e) {
     d.corner[q0] = f1;
     d.corner[q1] = f2;
     d.corner[q2] = f3;
+    if (!d.cfl_ord) return __int_as_float(0x7f800000);
+    // current-shape stable time: the reference's 0.4 * L_min / sqrt(E / rho)
+    // (femdomain.py:24) on the shortest edge of the deformed triangle
+    const float l0 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y);
+    const float l1 = (b.x - c.x) * (b.x - c.x) + (b.y - c.y) * (b.y - c.y);
+    const float l2 = (c.x - a.x) * (c.x - a.x) + (c.y - a.y) * (c.y - a.y);
+    return sqrtf(fminf(l0, fminf(l1, l2))) * d.body_cfl[fw::elem_body(m.word)];
   }
+}
+
+// Warp-shuffle minimum of the lanes' CFL bounds per scene (lanes of one warp
+// can hold triangles of different scenes), one atomic per scene and warp.
+__device__ __forceinline__ void cfl_reduce(const Dev& d, int e, float dtc) {
+  const unsigned mask = __activemask();
+  const int s = d.body_scene[fw::elem_body(d.emat[e].word)];
+  const unsigned grp = __match_any_sync(mask, s);
+  const int m = (int)__reduce_min_sync(grp, (unsigned)__float_as_int(dtc));
+  if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && m < 0x7f800000) atomicMin(d.cfl_ord + s, m);
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
@@ -207,12 +230,18 @@ __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
   if (d.use_chunks) {
     for (int c = blockIdx.x; c < d.n_e_chunks; c += gridDim.x) {
       const int2 ch = d.e_chunks[c];
-      if ((int)threadIdx.x < ch.y) element_step(d, ch.x + threadIdx.x);
+      if ((int)threadIdx.x < ch.y) {
+        const float dtc = element_step(d, ch.x + threadIdx.x);
+        if (d.cfl_ord) cfl_reduce(d, ch.x + threadIdx.x, dtc);
+      }
     }
     return;
   }
   const int stride = gridDim.x * blockDim.x;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) element_step(d, e);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) {
+    const float dtc = element_step(d, e);
+    if (d.cfl_ord) cfl_reduce(d, e, dtc);
+  }
 }
 
 // This substep's FEM-FEM contact forces on one node, in work-item order (the
@@ -609,6 +638,9 @@ struct Adj {
   double* Eb;    // d loss / d Young's modulus, per element
   float* young;  // Young's modulus per element
   float2* traj;  // recorded positions of the segment, [K][N]
+  float2* trajv;  // recorded velocities of the segment, [K][N] (contact damping terms)
+  float4* trajs;  // recorded J2 state of the segment, [K][E] (worlds with J2 triangles)
+  double* sb;     // adjoint of the J2 state (eps_p Voigt, eqps), 4 per element
   int32_t* gates;  // recorded broad-phase gates, [K][P]
   float2* io_x;  // FP32 staging of xb / vb / Eb for the C ABI
   float2* io_v;
@@ -654,12 +686,46 @@ __global__ void k_adj_prep(Dev d, Adj a, float dt, float damp) {
   if (i < d.N) adj_node_prep(d, a, i, dt, damp);
 }
 
-__global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
+__global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x, const float4* __restrict__ st) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.E) return;
   const ElemMat m = d.emat[e];
   const int c0 = d.conn[3 * e], c1 = d.conn[3 * e + 1], c2 = d.conn[3 * e + 2];
   const double2 b0 = a.fb[c0], b1 = a.fb[c1], b2 = a.fb[c2];
+  if (fw::elem_type(m.word) == fw::MAT_MISES) {
+    // transpose of the local Jacobian, column by column: 6 positions, 4 state, E
+    const float2 p0 = x[c0], p1 = x[c1], p2 = x[c2];
+    const float xs[6] = {p0.x, p0.y, p1.x, p1.y, p2.x, p2.y};
+    const float4 s4 = st[e];
+    const float ss[4] = {s4.x, s4.y, s4.z, s4.w};
+    double ob[10] = {b0.x, b0.y, b1.x, b1.y, b2.x, b2.y, 0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < 4; ++k) ob[6 + k] = a.sb[4 * (size_t)e + k];
+    const float young = a.young[e];
+    const float2 yp = d.j2par[e];
+    float corner[6];
+    double snew[4];
+    double eb = 0.0;
+    for (int col = 0; col < 11; ++col) {
+      fw::Dual X[6], S[4], F[6], SN[4];
+      for (int r = 0; r < 6; ++r) X[r] = fw::dmk(xs[r], col == r ? 1.f : 0.f);
+      for (int k = 0; k < 4; ++k) S[k] = fw::dmk(ss[k], col == 6 + k ? 1.f : 0.f);
+      const fw::Dual lam = fw::dmk(m.lam, col == 10 ? m.lam / young : 0.f);
+      const fw::Dual mu = fw::dmk(m.mu, col == 10 ? m.mu / young : 0.f);
+      fw::element_j2_dual(X, d.jinv[e], lam, mu, yp.x, yp.y, S, m.area, F, SN);
+      double dot = 0.0;
+      for (int r = 0; r < 6; ++r) dot += ob[r] * (double)F[r].d;
+      for (int k = 0; k < 4; ++k) dot += ob[6 + k] * (double)SN[k].d;
+      if (col < 6) corner[col] = (float)dot;
+      else if (col < 10) snew[col - 6] = dot;
+      else eb = dot;
+    }
+    d.corner[d.corner_pos[3 * e]] = make_float2(corner[0], corner[1]);
+    d.corner[d.corner_pos[3 * e + 1]] = make_float2(corner[2], corner[3]);
+    d.corner[d.corner_pos[3 * e + 2]] = make_float2(corner[4], corner[5]);
+    for (int k = 0; k < 4; ++k) a.sb[4 * (size_t)e + k] = snew[k];
+    a.Eb[e] += eb;
+    return;
+  }
   const float2 w0 = make_float2((float)b0.x, (float)b0.y), w1 = make_float2((float)b1.x, (float)b1.y),
                w2 = make_float2((float)b2.x, (float)b2.y);
   fw::Dual f[6];
@@ -674,8 +740,8 @@ __global__ void k_adj_elements(Dev d, Adj a, const float2* __restrict__ x) {
 
 // xb <- xb' + sum of element VJPs + plane-contact VJP; with prep, also the
 // force / velocity adjoints of the previous substep (fused, saves a launch).
-__global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const int32_t* __restrict__ gates,
-                            float dt, float damp, int prep) {
+__global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const float2* __restrict__ v,
+                            const int32_t* __restrict__ gates, float dt, float damp, int prep) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.N) return;
   double2 xb = a.xb[i];
@@ -688,18 +754,14 @@ __global__ void k_adj_nodes(Dev d, Adj a, const float2* __restrict__ x, const in
   const uint32_t w = d.node_word[i];
   if (w & fw::NODE_BOUNDARY) {
     const int b = (int)(w >> fw::NODE_BODY_SHIFT);
-    const float2 xi = x[i];
+    const float2 xi = x[i], vi = v[i];
+    double2 vb = a.vb[i];
     for (int q = 0; q < d.body_pair_cnt[b]; ++q) {
       const int p = d.body_pair_off[b] + q;
       if (!gates[p]) continue;
-      const Pair& pr = d.pairs[p];
-      const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
-      if (pen < 0.0f) {  // c = -k n pen  ->  dc/dx = -k n n^T
-        const double t = -(double)pr.penalty * (pr.f[2] * fb.x + pr.f[3] * fb.y);
-        xb.x += t * pr.f[2];
-        xb.y += t * pr.f[3];
-      }
+      fw::contact_vjp(d.pairs[p], d.heights, d.occ, xi, vi, dt, fb, xb, vb);
     }
+    a.vb[i] = vb;
   }
   a.xb[i] = xb;
   if (prep) adj_node_prep(d, a, i, dt, damp);
@@ -719,6 +781,7 @@ struct Tan {
   float* dE;     // perturbation of Young's modulus per element
   float* young;  // Young's modulus per element
   float2* xs;    // positions at the start of the substep
+  float2* vs;    // velocities at the start of the substep
   float2* io_x;  // FP32 staging for the C ABI
   float2* io_v;
 };
@@ -748,17 +811,11 @@ __global__ void k_tan_nodes(Dev d, Tan t, float dt, float damp) {
   double fx = 0.0, fy = 0.0;
   if (w & fw::NODE_BOUNDARY) {
     const int b = (int)(w >> fw::NODE_BODY_SHIFT);
-    const float2 xi = t.xs[i];
+    const float2 xi = t.xs[i], vi = t.vs[i];
     for (int q = 0; q < d.body_pair_cnt[b]; ++q) {
       const int p = d.body_pair_off[b] + q;
       if (!d.pair_active[p]) continue;
-      const Pair& pr = d.pairs[p];
-      const float pen = (xi.x - pr.f[0]) * pr.f[2] + (xi.y - pr.f[1]) * pr.f[3];
-      if (pen < 0.0f) {
-        const double s = -(double)pr.penalty * (pr.f[2] * dx.x + pr.f[3] * dx.y);
-        fx += s * pr.f[2];
-        fy += s * pr.f[3];
-      }
+      fw::contact_jvp(d.pairs[p], d.heights, d.occ, xi, vi, dt, dx, dv, fx, fy);
     }
   }
   for (int k = d.csr_off[i]; k < d.csr_end[i]; ++k) {
@@ -1040,6 +1097,7 @@ struct fw_ctx {
   struct FlexPair {
     int b1, b2;
     float pen, fric;
+    int tied;
   };
   std::vector<FlexPair> h_flex;
   struct FlexSceneHost {
@@ -1056,6 +1114,8 @@ struct fw_ctx {
   double flex_clock_all = 0.0;     // fw_set_flex_clock before fw_finalize
   double* d_flex_clock = nullptr;
   int* d_flex_err = nullptr;
+  int32_t* cfl_ord_buf = nullptr;  // CFL monitor (fw_set_cfl_monitor)
+  float* cfl_coef_buf = nullptr;
   // spring-mass domains: per body its node mass (0: an FEM body)
   std::vector<float> h_spring_mass;
   bool has_springs = false;
@@ -1610,9 +1670,10 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
       (rc = dalloc(c, &r.err, 1)))
     return rc;
   if (ll) {
-    if ((rc = dalloc(c, &r.xll, 4 * (size_t)N)) || (rc = dalloc(c, &r.bll, 8 * (size_t)c->B * P))) return rc;
+    const size_t nbll = 4 * (size_t)kBoxRing * c->B * P;
+    if ((rc = dalloc(c, &r.xll, 4 * (size_t)N)) || (rc = dalloc(c, &r.bll, nbll))) return rc;
     FW_CUDA(c, cudaMemsetAsync(r.xll, 0, sizeof(unsigned long long) * 4 * (size_t)N, c->stream));
-    FW_CUDA(c, cudaMemsetAsync(r.bll, 0, sizeof(unsigned long long) * 8 * (size_t)c->B * P, c->stream));
+    FW_CUDA(c, cudaMemsetAsync(r.bll, 0, sizeof(unsigned long long) * nbll, c->stream));
   }
   c->res_ll = ll;
   c->res_epoch = 1;
@@ -1641,7 +1702,7 @@ int launch_resident(fw_ctx* c, int n) {
   const bool ll = c->res_ll;
   if (ll && c->res_epoch > 0xF0000000u) {  // epochs about to wrap: clear the words, restart
     FW_CUDA(c, cudaMemsetAsync(c->res.xll, 0, sizeof(unsigned long long) * 4 * (size_t)c->N, c->stream));
-    FW_CUDA(c, cudaMemsetAsync(c->res.bll, 0, sizeof(unsigned long long) * 8 * (size_t)c->B * c->res.P,
+    FW_CUDA(c, cudaMemsetAsync(c->res.bll, 0, sizeof(unsigned long long) * 4 * (size_t)kBoxRing * c->B * c->res.P,
                                c->stream));
     c->res_epoch = 1;
   }
@@ -1960,7 +2021,15 @@ int fw_add_flex_pair(fw_ctx* c, int32_t body1, int32_t body2, float penalty, flo
   if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_add_flex_pair after fw_finalize / on an arena");
   if (body1 < 0 || body2 < 0 || body1 >= c->B || body2 >= c->B || body1 == body2)
     return fail(c, FW_ERR_ARG, "fw_add_flex_pair: bodies %d, %d", body1, body2);
-  c->h_flex.push_back(fw_ctx::FlexPair{body1, body2, penalty, friction});
+  c->h_flex.push_back(fw_ctx::FlexPair{body1, body2, penalty, friction, 0});
+  return FW_OK;
+}
+
+int fw_tie_flex_pair(fw_ctx* c, int32_t pair) {
+  if (!c) return FW_ERR_ARG;
+  if (c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_tie_flex_pair after fw_finalize / on an arena");
+  if (pair < 0 || pair >= (int)c->h_flex.size()) return fail(c, FW_ERR_ARG, "fw_tie_flex_pair: pair %d", pair);
+  c->h_flex[pair].tied = 1;
   return FW_OK;
 }
 
@@ -2188,6 +2257,7 @@ int build_flex(fw_ctx* c) {
   std::vector<int32_t> item_node, item_target, item_pair;
   std::vector<float> item_pen, item_fric;
   std::vector<int2> pair_body;
+  std::vector<int32_t> pair_tied;
   std::vector<int4> segs;  // (first item, count, pair in its scene, target)
   std::vector<FlexScene> scs;
   std::vector<int32_t> dom_obj, dom_body;
@@ -2232,6 +2302,8 @@ int build_flex(fw_ctx* c) {
     for (int lp = 0; lp < fsd.n_pairs; ++lp) {
       const fw_ctx::FlexPair& fp = c->h_flex[kv.second[lp]];
       pair_body.push_back(make_int2(fp.b1, fp.b2));
+      pair_tied.push_back(fp.tied);
+      (fp.tied ? fsd.n_tied : fsd.n_untied) += c->h_bncnt[fp.b1] + c->h_bncnt[fp.b2];
       for (int side = 0; side < 2; ++side) {
         const int src = side == 0 ? fp.b2 : fp.b1, dst = side == 0 ? fp.b1 : fp.b2;
         segs.push_back(make_int4((int)item_node.size(), c->h_bncnt[src], lp, dst));
@@ -2277,6 +2349,8 @@ int build_flex(fw_ctx* c) {
           *ebase = nullptr, *ccount = nullptr, *cstart = nullptr, *cend = nullptr, *cursor = nullptr,
           *sorted = nullptr, *dslot = nullptr, *dcnt = nullptr, *ditem = nullptr, *dsegoff = nullptr;
   float *ipen = nullptr, *ifric = nullptr;
+  int32_t *ptied = nullptr, *telem = nullptr;
+  float *tw0 = nullptr, *tw1 = nullptr, *tgap = nullptr;
   int2 *pbody = nullptr, *dbe = nullptr, *crange = nullptr, *ecell = nullptr, *scell = nullptr;
   int4 *srec = nullptr, *dseg = nullptr;
   float4 *dbox = nullptr, *ebox = nullptr;
@@ -2299,7 +2373,9 @@ int build_flex(fw_ctx* c) {
       (rc = upload(c, &dslot, slot)) || (rc = dalloc(c, &dcnt, std::max(1, n_slots))) ||
       (rc = dalloc(c, &ditem, std::max(1, n_slots) * kFlexListCap)) ||
       (rc = dalloc(c, &dforce, std::max(1, n_slots) * kFlexListCap)) || (rc = dalloc(c, &c->d_flex_clock, n_fs)) ||
-      (rc = dalloc(c, &c->d_flex_err, 1)))
+      (rc = dalloc(c, &c->d_flex_err, 1)) || (rc = upload(c, &ptied, pair_tied)) ||
+      (rc = upload(c, &telem, minus1)) || (rc = dalloc(c, &tw0, std::max(n_items, 1))) ||
+      (rc = dalloc(c, &tw1, std::max(n_items, 1))) || (rc = dalloc(c, &tgap, std::max(n_items, 1))))
     return rc;
   FW_CUDA(c, cudaMemsetAsync(grid, 0, sizeof(FlexGrid) * n_fs, c->stream));
   FW_CUDA(c, cudaMemsetAsync(c->d_flex_err, 0, sizeof(int), c->stream));
@@ -2316,6 +2392,7 @@ int build_flex(fw_ctx* c) {
   f.srec = srec; f.scell = scell;
   f.seg = dseg; f.seg_off = dsegoff;
   f.sc = dsc; f.clock_dt = c->d_flex_clock; f.err = c->d_flex_err;
+  f.pair_tied = ptied; f.tie_elem = telem; f.tie_w0 = tw0; f.tie_w1 = tw1; f.tie_gap = tgap;
   c->flex_pre_smem = sizeof(float4) * (size_t)max_dom_fem;
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
@@ -3018,9 +3095,6 @@ int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
   if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)
     return fail(c, FW_ERR_STATE, "the adjoint needs a finalized single-scene world on the gather or resident path");
   if (max_segment_steps <= 0) return fail(c, FW_ERR_ARG, "max_segment_steps must be > 0");
-  if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the adjoint covers Elastic and NeoHookean triangles (no J2)");
-  for (const Pair& p : c->h_pairs)
-    if (p.kind != fw::PAIR_PLANE) return fail(c, FW_ERR_ARG, "the adjoint covers plane contact only");
   int rc;
   Adj& a = c->adj;
   if (!a.young) {
@@ -3035,12 +3109,19 @@ int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
   if (c->adj_cap < max_segment_steps) {
     drop_graphs(c);  // graphs hold the old trajectory buffers
     if ((rc = dalloc(c, &a.traj, (size_t)max_segment_steps * c->N)) ||
+        (rc = dalloc(c, &a.trajv, (size_t)max_segment_steps * c->N)) ||
+        (rc = dalloc(c, &a.trajs, (size_t)max_segment_steps * (c->d.has_j2 ? c->E : 1))) ||
         (rc = dalloc(c, &a.gates, (size_t)max_segment_steps * std::max(1, c->d.P))))
       return rc;
     c->adj_cap = max_segment_steps;
   }
-  // Resident reverse pass when the world runs resident and the adjoint state fits on chip too.
-  if (c->path == FW_PATH_RESIDENT && !c->res_adj) {
+  if (c->d.has_j2 && !a.sb) {
+    if ((rc = dalloc(c, &a.sb, 4 * (size_t)c->E))) return rc;
+  }
+  if (a.sb) FW_CUDA(c, cudaMemsetAsync(a.sb, 0, sizeof(double) * 4 * (size_t)c->E, c->stream));
+  // Resident reverse pass when the world runs resident and the adjoint state
+  // fits on chip too (J2 worlds reverse on the gather kernels).
+  if (c->path == FW_PATH_RESIDENT && !c->res_adj && !c->d.has_j2) {
     int optin = 0, sms = 148;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -3075,6 +3156,7 @@ int fw_adj_seed(fw_ctx* c, const float* xbar, const float* vbar, int32_t on_devi
   k_adj_seed<<<(c->N + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->adj, c->N, xbar != nullptr, vbar != nullptr);
   c->launches += 1;
   FW_CUDA(c, cudaMemsetAsync(c->adj.Eb, 0, sizeof(double) * c->E, c->stream));
+  if (c->adj.sb) FW_CUDA(c, cudaMemsetAsync(c->adj.sb, 0, sizeof(double) * 4 * (size_t)c->E, c->stream));
   return check_kernel(c, "adjoint seed");
 }
 
@@ -3090,16 +3172,18 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
   if (c->res_adj) {
     // recompute on the resident step, recording positions and gates, then the resident reverse
     c->res.rec_x = a.traj;
+    c->res.rec_v = a.trajv;
     c->res.rec_gates = a.gates;
     c->res.rec_stride = P;
     rc = launch_resident(c, n_steps);
     c->res.rec_x = nullptr;
+    c->res.rec_v = nullptr;
     c->res.rec_gates = nullptr;
     if (rc) return rc;
     if (c->res_epoch > 0xF0000000u) {
       FW_CUDA(c, cudaMemsetAsync(c->fll, 0, sizeof(unsigned long long) * 8 * (size_t)N, c->stream));
       FW_CUDA(c, cudaMemsetAsync(c->res.xll, 0, sizeof(unsigned long long) * 4 * (size_t)N, c->stream));
-      FW_CUDA(c, cudaMemsetAsync(c->res.bll, 0, sizeof(unsigned long long) * 8 * (size_t)c->B * c->res.P,
+      FW_CUDA(c, cudaMemsetAsync(c->res.bll, 0, sizeof(unsigned long long) * 4 * (size_t)kBoxRing * c->B * c->res.P,
                                  c->stream));
       c->res_epoch = 1;
     }
@@ -3108,8 +3192,9 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
     float damp_f = c->h_damp.empty() ? 0.0f : c->h_damp[0];
     int nn = n_steps, gs = P;
     const float2* tx = a.traj;
+    const float2* tv = a.trajv;
     const int* tg = a.gates;
-    void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&c->adj, (void*)&tx, (void*)&tg, (void*)&gs,
+    void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&c->adj, (void*)&tx, (void*)&tv, (void*)&tg, (void*)&gs,
                     (void*)&c->fll, (void*)&nn, (void*)&dt, (void*)&damp_f, (void*)&ep0};
     FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)k_res_adj, dim3(c->res.P), dim3(kResThreads), args,
                                            c->res_adj_smem, c->stream));
@@ -3122,6 +3207,10 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
   rc = cached_graph(c, c->adj_graphs, (1ull << 62) | key_lo, [&] {
     for (int j = 0; j < n_steps; ++j) {
       cudaMemcpyAsync(a.traj + (size_t)j * N, c->d.x, sizeof(float2) * N, cudaMemcpyDeviceToDevice, c->stream);
+      cudaMemcpyAsync(a.trajv + (size_t)j * N, c->d.v, sizeof(float2) * N, cudaMemcpyDeviceToDevice, c->stream);
+      if (c->d.has_j2)
+        cudaMemcpyAsync(a.trajs + (size_t)j * E, c->d.j2state, sizeof(float4) * E, cudaMemcpyDeviceToDevice,
+                        c->stream);
       k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
       k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
       if (c->d.P > 0)
@@ -3142,8 +3231,9 @@ int fw_adj_segment(fw_ctx* c, int32_t n_steps, float dt) {
     k_adj_prep<<<gn, kBlock, 0, c->stream>>>(c->d, a, dt, damp);  // force / velocity adjoints of the last substep
     for (int j = n_steps - 1; j >= 0; --j) {
       const float2* x = a.traj + (size_t)j * N;
-      k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x);
-      k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, a.gates + (size_t)j * P, dt, damp, j > 0);
+      const float2* v = a.trajv + (size_t)j * N;
+      k_adj_elements<<<ge, kBlock, 0, c->stream>>>(c->d, a, x, a.trajs + (c->d.has_j2 ? (size_t)j * E : 0));
+      k_adj_nodes<<<gn, kBlock, 0, c->stream>>>(c->d, a, x, v, a.gates + (size_t)j * P, dt, damp, j > 0);
     }
   }, &g_rev);
   if (rc) return rc;
@@ -3173,15 +3263,14 @@ int fw_tan_begin(fw_ctx* c, const float* dx0, const float* dv0, const float* dE,
   if (!c->finalized || c->arena || c->S != 1 || c->path == FW_PATH_STREAM)
     return fail(c, FW_ERR_STATE, "the tangent needs a finalized single-scene world on the gather or resident path");
   if (c->d.has_j2) return fail(c, FW_ERR_ARG, "the tangent covers Elastic and NeoHookean triangles (no J2)");
-  for (const Pair& p : c->h_pairs)
-    if (p.kind != fw::PAIR_PLANE) return fail(c, FW_ERR_ARG, "the tangent covers plane contact only");
   Tan& t = c->tan;
   int rc;
   if (!c->adj.young && (rc = upload(c, &c->adj.young, c->h_E))) return rc;
   t.young = c->adj.young;
   if (!t.dx) {
     if ((rc = dalloc(c, &t.dx, c->N)) || (rc = dalloc(c, &t.dv, c->N)) || (rc = dalloc(c, &t.dE, c->E)) ||
-        (rc = dalloc(c, &t.xs, c->N)) || (rc = dalloc(c, &t.io_x, c->N)) || (rc = dalloc(c, &t.io_v, c->N)))
+        (rc = dalloc(c, &t.xs, c->N)) || (rc = dalloc(c, &t.vs, c->N)) || (rc = dalloc(c, &t.io_x, c->N)) ||
+        (rc = dalloc(c, &t.io_v, c->N)))
       return rc;
   }
   const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -3206,6 +3295,7 @@ int fw_tan_step(fw_ctx* c, int32_t n_steps, float dt) {
   int rc;
   for (int j = 0; j < n_steps; ++j) {
     FW_CUDA(c, cudaMemcpyAsync(t.xs, c->d.x, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    FW_CUDA(c, cudaMemcpyAsync(t.vs, c->d.v, sizeof(float2) * c->N, cudaMemcpyDeviceToDevice, c->stream));
     if ((rc = launch_step(c))) return rc;  // the substep itself (sets this substep's gates)
     c->host_counter += 1;
     k_tan_elements<<<ge, kBlock, 0, c->stream>>>(c->d, t);
@@ -3444,6 +3534,48 @@ int fw_clear_scene_status(fw_ctx* c, int32_t scene) {
   if (scene < -1 || scene >= c->S) return fail(c, FW_ERR_ARG, "scene %d out of range", scene);
   if (scene < 0) FW_CUDA(c, cudaMemsetAsync(c->d.scene_bad, 0, sizeof(int32_t) * c->S, c->stream));
   else FW_CUDA(c, cudaMemsetAsync(c->d.scene_bad + scene, 0, sizeof(int32_t), c->stream));
+  return FW_OK;
+}
+
+int fw_set_cfl_monitor(fw_ctx* c, const float* coef_per_body) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_set_cfl_monitor before fw_finalize");
+  if (coef_per_body && c->path != FW_PATH_GATHER)
+    return fail(c, FW_ERR_STATE, "the CFL monitor runs on the gather step (create the world with FW_PATH_GATHER)");
+  int rc;
+  drop_graphs(c);  // captured graphs hold the previous monitor pointers
+  if (!coef_per_body) {
+    c->d.cfl_ord = nullptr;
+    return FW_OK;
+  }
+  if (!c->cfl_ord_buf) {
+    if ((rc = dalloc(c, &c->cfl_ord_buf, (size_t)c->S)) || (rc = dalloc(c, &c->cfl_coef_buf, (size_t)c->B)))
+      return rc;
+  }
+  FW_CUDA(c, cudaMemcpyAsync(c->cfl_coef_buf, coef_per_body, sizeof(float) * c->B, cudaMemcpyHostToDevice, c->stream));
+  std::vector<int32_t> inf(c->S, 0x7f800000);
+  FW_CUDA(c, cudaMemcpyAsync(c->cfl_ord_buf, inf.data(), sizeof(int32_t) * c->S, cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->d.cfl_ord = c->cfl_ord_buf;
+  c->d.body_cfl = c->cfl_coef_buf;
+  return FW_OK;
+}
+
+int fw_read_cfl(fw_ctx* c, float* out, int32_t reset) {
+  if (!c || !out) return FW_ERR_ARG;
+  if (!c->d.cfl_ord) return fail(c, FW_ERR_STATE, "fw_read_cfl: the CFL monitor is off");
+  std::vector<int32_t> v(c->S);
+  FW_CUDA(c, cudaMemcpyAsync(v.data(), c->d.cfl_ord, sizeof(int32_t) * c->S, cudaMemcpyDeviceToHost, c->stream));
+  if (reset) {
+    std::vector<int32_t> inf(c->S, 0x7f800000);
+    FW_CUDA(c, cudaMemcpyAsync(c->d.cfl_ord, inf.data(), sizeof(int32_t) * c->S, cudaMemcpyHostToDevice, c->stream));
+  }
+  FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < c->S; ++s) {
+    float f;
+    std::memcpy(&f, &v[s], sizeof(float));
+    out[s] = f;
+  }
   return FW_OK;
 }
 

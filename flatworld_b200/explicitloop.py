@@ -367,3 +367,16 @@ class ExplicitLoop:
 
     def launch_count(self) -> int:
         return self._native.launch_count()
+
+    def enable_cfl_monitor(self, on: bool = True):
+        """Report the stable time of the current (deformed) mesh: the element
+        step also evaluates the reference's 0.4 * L_min / sqrt(E / rho)
+        (femdomain.py:24) on every triangle's current shortest edge, reduced
+        per scene on the GPU.  dt is not changed (the reference fixes it from
+        the rest shape).  Needs the gather step (``path="gather"``)."""
+        self._native.set_cfl_monitor(self._packed.cfl_coefficients() if on else None)
+
+    def currentStableTime(self, reset: bool = True) -> float:
+        """Smallest current-shape stable time of the loop's triangles over the
+        substeps since the last reset (+inf before any substep)."""
+        return float(self._native.read_cfl(1, reset)[0])

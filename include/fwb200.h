@@ -148,6 +148,15 @@ int fw_set_boundary_edges(fw_ctx* ctx, int32_t n_edges, const int32_t* edges, co
 int fw_set_flex_scene(fw_ctx* ctx, int32_t scene, int32_t skip_bvh, int32_t n_domains, const int32_t* dom_obj,
                       const int32_t* dom_body, const float* dom_box);
 int fw_add_flex_pair(fw_ctx* ctx, int32_t body1, int32_t body2, float penalty, float friction);
+/* Mark FEM-FEM pair `pair` (creation order of fw_add_flex_pair) tied, as
+ * ExplicitLoop(ties=[(i, j)]) marks the contact of domains i and j
+ * (flatworld/explicitloop.py:265-270, 400-439).  A tied pair's work items do
+ * not run the contact search; at the scene's first substep each finds the
+ * nearest boundary edge of the other body and from then on a penalty spring
+ * holds its node at that point of the edge, with the reactions on the edge's
+ * nodes (flatworld/mixedcontact.py:686-809, launched before the contact
+ * kernel, mixedcontact.py:1680-1690).  Before fw_finalize. */
+int fw_tie_flex_pair(fw_ctx* ctx, int32_t pair);
 int fw_set_flex_clock(fw_ctx* ctx, double dt);
 /* The same per scene (dt[scene], one entry per scene of the world; scenes
  * without FEM-FEM contact are ignored), for worlds whose scenes step with their
@@ -357,6 +366,20 @@ int fw_read_counters(fw_ctx* ctx, int64_t* counters);
  * only on buffer overflow, femspringmanager.py:708-730). */
 int fw_scene_status(fw_ctx* ctx, int32_t* bad, int32_t async);
 int fw_clear_scene_status(fw_ctx* ctx, int32_t scene);
+
+/* CFL monitor: the stable time of the current (deformed) shape, reported
+ * without changing dt.  The reference fixes dt once from the rest shape
+ * (explicitloop.py:160-166, femdomain.py:24: 0.4 * L_min / sqrt(E / rho));
+ * with the monitor on, the element kernel also evaluates that bound on every
+ * triangle's current shortest edge and reduces it per scene (warp shuffles,
+ * one atomic per warp and scene), so a caller can see a body's bound shrink
+ * as it compresses.  fw_set_cfl_monitor(ctx, coef): coef[b] = 0.4 /
+ * sqrt(E / rho) for body b (0 for spring domains); NULL turns it off.  Gather
+ * step only (FW_PATH_GATHER).  fw_read_cfl(ctx, out, reset): out[s] = the
+ * smallest bound of scene s over the substeps since the last reset (+inf if
+ * none); reset = 1 starts a new window.  No reference counterpart. */
+int fw_set_cfl_monitor(fw_ctx* ctx, const float* coef_per_body);
+int fw_read_cfl(fw_ctx* ctx, float* out, int32_t reset);
 
 /* Total energy per scene, reduced in FP64 on the device (deterministic order):
  * out[4 s + 0..3] = kinetic, strain, external potential (gravity -m g.x or

@@ -194,3 +194,67 @@ def test_torch_autograd_function():
     eb, vb, _ = sim.backward(2.0 * x.detach().cpu().numpy())
     assert np.allclose(E.grad.cpu().numpy(), eb) and np.allclose(v0.grad.cpu().numpy(), vb)
     assert torch.isfinite(E.grad).all() and E.grad.abs().sum() > 0
+
+
+@pytest.mark.parametrize("kind", ["plane", "heightfield", "voxel", "j2"])
+def test_gpu_adjoint_against_fp64_oracle_adjoint(kind):
+    """The CUDA adjoint (FP32 trajectory) against the oracle's FP64 adjoint
+    (FP64 trajectory; itself equal to FP64 central differences to 1e-6,
+    tests/test_oracle_adjoint.py) on a 12 x 12 block landing on a plane, a
+    height field and a voxel floor (contact with its velocity damping), and a
+    J2 block that yields on the plane (plastic state carried backward), for
+    L = <w, x_T> over 400 substeps.  What separates them is the FP32
+    trajectory's rounding; the tolerance is stated on the L2 norm of dL/dE and
+    dL/dv0."""
+    from tests.test_oracle_adjoint import DT, STEPS, block
+
+    build = block(kind)
+    doms = build()
+    sim = DiffSim(doms, DT, STEPS, checkpoint_every=50, path="gather")
+    o = oracle.OracleLoop(build(), DT, useAdapativeDT=False, precision="f64")
+    _, v0, _ = o.state()
+    w = np.random.default_rng(7).standard_normal((sim.N, 2))
+    _, vb64, eb64 = o.adjoint(STEPS, xbar=w)
+    sim.forward(sim.E0, v0.astype(np.float32))
+    eb, vb, _ = sim.backward(w)
+    e_err = float(np.linalg.norm(eb - eb64) / np.linalg.norm(eb64))
+    v_err = float(np.linalg.norm(vb - vb64) / np.linalg.norm(vb64))
+    print(f"{kind}: CUDA adjoint vs FP64 adjoint: dL/dE {e_err:.2e}, dL/dv0 {v_err:.2e} (relative L2)")
+    assert e_err < 1e-2 and v_err < 1e-2, (e_err, v_err)
+
+
+@pytest.mark.parametrize("kind", ["heightfield", "voxel"])
+def test_adjoint_is_the_transpose_of_the_tangent_with_ground_contact(kind):
+    """Dot-product test with height-field and voxel contact (penetration and
+    velocity-damping terms), with loop damping, on one FP32 trajectory."""
+    from tests.test_oracle_adjoint import DT, STEPS, block
+
+    sim = DiffSim(block(kind)(), DT, STEPS, checkpoint_every=50, damping=0.02)
+    rng = np.random.default_rng(31)
+    v0 = np.tile(np.array([0.3, -1.0], np.float32), (sim.N, 1))
+    w = rng.standard_normal((sim.N, 2))
+    sim.forward(sim.E0, v0)
+    eb, vb, _ = sim.backward(w)
+    for what in ("E", "v"):
+        dE = (sim.E0 * rng.standard_normal(sim.E)).astype(np.float32) if what == "E" else np.zeros(sim.E, np.float32)
+        dv = rng.standard_normal((sim.N, 2)).astype(np.float32) if what == "v" else np.zeros((sim.N, 2), np.float32)
+        _, dx = sim.jvp(sim.E0, v0, dE, dv)
+        tangent = float(np.sum(w * dx.astype(np.float64)))
+        a = float(np.dot(eb.astype(np.float64), dE)) + float(np.sum(vb.astype(np.float64) * dv))
+        err = abs(tangent - a) / max(abs(a), 1e-30)
+        print(f"dot-product test ({kind}, {what}): tangent {tangent:.9e} adjoint {a:.9e} rel {err:.2e}")
+        assert err < 1e-5, (kind, what, tangent, a)
+
+
+@pytest.mark.parametrize("kind", ["heightfield", "voxel"])
+def test_resident_reverse_equals_gather_reverse_with_ground_contact(kind):
+    from tests.test_oracle_adjoint import DT, STEPS, block
+
+    a = DiffSim(block(kind)(), DT, STEPS, checkpoint_every=50, damping=0.03)
+    b = DiffSim(block(kind)(), DT, STEPS, checkpoint_every=50, damping=0.03, path="gather")
+    assert a.native.get_path()[0] == 2 and b.native.get_path()[0] == 1
+    v0 = np.tile(np.array([0.3, -1.0], np.float32), (a.N, 1))
+    w = np.random.default_rng(4).standard_normal((a.N, 2)).astype(np.float32)
+    assert np.array_equal(a.forward(a.E0, v0), b.forward(b.E0, v0))
+    for u, v in zip(a.backward(w), b.backward(w)):
+        assert np.array_equal(u, v)
