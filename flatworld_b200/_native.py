@@ -56,6 +56,7 @@ _SIGNATURES = {
     "fw_set_flex_scene": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f32p]),
     "fw_add_flex_pair": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_float, C.c_float]),
     "fw_tie_flex_pair": (C.c_int, [_vp, C.c_int32]),
+    "fw_set_damping": (C.c_int, [_vp, C.c_int32, C.c_float]),
     "fw_set_flex_clock": (C.c_int, [_vp, C.c_double]),
     "fw_set_flex_clocks": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "fw_mass_scaling": (C.c_int, [_vp, C.c_float]),
@@ -228,6 +229,9 @@ class NativeWorld:
     def add_flex_pair(self, body1, body2, penalty, friction):
         self._check(self._L.fw_add_flex_pair(self._h, int(body1), int(body2), float(penalty), float(friction)),
                     "fw_add_flex_pair")
+
+    def set_damping(self, scene, damping):
+        self._check(self._L.fw_set_damping(self._h, int(scene), float(damping)), "fw_set_damping")
 
     def tie_flex_pair(self, pair):
         self._check(self._L.fw_tie_flex_pair(self._h, int(pair)), "fw_tie_flex_pair")

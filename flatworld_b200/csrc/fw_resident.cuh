@@ -354,6 +354,28 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
       // previous substep complete everywhere -> halo positions, body boxes
       if (k > 0 && LL) {
         const uint32_t want = ep0 + (uint32_t)k;
+        // Gates decided from this patch's own boundary nodes where that is
+        // exact (s_lbox: its partial boxes at the end of the previous
+        // substep): the body box contains the partial box, so a partial box
+        // that meets the ground box proves the gate on (on the 10%-growth
+        // substeps too: growth only enlarges both boxes); and a pair that can
+        // reach none of the patch's nodes changes no force here, on or off.
+        // Otherwise (and every kBoxSync substeps, and while gates are being
+        // recorded: s_need preset at the end of the previous substep) the
+        // patch reads every CTA's partial box.  Decided before the halo poll,
+        // which they do not depend on.
+        if (t < d.P) {
+          const Pair& pr = s.pairs[t];
+          const int* lb = s_lbox + 4 * pr.body;
+          const float lx = fw::ord2f(lb[0]), ly = fw::ord2f(lb[1]), hx = fw::ord2f(lb[2]), hy = fw::ord2f(lb[3]);
+          if (lx <= pr.ghi[0] && hx >= pr.glo[0] && ly <= pr.ghi[1] && hy >= pr.glo[1]) {
+            s.gate[t] = 1;
+          } else if (!pair_reachable(pr, lx, ly, hx, hy)) {
+            s.gate[t] = 0;
+          } else {
+            s_need = 1;
+          }
+        }
         const unsigned long long* src = r.xll + (size_t)(k & 1) * N * 2;
         for (int i = t; i < P.nh; i += FT) {
           const unsigned long long* w = src + 2 * (size_t)s.hidx[i];
@@ -371,28 +393,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           }
           s.x[P.no + i] = make_float2(__uint_as_float((uint32_t)wx), __uint_as_float((uint32_t)wy));
         }
-        // Gates decided from this patch's own boundary nodes where that is
-        // exact: the body box contains the patch's partial box, so a partial
-        // box that meets the ground box proves the gate on (on the 10%-growth
-        // substeps too: growth only enlarges both boxes); and a pair that can
-        // reach none of the patch's nodes changes no force here, on or off.
-        // Otherwise (and every kBoxSync substeps, and while gates are being
-        // recorded) the patch reads every CTA's partial box.
-        if (t == 0) s_need = (k % kBoxSync == 0 || r.rec_gates != nullptr) ? 1 : 0;
-        named_bar(1, FT);
-        if (t < d.P) {
-          const Pair& pr = s.pairs[t];
-          const int* lb = s_lbox + 4 * pr.body;
-          const float lx = fw::ord2f(lb[0]), ly = fw::ord2f(lb[1]), hx = fw::ord2f(lb[2]), hy = fw::ord2f(lb[3]);
-          if (lx <= pr.ghi[0] && hx >= pr.glo[0] && ly <= pr.ghi[1] && hy >= pr.glo[1]) {
-            s.gate[t] = 1;
-          } else if (!pair_reachable(pr, lx, ly, hx, hy)) {
-            s.gate[t] = 0;
-          } else {
-            s_need = 1;
-          }
-        }
-        named_bar(1, FT);
+        named_bar(1, FT);  // halo positions, local gates and s_need are final
         if (s_need && !s_abort) {
           const unsigned long long* bsrc = r.bll + (size_t)(k % kBoxRing) * B * r.P * 4;
           for (int j = t; j < B * r.P; j += FT) {
@@ -417,8 +418,8 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
             atomicMax(bx + 2, (int)(uint32_t)b2);
             atomicMax(bx + 3, (int)(uint32_t)b3);
           }
+          named_bar(1, FT);
         }
-        named_bar(1, FT);
       } else if (k > 0) {
         if (t == 0) {
           long long it = 0;
@@ -438,8 +439,9 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           for (int i = t; i < P.nh; i += FT) s.x[P.no + i] = __ldcg(src + s.hidx[i]);
         }
       }
+      const bool exact_gates = !LL || k == 0 || s_need;  // else decided locally above
       if (!s_abort) {
-        if (t < d.P && (!LL || k == 0 || s_need)) {
+        if (t < d.P && exact_gates) {
           const Pair& pr = s.pairs[t];
           int4 bb;
           if (LL)
@@ -453,8 +455,10 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
         }
         if (!LL && blockIdx.x == 0)
           for (int b = t; b < B; b += FT) aabb_reset(r.aabb3 + ((size_t)((g + 2) % 3) * B + b) * 4);
-        named_bar(1, FT);
-        if (LL && t < 4 * B) s_box[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
+        if (exact_gates) {
+          named_bar(1, FT);
+          if (LL && t < 4 * B) s_box[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
+        }
         for (int q = P.n_int + t; q < P.ne; q += FT) res_element(s, q);
       }
     }
@@ -523,6 +527,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           s_lbox[t] = s_pbox[t];
           s_pbox[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
         }
+        if (t == 0) s_need = ((k + 1) % kBoxSync == 0 || r.rec_gates != nullptr) ? 1 : 0;
       } else if (t == 0 && !withhold) {
         cuda::atomic_ref<int, cuda::thread_scope_device> a(*r.bar);
         a.fetch_add(1, cuda::memory_order_release);

@@ -1917,6 +1917,17 @@ int fw_set_scenes(fw_ctx* c, int32_t ns, const float* damping) {
   return FW_OK;
 }
 
+int fw_set_damping(fw_ctx* c, int32_t scene, float damping) {
+  if (!c) return FW_ERR_ARG;
+  if (!c->finalized || c->arena) return fail(c, FW_ERR_STATE, "fw_set_damping needs a finalized world (not an arena)");
+  if (scene < 0 || scene >= c->S) return fail(c, FW_ERR_ARG, "fw_set_damping: scene %d out of range", scene);
+  c->h_damp[scene] = damping;
+  // pageable source: the copy is staged before the call returns
+  FW_CUDA(c, cudaMemcpyAsync(c->d.scene_damp + scene, &c->h_damp[scene], sizeof(float), cudaMemcpyHostToDevice,
+                             c->stream));
+  return FW_OK;
+}
+
 static int add_pair(fw_ctx* c, Pair p, const float* lo, const float* hi) {
   if (!c) return FW_ERR_ARG;
   if (c->finalized && !c->arena) return fail(c, FW_ERR_STATE, "contact pair added after fw_finalize");

@@ -287,6 +287,20 @@ class ExplicitLoop:
                 if d.type in (DomainType.RIGID, DomainType.ANALYTICAL):  # height fields / voxel grids keep no state
                     d.attach(self, k)
 
+    @property
+    def damping(self) -> float:
+        return self._damping
+
+    @damping.setter
+    def damping(self, value):
+        """The reference reads ``self.damping`` at every substep
+        (explicitloop.py:528, 537): a new value applies from the next substep,
+        to the FEM update and to the rigid update."""
+        self._damping = float(value)
+        if getattr(self, "_native", None) is not None:
+            self._native.set_damping(0, float(np.float32(self._damping)))
+            self._rigid_clock = None  # the rigid schedule carries damping: re-sent at the next substep
+
     def _clock(self, dt: float):
         """Hand the substep's float64 dt to the FEM-FEM hash-refresh clock
         (femspringmanager.py:1035-1039 accumulates ``self.dt`` in float64) and

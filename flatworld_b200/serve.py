@@ -62,10 +62,14 @@ class Arena:
 
     def insert(self, domains, dt=0.0, useAdapativeDT=False, damping=0.0) -> int:
         layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT)
+        return self.insert_prepared(layout, PackedWorld([layout]))
+
+    def insert_prepared(self, layout: SceneLayout, packed: PackedWorld) -> int:
+        """Upload a scene whose host-side layout and packing are already built."""
         if layout.entries:
             raise NotImplementedError("rigid bodies and ground planes with BCs run in an ExplicitLoop or "
                                       "BatchedLoop, not in served worlds")
-        stage(self.native, PackedWorld([layout]))
+        stage(self.native, packed)
         s = self.native.arena_commit()
         self.layouts[s] = layout
         return s
@@ -191,20 +195,52 @@ class Server:
         self.admit_s = 0.0        # host time spent admitting new bodies
         self.last_admit_t = 0.0   # run clock of the last admission
         self.evicted = 0          # bodies removed because their state turned non-finite
+        self._prep = {}           # body -> (layout, packed, device bytes), built off the loop thread
+        self._prep_queue = None   # bodies waiting for the preparing thread (during run)
+        self._prep_wanted = set()
+
+    def _build(self, body):
+        """Host-side preparation of a body: its domains, scene layout, packed
+        arrays and device footprint (everything but the upload)."""
+        layout = SceneLayout(self.make_body(body))
+        return layout, PackedWorld([layout]), scene_device_bytes(layout)
+
+    def prepare(self, bodies):
+        """Build the host-side layouts of these bodies ahead of their first
+        request (a catalog load); their admission is then an upload only."""
+        for b in bodies:
+            if b not in self._prep:
+                self._prep[b] = self._build(b)
+
+    def _prep_worker(self):
+        while True:
+            b = self._prep_queue.get()
+            if b is None:
+                return
+            if b not in self._prep:
+                self._prep[b] = self._build(b)
 
     def _admit(self, body, t0=None):
         """True if resident now; "new" if admitted by this call; False if it
-        does not fit (the request waits)."""
+        does not fit or its layout is still being built off the loop thread
+        (the request waits)."""
         if body in self.resident:
             return True
+        ent = self._prep.get(body)
+        if ent is None:
+            if self._prep_queue is not None:  # built by the preparing thread, admitted later
+                if body not in self._prep_wanted:
+                    self._prep_wanted.add(body)
+                    self._prep_queue.put(body)
+                return False
+            ent = self._prep[body] = self._build(body)
         ta = time.perf_counter()
-        doms = self.make_body(body)
-        need = scene_device_bytes(SceneLayout(doms))
+        layout, packed, need = ent
         if self.used_bytes + need > self.budget:
             self.deferred_admissions += 1
             return False
         try:
-            s = self.arena.insert(doms)
+            s = self.arena.insert_prepared(layout, packed)
         except _native.NativeError:
             self.deferred_admissions += 1
             return False
@@ -230,10 +266,27 @@ class Server:
         Per-scene job state lives in arrays (dt of the current run, substeps
         left in it, busy / construction-step flags), so one iteration costs
         O(scenes) vector work plus Python only for requests whose run ends."""
-        import torch
+        import queue
+        import threading
 
         arrivals = list(requests)
         heapq.heapify(arrivals)
+        # bodies are prepared (domains, layout, packing) on a second thread as
+        # their first request arrives; the loop thread only uploads them
+        self._prep_queue = queue.Queue()
+        self._prep_wanted = set(self._prep)
+        worker = threading.Thread(target=self._prep_worker, daemon=True)
+        worker.start()
+        try:
+            return self._run(arrivals, requests, realtime)
+        finally:
+            self._prep_queue.put(None)
+            worker.join()
+            self._prep_queue = None
+
+    def _run(self, arrivals, requests, realtime):
+        import torch
+
         queues = collections.defaultdict(collections.deque)  # body -> waiting requests
         ready = set()      # idle bodies with a waiting request
         busy = {}          # scene -> job
@@ -307,8 +360,10 @@ class Server:
                 init_m[s] = job.init
                 n_el[s] = self.arena.layouts[s].n_elems
             if not busy:
-                if not arrivals and not pending_done and ready:
+                if not arrivals and not pending_done and ready and all(b in self._prep for b in ready):
                     raise RuntimeError("requests wait for bodies that cannot be admitted (arena or budget full)")
+                if ready and not any(b in self._prep for b in ready):
+                    time.sleep(0.0005)  # the preparing thread is building the waiting bodies
                 # nothing on the GPU: retire finished work, then wait for the next arrival
                 evict(self._retire(pending_done, done_at, failed, status, t0, block=True))
                 if arrivals and realtime:

@@ -105,6 +105,11 @@ int fw_set_bodies(fw_ctx* ctx, int32_t n_bodies, const int32_t* node_offset,
  * Replaces: ExplicitLoop.__init__ state, flatworld/explicitloop.py:72-85, 172-175. */
 int fw_set_scenes(fw_ctx* ctx, int32_t n_scenes, const float* damping);
 
+/* Change scene `scene`'s velocity damping after fw_finalize; it applies from
+ * the next substep on.  The reference reads ExplicitLoop.damping at every
+ * substep (explicitloop.py:528, 537), so assigning it mid-run takes effect. */
+int fw_set_damping(fw_ctx* ctx, int32_t scene, float damping);
+
 /* Contact pairs (one FEM body against one ground), in the reference's launch
  * order within a body: planes, then height fields, then voxel grids, each in
  * contact-creation order.  gate_lo/gate_hi is the ground's getBBox() box used

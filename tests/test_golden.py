@@ -28,7 +28,7 @@ from tests.golden.make_golden import CASES, FRAME, LOOP_KW
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 RTOL = 1e-5
-NEOHOOKEAN_CASES = {"nh_heightfield32"}
+NEOHOOKEAN_CASES = {"nh_heightfield32", "tied_slabs"}
 
 
 def load(name):

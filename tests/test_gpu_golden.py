@@ -26,7 +26,7 @@ from tests.golden.make_golden import CASES, FRAME, LOOP_KW
 pytestmark = pytest.mark.gpu
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 RTOL = 1e-5
-NEOHOOKEAN_CASES = {"nh_heightfield32"}
+NEOHOOKEAN_CASES = {"nh_heightfield32", "tied_slabs"}
 NO_RESIDENT = {"tied_slabs"}  # FEM-FEM contact: gather step only
 PATHS = {"gather": {"path": "gather"}, "resident": {"path": "resident"},
          "resident-counter": {"path": "resident", "res_sync": 1}, "stream": {"path": "stream"}}

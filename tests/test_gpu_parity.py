@@ -52,9 +52,20 @@ def gpu_state(loop):
     return m.coords.numpy()[:n], m.V.numpy()[:n]
 
 
-def run_pair(domains, steps, every, dt=None, adaptive=True, exact=False, build=None, track=None, path="auto"):
+def hf_gap(domains, x):
+    """Smallest height of a node above the scene's height field (its first
+    domain), linear interpolation between samples: negative = penetrating."""
+    hf = domains[0]
+    h = np.asarray(hf.height, np.float64)
+    xs = np.linspace(float(hf.lb[0]), float(hf.ub[0]), len(h))
+    return float((np.asarray(x, np.float64)[:, 1] - np.interp(np.asarray(x, np.float64)[:, 0], xs, h)).min())
+
+
+def run_pair(domains, steps, every, dt=None, adaptive=True, exact=False, build=None, track=None, path="auto",
+             track_fn=None):
     """Step GPU and FP32 oracle side by side; compare every `every` steps.
-    ``track`` (a list) receives the lowest node height at every checkpoint."""
+    ``track`` (a list) receives the lowest node height at every checkpoint,
+    or ``track_fn(x)`` of the GPU positions when that is given."""
     doms_gpu = build() if build else domains
     doms_or = build() if build else domains
     loop = fw.ExplicitLoop(dt or 0.0, doms_gpu, useAdapativeDT=adaptive, **loop_kw(path))
@@ -71,7 +82,7 @@ def run_pair(domains, steps, every, dt=None, adaptive=True, exact=False, build=N
         xo, vo, _ = o32.state()
         ex, ev = rel_linf(xg, xo), rel_linf(vg, vo)
         if track is not None:
-            track.append(float(xg[:, 1].min()))
+            track.append(track_fn(xg) if track_fn else float(xg[:, 1].min()))
         worst = (max(worst[0], ex), max(worst[1], ev))
         if exact:
             assert np.array_equal(xg.astype(np.float64), xo), f"x differs at step {done}: {ex:.3e}"
@@ -132,7 +143,10 @@ def test_voxel_disk_bitwise(path):
 def test_neohookean_heightfield_bitwise(path):
     """Reduced large-mesh workload (64 x 64 quads, NeoHookean, height field)."""
     build = lambda: scenes.plain_large_scene(fw, n=64, hf_offset=0.17)  # noqa: E731
-    loop, o32, worst = run_pair(None, 3000, 250, adaptive=True, build=build, path=path, exact=True)
+    gaps = []
+    loop, o32, worst = run_pair(None, 3000, 250, adaptive=True, build=build, path=path, exact=True, track=gaps,
+                                track_fn=lambda x: hf_gap(build(), x))
+    assert min(gaps) < 0.0, "the body must press into the height field (contact active)"
     xg, _ = gpu_state(loop)
     e64 = fp64_error(build(), 3000, loop.dt, xg, adaptive=True)
     print(f"NeoHookean 64x64: vs FP32 oracle {worst}, vs FP64 {e64:.3e}")
@@ -287,11 +301,31 @@ def test_plain_large_full_size_5000_steps_bitwise():
     FP32 oracle at every checkpoint; the FP64 distance is reported."""
     build = lambda: scenes.plain_large_scene(fw, n=256)  # noqa: E731
     low = []
-    loop, o32, worst = run_pair(None, 5000, 1000, adaptive=True, build=build, exact=True, track=low)
+    loop, o32, worst = run_pair(None, 5000, 1000, adaptive=True, build=build, exact=True, track=low,
+                                track_fn=lambda x: hf_gap(build(), x))
     assert loop.path == 2
+    assert min(low) < 0.0, "the body must reach the height field within the 5000 substeps (contact active)"
     xg, vg = gpu_state(loop)
     o64 = oracle.OracleLoop(build(), 0.0, useAdapativeDT=True, precision="f64", threads=16)
     o64.advance(5000)
     x64, v64, _ = o64.state()
     print(f"plain large 5000 substeps: bitwise vs FP32 oracle; vs FP64 x {rel_linf(xg, x64):.3e} "
-          f"v {rel_linf(vg, v64):.3e}; lowest node {min(low):.4f}")
+          f"v {rel_linf(vg, v64):.3e}; deepest penetration of the height field {-min(low):.2e}")
+
+
+@pytest.mark.parametrize("path", ["gather", "resident"])
+def test_damping_assigned_mid_run_applies_from_the_next_substep(path):
+    """The reference reads ExplicitLoop.damping at every substep
+    (explicitloop.py:528, 537): a value assigned between substeps applies from
+    the next one, on every step path."""
+    loop = fw.ExplicitLoop(1e-4, scenes.plain_small_low_scene(fw), useAdapativeDT=False, path=path)
+    o32 = oracle.OracleLoop(scenes.plain_small_low_scene(fw), 1e-4, useAdapativeDT=False)
+    loop.advance_n(200)
+    o32.advance(200)
+    loop.damping = 0.05
+    o32.damping = 0.05
+    loop.advance_n(300)
+    o32.advance(300)
+    xg, vg = gpu_state(loop)
+    xo, vo, _ = o32.state()
+    assert np.array_equal(xg.astype(np.float64), xo) and np.array_equal(vg.astype(np.float64), vo)
