@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--fifo-seconds", type=float, default=5.0, help="served: wall-time cap of the FIFO server")
     ap.add_argument("--scenes", type=int, default=2048, help="batched: number of bodies")
     ap.add_argument("--plain-sample", type=int, default=64, help="batched: bodies timed alone")
+    ap.add_argument("--stream-patch", choices=["auto", "64", "128"], default="auto",
+                    help="batched, stream path: owned nodes per patch (auto: tuned on a sample)")
     ap.add_argument("--batch-path", choices=["gather", "stream"], default="stream",
                     help="batched: step implementation (same bits)")
     return ap.parse_args()
@@ -271,9 +273,24 @@ def run_batched(args, rank, world, local):
     substeps = 100 * args.steps
     t0 = time.perf_counter()
     batch = scenes.ragged_batch(fw, args.scenes, seed=rank)
-    b = BatchedLoop(batch, dt=5e-5, useAdapativeDT=False, device=local, path=args.batch_path)
+    patch_tuning = None
+    stream_patch = 0
+    if args.batch_path == "stream":
+        if args.stream_patch == "auto":
+            # the patch size is fixed when a loop is built: pick it on a sample
+            # of the batch (every 8th body), each size with its tuned launch shape
+            sample = batch[::8]
+            stream_patch, patch_tuning = autotune.tune_stream_patch(
+                lambda p: BatchedLoop(sample, dt=5e-5, useAdapativeDT=False, device=local, path="stream",
+                                      stream_patch=p))
+        else:
+            stream_patch = int(args.stream_patch)
+    b = BatchedLoop(batch, dt=5e-5, useAdapativeDT=False, device=local, path=args.batch_path,
+                    stream_patch=stream_patch)
     build_s = time.perf_counter() - t0
     tuned = autotune.tune_batched(b)
+    if patch_tuning is not None:
+        tuned = dict(tuned, patch_candidates=patch_tuning)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     with torch.cuda.stream(stream):

@@ -31,6 +31,9 @@ FW_OPT_GRID_ELEMS = 4
 FW_OPT_RES_SYNC = 5
 FW_OPT_WAIT_LIMIT = 6
 FW_OPT_TEST_WITHHOLD = 7
+FW_OPT_STREAM_PATCH = 8
+FW_OPT_STREAM_MINB = 9
+FW_OPT_STREAM_BULK = 10
 
 _lock = threading.Lock()
 _lib = None

@@ -34,10 +34,12 @@ class BatchedLoop:
         path: "stream" (one patch-streaming kernel per substep, the faster one
             for many small scenes) or "gather" (two kernels per substep through
             a corner buffer, launch shape tunable); both give the same bits
+        stream_patch: owned nodes per patch of the stream step, 64 or 128
+            (0: 64); see flatworld_b200.autotune.tune_stream_patch
     """
 
     def __init__(self, scenes, dt=0.0, useAdapativeDT=True, damping=0.0, device=0,
-                 block_elems=0, block_nodes=0, path="stream"):
+                 block_elems=0, block_nodes=0, path="stream", stream_patch=0):
         S = len(scenes)
         dts = dt if np.iterable(dt) else [dt] * S
         ada = useAdapativeDT if np.iterable(useAdapativeDT) else [useAdapativeDT] * S
@@ -49,8 +51,10 @@ class BatchedLoop:
         self._has_rigid = any(lay.entries for lay in self.layouts)
         if path == "stream" and (self.packed.spring_bodies or self._has_flex or self._has_rigid):
             path = "gather"  # the patch-streaming step covers triangles without FEM-FEM / FEM-rigid contact
-        self._native = build_native(self.packed, device=device, path=path)
+        self._native = build_native(self.packed, device=device, path=path,
+                                    stream_patch=stream_patch if path == "stream" else 0)
         self.path = path
+        self.stream_patch = (stream_patch or 64) if path == "stream" else 0
         if block_elems or block_nodes:
             self.set_launch(block_elems, block_nodes)
         self.S = S
@@ -76,6 +80,15 @@ class BatchedLoop:
             self._native.set_option(_native.FW_OPT_BLOCK_ELEMS, block_elems)
         if block_nodes:
             self._native.set_option(_native.FW_OPT_BLOCK_NODES, block_nodes)
+
+    def set_stream_shape(self, minb=0, bulk=None):
+        """Stream step launch shape: the CTAs per SM its registers are budgeted
+        for (``minb``; 0 keeps it) and whether a patch's triangle records are
+        staged by one bulk copy (``bulk``; None keeps it).  Same bits."""
+        if minb:
+            self._native.set_option(_native.FW_OPT_STREAM_MINB, int(minb))
+        if bulk is not None:
+            self._native.set_option(_native.FW_OPT_STREAM_BULK, 1 if bulk else 0)
 
     def set_stream(self, stream_ptr):
         self._native.set_stream(stream_ptr)

@@ -20,15 +20,21 @@
 // (StreamElem per patch triangle, StreamNode per owned node; built by
 // k_stream_elems / k_stream_nodes and rebuilt when a Young's modulus changes):
 // a record is one load at the CTA's own offset rather than an index load
-// followed by a dependent gather.  Small CTAs (64 threads) capped at 32
-// registers keep 32 CTAs on an SM, which hides the rest of that latency.
+// followed by a dependent gather.  Launch shapes (run-time options, chosen by
+// the autotuner): patches of 64 or 128 owned nodes, one thread per owned node
+// (larger patches carry fewer halo nodes and cut triangles per triangle, at
+// the price of coarser load balance over ragged scenes); a register budget
+// set by the CTAs the kernel is compiled to fit on an SM; and, optionally,
+// the patch's triangle records staged into shared memory by one bulk copy
+// (cp.async.bulk, completion on an mbarrier) that overlaps the position
+// gather, instead of one load per triangle and thread.
 #pragma once
 
 namespace {
 
-constexpr int kStreamNodes = 64;  // owned nodes per patch (and threads per CTA): small
-                                  // patches balance the ragged scenes over the SMs
+constexpr int kStreamNodes = 64;  // default owned nodes per patch (and threads per CTA)
 constexpr int kStreamThreads = 64;
+constexpr long long kBulkWaitLimit = 1ll << 24;  // polls of the staged-copy barrier before giving up
 
 struct StreamPatch {
   int node_off, no;  // owned nodes: nodes[node_off .. +no), ascending
@@ -67,6 +73,7 @@ struct StreamDev {
   int no_max, nh_max, ne_max;
   StreamElem* elem;  // built from eid/conn by k_stream_elems
   StreamNode* node;  // built from nodes by k_stream_nodes
+  int* err;          // != 0: a staged copy did not complete in time
 };
 
 __global__ void k_stream_nodes(Dev d, const int32_t* nodes, StreamNode* out, int n) {
@@ -115,14 +122,36 @@ __device__ __forceinline__ void stream_element(const Dev& d, const float2* sx, f
   sf[3 * q + 2] = f3;
 }
 
-__global__ void __launch_bounds__(kStreamThreads, 32) k_stream(Dev d, StreamDev sd, const float2* __restrict__ x_in,
-                                                               float2* __restrict__ x_out, const float4* j2_in,
-                                                               float4* j2_out) {
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_done(uint32_t mb, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(mb), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Dynamic shared memory of a stream CTA: positions (owned, then halo), the
+// corner forces of its triangles, then (staged launches) its triangle records.
+__host__ __device__ inline size_t stream_rec_offset(int no_max, int nh_max, int ne_max) {
+  const size_t b = sizeof(float2) * (size_t)(no_max + nh_max) + sizeof(float2) * 3 * (size_t)ne_max;
+  return (b + 15) & ~(size_t)15;
+}
+
+template <int NT, int MINB, bool BULK>
+__global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const float2* __restrict__ x_in,
+                                                     float2* __restrict__ x_out, const float4* j2_in,
+                                                     float4* j2_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long s_mbar;
   float2* sx = reinterpret_cast<float2*>(smem_raw);  // owned, then halo
   float2* sf = sx + (sd.no_max + sd.nh_max);         // 3 per patch triangle
+  StreamElem* srec = reinterpret_cast<StreamElem*>(smem_raw + stream_rec_offset(sd.no_max, sd.nh_max, sd.ne_max));
   const StreamPatch P = sd.patch[blockIdx.x];
-  const int t = threadIdx.x, T = blockDim.x;
+  const int t = threadIdx.x, T = NT;
   const int mode = d.scene_mode[P.scene];
   if (mode == fw::MODE_FROZEN) {  // keep the state: carry it into the other buffers
     for (int i = t; i < P.no; i += T) {
@@ -136,16 +165,49 @@ __global__ void __launch_bounds__(kStreamThreads, 32) k_stream(Dev d, StreamDev 
       }
     return;
   }
-  static_assert(kStreamThreads == kStreamNodes, "one owned node per thread");
+  const bool staged = BULK && P.ne > 0;
+  if (staged && t == 0) {
+    // one bulk copy of the patch's contiguous triangle records (48 B each:
+    // 16-byte aligned, a multiple of 16 bytes), completing on s_mbar
+    const uint32_t mb = smem_addr(&s_mbar);
+    const uint32_t bytes = (uint32_t)P.ne * (uint32_t)sizeof(StreamElem);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(srec)),
+                 "l"(sd.elem + P.elem_off), "r"(bytes), "r"(mb)
+                 : "memory");
+  }
   // positions of the owned (one per thread) and halo nodes
   const bool valid = t < P.no;
   const int g = valid ? sd.nodes[P.node_off + t] : 0;
   if (valid) sx[t] = x_in[g];
   for (int h = t; h < P.nh; h += T) sx[P.no + h] = x_in[sd.halo[P.halo_off + h]];
-  __syncthreads();
+  __syncthreads();  // also orders the barrier's initialisation before the waits below
+  if (staged) {
+    // thread 0 waits (bounded) for the staged records; the barrier below
+    // hands them, or the failure, to the whole CTA.  On a timeout the error
+    // flag is set and thread 0 waits once more (the copy writes this CTA's
+    // shared memory) before the CTA leaves.
+    __shared__ int s_ok;
+    if (t == 0) {
+      const uint32_t mb = smem_addr(&s_mbar);
+      long long it = 0;
+      bool ok = mbar_done(mb, 0);
+      while (!ok && ++it < kBulkWaitLimit) ok = mbar_done(mb, 0);
+      s_ok = ok ? 1 : 0;
+      if (!ok) {
+        atomicExch(sd.err, 1);
+        for (it = 0; !ok && it < kBulkWaitLimit; ++it) ok = mbar_done(mb, 0);
+      }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+  }
   // triangles (element_step)
   for (int q = t; q < P.ne; q += T) {
-    const StreamElem r = sd.elem[P.elem_off + q];
+    const StreamElem r = staged ? srec[q] : sd.elem[P.elem_off + q];
     stream_element(d, sx, sf, q, r.e, r.conn, r.m, r.ji, j2_in, j2_out);
   }
   __syncthreads();

@@ -1068,6 +1068,10 @@ struct fw_ctx {
   size_t st_smem = 0;
   float2* x_buf0 = nullptr;  // the position buffer allocated first (parity of the swaps)
   int st_ne = 0, st_no = 0;  // patch triangles and owned nodes (record counts)
+  int st_nodes = kStreamNodes;  // FW_OPT_STREAM_PATCH: owned nodes per patch = threads per CTA
+  int st_minb = 32;             // FW_OPT_STREAM_MINB: CTAs per SM the kernel's registers are budgeted for
+  int st_bulk = 0;              // FW_OPT_STREAM_BULK: stage triangle records with one bulk copy
+  size_t st_smem_bulk = 0;
   bool res_adj = false;            // the reverse pass runs resident (k_res_adj)
   size_t res_adj_smem = 0;
   unsigned long long* fll = nullptr;  // [2][N][4] flag-in-data force adjoints of the reverse pass
@@ -1317,6 +1321,18 @@ int run_steps(fw_ctx* c, int n) {
 }
 
 
+using StreamKernel = void (*)(Dev, StreamDev, const float2*, float2*, const float4*, float4*);
+
+// The stream kernel of a launch shape (patch size, register budget, staging);
+// nullptr for a shape that is not built.
+StreamKernel stream_kernel(int nodes, int minb, int bulk) {
+  if (nodes == 64 && minb == 32) return bulk ? k_stream<64, 32, true> : k_stream<64, 32, false>;
+  if (nodes == 64 && minb == 16) return bulk ? k_stream<64, 16, true> : k_stream<64, 16, false>;
+  if (nodes == 128 && minb == 16) return bulk ? k_stream<128, 16, true> : k_stream<128, 16, false>;
+  if (nodes == 128 && minb == 8) return bulk ? k_stream<128, 8, true> : k_stream<128, 8, false>;
+  return nullptr;
+}
+
 // n substeps of the stream path: k_control + k_stream each, alternating the
 // position / J2 buffers; graphs of up to kGraphSteps substeps, cached per
 // (starting buffer, dt mode, dt, count).
@@ -1333,7 +1349,9 @@ int stream_steps(fw_ctx* c, int n) {
       float4 *ja = c->d.j2state, *jb = c->d.j2_alt;
       for (int k = 0; k < m; ++k) {
         k_control<<<1, kMaxBlock, 0, c->stream>>>(c->d);
-        k_stream<<<c->st_P, kStreamThreads, c->st_smem, c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
+        stream_kernel(c->st_nodes, c->st_minb, c->st_bulk)<<<c->st_P, c->st_nodes,
+                                                             c->st_bulk ? c->st_smem_bulk : c->st_smem,
+                                                             c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
         std::swap(xa, xb);
         std::swap(ja, jb);
       }
@@ -1367,7 +1385,7 @@ int stream_records(fw_ctx* c) {
 }
 
 // Patches of the stream path: each body cut into patches of at most
-// kStreamNodes nodes; per patch the owned nodes, the triangles touching them,
+// st_nodes nodes; per patch the owned nodes, the triangles touching them,
 // the halo nodes, local connectivity and the owned nodes' corner lists in the
 // global ascending-element order.
 int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<int32_t>& slot,
@@ -1378,7 +1396,7 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
   for (int b = 0; b < c->B; ++b) {
     const int n0 = c->h_noff[b], nn = c->h_ncnt[b];
     if (nn <= 0) continue;
-    const int np = (nn + kStreamNodes - 1) / kStreamNodes;
+    const int np = (nn + c->st_nodes - 1) / c->st_nodes;
     idx.resize(nn);
     for (int k = 0; k < nn; ++k) idx[k] = n0 + k;
     rcb(x0, idx, 0, nn, P, np, part);
@@ -1400,7 +1418,8 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
   int no_max = 1, nh_max = 1, ne_max = 1;
   for (int p = 0; p < P; ++p) {
     const std::vector<int>& ow = owned[p];
-    if ((int)ow.size() > kStreamNodes) return fail(c, FW_ERR_ARG, "stream path: patch larger than %d nodes", kStreamNodes);
+    if ((int)ow.size() > c->st_nodes)
+      return fail(c, FW_ERR_ARG, "stream path: patch larger than %d nodes", c->st_nodes);
     std::vector<int> tri;
     for (int n : ow)
       for (int k = off[n]; k < off[n + 1]; ++k) tri.push_back(slot[k] / 3);
@@ -1476,18 +1495,25 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
     FW_CUDA(c, cudaMemcpyAsync(c->d.j2_alt, c->d.j2state, sizeof(float4) * E, cudaMemcpyDeviceToDevice, c->stream));
   StreamElem* dse = nullptr;
   StreamNode* dsn = nullptr;
-  if ((r = dalloc(c, &dse, re.size())) || (r = dalloc(c, &dsn, rn.size()))) return r;
-  c->sd = StreamDev{dp, dn, dh, de, dc, dcp, dcs, no_max, nh_max, ne_max, dse, dsn};
+  int* derr = nullptr;
+  if ((r = dalloc(c, &dse, re.size())) || (r = dalloc(c, &dsn, rn.size())) || (r = dalloc(c, &derr, 1))) return r;
+  FW_CUDA(c, cudaMemsetAsync(derr, 0, sizeof(int), c->stream));
+  c->sd = StreamDev{dp, dn, dh, de, dc, dcp, dcs, no_max, nh_max, ne_max, dse, dsn, derr};
   c->st_ne = (int)re.size();
   c->st_no = (int)rn.size();
   if ((r = stream_records(c))) return r;
   c->st_P = P;
   c->st_smem = sizeof(float2) * (size_t)(no_max + nh_max) + sizeof(float2) * 3 * (size_t)ne_max;
+  c->st_smem_bulk = stream_rec_offset(no_max, nh_max, ne_max) + sizeof(StreamElem) * (size_t)ne_max;
   c->x_buf0 = c->d.x;
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if ((long)c->st_smem > optin) return fail(c, FW_ERR_ARG, "stream path: patch needs %zu B of shared memory", c->st_smem);
-  FW_CUDA(c, cudaFuncSetAttribute(k_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  if ((long)c->st_smem_bulk > optin) c->st_bulk = 0;  // staging does not fit: plain loads
+  for (int minb : {8, 16, 32})
+    for (int bulk = 0; bulk < 2; ++bulk)
+      if (StreamKernel k = stream_kernel(c->st_nodes, minb, bulk))
+        FW_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 64));
   return FW_OK;
 }
 
@@ -1742,6 +1768,12 @@ int check_device_error(fw_ctx* c) {
                   "a rigid body came within 0.01 of a ground or of another contact rigid (rigid-rigid and "
                   "rigid-ground contact, the reference's constraint solve, are outside this library), or its "
                   "state is no longer finite");
+  }
+  if (c->path == FW_PATH_STREAM && c->sd.err) {
+    int serr = 0;
+    FW_CUDA(c, cudaMemcpyAsync(&serr, c->sd.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (serr) return fail(c, FW_ERR_TIMEOUT, "stream step: a staged copy of triangle records did not complete");
   }
   if (c->path != FW_PATH_RESIDENT) return FW_OK;
   int err = 0;
@@ -2695,6 +2727,12 @@ int fw_set_path(fw_ctx* c, int32_t path, int32_t patches) {
   return FW_OK;
 }
 
+static int shared_optin(fw_ctx* c) {
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  return optin;
+}
+
 int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
   if (!c) return FW_ERR_ARG;
   switch (option) {
@@ -2730,6 +2768,29 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
       if (value < -1) return fail(c, FW_ERR_ARG, "FW_OPT_TEST_WITHHOLD must be >= -1");
       c->withhold_cta = value;
       return FW_OK;
+    case FW_OPT_STREAM_PATCH: {
+      if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_STREAM_PATCH after fw_finalize");
+      if (value != 64 && value != 128) return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_PATCH must be 64 or 128");
+      c->st_nodes = value;
+      c->st_minb = value == 64 ? 32 : 16;
+      return FW_OK;
+    }
+    case FW_OPT_STREAM_MINB: {
+      if (!stream_kernel(c->st_nodes, value, 0))
+        return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_MINB: %d-node patches are built for %s CTAs per SM", c->st_nodes,
+                    c->st_nodes == 64 ? "16 or 32" : "8 or 16");
+      c->st_minb = value;
+      drop_graphs(c);
+      return FW_OK;
+    }
+    case FW_OPT_STREAM_BULK: {
+      if (value != 0 && value != 1) return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_BULK must be 0 or 1");
+      if (value && c->finalized && c->path == FW_PATH_STREAM && c->st_smem_bulk + 64 > (size_t)shared_optin(c))
+        return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_BULK: the staged records do not fit in shared memory");
+      c->st_bulk = value;
+      drop_graphs(c);
+      return FW_OK;
+    }
     case FW_OPT_RES_SYNC: {
       if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_RES_SYNC after fw_finalize");
       if (value != 0 && value != 1) return fail(c, FW_ERR_ARG, "FW_OPT_RES_SYNC must be 0 or 1");

@@ -291,6 +291,17 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
  * time; they apply from the next launch. */
 #define FW_OPT_WAIT_LIMIT 6
 #define FW_OPT_TEST_WITHHOLD 7
+/* Stream path (FW_PATH_STREAM) launch shape:
+ * FW_OPT_STREAM_PATCH: owned nodes per patch = threads per CTA, 64 (default)
+ *   or 128; before fw_finalize (the patches are cut there).
+ * FW_OPT_STREAM_MINB: CTAs per SM the kernel's registers are budgeted for
+ *   (64-node patches: 32 (default) or 16; 128-node patches: 16 (default) or 8).
+ * FW_OPT_STREAM_BULK: 1 stages each patch's triangle records into shared
+ *   memory with one bulk copy instead of a load per triangle (default 0).
+ * All give the same bits; the autotuner picks them. */
+#define FW_OPT_STREAM_PATCH 8
+#define FW_OPT_STREAM_MINB 9
+#define FW_OPT_STREAM_BULK 10
 int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
 
 /* Checkpoint / resume: copy the whole step state (positions, velocities, J2
