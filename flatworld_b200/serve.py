@@ -195,9 +195,8 @@ class Server:
         self.admit_s = 0.0        # host time spent admitting new bodies
         self.last_admit_t = 0.0   # run clock of the last admission
         self.evicted = 0          # bodies removed because their state turned non-finite
-        self._prep = {}           # body -> (layout, packed, device bytes), built off the loop thread
-        self._prep_queue = None   # bodies waiting for the preparing thread (during run)
-        self._prep_wanted = set()
+        self._prep = {}           # body -> (layout, packed, device bytes), built ahead by prepare()
+        self.admit_budget_s = 0.002  # host time per loop iteration for admitting new bodies
 
     def _build(self, body):
         """Host-side preparation of a body: its domains, scene layout, packed
@@ -212,27 +211,13 @@ class Server:
             if b not in self._prep:
                 self._prep[b] = self._build(b)
 
-    def _prep_worker(self):
-        while True:
-            b = self._prep_queue.get()
-            if b is None:
-                return
-            if b not in self._prep:
-                self._prep[b] = self._build(b)
-
     def _admit(self, body, t0=None):
         """True if resident now; "new" if admitted by this call; False if it
-        does not fit or its layout is still being built off the loop thread
-        (the request waits)."""
+        does not fit (the request waits)."""
         if body in self.resident:
             return True
         ent = self._prep.get(body)
         if ent is None:
-            if self._prep_queue is not None:  # built by the preparing thread, admitted later
-                if body not in self._prep_wanted:
-                    self._prep_wanted.add(body)
-                    self._prep_queue.put(body)
-                return False
             ent = self._prep[body] = self._build(body)
         ta = time.perf_counter()
         layout, packed, need = ent
@@ -266,23 +251,9 @@ class Server:
         Per-scene job state lives in arrays (dt of the current run, substeps
         left in it, busy / construction-step flags), so one iteration costs
         O(scenes) vector work plus Python only for requests whose run ends."""
-        import queue
-        import threading
-
         arrivals = list(requests)
         heapq.heapify(arrivals)
-        # bodies are prepared (domains, layout, packing) on a second thread as
-        # their first request arrives; the loop thread only uploads them
-        self._prep_queue = queue.Queue()
-        self._prep_wanted = set(self._prep)
-        worker = threading.Thread(target=self._prep_worker, daemon=True)
-        worker.start()
-        try:
-            return self._run(arrivals, requests, realtime)
-        finally:
-            self._prep_queue.put(None)
-            worker.join()
-            self._prep_queue = None
+        return self._run(arrivals, requests, realtime)
 
     def _run(self, arrivals, requests, realtime):
         import torch
@@ -342,8 +313,13 @@ class Server:
                 queues[r.body].append(r)
                 if r.body not in busy_bodies:
                     ready.add(r.body)
-            # start the next request of every idle body that has one
+            # start the next request of every idle body that has one; new
+            # bodies are uploaded within a host-time budget per iteration, so a
+            # burst of first requests cannot stall the requests in flight
+            t_adm = time.perf_counter()
             for body in sorted(ready):
+                if body not in self.resident and time.perf_counter() - t_adm > self.admit_budget_s:
+                    continue  # admitted in a later iteration
                 adm = self._admit(body, t0)
                 if not adm:
                     continue
@@ -360,10 +336,9 @@ class Server:
                 init_m[s] = job.init
                 n_el[s] = self.arena.layouts[s].n_elems
             if not busy:
-                if not arrivals and not pending_done and ready and all(b in self._prep for b in ready):
+                if not arrivals and not pending_done and ready and not any(b in self.resident for b in ready) \
+                        and time.perf_counter() - t_adm <= self.admit_budget_s:
                     raise RuntimeError("requests wait for bodies that cannot be admitted (arena or budget full)")
-                if ready and not any(b in self._prep for b in ready):
-                    time.sleep(0.0005)  # the preparing thread is building the waiting bodies
                 # nothing on the GPU: retire finished work, then wait for the next arrival
                 evict(self._retire(pending_done, done_at, failed, status, t0, block=True))
                 if arrivals and realtime:
