@@ -61,6 +61,10 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=64, help="batched: bodies timed alone")
     ap.add_argument("--stream-patch", choices=["auto", "64", "128"], default="auto",
                     help="batched, stream path: owned nodes per patch (auto: tuned on a sample)")
+    ap.add_argument("--stream-minb", type=int, default=0,
+                    help="batched, stream path: CTAs per SM of the register budget (0: tuned)")
+    ap.add_argument("--stream-bulk", type=int, choices=[-1, 0, 1], default=-1,
+                    help="batched, stream path: stage triangle records by bulk copy (-1: tuned)")
     ap.add_argument("--batch-path", choices=["gather", "stream"], default="stream",
                     help="batched: step implementation (same bits)")
     return ap.parse_args()
@@ -288,7 +292,12 @@ def run_batched(args, rank, world, local):
     b = BatchedLoop(batch, dt=5e-5, useAdapativeDT=False, device=local, path=args.batch_path,
                     stream_patch=stream_patch)
     build_s = time.perf_counter() - t0
-    tuned = autotune.tune_batched(b)
+    if args.batch_path == "stream" and (args.stream_minb or args.stream_bulk >= 0):
+        b.set_stream_shape(args.stream_minb, None if args.stream_bulk < 0 else bool(args.stream_bulk))
+        tuned = {"path": "stream", "patch": b.stream_patch, "minb": args.stream_minb or "default",
+                 "bulk": args.stream_bulk, "chosen_by": "command line"}
+    else:
+        tuned = autotune.tune_batched(b)
     if patch_tuning is not None:
         tuned = dict(tuned, patch_candidates=patch_tuning)
     stream = torch.cuda.Stream()

@@ -51,7 +51,8 @@
  * products in index order; determinant(m) = m00*m11 - m01*m10; inverse(m22) =
  * adjugate * (1/det), the zero matrix when det == 0; round() rounds half away
  * from zero (C roundf); floor and sqrt are the C library functions; log is
- * or_logf below (or the C library's logf in liboracle_f32libm.so); the serial
+ * or_logf below, sin and cos or_sincosf (or the C library's logf, sinf and
+ * cosf in liboracle_f32libm.so); the serial
  * CPU device applies atomic_add in launch order.
  */
 #include <math.h>
@@ -64,11 +65,11 @@
 #define REAL float
 #endif
 
-/* log of the FP32 builds: unless USE_LIBM_LOG is defined, the method below
+/* log of the FP32 builds: unless USE_LIBM_MATH is defined, the method below
  * (Cody-Waite reduction + atanh series, IEEE + - * / only), which the CUDA
  * kernels evaluate with the same operations in the same order.  Any accurate
  * log is a faithful reading of the reference's wp.log; this one makes CPU and
- * GPU agree bit for bit.  USE_LIBM_LOG builds use the C library's logf, as the
+ * GPU agree bit for bit.  USE_LIBM_MATH builds use the C library's logf, as the
  * reference's Warp CPU device does. */
 static float or_logf(float x) {
   if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;
@@ -114,7 +115,7 @@ static float or_logf(float x) {
 #define R_POW pow
 #else
 #define R_SQRT sqrtf
-#if defined(USE_LIBM_LOG)
+#if defined(USE_LIBM_MATH)
 #define R_LOG logf
 #else
 #define R_LOG or_logf
@@ -1118,7 +1119,8 @@ static void flex_contacts(or_world* w, long counter) {
  * split into 1.5703125 + 0x1.fb4p-12 + 0x1.4442d2p-24 (the first two short
  * enough that k times them is exact for |k| < 2^13), then the Taylor series of
  * sin through r^9 and of cos through r^10 on |r| <= pi/4 (truncation error
- * below 2e-9), and the quadrant k mod 4. */
+ * below 2e-9), and the quadrant k mod 4.  USE_LIBM_MATH builds call the C
+ * library's sinf and cosf instead, as the reference's Warp CPU device does. */
 static void or_sincosf(float x, float* s_out, float* c_out) {
   const float k = floorf(x * 0.63661975f + 0.5f);
   const float r = ((x - k * 1.5703125f) - k * 4.837512969970703125e-4f) - k * 0x1.4442d2p-24f;
@@ -1136,6 +1138,9 @@ static void r_sincos(REAL x, REAL* s, REAL* c) {
 #if defined(REAL_IS_DOUBLE)
   *s = sin(x);
   *c = cos(x);
+#elif defined(USE_LIBM_MATH)
+  *s = sinf(x);
+  *c = cosf(x);
 #else
   or_sincosf(x, s, c);
 #endif

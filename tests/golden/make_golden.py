@@ -51,9 +51,27 @@ CASES = {
     "j2_block": ("j2_block_scene", {}, 5e-5, False, ("steps", 4000, 400)),
     "bcs": ("bcs_scene", {}, 0.0, True, ("frames", 60, 10)),
     "tied_slabs": ("tied_slabs_scene", {}, 1.25e-5, False, ("steps", 3000, 300)),
+    # row (f): FEM-FEM contact, rigid primitives, grounds with BCs, springs
+    "flex_circles": ("flex_circles", {}, 0.0, True, ("frames", 24, 4)),
+    "flex_stack": ("flex_stack", {}, 0.0, True, ("frames", 40, 8)),
+    "rigid_fixed_ball": ("rigid_fixed_ball", {}, 0.0, True, ("frames", 40, 8)),
+    "rigid_fixed_ball_tied": ("rigid_fixed_ball", {}, 0.0, True, ("frames", 40, 8)),
+    "rigid_pusher": ("rigid_pusher", {}, 0.0, True, ("frames", 14, 2)),
+    "rigid_free_ball": ("rigid_free_ball", {}, 0.0, True, ("frames", 40, 8)),
+    "rigid_bcs": ("rigid_bcs", {}, 0.0, True, ("frames", 30, 6)),
+    "ground_circle_fixed": ("ground_circle_fixed", {}, 0.0, True, ("frames", 30, 6)),
+    "ground_circle_moving": ("ground_circle_moving", {}, 0.0, True, ("frames", 30, 6)),
+    "fixed_heightfield": ("fixed_heightfield", {}, 0.0, True, ("frames", 30, 6)),
+    "spring_bcs": ("spring_bcs_scene", {}, 0.0, True, ("frames", 60, 10)),
+    "spring_mixed": ("spring_mixed_scene", {}, 0.0, True, ("frames", 30, 6)),
 }
 # ExplicitLoop keyword arguments beyond dt / useAdapativeDT, per case
-LOOP_KW = {"tied_slabs": {"ties": [(0, 1)]}}
+LOOP_KW = {"tied_slabs": {"ties": [(0, 1)]}, "rigid_fixed_ball_tied": {"ties": [(0, 1)]},
+           "rigid_bcs": {"damping": 0.5}}
+# cases whose worlds step on the gather path only (FEM-FEM contact, rigids, springs)
+GATHER_ONLY = {"tied_slabs", "flex_circles", "flex_stack", "rigid_fixed_ball", "rigid_fixed_ball_tied",
+               "rigid_pusher", "rigid_free_ball", "rigid_bcs", "ground_circle_fixed", "ground_circle_moving",
+               "fixed_heightfield", "spring_bcs", "spring_mixed"}
 
 
 def reference_api():

@@ -106,9 +106,10 @@ bool_ = _Scalar("bool", np.bool_, False)
 
 def _scalar_of(t):
     """Map a dtype spec (Python float/int, a _Scalar) to a _Scalar."""
-    if t is None or t is builtins.float:
+    g = globals()
+    if t is None or t is builtins.float or t is g.get("_kfloat"):  # inside kernels `float` is _kfloat
         return float32
-    if t is builtins.int:
+    if t is builtins.int or t is g.get("_kint"):
         return int32
     if t is builtins.bool:
         return bool_

@@ -495,3 +495,54 @@ def tied_slabs_scene(fw, disk=True):
                          [fw.Gravity([0.0, -9.8])], initials=[fw.InitialVel("ALL", [0.0, -0.5])])
         doms.append(c)
     return doms
+
+
+def ground_circle_fixed(fw):
+    """ground_circle with the plane held by Fixed([0]) (the rigid manager moves it: static bits)."""
+    return ground_circle(fw, [fw.Fixed([0])])
+
+
+def ground_circle_moving(fw):
+    """ground_circle with the plane driven by EnforceVel: its gate box moves, its contact stays."""
+    return ground_circle(fw, [fw.EnforceVel([0], [0.0, -0.5])])
+
+
+def fixed_heightfield(fw):
+    return fixed_ground_heightfield(fw, True)
+
+
+def spring_bcs_scene(fw):
+    """test2D/test_2Dspring_bcs.py:17-27: three spring squares under Force /
+    EnforceVel / EnforceAcc with two fixed nodes each."""
+    conn = np.array([[0, 1], [1, 2], [0, 2], [2, 3], [3, 1], [0, 3]], dtype=np.int32)
+    coords = np.array([[0.5, 0.5], [0.7, 0.5], [0.5, 0.7], [0.7, 0.7]], dtype=np.float32)
+    d0 = fw.SpringMassDomain(2, coords, conn, [100.0, 1.0, 1.0], [fw.Force([0, 1], [0, -1.0]), fw.Fixed([2, 3])],
+                             False)
+    d1 = fw.SpringMassDomain(2, coords - 0.25, conn, [100.0, 1.0, 1.0],
+                             [fw.EnforceVel([0, 1], [0, -1.0]), fw.Fixed([2, 3])], False)
+    d2 = fw.SpringMassDomain(2, coords - 0.5, conn, [100.0, 1.0, 1.0],
+                             [fw.EnforceAcc([0, 1], [0, -10.0]), fw.Fixed([2, 3])], False)
+    return [d0, d1, d2]
+
+
+def spring_mixed_scene(fw):
+    """An Elastic block and a 6 x 6 spring net (friction 0.1) falling on the
+    ground plane y = 0 side by side (spring-plane contact at 100 k, the
+    spring-FEM pair bounding dt)."""
+    n = 6
+    dx = 0.6 / n
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    grid = np.stack([dx * ii, dx * jj], axis=-1).reshape(-1, 2).astype(np.float32) + np.float32(0.25)
+    sconn = []
+    for i in range(n):
+        for j in range(n):
+            a, b, c = i * (n + 1) + j, i * (n + 1) + j + 1, (i + 1) * (n + 1) + j
+            sconn += [[a, b], [b, c], [c, a], [a, b]]
+    sconn = np.asarray(sconn, np.int32)
+    conn, coords = fw.structured_rectangle(8, 4, 0.2, 0.1, origin=(0.0, 0.05))
+    block = fw.FemDomain(fw.Mesh(2, conn, coords), fw.SolidProp(fw.Elastic(E=2e4, nu=0.3, rho=100.0)),
+                         [fw.Gravity([0.0, -9.8])])
+    xy = (grid - np.float32(0.25)) * np.float32(0.25) + np.float32([0.3, 0.03])
+    net = fw.SpringMassDomain(2, xy.astype(np.float32), sconn, [200.0, 0.5, 0.01], [fw.Gravity([0.0, -9.8])],
+                              friction=0.1)
+    return [fw.GroundDomain(2, [0.0, 0.0], [0.0, 1.0]), block, net]
