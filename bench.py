@@ -65,6 +65,8 @@ def parse():
                     help="batched, stream path: CTAs per SM of the register budget (0: tuned)")
     ap.add_argument("--stream-bulk", type=int, choices=[-1, 0, 1], default=-1,
                     help="batched, stream path: stage triangle records by bulk copy (-1: tuned)")
+    ap.add_argument("--serve-path", choices=["gather", "stream"], default="stream",
+                    help="served: arena step implementation (same bits)")
     ap.add_argument("--batch-path", choices=["gather", "stream"], default="stream",
                     help="batched: step implementation (same bits)")
     return ap.parse_args()
@@ -192,16 +194,23 @@ def ncu_traffic():
     return None
 
 
-def ncu_traffic_ratio_batched(step_path="gather"):
-    """DRAM bytes / algorithmic bytes of the batched step kernels, measured by
-    ncu on a 256-body batch (per-triangle and per-node traffic do not depend on
-    the batch size, so the ratio scales to the full batch)."""
+def ncu_traffic_ratio_batched(step_path="gather", shape=None):
+    """(DRAM bytes / algorithmic bytes, where it was measured) of the batched
+    step kernels, from ncu captures of a 256-body batch (per-triangle and
+    per-node traffic do not depend on the batch size, so the ratio scales to
+    the full batch).  On the stream path the ratio of the launch shape in use
+    (``BatchedLoop.stream_shape``) where one was captured."""
     path = os.path.join(ROOT, "profiles", "traffic_batched.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            d = json.load(f)
-        return d.get("stream_traffic_over_algorithmic") if step_path == "stream" else d.get("traffic_over_algorithmic")
-    return None
+    if not os.path.exists(path):
+        return None, None
+    with open(path) as f:
+        d = json.load(f)
+    if step_path != "stream":
+        return d.get("traffic_over_algorithmic"), d.get("source")
+    shapes = d.get("stream_shapes", {})
+    if shape in shapes:
+        return shapes[shape], f"{d.get('stream_shapes_source')}, shape {shape}"
+    return d.get("stream_traffic_over_algorithmic"), d.get("stream_source")
 
 
 def cpu_oracle_rate(fw, mesh, seconds, threads):
@@ -294,8 +303,7 @@ def run_batched(args, rank, world, local):
     build_s = time.perf_counter() - t0
     if args.batch_path == "stream" and (args.stream_minb or args.stream_bulk >= 0):
         b.set_stream_shape(args.stream_minb, None if args.stream_bulk < 0 else bool(args.stream_bulk))
-        tuned = {"path": "stream", "patch": b.stream_patch, "minb": args.stream_minb or "default",
-                 "bulk": args.stream_bulk, "chosen_by": "command line"}
+        tuned = {"path": "stream", "shape": b.stream_shape, "chosen_by": "command line"}
     else:
         tuned = autotune.tune_batched(b)
     if patch_tuning is not None:
@@ -364,6 +372,7 @@ def run_batched(args, rank, world, local):
     bstep = algorithmic_bytes_per_substep(b.n_nodes, E, nj2, nb, ground)
     achieved = bstep / (ms / 1e3 / substeps) / 1e9
     peak, which = peaks()
+    ratio, ratio_src = ncu_traffic_ratio_batched(args.batch_path, b.stream_shape if b.stream_patch else None)
     line = {
         "metric": "FEM element-steps/s (batched ragged bodies)", "value": value, "unit": "element-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -384,9 +393,9 @@ def run_batched(args, rank, world, local):
                                 else "substep = k_elements + k_nodes"), "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": which,
                      "algorithmic_bytes_per_substep": bstep,
-                     "traffic": (None if ncu_traffic_ratio_batched(args.batch_path) is None
-                                 else round(ncu_traffic_ratio_batched(args.batch_path) * bstep)),
-                     "traffic_note": "DRAM bytes per substep scaled from an ncu capture of a 256-body batch"},
+                     "traffic": None if ratio is None else round(ratio * bstep),
+                     "traffic_from": ("DRAM bytes per substep scaled from an ncu capture of a 256-body batch: "
+                                      f"{ratio_src}")},
         "e2e": {"value": work_e2e / (ms_e2e / 1e3), "unit": "element-steps/s",
                 "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8},
         "gpu_launches": launches, "clocks": clk.summary(),
@@ -432,26 +441,31 @@ def run_served(args, rank, world, local):
     population = scenes.ragged_batch(fw, args.scenes, seed=rank)  # request payloads, built client-side
     build_s = time.perf_counter() - t0
     reqs = poisson_requests(args.rate, args.duration, args.scenes, seed=17 + rank)
-    srv = Server(lambda b: population[b], budget_bytes=150e9, device=local)
-    # catalog load: every body's host-side layout built before the stream
-    # starts; admission (upload into the arena) happens at its first request
+    srv = Server(lambda b: population[b], budget_bytes=150e9, device=local, path=args.serve_path)
+    # catalog load: every body's pack (host-side layout, corner lists, stream
+    # patches, in page-locked memory) built before the stream starts;
+    # admission (an upload queued on the arena's stream) happens at its first request
     t1 = time.perf_counter()
     srv.prepare(range(args.scenes))
     prepare_s = time.perf_counter() - t1
     # warm-up: compile paths and touch the allocator with a few bodies
     warm = poisson_requests(200.0, 0.05, 8, seed=5)
-    Server(lambda b: scenes.ragged_batch_one(fw, 10_000 + b), arena_nodes=200_000, arena_elems=400_000,
-           arena_bodies=64, arena_scenes=64, device=local).run(warm, realtime=False)
+    wsrv = Server(lambda b: scenes.ragged_batch_one(fw, 10_000 + b), arena_nodes=200_000, arena_elems=400_000,
+                  arena_bodies=64, arena_scenes=64, device=local, path=args.serve_path)
+    wsrv.run(warm, realtime=False)
+    wsrv.close()
     barrier(dist)
     l0 = srv.arena.native.launch_count()
     with ClockSampler(local) as clk:
         out = srv.run(reqs, realtime=True)
     launches = srv.arena.native.launch_count() - l0
+    srv.close()
     # capacity: the requests of the first 10 s all queued at t = 0 (a fresh server)
     cap_reqs = [r for r in reqs if r.arrival < 10.0]
-    cap_srv = Server(lambda b: population[b], budget_bytes=150e9, device=local)
+    cap_srv = Server(lambda b: population[b], budget_bytes=150e9, device=local, path=args.serve_path)
     cap_srv.prepare(range(args.scenes))
     cap = cap_srv.run(cap_reqs, realtime=False)
+    cap_srv.close()
     steps_all, wall = shard.aggregate(out["element_steps"], out["wall_s"])
     lat = out["latency_s"] * 1e3
     steady = np.asarray([l for l, r in zip(lat, reqs) if r.arrival > out["last_admit_t"]])
@@ -471,17 +485,22 @@ def run_served(args, rank, world, local):
         "config": {"workload": f"served: {args.rate:.0f} req/s Poisson for {args.duration:.0f} s, "
                                f"{args.scenes} resident bodies, advanceWithTime(1/60) in U{{50..400}} substeps",
                    "requests": len(reqs), "population_build_s": build_s, "catalog_prepare_s": prepare_s,
+                   "step_path": args.serve_path,
                    "budget_bytes": 150e9,
                    "resident_bodies": out["resident_bodies"], "resident_bytes": out["used_bytes"],
                    "deferred_admissions": out["deferred_admissions"], "substeps_run": out["substeps"]},
         "capacity": {"requests": len(cap_reqs), "wall_s": cap["wall_s"],
                      "sims_per_s": len(cap_reqs) / cap["wall_s"],
                      "element_steps_per_s": cap["element_steps"] / cap["wall_s"],
+                     "native_calls": cap["native_calls"], "substeps": cap["substeps"],
+                     "device_busy_s": cap["device_s"], "admit_s": cap["admit_s"],
                      "note": "same requests all queued at t = 0 (saturated GPU); includes admitting 2048 bodies"},
         "served": {"sims_per_s": len(lat) / wall, "wall_s": wall, "substeps": out["substeps"],
-                   "native_calls": out["native_calls"], "admit_s": out["admit_s"],
+                   "native_calls": out["native_calls"], "admit_s": out["admit_s"], "device_busy_s": out["device_s"],
                    "last_admission_at_s": out["last_admit_t"], "evicted_bodies": out["evicted_bodies"],
-                   "failed_requests": len(out["failed"]),
+                   "readmitted_bodies": out["readmitted_bodies"], "failed_requests": len(out["failed"]),
+                   "failed_note": "bodies whose state turned non-finite (flagged on the device) are evicted and "
+                                  "their requests failed; a later request re-admits them afresh",
                    "latency_ms_after_last_admission": {
                        "requests": int(len(steady)),
                        "p50": percentile_ms(steady, 50) if len(steady) else None,

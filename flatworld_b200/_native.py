@@ -34,6 +34,7 @@ FW_OPT_TEST_WITHHOLD = 7
 FW_OPT_STREAM_PATCH = 8
 FW_OPT_STREAM_MINB = 9
 FW_OPT_STREAM_BULK = 10
+FW_PACK_PINNED = 1
 
 _lock = threading.Lock()
 _lib = None
@@ -87,6 +88,12 @@ _SIGNATURES = {
     "fw_arena_commit": (C.c_int, [_vp, _i32p]),
     "fw_arena_remove": (C.c_int, [_vp, C.c_int32]),
     "fw_arena_scene_info": (C.c_int, [_vp, C.c_int32, _i64p]),
+    "fw_arena_pack": (C.c_int, [_vp, C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    "fw_step_served_budget": (C.c_int, [_vp, _f32p, _i32p, C.c_int32]),
+    "fw_create_stage": (C.c_int, [C.POINTER(_vp)]),
+    "fw_arena_commit_pack": (C.c_int, [_vp, _vp, _i32p]),
+    "fw_pack_info": (C.c_int, [_vp, _i64p]),
+    "fw_pack_destroy": (None, [_vp]),
     "fw_restore": (C.c_int, [_vp, C.c_int32]),
     "fw_finalize": (C.c_int, [_vp]),
     "fw_step": (C.c_int, [_vp, C.c_int32, C.c_float]),
@@ -136,6 +143,26 @@ def lib():
         return _lib
 
 
+class ScenePack:
+    """A scene prepared for an arena (fw_arena_pack); freed by close() -- no
+    commit from it may still be in flight then."""
+
+    def __init__(self, L, handle):
+        self._L = L
+        self.handle = handle
+        info = np.zeros(8, dtype=np.int64)
+        L.fw_pack_info(handle, info.ctypes.data_as(_i64p))
+        self.device_bytes = int(info[0])
+        self.nodes, self.elems, self.bodies = int(info[1]), int(info[2]), int(info[3])
+        self.patch_nodes, self.patches, self.patch_elems = int(info[4]), int(info[5]), int(info[6])
+        self.pinned = bool(info[7])
+
+    def close(self):
+        if self.handle:
+            self._L.fw_pack_destroy(self.handle)
+            self.handle = None
+
+
 def _f(a):
     a = np.ascontiguousarray(a, dtype=np.float32)
     return a, a.ctypes.data_as(_f32p)
@@ -163,6 +190,20 @@ class NativeWorld:
                 "(flatworld_b200 runs on the GPU only)")
         self._h = h
         self.device = device
+
+    @classmethod
+    def stage(cls) -> "NativeWorld":
+        """A staging context (fw_create_stage): stages one scene at a time
+        for arena_pack, touches no device (works without a GPU)."""
+        w = cls.__new__(cls)
+        w._L = lib()
+        h = _vp()
+        rc = w._L.fw_create_stage(C.byref(h))
+        if rc != 0:
+            raise NativeError(f"fw_create_stage failed with code {rc}")
+        w._h = h
+        w.device = -1
+        return w
 
     def _check(self, rc: int, what: str):
         if rc != 0:
@@ -359,6 +400,20 @@ class NativeWorld:
     def arena_remove(self, scene: int):
         self._check(self._L.fw_arena_remove(self._h, int(scene)), "fw_arena_remove")
 
+    def arena_pack(self, patch_nodes: int, pinned: bool = False) -> "ScenePack":
+        """The scene staged on this (never finalized) context as a pack for
+        an arena with ``patch_nodes``-node stream patches (0: gather arena).
+        Host work only; the stage is cleared."""
+        h = _vp()
+        self._check(self._L.fw_arena_pack(self._h, int(patch_nodes), FW_PACK_PINNED if pinned else 0, C.byref(h)),
+                    "fw_arena_pack")
+        return ScenePack(self._L, h)
+
+    def arena_commit_pack(self, pack: "ScenePack") -> int:
+        s = C.c_int32()
+        self._check(self._L.fw_arena_commit_pack(self._h, pack.handle, C.byref(s)), "fw_arena_commit_pack")
+        return int(s.value)
+
     def arena_scene_info(self, scene: int):
         out = np.zeros(8, dtype=np.int64)
         self._check(self._L.fw_arena_scene_info(self._h, int(scene), out.ctypes.data_as(_i64p)), "fw_arena_scene_info")
@@ -390,6 +445,13 @@ class NativeWorld:
         """n_steps substeps with the same per-scene dt (see step_served)."""
         self._check(self._L.fw_step_served_n(self._h, dt_per_scene.ctypes.data_as(_f32p), int(n_steps)),
                     "fw_step_served_n")
+
+    def step_served_budget(self, dt_per_scene, budget, n_steps: int):
+        """Stream arenas: n_steps substeps in which scene s runs only its
+        first budget[s] substeps (fw_step_served_budget)."""
+        b = _i(budget)
+        self._check(self._L.fw_step_served_budget(self._h, dt_per_scene.ctypes.data_as(_f32p), b[1], int(n_steps)),
+                    "fw_step_served_budget")
 
     def set_active(self, active):
         a = _i(active)

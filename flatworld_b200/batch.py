@@ -55,6 +55,8 @@ class BatchedLoop:
                                     stream_patch=stream_patch if path == "stream" else 0)
         self.path = path
         self.stream_patch = (stream_patch or 64) if path == "stream" else 0
+        self.stream_minb = {64: 32, 128: 16}.get(self.stream_patch, 0)  # the built default budgets
+        self.stream_bulk = False
         if block_elems or block_nodes:
             self.set_launch(block_elems, block_nodes)
         self.S = S
@@ -87,8 +89,15 @@ class BatchedLoop:
         staged by one bulk copy (``bulk``; None keeps it).  Same bits."""
         if minb:
             self._native.set_option(_native.FW_OPT_STREAM_MINB, int(minb))
+            self.stream_minb = int(minb)
         if bulk is not None:
             self._native.set_option(_native.FW_OPT_STREAM_BULK, 1 if bulk else 0)
+            self.stream_bulk = bool(bulk)
+
+    @property
+    def stream_shape(self):
+        """The stream step's launch shape as "patch/minb/staged|loads"."""
+        return f"{self.stream_patch}/{self.stream_minb}/{'staged' if self.stream_bulk else 'loads'}"
 
     def set_stream(self, stream_ptr):
         self._native.set_stream(stream_ptr)

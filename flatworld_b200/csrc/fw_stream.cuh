@@ -74,6 +74,7 @@ struct StreamDev {
   StreamElem* elem;  // built from eid/conn by k_stream_elems
   StreamNode* node;  // built from nodes by k_stream_nodes
   int* err;          // != 0: a staged copy did not complete in time
+  const int32_t* list;  // arena worlds: CTA i runs patch list[i] (the active scenes' patches); else patch i
 };
 
 __global__ void k_stream_nodes(Dev d, const int32_t* nodes, StreamNode* out, int n) {
@@ -101,6 +102,24 @@ __global__ void k_stream_elems(Dev d, const int32_t* eid, const uint2* conn, Str
 }
 
 __global__ void k_control(Dev d) { step_control(d); }
+
+// Arena worlds step only the active scenes' patches, so after an odd number
+// of substeps their state sits in the other buffers: copy each listed
+// patch's owned positions (and the J2 state of the triangles it writes) back,
+// so that the first buffers hold every scene's state between calls.
+__global__ void k_stream_carry(StreamDev sd, const float2* __restrict__ x_from, float2* __restrict__ x_to,
+                               const float4* j2_from, float4* j2_to, int has_j2) {
+  const StreamPatch P = sd.patch[sd.list[blockIdx.x]];
+  for (int i = threadIdx.x; i < P.no; i += blockDim.x) {
+    const int g = sd.nodes[P.node_off + i];
+    x_to[g] = x_from[g];
+  }
+  if (has_j2)
+    for (int q = threadIdx.x; q < P.ne; q += blockDim.x) {
+      const StreamElem& r = sd.elem[P.elem_off + q];
+      if (r.conn.y >> 16) j2_to[r.e] = j2_from[r.e];
+    }
+}
 
 // One triangle of the patch (element_step on shared positions).
 __device__ __forceinline__ void stream_element(const Dev& d, const float2* sx, float2* sf, int q, int e, uint2 c,
@@ -150,7 +169,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
   float2* sx = reinterpret_cast<float2*>(smem_raw);  // owned, then halo
   float2* sf = sx + (sd.no_max + sd.nh_max);         // 3 per patch triangle
   StreamElem* srec = reinterpret_cast<StreamElem*>(smem_raw + stream_rec_offset(sd.no_max, sd.nh_max, sd.ne_max));
-  const StreamPatch P = sd.patch[blockIdx.x];
+  const StreamPatch P = sd.patch[sd.list ? sd.list[blockIdx.x] : (int)blockIdx.x];
   const int t = threadIdx.x, T = NT;
   const int mode = d.scene_mode[P.scene];
   if (mode == fw::MODE_FROZEN) {  // keep the state: carry it into the other buffers

@@ -77,6 +77,10 @@ struct Dev {
   int32_t* scene_mode_req;
   int32_t* scene_mode;
   int32_t* scene_bad;  // set to 1 when a node of the scene gets a non-finite position or velocity
+  // stream arenas (fw_step_served_budget): substeps each active scene may
+  // still run in this call; a scene whose budget is spent sits the rest out
+  // (null: no budgets)
+  int32_t* scene_budget;
   int32_t* aabb_ring;  // [2][B][4] ordered ints
   int N, E, B, S, P;
   int has_j2;
@@ -122,7 +126,12 @@ namespace {
 __device__ void step_control(const Dev& d) {
   const int t = threadIdx.x;
   for (int s = t; s < d.S; s += blockDim.x) {
-    const int act = d.scene_active[s];
+    int act = d.scene_active[s];
+    if (act && d.scene_budget) {
+      const int left = d.scene_budget[s];
+      if (left <= 0) act = 0;
+      else d.scene_budget[s] = left - 1;
+    }
     const int req = d.scene_mode_req[s];
     d.scene_mode[s] = act ? (req ? fw::MODE_INIT : fw::MODE_STEP) : fw::MODE_FROZEN;
     if (act && req) d.scene_mode_req[s] = 0;
@@ -1047,9 +1056,21 @@ struct fw_ctx {
   struct ArenaScene {
     bool live = false;
     int64_t n0 = 0, nn = 0, e0 = 0, ne = 0, b0 = 0, nb = 0, p0 = 0, np = 0, h0 = 0, nh = 0, o0 = 0, no = 0;
+    // stream arenas: patches, halo nodes, patch triangles, corner-list offsets
+    int64_t pp0 = 0, npp = 0, hh0 = 0, nhh = 0, t0 = 0, nt = 0, cp0 = 0, ncp = 0;
   };
   bool arena = false;
   FreeList fl_nodes, fl_elems, fl_bodies, fl_pairs, fl_heights, fl_occ;
+  // stream arenas (fw_set_path(FW_PATH_STREAM) before fw_arena_init): the
+  // records of each committed scene's patches; owned-node records use the
+  // scene's node range and corner lists its 3 x triangle range
+  bool a_stream = false;
+  FreeList fl_patch, fl_halo, fl_ptri, fl_csrp;
+  int32_t* d_plist = nullptr;     // the active scenes' patches (CTA -> patch)
+  int32_t* d_budget = nullptr;    // fw_step_served_budget: per-scene substep budgets
+  std::vector<int32_t> h_budget;
+  std::vector<int32_t> h_plist;
+  int st_list_n = 0;
   std::vector<ArenaScene> ascenes;
   std::vector<int> free_scene_ids;
   std::vector<int32_t> a_body_scene;
@@ -1293,8 +1314,11 @@ int rebuild_chunks(fw_ctx* c);
 
 int stream_steps(fw_ctx* c, int n);
 
+int arena_stream_steps(fw_ctx* c, int n);
+
 int run_steps(fw_ctx* c, int n) {
   int rc = FW_OK;
+  if (c->arena && c->a_stream) return arena_stream_steps(c, n);
   if (c->arena && (rc = rebuild_chunks(c))) return rc;
   if (c->path == FW_PATH_RESIDENT && c->d.uniform_dt) return launch_resident(c, n);
   if (c->path == FW_PATH_STREAM) return stream_steps(c, n);
@@ -1384,19 +1408,30 @@ int stream_records(fw_ctx* c) {
   return check_kernel(c, "stream records");
 }
 
-// Patches of the stream path: each body cut into patches of at most
-// st_nodes nodes; per patch the owned nodes, the triangles touching them,
-// the halo nodes, local connectivity and the owned nodes' corner lists in the
-// global ascending-element order.
-int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<int32_t>& slot,
-                 const std::vector<float2>& x0, bool has_j2) {
-  const int N = c->N, E = c->E;
+// Patches of the stream path (host side, no context state): each body
+// [noff[b], +ncnt[b]) of a node set cut into patches of at most patch_nodes
+// nodes; per patch the owned nodes, the triangles touching them, the halo
+// nodes, local connectivity and the owned nodes' corner lists in ascending
+// element order.  Ids in the result are those of the input (conn / off /
+// slot); a patch's scene is its first owned node's body's scene.
+struct PatchSet {
+  std::vector<StreamPatch> patches;
+  std::vector<int32_t> rn, rh, re;  // owned nodes, halo nodes, patch triangles
+  std::vector<uint2> rc;            // local corners of each patch triangle
+  std::vector<uint16_t> rcp, rcs;   // corner-list offsets, corner lists
+  int no_max = 1, nh_max = 1, ne_max = 1;
+};
+
+int make_patches(int N, int E, const int32_t* conn, const std::vector<int32_t>& off,
+                 const std::vector<int32_t>& slot, const std::vector<float2>& x0, const std::vector<int32_t>& noff,
+                 const std::vector<int32_t>& ncnt, const std::vector<int32_t>& body_scene, int patch_nodes,
+                 PatchSet& out, std::string& why) {
   std::vector<int> part(N, -1), idx;
   int P = 0;
-  for (int b = 0; b < c->B; ++b) {
-    const int n0 = c->h_noff[b], nn = c->h_ncnt[b];
+  for (size_t b = 0; b < noff.size(); ++b) {
+    const int n0 = noff[b], nn = ncnt[b];
     if (nn <= 0) continue;
-    const int np = (nn + c->st_nodes - 1) / c->st_nodes;
+    const int np = (nn + patch_nodes - 1) / patch_nodes;
     idx.resize(nn);
     for (int k = 0; k < nn; ++k) idx[k] = n0 + k;
     rcb(x0, idx, 0, nn, P, np, part);
@@ -1404,22 +1439,31 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
   }
   std::vector<std::vector<int>> owned(P);
   for (int i = 0; i < N; ++i) {
-    if (part[i] < 0) return fail(c, FW_ERR_ARG, "stream path: node %d belongs to no body", i);
+    if (part[i] < 0) {
+      why = "stream path: node " + std::to_string(i) + " belongs to no body";
+      return FW_ERR_ARG;
+    }
     owned[part[i]].push_back(i);
   }
   std::vector<int> node_scene(N, 0);
-  for (int b = 0; b < c->B; ++b)
-    for (int k = 0; k < c->h_ncnt[b]; ++k) node_scene[c->h_noff[b] + k] = c->h_scene[b];
-  std::vector<StreamPatch> patches(P);
-  std::vector<int32_t> rn, rh, re, rcp;
-  std::vector<uint2> rc;
-  std::vector<uint16_t> rcs;
+  for (size_t b = 0; b < noff.size(); ++b)
+    for (int k = 0; k < ncnt[b]; ++k) node_scene[noff[b] + k] = body_scene[b];
+  std::vector<StreamPatch>& patches = out.patches;
+  patches.assign(P, StreamPatch{});
+  std::vector<int32_t>& rn = out.rn;
+  std::vector<int32_t>& rh = out.rh;
+  std::vector<int32_t>& re = out.re;
+  std::vector<uint2>& rc = out.rc;
+  std::vector<uint16_t>& rcs = out.rcs;
+  std::vector<int32_t> rcp;
   std::vector<int> loc(N, -1), eloc(E, -1);
   int no_max = 1, nh_max = 1, ne_max = 1;
   for (int p = 0; p < P; ++p) {
     const std::vector<int>& ow = owned[p];
-    if ((int)ow.size() > c->st_nodes)
-      return fail(c, FW_ERR_ARG, "stream path: patch larger than %d nodes", c->st_nodes);
+    if ((int)ow.size() > patch_nodes) {
+      why = "stream path: patch larger than " + std::to_string(patch_nodes) + " nodes";
+      return FW_ERR_ARG;
+    }
     std::vector<int> tri;
     for (int n : ow)
       for (int k = off[n]; k < off[n + 1]; ++k) tri.push_back(slot[k] / 3);
@@ -1428,13 +1472,15 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
     std::vector<int> hal;
     for (int e : tri)
       for (int k = 0; k < 3; ++k) {
-        const int n = c->h_conn[3 * e + k];
+        const int n = conn[3 * e + k];
         if (part[n] != p) hal.push_back(n);
       }
     std::sort(hal.begin(), hal.end());
     hal.erase(std::unique(hal.begin(), hal.end()), hal.end());
-    if (ow.size() + hal.size() >= 65536 || 3 * tri.size() >= 65536)
-      return fail(c, FW_ERR_ARG, "stream path: patch too large for 16-bit local indices");
+    if (ow.size() + hal.size() >= 65536 || 3 * tri.size() >= 65536) {
+      why = "stream path: patch too large for 16-bit local indices";
+      return FW_ERR_ARG;
+    }
     StreamPatch& sp = patches[p];
     sp.node_off = (int)rn.size();
     sp.no = (int)ow.size();
@@ -1457,8 +1503,8 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
       const int e = tri[q];
       eloc[e] = q;
       re.push_back(e);
-      const uint32_t a = loc[c->h_conn[3 * e]], b = loc[c->h_conn[3 * e + 1]], cc = loc[c->h_conn[3 * e + 2]];
-      const uint32_t writer = part[c->h_conn[3 * e]] == p ? 1u : 0u;
+      const uint32_t a = loc[conn[3 * e]], b = loc[conn[3 * e + 1]], cc = loc[conn[3 * e + 2]];
+      const uint32_t writer = part[conn[3 * e]] == p ? 1u : 0u;
       rc.push_back(make_uint2(a | (b << 16), cc | (writer << 16)));
     }
     int cnt = 0;
@@ -1471,7 +1517,10 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
       }
     }
     rcp.push_back((int32_t)cnt);
-    if (cnt >= 65536) return fail(c, FW_ERR_ARG, "stream path: patch corner list too long");
+    if (cnt >= 65536) {
+      why = "stream path: patch corner list too long";
+      return FW_ERR_ARG;
+    }
     for (int n : ow) loc[n] = -1;
     for (int n : hal) loc[n] = -1;
     for (int e : tri) eloc[e] = -1;
@@ -1479,7 +1528,28 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
     nh_max = std::max(nh_max, sp.nh);
     ne_max = std::max(ne_max, sp.ne);
   }
-  std::vector<uint16_t> rcp16(rcp.begin(), rcp.end());
+  out.rcp.assign(rcp.begin(), rcp.end());
+  out.no_max = no_max;
+  out.nh_max = nh_max;
+  out.ne_max = ne_max;
+  return FW_OK;
+}
+
+// Stream path of a finalized world: its patches, device arrays and records.
+int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<int32_t>& slot,
+                 const std::vector<float2>& x0, bool has_j2) {
+  const int N = c->N, E = c->E;
+  PatchSet ps;
+  std::string why;
+  if (make_patches(N, E, c->h_conn.data(), off, slot, x0, c->h_noff, c->h_ncnt, c->h_scene, c->st_nodes, ps, why))
+    return fail(c, FW_ERR_ARG, "%s", why.c_str());
+  const int P = (int)ps.patches.size();
+  const std::vector<StreamPatch>& patches = ps.patches;
+  const std::vector<int32_t>&rn = ps.rn, &rh = ps.rh, &re = ps.re;
+  const std::vector<uint2>& rc = ps.rc;
+  const std::vector<uint16_t>& rcs = ps.rcs;
+  const int no_max = ps.no_max, nh_max = ps.nh_max, ne_max = ps.ne_max;
+  const std::vector<uint16_t>& rcp16 = ps.rcp;
   int r;
   StreamPatch* dp = nullptr;
   int32_t *dn = nullptr, *dh = nullptr, *de = nullptr;
@@ -1827,6 +1897,267 @@ int set_scene_dt(fw_ctx* c, const float* dt) {
   return FW_OK;
 }
 
+// Relocation of one committed scene's arrays from scene-local to arena ids
+// (fw_arena_commit_pack uploads them as packed).
+struct ArenaReloc {
+  int n0, e0, b0, p0, h0, o0, s;
+  int Ns, Es, Bs, Np;
+  int32_t* rn;  // stream arenas: the scene's owned-node, halo and triangle id ranges (else null)
+  int32_t* rh;
+  int32_t* re;
+  int Hs, Ts;
+  int64_t count;  // max of the counts above and 3 Es
+};
+
+__global__ void k_arena_reloc(Dev d, ArenaReloc r) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r.count; i += stride) {
+    if (i < r.Ns) {
+      const int64_t g = r.n0 + i;
+      d.node_word[g] += (uint32_t)r.b0 << fw::NODE_BODY_SHIFT;
+      d.csr_off[g] += 3 * r.e0;
+      d.csr_end[g] += 3 * r.e0;
+      if (r.rn) r.rn[i] += r.n0;
+    }
+    if (i < 3 * (int64_t)r.Es) {
+      const int64_t q = 3 * (int64_t)r.e0 + i;
+      d.csr_slot[q] += 3 * r.e0;
+      d.corner_pos[q] += 3 * r.e0;
+      d.conn[q] += r.n0;
+    }
+    if (i < r.Es) d.emat[r.e0 + i].word += r.b0 << 2;
+    if (i < r.Bs) {
+      d.body_pair_off[r.b0 + i] += r.p0;
+      d.body_scene[r.b0 + i] = r.s;
+    }
+    if (i < r.Np) {
+      Pair& pr = d.pairs[r.p0 + i];
+      pr.body += r.b0;
+      if (pr.kind == fw::PAIR_HEIGHTFIELD) pr.table += r.h0;
+      if (pr.kind == fw::PAIR_VOXEL) pr.table += r.o0;
+    }
+    if (r.rh && i < r.Hs) r.rh[i] += r.n0;
+    if (r.re && i < r.Ts) r.re[i] += r.e0;
+  }
+}
+
+// Shared memory of a stream launch for the given patch maxima.
+void stream_smem(int no_max, int nh_max, int ne_max, size_t* plain, size_t* bulk) {
+  *plain = sizeof(float2) * (size_t)(no_max + nh_max) + sizeof(float2) * 3 * (size_t)ne_max;
+  *bulk = stream_rec_offset(no_max, nh_max, ne_max) + sizeof(StreamElem) * (size_t)ne_max;
+}
+
+// Every built stream kernel of a patch size may use the device's opt-in shared memory.
+int stream_attrs(fw_ctx* c, int optin) {
+  for (int minb : {8, 16, 32})
+    for (int bulk = 0; bulk < 2; ++bulk)
+      if (StreamKernel k = stream_kernel(c->st_nodes, minb, bulk))
+        FW_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 64));
+  return FW_OK;
+}
+
+// n substeps of a stream arena: k_control + k_stream over the active scenes'
+// patches each, then (n odd) the carry back into the first buffers.
+int arena_stream_steps(fw_ctx* c, int n) {
+  if (c->chunks_dirty) {
+    c->h_plist.clear();
+    for (size_t s2 = 0; s2 < c->ascenes.size(); ++s2) {
+      const fw_ctx::ArenaScene& a = c->ascenes[s2];
+      if (!a.live || !c->cur_active[s2]) continue;
+      for (int64_t k = 0; k < a.npp; ++k) c->h_plist.push_back((int32_t)(a.pp0 + k));
+    }
+    if (!c->h_plist.empty())
+      FW_CUDA(c, cudaMemcpyAsync(c->d_plist, c->h_plist.data(), sizeof(int32_t) * c->h_plist.size(),
+                                 cudaMemcpyHostToDevice, c->stream));  // staged before the call returns
+    c->st_list_n = (int)c->h_plist.size();
+    c->chunks_dirty = false;
+  }
+  c->host_counter += n;
+  if (c->st_list_n == 0 || n <= 0) return FW_OK;
+  float2 *xa = c->d.x, *xb = c->d.x_alt;
+  float4 *ja = c->d.j2state, *jb = c->d.j2_alt;
+  const StreamKernel k = stream_kernel(c->st_nodes, c->st_minb, c->st_bulk);
+  const size_t smem = c->st_bulk ? c->st_smem_bulk : c->st_smem;
+  for (int j = 0; j < n; ++j) {
+    k_control<<<1, kMaxBlock, 0, c->stream>>>(c->d);
+    k<<<c->st_list_n, c->st_nodes, smem, c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
+    std::swap(xa, xb);
+    std::swap(ja, jb);
+  }
+  c->launches += 2 * (int64_t)n;
+  if (n & 1) {
+    k_stream_carry<<<c->st_list_n, c->st_nodes, 0, c->stream>>>(c->sd, xa, xb, ja, jb, c->d.has_j2);
+    c->launches += 1;
+  }
+  return check_kernel(c, "arena stream step");
+}
+
+}  // namespace
+
+// Host image of one staged scene with ids local to the scene (fw_arena_pack):
+// every array an arena holds per scene, laid out in one host block (page-
+// locked when asked for, so that a commit's copies run asynchronously).
+struct fw_pack {
+  enum Part {
+    X0, V0, BCV, WORD, CBEG, CEND, SLOT, CPOS, CONN, EMAT, J2PAR, YOUNG, POISSON, RHO, POFF, PCNT, PAIRS,
+    HEIGHTS, OCC, RN, RH, RE, RC, RCP, RCS, NPARTS
+  };
+  int64_t Ns = 0, Es = 0, Bs = 0, Np = 0, Nh = 0, No = 0;
+  int64_t Ps = 0, Hs = 0, Ts = 0, CPs = 0;  // stream records (patch_nodes > 0)
+  int patch_nodes = 0;
+  int no_max = 0, nh_max = 0, ne_max = 0;
+  float damp = 0.f;
+  std::vector<StreamPatch> patches;  // offsets local to the scene's record ranges
+  unsigned char* block = nullptr;
+  bool pinned = false;
+  size_t off[NPARTS] = {}, len[NPARTS] = {};
+  int64_t dev_bytes = 0;
+  const void* at(Part p) const { return block + off[p]; }
+  ~fw_pack() {
+    if (pinned) cudaFreeHost(block);
+    else free(block);
+  }
+};
+
+namespace {
+
+// The scene staged on context c (fw_set_nodes / fw_set_elements /
+// fw_set_bodies / fw_set_scenes(1, ...) / fw_add_*_pair, ids local to the
+// scene) as a pack; the stage is cleared.  Host work only.
+int build_pack(fw_ctx* c, int patch_nodes, bool pinned, fw_pack** out) {
+  const int64_t Ns = (int64_t)c->h_x.size() / 2, Es = (int64_t)c->h_conn.size() / 3;
+  const int Bs = (int)c->h_noff.size();
+  if (Ns <= 0 || Es <= 0 || Bs <= 0) return fail(c, FW_ERR_ARG, "fw_arena_pack: nothing staged");
+  for (int b = 0; b < Bs; ++b)
+    if (c->h_scene[b] != 0) return fail(c, FW_ERR_ARG, "fw_arena_pack: stage exactly one scene (scene 0)");
+  if (patch_nodes != 0 && patch_nodes != 64 && patch_nodes != 128)
+    return fail(c, FW_ERR_ARG, "fw_arena_pack: patch_nodes must be 0, 64 or 128");
+  if (c->has_springs || !c->h_flex.empty() || !c->h_rigid.empty())
+    return fail(c, FW_ERR_ARG, "fw_arena_pack: arena scenes hold FEM triangles and ground pairs only");
+  std::vector<int32_t> node_body(Ns, -1), elem_body(Es, -1);
+  for (int b = 0; b < Bs; ++b) {
+    if (c->h_noff[b] < 0 || c->h_noff[b] + (int64_t)c->h_ncnt[b] > Ns || c->h_eoff[b] < 0 ||
+        c->h_eoff[b] + (int64_t)c->h_ecnt[b] > Es)
+      return fail(c, FW_ERR_ARG, "fw_arena_pack: body %d range out of bounds", b);
+    for (int i = c->h_noff[b]; i < c->h_noff[b] + c->h_ncnt[b]; ++i) node_body[i] = b;
+    for (int e = c->h_eoff[b]; e < c->h_eoff[b] + c->h_ecnt[b]; ++e) elem_body[e] = b;
+  }
+  for (int64_t e = 0; e < Es; ++e)
+    for (int k = 0; k < 3; ++k) {
+      const int n = c->h_conn[3 * e + k];
+      if (elem_body[e] < 0 || n < 0 || n >= Ns || node_body[n] != elem_body[e])
+        return fail(c, FW_ERR_ARG, "fw_arena_pack: element %lld has a bad node id", (long long)e);
+    }
+  for (int64_t i = 0; i < Ns; ++i)
+    if (node_body[i] < 0) return fail(c, FW_ERR_ARG, "fw_arena_pack: node %lld belongs to no body", (long long)i);
+  // node records (body ids local; the commit adds the scene's first body)
+  std::vector<uint32_t> word(Ns);
+  std::vector<float2> x0(Ns), v0(Ns), bcv(Ns);
+  for (int64_t i = 0; i < Ns; ++i) {
+    word[i] = (uint32_t)c->h_bc[i] | ((uint32_t)node_body[i] << fw::NODE_BODY_SHIFT);
+    x0[i] = make_float2(c->h_x[2 * i], c->h_x[2 * i + 1]);
+    v0[i] = make_float2(c->h_v[2 * i], c->h_v[2 * i + 1]);
+    bcv[i] = make_float2(c->h_bcv[2 * i], c->h_bcv[2 * i + 1]);
+  }
+  for (int b = 0; b < Bs; ++b)
+    for (int k = 0; k < c->h_bncnt[b]; ++k) word[c->h_bnodes[c->h_bnoff[b] + k]] |= fw::NODE_BOUNDARY;
+  // triangles and the corner lists (ascending element per node)
+  std::vector<int32_t> conn(c->h_conn.begin(), c->h_conn.end()), cbeg(Ns), cend(Ns), slot(3 * Es), cpos(3 * Es);
+  std::vector<ElemMat> emat(Es);
+  std::vector<float2> j2par(Es);
+  for (int64_t e = 0; e < Es; ++e) {
+    emat[e].area = emat[e].lam = emat[e].mu = 0.f;
+    emat[e].word = (c->h_type[e] & 3) | (elem_body[e] << 2);
+    j2par[e] = make_float2(c->h_sy[e], c->h_H[e]);
+  }
+  std::vector<int32_t> off(Ns + 1, 0);
+  for (int64_t e = 0; e < Es; ++e)
+    for (int k = 0; k < 3; ++k) off[conn[3 * e + k] + 1]++;
+  for (int64_t i = 0; i < Ns; ++i) off[i + 1] += off[i];
+  {
+    std::vector<int32_t> fill(off.begin(), off.end() - 1);
+    for (int64_t e = 0; e < Es; ++e)
+      for (int k = 0; k < 3; ++k) {
+        const int32_t at = fill[conn[3 * e + k]]++;
+        slot[at] = (int32_t)(3 * e + k);
+        cpos[3 * e + k] = at;
+      }
+    for (int64_t i = 0; i < Ns; ++i) {
+      cbeg[i] = off[i];
+      cend[i] = off[i + 1];
+    }
+  }
+  // contact pairs grouped by body (stable: staging order within a body)
+  std::vector<Pair> pairs = c->h_pairs;
+  std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x.body < y.body; });
+  std::vector<int32_t> poff(Bs, 0), pcnt(Bs, 0);
+  for (const Pair& pr : pairs) {
+    if (pr.body < 0 || pr.body >= Bs) return fail(c, FW_ERR_ARG, "fw_arena_pack: pair body out of range");
+    pcnt[pr.body]++;
+  }
+  for (int b = 1; b < Bs; ++b) poff[b] = poff[b - 1] + pcnt[b - 1];
+  // stream records
+  PatchSet ps;
+  if (patch_nodes) {
+    std::string why;
+    std::vector<int32_t> bscene(Bs, 0);
+    if (make_patches((int)Ns, (int)Es, conn.data(), off, slot, x0, c->h_noff, c->h_ncnt, bscene, patch_nodes, ps, why))
+      return fail(c, FW_ERR_ARG, "%s", why.c_str());
+  }
+  fw_pack* pk = new fw_pack();
+  pk->Ns = Ns; pk->Es = Es; pk->Bs = Bs; pk->Np = (int64_t)pairs.size();
+  pk->Nh = (int64_t)c->h_heights.size(); pk->No = (int64_t)c->h_occ.size();
+  pk->damp = c->h_damp.empty() ? 0.f : c->h_damp[0];
+  pk->patch_nodes = patch_nodes;
+  pk->Ps = (int64_t)ps.patches.size(); pk->Hs = (int64_t)ps.rh.size(); pk->Ts = (int64_t)ps.re.size();
+  pk->CPs = (int64_t)ps.rcp.size();
+  pk->no_max = ps.no_max; pk->nh_max = ps.nh_max; pk->ne_max = ps.ne_max;
+  pk->patches = ps.patches;
+  struct Src { const void* p; size_t bytes; };
+  const Src src[fw_pack::NPARTS] = {
+      {x0.data(), sizeof(float2) * Ns}, {v0.data(), sizeof(float2) * Ns}, {bcv.data(), sizeof(float2) * Ns},
+      {word.data(), sizeof(uint32_t) * Ns}, {cbeg.data(), sizeof(int32_t) * Ns}, {cend.data(), sizeof(int32_t) * Ns},
+      {slot.data(), sizeof(int32_t) * 3 * Es}, {cpos.data(), sizeof(int32_t) * 3 * Es},
+      {conn.data(), sizeof(int32_t) * 3 * Es}, {emat.data(), sizeof(ElemMat) * Es}, {j2par.data(), sizeof(float2) * Es},
+      {c->h_E.data(), sizeof(float) * Es}, {c->h_nu.data(), sizeof(float) * Es}, {c->h_rho.data(), sizeof(float) * Es},
+      {poff.data(), sizeof(int32_t) * Bs}, {pcnt.data(), sizeof(int32_t) * Bs}, {pairs.data(), sizeof(Pair) * pairs.size()},
+      {c->h_heights.data(), sizeof(float) * c->h_heights.size()}, {c->h_occ.data(), c->h_occ.size()},
+      {ps.rn.data(), sizeof(int32_t) * ps.rn.size()}, {ps.rh.data(), sizeof(int32_t) * ps.rh.size()},
+      {ps.re.data(), sizeof(int32_t) * ps.re.size()}, {ps.rc.data(), sizeof(uint2) * ps.rc.size()},
+      {ps.rcp.data(), sizeof(uint16_t) * ps.rcp.size()}, {ps.rcs.data(), sizeof(uint16_t) * ps.rcs.size()}};
+  size_t total = 0;
+  for (int k = 0; k < fw_pack::NPARTS; ++k) {
+    pk->off[k] = total;
+    pk->len[k] = src[k].bytes;
+    total += (src[k].bytes + 15) & ~(size_t)15;
+  }
+  if (pinned && cudaHostAlloc((void**)&pk->block, total ? total : 16, cudaHostAllocDefault) == cudaSuccess) {
+    pk->pinned = true;
+  } else {
+    cudaGetLastError();
+    pk->block = (unsigned char*)malloc(total ? total : 16);
+    if (!pk->block) {
+      delete pk;
+      return fail(c, FW_ERR_OOM, "fw_arena_pack: host allocation of %zu bytes failed", total);
+    }
+  }
+  for (int k = 0; k < fw_pack::NPARTS; ++k)
+    if (src[k].bytes) memcpy(pk->block + pk->off[k], src[k].p, src[k].bytes);
+  // device bytes of the scene's ranges
+  int64_t dev = 48 * Ns + 136 * Es + 64 * pk->Np + 4 * pk->Nh + pk->No;
+  if (patch_nodes)
+    dev += (int64_t)sizeof(StreamPatch) * pk->Ps + 4 * pk->Hs + (4 + 8 + (int64_t)sizeof(StreamElem)) * pk->Ts +
+           2 * pk->CPs + 6 * Es + (4 + (int64_t)sizeof(StreamNode)) * Ns;
+  pk->dev_bytes = dev;
+  // clear the stage for the next scene
+  c->h_x.clear(); c->h_v.clear(); c->h_bc.clear(); c->h_bcv.clear();
+  c->h_conn.clear(); c->h_type.clear(); c->h_E.clear(); c->h_nu.clear(); c->h_rho.clear(); c->h_sy.clear(); c->h_H.clear();
+  c->h_noff.clear(); c->h_ncnt.clear(); c->h_eoff.clear(); c->h_ecnt.clear(); c->h_scene.clear();
+  c->h_bnoff.clear(); c->h_bncnt.clear(); c->h_bnodes.clear(); c->h_pairs.clear(); c->h_heights.clear(); c->h_occ.clear();
+  *out = pk;
+  return FW_OK;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -1851,8 +2182,20 @@ int fw_create(fw_ctx** out, int device) {
   return FW_OK;
 }
 
+int fw_create_stage(fw_ctx** out) {
+  if (!out) return FW_ERR_ARG;
+  fw_ctx* c = new fw_ctx();
+  c->device = -1;  // staging only: no device, no stream
+  *out = c;
+  return FW_OK;
+}
+
 void fw_destroy(fw_ctx* c) {
   if (!c) return;
+  if (c->device < 0) {
+    delete c;
+    return;
+  }
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
@@ -2455,6 +2798,7 @@ int build_flex(fw_ctx* c) {
 
 int fw_finalize(fw_ctx* c) {
   if (!c) return FW_ERR_ARG;
+  if (c->device < 0) return fail(c, FW_ERR_STATE, "fw_finalize on a staging context (fw_create_stage)");
   if (c->finalized) return fail(c, FW_ERR_STATE, "fw_finalize called twice");
   if (c->N <= 0 || c->E <= 0 || c->B <= 0 || c->S <= 0)
     return fail(c, FW_ERR_STATE, "fw_finalize: nodes, elements, bodies and scenes must be set");
@@ -2854,6 +3198,7 @@ int fw_restore(fw_ctx* c, int32_t slot) {
 int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_bodies, int32_t max_scenes,
                   int32_t max_pairs, int64_t max_heights, int64_t max_occ) {
   if (!c) return FW_ERR_ARG;
+  if (c->device < 0) return fail(c, FW_ERR_STATE, "fw_arena_init on a staging context (fw_create_stage)");
   if (c->finalized) return fail(c, FW_ERR_STATE, "fw_arena_init on a finalized context");
   if (max_nodes <= 0 || max_elems <= 0 || max_bodies <= 0 || max_scenes <= 0 || max_pairs < 0 ||
       max_heights < 0 || max_occ < 0)
@@ -2919,156 +3264,192 @@ int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_b
   c->finalized = true;
   c->path = FW_PATH_GATHER;
   c->chunks_dirty = true;
+  if (c->path_req == FW_PATH_STREAM) {
+    // stream arena: record capacities (patches of a body: at most nodes / patch + 1;
+    // patch triangles and halo nodes: at most twice the triangles / nodes, a
+    // scene needing more waits like any scene that does not fit)
+    const int64_t Pcap = N / c->st_nodes + B + 16, Hcap = 2 * N, Tcap = 2 * E, CPcap = N + Pcap;
+    StreamPatch* dp = nullptr;
+    int32_t *dn = nullptr, *dh = nullptr, *de = nullptr;
+    uint2* dc = nullptr;
+    uint16_t *dcp = nullptr, *dcs = nullptr;
+    StreamElem* dse = nullptr;
+    StreamNode* dsn = nullptr;
+    int* derr = nullptr;
+    if ((rc = dalloc(c, &dp, Pcap)) || (rc = dalloc(c, &dn, N)) || (rc = dalloc(c, &dh, Hcap)) ||
+        (rc = dalloc(c, &de, Tcap)) || (rc = dalloc(c, &dc, Tcap)) || (rc = dalloc(c, &dcp, CPcap)) ||
+        (rc = dalloc(c, &dcs, 3 * E)) || (rc = dalloc(c, &dse, Tcap)) || (rc = dalloc(c, &dsn, N)) ||
+        (rc = dalloc(c, &derr, 1)) || (rc = dalloc(c, &c->d_plist, Pcap)) || (rc = dalloc(c, &c->d_budget, S)) ||
+        (rc = dalloc(c, &d.x_alt, N)) ||
+        (rc = dalloc(c, &d.j2_alt, E)))
+      return rc;
+    FW_CUDA(c, cudaMemsetAsync(derr, 0, sizeof(int), c->stream));
+    c->sd = StreamDev{dp, dn, dh, de, dc, dcp, dcs, 1, 1, 1, dse, dsn, derr, c->d_plist};
+    c->fl_patch.init(Pcap);
+    c->fl_halo.init(Hcap);
+    c->fl_ptri.init(Tcap);
+    c->fl_csrp.init(CPcap);
+    stream_smem(1, 1, 1, &c->st_smem, &c->st_smem_bulk);
+    if ((rc = stream_attrs(c, shared_optin(c)))) return rc;
+    c->st_list_n = 0;
+    c->x_buf0 = d.x;
+    c->a_stream = true;
+    c->path = FW_PATH_STREAM;
+    FW_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   c->h_x.clear(); c->h_conn.clear(); c->h_pairs.clear(); c->h_heights.clear(); c->h_occ.clear();
+  return FW_OK;
+}
+
+int fw_arena_pack(fw_ctx* stage, int32_t patch_nodes, int32_t flags, fw_pack** out) {
+  if (!stage || !out) return FW_ERR_ARG;
+  *out = nullptr;
+  if (stage->finalized && !stage->arena)
+    return fail(stage, FW_ERR_STATE, "fw_arena_pack: stage on a context that is not finalized, or on an arena");
+  return build_pack(stage, patch_nodes, (flags & FW_PACK_PINNED) != 0, out);
+}
+
+int fw_pack_info(const fw_pack* pk, int64_t* info) {
+  if (!pk || !info) return FW_ERR_ARG;
+  info[0] = pk->dev_bytes; info[1] = pk->Ns; info[2] = pk->Es; info[3] = pk->Bs;
+  info[4] = pk->patch_nodes; info[5] = pk->Ps; info[6] = pk->Ts; info[7] = pk->pinned ? 1 : 0;
+  return FW_OK;
+}
+
+void fw_pack_destroy(fw_pack* pk) { delete pk; }
+
+int fw_arena_commit_pack(fw_ctx* c, const fw_pack* pk, int32_t* scene_out) {
+  if (!c || !pk || !scene_out) return FW_ERR_ARG;
+  if (!c->arena) return fail(c, FW_ERR_STATE, "fw_arena_commit_pack without fw_arena_init");
+  if (c->a_stream && pk->patch_nodes != c->st_nodes)
+    return fail(c, FW_ERR_ARG, "fw_arena_commit_pack: the pack is cut into %d-node patches, the arena steps %d-node "
+                               "patches", pk->patch_nodes, c->st_nodes);
+  if (c->free_scene_ids.empty()) return fail(c, FW_ERR_OOM, "arena: no free scene slot");
+  fw_ctx::ArenaScene a;
+  a.nn = pk->Ns; a.ne = pk->Es; a.nb = pk->Bs; a.np = pk->Np; a.nh = pk->Nh; a.no = pk->No;
+  if (c->a_stream) { a.npp = pk->Ps; a.nhh = pk->Hs; a.nt = pk->Ts; a.ncp = pk->CPs; }
+  fw_ctx::FreeList* lists[10] = {&c->fl_nodes, &c->fl_elems, &c->fl_bodies, &c->fl_pairs, &c->fl_heights,
+                                 &c->fl_occ, &c->fl_patch, &c->fl_halo, &c->fl_ptri, &c->fl_csrp};
+  int64_t* offs[10] = {&a.n0, &a.e0, &a.b0, &a.p0, &a.h0, &a.o0, &a.pp0, &a.hh0, &a.t0, &a.cp0};
+  const int64_t lens[10] = {a.nn, a.ne, a.nb, a.np, a.nh, a.no, a.npp, a.nhh, a.nt, a.ncp};
+  const int nl = c->a_stream ? 10 : 6;
+  for (int k = 0; k < nl; ++k)
+    if (!lists[k]->take(lens[k], offs[k])) {
+      for (int j = 0; j < k; ++j) lists[j]->give(*offs[j], lens[j]);
+      return fail(c, FW_ERR_OOM, "arena: not enough free capacity for this scene");
+    }
+  // stream arenas: the launch's shared memory covers the largest patch so far
+  int no_max = c->sd.no_max, nh_max = c->sd.nh_max, ne_max = c->sd.ne_max;
+  size_t smem = c->st_smem, smem_bulk = c->st_smem_bulk;
+  if (c->a_stream) {
+    no_max = std::max(no_max, pk->no_max);
+    nh_max = std::max(nh_max, pk->nh_max);
+    ne_max = std::max(ne_max, pk->ne_max);
+    stream_smem(no_max, nh_max, ne_max, &smem, &smem_bulk);
+    if ((long)smem > shared_optin(c) - 64) {
+      for (int j = 0; j < nl; ++j) lists[j]->give(*offs[j], lens[j]);
+      return fail(c, FW_ERR_ARG, "arena: a patch of this scene needs %zu B of shared memory", smem);
+    }
+  }
+  const int s = c->free_scene_ids.back();
+  c->free_scene_ids.pop_back();
+  a.live = true;
+  // upload (queued on the stream: the steps that follow see the scene, and a
+  // pinned pack's copies run asynchronously)
+  Dev& d = c->d;
+  auto up = [&](void* dst, fw_pack::Part part) -> int {
+    if (!pk->len[part]) return FW_OK;
+    FW_CUDA(c, cudaMemcpyAsync(dst, pk->at(part), pk->len[part], cudaMemcpyHostToDevice, c->stream));
+    return FW_OK;
+  };
+  const int64_t n0 = a.n0, e0 = a.e0;
+  int rc;
+  if ((rc = up(d.x0 + n0, fw_pack::X0)) || (rc = up(d.x + n0, fw_pack::X0)) || (rc = up(d.v + n0, fw_pack::V0)) ||
+      (rc = up(d.bcv + n0, fw_pack::BCV)) || (rc = up(d.node_word + n0, fw_pack::WORD)) ||
+      (rc = up(d.csr_off + n0, fw_pack::CBEG)) || (rc = up(d.csr_end + n0, fw_pack::CEND)) ||
+      (rc = up(d.csr_slot + 3 * e0, fw_pack::SLOT)) || (rc = up(d.corner_pos + 3 * e0, fw_pack::CPOS)) ||
+      (rc = up(d.conn + 3 * e0, fw_pack::CONN)) || (rc = up(d.emat + e0, fw_pack::EMAT)) ||
+      (rc = up(d.j2par + e0, fw_pack::J2PAR)) || (rc = up(c->a_young + e0, fw_pack::YOUNG)) ||
+      (rc = up(c->a_poisson + e0, fw_pack::POISSON)) || (rc = up(c->a_rho + e0, fw_pack::RHO)) ||
+      (rc = up(d.body_pair_off + a.b0, fw_pack::POFF)) || (rc = up(d.body_pair_cnt + a.b0, fw_pack::PCNT)) ||
+      (rc = up(d.pairs + a.p0, fw_pack::PAIRS)) || (rc = up(d.heights + a.h0, fw_pack::HEIGHTS)) ||
+      (rc = up(d.occ + a.o0, fw_pack::OCC)))
+    return rc;
+  FW_CUDA(c, cudaMemsetAsync(d.j2state + e0, 0, sizeof(float4) * a.ne, c->stream));
+  ArenaReloc r{};
+  r.n0 = (int)n0; r.e0 = (int)e0; r.b0 = (int)a.b0; r.p0 = (int)a.p0; r.h0 = (int)a.h0; r.o0 = (int)a.o0; r.s = s;
+  r.Ns = (int)a.nn; r.Es = (int)a.ne; r.Bs = (int)a.nb; r.Np = (int)a.np;
+  if (c->a_stream) {
+    int32_t* rn = const_cast<int32_t*>(c->sd.nodes) + n0;
+    int32_t* rh = const_cast<int32_t*>(c->sd.halo) + a.hh0;
+    int32_t* re = const_cast<int32_t*>(c->sd.eid) + a.t0;
+    std::vector<StreamPatch> pat = pk->patches;
+    for (StreamPatch& sp : pat) {
+      sp.node_off += (int)n0;
+      sp.halo_off += (int)a.hh0;
+      sp.elem_off += (int)a.t0;
+      sp.csrp_off += (int)a.cp0;
+      sp.csr_off += (int)(3 * e0);
+      sp.scene = s;
+    }
+    if (!pat.empty())
+      FW_CUDA(c, cudaMemcpyAsync(const_cast<StreamPatch*>(c->sd.patch) + a.pp0, pat.data(),
+                                 sizeof(StreamPatch) * pat.size(), cudaMemcpyHostToDevice, c->stream));
+    if ((rc = up(rn, fw_pack::RN)) || (rc = up(rh, fw_pack::RH)) || (rc = up(re, fw_pack::RE)) ||
+        (rc = up(const_cast<uint2*>(c->sd.conn) + a.t0, fw_pack::RC)) ||
+        (rc = up(const_cast<uint16_t*>(c->sd.csrp) + a.cp0, fw_pack::RCP)) ||
+        (rc = up(const_cast<uint16_t*>(c->sd.csrs) + 3 * e0, fw_pack::RCS)))
+      return rc;
+    r.rn = rn; r.rh = rh; r.re = re; r.Hs = (int)a.nhh; r.Ts = (int)a.nt;
+  }
+  r.count = std::max<int64_t>({3 * a.ne, a.nn, a.nb, a.np, a.nhh, a.nt});
+  k_arena_reloc<<<(int)std::min<int64_t>((r.count + kBlock - 1) / kBlock, 8 * c->sms), kBlock, 0, c->stream>>>(d, r);
+  const int e_lo = (int)e0, e_hi = (int)(e0 + a.ne), n_lo = (int)n0, n_hi = (int)(n0 + a.nn);
+  k_prepare_elements<<<(int)((a.ne + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->a_young + e0, c->a_poisson + e0,
+                                                                                  c->a_rho + e0, e_lo, e_hi);
+  k_prepare_mass<<<(int)((a.nn + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, n_lo, n_hi);
+  c->launches += 3;
+  if (c->a_stream) {
+    if (a.nt > 0)
+      k_stream_elems<<<(int)((a.nt + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->sd.eid + a.t0,
+                                                                                    c->sd.conn + a.t0,
+                                                                                    c->sd.elem + a.t0, (int)a.nt);
+    k_stream_nodes<<<(int)((a.nn + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->sd.nodes + n0,
+                                                                                  c->sd.node + n0, (int)a.nn);
+    c->launches += 2;
+    c->sd.no_max = no_max; c->sd.nh_max = nh_max; c->sd.ne_max = ne_max;
+    c->st_smem = smem;
+    c->st_smem_bulk = smem_bulk;
+    if ((long)smem_bulk > shared_optin(c) - 64) c->st_bulk = 0;  // staging no longer fits: plain loads
+  }
+  const float damp = pk->damp;
+  const int32_t one = 1, zero = 0;
+  auto up1 = [&](void* dst, const void* v) -> int {
+    FW_CUDA(c, cudaMemcpyAsync(dst, v, 4, cudaMemcpyHostToDevice, c->stream));  // staged before the call returns
+    return FW_OK;
+  };
+  if ((rc = up1(d.scene_damp + s, &damp)) || (rc = up1(d.scene_counter + s, &zero)) ||
+      (rc = up1(d.scene_mode_req + s, &one)) || (rc = up1(d.scene_active + s, &one)) ||
+      (rc = up1(d.scene_bad + s, &zero)))
+    return rc;
+  if ((rc = check_kernel(c, "arena commit"))) return rc;
+  c->ascenes[s] = a;
+  for (int64_t b = 0; b < a.nb; ++b) c->a_body_scene[a.b0 + b] = s;
+  c->cur_active[s] = 1;
+  c->chunks_dirty = true;
+  *scene_out = s;
   return FW_OK;
 }
 
 int fw_arena_commit(fw_ctx* c, int32_t* scene_out) {
   if (!c || !scene_out) return FW_ERR_ARG;
   if (!c->arena) return fail(c, FW_ERR_STATE, "fw_arena_commit without fw_arena_init");
-  // staged by fw_set_nodes / fw_set_elements / fw_set_bodies / fw_add_*_pair (local ids)
-  const int64_t Ns = (int64_t)c->h_x.size() / 2, Es = (int64_t)c->h_conn.size() / 3;
-  const int Bs = (int)c->h_noff.size();
-  if (Ns <= 0 || Es <= 0 || Bs <= 0) return fail(c, FW_ERR_ARG, "fw_arena_commit: nothing staged");
-  for (int b = 0; b < Bs; ++b)
-    if (c->h_scene[b] != 0) return fail(c, FW_ERR_ARG, "fw_arena_commit: stage exactly one scene (scene 0)");
-  // validate local ranges
-  std::vector<int32_t> node_body(Ns, -1), elem_body(Es, -1);
-  for (int b = 0; b < Bs; ++b) {
-    if (c->h_noff[b] < 0 || c->h_noff[b] + (int64_t)c->h_ncnt[b] > Ns || c->h_eoff[b] < 0 ||
-        c->h_eoff[b] + (int64_t)c->h_ecnt[b] > Es)
-      return fail(c, FW_ERR_ARG, "fw_arena_commit: body %d range out of bounds", b);
-    for (int i = c->h_noff[b]; i < c->h_noff[b] + c->h_ncnt[b]; ++i) node_body[i] = b;
-    for (int e = c->h_eoff[b]; e < c->h_eoff[b] + c->h_ecnt[b]; ++e) elem_body[e] = b;
-  }
-  for (int64_t e = 0; e < Es; ++e)
-    for (int k = 0; k < 3; ++k) {
-      const int n = c->h_conn[3 * e + k];
-      if (elem_body[e] < 0 || n < 0 || n >= Ns || node_body[n] != elem_body[e])
-        return fail(c, FW_ERR_ARG, "fw_arena_commit: element %lld has a bad node id", (long long)e);
-    }
-  for (int64_t i = 0; i < Ns; ++i)
-    if (node_body[i] < 0) return fail(c, FW_ERR_ARG, "fw_arena_commit: node %lld belongs to no body", (long long)i);
-  // ranges
-  if (c->free_scene_ids.empty()) return fail(c, FW_ERR_OOM, "arena: no free scene slot");
-  fw_ctx::ArenaScene a;
-  a.nn = Ns; a.ne = Es; a.nb = Bs; a.np = (int64_t)c->h_pairs.size();
-  a.nh = (int64_t)c->h_heights.size(); a.no = (int64_t)c->h_occ.size();
-  fw_ctx::FreeList* lists[6] = {&c->fl_nodes, &c->fl_elems, &c->fl_bodies, &c->fl_pairs, &c->fl_heights, &c->fl_occ};
-  int64_t* offs[6] = {&a.n0, &a.e0, &a.b0, &a.p0, &a.h0, &a.o0};
-  const int64_t lens[6] = {a.nn, a.ne, a.nb, a.np, a.nh, a.no};
-  for (int k = 0; k < 6; ++k)
-    if (!lists[k]->take(lens[k], offs[k])) {
-      for (int j = 0; j < k; ++j) lists[j]->give(*offs[j], lens[j]);
-      return fail(c, FW_ERR_OOM, "arena: not enough free capacity for this scene");
-    }
-  const int s = c->free_scene_ids.back();
-  c->free_scene_ids.pop_back();
-  a.live = true;
-  // pack with global ids
-  std::vector<uint32_t> word(Ns);
-  std::vector<float2> x0(Ns), v0(Ns), bcv(Ns);
-  for (int64_t i = 0; i < Ns; ++i) {
-    word[i] = (uint32_t)c->h_bc[i] | ((uint32_t)(a.b0 + node_body[i]) << fw::NODE_BODY_SHIFT);
-    x0[i] = make_float2(c->h_x[2 * i], c->h_x[2 * i + 1]);
-    v0[i] = make_float2(c->h_v[2 * i], c->h_v[2 * i + 1]);
-    bcv[i] = make_float2(c->h_bcv[2 * i], c->h_bcv[2 * i + 1]);
-  }
-  for (int b = 0; b < Bs; ++b)
-    for (int k = 0; k < c->h_bncnt[b]; ++k) word[c->h_bnodes[c->h_bnoff[b] + k]] |= fw::NODE_BOUNDARY;
-  std::vector<int32_t> conn(3 * Es), cbeg(Ns), cend(Ns), slot(3 * Es), cpos(3 * Es);
-  std::vector<ElemMat> emat(Es);
-  std::vector<float2> j2par(Es);
-  for (int64_t e = 0; e < Es; ++e) {
-    for (int k = 0; k < 3; ++k) conn[3 * e + k] = (int32_t)(a.n0 + c->h_conn[3 * e + k]);
-    emat[e].area = emat[e].lam = emat[e].mu = 0.f;
-    emat[e].word = (c->h_type[e] & 3) | ((int)(a.b0 + elem_body[e]) << 2);
-    j2par[e] = make_float2(c->h_sy[e], c->h_H[e]);
-  }
-  {
-    std::vector<int32_t> cnt(Ns + 1, 0);
-    for (int64_t e = 0; e < Es; ++e)
-      for (int k = 0; k < 3; ++k) cnt[c->h_conn[3 * e + k] + 1]++;
-    for (int64_t i = 0; i < Ns; ++i) cnt[i + 1] += cnt[i];
-    std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
-    for (int64_t e = 0; e < Es; ++e)
-      for (int k = 0; k < 3; ++k) {
-        const int32_t at = fill[c->h_conn[3 * e + k]]++;
-        slot[at] = (int32_t)(3 * (a.e0 + e) + k);
-        cpos[3 * e + k] = (int32_t)(3 * a.e0 + at);
-      }
-    for (int64_t i = 0; i < Ns; ++i) {
-      cbeg[i] = (int32_t)(3 * a.e0 + cnt[i]);
-      cend[i] = (int32_t)(3 * a.e0 + cnt[i + 1]);
-    }
-  }
-  std::vector<Pair> pairs = c->h_pairs;
-  std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x.body < y.body; });
-  std::vector<int32_t> poff(Bs, 0), pcnt(Bs, 0), bscene(Bs, s);
-  for (size_t k = 0; k < pairs.size(); ++k) {
-    if (pairs[k].body < 0 || pairs[k].body >= Bs) return fail(c, FW_ERR_ARG, "fw_arena_commit: pair body out of range");
-    pcnt[pairs[k].body]++;
-  }
-  for (int b = 1; b < Bs; ++b) poff[b] = poff[b - 1] + pcnt[b - 1];
-  for (int b = 0; b < Bs; ++b) poff[b] += (int32_t)a.p0;
-  for (Pair& pr : pairs) {
-    pr.body += (int)a.b0;
-    if (pr.kind == fw::PAIR_HEIGHTFIELD) pr.table += (int)a.h0;
-    if (pr.kind == fw::PAIR_VOXEL) pr.table += (int)a.o0;
-  }
-  // upload
-  Dev& d = c->d;
-  auto up = [&](void* dst, const void* src, size_t bytes) -> int {
-    if (!bytes) return FW_OK;
-    FW_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
-    return FW_OK;
-  };
-  int rc;
-  if ((rc = up(d.x0 + a.n0, x0.data(), sizeof(float2) * Ns)) || (rc = up(d.x + a.n0, x0.data(), sizeof(float2) * Ns)) ||
-      (rc = up(d.v + a.n0, v0.data(), sizeof(float2) * Ns)) || (rc = up(d.bcv + a.n0, bcv.data(), sizeof(float2) * Ns)) ||
-      (rc = up(d.node_word + a.n0, word.data(), sizeof(uint32_t) * Ns)) ||
-      (rc = up(d.csr_off + a.n0, cbeg.data(), sizeof(int32_t) * Ns)) ||
-      (rc = up(d.csr_end + a.n0, cend.data(), sizeof(int32_t) * Ns)) ||
-      (rc = up(d.csr_slot + 3 * a.e0, slot.data(), sizeof(int32_t) * 3 * Es)) ||
-      (rc = up(d.corner_pos + 3 * a.e0, cpos.data(), sizeof(int32_t) * 3 * Es)) ||
-      (rc = up(d.conn + 3 * a.e0, conn.data(), sizeof(int32_t) * 3 * Es)) ||
-      (rc = up(d.emat + a.e0, emat.data(), sizeof(ElemMat) * Es)) ||
-      (rc = up(d.j2par + a.e0, j2par.data(), sizeof(float2) * Es)) ||
-      (rc = up(c->a_young + a.e0, c->h_E.data(), sizeof(float) * Es)) ||
-      (rc = up(c->a_poisson + a.e0, c->h_nu.data(), sizeof(float) * Es)) ||
-      (rc = up(c->a_rho + a.e0, c->h_rho.data(), sizeof(float) * Es)) ||
-      (rc = up(d.body_scene + a.b0, bscene.data(), sizeof(int32_t) * Bs)) ||
-      (rc = up(d.body_pair_off + a.b0, poff.data(), sizeof(int32_t) * Bs)) ||
-      (rc = up(d.body_pair_cnt + a.b0, pcnt.data(), sizeof(int32_t) * Bs)) ||
-      (rc = up(d.pairs + a.p0, pairs.data(), sizeof(Pair) * pairs.size())) ||
-      (rc = up(d.heights + a.h0, c->h_heights.data(), sizeof(float) * a.nh)) ||
-      (rc = up(d.occ + a.o0, c->h_occ.data(), a.no)))
-    return rc;
-  FW_CUDA(c, cudaMemsetAsync(d.j2state + a.e0, 0, sizeof(float4) * Es, c->stream));
-  const float damp = c->h_damp.empty() ? 0.f : c->h_damp[0];
-  const int32_t one = 1, zero = 0;
-  if ((rc = up(d.scene_damp + s, &damp, sizeof(float))) || (rc = up(d.scene_counter + s, &zero, sizeof(int32_t))) ||
-      (rc = up(d.scene_mode_req + s, &one, sizeof(int32_t))) || (rc = up(d.scene_active + s, &one, sizeof(int32_t))) ||
-      (rc = up(d.scene_bad + s, &zero, sizeof(int32_t))))
-    return rc;
-  const int e_lo = (int)a.e0, e_hi = (int)(a.e0 + Es), n_lo = (int)a.n0, n_hi = (int)(a.n0 + Ns);
-  k_prepare_elements<<<(int)((Es + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->a_young + a.e0, c->a_poisson + a.e0,
-                                                                                c->a_rho + a.e0, e_lo, e_hi);
-  k_prepare_mass<<<(int)((Ns + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, n_lo, n_hi);
-  c->launches += 2;
-  if ((rc = check_kernel(c, "arena prepare"))) return rc;
-  FW_CUDA(c, cudaStreamSynchronize(c->stream));
-  c->ascenes[s] = a;
-  for (int b = 0; b < Bs; ++b) c->a_body_scene[a.b0 + b] = s;
-  c->cur_active[s] = 1;
-  c->chunks_dirty = true;
-  // clear the stage for the next scene
-  c->h_x.clear(); c->h_v.clear(); c->h_bc.clear(); c->h_bcv.clear();
-  c->h_conn.clear(); c->h_type.clear(); c->h_E.clear(); c->h_nu.clear(); c->h_rho.clear(); c->h_sy.clear(); c->h_H.clear();
-  c->h_noff.clear(); c->h_ncnt.clear(); c->h_eoff.clear(); c->h_ecnt.clear(); c->h_scene.clear();
-  c->h_bnoff.clear(); c->h_bncnt.clear(); c->h_bnodes.clear(); c->h_pairs.clear(); c->h_heights.clear(); c->h_occ.clear();
-  *scene_out = s;
-  return FW_OK;
+  fw_pack* pk = nullptr;
+  int rc = build_pack(c, c->a_stream ? c->st_nodes : 0, false, &pk);
+  if (rc) return rc;
+  rc = fw_arena_commit_pack(c, pk, scene_out);
+  delete pk;  // pageable: its copies were staged before they returned
+  return rc;
 }
 
 int fw_arena_remove(fw_ctx* c, int32_t s) {
@@ -3089,6 +3470,12 @@ int fw_arena_remove(fw_ctx* c, int32_t s) {
   c->fl_pairs.give(a.p0, a.np);
   c->fl_heights.give(a.h0, a.nh);
   c->fl_occ.give(a.o0, a.no);
+  if (c->a_stream) {
+    c->fl_patch.give(a.pp0, a.npp);
+    c->fl_halo.give(a.hh0, a.nhh);
+    c->fl_ptri.give(a.t0, a.nt);
+    c->fl_csrp.give(a.cp0, a.ncp);
+  }
   a = fw_ctx::ArenaScene{};
   c->cur_active[s] = 0;
   c->free_scene_ids.push_back(s);
@@ -3119,11 +3506,27 @@ int fw_step_served_n(fw_ctx* c, const float* dt, int32_t n_steps) {
   FW_CUDA(c, cudaMemcpyAsync(c->d.scene_dt, c->cur_dt.data(), sizeof(float) * c->S, cudaMemcpyHostToDevice,
                              c->stream));
   c->d.uniform_dt = 0;
+  if (c->arena && c->a_stream) return arena_stream_steps(c, n_steps);
   int rc;
   if (c->arena && (rc = rebuild_chunks(c))) return rc;
   for (int k = 0; k < n_steps; ++k)
     if ((rc = launch_step(c))) return rc;
   return FW_OK;
+}
+
+int fw_step_served_budget(fw_ctx* c, const float* dt, const int32_t* budget, int32_t n_steps) {
+  if (!c || !dt || !budget || n_steps < 0) return FW_ERR_ARG;
+  if (!c->arena || !c->a_stream)
+    return fail(c, FW_ERR_STATE, "fw_step_served_budget needs a stream arena (fw_set_path FW_PATH_STREAM before "
+                                 "fw_arena_init)");
+  if (n_steps == 0) return FW_OK;
+  c->h_budget.assign(budget, budget + c->S);
+  FW_CUDA(c, cudaMemcpyAsync(c->d_budget, c->h_budget.data(), sizeof(int32_t) * c->S, cudaMemcpyHostToDevice,
+                             c->stream));  // staged before the call returns
+  c->d.scene_budget = c->d_budget;
+  const int rc = fw_step_served_n(c, dt, n_steps);
+  c->d.scene_budget = nullptr;
+  return rc;
 }
 
 int fw_arena_scene_info(fw_ctx* c, int32_t s, int64_t* info) {

@@ -36,8 +36,9 @@ from .world import PackedWorld, SceneLayout, stage, substep_schedule
 
 
 def scene_device_bytes(layout: SceneLayout) -> int:
-    """Device bytes a scene occupies in the arena (per-node and per-triangle
-    arrays, voxel cells and height samples)."""
+    """Device bytes a scene occupies in a gather arena (per-node and
+    per-triangle arrays, voxel cells and height samples); a pack reports its
+    own exact figure (ScenePack.device_bytes)."""
     nodes = layout.n_nodes
     elems = layout.n_elems
     ground = 0
@@ -50,15 +51,42 @@ def scene_device_bytes(layout: SceneLayout) -> int:
 
 
 class Arena:
-    """Resident scenes in one device arena."""
+    """Resident scenes in one device arena.
+
+    Args:
+        max_*: capacities reserved once
+        path: "stream" (the patch-streaming step, one CTA per patch of the
+            active scenes; the default) or "gather" (two kernels per
+            substep); both give the same bits
+        stream_patch: owned nodes per patch of a stream arena (64 or 128)
+    """
 
     def __init__(self, max_nodes, max_elems, max_bodies=4096, max_scenes=4096, max_pairs=4096,
-                 max_heights=1 << 20, max_occ=1 << 26, device=0):
+                 max_heights=1 << 20, max_occ=1 << 26, device=0, path="stream", stream_patch=64):
         self.native = _native.NativeWorld(device)
+        if path == "stream":
+            self.native.set_path(_native.FW_PATH_STREAM)
+            self.native.set_option(_native.FW_OPT_STREAM_PATCH, int(stream_patch))
+        elif path != "gather":
+            raise ValueError(f"arena path must be 'stream' or 'gather', not {path!r}")
         self.native.arena_init(max_nodes, max_elems, max_bodies, max_scenes, max_pairs, max_heights, max_occ)
+        self.path = path
+        self.patch_nodes = int(stream_patch) if path == "stream" else 0
         self.max_scenes = max_scenes
         self.S = max_scenes + 1
         self.layouts = {}
+        self._stage = _native.NativeWorld.stage()
+
+    def pack(self, layout: SceneLayout, packed: PackedWorld, pinned: bool = False) -> _native.ScenePack:
+        """Host-side preparation of a scene for this arena (validation,
+        corner lists, stream patches); touches neither the device nor the
+        arena, so another thread may run it while the arena steps (one
+        thread at a time per Arena)."""
+        if layout.entries:
+            raise NotImplementedError("rigid bodies and ground planes with BCs run in an ExplicitLoop or "
+                                      "BatchedLoop, not in served worlds")
+        stage(self._stage, packed)
+        return self._stage.arena_pack(self.patch_nodes, pinned)
 
     def insert(self, domains, dt=0.0, useAdapativeDT=False, damping=0.0) -> int:
         layout = SceneLayout(domains, dt=dt, damping=damping, useAdapativeDT=useAdapativeDT)
@@ -66,11 +94,15 @@ class Arena:
 
     def insert_prepared(self, layout: SceneLayout, packed: PackedWorld) -> int:
         """Upload a scene whose host-side layout and packing are already built."""
-        if layout.entries:
-            raise NotImplementedError("rigid bodies and ground planes with BCs run in an ExplicitLoop or "
-                                      "BatchedLoop, not in served worlds")
-        stage(self.native, packed)
-        s = self.native.arena_commit()
+        pk = self.pack(layout, packed)
+        try:
+            return self.insert_pack(layout, pk)
+        finally:
+            pk.close()  # pageable: its copies were staged when they were queued
+
+    def insert_pack(self, layout: SceneLayout, pk: _native.ScenePack) -> int:
+        """Upload a prepared scene (queued on the arena's stream; no wait)."""
+        s = self.native.arena_commit_pack(pk)
         self.layouts[s] = layout
         return s
 
@@ -92,6 +124,10 @@ class Arena:
     def energy(self, scene: int):
         """FP64 energies of one resident scene: kinetic, strain, external, contact."""
         return self.native.energy(self.S)[scene]
+
+    def close(self):
+        self._stage.close()
+        self.native.close()
 
 
 @dataclass(order=True)
@@ -155,12 +191,15 @@ class _Job:
 class Server:
     """Continuous-batching request loop over resident bodies.
 
-    Each iteration runs K substeps in one native call (fw_step_served_n),
-    where K is the fewest substeps any in-flight request has left at its
-    current dt -- so a request leaves the batch at the very substep it
-    finishes -- and, with real-time arrivals, no more than fit before the next
-    arrival (from the measured device time per substep), so new requests join
-    within about one arrival gap.
+    Each iteration runs K substeps in one native call.  On a stream arena
+    (fw_step_served_budget) every in-flight request's scene runs only the
+    substeps its request has left at its current dt within the call, so a
+    request leaves the batch at the very substep it finishes while the call
+    goes on for the others; K is capped by max_batch_substeps and, with
+    real-time arrivals, by what fits before the next arrival (from the
+    measured device time per substep), so new requests join within about one
+    arrival gap.  On a gather arena (fw_step_served_n) K also stops at the
+    nearest request end.
 
     Args:
         make_body: body id -> list of domains (the scene of that body)
@@ -173,14 +212,14 @@ class Server:
 
     def __init__(self, make_body, budget_bytes=150e9, arena_nodes=8_500_000, arena_elems=17_000_000,
                  arena_bodies=4096, arena_scenes=4096, frame_dt=1.0 / 60.0, max_inflight=4, device=0,
-                 max_batch_substeps=64):
+                 max_batch_substeps=64, path="stream", stream_patch=64):
         import torch
 
         self.make_body = make_body
         self.budget = float(budget_bytes)
         self.frame_dt = frame_dt
         self.arena = Arena(arena_nodes, arena_elems, arena_bodies, arena_scenes, arena_bodies,
-                           device=device)
+                           device=device, path=path, stream_patch=stream_patch)
         self.device = device
         self.stream = torch.cuda.Stream(device=device)
         self.arena.native.set_stream(self.stream.cuda_stream)
@@ -193,23 +232,37 @@ class Server:
         self.deferred_admissions = 0
         self.element_steps = 0
         self.admit_s = 0.0        # host time spent admitting new bodies
-        self.last_admit_t = 0.0   # run clock of the last admission
+        self.last_admit_t = 0.0   # run clock of the last first admission of a body
         self.evicted = 0          # bodies removed because their state turned non-finite
-        self._prep = {}           # body -> (layout, packed, device bytes), built ahead by prepare()
+        self.readmitted = 0       # admissions of bodies that were resident before (after an eviction)
+        self._prep = {}           # body -> (layout, pack), built ahead by prepare() or at first admission
+        self._ever = set()        # bodies admitted at least once
         self.admit_budget_s = 0.002  # host time per loop iteration for admitting new bodies
+        self.admit_span = 8          # call length while admissions wait (stream arenas)
+        self.host_us = 100.0         # host time of one loop iteration, refined as the loop runs
+        self.device_s = 0.0          # device time of the native calls (CUDA events around each call)
 
     def _build(self, body):
-        """Host-side preparation of a body: its domains, scene layout, packed
-        arrays and device footprint (everything but the upload)."""
+        """Host-side preparation of a body: its domains, scene layout and its
+        arena pack in page-locked memory (everything but the upload)."""
         layout = SceneLayout(self.make_body(body))
-        return layout, PackedWorld([layout]), scene_device_bytes(layout)
+        return layout, self.arena.pack(layout, PackedWorld([layout]), pinned=True)
 
     def prepare(self, bodies):
-        """Build the host-side layouts of these bodies ahead of their first
-        request (a catalog load); their admission is then an upload only."""
+        """Build these bodies' packs ahead of their first request (a catalog
+        load); their admission is then an upload queued on the stream.  A
+        pack is kept and commits the body afresh if it is evicted."""
         for b in bodies:
             if b not in self._prep:
                 self._prep[b] = self._build(b)
+
+    def close(self):
+        """Wait for the arena's stream, then free the packs and the arena."""
+        self.arena.native.synchronize()
+        for _, pk in self._prep.values():
+            pk.close()
+        self._prep.clear()
+        self.arena.close()
 
     def _admit(self, body, t0=None):
         """True if resident now; "new" if admitted by this call; False if it
@@ -220,12 +273,13 @@ class Server:
         if ent is None:
             ent = self._prep[body] = self._build(body)
         ta = time.perf_counter()
-        layout, packed, need = ent
+        layout, pk = ent
+        need = pk.device_bytes
         if self.used_bytes + need > self.budget:
             self.deferred_admissions += 1
             return False
         try:
-            s = self.arena.insert_prepared(layout, packed)
+            s = self.arena.insert_pack(layout, pk)
         except _native.NativeError:
             self.deferred_admissions += 1
             return False
@@ -234,8 +288,11 @@ class Server:
         self.used_bytes += need
         tb = time.perf_counter()
         self.admit_s += tb - ta
-        if t0 is not None:
-            self.last_admit_t = tb - t0
+        if body in self._ever:
+            self.readmitted += 1
+        elif t0 is not None:
+            self.last_admit_t = tb - t0  # first admissions only: re-admissions follow evictions
+        self._ever.add(body)
         return "new"
 
     def release(self, body):
@@ -268,6 +325,8 @@ class Server:
         busy_m = np.zeros(S, dtype=bool)
         init_m = np.zeros(S, dtype=bool)
         n_el = np.zeros(S, dtype=np.int64)
+        ran = np.zeros(S, dtype=np.int32)        # substeps each scene runs in the current call
+        budgets = self.arena.path == "stream"  # per-scene budgets: a call need not stop at each request end
         dts = np.zeros(S, dtype=np.float32)
         inflight = collections.deque()
         done_at = {}
@@ -307,7 +366,8 @@ class Server:
                 status[:, sc] = 0   # copies queued before the release must not flag the slot's next body
                 self.evicted += 1
         while arrivals or busy or ready or pending_done:
-            now = time.perf_counter() - t0
+            t_iter = time.perf_counter()
+            now = t_iter - t0
             while arrivals and (not realtime or arrivals[0].arrival <= now):
                 r = heapq.heappop(arrivals)
                 queues[r.body].append(r)
@@ -345,19 +405,31 @@ class Server:
                     time.sleep(max(0.0, arrivals[0].arrival - (time.perf_counter() - t0)))
                 continue
             np.copyto(dts, np.where(busy_m, cur_dt, np.float32(0.0)))
-            span = int(min(self.max_batch_substeps, left[busy_m].min()))
+            cap = self.max_batch_substeps
             if realtime and arrivals:
+                # end the call near the next arrival, but not before one host
+                # iteration's worth of device time (a shorter call idles the GPU)
                 gap_us = (arrivals[0].arrival - (time.perf_counter() - t0)) * 1e6
-                span = min(span, max(1, int(gap_us / self.us_per_substep)))
+                cap = min(cap, max(1, int(max(gap_us, self.host_us) / self.us_per_substep)))
+            if budgets and any(b not in self.resident for b in ready):
+                cap = min(cap, self.admit_span)  # bodies wait for admission: short calls let it catch up
             ev0 = torch.cuda.Event(enable_timing=True)
             ev0.record(self.stream)
-            self.arena.native.step_served_n(dts, span)
+            if budgets:
+                # one call spans request ends: each scene runs its own remaining substeps
+                span = int(min(cap, left[busy_m].max()))
+                np.copyto(ran, np.where(busy_m, np.minimum(left, span), 0))
+                self.arena.native.step_served_budget(dts, ran, span)
+            else:
+                span = int(min(cap, left[busy_m].min()))
+                np.copyto(ran, np.where(busy_m, span, 0))
+                self.arena.native.step_served_n(dts, span)
             self.arena.native.scene_status(S, out=status[slot], asynchronous=True)
             n_sub += span
             n_calls += 1
-            self.element_steps += int(n_el[busy_m].sum()) * span - int(n_el[busy_m & init_m].sum())
+            self.element_steps += int((n_el * ran).sum()) - int(n_el[busy_m & init_m].sum())
             init_m[busy_m] = False
-            left[busy_m] -= span
+            left[busy_m] -= ran[busy_m]
             finished = []
             for s in np.nonzero(busy_m & (left == 0))[0].tolist():
                 job = busy[s]
@@ -378,6 +450,8 @@ class Server:
             pending_done.append((ev, finished, ev0, span, slot))
             slot = (slot + 1) % ring
             inflight.append(ev)
+            # host time of an iteration that issues a call (before any wait on the GPU)
+            self.host_us = 0.9 * self.host_us + 0.1 * (time.perf_counter() - t_iter) * 1e6
             if len(inflight) > self.max_inflight:
                 inflight.popleft().synchronize()
             evict(self._retire(pending_done, done_at, failed, status, t0, block=False))
@@ -386,10 +460,10 @@ class Server:
         ends = {**done_at, **failed}
         lat = np.array([ends[r.rid] - r.arrival if realtime else ends[r.rid] for r in requests])
         return {"latency_s": lat, "wall_s": wall, "substeps": n_sub, "native_calls": n_calls,
-                "failed": sorted(failed), "evicted_bodies": self.evicted,
+                "failed": sorted(failed), "evicted_bodies": self.evicted, "readmitted_bodies": self.readmitted,
                 "element_steps": self.element_steps, "deferred_admissions": self.deferred_admissions,
                 "resident_bodies": len(self.resident), "used_bytes": self.used_bytes,
-                "admit_s": self.admit_s, "last_admit_t": self.last_admit_t}
+                "admit_s": self.admit_s, "last_admit_t": self.last_admit_t, "device_s": self.device_s}
 
     def _retire(self, pending_done, done_at, failed, status, t0, block):
         """Retire completed calls in order; returns the scenes whose state
@@ -409,7 +483,9 @@ class Server:
                     failed[j.req.rid] = t
                 else:
                     done_at[j.req.rid] = t
-            self.us_per_substep = 0.8 * self.us_per_substep + 0.2 * max(1.0, ev0.elapsed_time(ev) * 1e3 / span)
+            call_ms = ev0.elapsed_time(ev)
+            self.device_s += call_ms * 1e-3
+            self.us_per_substep = 0.8 * self.us_per_substep + 0.2 * max(1.0, call_ms * 1e3 / span)
             pending_done.pop(0)
         return bad
 

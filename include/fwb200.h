@@ -67,6 +67,7 @@ extern "C" {
 #define FW_PATH_STREAM 3   /* one patch-streaming kernel per substep (worlds of many scenes) */
 
 typedef struct fw_ctx fw_ctx;
+typedef struct fw_pack fw_pack; /* a scene prepared for an arena (fw_arena_pack) */
 
 /* Create / destroy a context on CUDA device `device`.
  * Replaces: FemSpringManager.__init__ buffer allocation,
@@ -339,6 +340,14 @@ int fw_step_served(fw_ctx* ctx, const float* dt);
  * current dt, so requests still leave the batch at the substep they finish. */
 int fw_step_served_n(fw_ctx* ctx, const float* dt, int32_t n_steps);
 
+/* Stream arenas: n_steps substeps of fw_step_served in which scene s (dt[s]
+ * > 0) runs only its first budget[s] substeps and sits out the rest (its
+ * state carried unchanged); budget has one entry per scene.  A request loop
+ * passes each in-flight request's remaining substeps, so one call can span
+ * many request ends.  Same bits as calls of fw_step_served_n that stop at
+ * each end. */
+int fw_step_served_budget(fw_ctx* ctx, const float* dt, const int32_t* budget, int32_t n_steps);
+
 /* Mark scenes active (1) / frozen (0).  Frozen scenes keep their state and do
  * not advance. */
 int fw_set_active(fw_ctx* ctx, const int32_t* active);
@@ -454,21 +463,51 @@ int fw_step_noalloc(int32_t n_nodes, int32_t n_elems, int32_t n_steps, float dt,
 
 /* Arena (served form).  fw_arena_init replaces the fw_set_* / fw_finalize
  * flow: it reserves device capacity once (nodes, triangles, bodies, scenes,
- * contact pairs, height samples, voxel cells).  Then, any number of times:
- * stage ONE scene with fw_set_nodes / fw_set_elements / fw_set_bodies
- * (scene 0) / fw_set_scenes(1, ...) / fw_add_*_pair using ids local to that
- * scene, and fw_arena_commit copies it into free ranges, precomputes its
- * reference shape and schedules its zero-dt construction step for the next
- * substep; fw_arena_remove frees a scene's ranges.  Steps touch only the
- * active scenes' ranges.  fw_step_scenes then takes max_scenes + 1 dt values.
- * fw_arena_scene_info fills info[8] = {first node, nodes, first triangle,
- * triangles, first body, bodies, free node capacity, free triangle capacity}.
+ * contact pairs, height samples, voxel cells).  With fw_set_path(ctx,
+ * FW_PATH_STREAM, 0) (and FW_OPT_STREAM_PATCH) before fw_arena_init the arena
+ * steps on the patch-streaming kernel: each committed scene also holds its
+ * patch records, and a substep runs one CTA per patch of the active scenes
+ * only; otherwise it steps on the gather kernels.  Both give the same bits.
+ * Then, any number of times: stage ONE scene with fw_set_nodes /
+ * fw_set_elements / fw_set_bodies (scene 0) / fw_set_scenes(1, ...) /
+ * fw_add_*_pair using ids local to that scene, and fw_arena_commit copies it
+ * into free ranges, precomputes its reference shape and schedules its zero-dt
+ * construction step for the next substep (queued on the stream; the call does
+ * not wait for the device); fw_arena_remove frees a scene's ranges (it waits
+ * for the stream).  Steps touch only the active scenes' ranges.
+ * fw_step_scenes then takes max_scenes + 1 dt values.  fw_arena_scene_info
+ * fills info[8] = {first node, nodes, first triangle, triangles, first body,
+ * bodies, free node capacity, free triangle capacity}.
  * No reference counterpart: each reference ExplicitLoop is built once
  * (flatworld/explicitloop.py:72-398). */
 int fw_arena_init(fw_ctx* ctx, int64_t max_nodes, int64_t max_elems, int32_t max_bodies,
                   int32_t max_scenes, int32_t max_pairs, int64_t max_heights, int64_t max_occ);
 int fw_arena_commit(fw_ctx* ctx, int32_t* scene_out);
 int fw_arena_remove(fw_ctx* ctx, int32_t scene);
+
+/* Split commit, so that a scene is prepared away from the thread that steps
+ * the arena.  fw_arena_pack: the scene staged on `stage` (a context of its
+ * own, never finalized, used by one thread at a time; the staging calls as
+ * above) becomes a pack -- validation, corner lists, contact-pair order and,
+ * for patch_nodes 64 or 128 (that of the arena it goes to; 0 for a gather
+ * arena), its stream patches -- host work only; the stage is cleared.  With
+ * flags & FW_PACK_PINNED the pack lives in page-locked memory, so the
+ * commit's copies do not wait for the stream.  fw_arena_commit_pack uploads a
+ * pack into an arena (queued on the arena's stream, ids relocated on the
+ * device) and may be called again with the same pack to commit the scene
+ * afresh.  fw_pack_info fills info[8] = {device bytes the scene occupies,
+ * nodes, triangles, bodies, patch nodes, patches, patch triangles, pinned}.
+ * fw_pack_destroy frees a pack; no commit from it may still be in flight
+ * (synchronize the arena's stream first). */
+#define FW_PACK_PINNED 1
+int fw_arena_pack(fw_ctx* stage, int32_t patch_nodes, int32_t flags, fw_pack** out);
+/* A staging context: holds staged scene data for fw_arena_pack and nothing
+ * else (no device, no stream; fw_finalize and fw_arena_init refuse it).  Works
+ * without a GPU.  Free it with fw_destroy. */
+int fw_create_stage(fw_ctx** out);
+int fw_arena_commit_pack(fw_ctx* ctx, const fw_pack* pack, int32_t* scene_out);
+int fw_pack_info(const fw_pack* pack, int64_t* info);
+void fw_pack_destroy(fw_pack* pack);
 int fw_arena_scene_info(fw_ctx* ctx, int32_t scene, int64_t* info);
 
 /* Differentiable form.  fw_set_element_young: new per-element Young's moduli

@@ -1,13 +1,16 @@
 """Served form (GPU): continuous batching over an arena of resident bodies.
 
 Each body's result after its requests must be bit-identical to running the
-same requests alone, one ExplicitLoop per body; bodies admitted, removed and
-re-admitted reuse arena ranges correctly."""
+same requests alone, one ExplicitLoop per body, on both arena step paths
+(stream: one CTA per patch of the active scenes; gather); bodies admitted,
+removed and re-admitted reuse arena ranges correctly; scenes that sit out
+some calls (of odd or even substep counts) keep their state."""
 
 import numpy as np
 import pytest
 
 import flatworld_b200 as fw
+from flatworld_b200 import _native
 from flatworld_b200.serve import Arena, FifoPlainServer, Request, Server, poisson_requests, request_substeps
 from flatworld_b200.world import substep_schedule
 from tests import scenes
@@ -32,10 +35,11 @@ def alone(body, reqs):
     return lp.femSpringManager.coords.numpy()[: lp._packed.N], lp.femSpringManager.V.numpy()[: lp._packed.N]
 
 
-def test_served_results_equal_alone():
+@pytest.mark.parametrize("path", ["stream", "gather"])
+def test_served_results_equal_alone(path):
     reqs = poisson_requests(rate=400.0, duration=0.1, n_bodies=6, seed=3, substeps=(20, 60))
     assert len(reqs) >= 20
-    srv = Server(small_body, arena_nodes=60_000, arena_elems=120_000, arena_bodies=64, arena_scenes=64)
+    srv = Server(small_body, arena_nodes=60_000, arena_elems=120_000, arena_bodies=64, arena_scenes=64, path=path)
     out = srv.run(reqs, realtime=False)
     assert len(out["latency_s"]) == len(reqs)
     for body in sorted({r.body for r in reqs}):
@@ -59,13 +63,14 @@ def exploding_body(i):
     return [fem]
 
 
-def test_nonfinite_body_is_evicted_and_others_are_untouched():
+@pytest.mark.parametrize("path", ["stream", "gather"])
+def test_nonfinite_body_is_evicted_and_others_are_untouched(path):
     """A body whose state turns NaN is flagged on the device, its requests fail,
     it is removed from the arena, and the other bodies' results are the same
     bits as alone."""
     body_fn = lambda b: exploding_body(b) if b == 4 else small_body(b)  # noqa: E731
     reqs = [Request(0.0, k, k % 5, 40) for k in range(15)]
-    srv = Server(body_fn, arena_nodes=60_000, arena_elems=120_000, arena_bodies=64, arena_scenes=64)
+    srv = Server(body_fn, arena_nodes=60_000, arena_elems=120_000, arena_bodies=64, arena_scenes=64, path=path)
     out = srv.run(reqs, realtime=False)
     bad = {r.rid for r in reqs if r.body == 4}
     assert set(out["failed"]) == bad
@@ -83,8 +88,9 @@ def test_nonfinite_body_is_evicted_and_others_are_untouched():
         assert lp._native.scene_status(1)[0] == 0
 
 
-def test_arena_reuses_ranges_after_remove():
-    ar = Arena(40_000, 80_000, 16, 16, 16, 1 << 16, 1 << 20)
+@pytest.mark.parametrize("path", ["stream", "gather"])
+def test_arena_reuses_ranges_after_remove(path):
+    ar = Arena(40_000, 80_000, 16, 16, 16, 1 << 16, 1 << 20, path=path)
     a = ar.insert(small_body(0), dt=5e-5)
     b = ar.insert(small_body(1), dt=5e-5)
     info_a = ar.info(a)
@@ -98,6 +104,73 @@ def test_arena_reuses_ranges_after_remove():
     lp = fw.ExplicitLoop(5e-5, small_body(0), useAdapativeDT=False, path="gather")
     lp.advance_n(100)
     assert np.array_equal(ar.coords(c), lp.femSpringManager.coords.numpy()[: lp._packed.N])
+
+
+@pytest.mark.parametrize("patch", [64, 128])
+def test_stream_arena_idle_scenes_keep_their_state(patch):
+    """Three scenes on a stream arena step in calls of odd and even substep
+    counts while the others sit out (the active scenes' state is carried back
+    into the first buffers after an odd count); each ends bit-identical to
+    its own run alone.  The pack of scene 0 is committed twice (a second
+    resident copy), as a server re-admits an evicted body."""
+    ar = Arena(60_000, 120_000, 16, 16, 16, 1 << 16, 1 << 22, path="stream", stream_patch=patch)
+    from flatworld_b200.world import PackedWorld, SceneLayout
+
+    lay = SceneLayout(small_body(0))
+    pk = ar.pack(lay, PackedWorld([lay]), pinned=True)
+    assert pk.patch_nodes == patch and pk.patches >= (pk.nodes + patch - 1) // patch and pk.patch_elems >= pk.elems
+    a = ar.insert_pack(lay, pk)
+    b = ar.insert(small_body(1))
+    a2 = ar.insert_pack(lay, pk)
+    dt = np.float32(5e-5)
+    plan = [({a, b, a2}, 1), ({a}, 7), ({b, a2}, 12), ({a, b}, 5), ({a2}, 3), ({a, b, a2}, 8)]
+    ran = {a: 0, b: 0, a2: 0}
+    for active, n in plan:
+        dts = np.zeros(ar.S, np.float32)
+        for s_ in active:
+            dts[s_] = dt
+            ran[s_] += n
+        ar.native.step_served_n(dts, n)
+    ar.native.synchronize()
+    pk.close()
+    for s_, body in ((a, 0), (b, 1), (a2, 0)):
+        lp = fw.ExplicitLoop(5e-5, small_body(body), useAdapativeDT=False, path="gather")
+        lp.advance_n(ran[s_] - 1)  # the first substep of a committed scene is its construction step
+        n = lp._packed.N
+        assert np.array_equal(ar.coords(s_), lp.femSpringManager.coords.numpy()[:n]), (s_, ran[s_])
+        assert np.array_equal(ar.velocities(s_), lp.femSpringManager.V.numpy()[:n]), (s_, ran[s_])
+    ar.close()
+
+
+def test_stream_arena_budgets_equal_separate_calls():
+    """fw_step_served_budget: in one call of n substeps each scene runs only
+    its own budget and then sits out (its state carried unchanged between the
+    buffers) -- the same bits as running each scene's substeps alone."""
+    ar = Arena(60_000, 120_000, 16, 16, 16, 1 << 16, 1 << 22, path="stream")
+    sc = [ar.insert(small_body(i)) for i in range(3)]
+    dt = np.float32(5e-5)
+    ran = dict.fromkeys(sc, 0)
+    for n, budgets in ((9, (9, 4, 1)), (16, (3, 16, 11)), (7, (7, 0, 2)), (12, (1, 12, 12))):
+        dts = np.zeros(ar.S, np.float32)
+        bud = np.zeros(ar.S, np.int32)
+        for s_, b_ in zip(sc, budgets):
+            if b_:
+                dts[s_] = dt
+                bud[s_] = b_
+                ran[s_] += b_
+        ar.native.step_served_budget(dts, bud, n)
+    ar.native.synchronize()
+    for s_, body in zip(sc, range(3)):
+        lp = fw.ExplicitLoop(5e-5, small_body(body), useAdapativeDT=False, path="gather")
+        lp.advance_n(ran[s_] - 1)  # the first substep is the construction step
+        n = lp._packed.N
+        assert np.array_equal(ar.coords(s_), lp.femSpringManager.coords.numpy()[:n]), (s_, ran[s_])
+        assert np.array_equal(ar.velocities(s_), lp.femSpringManager.V.numpy()[:n]), (s_, ran[s_])
+    gather = Arena(10_000, 20_000, 4, 4, 4, 1, 1, path="gather")
+    with pytest.raises(_native.NativeError, match="stream arena"):
+        gather.native.step_served_budget(np.zeros(gather.S, np.float32), np.zeros(gather.S, np.int32), 1)
+    ar.close()
+    gather.close()
 
 
 def test_fifo_plain_server_runs():
