@@ -89,7 +89,7 @@ _SIGNATURES = {
     "fw_arena_remove": (C.c_int, [_vp, C.c_int32]),
     "fw_arena_scene_info": (C.c_int, [_vp, C.c_int32, _i64p]),
     "fw_arena_pack": (C.c_int, [_vp, C.c_int32, C.c_int32, C.POINTER(_vp)]),
-    "fw_step_served_budget": (C.c_int, [_vp, _f32p, _i32p, C.c_int32]),
+    "fw_step_served_budget": (C.c_int, [_vp, _f32p, _i32p, _f32p, _i32p, C.c_int32]),
     "fw_create_stage": (C.c_int, [C.POINTER(_vp)]),
     "fw_arena_commit_pack": (C.c_int, [_vp, _vp, _i32p]),
     "fw_pack_info": (C.c_int, [_vp, _i64p]),
@@ -446,12 +446,18 @@ class NativeWorld:
         self._check(self._L.fw_step_served_n(self._h, dt_per_scene.ctypes.data_as(_f32p), int(n_steps)),
                     "fw_step_served_n")
 
-    def step_served_budget(self, dt_per_scene, budget, n_steps: int):
+    def step_served_budget(self, dt_per_scene, budget, n_steps: int, dt_next=None, budget_next=None):
         """Stream arenas: n_steps substeps in which scene s runs only its
-        first budget[s] substeps (fw_step_served_budget)."""
+        first budget[s] substeps, then budget_next[s] at dt_next[s] when
+        given (fw_step_served_budget)."""
         b = _i(budget)
-        self._check(self._L.fw_step_served_budget(self._h, dt_per_scene.ctypes.data_as(_f32p), b[1], int(n_steps)),
-                    "fw_step_served_budget")
+        if dt_next is None:
+            p_dt2 = p_b2 = None
+        else:
+            d2, p_dt2 = _f(dt_next)
+            b2, p_b2 = _i(budget_next)
+        self._check(self._L.fw_step_served_budget(self._h, dt_per_scene.ctypes.data_as(_f32p), b[1], p_dt2, p_b2,
+                                                  int(n_steps)), "fw_step_served_budget")
 
     def set_active(self, active):
         a = _i(active)

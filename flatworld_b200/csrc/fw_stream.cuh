@@ -28,6 +28,12 @@
 // the patch's triangle records staged into shared memory by one bulk copy
 // (cp.async.bulk, completion on an mbarrier) that overlaps the position
 // gather, instead of one load per triangle and thread.
+//
+// Arena worlds (the served form) launch one CTA per patch of the scenes that
+// are active in the call only (StreamDev::list); their per-scene control runs
+// in k_control_scenes over the active scenes' body and pair ranges, and after
+// an odd number of substeps k_stream_carry copies their state back into the
+// first buffers, so the scenes that sat the call out are never touched.
 #pragma once
 
 namespace {

@@ -81,6 +81,10 @@ struct Dev {
   // still run in this call; a scene whose budget is spent sits the rest out
   // (null: no budgets)
   int32_t* scene_budget;
+  // optional second segment: once scene_budget[s] is spent the scene runs
+  // scene_budget_next[s] more substeps at scene_dt_next[s] (null: none)
+  int32_t* scene_budget_next;
+  float* scene_dt_next;
   int32_t* aabb_ring;  // [2][B][4] ordered ints
   int N, E, B, S, P;
   int has_j2;
@@ -126,12 +130,7 @@ namespace {
 __device__ void step_control(const Dev& d) {
   const int t = threadIdx.x;
   for (int s = t; s < d.S; s += blockDim.x) {
-    int act = d.scene_active[s];
-    if (act && d.scene_budget) {
-      const int left = d.scene_budget[s];
-      if (left <= 0) act = 0;
-      else d.scene_budget[s] = left - 1;
-    }
+    const int act = d.scene_active[s];
     const int req = d.scene_mode_req[s];
     d.scene_mode[s] = act ? (req ? fw::MODE_INIT : fw::MODE_STEP) : fw::MODE_FROZEN;
     if (act && req) d.scene_mode_req[s] = 0;
@@ -170,6 +169,61 @@ __device__ void step_control(const Dev& d) {
     r[1] = fw::f2ord(1e30f);
     r[2] = fw::f2ord(-1e30f);
     r[3] = fw::f2ord(-1e30f);
+  }
+}
+
+// step_control for a list of scenes (stream arenas: the active scenes of the
+// call), one thread per scene: the same four steps for that scene -- mode
+// (and budget), its pairs' gates from the box of the previous substep, its
+// counter, the reset of its bodies' next box slot -- in the same order.
+// Budgets (fw_step_served_budget): a scene runs scene_budget[s] substeps at
+// its dt, then scene_budget_next[s] at scene_dt_next[s], then sits out.
+// rng[s] = (first body, bodies, first pair, pairs) of scene s.
+__global__ void k_control_scenes(Dev d, const int32_t* __restrict__ list, int n, const int4* __restrict__ rng) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = list[i];
+  int act = d.scene_active[s];
+  if (act && d.scene_budget) {
+    const int left = d.scene_budget[s];
+    if (left > 0) {
+      d.scene_budget[s] = left - 1;
+    } else {
+      const int left2 = d.scene_budget_next ? d.scene_budget_next[s] : 0;
+      if (left2 > 0) {  // the second segment: switch to its step size once
+        if (left == 0) {
+          d.scene_dt[s] = d.scene_dt_next[s];
+          d.scene_budget[s] = -1;
+        }
+        d.scene_budget_next[s] = left2 - 1;
+      } else {
+        act = 0;
+      }
+    }
+  }
+  const int req = d.scene_mode_req[s];
+  const int mode = act ? (req ? fw::MODE_INIT : fw::MODE_STEP) : fw::MODE_FROZEN;
+  d.scene_mode[s] = mode;
+  if (act && req) d.scene_mode_req[s] = 0;
+  if (mode != fw::MODE_STEP && mode != fw::MODE_INIT) return;
+  const int4 r = rng[s];
+  if (mode == fw::MODE_STEP) {
+    const int k = d.scene_counter[s];
+    for (int p = r.z; p < r.z + r.w; ++p) {
+      const Pair& pr = d.pairs[p];
+      const int* box = d.aabb_ring + ((size_t)(k & 1) * d.B + pr.body) * 4;
+      d.pair_active[p] = fw::pair_gate(pr, fw::ord2f(box[0]), fw::ord2f(box[1]), fw::ord2f(box[2]),
+                                       fw::ord2f(box[3]), k) ? 1 : 0;
+    }
+    d.scene_counter[s] = k + 1;
+  }
+  const int k2 = d.scene_counter[s];
+  for (int b = r.x; b < r.x + r.y; ++b) {
+    int* box = d.aabb_ring + ((size_t)(k2 & 1) * d.B + b) * 4;
+    box[0] = fw::f2ord(1e30f);
+    box[1] = fw::f2ord(1e30f);
+    box[2] = fw::f2ord(-1e30f);
+    box[3] = fw::f2ord(-1e30f);
   }
 }
 
@@ -1068,7 +1122,16 @@ struct fw_ctx {
   FreeList fl_patch, fl_halo, fl_ptri, fl_csrp;
   int32_t* d_plist = nullptr;     // the active scenes' patches (CTA -> patch)
   int32_t* d_budget = nullptr;    // fw_step_served_budget: per-scene substep budgets
-  std::vector<int32_t> h_budget;
+  int32_t* d_budget2 = nullptr;   // ... of the second segment
+  float* d_dt2 = nullptr;         // ... and its step sizes
+  std::vector<int32_t> h_budget, h_budget2;
+  std::vector<float> h_dt2;
+  unsigned char* d_stage = nullptr;  // device staging buffer of fw_arena_commit_pack
+  size_t stage_cap = 0;
+  int32_t* d_slist = nullptr;     // the active scenes (k_control_scenes)
+  int4* d_srng = nullptr;         // per scene: first body, bodies, first pair, pairs
+  std::vector<int32_t> h_slist;
+  int st_slist_n = 0;
   std::vector<int32_t> h_plist;
   int st_list_n = 0;
   std::vector<ArenaScene> ascenes;
@@ -1898,7 +1961,8 @@ int set_scene_dt(fw_ctx* c, const float* dt) {
 }
 
 // Relocation of one committed scene's arrays from scene-local to arena ids
-// (fw_arena_commit_pack uploads them as packed).
+// (fw_arena_commit_pack uploads them as packed), and the scene's control
+// words (thread 0).
 struct ArenaReloc {
   int n0, e0, b0, p0, h0, o0, s;
   int Ns, Es, Bs, Np;
@@ -1906,12 +1970,25 @@ struct ArenaReloc {
   int32_t* rh;
   int32_t* re;
   int Hs, Ts;
+  StreamPatch* patch;  // stream arenas: the scene's patch records
+  int Ps, hh0, t0, cp0;
+  int4* srng;  // stream arenas: per-scene body / pair ranges
+  float damp;
   int64_t count;  // max of the counts above and 3 Es
 };
 
 __global__ void k_arena_reloc(Dev d, ArenaReloc r) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < r.count; i += stride) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) {
+    d.scene_damp[r.s] = r.damp;
+    d.scene_counter[r.s] = 0;
+    d.scene_mode_req[r.s] = 1;  // the zero-dt construction step at the next substep it runs
+    d.scene_active[r.s] = 1;
+    d.scene_bad[r.s] = 0;
+    if (r.srng) r.srng[r.s] = make_int4(r.b0, r.Bs, r.p0, r.Np);
+  }
+  for (int64_t i = tid; i < r.count; i += stride) {
     if (i < r.Ns) {
       const int64_t g = r.n0 + i;
       d.node_word[g] += (uint32_t)r.b0 << fw::NODE_BODY_SHIFT;
@@ -1938,6 +2015,41 @@ __global__ void k_arena_reloc(Dev d, ArenaReloc r) {
     }
     if (r.rh && i < r.Hs) r.rh[i] += r.n0;
     if (r.re && i < r.Ts) r.re[i] += r.e0;
+    if (r.patch && i < r.Ps) {
+      StreamPatch& sp = r.patch[i];
+      sp.node_off += r.n0;
+      sp.halo_off += r.hh0;
+      sp.elem_off += r.t0;
+      sp.csrp_off += r.cp0;
+      sp.csr_off += 3 * r.e0;
+      sp.scene = r.s;
+    }
+  }
+}
+
+// Parts of a pack copied from the device staging buffer to their arena
+// ranges: part k = stage[off[k] .. +len[k]) -> dst[k] (blockIdx.y = part).
+constexpr int kScatterParts = 27;  // the pack's parts and the rest positions again (as the current ones)
+struct ArenaScatter {
+  unsigned char* dst[kScatterParts];
+  uint32_t off[kScatterParts];
+  uint32_t len[kScatterParts];
+};
+
+__global__ void k_arena_scatter(const unsigned char* __restrict__ stage, ArenaScatter sc) {
+  const int k = blockIdx.y;
+  const uint32_t len = sc.len[k];
+  if (!len) return;
+  const unsigned char* src = stage + sc.off[k];
+  unsigned char* dst = sc.dst[k];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (((uintptr_t)dst & 3) == 0 && (len & 3) == 0) {  // the source parts are 16-byte aligned
+    const uint32_t* s4 = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d4 = reinterpret_cast<uint32_t*>(dst);
+    for (uint32_t i = t; i < len / 4; i += stride) d4[i] = s4[i];
+  } else {
+    for (uint32_t i = t; i < len; i += stride) dst[i] = src[i];
   }
 }
 
@@ -1961,15 +2073,22 @@ int stream_attrs(fw_ctx* c, int optin) {
 int arena_stream_steps(fw_ctx* c, int n) {
   if (c->chunks_dirty) {
     c->h_plist.clear();
+    c->h_slist.clear();
     for (size_t s2 = 0; s2 < c->ascenes.size(); ++s2) {
       const fw_ctx::ArenaScene& a = c->ascenes[s2];
       if (!a.live || !c->cur_active[s2]) continue;
+      c->h_slist.push_back((int32_t)s2);
       for (int64_t k = 0; k < a.npp; ++k) c->h_plist.push_back((int32_t)(a.pp0 + k));
     }
+    // staged before the calls return
     if (!c->h_plist.empty())
       FW_CUDA(c, cudaMemcpyAsync(c->d_plist, c->h_plist.data(), sizeof(int32_t) * c->h_plist.size(),
-                                 cudaMemcpyHostToDevice, c->stream));  // staged before the call returns
+                                 cudaMemcpyHostToDevice, c->stream));
+    if (!c->h_slist.empty())
+      FW_CUDA(c, cudaMemcpyAsync(c->d_slist, c->h_slist.data(), sizeof(int32_t) * c->h_slist.size(),
+                                 cudaMemcpyHostToDevice, c->stream));
     c->st_list_n = (int)c->h_plist.size();
+    c->st_slist_n = (int)c->h_slist.size();
     c->chunks_dirty = false;
   }
   c->host_counter += n;
@@ -1978,8 +2097,9 @@ int arena_stream_steps(fw_ctx* c, int n) {
   float4 *ja = c->d.j2state, *jb = c->d.j2_alt;
   const StreamKernel k = stream_kernel(c->st_nodes, c->st_minb, c->st_bulk);
   const size_t smem = c->st_bulk ? c->st_smem_bulk : c->st_smem;
+  const int gs = (c->st_slist_n + 127) / 128;
   for (int j = 0; j < n; ++j) {
-    k_control<<<1, kMaxBlock, 0, c->stream>>>(c->d);
+    k_control_scenes<<<gs, 128, 0, c->stream>>>(c->d, c->d_slist, c->st_slist_n, c->d_srng);
     k<<<c->st_list_n, c->st_nodes, smem, c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
     std::swap(xa, xb);
     std::swap(ja, jb);
@@ -2000,16 +2120,16 @@ int arena_stream_steps(fw_ctx* c, int n) {
 struct fw_pack {
   enum Part {
     X0, V0, BCV, WORD, CBEG, CEND, SLOT, CPOS, CONN, EMAT, J2PAR, YOUNG, POISSON, RHO, POFF, PCNT, PAIRS,
-    HEIGHTS, OCC, RN, RH, RE, RC, RCP, RCS, NPARTS
+    HEIGHTS, OCC, RN, RH, RE, RC, RCP, RCS, PATCH, NPARTS
   };
   int64_t Ns = 0, Es = 0, Bs = 0, Np = 0, Nh = 0, No = 0;
   int64_t Ps = 0, Hs = 0, Ts = 0, CPs = 0;  // stream records (patch_nodes > 0)
   int patch_nodes = 0;
   int no_max = 0, nh_max = 0, ne_max = 0;
   float damp = 0.f;
-  std::vector<StreamPatch> patches;  // offsets local to the scene's record ranges
   unsigned char* block = nullptr;
   bool pinned = false;
+  size_t bytes = 0;  // the block's size (parts 16-byte aligned)
   size_t off[NPARTS] = {}, len[NPARTS] = {};
   int64_t dev_bytes = 0;
   const void* at(Part p) const { return block + off[p]; }
@@ -2112,7 +2232,6 @@ int build_pack(fw_ctx* c, int patch_nodes, bool pinned, fw_pack** out) {
   pk->Ps = (int64_t)ps.patches.size(); pk->Hs = (int64_t)ps.rh.size(); pk->Ts = (int64_t)ps.re.size();
   pk->CPs = (int64_t)ps.rcp.size();
   pk->no_max = ps.no_max; pk->nh_max = ps.nh_max; pk->ne_max = ps.ne_max;
-  pk->patches = ps.patches;
   struct Src { const void* p; size_t bytes; };
   const Src src[fw_pack::NPARTS] = {
       {x0.data(), sizeof(float2) * Ns}, {v0.data(), sizeof(float2) * Ns}, {bcv.data(), sizeof(float2) * Ns},
@@ -2124,13 +2243,15 @@ int build_pack(fw_ctx* c, int patch_nodes, bool pinned, fw_pack** out) {
       {c->h_heights.data(), sizeof(float) * c->h_heights.size()}, {c->h_occ.data(), c->h_occ.size()},
       {ps.rn.data(), sizeof(int32_t) * ps.rn.size()}, {ps.rh.data(), sizeof(int32_t) * ps.rh.size()},
       {ps.re.data(), sizeof(int32_t) * ps.re.size()}, {ps.rc.data(), sizeof(uint2) * ps.rc.size()},
-      {ps.rcp.data(), sizeof(uint16_t) * ps.rcp.size()}, {ps.rcs.data(), sizeof(uint16_t) * ps.rcs.size()}};
+      {ps.rcp.data(), sizeof(uint16_t) * ps.rcp.size()}, {ps.rcs.data(), sizeof(uint16_t) * ps.rcs.size()},
+      {ps.patches.data(), sizeof(StreamPatch) * ps.patches.size()}};
   size_t total = 0;
   for (int k = 0; k < fw_pack::NPARTS; ++k) {
     pk->off[k] = total;
     pk->len[k] = src[k].bytes;
     total += (src[k].bytes + 15) & ~(size_t)15;
   }
+  pk->bytes = total;
   if (pinned && cudaHostAlloc((void**)&pk->block, total ? total : 16, cudaHostAllocDefault) == cudaSuccess) {
     pk->pinned = true;
   } else {
@@ -3229,6 +3350,8 @@ int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_b
       (rc = dalloc(c, &c->a_poisson, E)) || (rc = dalloc(c, &c->a_rho, E)) || (rc = dalloc(c, &d.scene_bad, S)))
     return rc;
   FW_CUDA(c, cudaMemsetAsync(d.scene_bad, 0, sizeof(int32_t) * S, c->stream));
+  c->stage_cap = (size_t)64 << 20;  // packs up to 64 MB commit in one copy (larger ones part by part)
+  if ((rc = dalloc(c, &c->d_stage, c->stage_cap))) return rc;
   c->chunk_cap = E / 32 + N / 32 + 2 * (int64_t)S + 16;
   if ((rc = dalloc(c, &c->d_echunks, c->chunk_cap)) || (rc = dalloc(c, &c->d_nchunks, c->chunk_cap))) return rc;
   std::vector<int32_t> dead(B, S - 1);
@@ -3280,6 +3403,8 @@ int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_b
         (rc = dalloc(c, &de, Tcap)) || (rc = dalloc(c, &dc, Tcap)) || (rc = dalloc(c, &dcp, CPcap)) ||
         (rc = dalloc(c, &dcs, 3 * E)) || (rc = dalloc(c, &dse, Tcap)) || (rc = dalloc(c, &dsn, N)) ||
         (rc = dalloc(c, &derr, 1)) || (rc = dalloc(c, &c->d_plist, Pcap)) || (rc = dalloc(c, &c->d_budget, S)) ||
+        (rc = dalloc(c, &c->d_budget2, S)) || (rc = dalloc(c, &c->d_dt2, S)) ||
+        (rc = dalloc(c, &c->d_slist, S)) || (rc = dalloc(c, &c->d_srng, S)) ||
         (rc = dalloc(c, &d.x_alt, N)) ||
         (rc = dalloc(c, &d.j2_alt, E)))
       return rc;
@@ -3355,54 +3480,67 @@ int fw_arena_commit_pack(fw_ctx* c, const fw_pack* pk, int32_t* scene_out) {
   c->free_scene_ids.pop_back();
   a.live = true;
   // upload (queued on the stream: the steps that follow see the scene, and a
-  // pinned pack's copies run asynchronously)
+  // pinned pack's copy runs asynchronously): the whole pack in one copy to
+  // the device staging buffer, then one kernel puts each part in its range
   Dev& d = c->d;
-  auto up = [&](void* dst, fw_pack::Part part) -> int {
-    if (!pk->len[part]) return FW_OK;
-    FW_CUDA(c, cudaMemcpyAsync(dst, pk->at(part), pk->len[part], cudaMemcpyHostToDevice, c->stream));
-    return FW_OK;
-  };
   const int64_t n0 = a.n0, e0 = a.e0;
-  int rc;
-  if ((rc = up(d.x0 + n0, fw_pack::X0)) || (rc = up(d.x + n0, fw_pack::X0)) || (rc = up(d.v + n0, fw_pack::V0)) ||
-      (rc = up(d.bcv + n0, fw_pack::BCV)) || (rc = up(d.node_word + n0, fw_pack::WORD)) ||
-      (rc = up(d.csr_off + n0, fw_pack::CBEG)) || (rc = up(d.csr_end + n0, fw_pack::CEND)) ||
-      (rc = up(d.csr_slot + 3 * e0, fw_pack::SLOT)) || (rc = up(d.corner_pos + 3 * e0, fw_pack::CPOS)) ||
-      (rc = up(d.conn + 3 * e0, fw_pack::CONN)) || (rc = up(d.emat + e0, fw_pack::EMAT)) ||
-      (rc = up(d.j2par + e0, fw_pack::J2PAR)) || (rc = up(c->a_young + e0, fw_pack::YOUNG)) ||
-      (rc = up(c->a_poisson + e0, fw_pack::POISSON)) || (rc = up(c->a_rho + e0, fw_pack::RHO)) ||
-      (rc = up(d.body_pair_off + a.b0, fw_pack::POFF)) || (rc = up(d.body_pair_cnt + a.b0, fw_pack::PCNT)) ||
-      (rc = up(d.pairs + a.p0, fw_pack::PAIRS)) || (rc = up(d.heights + a.h0, fw_pack::HEIGHTS)) ||
-      (rc = up(d.occ + a.o0, fw_pack::OCC)))
-    return rc;
+  static_assert(kScatterParts == fw_pack::NPARTS + 1, "one scatter slot per pack part, plus the current positions");
+  unsigned char* dst[fw_pack::NPARTS] = {};
+  auto B = [](const void* p) { return (unsigned char*)const_cast<void*>(p); };
+  dst[fw_pack::X0] = B(d.x0 + n0); dst[fw_pack::V0] = B(d.v + n0); dst[fw_pack::BCV] = B(d.bcv + n0);
+  dst[fw_pack::WORD] = B(d.node_word + n0); dst[fw_pack::CBEG] = B(d.csr_off + n0); dst[fw_pack::CEND] = B(d.csr_end + n0);
+  dst[fw_pack::SLOT] = B(d.csr_slot + 3 * e0); dst[fw_pack::CPOS] = B(d.corner_pos + 3 * e0);
+  dst[fw_pack::CONN] = B(d.conn + 3 * e0); dst[fw_pack::EMAT] = B(d.emat + e0); dst[fw_pack::J2PAR] = B(d.j2par + e0);
+  dst[fw_pack::YOUNG] = B(c->a_young + e0); dst[fw_pack::POISSON] = B(c->a_poisson + e0);
+  dst[fw_pack::RHO] = B(c->a_rho + e0); dst[fw_pack::POFF] = B(d.body_pair_off + a.b0);
+  dst[fw_pack::PCNT] = B(d.body_pair_cnt + a.b0); dst[fw_pack::PAIRS] = B(d.pairs + a.p0);
+  dst[fw_pack::HEIGHTS] = B(d.heights + a.h0); dst[fw_pack::OCC] = B(d.occ + a.o0);
+  if (c->a_stream) {
+    dst[fw_pack::RN] = B(c->sd.nodes + n0); dst[fw_pack::RH] = B(c->sd.halo + a.hh0); dst[fw_pack::RE] = B(c->sd.eid + a.t0);
+    dst[fw_pack::RC] = B(c->sd.conn + a.t0); dst[fw_pack::RCP] = B(c->sd.csrp + a.cp0);
+    dst[fw_pack::RCS] = B(c->sd.csrs + 3 * e0); dst[fw_pack::PATCH] = B(c->sd.patch + a.pp0);
+  }
+  if (pk->bytes <= c->stage_cap) {
+    FW_CUDA(c, cudaMemcpyAsync(c->d_stage, pk->block, pk->bytes, cudaMemcpyHostToDevice, c->stream));
+    ArenaScatter sc{};
+    uint32_t most = 0;
+    for (int k = 0; k < fw_pack::NPARTS; ++k) {
+      sc.dst[k] = dst[k];
+      sc.off[k] = (uint32_t)pk->off[k];
+      sc.len[k] = dst[k] ? (uint32_t)pk->len[k] : 0u;
+      most = std::max(most, sc.len[k]);
+    }
+    sc.dst[fw_pack::NPARTS] = B(d.x + n0);  // the current positions start at the rest positions
+    sc.off[fw_pack::NPARTS] = (uint32_t)pk->off[fw_pack::X0];
+    sc.len[fw_pack::NPARTS] = (uint32_t)pk->len[fw_pack::X0];
+    const int gx = (int)std::max<uint32_t>(1u, std::min<uint32_t>((most / 4 + kBlock - 1) / kBlock, 256u));
+    k_arena_scatter<<<dim3(gx, kScatterParts), kBlock, 0, c->stream>>>(c->d_stage, sc);
+    c->launches += 1;
+  } else {  // larger than the staging buffer: one copy per part
+    for (int k = 0; k < fw_pack::NPARTS; ++k)
+      if (dst[k] && pk->len[k])
+        FW_CUDA(c, cudaMemcpyAsync(dst[k], pk->at((fw_pack::Part)k), pk->len[k], cudaMemcpyHostToDevice, c->stream));
+    FW_CUDA(c, cudaMemcpyAsync(d.x + n0, pk->at(fw_pack::X0), pk->len[fw_pack::X0], cudaMemcpyHostToDevice, c->stream));
+  }
   FW_CUDA(c, cudaMemsetAsync(d.j2state + e0, 0, sizeof(float4) * a.ne, c->stream));
   ArenaReloc r{};
   r.n0 = (int)n0; r.e0 = (int)e0; r.b0 = (int)a.b0; r.p0 = (int)a.p0; r.h0 = (int)a.h0; r.o0 = (int)a.o0; r.s = s;
   r.Ns = (int)a.nn; r.Es = (int)a.ne; r.Bs = (int)a.nb; r.Np = (int)a.np;
+  r.damp = pk->damp;
   if (c->a_stream) {
-    int32_t* rn = const_cast<int32_t*>(c->sd.nodes) + n0;
-    int32_t* rh = const_cast<int32_t*>(c->sd.halo) + a.hh0;
-    int32_t* re = const_cast<int32_t*>(c->sd.eid) + a.t0;
-    std::vector<StreamPatch> pat = pk->patches;
-    for (StreamPatch& sp : pat) {
-      sp.node_off += (int)n0;
-      sp.halo_off += (int)a.hh0;
-      sp.elem_off += (int)a.t0;
-      sp.csrp_off += (int)a.cp0;
-      sp.csr_off += (int)(3 * e0);
-      sp.scene = s;
-    }
-    if (!pat.empty())
-      FW_CUDA(c, cudaMemcpyAsync(const_cast<StreamPatch*>(c->sd.patch) + a.pp0, pat.data(),
-                                 sizeof(StreamPatch) * pat.size(), cudaMemcpyHostToDevice, c->stream));
-    if ((rc = up(rn, fw_pack::RN)) || (rc = up(rh, fw_pack::RH)) || (rc = up(re, fw_pack::RE)) ||
-        (rc = up(const_cast<uint2*>(c->sd.conn) + a.t0, fw_pack::RC)) ||
-        (rc = up(const_cast<uint16_t*>(c->sd.csrp) + a.cp0, fw_pack::RCP)) ||
-        (rc = up(const_cast<uint16_t*>(c->sd.csrs) + 3 * e0, fw_pack::RCS)))
-      return rc;
-    r.rn = rn; r.rh = rh; r.re = re; r.Hs = (int)a.nhh; r.Ts = (int)a.nt;
+    r.rn = const_cast<int32_t*>(c->sd.nodes) + n0;
+    r.rh = const_cast<int32_t*>(c->sd.halo) + a.hh0;
+    r.re = const_cast<int32_t*>(c->sd.eid) + a.t0;
+    r.Hs = (int)a.nhh;
+    r.Ts = (int)a.nt;
+    r.patch = const_cast<StreamPatch*>(c->sd.patch) + a.pp0;
+    r.Ps = (int)a.npp;
+    r.hh0 = (int)a.hh0;
+    r.t0 = (int)a.t0;
+    r.cp0 = (int)a.cp0;
+    r.srng = c->d_srng;
   }
-  r.count = std::max<int64_t>({3 * a.ne, a.nn, a.nb, a.np, a.nhh, a.nt});
+  r.count = std::max<int64_t>({3 * a.ne, a.nn, a.nb, a.np, a.nhh, a.nt, a.npp});
   k_arena_reloc<<<(int)std::min<int64_t>((r.count + kBlock - 1) / kBlock, 8 * c->sms), kBlock, 0, c->stream>>>(d, r);
   const int e_lo = (int)e0, e_hi = (int)(e0 + a.ne), n_lo = (int)n0, n_hi = (int)(n0 + a.nn);
   k_prepare_elements<<<(int)((a.ne + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->a_young + e0, c->a_poisson + e0,
@@ -3422,16 +3560,7 @@ int fw_arena_commit_pack(fw_ctx* c, const fw_pack* pk, int32_t* scene_out) {
     c->st_smem_bulk = smem_bulk;
     if ((long)smem_bulk > shared_optin(c) - 64) c->st_bulk = 0;  // staging no longer fits: plain loads
   }
-  const float damp = pk->damp;
-  const int32_t one = 1, zero = 0;
-  auto up1 = [&](void* dst, const void* v) -> int {
-    FW_CUDA(c, cudaMemcpyAsync(dst, v, 4, cudaMemcpyHostToDevice, c->stream));  // staged before the call returns
-    return FW_OK;
-  };
-  if ((rc = up1(d.scene_damp + s, &damp)) || (rc = up1(d.scene_counter + s, &zero)) ||
-      (rc = up1(d.scene_mode_req + s, &one)) || (rc = up1(d.scene_active + s, &one)) ||
-      (rc = up1(d.scene_bad + s, &zero)))
-    return rc;
+  int rc;
   if ((rc = check_kernel(c, "arena commit"))) return rc;
   c->ascenes[s] = a;
   for (int64_t b = 0; b < a.nb; ++b) c->a_body_scene[a.b0 + b] = s;
@@ -3514,18 +3643,31 @@ int fw_step_served_n(fw_ctx* c, const float* dt, int32_t n_steps) {
   return FW_OK;
 }
 
-int fw_step_served_budget(fw_ctx* c, const float* dt, const int32_t* budget, int32_t n_steps) {
-  if (!c || !dt || !budget || n_steps < 0) return FW_ERR_ARG;
+int fw_step_served_budget(fw_ctx* c, const float* dt, const int32_t* budget, const float* dt_next,
+                          const int32_t* budget_next, int32_t n_steps) {
+  if (!c || !dt || !budget || n_steps < 0 || (!dt_next) != (!budget_next)) return FW_ERR_ARG;
   if (!c->arena || !c->a_stream)
     return fail(c, FW_ERR_STATE, "fw_step_served_budget needs a stream arena (fw_set_path FW_PATH_STREAM before "
                                  "fw_arena_init)");
   if (n_steps == 0) return FW_OK;
+  // staged before the calls return
   c->h_budget.assign(budget, budget + c->S);
   FW_CUDA(c, cudaMemcpyAsync(c->d_budget, c->h_budget.data(), sizeof(int32_t) * c->S, cudaMemcpyHostToDevice,
-                             c->stream));  // staged before the call returns
+                             c->stream));
   c->d.scene_budget = c->d_budget;
+  if (budget_next) {
+    c->h_budget2.assign(budget_next, budget_next + c->S);
+    c->h_dt2.assign(dt_next, dt_next + c->S);
+    FW_CUDA(c, cudaMemcpyAsync(c->d_budget2, c->h_budget2.data(), sizeof(int32_t) * c->S, cudaMemcpyHostToDevice,
+                               c->stream));
+    FW_CUDA(c, cudaMemcpyAsync(c->d_dt2, c->h_dt2.data(), sizeof(float) * c->S, cudaMemcpyHostToDevice, c->stream));
+    c->d.scene_budget_next = c->d_budget2;
+    c->d.scene_dt_next = c->d_dt2;
+  }
   const int rc = fw_step_served_n(c, dt, n_steps);
   c->d.scene_budget = nullptr;
+  c->d.scene_budget_next = nullptr;
+  c->d.scene_dt_next = nullptr;
   return rc;
 }
 

@@ -241,6 +241,7 @@ class Server:
         self.admit_span = 8          # call length while admissions wait (stream arenas)
         self.host_us = 100.0         # host time of one loop iteration, refined as the loop runs
         self.device_s = 0.0          # device time of the native calls (CUDA events around each call)
+        self.trace = None            # a list: one (span, scenes in the call, substeps they ran) per call
 
     def _build(self, body):
         """Host-side preparation of a body: its domains, scene layout and its
@@ -255,6 +256,15 @@ class Server:
         for b in bodies:
             if b not in self._prep:
                 self._prep[b] = self._build(b)
+
+    def _queued_work(self, queue, body):
+        """Substeps the requests waiting for a body will run (request counts
+        raised to the body's stable count, as the jobs will be)."""
+        ent = self._prep.get(body)
+        if ent is None:
+            return sum(r.substeps for r in queue)
+        st = ent[0].stableTime
+        return sum(request_substeps(r, self.frame_dt, st) for r in queue)
 
     def close(self):
         """Wait for the arena's stream, then free the packs and the arena."""
@@ -325,7 +335,10 @@ class Server:
         busy_m = np.zeros(S, dtype=bool)
         init_m = np.zeros(S, dtype=bool)
         n_el = np.zeros(S, dtype=np.int64)
+        adm_set, adm_order = set(), []           # bodies waiting for admission, most queued work first
         ran = np.zeros(S, dtype=np.int32)        # substeps each scene runs in the current call
+        bud2 = np.zeros(S, dtype=np.int32)       # ... in its second segment (stream arenas)
+        dt2 = np.zeros(S, dtype=np.float32)
         budgets = self.arena.path == "stream"  # per-scene budgets: a call need not stop at each request end
         dts = np.zeros(S, dtype=np.float32)
         inflight = collections.deque()
@@ -377,9 +390,15 @@ class Server:
             # bodies are uploaded within a host-time budget per iteration, so a
             # burst of first requests cannot stall the requests in flight
             t_adm = time.perf_counter()
-            for body in sorted(ready):
+            # resident bodies first; then bodies to admit, the most queued work
+            # first (the longest queues set the end of a burst)
+            new_bodies = {b for b in ready if b not in self.resident}
+            if new_bodies != adm_set:  # bodies joined (or left) the wait: order them again
+                adm_set = new_bodies
+                adm_order = sorted(new_bodies, key=lambda b: (-self._queued_work(queues[b], b), b))
+            for body in sorted(b for b in ready if b in self.resident) + adm_order:
                 if body not in self.resident and time.perf_counter() - t_adm > self.admit_budget_s:
-                    continue  # admitted in a later iteration
+                    break  # admitted in a later iteration
                 adm = self._admit(body, t0)
                 if not adm:
                     continue
@@ -395,6 +414,9 @@ class Server:
                 busy_m[s] = True
                 init_m[s] = job.init
                 n_el[s] = self.arena.layouts[s].n_elems
+            if adm_set:
+                adm_order = [b for b in adm_order if b not in self.resident]
+                adm_set = set(adm_order)
             if not busy:
                 if not arrivals and not pending_done and ready and not any(b in self.resident for b in ready) \
                         and time.perf_counter() - t_adm <= self.admit_budget_s:
@@ -404,33 +426,73 @@ class Server:
                 if arrivals and realtime:
                     time.sleep(max(0.0, arrivals[0].arrival - (time.perf_counter() - t0)))
                 continue
+            waiting = budgets and bool(adm_set)  # bodies wait for admission
+            if waiting and len(pending_done) >= 2:
+                # bodies wait for admission and the GPU still has two calls to run:
+                # spend this iteration admitting rather than queueing a third call
+                evict(self._retire(pending_done, done_at, failed, status, t0, block=False))
+                continue
             np.copyto(dts, np.where(busy_m, cur_dt, np.float32(0.0)))
+            # a call shorter than one host iteration's worth of device time idles the GPU
+            floor = max(1, int(self.host_us / self.us_per_substep))
             cap = self.max_batch_substeps
-            if realtime and arrivals:
-                # end the call near the next arrival, but not before one host
-                # iteration's worth of device time (a shorter call idles the GPU)
+            if realtime and arrivals:  # end the call near the next arrival
                 gap_us = (arrivals[0].arrival - (time.perf_counter() - t0)) * 1e6
-                cap = min(cap, max(1, int(max(gap_us, self.host_us) / self.us_per_substep)))
-            if budgets and any(b not in self.resident for b in ready):
-                cap = min(cap, self.admit_span)  # bodies wait for admission: short calls let it catch up
+                cap = min(cap, max(floor, int(gap_us / self.us_per_substep)))
+            if waiting:
+                cap = min(cap, max(floor, self.admit_span))  # bodies wait for admission: let it catch up
             ev0 = torch.cuda.Event(enable_timing=True)
             ev0.record(self.stream)
+            second = []  # (scene, the body's next job or None for the request's own next run)
             if budgets:
-                # one call spans request ends: each scene runs its own remaining substeps
+                # one call spans request ends: each scene runs its own remaining
+                # substeps, then its next run -- the request's remainder at its
+                # own dt, or the body's next queued request -- within the call
                 span = int(min(cap, left[busy_m].max()))
                 np.copyto(ran, np.where(busy_m, np.minimum(left, span), 0))
-                self.arena.native.step_served_budget(dts, ran, span)
+                bud2.fill(0)
+                for s in np.nonzero(busy_m & (left < span))[0].tolist():
+                    job = busy[s]
+                    if job.pos + 1 < len(job.runs):
+                        n2, d2 = job.runs[job.pos + 1]
+                        nxt = None
+                    elif queues[job.req.body]:
+                        nxt = _Job(queues[job.req.body][0], self.frame_dt, self.arena.layouts[s].stableTime)
+                        n2, d2 = nxt.runs[0]
+                    else:
+                        continue
+                    bud2[s] = min(n2, span - int(left[s]))
+                    dt2[s] = np.float32(d2)
+                    second.append((s, nxt))
+                if second:
+                    self.arena.native.step_served_budget(dts, ran, span, dt2, bud2)
+                else:
+                    self.arena.native.step_served_budget(dts, ran, span)
             else:
                 span = int(min(cap, left[busy_m].min()))
                 np.copyto(ran, np.where(busy_m, span, 0))
                 self.arena.native.step_served_n(dts, span)
             self.arena.native.scene_status(S, out=status[slot], asynchronous=True)
+            if self.trace is not None:
+                self.trace.append((span, int(busy_m.sum()), int(ran.sum()) + int(bud2.sum()) if second else int(ran.sum())))
             n_sub += span
             n_calls += 1
             self.element_steps += int((n_el * ran).sum()) - int(n_el[busy_m & init_m].sum())
             init_m[busy_m] = False
             left[busy_m] -= ran[busy_m]
             finished = []
+            for s, nxt in second:  # the second segments (their first run has just ended)
+                job = busy[s]
+                self.element_steps += int(n_el[s]) * int(bud2[s])
+                if nxt is None:
+                    job.pos += 1
+                else:
+                    finished.append(job)
+                    queues[job.req.body].popleft()
+                    nxt.start = now
+                    busy[s] = job = nxt
+                cur_dt[s] = job.runs[job.pos][1]
+                left[s] = job.runs[job.pos][0] - int(bud2[s])
             for s in np.nonzero(busy_m & (left == 0))[0].tolist():
                 job = busy[s]
                 job.pos += 1

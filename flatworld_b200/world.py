@@ -12,6 +12,7 @@ the same per-scene results as S separate loops.
 
 from __future__ import annotations
 
+import functools
 import warnings
 from dataclasses import dataclass
 
@@ -600,7 +601,13 @@ def _rigid_bcs(bcs, f):
 
 def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):
     """advanceWithTime's float64 substep loop (explicitloop.py:573-586) as a list
-    of (count, dt) runs."""
+    of (count, dt) runs.  Memoised: a request loop asks for the same few
+    (frame, dt) pairs over and over, and the loop walks every substep."""
+    return list(_substep_schedule(float(frame_dt), float(stable), float(default_dt), bool(adaptive)))
+
+
+@functools.lru_cache(maxsize=4096)
+def _substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive: bool):
     remaining = float(frame_dt)
     runs = []
     while remaining > 1e-12:
@@ -611,4 +618,4 @@ def substep_schedule(frame_dt: float, stable: float, default_dt: float, adaptive
         else:
             runs.append([1, sub])
         remaining -= sub
-    return [(n, d) for n, d in runs]
+    return tuple((n, d) for n, d in runs)

@@ -341,12 +341,16 @@ int fw_step_served(fw_ctx* ctx, const float* dt);
 int fw_step_served_n(fw_ctx* ctx, const float* dt, int32_t n_steps);
 
 /* Stream arenas: n_steps substeps of fw_step_served in which scene s (dt[s]
- * > 0) runs only its first budget[s] substeps and sits out the rest (its
- * state carried unchanged); budget has one entry per scene.  A request loop
- * passes each in-flight request's remaining substeps, so one call can span
- * many request ends.  Same bits as calls of fw_step_served_n that stop at
- * each end. */
-int fw_step_served_budget(fw_ctx* ctx, const float* dt, const int32_t* budget, int32_t n_steps);
+ * > 0) runs only its first budget[s] substeps at dt[s], then (when given)
+ * budget_next[s] substeps at dt_next[s], and sits out the rest (its state
+ * carried unchanged); every array has one entry per scene, dt_next and
+ * budget_next both or neither.  A request loop passes each in-flight
+ * request's remaining substeps, and the next run (the request's own
+ * remainder, or the body's next queued request), so one call spans many
+ * request ends and a body does not wait for the call to end to go on.  Same
+ * bits as calls of fw_step_served_n that stop at each end. */
+int fw_step_served_budget(fw_ctx* ctx, const float* dt, const int32_t* budget, const float* dt_next,
+                          const int32_t* budget_next, int32_t n_steps);
 
 /* Mark scenes active (1) / frozen (0).  Frozen scenes keep their state and do
  * not advance. */

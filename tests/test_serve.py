@@ -143,29 +143,45 @@ def test_stream_arena_idle_scenes_keep_their_state(patch):
 
 
 def test_stream_arena_budgets_equal_separate_calls():
-    """fw_step_served_budget: in one call of n substeps each scene runs only
-    its own budget and then sits out (its state carried unchanged between the
-    buffers) -- the same bits as running each scene's substeps alone."""
+    """fw_step_served_budget: in one call of n substeps each scene runs its
+    budget at its dt, then (second segment) its next budget at another dt,
+    then sits out (its state carried unchanged between the buffers) -- the
+    same bits as running each scene's runs alone, in order."""
     ar = Arena(60_000, 120_000, 16, 16, 16, 1 << 16, 1 << 22, path="stream")
     sc = [ar.insert(small_body(i)) for i in range(3)]
-    dt = np.float32(5e-5)
-    ran = dict.fromkeys(sc, 0)
-    for n, budgets in ((9, (9, 4, 1)), (16, (3, 16, 11)), (7, (7, 0, 2)), (12, (1, 12, 12))):
+    d1, d2 = np.float32(5e-5), np.float32(3e-5)
+    runs = {s_: [] for s_ in sc}  # (substeps, dt) in order, per scene
+    plan = (  # n, per scene (budget, budget of the second segment at d2)
+        (9, ((9, 0), (4, 5), (1, 0))),
+        (16, ((3, 13), (16, 0), (11, 2))),
+        (7, ((7, 0), (0, 0), (2, 5))),
+        (12, ((1, 11), (12, 0), (12, 0))),
+    )
+    for n, budgets in plan:
         dts = np.zeros(ar.S, np.float32)
         bud = np.zeros(ar.S, np.int32)
-        for s_, b_ in zip(sc, budgets):
-            if b_:
-                dts[s_] = dt
-                bud[s_] = b_
-                ran[s_] += b_
-        ar.native.step_served_budget(dts, bud, n)
+        dt_next = np.zeros(ar.S, np.float32)
+        bud_next = np.zeros(ar.S, np.int32)
+        for s_, (b1, b2) in zip(sc, budgets):
+            if b1:
+                dts[s_], bud[s_] = d1, b1
+                runs[s_].append((b1, d1))
+                if b2:
+                    dt_next[s_], bud_next[s_] = d2, b2
+                    runs[s_].append((b2, d2))
+        ar.native.step_served_budget(dts, bud, n, dt_next, bud_next)
     ar.native.synchronize()
     for s_, body in zip(sc, range(3)):
         lp = fw.ExplicitLoop(5e-5, small_body(body), useAdapativeDT=False, path="gather")
-        lp.advance_n(ran[s_] - 1)  # the first substep is the construction step
+        first = True
+        for k, d in runs[s_]:
+            k -= 1 if first else 0  # the first substep is the construction step
+            first = False
+            if k:
+                lp.advance_n(k, float(d))
         n = lp._packed.N
-        assert np.array_equal(ar.coords(s_), lp.femSpringManager.coords.numpy()[:n]), (s_, ran[s_])
-        assert np.array_equal(ar.velocities(s_), lp.femSpringManager.V.numpy()[:n]), (s_, ran[s_])
+        assert np.array_equal(ar.coords(s_), lp.femSpringManager.coords.numpy()[:n]), (s_, runs[s_])
+        assert np.array_equal(ar.velocities(s_), lp.femSpringManager.V.numpy()[:n]), (s_, runs[s_])
     gather = Arena(10_000, 20_000, 4, 4, 4, 1, 1, path="gather")
     with pytest.raises(_native.NativeError, match="stream arena"):
         gather.native.step_served_budget(np.zeros(gather.S, np.float32), np.zeros(gather.S, np.int32), 1)
