@@ -34,6 +34,7 @@ FW_OPT_TEST_WITHHOLD = 7
 FW_OPT_STREAM_PATCH = 8
 FW_OPT_STREAM_MINB = 9
 FW_OPT_STREAM_BULK = 10
+FW_OPT_RES_THREADS = 11
 FW_PACK_PINNED = 1
 
 _lock = threading.Lock()

@@ -16,12 +16,14 @@
 // ("group 1").  Per substep, per CTA:
 //   1. wait until every CTA has arrived for the previous substep (bounded
 //      spin), then fetch halo positions and the body boxes (one L2 round trip)
-//   2. broad-phase gates; corner forces of the cut triangles
-//   3. group-1 nodes: contact, corner forces summed in ascending element
-//      order, boundary conditions, symplectic Euler; publish positions; box
-//      reduction (ordered-int atomics); then fence and arrive
-//   4. group-2 nodes, then the interior triangles of the next substep -- this
-//      work overlaps the other CTAs' progress towards the barrier
+//   2. broad-phase gates; corner forces of the cut triangles (the interior
+//      triangles were done by the other warps meanwhile)
+//   3. all threads: every owned node -- contact, corner forces summed in
+//      ascending element order, boundary conditions, symplectic Euler --
+//      group 1 first, each group-1 position published as soon as it is
+//      computed, the body-box reduction (ordered-int atomics)
+//   4. box hand-off (fence and arrive), then the interior triangles of the
+//      next substep -- this work overlaps the other CTAs' progress
 // The node sums use the same ascending-element order as the gather path, so
 // both paths produce identical bits.  Every wait is bounded: after
 // kSpinLimit polls the CTA sets the error flag and leaves the loop, so a
@@ -270,14 +272,15 @@ __device__ __forceinline__ void named_bar(int id, int count) {
 }
 
 // Warp-specialised substep loop.  Warps [0, FRONT) run the critical chain
-// (barrier wait, halo and box loads, gates, cut triangles, group-1 nodes,
-// publish + arrive); the other warps compute the interior triangles of the
-// next substep and the group-2 nodes, which need no data from other CTAs.
-// Shared-memory hazards: interior and cut triangles write disjoint corner
-// slots; group-1 and group-2 nodes are disjoint; the halo part of x is only
-// read by the front warps; two CTA-wide barriers per substep order the rest.
-template <int FRONT, bool LL>
-__global__ void __launch_bounds__(kResThreads, 1)
+// (barrier wait, halo and box loads, gates, cut triangles, box hand-off);
+// the other warps compute the interior triangles of the next substep, which
+// need no data from other CTAs; all warps update the owned nodes together,
+// group 1 first (published as they are computed).  Shared-memory hazards:
+// interior and cut triangles write disjoint corner slots; the halo part of x
+// is only read by the front warps; two CTA-wide barriers per substep order
+// the rest.
+template <int FRONT, bool LL, int NT>
+__global__ void __launch_bounds__(NT, 1)
 k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t ep0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_abort;
@@ -347,7 +350,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
     }
   if (!front)
     for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
-  const int g1_trips = (P.n_g1 + FT - 1) / FT;
+  const int node_trips = (P.no + T - 1) / T;
   for (int k = 0; k < nsteps; ++k) {
     const int g = step0 + k;
     if (front) {
@@ -464,29 +467,35 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
     }
     __syncthreads();  // every triangle of substep k is done
     if (s_abort) break;
-    if (front) {
+    {
+      // Every owned node, all threads together (one pass when the patch has
+      // at most T nodes); the nodes other CTAs read or that feed the body box
+      // ([0, n_g1)) are the first ones, and each is published as soon as it
+      // is computed.
       float2* dst = r.xpub + (size_t)((k + 1) & 1) * N;
       unsigned long long* dll = r.xll + (size_t)((k + 1) & 1) * N * 2;
       const uint32_t ep_out = ep0 + (uint32_t)k + 1u;
       int* box_w = r.aabb3 + (size_t)((g + 1) % 3) * B * 4;
-      for (int trip = 0; trip < g1_trips; ++trip) {
-        const int i = trip * FT + t;
+      for (int trip = 0; trip < node_trips; ++trip) {
+        const int i = trip * T + t;
         bool bnd = false;
         int body = 0;
         float2 x = make_float2(0.f, 0.f);
-        if (i < P.n_g1) {
+        if (i < P.no) {
           x = res_node(d, s, heights, occ, i, dt, damp);
-          const uint32_t w = s.w[i];
-          body = (int)(w >> fw::NODE_BODY_SHIFT);
-          bnd = (w & fw::NODE_BOUNDARY) != 0;
-          const int gid = s.gid[i];
-          if (gid < 0 && !(k == 0 && (int)blockIdx.x == r.withhold_cta)) {
-            const size_t gi = (size_t)(gid & 0x7FFFFFFF);
-            if (LL) {
-              ll_store(dll + 2 * gi, ll_pack(ep_out, __float_as_uint(x.x)));
-              ll_store(dll + 2 * gi + 1, ll_pack(ep_out, __float_as_uint(x.y)));
-            } else {
-              __stcg(dst + gi, x);
+          if (i < P.n_g1) {
+            const uint32_t w = s.w[i];
+            body = (int)(w >> fw::NODE_BODY_SHIFT);
+            bnd = (w & fw::NODE_BOUNDARY) != 0;
+            const int gid = s.gid[i];
+            if (gid < 0 && !(k == 0 && (int)blockIdx.x == r.withhold_cta)) {
+              const size_t gi = (size_t)(gid & 0x7FFFFFFF);
+              if (LL) {
+                ll_store(dll + 2 * gi, ll_pack(ep_out, __float_as_uint(x.x)));
+                ll_store(dll + 2 * gi + 1, ll_pack(ep_out, __float_as_uint(x.y)));
+              } else {
+                __stcg(dst + gi, x);
+              }
             }
           }
         }
@@ -515,27 +524,27 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           }
         }
       }
-      named_bar(1, FT);
+    }
+    __syncthreads();  // every owned node of substep k is updated; this CTA's box partials are final
+    if (front) {
       const bool withhold = k == 0 && (int)blockIdx.x == r.withhold_cta;
       if (LL) {
         if (t < 4 * B && !withhold) {  // this CTA's partial box of body t / 4, component t % 4
           unsigned long long* bdst =
               r.bll + ((size_t)((k + 1) % kBoxRing) * B * r.P + (size_t)(t >> 2) * r.P + blockIdx.x) * 4;
-          ll_store(bdst + (t & 3), ll_pack(ep_out, (uint32_t)s_pbox[t]));
+          ll_store(bdst + (t & 3), ll_pack(ep0 + (uint32_t)k + 1u, (uint32_t)s_pbox[t]));
         }
         if (t < 4 * B) {
           s_lbox[t] = s_pbox[t];
           s_pbox[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
         }
         if (t == 0) s_need = ((k + 1) % kBoxSync == 0 || r.rec_gates != nullptr) ? 1 : 0;
+        named_bar(1, FT);  // s_lbox and s_need before the next substep's gate decisions
       } else if (t == 0 && !withhold) {
         cuda::atomic_ref<int, cuda::thread_scope_device> a(*r.bar);
         a.fetch_add(1, cuda::memory_order_release);
       }
-    } else {
-      for (int i = P.n_g1 + bt; i < P.no; i += BT) res_node(d, s, heights, occ, i, dt, damp);
     }
-    __syncthreads();  // every owned node of substep k is updated
     if (r.rec_x && k + 1 < nsteps)  // owned positions stay as they are until the next CTA barrier
       for (int i = t; i < P.no; i += T) {
         r.rec_x[(size_t)(k + 1) * N + (s.gid[i] & 0x7FFFFFFF)] = s.x[i];
@@ -753,13 +762,21 @@ k_res_adj(Dev d, Res r, Adj a, const float2* __restrict__ rec_x, const float2* _
 }
 
 using ResKernel = void (*)(Dev, Res, int, int, float, float, uint32_t);
-constexpr int kFrontChoices[] = {2, 4, 6, 8};
-inline ResKernel res_kernel(int front, bool ll) {
+constexpr int kFrontChoices[] = {2, 4, 6, 8};          // of 16 warps (512 threads)
+constexpr int kFrontChoices1024[] = {8, 12, 16};       // of 32 warps (1024 threads, 64 registers)
+inline ResKernel res_kernel(int front, bool ll, int threads) {
+  if (threads == 1024) {
+    switch (front) {
+      case 8: return ll ? k_resident<8, true, 1024> : k_resident<8, false, 1024>;
+      case 16: return ll ? k_resident<16, true, 1024> : k_resident<16, false, 1024>;
+      default: return ll ? k_resident<12, true, 1024> : k_resident<12, false, 1024>;
+    }
+  }
   switch (front) {
-    case 2: return ll ? k_resident<2, true> : k_resident<2, false>;
-    case 6: return ll ? k_resident<6, true> : k_resident<6, false>;
-    case 8: return ll ? k_resident<8, true> : k_resident<8, false>;
-    default: return ll ? k_resident<4, true> : k_resident<4, false>;
+    case 2: return ll ? k_resident<2, true, 512> : k_resident<2, false, 512>;
+    case 6: return ll ? k_resident<6, true, 512> : k_resident<6, false, 512>;
+    case 8: return ll ? k_resident<8, true, 512> : k_resident<8, false, 512>;
+    default: return ll ? k_resident<4, true, 512> : k_resident<4, false, 512>;
   }
 }
 

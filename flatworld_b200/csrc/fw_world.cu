@@ -1163,6 +1163,7 @@ struct fw_ctx {
   // path selection and the resident (shared-memory) step
   int path_req = FW_PATH_AUTO, patches_req = 0;
   int front_warps = 6;
+  int res_threads = 512;     // FW_OPT_RES_THREADS
   int res_sync = 0;          // FW_OPT_RES_SYNC
   int64_t wait_limit = 0;    // FW_OPT_WAIT_LIMIT (0: the built-in limits)
   int withhold_cta = -1;     // FW_OPT_TEST_WITHHOLD
@@ -1802,7 +1803,7 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
     return 1;
   }
   const bool ll = c->res_sync == 0 && c->B <= kLLMaxBodies;
-  ResKernel kern = res_kernel(c->front_warps, ll);
+  ResKernel kern = res_kernel(c->front_warps, ll, c->res_threads);
   // The attribute is per function and process-wide: every context sets it to
   // the device maximum, so a context with small patches cannot lower the limit
   // below what another context launches with.
@@ -1811,7 +1812,7 @@ int build_resident(fw_ctx* c, const std::vector<int32_t>& off, const std::vector
   cudaError_t e1 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         optin - (int)fa.sharedSizeBytes);
   int per_sm = 0;
-  cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kResThreads, smem);
+  cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, c->res_threads, smem);
   if (e1 != cudaSuccess || e2 != cudaSuccess || per_sm * sms < P) {
     cudaGetLastError();
     c->res_reason = "patches cannot all be resident";
@@ -1872,8 +1873,8 @@ int launch_resident(fw_ctx* c, int n) {
   k_res_prologue<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, ll ? 1 : 0);
   float dt = c->d.dt_uniform, damp = c->h_damp[0];
   void* args[] = {(void*)&c->d, (void*)&c->res, (void*)&step0, (void*)&n, (void*)&dt, (void*)&damp, (void*)&ep0};
-  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)res_kernel(c->front_warps, ll), dim3(c->res.P),
-                                         dim3(kResThreads), args, c->res_smem, c->stream));
+  FW_CUDA(c, cudaLaunchCooperativeKernel((const void*)res_kernel(c->front_warps, ll, c->res_threads),
+                                         dim3(c->res.P), dim3(c->res_threads), args, c->res_smem, c->stream));
   if (ll)
     k_res_epilogue_ll<<<1, 256, 0, c->stream>>>(c->d, c->res, step0, n);
   else
@@ -3204,9 +3205,21 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
     case FW_OPT_FRONT_WARPS: {
       if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_FRONT_WARPS after fw_finalize");
       bool ok = false;
-      for (int v : kFrontChoices) ok |= v == value;
-      if (!ok) return fail(c, FW_ERR_ARG, "FW_OPT_FRONT_WARPS must be 2, 4, 6 or 8");
+      if (c->res_threads == 1024)
+        for (int v : kFrontChoices1024) ok |= v == value;
+      else
+        for (int v : kFrontChoices) ok |= v == value;
+      if (!ok)
+        return fail(c, FW_ERR_ARG, "FW_OPT_FRONT_WARPS must be %s", c->res_threads == 1024 ? "8, 12 or 16 (1024 threads)"
+                                                                                          : "2, 4, 6 or 8");
       c->front_warps = value;
+      return FW_OK;
+    }
+    case FW_OPT_RES_THREADS: {
+      if (c->finalized) return fail(c, FW_ERR_STATE, "FW_OPT_RES_THREADS after fw_finalize");
+      if (value != 512 && value != 1024) return fail(c, FW_ERR_ARG, "FW_OPT_RES_THREADS must be 512 or 1024");
+      c->res_threads = value;
+      c->front_warps = value == 1024 ? 12 : 6;  // the default split for that size
       return FW_OK;
     }
     case FW_OPT_BLOCK_ELEMS:

@@ -246,7 +246,7 @@ class ExplicitLoop:
     def __init__(self, dt, domains, joints=[], ties=None, damping=0.0, useAdapativeDT=True,
                  skip_spatial_hash=False, considerRigidRigidContact=True, use_pd=0,
                  mass_scaling_dt=0.0, max_contact_velocity=50.0, device=0, path="auto", patches=0,
-                 front_warps=0, res_sync=0):
+                 front_warps=0, res_sync=0, res_threads=0):
         if joints:
             raise NotImplementedError("joints belong to the rigid-body constraint solver, outside flatworld_b200")
         if not considerRigidRigidContact and any(d.type == DomainType.RIGID for d in domains):
@@ -272,7 +272,7 @@ class ExplicitLoop:
         self._counter_py = 0
         self._packed = PackedWorld([layout])
         self._native = build_native(self._packed, device=device, path=path, patches=patches,
-                                    front_warps=front_warps, res_sync=res_sync)
+                                    front_warps=front_warps, res_sync=res_sync, res_threads=res_threads)
         if layout.mass_scaling_dt > 0.0:  # applyMassScaling after setGlobalAABB (explicitloop.py:168-169)
             self._native.mass_scaling(float(np.float32(layout.mass_scaling_dt)))
         self.path, self.patches = self._native.get_path()

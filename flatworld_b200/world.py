@@ -441,15 +441,19 @@ class PackedWorld:
 
 
 def build_native(packed: PackedWorld, device: int = 0, path: str = "auto", patches: int = 0,
-                 front_warps: int = 0, res_sync: int = 0, stream_patch: int = 0) -> _native.NativeWorld:
+                 front_warps: int = 0, res_sync: int = 0, stream_patch: int = 0,
+                 res_threads: int = 0) -> _native.NativeWorld:
     """Create the device world.  ``path``: "auto" (shared-memory-resident step
     when the world fits on chip, else the gather step), "gather" or "resident";
     ``patches`` / ``front_warps``: resident-step tuning (0 = default);
     ``res_sync``: 0 = flag-in-data hand-off between resident CTAs, 1 = arrival
     counter (FW_OPT_RES_SYNC); ``stream_patch``: owned nodes per patch of the
-    stream step (64 or 128; 0 = default)."""
+    stream step (64 or 128; 0 = default); ``res_threads``: threads of a
+    resident CTA (512 or 1024; 0 = default)."""
     nw = _native.NativeWorld(device)
     nw.set_path(_native.PATHS[path], patches)
+    if res_threads:
+        nw.set_option(_native.FW_OPT_RES_THREADS, res_threads)
     if front_warps:
         nw.set_option(_native.FW_OPT_FRONT_WARPS, front_warps)
     if res_sync:

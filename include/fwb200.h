@@ -303,6 +303,12 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
 #define FW_OPT_STREAM_PATCH 8
 #define FW_OPT_STREAM_MINB 9
 #define FW_OPT_STREAM_BULK 10
+/* FW_OPT_RES_THREADS: threads of a resident CTA, 512 (default; up to 128
+ * registers per thread) or 1024 (32 warps, 64 registers); before
+ * fw_finalize, and before FW_OPT_FRONT_WARPS, whose choices it sets: 2, 4,
+ * 6 or 8 of 16 warps (default 6), or 8, 12 or 16 of 32 (default 12).  Same
+ * bits. */
+#define FW_OPT_RES_THREADS 11
 int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
 
 /* Checkpoint / resume: copy the whole step state (positions, velocities, J2

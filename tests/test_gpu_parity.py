@@ -273,6 +273,24 @@ def test_resident_patch_counts_bitwise(patches, res_sync):
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
 
 
+@pytest.mark.parametrize("res_sync", [0, 1], ids=["flag-in-data", "counter"])
+@pytest.mark.parametrize("threads,front", [(512, 2), (512, 8), (1024, 8), (1024, 12), (1024, 16)])
+def test_resident_launch_shapes_bitwise(threads, front, res_sync):
+    """Every resident CTA size and split of front warps gives the gather
+    path's bits (the node pass and the warp split change no sum's order)."""
+    doms = lambda: scenes.plain_large_scene(fw, n=64, hf_offset=0.17)  # noqa: E731
+    a = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="resident", res_threads=threads, front_warps=front,
+                        res_sync=res_sync)
+    b = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="gather")
+    assert a.path == 2
+    for _ in range(10):
+        a.advanceWithTime(FRAME)
+        b.advanceWithTime(FRAME)
+    xa, va = gpu_state(a)
+    xb, vb = gpu_state(b)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
 @pytest.mark.parametrize("n_bodies", [3, 10])
 def test_resident_multi_body_bitwise(n_bodies):
     """Several bodies in one scene, all three laws, plane contact: the body
