@@ -52,13 +52,12 @@ struct StreamPatch {
   int pad[3];
 };
 
-// Static data of one patch triangle, in patch order.
+// Static data of one patch triangle, in patch order (32 B; its local corners
+// are StreamDev::conn and its global index, needed by J2 triangles only,
+// StreamDev::eid, at the same position).
 struct __align__(16) StreamElem {
   ElemMat m;   // emat[e]
   float4 ji;   // jinv[e]
-  uint2 conn;  // local corners: x = a | b << 16, y = c | writer << 16 (writer: this patch owns corner a)
-  int e;       // global triangle index (J2 state)
-  int pad;
 };
 
 // Static data of one owned node, in patch order.
@@ -77,7 +76,7 @@ struct StreamDev {
   const uint16_t* csrp;
   const uint16_t* csrs;
   int no_max, nh_max, ne_max;
-  StreamElem* elem;  // built from eid/conn by k_stream_elems
+  StreamElem* elem;  // built from eid by k_stream_elems
   StreamNode* node;  // built from nodes by k_stream_nodes
   int* err;          // != 0: a staged copy did not complete in time
   const int32_t* list;  // arena worlds: CTA i runs patch list[i] (the active scenes' patches); else patch i
@@ -94,16 +93,13 @@ __global__ void k_stream_nodes(Dev d, const int32_t* nodes, StreamNode* out, int
   out[i] = r;
 }
 
-__global__ void k_stream_elems(Dev d, const int32_t* eid, const uint2* conn, StreamElem* out, int n) {
+__global__ void k_stream_elems(Dev d, const int32_t* eid, StreamElem* out, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int e = eid[i];
   StreamElem r;
   r.m = d.emat[e];
   r.ji = d.jinv[e];
-  r.conn = conn[i];
-  r.e = e;
-  r.pad = 0;
   out[i] = r;
 }
 
@@ -121,19 +117,23 @@ __global__ void k_stream_carry(StreamDev sd, const float2* __restrict__ x_from, 
     x_to[g] = x_from[g];
   }
   if (has_j2)
-    for (int q = threadIdx.x; q < P.ne; q += blockDim.x) {
-      const StreamElem& r = sd.elem[P.elem_off + q];
-      if (r.conn.y >> 16) j2_to[r.e] = j2_from[r.e];
-    }
+    for (int q = threadIdx.x; q < P.ne; q += blockDim.x)
+      if (sd.conn[P.elem_off + q].y >> 16) {
+        const int e = sd.eid[P.elem_off + q];
+        j2_to[e] = j2_from[e];
+      }
 }
 
 // One triangle of the patch (element_step on shared positions).
-__device__ __forceinline__ void stream_element(const Dev& d, const float2* sx, float2* sf, int q, int e, uint2 c,
-                                               ElemMat m, float4 ji, const float4* j2_in, float4* j2_out) {
+__device__ __forceinline__ void stream_element(const Dev& d, const float2* sx, float2* sf, int q,
+                                               const int32_t* eid, uint2 c, ElemMat m, float4 ji,
+                                               const float4* j2_in, float4* j2_out) {
   float4 j2 = make_float4(0.f, 0.f, 0.f, 0.f);
   float sy = 0.f, H = 0.f;
   const bool mises = fw::elem_type(m.word) == fw::MAT_MISES;
-  if (mises) {
+  int e = 0;
+  if (mises) {  // the global index only for J2 triangles (their state and parameters)
+    e = eid[q];
     j2 = j2_in[e];
     const float2 jp = d.j2par[e];
     sy = jp.x;
@@ -184,15 +184,16 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
       x_out[g] = x_in[g];
     }
     if (d.has_j2)
-      for (int q = t; q < P.ne; q += T) {
-        const StreamElem& r = sd.elem[P.elem_off + q];
-        if (r.conn.y >> 16) j2_out[r.e] = j2_in[r.e];
-      }
+      for (int q = t; q < P.ne; q += T)
+        if (sd.conn[P.elem_off + q].y >> 16) {
+          const int e = sd.eid[P.elem_off + q];
+          j2_out[e] = j2_in[e];
+        }
     return;
   }
   const bool staged = BULK && P.ne > 0;
   if (staged && t == 0) {
-    // one bulk copy of the patch's contiguous triangle records (48 B each:
+    // one bulk copy of the patch's contiguous triangle records (32 B each:
     // 16-byte aligned, a multiple of 16 bytes), completing on s_mbar
     const uint32_t mb = smem_addr(&s_mbar);
     const uint32_t bytes = (uint32_t)P.ne * (uint32_t)sizeof(StreamElem);
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
   // triangles (element_step)
   for (int q = t; q < P.ne; q += T) {
     const StreamElem r = staged ? srec[q] : sd.elem[P.elem_off + q];
-    stream_element(d, sx, sf, q, r.e, r.conn, r.m, r.ji, j2_in, j2_out);
+    stream_element(d, sx, sf, q, sd.eid + P.elem_off, sd.conn[P.elem_off + q], r.m, r.ji, j2_in, j2_out);
   }
   __syncthreads();
   // owned nodes (node_step)

@@ -1463,8 +1463,8 @@ void rcb(const std::vector<float2>& x, std::vector<int>& idx, int lo, int hi, in
 // node arrays (after finalize, and after a Young's modulus changes).
 int stream_records(fw_ctx* c) {
   if (c->st_ne > 0)
-    k_stream_elems<<<(c->st_ne + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.eid, c->sd.conn,
-                                                                               c->sd.elem, c->st_ne);
+    k_stream_elems<<<(c->st_ne + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.eid, c->sd.elem,
+                                                                               c->st_ne);
   if (c->st_no > 0)
     k_stream_nodes<<<(c->st_no + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.nodes, c->sd.node,
                                                                                c->st_no);
@@ -3563,7 +3563,6 @@ int fw_arena_commit_pack(fw_ctx* c, const fw_pack* pk, int32_t* scene_out) {
   if (c->a_stream) {
     if (a.nt > 0)
       k_stream_elems<<<(int)((a.nt + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->sd.eid + a.t0,
-                                                                                    c->sd.conn + a.t0,
                                                                                     c->sd.elem + a.t0, (int)a.nt);
     k_stream_nodes<<<(int)((a.nn + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->sd.nodes + n0,
                                                                                   c->sd.node + n0, (int)a.nn);
