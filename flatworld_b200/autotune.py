@@ -65,7 +65,7 @@ def _time_steps(native, steps, dt, stream):
     return s.elapsed_time(e) / steps
 
 
-STREAM_MINB = {64: (32, 16), 128: (16, 8)}  # register budgets built per patch size
+STREAM_MINB = {64: (32, 24, 20, 16), 128: (16, 12, 10, 8)}  # register budgets built per patch size
 
 
 def tune_stream(loop, steps=16, use_cache=True):

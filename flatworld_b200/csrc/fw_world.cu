@@ -1418,6 +1418,11 @@ StreamKernel stream_kernel(int nodes, int minb, int bulk) {
   if (nodes == 64 && minb == 16) return bulk ? k_stream<64, 16, true> : k_stream<64, 16, false>;
   if (nodes == 128 && minb == 16) return bulk ? k_stream<128, 16, true> : k_stream<128, 16, false>;
   if (nodes == 128 && minb == 8) return bulk ? k_stream<128, 8, true> : k_stream<128, 8, false>;
+  // intermediate register budgets (40 and 48 registers), per-thread record loads only
+  if (!bulk && nodes == 64 && minb == 24) return k_stream<64, 24, false>;
+  if (!bulk && nodes == 64 && minb == 20) return k_stream<64, 20, false>;
+  if (!bulk && nodes == 128 && minb == 12) return k_stream<128, 12, false>;
+  if (!bulk && nodes == 128 && minb == 10) return k_stream<128, 10, false>;
   return nullptr;
 }
 
@@ -1644,7 +1649,7 @@ int build_stream(fw_ctx* c, const std::vector<int32_t>& off, const std::vector<i
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if ((long)c->st_smem > optin) return fail(c, FW_ERR_ARG, "stream path: patch needs %zu B of shared memory", c->st_smem);
   if ((long)c->st_smem_bulk > optin) c->st_bulk = 0;  // staging does not fit: plain loads
-  for (int minb : {8, 16, 32})
+  for (int minb : {8, 10, 12, 16, 20, 24, 32})
     for (int bulk = 0; bulk < 2; ++bulk)
       if (StreamKernel k = stream_kernel(c->st_nodes, minb, bulk))
         FW_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 64));
@@ -2062,7 +2067,7 @@ void stream_smem(int no_max, int nh_max, int ne_max, size_t* plain, size_t* bulk
 
 // Every built stream kernel of a patch size may use the device's opt-in shared memory.
 int stream_attrs(fw_ctx* c, int optin) {
-  for (int minb : {8, 16, 32})
+  for (int minb : {8, 10, 12, 16, 20, 24, 32})
     for (int bulk = 0; bulk < 2; ++bulk)
       if (StreamKernel k = stream_kernel(c->st_nodes, minb, bulk))
         FW_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 64));
@@ -3256,8 +3261,9 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
     case FW_OPT_STREAM_MINB: {
       if (!stream_kernel(c->st_nodes, value, 0))
         return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_MINB: %d-node patches are built for %s CTAs per SM", c->st_nodes,
-                    c->st_nodes == 64 ? "16 or 32" : "8 or 16");
+                    c->st_nodes == 64 ? "16, 20, 24 or 32" : "8, 10, 12 or 16");
       c->st_minb = value;
+      if (c->st_bulk && !stream_kernel(c->st_nodes, value, 1)) c->st_bulk = 0;  // loads-only budget
       drop_graphs(c);
       return FW_OK;
     }
@@ -3265,6 +3271,8 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
       if (value != 0 && value != 1) return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_BULK must be 0 or 1");
       if (value && c->finalized && c->path == FW_PATH_STREAM && c->st_smem_bulk + 64 > (size_t)shared_optin(c))
         return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_BULK: the staged records do not fit in shared memory");
+      if (value && !stream_kernel(c->st_nodes, c->st_minb, 1))
+        return fail(c, FW_ERR_ARG, "FW_OPT_STREAM_BULK: no staged variant at %d CTAs per SM", c->st_minb);
       c->st_bulk = value;
       drop_graphs(c);
       return FW_OK;

@@ -296,7 +296,9 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
  * FW_OPT_STREAM_PATCH: owned nodes per patch = threads per CTA, 64 (default)
  *   or 128; before fw_finalize (the patches are cut there).
  * FW_OPT_STREAM_MINB: CTAs per SM the kernel's registers are budgeted for
- *   (64-node patches: 32 (default) or 16; 128-node patches: 16 (default) or 8).
+ *   (64-node patches: 32 (default), 24, 20 or 16; 128-node patches: 16
+ *   (default), 12, 10 or 8; the intermediate budgets stage no records, so
+ *   selecting one turns FW_OPT_STREAM_BULK off).
  * FW_OPT_STREAM_BULK: 1 stages each patch's triangle records into shared
  *   memory with one bulk copy instead of a load per triangle (default 0).
  * All give the same bits; the autotuner picks them. */
