@@ -207,8 +207,8 @@ class BatchedLoop:
 
     def enable_cfl_monitor(self, on: bool = True):
         """Per-scene stable time of the current (deformed) shapes, reduced on
-        the GPU in the element step (gather path; see
-        ExplicitLoop.enable_cfl_monitor).  dt is not changed."""
+        the GPU in the step (either path; see ExplicitLoop.enable_cfl_monitor).
+        dt is not changed."""
         self._native.set_cfl_monitor(self.packed.cfl_coefficients() if on else None)
 
     def currentStableTimes(self, reset: bool = True):

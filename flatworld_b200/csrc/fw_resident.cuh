@@ -186,7 +186,9 @@ __host__ __device__ inline size_t res_layout(const Res& r, unsigned char* base, 
   return o;
 }
 
-__device__ __forceinline__ void res_element(const ResSmem& s, int q) {
+// Corner forces of patch triangle q; returns its current-shape CFL bound when
+// body_cfl is given (the monitor is on), else +inf.
+__device__ __forceinline__ float res_element(const ResSmem& s, int q, const float* body_cfl) {
   const uint2 c = s.conn[q];
   const float2 a = s.x[c.x & 0xFFFFu], b = s.x[c.x >> 16], cc = s.x[c.y & 0xFFFFu];
   const ElemMat m = s.mat[q];
@@ -204,6 +206,14 @@ __device__ __forceinline__ void res_element(const ResSmem& s, int q) {
   s.f[3 * q] = f1;
   s.f[3 * q + 1] = f2;
   s.f[3 * q + 2] = f3;
+  return body_cfl ? cfl_bound(a, b, cc, body_cfl[fw::elem_body(m.word)]) : __int_as_float(0x7f800000);
+}
+
+// CFL monitor: a warp's minimum over the triangles its lanes evaluated, folded
+// into the CTA's minimum (shared memory) -- every lane of the warp present.
+__device__ __forceinline__ void res_cfl_fold(int* s_cfl, float v) {
+  const int mb = warp_min_bits(v);
+  if ((threadIdx.x & 31) == 0 && mb < 0x7f800000) atomicMin(s_cfl, mb);
 }
 
 __device__ __forceinline__ void aabb_reset(int* r) {
@@ -288,6 +298,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
   __shared__ int s_pbox[LL ? 4 * kLLMaxBodies : 1];  // this CTA's partial boxes
   __shared__ int s_lbox[LL ? 4 * kLLMaxBodies : 1];  // the same, as of the end of the previous substep
   __shared__ int s_need;                              // a gate needs everyone's boxes this substep
+  __shared__ int s_cfl;                               // CFL monitor: this CTA's minimum (float bits)
   ResSmem s;
   res_layout(r, smem_raw, &s);
   const ResPatch P = r.patch[blockIdx.x];
@@ -329,7 +340,14 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
     s.bpo[b] = d.body_pair_off[b];
     s.bpc[b] = d.body_pair_cnt[b];
   }
-  if (t == 0) s_abort = 0;
+  if (t == 0) {
+    s_abort = 0;
+    s_cfl = 0x7f800000;
+  }
+  // CFL monitor (d.cfl_ord set): each thread keeps the minimum over the
+  // triangles it evaluates in this launch; folded per CTA at the end
+  const float* bcfl = d.cfl_ord ? d.body_cfl : nullptr;
+  float cfl = __int_as_float(0x7f800000);
   if (LL && t < 4 * B) {
     const int ident = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
     s_box[t] = ident;
@@ -349,7 +367,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
       r.rec_v[s.gid[i] & 0x7FFFFFFF] = s.v[i];
     }
   if (!front)
-    for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
+    for (int q = bt; q < P.n_int; q += BT) cfl = fminf(cfl, res_element(s, q, bcfl));
   const int node_trips = (P.no + T - 1) / T;
   for (int k = 0; k < nsteps; ++k) {
     const int g = step0 + k;
@@ -462,7 +480,7 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
           named_bar(1, FT);
           if (LL && t < 4 * B) s_box[t] = (t & 3) < 2 ? fw::f2ord(1e30f) : fw::f2ord(-1e30f);
         }
-        for (int q = P.n_int + t; q < P.ne; q += FT) res_element(s, q);
+        for (int q = P.n_int + t; q < P.ne; q += FT) cfl = fminf(cfl, res_element(s, q, bcfl));
       }
     }
     __syncthreads();  // every triangle of substep k is done
@@ -551,10 +569,15 @@ k_resident(Dev d, Res r, int step0, int nsteps, float dt, float damp, uint32_t e
         r.rec_v[(size_t)(k + 1) * N + (s.gid[i] & 0x7FFFFFFF)] = s.v[i];
       }
     if (!front && k + 1 < nsteps)
-      for (int q = bt; q < P.n_int; q += BT) res_element(s, q);
+      for (int q = bt; q < P.n_int; q += BT) cfl = fminf(cfl, res_element(s, q, bcfl));
   }
   // ---- write the patch state back
   __syncthreads();
+  if (d.cfl_ord) {  // one atomic per CTA and launch (a single-scene world)
+    res_cfl_fold(&s_cfl, cfl);
+    __syncthreads();
+    if (t == 0 && s_cfl < 0x7f800000) atomicMin(d.cfl_ord, s_cfl);
+  }
   for (int i = t; i < P.no; i += T) {
     const int gi = s.gid[i] & 0x7FFFFFFF;
     d.x[gi] = s.x[i];

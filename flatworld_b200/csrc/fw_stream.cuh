@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
                                                      float4* j2_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long s_mbar;
+  __shared__ int s_cfl;  // CFL monitor: this patch's minimum bound (float bits)
   float2* sx = reinterpret_cast<float2*>(smem_raw);  // owned, then halo
   float2* sf = sx + (sd.no_max + sd.nh_max);         // 3 per patch triangle
   StreamElem* srec = reinterpret_cast<StreamElem*>(smem_raw + stream_rec_offset(sd.no_max, sd.nh_max, sd.ne_max));
@@ -191,6 +192,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
         }
     return;
   }
+  if (t == 0) s_cfl = 0x7f800000;  // ordered before the triangles by the barrier below
   const bool staged = BULK && P.ne > 0;
   if (staged && t == 0) {
     // one bulk copy of the patch's contiguous triangle records (32 B each:
@@ -236,7 +238,15 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
     const StreamElem r = staged ? srec[q] : sd.elem[P.elem_off + q];
     stream_element(d, sx, sf, q, sd.eid + P.elem_off, sd.conn[P.elem_off + q], r.m, r.ji, j2_in, j2_out);
   }
+  if (d.cfl_ord)  // CFL monitor: each patch triangle's current-shape bound into the CTA's minimum
+    for (int q = t; q < P.ne; q += T) {
+      const uint2 c = sd.conn[P.elem_off + q];
+      const int word = staged ? srec[q].m.word : sd.elem[P.elem_off + q].m.word;
+      const float b = cfl_bound(sx[c.x & 0xFFFFu], sx[c.x >> 16], sx[c.y & 0xFFFFu], d.body_cfl[fw::elem_body(word)]);
+      atomicMin(&s_cfl, __float_as_int(b));
+    }
   __syncthreads();
+  if (t == 0 && d.cfl_ord && s_cfl < 0x7f800000) atomicMin(d.cfl_ord + P.scene, s_cfl);  // one per patch
   // owned nodes (node_step)
   const StreamNode nr = valid ? sd.node[P.node_off + t] : StreamNode{0u, 1.0f, make_float2(0.f, 0.f)};
   const float2 v0 = valid ? d.v[g] : make_float2(0.f, 0.f);

@@ -227,6 +227,23 @@ __global__ void k_control_scenes(Dev d, const int32_t* __restrict__ list, int n,
   }
 }
 
+// CFL monitor: the current-shape stable time of one triangle, the reference's
+// 0.4 * L_min / sqrt(E / rho) (femdomain.py:24) on the shortest edge of the
+// deformed triangle (coef = 0.4 / sqrt(E / rho) of its body).  Every step
+// implementation evaluates it with these operations.
+__device__ __forceinline__ float cfl_bound(float2 a, float2 b, float2 c, float coef) {
+  const float l0 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y);
+  const float l1 = (b.x - c.x) * (b.x - c.x) + (b.y - c.y) * (b.y - c.y);
+  const float l2 = (c.x - a.x) * (c.x - a.x) + (c.y - a.y) * (c.y - a.y);
+  return sqrtf(fminf(l0, fminf(l1, l2))) * coef;
+}
+
+// Minimum over a whole warp (every lane present) of a non-negative float;
+// +inf where no lane had a value.
+__device__ __forceinline__ int warp_min_bits(float v) {
+  return (int)__reduce_min_sync(0xFFFFFFFFu, (unsigned)__float_as_int(v));
+}
+
 // Loads that depend only on the triangle index are issued before the scene
 // check, so the gather of corner positions does not wait for it.
 __device__ __forceinline__ float element_step(const Dev& d, int e) {
@@ -269,12 +286,7 @@ __device__ __forceinline__ float element_step(const Dev& d, int e) {
     d.corner[q1] = f2;
     d.corner[q2] = f3;
     if (!d.cfl_ord) return __int_as_float(0x7f800000);
-    // current-shape stable time: the reference's 0.4 * L_min / sqrt(E / rho)
-    // (femdomain.py:24) on the shortest edge of the deformed triangle
-    const float l0 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y);
-    const float l1 = (b.x - c.x) * (b.x - c.x) + (b.y - c.y) * (b.y - c.y);
-    const float l2 = (c.x - a.x) * (c.x - a.x) + (c.y - a.y) * (c.y - a.y);
-    return sqrtf(fminf(l0, fminf(l1, l2))) * d.body_cfl[fw::elem_body(m.word)];
+    return cfl_bound(a, b, c, d.body_cfl[fw::elem_body(m.word)]);
   }
 }
 
@@ -4177,8 +4189,7 @@ int fw_clear_scene_status(fw_ctx* c, int32_t scene) {
 int fw_set_cfl_monitor(fw_ctx* c, const float* coef_per_body) {
   if (!c) return FW_ERR_ARG;
   if (!c->finalized) return fail(c, FW_ERR_STATE, "fw_set_cfl_monitor before fw_finalize");
-  if (coef_per_body && c->path != FW_PATH_GATHER)
-    return fail(c, FW_ERR_STATE, "the CFL monitor runs on the gather step (create the world with FW_PATH_GATHER)");
+
   int rc;
   drop_graphs(c);  // captured graphs hold the previous monitor pointers
   if (!coef_per_body) {

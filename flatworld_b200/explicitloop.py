@@ -383,11 +383,11 @@ class ExplicitLoop:
         return self._native.launch_count()
 
     def enable_cfl_monitor(self, on: bool = True):
-        """Report the stable time of the current (deformed) mesh: the element
-        step also evaluates the reference's 0.4 * L_min / sqrt(E / rho)
+        """Report the stable time of the current (deformed) mesh: the step
+        also evaluates the reference's 0.4 * L_min / sqrt(E / rho)
         (femdomain.py:24) on every triangle's current shortest edge, reduced
-        per scene on the GPU.  dt is not changed (the reference fixes it from
-        the rest shape).  Needs the gather step (``path="gather"``)."""
+        per scene on the GPU (every step implementation).  dt is not changed
+        (the reference fixes it from the rest shape)."""
         self._native.set_cfl_monitor(self._packed.cfl_coefficients() if on else None)
 
     def currentStableTime(self, reset: bool = True) -> float:

@@ -407,12 +407,13 @@ int fw_clear_scene_status(fw_ctx* ctx, int32_t scene);
 /* CFL monitor: the stable time of the current (deformed) shape, reported
  * without changing dt.  The reference fixes dt once from the rest shape
  * (explicitloop.py:160-166, femdomain.py:24: 0.4 * L_min / sqrt(E / rho));
- * with the monitor on, the element kernel also evaluates that bound on every
- * triangle's current shortest edge and reduces it per scene (warp shuffles,
- * one atomic per warp and scene), so a caller can see a body's bound shrink
- * as it compresses.  fw_set_cfl_monitor(ctx, coef): coef[b] = 0.4 /
- * sqrt(E / rho) for body b (0 for spring domains); NULL turns it off.  Gather
- * step only (FW_PATH_GATHER).  fw_read_cfl(ctx, out, reset): out[s] = the
+ * with the monitor on, the step that evaluates the triangles also evaluates
+ * that bound on every triangle's current shortest edge and reduces it per
+ * scene (warp shuffles; gather and stream steps: one atomic per warp and
+ * scene; resident step: one per CTA and launch), so a caller can see a body's
+ * bound shrink as it compresses.  fw_set_cfl_monitor(ctx, coef): coef[b] =
+ * 0.4 / sqrt(E / rho) for body b (0 for spring domains); NULL turns it off.
+ * Every step implementation.  fw_read_cfl(ctx, out, reset): out[s] = the
  * smallest bound of scene s over the substeps since the last reset (+inf if
  * none); reset = 1 starts a new window.  No reference counterpart. */
 int fw_set_cfl_monitor(fw_ctx* ctx, const float* coef_per_body);

@@ -1,5 +1,6 @@
 """CFL monitor: the stable time of the current (deformed) mesh, reduced on the
-GPU inside the element step (warp shuffles, one atomic per warp and scene).
+GPU inside the step (warp shuffles; gather and stream steps one atomic per
+warp and scene, the resident step one per CTA and launch).
 
 The reference's dt is fixed at construction from the rest shape
 (explicitloop.py:160-166; FemDomain.stableTime = 0.4 * L_min / sqrt(E / rho),
@@ -71,7 +72,36 @@ def test_cfl_monitor_per_scene_in_a_batch():
         assert abs(got[s] - doms[1].stableTime) <= 1e-6 * doms[1].stableTime, (s, got[s], doms[1].stableTime)
 
 
-def test_cfl_monitor_needs_the_gather_step():
-    loop = fw.ExplicitLoop(0.0, scenes.plain_large_scene(fw, n=32), useAdapativeDT=True, path="resident")
-    with pytest.raises(RuntimeError, match="gather step"):
-        loop.enable_cfl_monitor()
+@pytest.mark.parametrize("path", ["resident", "stream"])
+def test_cfl_monitor_same_on_every_step(path):
+    """The resident and stream steps report the gather step's bound bit for
+    bit (the same operations on the same positions), window by window, and
+    the trajectory is unchanged by the monitor."""
+    build = lambda: scenes.plain_large_scene(fw, n=32, hf_offset=0.17)  # noqa: E731
+    if path == "resident":
+        a = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, path="resident")
+        assert a.path == 2
+        a.enable_cfl_monitor()
+        read = lambda: a.currentStableTime()  # noqa: E731
+        step = lambda n: a.advance_n(n)  # noqa: E731
+    else:
+        a = BatchedLoop([build(), scenes.j2_block_scene(fw)], dt=3e-5, useAdapativeDT=False, path="stream")
+        assert a.path == "stream"
+        a.enable_cfl_monitor()
+        read = lambda: a.currentStableTimes()  # noqa: E731
+        step = lambda n: a.advance(n)  # noqa: E731
+    if path == "resident":
+        g = fw.ExplicitLoop(0.0, build(), useAdapativeDT=True, path="gather")
+        g.enable_cfl_monitor()
+        gread, gstep = (lambda: g.currentStableTime()), (lambda n: g.advance_n(n))
+    else:
+        g = BatchedLoop([build(), scenes.j2_block_scene(fw)], dt=3e-5, useAdapativeDT=False, path="gather")
+        g.enable_cfl_monitor()
+        gread, gstep = (lambda: g.currentStableTimes()), (lambda n: g.advance(n))
+    for n in (1, 37, 300, 1000):
+        step(n)
+        gstep(n)
+        assert np.array_equal(np.asarray(read()), np.asarray(gread())), n
+    xa = a.femSpringManager.coords.numpy() if path == "resident" else a.all_coords()
+    xg = g.femSpringManager.coords.numpy() if path == "resident" else g.all_coords()
+    assert np.array_equal(xa, xg)
