@@ -705,7 +705,7 @@ def run_flex(args, rank, world, local):
     loop._native.set_stream(stream.cuda_stream)
     pk = loop._packed
     N, E = pk.N, pk.E
-    n_items = sum(int(pk.bncnt[b1] + pk.bncnt[b2]) for _, _, _, _, _, prs in pk.flex_records() for b1, b2, _, _ in prs)
+    n_items = sum(int(pk.bncnt[b1] + pk.bncnt[b2]) for _, _, _, _, _, prs in pk.flex_records() for b1, b2, *_ in prs)
     per = 100
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
