@@ -213,6 +213,12 @@ def ncu_traffic_ratio_batched(step_path="gather", shape=None):
     return d.get("stream_traffic_over_algorithmic"), d.get("stream_source")
 
 
+def flex_work_items(pk):
+    """FEM-FEM contact work items of a packed world: per pair, the boundary
+    nodes of both bodies (each node a query against the other body)."""
+    return sum(int(pk.bncnt[b1] + pk.bncnt[b2]) for _, _, _, _, _, prs in pk.flex_records() for b1, b2, *_ in prs)
+
+
 def cpu_oracle_rate(fw, mesh, seconds, threads):
     """Element-steps/s of the CPU restatement on this host (bounded sample)."""
     import oracle
@@ -705,7 +711,7 @@ def run_flex(args, rank, world, local):
     loop._native.set_stream(stream.cuda_stream)
     pk = loop._packed
     N, E = pk.N, pk.E
-    n_items = sum(int(pk.bncnt[b1] + pk.bncnt[b2]) for _, _, _, _, _, prs in pk.flex_records() for b1, b2, *_ in prs)
+    n_items = flex_work_items(pk)
     per = 100
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
