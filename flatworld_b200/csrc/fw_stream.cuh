@@ -178,12 +178,19 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
   StreamElem* srec = reinterpret_cast<StreamElem*>(smem_raw + stream_rec_offset(sd.no_max, sd.nh_max, sd.ne_max));
   const StreamPatch P = sd.patch[sd.list ? sd.list[blockIdx.x] : (int)blockIdx.x];
   const int t = threadIdx.x, T = NT;
+  // positions of the owned (one per thread) and halo nodes
+  const bool valid = t < P.no;
+  const int g = valid ? sd.nodes[P.node_off + t] : 0;
+  if (valid) sx[t] = x_in[g];
+  for (int h = t; h < P.nh; h += T) sx[P.no + h] = x_in[sd.halo[P.halo_off + h]];
+  // Arena calls launch this kernel as a programmatic dependent of the scene
+  // control (k_control_scenes): the loads above touch nothing the control
+  // writes, so they overlap it; here the control's results become visible.
+  // (Returns at once for an ordinary launch.)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int mode = d.scene_mode[P.scene];
   if (mode == fw::MODE_FROZEN) {  // keep the state: carry it into the other buffers
-    for (int i = t; i < P.no; i += T) {
-      const int g = sd.nodes[P.node_off + i];
-      x_out[g] = x_in[g];
-    }
+    if (valid) x_out[g] = sx[t];
     if (d.has_j2)
       for (int q = t; q < P.ne; q += T)
         if (sd.conn[P.elem_off + q].y >> 16) {
@@ -207,11 +214,6 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
                  "l"(sd.elem + P.elem_off), "r"(bytes), "r"(mb)
                  : "memory");
   }
-  // positions of the owned (one per thread) and halo nodes
-  const bool valid = t < P.no;
-  const int g = valid ? sd.nodes[P.node_off + t] : 0;
-  if (valid) sx[t] = x_in[g];
-  for (int h = t; h < P.nh; h += T) sx[P.no + h] = x_in[sd.halo[P.halo_off + h]];
   __syncthreads();  // also orders the barrier's initialisation before the waits below
   if (staged) {
     // thread 0 waits (bounded) for the staged records; the barrier below

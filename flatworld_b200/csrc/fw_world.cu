@@ -180,6 +180,10 @@ __device__ void step_control(const Dev& d) {
 // its dt, then scene_budget_next[s] at scene_dt_next[s], then sits out.
 // rng[s] = (first body, bodies, first pair, pairs) of scene s.
 __global__ void k_control_scenes(Dev d, const int32_t* __restrict__ list, int n, const int4* __restrict__ rng) {
+  // the patch step that follows may start now: it gathers positions, which
+  // this kernel does not touch, and waits for this kernel before reading what
+  // it writes (griddepcontrol.wait)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int s = list[i];
@@ -2116,9 +2120,21 @@ int arena_stream_steps(fw_ctx* c, int n) {
   const StreamKernel k = stream_kernel(c->st_nodes, c->st_minb, c->st_bulk);
   const size_t smem = c->st_bulk ? c->st_smem_bulk : c->st_smem;
   const int gs = (c->st_slist_n + 127) / 128;
+  // the patch step is a programmatic dependent of the control kernel (its
+  // position gather overlaps the control; see k_stream)
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(c->st_list_n);
+  cfg.blockDim = dim3(c->st_nodes);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cfg.attrs = pdl;
+  cfg.numAttrs = 1;
   for (int j = 0; j < n; ++j) {
     k_control_scenes<<<gs, 128, 0, c->stream>>>(c->d, c->d_slist, c->st_slist_n, c->d_srng);
-    k<<<c->st_list_n, c->st_nodes, smem, c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
+    FW_CUDA(c, cudaLaunchKernelEx(&cfg, k, c->d, c->sd, (const float2*)xa, xb, (const float4*)ja, jb));
     std::swap(xa, xb);
     std::swap(ja, jb);
   }

@@ -59,10 +59,13 @@ class Arena:
             active scenes; the default) or "gather" (two kernels per
             substep); both give the same bits
         stream_patch: owned nodes per patch of a stream arena (64 or 128)
+        stream_minb: CTAs per SM its patch step's registers are budgeted for
+            (0: 24 for 64-node patches, 12 for 128-node ones -- the 40-register
+            shapes, the fastest at the batch sizes of a request loop)
     """
 
     def __init__(self, max_nodes, max_elems, max_bodies=4096, max_scenes=4096, max_pairs=4096,
-                 max_heights=1 << 20, max_occ=1 << 26, device=0, path="stream", stream_patch=64):
+                 max_heights=1 << 20, max_occ=1 << 26, device=0, path="stream", stream_patch=64, stream_minb=0):
         self.native = _native.NativeWorld(device)
         if path == "stream":
             self.native.set_path(_native.FW_PATH_STREAM)
@@ -70,6 +73,8 @@ class Arena:
         elif path != "gather":
             raise ValueError(f"arena path must be 'stream' or 'gather', not {path!r}")
         self.native.arena_init(max_nodes, max_elems, max_bodies, max_scenes, max_pairs, max_heights, max_occ)
+        if path == "stream":
+            self.native.set_option(_native.FW_OPT_STREAM_MINB, int(stream_minb or {64: 24, 128: 12}[int(stream_patch)]))
         self.path = path
         self.patch_nodes = int(stream_patch) if path == "stream" else 0
         self.max_scenes = max_scenes
