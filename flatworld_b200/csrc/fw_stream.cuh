@@ -103,7 +103,10 @@ __global__ void k_stream_elems(Dev d, const int32_t* eid, StreamElem* out, int n
   out[i] = r;
 }
 
-__global__ void k_control(Dev d) { step_control(d); }
+__global__ void k_control(Dev d) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");  // the patch step may start its gather
+  step_control(d);
+}
 
 // Arena worlds step only the active scenes' patches, so after an odd number
 // of substeps their state sits in the other buffers: copy each listed
@@ -178,27 +181,6 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
   StreamElem* srec = reinterpret_cast<StreamElem*>(smem_raw + stream_rec_offset(sd.no_max, sd.nh_max, sd.ne_max));
   const StreamPatch P = sd.patch[sd.list ? sd.list[blockIdx.x] : (int)blockIdx.x];
   const int t = threadIdx.x, T = NT;
-  // positions of the owned (one per thread) and halo nodes
-  const bool valid = t < P.no;
-  const int g = valid ? sd.nodes[P.node_off + t] : 0;
-  if (valid) sx[t] = x_in[g];
-  for (int h = t; h < P.nh; h += T) sx[P.no + h] = x_in[sd.halo[P.halo_off + h]];
-  // Arena calls launch this kernel as a programmatic dependent of the scene
-  // control (k_control_scenes): the loads above touch nothing the control
-  // writes, so they overlap it; here the control's results become visible.
-  // (Returns at once for an ordinary launch.)
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  const int mode = d.scene_mode[P.scene];
-  if (mode == fw::MODE_FROZEN) {  // keep the state: carry it into the other buffers
-    if (valid) x_out[g] = sx[t];
-    if (d.has_j2)
-      for (int q = t; q < P.ne; q += T)
-        if (sd.conn[P.elem_off + q].y >> 16) {
-          const int e = sd.eid[P.elem_off + q];
-          j2_out[e] = j2_in[e];
-        }
-    return;
-  }
   if (t == 0) s_cfl = 0x7f800000;  // ordered before the triangles by the barrier below
   const bool staged = BULK && P.ne > 0;
   if (staged && t == 0) {
@@ -213,6 +195,33 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
                      smem_addr(srec)),
                  "l"(sd.elem + P.elem_off), "r"(bytes), "r"(mb)
                  : "memory");
+  }
+  // positions of the owned (one per thread) and halo nodes
+  const bool valid = t < P.no;
+  const int g = valid ? sd.nodes[P.node_off + t] : 0;
+  if (valid) sx[t] = x_in[g];
+  for (int h = t; h < P.nh; h += T) sx[P.no + h] = x_in[sd.halo[P.halo_off + h]];
+  // Launched as a programmatic dependent of the scene control (k_control,
+  // k_control_scenes): the loads above touch nothing the control writes, so
+  // they overlap it; here the control's results become visible.  (Returns at
+  // once for an ordinary launch.)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const int mode = d.scene_mode[P.scene];
+  if (mode == fw::MODE_FROZEN) {  // keep the state: carry it into the other buffers
+    if (valid) x_out[g] = sx[t];
+    if (d.has_j2)
+      for (int q = t; q < P.ne; q += T)
+        if (sd.conn[P.elem_off + q].y >> 16) {
+          const int e = sd.eid[P.elem_off + q];
+          j2_out[e] = j2_in[e];
+        }
+    if (staged && t == 0) {  // the staged copy writes this CTA's shared memory: let it land (bounded)
+      const uint32_t mb = smem_addr(&s_mbar);
+      bool ok = mbar_done(mb, 0);
+      for (long long it = 0; !ok && it < kBulkWaitLimit; ++it) ok = mbar_done(mb, 0);
+      if (!ok) atomicExch(sd.err, 1);
+    }
+    return;
   }
   __syncthreads();  // also orders the barrier's initialisation before the waits below
   if (staged) {

@@ -1458,9 +1458,19 @@ int stream_steps(fw_ctx* c, int n) {
       float4 *ja = c->d.j2state, *jb = c->d.j2_alt;
       for (int k = 0; k < m; ++k) {
         k_control<<<1, kMaxBlock, 0, c->stream>>>(c->d);
-        stream_kernel(c->st_nodes, c->st_minb, c->st_bulk)<<<c->st_P, c->st_nodes,
-                                                             c->st_bulk ? c->st_smem_bulk : c->st_smem,
-                                                             c->stream>>>(c->d, c->sd, xa, xb, ja, jb);
+        // the patch step as a programmatic dependent of the control (see k_stream)
+        cudaLaunchAttribute pdl[1];
+        pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        pdl[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c->st_P);
+        cfg.blockDim = dim3(c->st_nodes);
+        cfg.dynamicSmemBytes = c->st_bulk ? c->st_smem_bulk : c->st_smem;
+        cfg.stream = c->stream;
+        cfg.attrs = pdl;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, stream_kernel(c->st_nodes, c->st_minb, c->st_bulk), c->d, c->sd,
+                           (const float2*)xa, xb, (const float4*)ja, jb);
         std::swap(xa, xb);
         std::swap(ja, jb);
       }
