@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-from flatworld_b200 import shard  # noqa: E402
+from flatworld_b200 import _native, shard  # noqa: E402
 
 FRAME = 1.0 / 60.0
 
@@ -1167,7 +1167,8 @@ def main():
                        "elements": E, "nodes": N, "step": "advanceWithTime(1/60)",
                        "substeps_per_step": substeps, "dt": loop.stableTime,
                        "l2": "flushed between steps (256 MiB write)", "replicas": world,
-                       "path": {1: "gather", 2: "resident"}.get(loop.path, loop.path), "patches": loop.patches},
+                       "path": {1: "gather", 2: "resident"}.get(loop.path, loop.path), "patches": loop.patches,
+                       "front_warps": loop._native.get_option(_native.FW_OPT_FRONT_WARPS) if loop.path == 2 else None},
             "roofline": {"bound": "hbm",
                          "kernel": "k_resident (all substeps of a step)" if loop.path == 2 else
                                    "substep = k_elements + k_nodes",

@@ -76,6 +76,7 @@ _SIGNATURES = {
     "fw_set_path": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "fw_get_path": (C.c_int, [_vp, _i32p, _i32p]),
     "fw_set_option": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "fw_get_option": (C.c_int, [_vp, C.c_int32, _i32p]),
     "fw_snapshot": (C.c_int, [_vp, C.c_int32]),
     "fw_set_element_young": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.c_int32]),
     "fw_adj_begin": (C.c_int, [_vp, C.c_int32]),
@@ -341,6 +342,11 @@ class NativeWorld:
 
     def set_option(self, option: int, value: int):
         self._check(self._L.fw_set_option(self._h, int(option), int(value)), "fw_set_option")
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int32(0)
+        self._check(self._L.fw_get_option(self._h, int(option), C.byref(v)), "fw_get_option")
+        return int(v.value)
 
     def snapshot(self, slot: int = 0):
         self._check(self._L.fw_snapshot(self._h, int(slot)), "fw_snapshot")

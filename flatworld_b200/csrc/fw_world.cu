@@ -3326,6 +3326,21 @@ int fw_set_option(fw_ctx* c, int32_t option, int32_t value) {
   }
 }
 
+int fw_get_option(const fw_ctx* c, int32_t option, int32_t* value) {
+  if (!c || !value) return FW_ERR_ARG;
+  switch (option) {
+    case FW_OPT_FRONT_WARPS: *value = c->front_warps; return FW_OK;
+    case FW_OPT_RES_THREADS: *value = c->res_threads; return FW_OK;
+    case FW_OPT_BLOCK_ELEMS: *value = c->block_e; return FW_OK;
+    case FW_OPT_BLOCK_NODES: *value = c->block_n; return FW_OK;
+    case FW_OPT_STREAM_PATCH: *value = c->st_nodes; return FW_OK;
+    case FW_OPT_STREAM_MINB: *value = c->st_minb; return FW_OK;
+    case FW_OPT_STREAM_BULK: *value = c->st_bulk; return FW_OK;
+    case FW_OPT_RES_SYNC: *value = c->res_sync; return FW_OK;
+    default: return FW_ERR_ARG;
+  }
+}
+
 int fw_snapshot(fw_ctx* c, int32_t slot) {
   if (c && c->has_rigid) return fail(c, FW_ERR_STATE, "snapshots do not hold the rigid bodies' state");
   if (c && c->has_flex)

@@ -312,6 +312,10 @@ int fw_set_path(fw_ctx* ctx, int32_t path, int32_t patches);
  * bits. */
 #define FW_OPT_RES_THREADS 11
 int fw_set_option(fw_ctx* ctx, int32_t option, int32_t value);
+/* The value an option has now.  Readable: FRONT_WARPS, RES_THREADS,
+ * BLOCK_ELEMS, BLOCK_NODES, STREAM_PATCH, STREAM_MINB, STREAM_BULK, RES_SYNC;
+ * FW_ERR_ARG for the others.  No reference counterpart (a tuning readout). */
+int fw_get_option(const fw_ctx* ctx, int32_t option, int32_t* value);
 
 /* Checkpoint / resume: copy the whole step state (positions, velocities, J2
  * state, step counters, body boxes) into snapshot `slot` (device memory owned

@@ -67,3 +67,19 @@ def test_stage_context_cannot_be_finalized():
     with pytest.raises(_native.NativeError, match="staging context"):
         st.arena_init(100, 100, 1, 1, 1, 1, 1)
     st.close()
+
+
+def test_options_read_back():
+    """fw_get_option reads the launch-shape options back (a staging context
+    needs no device), and refuses an option it cannot read."""
+    st = _native.NativeWorld.stage()
+    assert st.get_option(_native.FW_OPT_FRONT_WARPS) == 6
+    assert st.get_option(_native.FW_OPT_RES_THREADS) == 512
+    st.set_option(_native.FW_OPT_RES_THREADS, 1024)
+    st.set_option(_native.FW_OPT_FRONT_WARPS, 16)
+    assert (st.get_option(_native.FW_OPT_RES_THREADS), st.get_option(_native.FW_OPT_FRONT_WARPS)) == (1024, 16)
+    st.set_option(_native.FW_OPT_STREAM_PATCH, 128)
+    assert (st.get_option(_native.FW_OPT_STREAM_PATCH), st.get_option(_native.FW_OPT_STREAM_MINB)) == (128, 16)
+    with pytest.raises(_native.NativeError):
+        st.get_option(_native.FW_OPT_WAIT_LIMIT)
+    st.close()

@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import flatworld_b200 as fw
+from flatworld_b200 import _native
 import oracle
 from tests import scenes
 
@@ -283,6 +284,8 @@ def test_resident_launch_shapes_bitwise(threads, front, res_sync):
                         res_sync=res_sync)
     b = fw.ExplicitLoop(0.0, doms(), useAdapativeDT=True, path="gather")
     assert a.path == 2
+    assert a._native.get_option(_native.FW_OPT_FRONT_WARPS) == front
+    assert a._native.get_option(_native.FW_OPT_RES_THREADS) == threads
     for _ in range(10):
         a.advanceWithTime(FRAME)
         b.advanceWithTime(FRAME)
