@@ -379,3 +379,4 @@ def test_gpu_spring_rigid_equals_oracle():
         o.advance_with_time(FRAME)
         _compare(lp, o, o.N, f)
 
+
