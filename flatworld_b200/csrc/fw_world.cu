@@ -111,6 +111,13 @@ struct Dev {
   Rigid* rig;
   float4* ritem;
   int32_t* bslot;
+  // The work items are evaluated by the element step's trailing blocks
+  // (their inputs are the substep's start state): rwork[it] = (pair, node),
+  // rforce[it] = the force the item adds to its node (when ritem[it] is a
+  // hit); the node step adds the gated ones in pair order.
+  int2* rwork;
+  float2* rforce;
+  int n_ritems;
   // CFL monitor (cfl_ord == nullptr: off): per scene, the smallest current-
   // shape stable time 0.4 L / c of its triangles since the last read, as the
   // int bits of a non-negative float (int order = float order); body_cfl =
@@ -304,10 +311,11 @@ __device__ __forceinline__ void cfl_reduce(const Dev& d, int e, float dtc) {
   if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && m < 0x7f800000) atomicMin(d.cfl_ord + s, m);
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
+// The element step over blocks [0, nb) of the grid.
+__device__ __forceinline__ void elements_pass(const Dev& d, int nb) {
   if (blockIdx.x == 0) step_control(d);
   if (d.use_chunks) {
-    for (int c = blockIdx.x; c < d.n_e_chunks; c += gridDim.x) {
+    for (int c = blockIdx.x; c < d.n_e_chunks; c += nb) {
       const int2 ch = d.e_chunks[c];
       if ((int)threadIdx.x < ch.y) {
         const float dtc = element_step(d, ch.x + threadIdx.x);
@@ -316,10 +324,36 @@ __global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) {
     }
     return;
   }
-  const int stride = gridDim.x * blockDim.x;
+  const int stride = nb * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d.E; e += stride) {
     const float dtc = element_step(d, e);
     if (d.cfl_ord) cfl_reduce(d, e, dtc);
+  }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_elements(Dev d) { elements_pass(d, gridDim.x); }
+
+// Worlds with FEM-rigid contact: blocks [0, eb) run the element step, the
+// others evaluate every FEM-rigid work item -- one thread per item instead of
+// one thread per boundary node walking all its rigid pairs -- from the
+// substep's start state, whatever the gate and the scene's mode (the node
+// step uses an item only when its scene steps and its pair is gated on).
+// rigid_item adds its force to a -0 start, which leaves it exactly as it
+// would be added to the node's sum.
+__global__ void __launch_bounds__(kMaxBlock) k_elements_rigid(Dev d, int eb) {
+  if ((int)blockIdx.x < eb) {
+    elements_pass(d, eb);
+    return;
+  }
+  const int stride = (gridDim.x - eb) * blockDim.x;
+  for (int it = (blockIdx.x - eb) * blockDim.x + threadIdx.x; it < d.n_ritems; it += stride) {
+    const int2 w = d.rwork[it];
+    const Pair& pr = d.pairs[w.x];
+    const float dt = d.uniform_dt ? d.dt_uniform : d.scene_dt[d.body_scene[pr.body]];
+    float2 f = make_float2(-0.0f, -0.0f);
+    d.ritem[it] = fw::rigid_item(d.rig[pr.table], pr.table, pr.penalty, pr.f[0], pr.pad != 0, d.x[w.y], d.v[w.y],
+                                 dt, f);
+    d.rforce[it] = f;
   }
 }
 
@@ -392,13 +426,17 @@ __device__ __forceinline__ void node_step(const Dev& d, int i, bool valid) {
           flex_done = true;
         }
         if (RIGID && d.pairs[p0 + k].kind == fw::PAIR_RIGID) {
-          const Pair& pr = d.pairs[p0 + k];
-          const int slot = pr.n0 + bs;
-          const float4 rec = d.pair_active[p0 + k]
-                                 ? fw::rigid_item(d.rig[pr.table], pr.table, pr.penalty, pr.f[0], pr.pad != 0, x,
-                                                  v, dt, f)
-                                 : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-          d.ritem[slot] = rec;
+          // the item was evaluated by k_elements_rigid from this same state
+          const int slot = d.pairs[p0 + k].n0 + bs;
+          if (d.pair_active[p0 + k]) {
+            if (__float_as_int(d.ritem[slot].w) >= 0) {
+              const float2 rf = d.rforce[slot];
+              f.x += rf.x;
+              f.y += rf.y;
+            }
+          } else {
+            d.ritem[slot] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+          }
           continue;
         }
         if (!d.pair_active[p0 + k]) continue;
@@ -1310,8 +1348,10 @@ int step_launches(const fw_ctx* c) { return 2 + (c->has_flex ? 2 : 0) + (c->has_
 
 int launch_step(fw_ctx* c) {
   if (c->has_flex) flex_launch(c, 0);
-  k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
   if (c->has_rigid) {
+    // the element step plus one thread per FEM-rigid work item
+    const int rb = std::max(1, std::min((c->d.n_ritems + c->block_e - 1) / c->block_e, c->sms * 8));
+    k_elements_rigid<<<c->grid_e + rb, c->block_e, 0, c->stream>>>(c->d, c->grid_e);
     if (c->has_flex)
       k_nodes_rigid<true><<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
     else
@@ -1321,10 +1361,12 @@ int launch_step(fw_ctx* c) {
     else
       k_rigid<<<(c->rd.n + kRigidThreads / 32 - 1) / (kRigidThreads / 32), kRigidThreads, 0, c->stream>>>(c->d, c->rd);
     c->launches += 1;
-  } else if (c->has_flex) {
-    k_nodes_flex<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
   } else {
-    k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+    k_elements<<<c->grid_e, c->block_e, 0, c->stream>>>(c->d);
+    if (c->has_flex)
+      k_nodes_flex<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
+    else
+      k_nodes<<<c->grid_n, c->block_n, 0, c->stream>>>(c->d);
   }
   c->launches += 2;
   return check_kernel(c, "step");
@@ -3139,6 +3181,14 @@ int fw_finalize(fw_ctx* c) {
     std::vector<int32_t> bslot(N, 0);
     for (int b = 0; b < B; ++b)
       for (int k = 0; k < c->h_bncnt[b]; ++k) bslot[c->h_bnodes[c->h_bnoff[b] + k]] = k;
+    // work item -> (pair, boundary node), for the element step's item blocks
+    std::vector<int2> rwork(std::max(1, n_ritems), make_int2(0, 0));
+    for (size_t q = 0; q < pairs.size(); ++q)
+      if (pairs[q].kind == fw::PAIR_RIGID) {
+        const Pair& p = pairs[q];
+        for (int k = 0; k < c->h_bncnt[p.body]; ++k)
+          rwork[p.n0 + k] = make_int2((int)q, c->h_bnodes[c->h_bnoff[p.body] + k]);
+      }
     // per rigid, its pairs' item ranges in pair (= item) order; `pairs` is
     // grouped by body by now, so order the rigid pairs by first item again
     std::vector<Pair> rpairs;
@@ -3177,6 +3227,7 @@ int fw_finalize(fw_ctx* c) {
     r.n_rs = (int)rs.size();
     std::vector<fw::RigidClock> ck(S, fw::RigidClock{1, 0.0f, 0.0f, 0});
     if ((rc = upload(c, &r.rig, c->h_rigid)) || (rc = upload(c, &d.bslot, bslot)) ||
+        (rc = upload(c, &d.rwork, rwork)) || (rc = dalloc(c, &d.rforce, (size_t)std::max(1, n_ritems))) ||
         (rc = dalloc(c, &r.item, (size_t)n_ritems)) || (rc = upload(c, &r.gbox, c->h_gbox)) ||
         (rc = upload(c, &r.gkind, c->h_gkind)) || (rc = upload(c, &r.rp_off, rp_off)) ||
         (rc = upload(c, &r.rp_rng, rp_rng)) || (rc = upload(c, &r.rs, rs)) ||
@@ -3189,6 +3240,7 @@ int fw_finalize(fw_ctx* c) {
     r.clock = c->d_rclock;
     d.rig = r.rig;
     d.ritem = r.item;
+    d.n_ritems = n_ritems;
     k_rigid_init<<<(r.n + 127) / 128, 128, 0, c->stream>>>(r.rig, r.n);
     c->launches += 1;
     if ((rc = check_kernel(c, "rigid init"))) return rc;
