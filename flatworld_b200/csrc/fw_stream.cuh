@@ -49,14 +49,20 @@ struct StreamPatch {
   int csrp_off;      // csrp[csrp_off .. +no+1): local corner-list offsets of the owned nodes
   int csr_off;       // csrs[csr_off + csrp[..]]: 3 * local triangle + corner
   int scene;
-  int pad[3];
+  int body;          // the body its nodes and triangles belong to
+  int pad[2];
 };
 
-// Static data of one patch triangle, in patch order (32 B; its local corners
-// are StreamDev::conn and its global index, needed by J2 triangles only,
-// StreamDev::eid, at the same position).
+// Static data of one patch triangle, in patch order (32 B: what the triangle
+// step reads, in one record).  Its Lame constants come from its body's entry
+// of Dev::body_lm -- a body's triangles share one material -- unless
+// StreamDev::lm holds them per triangle (after a per-element Young's modulus
+// change); its global index, needed by J2 triangles only, is StreamDev::eid
+// at the same position.
 struct __align__(16) StreamElem {
-  ElemMat m;   // emat[e]
+  float area;  // emat[e].area
+  int word;    // emat[e].word (type, body)
+  uint2 conn;  // StreamDev::conn: local corner ids
   float4 ji;   // jinv[e]
 };
 
@@ -80,6 +86,7 @@ struct StreamDev {
   StreamNode* node;  // built from nodes by k_stream_nodes
   int* err;          // != 0: a staged copy did not complete in time
   const int32_t* list;  // arena worlds: CTA i runs patch list[i] (the active scenes' patches); else patch i
+  float2* lm;           // per patch triangle (lam, mu) once a triangle's Young's modulus was set; else null
 };
 
 __global__ void k_stream_nodes(Dev d, const int32_t* nodes, StreamNode* out, int n) {
@@ -93,14 +100,23 @@ __global__ void k_stream_nodes(Dev d, const int32_t* nodes, StreamNode* out, int
   out[i] = r;
 }
 
-__global__ void k_stream_elems(Dev d, const int32_t* eid, StreamElem* out, int n) {
+// Records of n patch triangles.  Without lm, each also writes its body's
+// Lame constants to Dev::body_lm (the body's triangles all hold the same).
+__global__ void k_stream_elems(Dev d, const int32_t* eid, const uint2* conn, StreamElem* out, float2* lm, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int e = eid[i];
+  const ElemMat m = d.emat[e];
   StreamElem r;
-  r.m = d.emat[e];
+  r.area = m.area;
+  r.word = m.word;
+  r.conn = conn[i];
   r.ji = d.jinv[e];
   out[i] = r;
+  if (lm)
+    lm[i] = make_float2(m.lam, m.mu);
+  else
+    d.body_lm[fw::elem_body(m.word)] = make_float2(m.lam, m.mu);
 }
 
 __global__ void k_control(Dev d) {
@@ -180,6 +196,7 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
   float2* sf = sx + (sd.no_max + sd.nh_max);         // 3 per patch triangle
   StreamElem* srec = reinterpret_cast<StreamElem*>(smem_raw + stream_rec_offset(sd.no_max, sd.nh_max, sd.ne_max));
   const StreamPatch P = sd.patch[sd.list ? sd.list[blockIdx.x] : (int)blockIdx.x];
+  const float2 blm = d.body_lm[P.body];  // the patch's Lame constants (sd.lm null)
   const int t = threadIdx.x, T = NT;
   if (t == 0) s_cfl = 0x7f800000;  // ordered before the triangles by the barrier below
   const bool staged = BULK && P.ne > 0;
@@ -247,12 +264,18 @@ __global__ void __launch_bounds__(NT, MINB) k_stream(Dev d, StreamDev sd, const 
   // triangles (element_step)
   for (int q = t; q < P.ne; q += T) {
     const StreamElem r = staged ? srec[q] : sd.elem[P.elem_off + q];
-    stream_element(d, sx, sf, q, sd.eid + P.elem_off, sd.conn[P.elem_off + q], r.m, r.ji, j2_in, j2_out);
+    const float2 lm = sd.lm ? sd.lm[P.elem_off + q] : blm;
+    ElemMat m;
+    m.area = r.area;
+    m.lam = lm.x;
+    m.mu = lm.y;
+    m.word = r.word;
+    stream_element(d, sx, sf, q, sd.eid + P.elem_off, r.conn, m, r.ji, j2_in, j2_out);
   }
   if (d.cfl_ord)  // CFL monitor: each patch triangle's current-shape bound into the CTA's minimum
     for (int q = t; q < P.ne; q += T) {
       const uint2 c = sd.conn[P.elem_off + q];
-      const int word = staged ? srec[q].m.word : sd.elem[P.elem_off + q].m.word;
+      const int word = staged ? srec[q].word : sd.elem[P.elem_off + q].word;
       const float b = cfl_bound(sx[c.x & 0xFFFFu], sx[c.x >> 16], sx[c.y & 0xFFFFu], d.body_cfl[fw::elem_body(word)]);
       atomicMin(&s_cfl, __float_as_int(b));
     }

@@ -59,6 +59,7 @@ struct Dev {
   int32_t* conn;
   float4* jinv;
   ElemMat* emat;
+  float2* body_lm;     // stream path: each body's Lame constants (its triangles share them)
   float2* j2par;
   float4* j2state;
   float4* j2_alt;      // stream path: the other J2 state buffer
@@ -1536,8 +1537,8 @@ void rcb(const std::vector<float2>& x, std::vector<int>& idx, int lo, int hi, in
 // node arrays (after finalize, and after a Young's modulus changes).
 int stream_records(fw_ctx* c) {
   if (c->st_ne > 0)
-    k_stream_elems<<<(c->st_ne + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.eid, c->sd.elem,
-                                                                               c->st_ne);
+    k_stream_elems<<<(c->st_ne + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.eid, c->sd.conn,
+                                                                               c->sd.elem, c->sd.lm, c->st_ne);
   if (c->st_no > 0)
     k_stream_nodes<<<(c->st_no + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, c->sd.nodes, c->sd.node,
                                                                                c->st_no);
@@ -1582,9 +1583,12 @@ int make_patches(int N, int E, const int32_t* conn, const std::vector<int32_t>& 
     }
     owned[part[i]].push_back(i);
   }
-  std::vector<int> node_scene(N, 0);
+  std::vector<int> node_scene(N, 0), node_body(N, 0);
   for (size_t b = 0; b < noff.size(); ++b)
-    for (int k = 0; k < ncnt[b]; ++k) node_scene[noff[b] + k] = body_scene[b];
+    for (int k = 0; k < ncnt[b]; ++k) {
+      node_scene[noff[b] + k] = body_scene[b];
+      node_body[noff[b] + k] = (int)b;
+    }
   std::vector<StreamPatch>& patches = out.patches;
   patches.assign(P, StreamPatch{});
   std::vector<int32_t>& rn = out.rn;
@@ -1628,6 +1632,7 @@ int make_patches(int N, int E, const int32_t* conn, const std::vector<int32_t>& 
     sp.csrp_off = (int)rcp.size();
     sp.csr_off = (int)rcs.size();
     sp.scene = node_scene[ow[0]];
+    sp.body = node_body[ow[0]];
     for (int i = 0; i < sp.no; ++i) {
       loc[ow[i]] = i;
       rn.push_back(ow[i]);
@@ -2097,6 +2102,7 @@ __global__ void k_arena_reloc(Dev d, ArenaReloc r) {
       sp.csrp_off += r.cp0;
       sp.csr_off += 3 * r.e0;
       sp.scene = r.s;
+      sp.body += r.b0;
     }
   }
 }
@@ -3130,6 +3136,7 @@ int fw_finalize(fw_ctx* c) {
       (rc = upload(c, &d.j2par, j2par)) || (rc = dalloc(c, &d.j2state, has_j2 ? E : 1)) ||
       (rc = dalloc(c, &d.ndmass, E)) || (rc = dalloc(c, &d.corner, 3 * (size_t)E)) ||
       (rc = upload(c, &d.body_scene, c->h_scene)) || (rc = upload(c, &d.body_pair_off, poff)) ||
+      (rc = dalloc(c, &d.body_lm, B)) ||
       (rc = upload(c, &d.body_pair_cnt, pcnt)) || (rc = upload(c, &d.pairs, pairs)) ||
       (rc = dalloc(c, &d.pair_active, pairs.size())) || (rc = upload(c, &d.heights, c->h_heights)) ||
       (rc = upload(c, &d.occ, c->h_occ)) || (rc = dalloc(c, &d.scene_dt, S)) ||
@@ -3467,6 +3474,7 @@ int fw_arena_init(fw_ctx* c, int64_t max_nodes, int64_t max_elems, int32_t max_b
       (rc = dalloc(c, &d.j2par, E)) || (rc = dalloc(c, &d.j2state, E)) || (rc = dalloc(c, &d.ndmass, E)) ||
       (rc = dalloc(c, &d.corner, 3 * E)) || (rc = dalloc(c, &d.body_scene, B)) ||
       (rc = dalloc(c, &d.body_pair_off, B)) || (rc = dalloc(c, &d.body_pair_cnt, B)) ||
+      (rc = dalloc(c, &d.body_lm, B)) ||
       (rc = dalloc(c, &d.pairs, max_pairs)) || (rc = dalloc(c, &d.pair_active, max_pairs)) ||
       (rc = dalloc(c, &d.heights, max_heights)) || (rc = dalloc(c, &d.occ, max_occ)) ||
       (rc = dalloc(c, &d.scene_dt, S)) || (rc = dalloc(c, &d.scene_damp, S)) ||
@@ -3675,8 +3683,8 @@ int fw_arena_commit_pack(fw_ctx* c, const fw_pack* pk, int32_t* scene_out) {
   c->launches += 3;
   if (c->a_stream) {
     if (a.nt > 0)
-      k_stream_elems<<<(int)((a.nt + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->sd.eid + a.t0,
-                                                                                    c->sd.elem + a.t0, (int)a.nt);
+      k_stream_elems<<<(int)((a.nt + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(
+          d, c->sd.eid + a.t0, c->sd.conn + a.t0, c->sd.elem + a.t0, nullptr, (int)a.nt);
     k_stream_nodes<<<(int)((a.nn + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(d, c->sd.nodes + n0,
                                                                                   c->sd.node + n0, (int)a.nn);
     c->launches += 2;
@@ -3825,7 +3833,14 @@ int fw_set_element_young(fw_ctx* c, int32_t first, int32_t count, const float* y
   k_set_young<<<(count + kBlock - 1) / kBlock, kBlock, 0, c->stream>>>(c->d, dst, c->d_poisson, first, first + count);
   c->launches += 1;
   if ((rc = check_kernel(c, "set young"))) return rc;
-  return c->path == FW_PATH_STREAM ? stream_records(c) : FW_OK;
+  if (c->path != FW_PATH_STREAM) return FW_OK;
+  // a body's triangles may now differ: the stream records take their Lame
+  // constants per triangle from here on
+  if (!c->sd.lm) {
+    if ((rc = dalloc(c, &c->sd.lm, (size_t)std::max(1, c->st_ne)))) return rc;
+    drop_graphs(c);
+  }
+  return stream_records(c);
 }
 
 int fw_adj_begin(fw_ctx* c, int32_t max_segment_steps) {
