@@ -538,8 +538,11 @@ int fw_arena_scene_info(fw_ctx* ctx, int32_t scene, int64_t* info);
  *                             checkpoint first with fw_restore) recompute n
  *                             substeps, then run them backward
  *   fw_adj_read(ctx, xb, vb, Eb) dL/dx, dL/dv at the segment start; dL/dE
- * Covers Elastic and NeoHookean triangles, plane contact, gravity / nodal
- * force / fixed / enforced-velocity BCs. */
+ * Covers Elastic, NeoHookean and J2 triangles (the plastic state carried
+ * backward), plane, height-field and voxel contact (penalty and velocity
+ * damping), gravity / nodal force / fixed / enforced-velocity / enforced-
+ * acceleration BCs; refuses FEM-FEM contact, spring-mass domains, rigid bodies,
+ * worlds of several scenes, arenas and the stream path. */
 int fw_set_element_young(fw_ctx* ctx, int32_t first, int32_t count, const float* young,
                          int32_t on_device);
 int fw_adj_begin(fw_ctx* ctx, int32_t max_segment_steps);
